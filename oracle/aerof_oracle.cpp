@@ -1,0 +1,1429 @@
+// aerof_oracle.cpp -- CPU restatement of AERO-F's implicit edge-based
+// finite-volume hot path, used ONLY as test infrastructure: the checker in
+// tests/, the CPU baseline leg of bench.py and __graft_entry__.smoke().
+// Nothing in the product links, loads or calls this file.
+//
+// Parity status: the reconstruction (RecFcnVanAlbada/RecFcnLinear) and gas
+// conversions (VarFcnSGEuler) are pinned against golden vectors produced by
+// the reference's own headers (oracle/ref_golden.cpp -> tests/golden/).  The
+// Fortran kernels (roeflux7.f, boundflux5.f, roejac6.f) cannot be compiled
+// here (no Fortran compiler), so they are pinned by self-consistency only:
+// free-stream preservation, flux antisymmetry/consistency and FD checks.
+//
+// Every function follows one reference routine, cited as file:line (paths
+// relative to the AERO-F source tree).  Operation order follows the
+// reference's source order, including Fortran left-to-right evaluation, so
+// that a double instantiation reproduces the reference's arithmetic.
+// Everything is templated on the scalar type: T=double is the reference
+// arithmetic, T=Dual gives exact forward-mode derivatives of the same code
+// (used to check the GPU's Jacobian-vector and dR/dX kernels).
+//
+// Build: g++ -O3 -march=native -fopenmp -ffp-contract=off -shared -fPIC
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace orc {
+
+// ---------------------------------------------------------------- dual type
+struct Dual {
+  double v, d;
+  Dual() : v(0), d(0) {}
+  Dual(double a) : v(a), d(0) {}
+  Dual(double a, double b) : v(a), d(b) {}
+};
+inline Dual operator+(Dual a, Dual b) { return Dual(a.v + b.v, a.d + b.d); }
+inline Dual operator-(Dual a, Dual b) { return Dual(a.v - b.v, a.d - b.d); }
+inline Dual operator-(Dual a) { return Dual(-a.v, -a.d); }
+inline Dual operator*(Dual a, Dual b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
+inline Dual operator/(Dual a, Dual b) {
+  double q = a.v / b.v;
+  return Dual(q, (a.d - q * b.d) / b.v);
+}
+inline Dual& operator+=(Dual& a, Dual b) { a = a + b; return a; }
+inline Dual& operator-=(Dual& a, Dual b) { a = a - b; return a; }
+inline Dual& operator*=(Dual& a, Dual b) { a = a * b; return a; }
+inline bool operator>(Dual a, Dual b) { return a.v > b.v; }
+inline bool operator<(Dual a, Dual b) { return a.v < b.v; }
+inline bool operator>=(Dual a, Dual b) { return a.v >= b.v; }
+inline bool operator<=(Dual a, Dual b) { return a.v <= b.v; }
+inline bool operator==(Dual a, Dual b) { return a.v == b.v; }
+inline Dual sqrt(Dual a) { double s = std::sqrt(a.v); return Dual(s, a.d / (2.0 * s)); }
+inline Dual fabs(Dual a) { return a.v < 0 ? -a : a; }
+inline double val(double a) { return a; }
+inline double val(Dual a) { return a.v; }
+using std::sqrt;
+using std::fabs;
+template <class T> inline T tmax(T a, T b) { return val(a) < val(b) ? b : a; }
+template <class T> inline T tmin(T a, T b) { return val(b) < val(a) ? b : a; }
+
+// ---------------------------------------------------------------- constants
+constexpr int BC_SLIP_WALL_MOVING = -2;
+constexpr int BC_INLET_MOVING = -4;
+constexpr int BC_OUTLET_MOVING = -5;
+static const double third = 1.0 / 3.0;
+static const double twelfth = 1.0 / 12.0;
+static const double sixth = 1.0 / 6.0;
+
+// ElemTet tables (ElemTetCore.C:19-21)
+static const int edgeEndTet[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+static const int edgeFaceTet[6][2] = {{0, 1}, {2, 0}, {1, 2}, {0, 3}, {3, 1}, {2, 3}};
+
+// ---------------------------------------------------------------- vec3 helpers
+template <class T> struct V3 {
+  T x[3];
+  V3() { x[0] = x[1] = x[2] = T(0.0); }
+  V3(T a, T b, T c) { x[0] = a; x[1] = b; x[2] = c; }
+  T& operator[](int i) { return x[i]; }
+  const T& operator[](int i) const { return x[i]; }
+};
+template <class T> inline V3<T> operator+(const V3<T>& a, const V3<T>& b) { return V3<T>(a[0] + b[0], a[1] + b[1], a[2] + b[2]); }
+template <class T> inline V3<T> operator-(const V3<T>& a, const V3<T>& b) { return V3<T>(a[0] - b[0], a[1] - b[1], a[2] - b[2]); }
+template <class T> inline V3<T> operator*(double c, const V3<T>& a) { return V3<T>(c * a[0], c * a[1], c * a[2]); }
+// Vec3D::operator^ (Vector3D.h:266-274)
+template <class T> inline V3<T> cross(const V3<T>& a, const V3<T>& b) {
+  return V3<T>(a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]);
+}
+template <class T> inline T dot(const V3<T>& a, const V3<T>& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+// ---------------------------------------------------------------- mesh
+struct Mesh {
+  int N = 0, T = 0, F = 0, E = 0;
+  double gam = 1.4;
+  std::vector<double> X;       // [N][3]
+  std::vector<int> tets;       // [T][4]
+  std::vector<int> faces;      // [F][3]
+  std::vector<int> codes;      // [F]
+  std::vector<int> edges;      // [E][2], i<j, lexicographic
+  std::vector<int> tetEdge;    // [T][6]
+  std::vector<int> nodeEdgePtr, nodeEdgeIdx;  // node -> incident edges, ascending
+  // geometry (double instantiation)
+  std::vector<double> edgeNorm, faceNorm, ctrlVol, Rlsq;
+};
+
+// EdgeSet::find + createPointers (EdgeCore.C:55-117): edges are the unique
+// (min,max) node pairs of the elements, numbered lexicographically.
+static void build_edges(Mesh& m) {
+  std::vector<uint64_t> keys;
+  keys.reserve((size_t)m.T * 6);
+  for (int t = 0; t < m.T; ++t)
+    for (int l = 0; l < 6; ++l) {
+      uint64_t a = (uint32_t)m.tets[4 * t + edgeEndTet[l][0]];
+      uint64_t b = (uint32_t)m.tets[4 * t + edgeEndTet[l][1]];
+      if (a > b) std::swap(a, b);
+      keys.push_back((a << 32) | b);
+    }
+  std::vector<uint64_t> u(keys);
+  std::sort(u.begin(), u.end());
+  u.erase(std::unique(u.begin(), u.end()), u.end());
+  m.E = (int)u.size();
+  m.edges.resize(2 * (size_t)m.E);
+  for (int l = 0; l < m.E; ++l) {
+    m.edges[2 * l] = (int)(u[l] >> 32);
+    m.edges[2 * l + 1] = (int)(u[l] & 0xffffffffu);
+  }
+  m.tetEdge.resize((size_t)m.T * 6);
+  for (size_t k = 0; k < keys.size(); ++k)
+    m.tetEdge[k] = (int)(std::lower_bound(u.begin(), u.end(), keys[k]) - u.begin());
+  std::vector<int> cnt(m.N + 1, 0);
+  for (int l = 0; l < m.E; ++l) { cnt[m.edges[2 * l] + 1]++; cnt[m.edges[2 * l + 1] + 1]++; }
+  for (int i = 0; i < m.N; ++i) cnt[i + 1] += cnt[i];
+  m.nodeEdgePtr = cnt;
+  m.nodeEdgeIdx.resize(2 * (size_t)m.E);
+  std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+  for (int l = 0; l < m.E; ++l) {
+    m.nodeEdgeIdx[pos[m.edges[2 * l]]++] = l;
+    m.nodeEdgeIdx[pos[m.edges[2 * l + 1]]++] = l;
+  }
+}
+
+// ---------------------------------------------------------------- geometry
+// Control volumes: ElemTet::computeVolume + computeControlVolumes
+// (ElemTetCore.C:24-39, 102-112).
+// Edge normals: ElemTet::computeEdgeNormalsGCL1 (ElemTetCore.C:281-330) with
+// Xn = Xnp1 = X, the form a static mesh takes (GeoData.C:32, DistGeoState.C:
+// 565-568): n = 0.5*((xg1^xg0)+(xg1^xg0)) + 0.25*((xg1^xg0)+(xg1^xg0)).
+// Face normals: FaceTria::computeNormalGCL1 (FaceTriaCore.C:65-82), Xn=Xnp1.
+// Edge/face normal velocities are zero (DGCL IMPLICIT_ZERO velocities).
+template <class T>
+static void compute_geometry(const Mesh& m, const T* X, std::vector<T>& edgeNorm,
+                             std::vector<T>& faceNorm, std::vector<T>& ctrlVol) {
+  edgeNorm.assign(3 * (size_t)m.E, T(0.0));
+  faceNorm.assign(3 * (size_t)m.F, T(0.0));
+  ctrlVol.assign(m.N, T(0.0));
+  auto P = [&](int n) { return V3<T>(X[3 * n], X[3 * n + 1], X[3 * n + 2]); };
+  for (int t = 0; t < m.T; ++t) {
+    const int* nd = &m.tets[4 * t];
+    V3<T> x[4] = {P(nd[0]), P(nd[1]), P(nd[2]), P(nd[3])};
+    V3<T> v1 = x[1] - x[0], v2 = x[2] - x[0], v3 = x[3] - x[0];
+    T volume = sixth * dot(v3, cross(v1, v2));
+    for (int j = 0; j < 4; ++j) ctrlVol[nd[j]] += 0.25 * volume;
+  }
+  for (int t = 0; t < m.T; ++t) {
+    const int* nd = &m.tets[4 * t];
+    V3<T> x[4] = {P(nd[0]), P(nd[1]), P(nd[2]), P(nd[3])};
+    V3<T> f[4];
+    f[0] = third * (x[0] + x[1] + x[2]);
+    f[1] = third * (x[0] + x[1] + x[3]);
+    f[2] = third * (x[0] + x[2] + x[3]);
+    f[3] = third * (x[1] + x[2] + x[3]);
+    V3<T> g = 0.25 * (x[0] + x[1] + x[2] + x[3]);
+    for (int l = 0; l < 6; ++l) {
+      V3<T> xg0 = f[edgeFaceTet[l][0]] - g;
+      V3<T> xg1 = f[edgeFaceTet[l][1]] - g;
+      V3<T> c = cross(xg1, xg0);
+      V3<T> n = 0.5 * (c + c) + 0.25 * (c + c);
+      int e = m.tetEdge[6 * t + l];
+      if (nd[edgeEndTet[l][0]] < nd[edgeEndTet[l][1]]) {
+        for (int k = 0; k < 3; ++k) edgeNorm[3 * e + k] += n[k];
+      } else {
+        for (int k = 0; k < 3; ++k) edgeNorm[3 * e + k] -= n[k];
+      }
+    }
+  }
+  for (int f = 0; f < m.F; ++f) {
+    const int* nd = &m.faces[3 * f];
+    V3<T> x0 = P(nd[0]), x1 = P(nd[1]), x2 = P(nd[2]);
+    V3<T> x01 = x1 - x0, x02 = x2 - x0;
+    V3<T> a = 2.0 * x02 + x02;
+    V3<T> s = cross(a, x01) + cross(a, x01);
+    V3<T> n = twelfth * s;
+    for (int k = 0; k < 3; ++k) faceNorm[3 * f + k] = n[k];
+  }
+}
+
+// SubDomain::computeWeightsLeastSquaresEdgePart (SubDomainCore.C:1334-1381)
+// and NodePart (SubDomainCore.C:1755-1777): R = upper Cholesky factor of
+// sum_j dx dx^T, stored (r11,r12,r13,r22,r23,r33).
+template <class T>
+static void compute_lsq_R(const Mesh& m, const T* X, std::vector<T>& R) {
+  R.assign(6 * (size_t)m.N, T(0.0));
+  for (int l = 0; l < m.E; ++l) {
+    int i = m.edges[2 * l], j = m.edges[2 * l + 1];
+    T dx[3] = {X[3 * j] - X[3 * i], X[3 * j + 1] - X[3 * i + 1], X[3 * j + 2] - X[3 * i + 2]};
+    T dxdx = dx[0] * dx[0], dydy = dx[1] * dx[1], dzdz = dx[2] * dx[2];
+    T dxdy = dx[0] * dx[1], dxdz = dx[0] * dx[2], dydz = dx[1] * dx[2];
+    R[6 * i + 0] += dxdx; R[6 * j + 0] += dxdx;
+    R[6 * i + 1] += dxdy; R[6 * j + 1] += dxdy;
+    R[6 * i + 2] += dxdz; R[6 * j + 2] += dxdz;
+    R[6 * i + 3] += dydy; R[6 * j + 3] += dydy;
+    R[6 * i + 4] += dydz; R[6 * j + 4] += dydz;
+    R[6 * i + 5] += dzdz; R[6 * j + 5] += dzdz;
+  }
+  for (int i = 0; i < m.N; ++i) {
+    T* r = &R[6 * i];
+    T r11 = sqrt(r[0]);
+    T or11 = 1.0 / r11;
+    T r12 = r[1] * or11;
+    T r13 = r[2] * or11;
+    T r22 = sqrt(r[3] - r12 * r12);
+    T r23 = (r[4] - r12 * r13) / r22;
+    T r33 = sqrt(r[5] - (r13 * r13 + r23 * r23));
+    r[0] = r11; r[1] = r12; r[2] = r13; r[3] = r22; r[4] = r23; r[5] = r33;
+  }
+}
+
+// computeLocalWeightsLeastSquares (SubDomain.C:137-159)
+template <class T>
+static inline void lsq_weights(const T dx[3], const T* R, T W[3]) {
+  T or11 = 1.0 / R[0];
+  T or22 = 1.0 / R[3];
+  T or33 = 1.0 / R[5];
+  T r12or11 = R[1] * or11;
+  T r23or22 = R[4] * or22;
+  T psi = (R[1] * R[4] - R[2] * R[3]) * or11 * or22;
+  T alpha1 = dx[0] * or11 * or11;
+  T alpha2 = (dx[1] - r12or11 * dx[0]) * or22 * or22;
+  T alpha3 = (dx[2] - r23or22 * dx[1] + psi * dx[0]) * or33 * or33;
+  W[0] = alpha1 - r12or11 * alpha2 + psi * alpha3;
+  W[1] = alpha2 - r23or22 * alpha3;
+  W[2] = alpha3;
+}
+
+// VarFcnSGEuler::conservativeToPrimitive (VarFcnSGEuler.h:307-327), Pstiff=0
+template <class T>
+static inline void cons2prim(double gam, const T* U, T* V) {
+  V[0] = U[0];
+  T invRho = 1.0 / U[0];
+  V[1] = U[1] * invRho;
+  V[2] = U[2] * invRho;
+  V[3] = U[3] * invRho;
+  T vel2 = V[1] * V[1] + V[2] * V[2] + V[3] * V[3];
+  V[4] = (gam - 1.0) * (U[4] - 0.5 * U[0] * vel2) - gam * 0.0;
+}
+
+// SubDomain::computeGradientsLeastSquares (SubDomain.C:297-374)
+template <class T>
+static void compute_gradients(const Mesh& m, const T* X, const T* R, const T* V,
+                              T* ddx, T* ddy, T* ddz) {
+  for (size_t k = 0; k < 5 * (size_t)m.N; ++k) ddx[k] = ddy[k] = ddz[k] = T(0.0);
+  for (int l = 0; l < m.E; ++l) {
+    int i = m.edges[2 * l], j = m.edges[2 * l + 1];
+    T Wi[3], Wj[3];
+    T dx[3] = {X[3 * j] - X[3 * i], X[3 * j + 1] - X[3 * i + 1], X[3 * j + 2] - X[3 * i + 2]};
+    lsq_weights(dx, &R[6 * i], Wi);
+    dx[0] = -dx[0]; dx[1] = -dx[1]; dx[2] = -dx[2];
+    lsq_weights(dx, &R[6 * j], Wj);
+    for (int k = 0; k < 5; ++k) {
+      T dv = V[5 * j + k] - V[5 * i + k];
+      ddx[5 * i + k] += Wi[0] * dv;
+      ddy[5 * i + k] += Wi[1] * dv;
+      ddz[5 * i + k] += Wi[2] * dv;
+      ddx[5 * j + k] -= Wj[0] * dv;
+      ddy[5 * j + k] -= Wj[1] * dv;
+      ddz[5 * j + k] -= Wj[2] * dv;
+    }
+  }
+}
+
+// RecFcn::computeVanAlbadaFcn (RecFcn.h:268-281)
+template <class T>
+static inline T vanalbada_fcn(double eps, T a, T b) {
+  T a2 = a * a;
+  T b2 = b * b;
+  if (val(a * b) > 0.0) return (a * (b2 + eps) + b * (a2 + eps)) / (a2 + b2 + 2.0 * eps);
+  else if (val(a * b) == 0.0) return 0.5 * eps * (a + b) / (a2 + b2 + 2.0 * eps);
+  else return T(0.0);
+}
+
+// RecFcn constructor (RecFcn.h:40-49) and vanalbada (RecFcn.h:432-446),
+// linear (RecFcn.h:240-249); beta = 1/3 (IoDataCore.C:2425).
+struct RecParams {
+  double beta, beta1, beta2, eps0;
+};
+static inline RecParams rec_params(double beta) {
+  RecParams p;
+  p.beta = beta;
+  p.beta1 = 0.5 - beta;
+  p.beta2 = 1.0 - 2.0 * beta;
+  p.eps0 = 1.e-16;
+  return p;
+}
+template <class T>
+static inline void vanalbada(const RecParams& p, T Vi, T ddVij, T Vj, T ddVji, T& Vij, T& Vji) {
+  T dVji = Vj - Vi;
+  T dV = p.beta2 * dVji;
+  T dVi = dV + 2.0 * p.beta * ddVij;
+  T dVj = dV + 2.0 * p.beta * ddVji;
+  Vij = Vi + 0.5 * vanalbada_fcn(p.eps0, dVi, dVji);
+  Vji = Vj - 0.5 * vanalbada_fcn(p.eps0, dVj, dVji);
+}
+template <class T>
+static inline void linear_rec(const RecParams& p, T Vi, T ddVij, T Vj, T ddVji, T& Vij, T& Vji) {
+  T dV = p.beta1 * (Vj - Vi);
+  Vij = Vi + dV + p.beta * ddVij;
+  Vji = Vj - dV - p.beta * ddVji;
+}
+
+// roeflux7.f:1-202 (type 0): Roe flux with one-wave dissipation, gamma=1.
+template <class T>
+static void roeflux7(double gam, double pstiff, const T* enormal, T evitno, const T* Ug,
+                     const T* Ud, T* phi) {
+  double gam1 = gam - 1.0;
+  double invgam1 = 1.0 / gam1;
+  T rnorm = sqrt(enormal[0] * enormal[0] + enormal[1] * enormal[1] + enormal[2] * enormal[2]);
+  T invnorm = 1.0 / rnorm;
+  T normal[3] = {enormal[0] * invnorm, enormal[1] * invnorm, enormal[2] * invnorm};
+  T vitno = evitno * invnorm;
+  T vitg2 = Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3];
+  T vitd2 = Ud[1] * Ud[1] + Ud[2] * Ud[2] + Ud[3] * Ud[3];
+  T squsr1 = sqrt(Ug[0]);
+  T squsr2 = sqrt(Ud[0]);
+  T ener1 = (Ug[4] + gam * pstiff) * invgam1 + 0.5 * Ug[0] * vitg2;
+  T ener2 = (Ud[4] + gam * pstiff) * invgam1 + 0.5 * Ud[0] * vitd2;
+  T usro = 1.0 / (squsr1 + squsr2);
+  T uar2 = (squsr1 * Ug[1] + squsr2 * Ud[1]) * usro;
+  T uar3 = (squsr1 * Ug[2] + squsr2 * Ud[2]) * usro;
+  T uar4 = (squsr1 * Ug[3] + squsr2 * Ud[3]) * usro;
+  T uar5 = ((ener1 + Ug[4]) / squsr1 + (ener2 + Ud[4]) / squsr2) * usro;
+  T VdotNt = normal[0] * uar2 + normal[1] * uar3 + normal[2] * uar4;
+  T VdotN, H;
+  if (val(VdotNt - vitno) > 0) {
+    VdotN = Ug[1] * normal[0] + Ug[2] * normal[1] + Ug[3] * normal[2];
+    H = gam * (Ug[4] + pstiff) + 0.5 * gam1 * Ug[0] * vitg2;
+    H = H / (gam1 * Ug[0]);
+    phi[0] = Ug[0] * (VdotN - vitno);
+    phi[1] = phi[0] * Ug[1] + Ug[4] * normal[0];
+    phi[2] = phi[0] * Ug[2] + Ug[4] * normal[1];
+    phi[3] = phi[0] * Ug[3] + Ug[4] * normal[2];
+    phi[4] = phi[0] * H + Ug[4] * vitno;
+  } else {
+    VdotN = Ud[1] * normal[0] + Ud[2] * normal[1] + Ud[3] * normal[2];
+    H = gam * (Ud[4] + pstiff) + 0.5 * gam1 * Ud[0] * vitd2;
+    H = H / (gam1 * Ud[0]);
+    phi[0] = Ud[0] * (VdotN - vitno);
+    phi[1] = phi[0] * Ud[1] + Ud[4] * normal[0];
+    phi[2] = phi[0] * Ud[2] + Ud[4] * normal[1];
+    phi[3] = phi[0] * Ud[3] + Ud[4] * normal[2];
+    phi[4] = phi[0] * H + Ud[4] * vitno;
+  }
+  VdotN = VdotNt;
+  T qir = 0.5 * (uar2 * uar2 + uar3 * uar3 + uar4 * uar4);
+  T cr2 = gam1 * (uar5 - qir);
+  T cr = sqrt(cr2);
+  cr2 = 1.0 / cr2;
+  T vp1 = VdotN;
+  T vp4 = VdotN + cr;
+  T vp5 = VdotN - cr;
+  T r = cr;
+  T s = -cr;
+  T cr2byt = -cr;
+  T invtbeta2 = -1.0 / cr;
+  T dif1 = -Ug[0] + Ud[0];
+  T dif2 = -Ug[0] * Ug[1] + Ud[0] * Ud[1];
+  T dif3 = -Ug[0] * Ug[2] + Ud[0] * Ud[2];
+  T dif4 = -Ug[0] * Ug[3] + Ud[0] * Ud[3];
+  T dif5 = -ener1 + ener2;
+  vp1 = vp1 - vitno;
+  vp4 = vp4 - vitno;
+  vp5 = vp5 - vitno;
+  (void)vp1;
+  T flur4, flur5;
+  if (val(VdotNt - vitno) <= 0) {
+    flur4 = tmax(vp4, T(0.0)) *
+            (cr2byt * (VdotN * dif1 - normal[0] * dif2 - normal[1] * dif3 - normal[2] * dif4) +
+             gam1 * s * invtbeta2 * (qir * dif1 - uar2 * dif2 - uar3 * dif3 - uar4 * dif4 + dif5));
+    flur5 = T(0.0);
+  } else {
+    flur4 = T(0.0);
+    flur5 = -tmin(vp5, T(0.0)) *
+            (-cr2byt * (VdotN * dif1 - normal[0] * dif2 - normal[1] * dif3 - normal[2] * dif4) +
+             (-gam1 * r * invtbeta2 * (qir * dif1 - uar2 * dif2 - uar3 * dif3 - uar4 * dif4 + dif5)));
+  }
+  phi[0] = phi[0] - 0.5 * (flur4 + flur5) * cr2;
+  phi[1] = phi[1] - (normal[0] * (r * flur4 + s * flur5) + uar2 * (flur4 + flur5)) * 0.5 * cr2;
+  phi[2] = phi[2] - (normal[1] * (r * flur4 + s * flur5) + uar3 * (flur4 + flur5)) * 0.5 * cr2;
+  phi[3] = phi[3] - (normal[2] * (r * flur4 + s * flur5) + uar4 * (flur4 + flur5)) * 0.5 * cr2;
+  phi[4] = phi[4] - (VdotN * (r * flur4 + s * flur5) + uar5 * (flur4 + flur5)) * 0.5 * cr2;
+  for (int k = 0; k < 5; ++k) phi[k] = phi[k] * rnorm;
+}
+
+// boundflux5.f:1-111 (type 0): Steger-Warming far-field flux
+// A+(V)U + A-(V)Ub; ua primitive, ub conservative.
+template <class T>
+static void boundflux5(double gam, const T* normal, T sig, const T* ua, const double* ub, T* flux) {
+  double gam1 = gam - 1.0;
+  T vnx = normal[0], vny = normal[1], vnz = normal[2];
+  T cap = sqrt(vnx * vnx + vny * vny + vnz * vnz);
+  T capd1 = vnx / cap, capd2 = vny / cap, capd3 = vnz / cap;
+  T ro = ua[0];
+  T usro = 1.0 / ro;
+  T u = ua[1], v = ua[2], w = ua[3];
+  T vit = u * u + v * v + w * w;
+  T pm = ua[4];
+  T rhoE = pm / gam1 + 0.5 * ro * vit;
+  T c2 = gam * pm * usro;
+  T c = sqrt(c2);
+  T usc = 1.0 / c;
+  T cc = 0.5 * vit + c2 / gam1;
+  T unx = capd1 * u + capd2 * v + capd3 * w;
+  T vp1 = tmax(cap * unx - sig, T(0.0));
+  T vp4 = tmax(cap * (unx + c) - sig, T(0.0));
+  T vp5 = tmax(cap * (unx - c) - sig, T(0.0));
+  T vpp = vp4 + vp5;
+  T vpm = vp4 - vp5;
+  T fgp[5];
+  fgp[0] = (gam1 * ro * vp1 + 0.5 * ro * vpp) / gam;
+  fgp[1] = fgp[0] * u + 0.5 * pm * usc * capd1 * vpm;
+  fgp[2] = fgp[0] * v + 0.5 * pm * usc * capd2 * vpm;
+  fgp[3] = fgp[0] * w + 0.5 * pm * usc * capd3 * vpm;
+  fgp[4] = 0.5 * ((gam1 / gam) * ro * vit * (vp1 - 0.5 * vpp) + rhoE * vpp + ro * unx * c * vpm / gam);
+  vp1 = tmin(cap * unx - sig, T(0.0));
+  vp4 = tmin(cap * (unx + c) - sig, T(0.0));
+  vp5 = tmin(cap * (unx - c) - sig, T(0.0));
+  vpp = vp1 - 0.5 * (vp4 + vp5);
+  vpm = 0.5 * (vp5 - vp4);
+  T xn1 = gam1 * usc * (-(0.5 * vit * ub[0]) + u * ub[1] + v * ub[2] + w * ub[3] - ub[4]);
+  T xn2 = unx * ub[0] - capd1 * ub[1] - capd2 * ub[2] - capd3 * ub[3];
+  T ff = usc * (vpp * xn1 + vpm * xn2);
+  T gg = vpm * xn1 + vpp * xn2;
+  T fgm[5];
+  fgm[0] = vp1 * ub[0] + ff;
+  fgm[1] = vp1 * ub[1] + u * ff + capd1 * gg;
+  fgm[2] = vp1 * ub[2] + v * ff + capd2 * gg;
+  fgm[3] = vp1 * ub[3] + w * ff + capd3 * gg;
+  fgm[4] = vp1 * ub[4] + cc * ff + unx * gg;
+  for (int k = 0; k < 5; ++k) flux[k] = fgp[k] + fgm[k];
+}
+
+// FluxFcnSGWallEuler3D::compute (FluxFcnDescSG.C:779-789)
+template <class T>
+static inline void wallflux(const T* normal, T normalVel, const T* V, T* flux) {
+  flux[0] = T(0.0);
+  flux[1] = V[4] * normal[0];
+  flux[2] = V[4] * normal[1];
+  flux[3] = V[4] * normal[2];
+  flux[4] = V[4] * normalVel;
+}
+
+template <class T>
+static inline void face_flux(double gam, int code, const T* n3, const T* V, const double* Ub, T* flux) {
+  if (code == BC_SLIP_WALL_MOVING) wallflux(n3, T(0.0), V, flux);
+  else boundflux5(gam, n3, T(0.0), V, Ub, flux);
+}
+
+// ---------------------------------------------------------------- residual
+// SpaceOperator::computeResidual (SpaceOperator.C:524-634) restricted to the
+// Euler / finite-volume / NONDESCRIPTOR path:
+//   R=0; V=prim(U); [LSQ gradients]; edge loop (Edge.C:371-439) with
+//   reconstruction, positivity check (EdgeCore.C:137-168), Roe flux; face
+//   loop (Face.C:354-389, 1185-1215) with subface normals n_f/3
+//   (FaceTriaCore.C:288-308); R *= 1/ctrlVol (SpaceOperator.C:614-620).
+// order: 1 = RecFcnConstant, 2 = LSQ + van Albada, 3 = LSQ + linear.
+// Failsafe (Domain.C:876-918): when failsafe != 0 and a reconstructed
+// density/pressure is non-positive, the offending nodes are tagged, their
+// gradients zeroed, and the edge loop is re-run.  Returns the number of
+// non-positive reconstructed states of the first pass.
+template <class T>
+struct Work {
+  std::vector<T> V, ddx, ddy, ddz;
+};
+
+template <class T>
+static int residual_t(const Mesh& m, const T* X, const std::vector<T>& edgeNorm,
+                      const std::vector<T>& faceNorm, const std::vector<T>& ctrlVol,
+                      const std::vector<T>& Rlsq, const T* U, const double* Ub, int order,
+                      double beta, int failsafe, T* R, Work<T>& w) {
+  const double gam = m.gam;
+  const int N = m.N;
+  w.V.resize(5 * (size_t)N);
+  for (int i = 0; i < N; ++i) cons2prim(gam, &U[5 * i], &w.V[5 * i]);
+  const T* V = w.V.data();
+  if (order > 1) {
+    w.ddx.resize(5 * (size_t)N); w.ddy.resize(5 * (size_t)N); w.ddz.resize(5 * (size_t)N);
+    compute_gradients(m, X, Rlsq.data(), V, w.ddx.data(), w.ddy.data(), w.ddz.data());
+  }
+  RecParams rp = rec_params(order == 1 ? 0.0 : beta);
+  std::vector<char> tag;
+  int ierr_first = 0;
+  for (int pass = 0; pass < 2; ++pass) {
+    for (size_t k = 0; k < 5 * (size_t)N; ++k) R[k] = T(0.0);
+    int ierr = 0;
+    for (int l = 0; l < m.E; ++l) {
+      int i = m.edges[2 * l], j = m.edges[2 * l + 1];
+      T dx[3] = {X[3 * j] - X[3 * i], X[3 * j + 1] - X[3 * i + 1], X[3 * j + 2] - X[3 * i + 2]};
+      T Vi[5], Vj[5];
+      if (order == 1) {
+        for (int k = 0; k < 5; ++k) { Vi[k] = V[5 * i + k]; Vj[k] = V[5 * j + k]; }
+      } else {
+        for (int k = 0; k < 5; ++k) {
+          T ddVij = dx[0] * w.ddx[5 * i + k] + dx[1] * w.ddy[5 * i + k] + dx[2] * w.ddz[5 * i + k];
+          T ddVji = dx[0] * w.ddx[5 * j + k] + dx[1] * w.ddy[5 * j + k] + dx[2] * w.ddz[5 * j + k];
+          if (order == 2) vanalbada(rp, V[5 * i + k], ddVij, V[5 * j + k], ddVji, Vi[k], Vj[k]);
+          else linear_rec(rp, V[5 * i + k], ddVij, V[5 * j + k], ddVji, Vi[k], Vj[k]);
+        }
+      }
+      // VarFcnSGEuler::checkReconstructedValues (VarFcnSGEuler.h:90-110)
+      bool bi = val(Vi[0]) <= 0.0 || val(Vi[4]) + 0.0 <= 0.0;
+      bool bj = val(Vj[0]) <= 0.0 || val(Vj[4]) + 0.0 <= 0.0;
+      if (bi || bj) {
+        ierr += (int)bi + (int)bj;
+        if (pass == 0 && failsafe) {
+          if (tag.empty()) tag.assign(N, 0);
+          if (bi) tag[i] = 1;
+          if (bj) tag[j] = 1;
+        }
+        continue;
+      }
+      const T* nl = &edgeNorm[3 * l];
+      T nn = sqrt(nl[0] * nl[0] + nl[1] * nl[1] + nl[2] * nl[2]);
+      if (val(nn) < 1e-18) continue;
+      T flux[5];
+      roeflux7(gam, 0.0, nl, T(0.0), Vi, Vj, flux);
+      for (int k = 0; k < 5; ++k) { R[5 * i + k] += flux[k]; R[5 * j + k] -= flux[k]; }
+    }
+    if (pass == 0) ierr_first = ierr;
+    if (pass == 0 && ierr && failsafe && order > 1) {
+      for (int i = 0; i < N; ++i)
+        if (tag[i])
+          for (int k = 0; k < 5; ++k) w.ddx[5 * i + k] = w.ddy[5 * i + k] = w.ddz[5 * i + k] = T(0.0);
+      continue;
+    }
+    break;
+  }
+  for (int f = 0; f < m.F; ++f) {
+    T n3[3] = {third * faceNorm[3 * f], third * faceNorm[3 * f + 1], third * faceNorm[3 * f + 2]};
+    for (int l = 0; l < 3; ++l) {
+      int nd = m.faces[3 * f + l];
+      T flux[5];
+      face_flux(gam, m.codes[f], n3, &V[5 * nd], Ub, flux);
+      for (int k = 0; k < 5; ++k) R[5 * nd + k] += flux[k];
+    }
+  }
+  for (int i = 0; i < N; ++i) {
+    T invcv = 1.0 / ctrlVol[i];
+    for (int k = 0; k < 5; ++k) R[5 * i + k] *= invcv;
+  }
+  return ierr_first;
+}
+
+// Threaded second-order residual for the CPU baseline timing: the edge list
+// is cut into nthreads contiguous chunks, each accumulated into a private
+// array and summed in chunk order, the way AERO-F's OpenMP loop over
+// subdomains accumulates per-subdomain arrays that CommPattern then adds
+// (Domain.C:868-928).
+static void residual_threaded(const Mesh& m, const double* U, const double* Ub, int order,
+                              double beta, int nthreads, double* R,
+                              std::vector<double>& V, std::vector<double>& G,
+                              std::vector<double>& priv) {
+  const int N = m.N, E = m.E;
+  const double gam = m.gam;
+  V.resize(5 * (size_t)N);
+  G.resize(15 * (size_t)N);
+  priv.resize((size_t)nthreads * 15 * N);
+  const double* X = m.X.data();
+  RecParams rp = rec_params(order == 1 ? 0.0 : beta);
+#pragma omp parallel num_threads(nthreads)
+  {
+#ifdef _OPENMP
+    int t = omp_get_thread_num();
+#else
+    int t = 0;
+#endif
+    int l0 = (int)((int64_t)E * t / nthreads), l1 = (int)((int64_t)E * (t + 1) / nthreads);
+#pragma omp for schedule(static)
+    for (int i = 0; i < N; ++i) cons2prim(gam, &U[5 * i], &V[5 * i]);
+    if (order > 1) {
+      double* g = &priv[(size_t)t * 15 * N];
+      std::memset(g, 0, sizeof(double) * 15 * (size_t)N);
+      for (int l = l0; l < l1; ++l) {
+        int i = m.edges[2 * l], j = m.edges[2 * l + 1];
+        double Wi[3], Wj[3];
+        double dx[3] = {X[3 * j] - X[3 * i], X[3 * j + 1] - X[3 * i + 1], X[3 * j + 2] - X[3 * i + 2]};
+        lsq_weights(dx, &m.Rlsq[6 * i], Wi);
+        dx[0] = -dx[0]; dx[1] = -dx[1]; dx[2] = -dx[2];
+        lsq_weights(dx, &m.Rlsq[6 * j], Wj);
+        for (int k = 0; k < 5; ++k) {
+          double dv = V[5 * j + k] - V[5 * i + k];
+          g[15 * i + k] += Wi[0] * dv; g[15 * i + 5 + k] += Wi[1] * dv; g[15 * i + 10 + k] += Wi[2] * dv;
+          g[15 * j + k] -= Wj[0] * dv; g[15 * j + 5 + k] -= Wj[1] * dv; g[15 * j + 10 + k] -= Wj[2] * dv;
+        }
+      }
+#pragma omp barrier
+#pragma omp for schedule(static)
+      for (int i = 0; i < N; ++i)
+        for (int k = 0; k < 15; ++k) {
+          double s = 0.0;
+          for (int q = 0; q < nthreads; ++q) s += priv[(size_t)q * 15 * N + 15 * i + k];
+          G[15 * i + k] = s;
+        }
+    }
+    double* r = &priv[(size_t)t * 15 * N];
+#pragma omp barrier
+    std::memset(r, 0, sizeof(double) * 5 * (size_t)N);
+    for (int l = l0; l < l1; ++l) {
+      int i = m.edges[2 * l], j = m.edges[2 * l + 1];
+      double Vi[5], Vj[5];
+      if (order == 1) {
+        for (int k = 0; k < 5; ++k) { Vi[k] = V[5 * i + k]; Vj[k] = V[5 * j + k]; }
+      } else {
+        double dx[3] = {X[3 * j] - X[3 * i], X[3 * j + 1] - X[3 * i + 1], X[3 * j + 2] - X[3 * i + 2]};
+        for (int k = 0; k < 5; ++k) {
+          double ddVij = dx[0] * G[15 * i + k] + dx[1] * G[15 * i + 5 + k] + dx[2] * G[15 * i + 10 + k];
+          double ddVji = dx[0] * G[15 * j + k] + dx[1] * G[15 * j + 5 + k] + dx[2] * G[15 * j + 10 + k];
+          vanalbada(rp, V[5 * i + k], ddVij, V[5 * j + k], ddVji, Vi[k], Vj[k]);
+        }
+      }
+      double flux[5];
+      roeflux7(gam, 0.0, &m.edgeNorm[3 * l], 0.0, Vi, Vj, flux);
+      for (int k = 0; k < 5; ++k) { r[5 * i + k] += flux[k]; r[5 * j + k] -= flux[k]; }
+    }
+    if (t == 0) {
+      for (int f = 0; f < m.F; ++f) {
+        double n3[3] = {third * m.faceNorm[3 * f], third * m.faceNorm[3 * f + 1], third * m.faceNorm[3 * f + 2]};
+        for (int l = 0; l < 3; ++l) {
+          int nd = m.faces[3 * f + l];
+          double flux[5];
+          face_flux(gam, m.codes[f], n3, &V[5 * nd], Ub, flux);
+          for (int k = 0; k < 5; ++k) r[5 * nd + k] += flux[k];
+        }
+      }
+    }
+#pragma omp barrier
+#pragma omp for schedule(static)
+    for (int i = 0; i < N; ++i) {
+      double invcv = 1.0 / m.ctrlVol[i];
+      for (int k = 0; k < 5; ++k) {
+        double s = 0.0;
+        for (int q = 0; q < nthreads; ++q) s += priv[(size_t)q * 15 * N + 5 * i + k];
+        R[5 * i + k] = s * invcv;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- time step
+// EdgeSet::computeTimeStep (Edge.C:87-143), Face::computeTimeStep
+// (Face.C:242-289) and the dt formula of Domain::computeTimeStep
+// (Domain.C:70-96): dt_i = cfl*vol_i / (-idti_i), beta = 1 (no low-Mach
+// preconditioning, LowMachPrec.h:89-92).
+static void timestep(const Mesh& m, const double* U, double cfl, double* dt) {
+  const double gam = m.gam;
+  std::vector<double> V(5 * (size_t)m.N), idti(m.N, 0.0);
+  for (int i = 0; i < m.N; ++i) cons2prim(gam, &U[5 * i], &V[5 * i]);
+  const double locbeta = 1.0, beta2 = locbeta * locbeta;
+  for (int l = 0; l < m.E; ++l) {
+    int i = m.edges[2 * l], j = m.edges[2 * l + 1];
+    const double* nl = &m.edgeNorm[3 * l];
+    double S = std::sqrt(nl[0] * nl[0] + nl[1] * nl[1] + nl[2] * nl[2]);
+    double invS = 1.0 / S;
+    double n[3] = {invS * nl[0], invS * nl[1], invS * nl[2]};
+    double ndot = invS * 0.0;
+    double Vmid[5];
+    for (int k = 0; k < 5; ++k) Vmid[k] = 0.5 * (V[5 * i + k] + V[5 * j + k]);
+    double a = std::sqrt(gam * (Vmid[4] + 0.0) / Vmid[0]);
+    double un = Vmid[1] * n[0] + Vmid[2] * n[1] + Vmid[3] * n[2] - ndot;
+    double coeff1 = (1.0 + beta2) * un;
+    double coeff2 = std::pow(std::pow((1.0 - beta2) * un, 2.0) + std::pow(2.0 * locbeta * a, 2.0), 0.5);
+    idti[i] += std::min(0.5 * (coeff1 - coeff2), 0.0) * S;
+    idti[j] += std::min(0.5 * (-coeff1 - coeff2), 0.0) * S;
+  }
+  for (int f = 0; f < m.F; ++f) {
+    const double* nf = &m.faceNorm[3 * f];
+    double S = std::sqrt(nf[0] * nf[0] + nf[1] * nf[1] + nf[2] * nf[2]);
+    double invS = 1.0 / S;
+    double n[3] = {invS * nf[0], invS * nf[1], invS * nf[2]};
+    double ndot = invS * 0.0;
+    for (int l = 0; l < 3; ++l) {
+      int nd = m.faces[3 * f + l];
+      const double* v = &V[5 * nd];
+      double a = std::sqrt(gam * (v[4] + 0.0) / v[0]);
+      double un = v[1] * n[0] + v[2] * n[1] + v[3] * n[2] - ndot;
+      double coeff1 = (1.0 + beta2) * un;
+      double coeff2 = std::pow(std::pow((1.0 - beta2) * un, 2.0) + std::pow(2.0 * locbeta * a, 2.0), 0.5);
+      idti[nd] += std::min(0.5 * (coeff1 - coeff2), 0.0) * S / 3;
+    }
+  }
+  for (int i = 0; i < m.N; ++i) dt[i] = cfl * m.ctrlVol[i] / (-1.0 * idti[i] + 0.0 * 0.0);
+}
+
+// ---------------------------------------------------------------- Jacobians
+// VarFcnSGEuler::computedVdU (VarFcnSGEuler.h:588-603) and
+// VarFcnBase::postMultiplyBydVdU (VarFcnBase.h:372-400).
+static void post_dVdU(double gam, const double* V, const double* mat, double* res) {
+  double gam1 = gam - 1.0;
+  double d[25] = {0};
+  double invrho = 1.0 / V[0];
+  d[0] = 1.0;
+  d[5] = -invrho * V[1]; d[6] = invrho;
+  d[10] = -invrho * V[2]; d[12] = invrho;
+  d[15] = -invrho * V[3]; d[18] = invrho;
+  d[20] = gam1 * 0.5 * (V[1] * V[1] + V[2] * V[2] + V[3] * V[3]);
+  d[21] = -gam1 * V[1]; d[22] = -gam1 * V[2]; d[23] = -gam1 * V[3]; d[24] = gam1;
+  for (int r = 0; r < 5; ++r) {
+    const double* m = &mat[5 * r];
+    double* o = &res[5 * r];
+    o[0] = m[0] * d[0] + m[1] * d[5] + m[2] * d[10] + m[3] * d[15] + m[4] * d[20];
+    o[1] = m[1] * d[6] + m[4] * d[21];
+    o[2] = m[2] * d[12] + m[4] * d[22];
+    o[3] = m[3] * d[18] + m[4] * d[23];
+    o[4] = m[4] * d[24];
+  }
+}
+
+// roejac6.f:1-316 with type=0, prec=0 (beta=1), dissipation gamma=1.
+static void roejac6(double gamma, double gam, double pstiff, const double* enormal, double evitno,
+                    const double* Ug, const double* Ud, double* jac, int sw) {
+  double gam1 = gam - 1.0;
+  double rnorm = std::sqrt(enormal[0] * enormal[0] + enormal[1] * enormal[1] + enormal[2] * enormal[2]);
+  double invnorm = 1.0 / rnorm;
+  double normal[3] = {enormal[0] * invnorm, enormal[1] * invnorm, enormal[2] * invnorm};
+  double vitno = evitno * invnorm;
+  double H[5][5], tmw[5][5], dmat[5][5];
+  double VdotN = Ug[1] * normal[0] + Ug[2] * normal[1] + Ug[3] * normal[2];
+  double qir = 0.5 * (Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3]);
+  double enth = gam * (Ug[4] + pstiff) + gam1 * Ug[0] * qir;
+  enth = enth / (gam1 * Ug[0]);
+  H[0][0] = -vitno; H[0][1] = normal[0]; H[0][2] = normal[1]; H[0][3] = normal[2]; H[0][4] = 0.0;
+  H[1][0] = gam1 * normal[0] * qir - Ug[1] * VdotN;
+  H[1][1] = (1.0 - gam1) * normal[0] * Ug[1] + VdotN - vitno;
+  H[1][2] = -gam1 * normal[0] * Ug[2] + Ug[1] * normal[1];
+  H[1][3] = -gam1 * normal[0] * Ug[3] + Ug[1] * normal[2];
+  H[1][4] = gam1 * normal[0];
+  H[2][0] = gam1 * normal[1] * qir - Ug[2] * VdotN;
+  H[2][1] = -gam1 * normal[1] * Ug[1] + Ug[2] * normal[0];
+  H[2][2] = (1.0 - gam1) * normal[1] * Ug[2] + VdotN - vitno;
+  H[2][3] = -gam1 * normal[1] * Ug[3] + Ug[2] * normal[2];
+  H[2][4] = gam1 * normal[1];
+  H[3][0] = gam1 * normal[2] * qir - Ug[3] * VdotN;
+  H[3][1] = -gam1 * normal[2] * Ug[1] + Ug[3] * normal[0];
+  H[3][2] = -gam1 * normal[2] * Ug[2] + Ug[3] * normal[1];
+  H[3][3] = (1.0 - gam1) * normal[2] * Ug[3] + VdotN - vitno;
+  H[3][4] = gam1 * normal[2];
+  H[4][0] = (gam1 * qir - enth) * VdotN;
+  H[4][1] = enth * normal[0] - gam1 * Ug[1] * VdotN;
+  H[4][2] = enth * normal[1] - gam1 * Ug[2] * VdotN;
+  H[4][3] = enth * normal[2] - gam1 * Ug[3] * VdotN;
+  H[4][4] = (1.0 + gam1) * VdotN - vitno;
+  double squsr1 = std::sqrt(Ug[0]);
+  double squsr2 = std::sqrt(Ud[0]);
+  double ener1 = (Ug[4] + gam * pstiff) / gam1 + 0.5 * Ug[0] * (Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3]);
+  double ener2 = (Ud[4] + gam * pstiff) / gam1 + 0.5 * Ud[0] * (Ud[1] * Ud[1] + Ud[2] * Ud[2] + Ud[3] * Ud[3]);
+  double usro = 1.0 / (squsr1 + squsr2);
+  double uar2 = (squsr1 * Ug[1] + squsr2 * Ud[1]) * usro;
+  double uar3 = (squsr1 * Ug[2] + squsr2 * Ud[2]) * usro;
+  double uar4 = (squsr1 * Ug[3] + squsr2 * Ud[3]) * usro;
+  double uar5 = ((ener1 + Ug[4]) / squsr1 + (ener2 + Ud[4]) / squsr2) * usro;
+  enth = uar5;
+  VdotN = normal[0] * uar2 + normal[1] * uar3 + normal[2] * uar4;
+  qir = 0.5 * (uar2 * uar2 + uar3 * uar3 + uar4 * uar4);
+  double cr2 = gam1 * (uar5 - qir);
+  double cr = std::sqrt(cr2);
+  cr2 = 1.0 / cr2;
+  double gc = gam1 / (cr * cr);
+  double usc2 = 0.5 / (cr * cr);
+  double beta = 1.0;
+  double betaRT2 = beta * beta;
+  double vp1 = VdotN;
+  double sq = std::sqrt(((1.0 - betaRT2) * VdotN) * ((1.0 - betaRT2) * VdotN) + 4.0 * betaRT2 * (cr * cr));
+  double vp4 = 0.5 * ((1.0 + betaRT2) * VdotN + sq);
+  double vp5 = 0.5 * ((1.0 + betaRT2) * VdotN - sq);
+  double rRT = vp4 - vp1 * betaRT2;
+  double sRT = vp5 - vp1 * betaRT2;
+  double tRT = 0.5 * (vp5 - vp4);
+  vp1 = std::fabs(vp1 - vitno) * gamma;
+  vp4 = std::fabs(vp4 - vitno) * gamma;
+  vp5 = std::fabs(vp5 - vitno) * gamma;
+  const double* n = normal;
+  tmw[0][0] = n[0] + n[1] * uar4 - uar3 * n[2] - gc * n[0] * qir;
+  tmw[0][1] = gc * n[0] * uar2;
+  tmw[0][2] = gc * n[0] * uar3 + n[2];
+  tmw[0][3] = gc * n[0] * uar4 - n[1];
+  tmw[0][4] = -gc * n[0];
+  tmw[1][0] = n[1] + n[2] * uar2 - uar4 * n[0] - gc * n[1] * qir;
+  tmw[1][1] = gc * n[1] * uar2 - n[2];
+  tmw[1][2] = gc * n[1] * uar3;
+  tmw[1][3] = gc * n[1] * uar4 + n[0];
+  tmw[1][4] = -gc * n[1];
+  tmw[2][0] = n[2] + n[0] * uar3 - uar2 * n[1] - gc * n[2] * qir;
+  tmw[2][1] = gc * n[2] * uar2 + n[1];
+  tmw[2][2] = gc * n[2] * uar3 - n[0];
+  tmw[2][3] = gc * n[2] * uar4;
+  tmw[2][4] = -gc * n[2];
+  double crsq = cr * cr;
+  tmw[3][0] = gam1 * qir * sRT / (betaRT2 * tRT) + VdotN * crsq / tRT;
+  tmw[3][1] = -gam1 * uar2 * sRT / (betaRT2 * tRT) - crsq * n[0] / tRT;
+  tmw[3][2] = -gam1 * uar3 * sRT / (betaRT2 * tRT) - crsq * n[1] / tRT;
+  tmw[3][3] = -gam1 * uar4 * sRT / (betaRT2 * tRT) - crsq * n[2] / tRT;
+  tmw[3][4] = gam1 * sRT / (betaRT2 * tRT);
+  tmw[4][0] = -gam1 * qir * rRT / (betaRT2 * tRT) - VdotN * crsq / tRT;
+  tmw[4][1] = gam1 * uar2 * rRT / (betaRT2 * tRT) + crsq * n[0] / tRT;
+  tmw[4][2] = gam1 * uar3 * rRT / (betaRT2 * tRT) + crsq * n[1] / tRT;
+  tmw[4][3] = gam1 * uar4 * rRT / (betaRT2 * tRT) + crsq * n[2] / tRT;
+  tmw[4][4] = -gam1 * rRT / (betaRT2 * tRT);
+  for (int j = 0; j < 5; ++j) {
+    dmat[0][j] = vp1 * (n[0] * tmw[0][j] + n[1] * tmw[1][j] + n[2] * tmw[2][j]) + vp4 * usc2 * tmw[3][j] +
+                 vp5 * usc2 * tmw[4][j];
+    dmat[1][j] = vp1 * (n[0] * uar2 * tmw[0][j] + (n[1] * uar2 - n[2]) * tmw[1][j] + (n[2] * uar2 + n[1]) * tmw[2][j]) +
+                 vp4 * (usc2 * (uar2 + rRT * n[0])) * tmw[3][j] + vp5 * (usc2 * (uar2 + sRT * n[0])) * tmw[4][j];
+    dmat[2][j] = vp1 * (n[1] * uar3 * tmw[1][j] + (n[0] * uar3 + n[2]) * tmw[0][j] + (n[2] * uar3 - n[0]) * tmw[2][j]) +
+                 vp4 * (usc2 * (uar3 + rRT * n[1])) * tmw[3][j] + vp5 * (usc2 * (uar3 + sRT * n[1])) * tmw[4][j];
+    dmat[3][j] = vp1 * (n[2] * uar4 * tmw[2][j] + (n[0] * uar4 - n[1]) * tmw[0][j] + (n[1] * uar4 + n[0]) * tmw[1][j]) +
+                 vp4 * (usc2 * (uar4 + rRT * n[2])) * tmw[3][j] + vp5 * (usc2 * (uar4 + sRT * n[2])) * tmw[4][j];
+    dmat[4][j] = vp1 * ((n[0] * qir + (n[2] * uar3 - n[1] * uar4)) * tmw[0][j] +
+                        (n[1] * qir + (n[0] * uar4 - n[2] * uar2)) * tmw[1][j] +
+                        (n[2] * qir + (n[1] * uar2 - n[0] * uar3)) * tmw[2][j]) +
+                 vp4 * (usc2 * (enth + VdotN * rRT)) * tmw[3][j] + vp5 * (usc2 * (enth + VdotN * sRT)) * tmw[4][j];
+  }
+  (void)cr2;
+  for (int i = 0; i < 5; ++i)
+    for (int k = 0; k < 5; ++k) {
+      if (sw == 1) H[i][k] = H[i][k] + dmat[i][k];
+      if (sw == 2) H[i][k] = H[i][k] - dmat[i][k];
+    }
+  for (int i = 0; i < 5; ++i)
+    for (int k = 0; k < 5; ++k) jac[5 * i + k] = 0.5 * H[i][k] * rnorm;
+}
+
+// FluxFcnFD<5>::computeJacobian (FluxFcnBase.h:112-159) around a face flux,
+// then postMultiplyBydVdU (CONSERVATIVE Jacobian type).
+static void face_jac_fd(double gam, int code, const double* n3, const double* VL, const double* Ub,
+                        double* jac) {
+  const double eps0 = 1.e-6;
+  double Veps[5], flux[5], fluxeps[5], dfdV[25];
+  face_flux(gam, code, n3, VL, Ub, flux);
+  for (int k = 0; k < 5; ++k) Veps[k] = VL[k];
+  for (int k = 0; k < 5; ++k) {
+    double eps = (std::fabs(Veps[k]) < 1.e-10) ? eps0 : eps0 * Veps[k];
+    double inveps = 1.0 / eps;
+    Veps[k] += eps;
+    if (k != 0) Veps[k - 1] = VL[k - 1];
+    face_flux(gam, code, n3, Veps, Ub, fluxeps);
+    for (int j = 0; j < 5; ++j) dfdV[5 * j + k] = (fluxeps[j] - flux[j]) * inveps;
+  }
+  post_dVdU(gam, VL, dfdV, jac);
+}
+
+// FluxFcnSGWallEuler3D::computeJacobian (FluxFcnDescSG.C:838-886)
+static void wall_jac(double gam, const double* n3, double ndot, const double* V, double* jac) {
+  double dfdV[25] = {0};
+  dfdV[9] = n3[0]; dfdV[14] = n3[1]; dfdV[19] = n3[2]; dfdV[24] = ndot;
+  post_dVdU(gam, V, dfdV, jac);
+}
+
+// H1 Jacobian in MvpMat layout a[N + 2E][25] (MvpMatrix.h:10-80):
+// EdgeSet::computeJacobianFiniteVolumeTerm (Edge.C:4472-4526) with the
+// approximate Roe Jacobians roejacappr3Dgas (FluxFcnDescSG.C:155-262),
+// Face::computeJacobianFiniteVolumeTerm (Face.C:814-847), diag *= 1/vol
+// (SubDomain.C:1760-1765), then TimeState::addToJacobianNoPrecLocal
+// (TimeState.C:731-756): A_ii += 1/dt_i (backward Euler, NONDESCRIPTOR).
+static void jacobian(const Mesh& m, const double* U, const double* Ub, const double* dt, double* A) {
+  const double gam = m.gam;
+  const int N = m.N;
+  std::vector<double> V(5 * (size_t)N);
+  for (int i = 0; i < N; ++i) cons2prim(gam, &U[5 * i], &V[5 * i]);
+  std::memset(A, 0, sizeof(double) * 25 * ((size_t)N + 2 * (size_t)m.E));
+  for (int l = 0; l < m.E; ++l) {
+    int i = m.edges[2 * l], j = m.edges[2 * l + 1];
+    const double* nl = &m.edgeNorm[3 * l];
+    double nn = std::sqrt(nl[0] * nl[0] + nl[1] * nl[1] + nl[2] * nl[2]);
+    if (nn < 1e-18) continue;
+    double n[3] = {nl[0], nl[1], nl[2]};
+    double dfdUi[25], dfdUj[25];
+    roejac6(1.0, gam, 0.0, n, 0.0, &V[5 * i], &V[5 * j], dfdUi, 1);
+    roejac6(1.0, gam, 0.0, n, 0.0, &V[5 * j], &V[5 * i], dfdUj, 2);
+    double* Aii = &A[25 * (size_t)i];
+    double* Ajj = &A[25 * (size_t)j];
+    for (int k = 0; k < 25; ++k) { Aii[k] += dfdUi[k]; Ajj[k] -= dfdUj[k]; }
+    double* Aij = &A[25 * ((size_t)N + 2 * (size_t)l)];
+    double* Aji = &A[25 * ((size_t)N + 2 * (size_t)l + 1)];
+    double voli = 1.0 / m.ctrlVol[i];
+    double volj = 1.0 / m.ctrlVol[j];
+    for (int k = 0; k < 25; ++k) { Aij[k] += dfdUj[k] * voli; Aji[k] -= dfdUi[k] * volj; }
+  }
+  for (int f = 0; f < m.F; ++f) {
+    double n3[3] = {third * m.faceNorm[3 * f], third * m.faceNorm[3 * f + 1], third * m.faceNorm[3 * f + 2]};
+    for (int l = 0; l < 3; ++l) {
+      int nd = m.faces[3 * f + l];
+      double jac[25];
+      if (m.codes[f] == BC_SLIP_WALL_MOVING) wall_jac(gam, n3, third * 0.0, &V[5 * nd], jac);
+      else face_jac_fd(gam, m.codes[f], n3, &V[5 * nd], Ub, jac);
+      double* Aii = &A[25 * (size_t)nd];
+      for (int k = 0; k < 25; ++k) Aii[k] += jac[k];
+    }
+  }
+  for (int i = 0; i < N; ++i) {
+    double voli = 1.0 / m.ctrlVol[i];
+    double* Aii = &A[25 * (size_t)i];
+    for (int k = 0; k < 25; ++k) Aii[k] *= voli;
+  }
+  if (dt) {
+    for (int i = 0; i < N; ++i) {
+      double c_np1 = 1.0 / dt[i];
+      for (int k = 0; k < 5; ++k) A[25 * (size_t)i + 6 * k] += c_np1;
+    }
+  }
+}
+
+// SubDomain::computeMatVecProdH1 / H1transpose (SubDomain.C:3916-3995) with
+// DenseMatrixOp::applyAndAddToVector (DenseMatrixOps.h:670-773).
+static void matvec(const Mesh& m, const double* A, const double* p, double* y, int transpose) {
+  const int N = m.N;
+  for (size_t k = 0; k < 5 * (size_t)N; ++k) y[k] = 0.0;
+  auto apply = [&](const double* a, const double* x, double* o) {
+    for (int r = 0; r < 5; ++r) {
+      double s = 0.0;
+      for (int c = 0; c < 5; ++c) s += a[5 * r + c] * x[c];
+      o[r] += s;
+    }
+  };
+  auto applyT = [&](const double* a, const double* x, double* o) {
+    for (int r = 0; r < 5; ++r) {
+      double s = 0.0;
+      for (int c = 0; c < 5; ++c) s += a[5 * c + r] * x[c];
+      o[r] += s;
+    }
+  };
+  for (int i = 0; i < N; ++i) {
+    if (!transpose) apply(&A[25 * (size_t)i], &p[5 * i], &y[5 * i]);
+    else applyT(&A[25 * (size_t)i], &p[5 * i], &y[5 * i]);
+  }
+  for (int l = 0; l < m.E; ++l) {
+    int i = m.edges[2 * l], j = m.edges[2 * l + 1];
+    const double* aij = &A[25 * ((size_t)N + 2 * (size_t)l)];
+    const double* aji = &A[25 * ((size_t)N + 2 * (size_t)l + 1)];
+    if (!transpose) {
+      apply(aij, &p[5 * j], &y[5 * i]);
+      apply(aji, &p[5 * i], &y[5 * j]);
+    } else {
+      applyT(aij, &p[5 * i], &y[5 * j]);
+      applyT(aji, &p[5 * j], &y[5 * i]);
+    }
+  }
+}
+
+// invertDenseMatrix (DenseMatrixOps.h:1164-1185): LINPACK dgefa (Gaussian
+// elimination, partial pivoting) + dgedi (inverse) on the transposed block.
+// Returns the LINPACK info code (k>0: zero pivot at step k).
+template <class S>
+static int invert5(S* a) {
+  const int n = 5;
+  S t_[25];
+  for (int r = 0; r < 5; ++r)
+    for (int c = 0; c < 5; ++c) t_[5 * c + r] = a[5 * r + c];
+  // column-major view: A(r,c) = t_[r + 5*c]
+  auto A = [&](int r, int c) -> S& { return t_[r + 5 * c]; };
+  int ipvt[5];
+  for (int k = 0; k < n - 1; ++k) {
+    int l = k;
+    S mx = std::fabs(A(k, k));
+    for (int r = k + 1; r < n; ++r)
+      if (std::fabs(A(r, k)) > mx) { mx = std::fabs(A(r, k)); l = r; }
+    ipvt[k] = l;
+    if (A(l, k) == S(0)) return k + 1;
+    if (l != k) std::swap(A(l, k), A(k, k));
+    S t = S(-1.0) / A(k, k);
+    for (int r = k + 1; r < n; ++r) A(r, k) *= t;
+    for (int j = k + 1; j < n; ++j) {
+      S tt = A(l, j);
+      if (l != k) { A(l, j) = A(k, j); A(k, j) = tt; }
+      for (int r = k + 1; r < n; ++r) A(r, j) += tt * A(r, k);
+    }
+  }
+  ipvt[n - 1] = n - 1;
+  if (A(n - 1, n - 1) == S(0)) return n;
+  // inverse(U)
+  for (int k = 0; k < n; ++k) {
+    A(k, k) = S(1.0) / A(k, k);
+    S t = -A(k, k);
+    for (int r = 0; r < k; ++r) A(r, k) *= t;
+    for (int j = k + 1; j < n; ++j) {
+      S tt = A(k, j);
+      A(k, j) = S(0);
+      for (int r = 0; r <= k; ++r) A(r, j) += tt * A(r, k);
+    }
+  }
+  // inverse(U) * inverse(L)
+  S work[5];
+  for (int kb = 1; kb <= n - 1; ++kb) {
+    int k = n - 1 - kb;
+    for (int i = k + 1; i < n; ++i) { work[i] = A(i, k); A(i, k) = S(0); }
+    for (int j = k + 1; j < n; ++j) {
+      S tt = work[j];
+      for (int r = 0; r < n; ++r) A(r, k) += tt * A(r, j);
+    }
+    int l = ipvt[k];
+    if (l != k)
+      for (int r = 0; r < n; ++r) std::swap(A(r, k), A(r, l));
+  }
+  for (int r = 0; r < 5; ++r)
+    for (int c = 0; c < 5; ++c) a[5 * r + c] = t_[5 * c + r];
+  return 0;
+}
+
+// ---------------------------------------------------------------- GMRES
+// GmresSolver::solve (KspSolver.C:351-492) with right preconditioning
+// (typePrec = 2), modified Gram-Schmidt and Givens rotations
+// (KspSolver.C:917-982).  x starts at 0 (ImplicitCoupledTsDesc.C:292).
+struct Operator {
+  const Mesh* m;
+  const double* A;           // H1 Jacobian (MvpMat layout)
+  std::vector<double> Dinv;  // block-Jacobi inverses (FP64 or rounded FP32)
+  int transpose = 0;
+};
+
+static double dotv(const std::vector<double>& a, const std::vector<double>& b) {
+  double s = 0.0;
+  for (size_t k = 0; k < a.size(); ++k) s += a[k] * b[k];
+  return s;
+}
+
+static void bj_apply(const Operator& op, const std::vector<double>& x, std::vector<double>& y) {
+  const int N = op.m->N;
+  for (int i = 0; i < N; ++i) {
+    const double* d = &op.Dinv[25 * (size_t)i];
+    for (int r = 0; r < 5; ++r) {
+      double s = 0.0;
+      for (int c = 0; c < 5; ++c) s += (op.transpose ? d[5 * c + r] : d[5 * r + c]) * x[5 * i + c];
+      y[5 * i + r] = s;
+    }
+  }
+}
+
+static int gmres(const Operator& op, const std::vector<double>& b, std::vector<double>& x, int numVec,
+                 int maxits, double eps, double* final_res) {
+  const size_t n = b.size();
+  std::vector<std::vector<double>> Vb(numVec + 1, std::vector<double>(n));
+  std::vector<double> w(n), r(n);
+  std::vector<double> H((numVec + 1) * numVec, 0.0), cs(2 * numVec), g(numVec + 1), y(numVec);
+  auto h = [&](int i, int j) -> double& { return H[(size_t)i * numVec + j]; };
+  int iter = 0, exitLoop = 0;
+  double target = 0.0, l2res = 0.0;
+  do {
+    matvec(*op.m, op.A, x.data(), w.data(), op.transpose);
+    for (size_t k = 0; k < n; ++k) r[k] = b[k] - w[k];
+    double beta = std::sqrt(dotv(r, r));
+    if (iter == 0) target = eps * std::sqrt(dotv(b, b));
+    if (beta == 0.0) { if (final_res) *final_res = 0.0; return 0; }
+    for (size_t k = 0; k < n; ++k) Vb[0][k] = (1.0 / beta) * r[k];
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int j;
+    for (j = 0; j < numVec; ++j) {
+      bj_apply(op, Vb[j], r);
+      matvec(*op.m, op.A, r.data(), w.data(), op.transpose);
+      for (int i = 0; i <= j; ++i) {
+        h(i, j) = dotv(w, Vb[i]);
+        for (size_t k = 0; k < n; ++k) w[k] -= h(i, j) * Vb[i][k];
+      }
+      h(j + 1, j) = std::sqrt(dotv(w, w));
+      bool breakdown = (h(j + 1, j) == 0.0);
+      if (!breakdown)
+        for (size_t k = 0; k < n; ++k) Vb[j + 1][k] = (1. / h(j + 1, j)) * w[k];
+      for (int i = 0; i < j; ++i) {
+        double hj = cs[2 * i + 1] * h(i, j) + cs[2 * i] * h(i + 1, j);
+        double hjp1 = -cs[2 * i] * h(i, j) + cs[2 * i + 1] * h(i + 1, j);
+        h(i, j) = hj; h(i + 1, j) = hjp1;
+      }
+      if (h(j, j) * h(j, j) == 0.0) { cs[2 * j + 1] = 0.0; cs[2 * j] = 1.0; }
+      else {
+        double coef = 1.0 / std::sqrt(h(j, j) * h(j, j) + h(j + 1, j) * h(j + 1, j));
+        cs[2 * j + 1] = std::sqrt(h(j, j) * h(j, j)) * coef;
+        cs[2 * j] = cs[2 * j + 1] * h(j + 1, j) / h(j, j);
+      }
+      h(j, j) = cs[2 * j + 1] * h(j, j) + cs[2 * j] * h(j + 1, j);
+      h(j + 1, j) = 0.0;
+      g[j + 1] = -cs[2 * j] * g[j];
+      g[j] = cs[2 * j + 1] * g[j];
+      ++iter;
+      if (breakdown) { exitLoop = 1; break; }
+      l2res = std::fabs(g[j + 1]);
+      if (l2res <= target || iter >= maxits) { exitLoop = 1; break; }
+    }
+    if (j == numVec) --j;
+    for (int i = j; i >= 0; --i) {
+      y[i] = g[i];
+      for (int k = j; k >= i + 1; --k) y[i] -= h(i, k) * y[k];
+      y[i] /= h(i, i);
+    }
+    std::fill(w.begin(), w.end(), 0.0);
+    for (int mm = 0; mm <= j; ++mm)
+      for (size_t k = 0; k < n; ++k) w[k] += y[mm] * Vb[mm][k];
+    bj_apply(op, w, r);
+    for (size_t k = 0; k < n; ++k) x[k] += r[k];
+  } while (exitLoop == 0);
+  if (final_res) *final_res = l2res;
+  return iter;
+}
+
+}  // namespace orc
+
+using namespace orc;
+
+// ============================================================== C interface
+extern "C" {
+
+void* orc_create(int N, int T, int F, const double* X, const int* tets, const int* faces,
+                 const int* codes, double gam) {
+  Mesh* m = new Mesh();
+  m->N = N; m->T = T; m->F = F; m->gam = gam;
+  m->X.assign(X, X + 3 * (size_t)N);
+  m->tets.assign(tets, tets + 4 * (size_t)T);
+  m->faces.assign(faces, faces + 3 * (size_t)F);
+  m->codes.assign(codes, codes + F);
+  build_edges(*m);
+  compute_geometry<double>(*m, m->X.data(), m->edgeNorm, m->faceNorm, m->ctrlVol);
+  compute_lsq_R<double>(*m, m->X.data(), m->Rlsq);
+  return m;
+}
+
+void orc_destroy(void* h) { delete (Mesh*)h; }
+int orc_num_edges(void* h) { return ((Mesh*)h)->E; }
+void orc_get_edges(void* h, int* e) {
+  Mesh* m = (Mesh*)h;
+  std::memcpy(e, m->edges.data(), sizeof(int) * 2 * (size_t)m->E);
+}
+void orc_get_geometry(void* h, double* edgeNorm, double* faceNorm, double* ctrlVol, double* Rlsq) {
+  Mesh* m = (Mesh*)h;
+  if (edgeNorm) std::memcpy(edgeNorm, m->edgeNorm.data(), sizeof(double) * 3 * (size_t)m->E);
+  if (faceNorm) std::memcpy(faceNorm, m->faceNorm.data(), sizeof(double) * 3 * (size_t)m->F);
+  if (ctrlVol) std::memcpy(ctrlVol, m->ctrlVol.data(), sizeof(double) * (size_t)m->N);
+  if (Rlsq) std::memcpy(Rlsq, m->Rlsq.data(), sizeof(double) * 6 * (size_t)m->N);
+}
+
+void orc_prim(void* h, const double* U, double* V) {
+  Mesh* m = (Mesh*)h;
+  for (int i = 0; i < m->N; ++i) cons2prim(m->gam, &U[5 * i], &V[5 * i]);
+}
+
+void orc_gradients(void* h, const double* V, double* ddx, double* ddy, double* ddz) {
+  Mesh* m = (Mesh*)h;
+  compute_gradients<double>(*m, m->X.data(), m->Rlsq.data(), V, ddx, ddy, ddz);
+}
+
+int orc_residual(void* h, const double* U, const double* Ub, int order, double beta, int failsafe,
+                 double* R) {
+  Mesh* m = (Mesh*)h;
+  Work<double> w;
+  return residual_t<double>(*m, m->X.data(), m->edgeNorm, m->faceNorm, m->ctrlVol, m->Rlsq, U, Ub,
+                            order, beta, failsafe, R, w);
+}
+
+// Timed CPU baseline: threaded residual (order 1 or 2, van Albada).
+struct Baseline {
+  std::vector<double> V, G, priv;
+};
+void* orc_baseline_create() { return new Baseline(); }
+void orc_baseline_destroy(void* b) { delete (Baseline*)b; }
+void orc_residual_threaded(void* h, void* b, const double* U, const double* Ub, int order, int nthreads,
+                           double* R) {
+  Mesh* m = (Mesh*)h;
+  Baseline* bl = (Baseline*)b;
+  residual_threaded(*m, U, Ub, order, 1.0 / 3.0, nthreads, R, bl->V, bl->G, bl->priv);
+}
+
+void orc_timestep(void* h, const double* U, double cfl, double* dt) { timestep(*(Mesh*)h, U, cfl, dt); }
+
+// ExplicitTsDesc::computeRKSecondOrder (ExplicitTsDesc.C:98-117) with local
+// time stepping (TimeData.C:11-18 for a steady problem):
+// k1 = dt R(U); U0 = U - k1; k2 = dt R(U0); U = U - 1/2 (k1 + k2).
+void orc_rk2(void* h, double* U, const double* Ub, int order, double cfl, int nsteps) {
+  Mesh* m = (Mesh*)h;
+  const size_t n5 = 5 * (size_t)m->N;
+  std::vector<double> dt(m->N), k1(n5), k2(n5), U0(n5);
+  for (int s = 0; s < nsteps; ++s) {
+    timestep(*m, U, cfl, dt.data());
+    orc_residual(h, U, Ub, order, 1.0 / 3.0, 0, k1.data());
+    for (int i = 0; i < m->N; ++i)
+      for (int k = 0; k < 5; ++k) k1[5 * i + k] *= dt[i];
+    for (size_t k = 0; k < n5; ++k) U0[k] = U[k] - k1[k];
+    orc_residual(h, U0.data(), Ub, order, 1.0 / 3.0, 0, k2.data());
+    for (int i = 0; i < m->N; ++i)
+      for (int k = 0; k < 5; ++k) k2[5 * i + k] *= dt[i];
+    for (size_t k = 0; k < n5; ++k) U[k] = U[k] - 1.0 / 2.0 * (k1[k] + k2[k]);
+  }
+}
+
+void orc_roeflux7(double gam, const double* n, double ndot, const double* Vi, const double* Vj,
+                  double* phi) {
+  roeflux7<double>(gam, 0.0, n, ndot, Vi, Vj, phi);
+}
+void orc_boundflux5(double gam, const double* n, double sig, const double* V, const double* Ub,
+                    double* flux) {
+  boundflux5<double>(gam, n, sig, V, Ub, flux);
+}
+void orc_roejac6(double gam, const double* n, const double* Vi, const double* Vj, double* jacL,
+                 double* jacR) {
+  double nn[3] = {n[0], n[1], n[2]};
+  roejac6(1.0, gam, 0.0, nn, 0.0, Vi, Vj, jacL, 1);
+  roejac6(1.0, gam, 0.0, nn, 0.0, Vj, Vi, jacR, 2);
+}
+void orc_vanalbada(double beta, const double* Vi, const double* ddVij, const double* Vj,
+                   const double* ddVji, double* Vij, double* Vji) {
+  RecParams p = rec_params(beta);
+  for (int k = 0; k < 5; ++k) vanalbada(p, Vi[k], ddVij[k], Vj[k], ddVji[k], Vij[k], Vji[k]);
+}
+void orc_linear_rec(double beta, const double* Vi, const double* ddVij, const double* Vj,
+                    const double* ddVji, double* Vij, double* Vji) {
+  RecParams p = rec_params(beta);
+  for (int k = 0; k < 5; ++k) linear_rec(p, Vi[k], ddVij[k], Vj[k], ddVji[k], Vij[k], Vji[k]);
+}
+void orc_cons2prim(double gam, const double* U, double* V) { cons2prim<double>(gam, U, V); }
+void orc_post_dVdU(double gam, const double* V, const double* mat, double* res) { post_dVdU(gam, V, mat, res); }
+int orc_invert5(double* a) { return invert5<double>(a); }
+int orc_invert5f(float* a) { return invert5<float>(a); }
+
+void orc_jacobian(void* h, const double* U, const double* Ub, const double* dt, double* A) {
+  jacobian(*(Mesh*)h, U, Ub, dt, A);
+}
+void orc_matvec(void* h, const double* A, const double* p, double* y, int transpose) {
+  matvec(*(Mesh*)h, A, p, y, transpose);
+}
+
+// Block-Jacobi inverses of the diagonal blocks (JacobiPrec::setup,
+// KspPrec.C:75-82; DiagMat::invert, DiagMatrix.C:44-80). fp32 != 0 stores
+// the blocks as float before inverting (PrecScalar = float,
+// CMakeLists.txt:654).  Returns the number of singular blocks.
+int orc_bj_invert(void* h, const double* A, double* Dinv, int fp32) {
+  Mesh* m = (Mesh*)h;
+  int bad = 0;
+  for (int i = 0; i < m->N; ++i) {
+    if (fp32) {
+      float a[25];
+      for (int k = 0; k < 25; ++k) a[k] = (float)A[25 * (size_t)i + k];
+      if (invert5<float>(a)) ++bad;
+      for (int k = 0; k < 25; ++k) Dinv[25 * (size_t)i + k] = a[k];
+    } else {
+      double a[25];
+      for (int k = 0; k < 25; ++k) a[k] = A[25 * (size_t)i + k];
+      if (invert5<double>(a)) ++bad;
+      for (int k = 0; k < 25; ++k) Dinv[25 * (size_t)i + k] = a[k];
+    }
+  }
+  return bad;
+}
+
+int orc_gmres(void* h, const double* A, const double* Dinv, const double* b, double* x, int numVec,
+              int maxits, double eps, int transpose, double* final_res) {
+  Mesh* m = (Mesh*)h;
+  Operator op;
+  op.m = m; op.A = A; op.transpose = transpose;
+  op.Dinv.assign(Dinv, Dinv + 25 * (size_t)m->N);
+  std::vector<double> bb(b, b + 5 * (size_t)m->N), xx(5 * (size_t)m->N, 0.0);
+  int its = gmres(op, bb, xx, numVec, maxits, eps, final_res);
+  std::memcpy(x, xx.data(), sizeof(double) * xx.size());
+  return its;
+}
+
+// Pseudo-transient Newton (TsSolver::resolve, TsSolver.h:231-380;
+// NewtonSolver::solve with maxIts=1, NewtonSolver.h:70-231;
+// ImplicitCoupledTsDesc::computeJacobian/setOperators/solveLinearSystem,
+// ImplicitCoupledTsDesc.C:85-300) with the RESIDUAL CFL law
+// (TsParameters.C:182-217,290): cfl *= (res_{k-1}/res_k)^ser, clipped to
+// [cflMin, cflMax].  The Jacobian is the first-order H1 approximation in
+// FP64; block-Jacobi in FP32 (fp32_prec) or FP64.  Stops when
+// ||R(Q)||/||R(Q0)|| <= tol or after max_steps.  history (max_steps+1
+// entries) receives the relative residuals; returns the steps taken.
+int orc_newton(void* h, double* U, const double* Ub, int order, double cfl0, double cflMin,
+               double cflMax, double ser, int numVec, int maxits, double eps, double tol,
+               int max_steps, int fp32_prec, double* history, int* lin_its) {
+  Mesh* m = (Mesh*)h;
+  const int N = m->N;
+  const size_t n5 = 5 * (size_t)N;
+  std::vector<double> R(n5), dt(N), A(25 * ((size_t)N + 2 * (size_t)m->E)), Dinv(25 * (size_t)N), dQ(n5);
+  double res0 = 0.0, cfl = cfl0, rel_prev = 1.0;
+  int k;
+  for (k = 0; k <= max_steps; ++k) {
+    orc_residual(h, U, Ub, order, 1.0 / 3.0, 0, R.data());
+    double res = std::sqrt(std::inner_product(R.begin(), R.end(), R.begin(), 0.0));
+    if (k == 0) res0 = res;
+    double rel = res / res0;
+    if (history) history[k] = rel;
+    if (rel <= tol || k == max_steps) break;
+    if (k > 0) cfl = std::min(std::max(cfl * std::pow(rel_prev / rel, ser), cflMin), cflMax);
+    rel_prev = rel;
+    timestep(*m, U, cfl, dt.data());
+    jacobian(*m, U, Ub, dt.data(), A.data());
+    orc_bj_invert(h, A.data(), Dinv.data(), fp32_prec);
+    for (size_t q = 0; q < n5; ++q) R[q] = -1.0 * R[q];
+    int its = orc_gmres(h, A.data(), Dinv.data(), R.data(), dQ.data(), numVec, maxits, eps, 0, nullptr);
+    if (lin_its) lin_its[k] = its;
+    for (size_t q = 0; q < n5; ++q) U[q] += dQ[q];
+  }
+  return k;
+}
+
+// Exact forward-mode linearisation of the residual (T = Dual):
+// Jv = dR/dU . v  (the operator MatVecProdH2 applies, MatVecProd.C:1462-1704)
+int orc_jvp(void* h, const double* U, const double* Ub, int order, const double* v, double* Jv) {
+  Mesh* m = (Mesh*)h;
+  const size_t n5 = 5 * (size_t)m->N;
+  std::vector<Dual> Ud(n5), Rd(n5), Xd(3 * (size_t)m->N);
+  for (size_t k = 0; k < n5; ++k) Ud[k] = Dual(U[k], v[k]);
+  for (size_t k = 0; k < 3 * (size_t)m->N; ++k) Xd[k] = Dual(m->X[k]);
+  std::vector<Dual> en, fn, cv, Rl;
+  compute_geometry<Dual>(*m, Xd.data(), en, fn, cv);
+  compute_lsq_R<Dual>(*m, Xd.data(), Rl);
+  Work<Dual> w;
+  int ierr = residual_t<Dual>(*m, Xd.data(), en, fn, cv, Rl, Ud.data(), Ub, order, 1.0 / 3.0, 0, Rd.data(), w);
+  for (size_t k = 0; k < n5; ++k) Jv[k] = Rd[k].d;
+  return ierr;
+}
+
+// Exact forward-mode derivative of the residual w.r.t. node coordinates:
+// dR = dR/dX . Xdot, through edge/face normals, control volumes, LSQ R and
+// dx (the quantities SpaceOperator::computeDerivativeOfResidual differentiates).
+int orc_dRdX(void* h, const double* U, const double* Ub, int order, const double* Xdot, double* dR,
+             double* R) {
+  Mesh* m = (Mesh*)h;
+  const size_t n5 = 5 * (size_t)m->N;
+  std::vector<Dual> Ud(n5), Rd(n5), Xd(3 * (size_t)m->N);
+  for (size_t k = 0; k < n5; ++k) Ud[k] = Dual(U[k]);
+  for (size_t k = 0; k < 3 * (size_t)m->N; ++k) Xd[k] = Dual(m->X[k], Xdot[k]);
+  std::vector<Dual> en, fn, cv, Rl;
+  compute_geometry<Dual>(*m, Xd.data(), en, fn, cv);
+  compute_lsq_R<Dual>(*m, Xd.data(), Rl);
+  Work<Dual> w;
+  int ierr = residual_t<Dual>(*m, Xd.data(), en, fn, cv, Rl, Ud.data(), Ub, order, 1.0 / 3.0, 0, Rd.data(), w);
+  for (size_t k = 0; k < n5; ++k) { dR[k] = Rd[k].d; if (R) R[k] = Rd[k].v; }
+  return ierr;
+}
+
+// Residual on displaced coordinates X (geometry recomputed), for central
+// finite differences of shape sensitivities.
+int orc_residual_at(void* h, const double* X, const double* U, const double* Ub, int order, double* R) {
+  Mesh* m = (Mesh*)h;
+  std::vector<double> en, fn, cv, Rl;
+  compute_geometry<double>(*m, X, en, fn, cv);
+  compute_lsq_R<double>(*m, X, Rl);
+  Work<double> w;
+  return residual_t<double>(*m, X, en, fn, cv, Rl, U, Ub, order, 1.0 / 3.0, 0, R, w);
+}
+
+// z-force functional on the z=0 boundary faces: J = sum_f p_f * (-n_z(f)),
+// p_f the mean of the 3 node pressures, n_f the outward area normal
+// (pressure force along +z on the bottom wall, cf. PostOperator.C:379-).
+}  // extern "C"
+template <class T>
+static T zforce_t(const Mesh& m, const T* X, const T* U, const int* zfaces, int nz) {
+  T J(0.0);
+  for (int q = 0; q < nz; ++q) {
+    int f = zfaces[q];
+    const int* nd = &m.faces[3 * f];
+    V3<T> x0(X[3 * nd[0]], X[3 * nd[0] + 1], X[3 * nd[0] + 2]);
+    V3<T> x1(X[3 * nd[1]], X[3 * nd[1] + 1], X[3 * nd[1] + 2]);
+    V3<T> x2(X[3 * nd[2]], X[3 * nd[2] + 1], X[3 * nd[2] + 2]);
+    V3<T> n = 0.5 * cross(x2 - x0, x1 - x0);
+    T p(0.0);
+    for (int l = 0; l < 3; ++l) {
+      T V[5];
+      cons2prim(m.gam, &U[5 * nd[l]], V);
+      p = p + V[4];
+    }
+    p = third * p;
+    J = J + p * (-n[2]);
+  }
+  return J;
+}
+extern "C" {
+double orc_zforce(void* h, const double* X, const double* U, const int* zfaces, int nz) {
+  Mesh* m = (Mesh*)h;
+  return zforce_t<double>(*m, X ? X : m->X.data(), U, zfaces, nz);
+}
+// dJ/dU (gradient, [N][5]): J depends on U only through the face-node
+// pressures p = (gam-1)(E - |m|^2/(2 rho)), so
+// dJ/dU_i = sum_{faces f at i} third*(-n_z(f)) * dp/dU_i.
+void orc_zforce_dU(void* h, const double* U, const int* zfaces, int nz, double* g) {
+  Mesh* m = (Mesh*)h;
+  const size_t n5 = 5 * (size_t)m->N;
+  std::fill(g, g + n5, 0.0);
+  const double* X = m->X.data();
+  for (int q = 0; q < nz; ++q) {
+    int f = zfaces[q];
+    const int* nd = &m->faces[3 * f];
+    V3<double> x0(X[3 * nd[0]], X[3 * nd[0] + 1], X[3 * nd[0] + 2]);
+    V3<double> x1(X[3 * nd[1]], X[3 * nd[1] + 1], X[3 * nd[1] + 2]);
+    V3<double> x2(X[3 * nd[2]], X[3 * nd[2] + 1], X[3 * nd[2] + 2]);
+    V3<double> n = 0.5 * cross(x2 - x0, x1 - x0);
+    double w = third * (-n[2]);
+    for (int l = 0; l < 3; ++l) {
+      const double* u = &U[5 * nd[l]];
+      double ux = u[1] / u[0], uy = u[2] / u[0], uz = u[3] / u[0];
+      double gm1 = m->gam - 1.0;
+      double* gi = &g[5 * nd[l]];
+      gi[0] += w * gm1 * 0.5 * (ux * ux + uy * uy + uz * uz);
+      gi[1] += w * (-gm1 * ux);
+      gi[2] += w * (-gm1 * uy);
+      gi[3] += w * (-gm1 * uz);
+      gi[4] += w * gm1;
+    }
+  }
+}
+double orc_zforce_dX(void* h, const double* U, const int* zfaces, int nz, const double* Xdot) {
+  Mesh* m = (Mesh*)h;
+  const size_t n5 = 5 * (size_t)m->N;
+  std::vector<Dual> Xd(3 * (size_t)m->N), Ud(n5);
+  for (size_t k = 0; k < 3 * (size_t)m->N; ++k) Xd[k] = Dual(m->X[k], Xdot[k]);
+  for (size_t k = 0; k < n5; ++k) Ud[k] = Dual(U[k]);
+  return zforce_t<Dual>(*m, Xd.data(), Ud.data(), zfaces, nz).d;
+}
+
+}  // extern "C"

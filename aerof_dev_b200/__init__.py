@@ -1,0 +1,394 @@
+"""B200 (sm_100a) implementation of AERO-F's implicit edge-based FV hot path.
+
+The compute lives in ``libaerof_gpu.so`` (hand-written CUDA behind the C ABI
+of ``include/aerof_gpu.h``).  This module is the Python host side of that
+ABI and mirrors the reference's C++ call surface for the path:
+
+* :class:`SpaceOperator`  -- ``SpaceOperator<5>::computeResidual``,
+  ``DistTimeState::computeTimeStep``, ``DistNodalGrad::compute``
+* :class:`MatVecProdH1`   -- ``MatVecProdH1<5,MatScalar,5>::evaluate/apply/applyTranspose``
+* :class:`JacobiPrec`     -- ``JacobiPrec<PrecScalar,5>::setup/apply/applyT``
+* :class:`GmresSolver`    -- ``GmresSolver<...>::solve/solveT``
+* :class:`ImplicitSteadySolver` -- the pseudo-transient Newton loop
+* :class:`ExplicitRK2`    -- ``ExplicitTsDesc::computeRKSecondOrder``
+* :class:`Sensitivity`    -- exact J v, J^T w, dR/dX . Xdot, (dR/dX)^T lambda
+
+Arrays may be numpy arrays (host memory) or torch CUDA tensors (device
+memory); results come back in the same kind of container as the input.
+There is no CPU fallback: importing works anywhere, but creating a
+:class:`Context` needs the built library and a CUDA device, and fails loudly
+otherwise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import workloads  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libaerof_gpu.so")
+
+AEROF_OK = 0
+ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ETIMEDOUT", -5: "ESINGULAR", -6: "ESTATE"}
+REC_CONSTANT, REC_VANALBADA, REC_LINEAR = 1, 2, 3
+PREC_FP32, PREC_FP64 = 32, 64
+
+# every entry point of include/aerof_gpu.h
+EXPORTS = [
+    "aerof_gpu_create", "aerof_gpu_destroy", "aerof_gpu_set_stream", "aerof_gpu_last_error",
+    "aerof_gpu_set_mesh", "aerof_gpu_mesh_sizes", "aerof_gpu_get_edges", "aerof_gpu_get_geometry",
+    "aerof_gpu_residual", "aerof_gpu_gradients", "aerof_gpu_timestep", "aerof_gpu_rk2",
+    "aerof_gpu_jacobian", "aerof_gpu_get_jacobian", "aerof_gpu_matvec", "aerof_gpu_prec_setup",
+    "aerof_gpu_prec_apply", "aerof_gpu_gmres", "aerof_gpu_newton",
+    "aerof_gpu_jvp", "aerof_gpu_vjp", "aerof_gpu_dRdX", "aerof_gpu_dRdX_T",
+]
+
+
+class AerofError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"aerof_gpu error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class Config(C.Structure):
+    _fields_ = [("gamma", C.c_double), ("beta", C.c_double), ("reconstruction", C.c_int),
+                ("failsafe", C.c_int), ("device", C.c_int), ("reserved", C.c_int * 5)]
+
+
+class NewtonParams(C.Structure):
+    _fields_ = [("cfl0", C.c_double), ("cfl_min", C.c_double), ("cfl_max", C.c_double),
+                ("ser", C.c_double), ("ksp_eps", C.c_double), ("tol", C.c_double),
+                ("ksp_krylov", C.c_int), ("ksp_maxits", C.c_int), ("max_steps", C.c_int),
+                ("precision", C.c_int), ("reserved", C.c_int * 4)]
+
+
+class NewtonResult(C.Structure):
+    _fields_ = [("steps", C.c_int), ("linear_its", C.c_int), ("rel_residual", C.c_double),
+                ("seconds", C.c_double)]
+
+
+_lib = None
+
+
+def library(path: str | None = None):
+    """Load libaerof_gpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        p = path or LIB_PATH
+        if not os.path.exists(p):
+            raise AerofError(-3, f"{p} is missing: build it with `python -m aerof_dev_b200.build`")
+        L = C.CDLL(p)
+        vp, dp, ip = C.c_void_p, C.c_void_p, C.c_void_p
+        sig = {
+            "aerof_gpu_create": [C.POINTER(Config), C.POINTER(C.c_void_p)],
+            "aerof_gpu_destroy": [vp],
+            "aerof_gpu_set_stream": [vp, vp],
+            "aerof_gpu_last_error": [vp, C.c_char_p, C.c_int],
+            "aerof_gpu_set_mesh": [vp, C.c_int, C.c_int, C.c_int, dp, ip, ip, ip, dp],
+            "aerof_gpu_mesh_sizes": [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
+            "aerof_gpu_get_edges": [vp, ip],
+            "aerof_gpu_get_geometry": [vp, dp, dp, dp, dp],
+            "aerof_gpu_residual": [vp, dp, dp],
+            "aerof_gpu_gradients": [vp, dp, dp, dp, dp],
+            "aerof_gpu_timestep": [vp, dp, C.c_double, dp],
+            "aerof_gpu_rk2": [vp, dp, C.c_double, C.c_int],
+            "aerof_gpu_jacobian": [vp, dp, dp, C.c_int],
+            "aerof_gpu_get_jacobian": [vp, dp],
+            "aerof_gpu_matvec": [vp, dp, dp, C.c_int],
+            "aerof_gpu_prec_setup": [vp],
+            "aerof_gpu_prec_apply": [vp, dp, dp, C.c_int],
+            "aerof_gpu_gmres": [vp, dp, dp, C.c_int, C.c_int, C.c_double, C.c_int,
+                                C.POINTER(C.c_int), C.POINTER(C.c_double)],
+            "aerof_gpu_newton": [vp, dp, C.POINTER(NewtonParams), C.POINTER(NewtonResult), dp],
+            "aerof_gpu_jvp": [vp, dp, dp, dp],
+            "aerof_gpu_vjp": [vp, dp, dp, dp],
+            "aerof_gpu_dRdX": [vp, dp, dp, dp],
+            "aerof_gpu_dRdX_T": [vp, dp, dp, dp],
+        }
+        for name, args in sig.items():
+            if hasattr(L, name):
+                f = getattr(L, name)
+                f.argtypes = args
+                f.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+# ----------------------------------------------------------------- buffers
+def _is_torch(a) -> bool:
+    return type(a).__module__.startswith("torch")
+
+
+class _Arg:
+    """Pointer to a float64/int32 array: numpy (host) or torch CUDA tensor."""
+
+    def __init__(self, a, dtype, shape=None, writable=False):
+        if _is_torch(a):
+            import torch
+            want = torch.float64 if dtype == np.float64 else torch.int32
+            if a.dtype != want or not a.is_contiguous():
+                if writable:
+                    raise ValueError("output tensors must be contiguous with the right dtype")
+                a = a.to(want).contiguous()
+            self.obj = a
+            self.ptr = C.c_void_p(a.data_ptr())
+        else:
+            if writable:
+                if not (isinstance(a, np.ndarray) and a.dtype == dtype and a.flags.c_contiguous):
+                    raise ValueError("output arrays must be C-contiguous " + str(np.dtype(dtype)))
+                self.obj = a
+            else:
+                self.obj = np.ascontiguousarray(a, dtype=dtype)
+            self.ptr = C.c_void_p(self.obj.ctypes.data)
+        if shape is not None and 0 not in shape and tuple(self.obj.shape) != tuple(shape):
+            if int(np.prod(self.obj.shape)) != int(np.prod(shape)):
+                raise ValueError(f"array of shape {tuple(self.obj.shape)}, expected {tuple(shape)}")
+
+
+def _like(a, shape, dtype=np.float64):
+    if _is_torch(a):
+        import torch
+        return torch.empty(shape, dtype=torch.float64 if dtype == np.float64 else torch.int32, device=a.device)
+    return np.empty(shape, dtype=dtype)
+
+
+class Context:
+    """One GPU context: ``aerof_gpu_create`` + ``aerof_gpu_set_mesh``."""
+
+    def __init__(self, reconstruction: int = REC_VANALBADA, gamma: float = 1.4, beta: float = 1.0 / 3.0,
+                 failsafe: int = 0, device: int = 0):
+        self.L = library()
+        cfg = Config(gamma, beta, reconstruction, failsafe, device)
+        h = C.c_void_p()
+        self._check(self.L.aerof_gpu_create(C.byref(cfg), C.byref(h)), None)
+        self.h = h
+        self.cfg = cfg
+        self.N = self.E = self.F = 0
+
+    def _check(self, rc: int, h=0):
+        if rc < 0:
+            msg = ""
+            hh = self.h if h == 0 else h
+            if hh:
+                buf = C.create_string_buffer(512)
+                self.L.aerof_gpu_last_error(hh, buf, 512)
+                msg = buf.value.decode()
+            raise AerofError(rc, msg)
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.aerof_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(self.L.aerof_gpu_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
+
+    def set_mesh(self, X, tets, faces, codes, Ub):
+        X = _Arg(X, np.float64)
+        t = _Arg(tets, np.int32)
+        f = _Arg(faces, np.int32)
+        c = _Arg(codes, np.int32)
+        ub = _Arg(Ub, np.float64)
+        N, T, F = X.obj.shape[0], t.obj.shape[0], f.obj.shape[0]
+        self._check(self.L.aerof_gpu_set_mesh(self.h, N, T, F, X.ptr, t.ptr, f.ptr, c.ptr, ub.ptr))
+        n, e, ff = C.c_int(), C.c_int(), C.c_int()
+        self._check(self.L.aerof_gpu_mesh_sizes(self.h, C.byref(n), C.byref(e), C.byref(ff)))
+        self.N, self.E, self.F = n.value, e.value, ff.value
+        return self
+
+    @classmethod
+    def from_mesh(cls, mesh: dict, Ub, **kw) -> "Context":
+        ctx = cls(**kw)
+        return ctx.set_mesh(mesh["X"], mesh["tets"], mesh["faces"], mesh["codes"], Ub)
+
+    def edges(self) -> np.ndarray:
+        e = np.empty((self.E, 2), dtype=np.int32)
+        self._check(self.L.aerof_gpu_get_edges(self.h, C.c_void_p(e.ctypes.data)))
+        return e
+
+    def geometry(self) -> dict:
+        en = np.empty((self.E, 3)); fn = np.empty((max(self.F, 1), 3)); cv = np.empty(self.N)
+        R = np.empty((self.N, 6))
+        p = lambda a: C.c_void_p(a.ctypes.data)
+        self._check(self.L.aerof_gpu_get_geometry(self.h, p(en), p(fn), p(cv), p(R)))
+        return {"edge_normal": en, "face_normal": fn[: self.F], "ctrl_vol": cv, "lsq_R": R}
+
+
+class SpaceOperator:
+    """``SpaceOperator<5>`` on the GPU (SpaceOperator.C:524-634)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+
+    def computeResidual(self, U, R=None):
+        """R = residual(U) / ctrlVol.  Returns (R, n_unphysical)."""
+        ctx = self.ctx
+        u = _Arg(U, np.float64, (ctx.N, 5))
+        R = _like(U, (ctx.N, 5)) if R is None else R
+        r = _Arg(R, np.float64, (ctx.N, 5), writable=True)
+        bad = ctx._check(ctx.L.aerof_gpu_residual(ctx.h, u.ptr, r.ptr))
+        return r.obj, bad
+
+    def computeGradients(self, V):
+        ctx = self.ctx
+        v = _Arg(V, np.float64, (ctx.N, 5))
+        out = [_like(V, (ctx.N, 5)) for _ in range(3)]
+        a = [_Arg(o, np.float64, writable=True) for o in out]
+        ctx._check(ctx.L.aerof_gpu_gradients(ctx.h, v.ptr, a[0].ptr, a[1].ptr, a[2].ptr))
+        return tuple(x.obj for x in a)
+
+    def computeTimeStep(self, U, cfl):
+        ctx = self.ctx
+        u = _Arg(U, np.float64, (ctx.N, 5))
+        dt = _like(U, (ctx.N,))
+        d = _Arg(dt, np.float64, writable=True)
+        ctx._check(ctx.L.aerof_gpu_timestep(ctx.h, u.ptr, float(cfl), d.ptr))
+        return d.obj
+
+
+class ExplicitRK2:
+    """``ExplicitTsDesc::computeRKSecondOrder`` with local time stepping."""
+
+    def __init__(self, ctx: Context, cfl: float):
+        self.ctx, self.cfl = ctx, cfl
+
+    def run(self, U, nsteps: int):
+        ctx = self.ctx
+        if _is_torch(U):
+            out = U.clone()
+        else:
+            out = np.array(U, dtype=np.float64, copy=True, order="C")
+        a = _Arg(out, np.float64, (ctx.N, 5), writable=True)
+        bad = ctx._check(ctx.L.aerof_gpu_rk2(ctx.h, a.ptr, float(self.cfl), int(nsteps)))
+        return a.obj, bad
+
+
+class MatVecProdH1:
+    """Assembled first-order Jacobian (``MatVecProdH1``, MatVecProd.C:945-1208)."""
+
+    def __init__(self, ctx: Context, precision: int = PREC_FP32):
+        self.ctx, self.precision = ctx, precision
+
+    def evaluate(self, U, dt=None):
+        ctx = self.ctx
+        u = _Arg(U, np.float64, (ctx.N, 5))
+        d = _Arg(dt, np.float64, (ctx.N,)) if dt is not None else None
+        ctx._check(ctx.L.aerof_gpu_jacobian(ctx.h, u.ptr, d.ptr if d else None, int(self.precision)))
+
+    def apply(self, p, transpose=False):
+        ctx = self.ctx
+        a = _Arg(p, np.float64, (ctx.N, 5))
+        y = _like(p, (ctx.N, 5))
+        b = _Arg(y, np.float64, writable=True)
+        ctx._check(ctx.L.aerof_gpu_matvec(ctx.h, a.ptr, b.ptr, int(transpose)))
+        return b.obj
+
+    def applyTranspose(self, p):
+        return self.apply(p, transpose=True)
+
+    def blocks(self) -> np.ndarray:
+        """The operator in MvpMat layout a[N+2E][5][5] (reference numbering)."""
+        ctx = self.ctx
+        A = np.empty((ctx.N + 2 * ctx.E, 5, 5))
+        ctx._check(ctx.L.aerof_gpu_get_jacobian(ctx.h, C.c_void_p(A.ctypes.data)))
+        return A
+
+
+class JacobiPrec:
+    """Block-Jacobi preconditioner (``JacobiPrec``, KspPrec.C:9-124)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+
+    def setup(self):
+        self.ctx._check(self.ctx.L.aerof_gpu_prec_setup(self.ctx.h))
+
+    def apply(self, x, transpose=False):
+        ctx = self.ctx
+        a = _Arg(x, np.float64, (ctx.N, 5))
+        y = _like(x, (ctx.N, 5))
+        b = _Arg(y, np.float64, writable=True)
+        ctx._check(ctx.L.aerof_gpu_prec_apply(ctx.h, a.ptr, b.ptr, int(transpose)))
+        return b.obj
+
+    def applyT(self, x):
+        return self.apply(x, transpose=True)
+
+
+class GmresSolver:
+    """``GmresSolver`` (KspSolver.C:351-492): right-preconditioned GMRES."""
+
+    def __init__(self, ctx: Context, krylov: int = 30, maxits: int = 30, eps: float = 1e-2):
+        self.ctx, self.krylov, self.maxits, self.eps = ctx, krylov, maxits, eps
+
+    def solve(self, b, transpose=False):
+        ctx = self.ctx
+        bb = _Arg(b, np.float64, (ctx.N, 5))
+        x = _like(b, (ctx.N, 5))
+        xx = _Arg(x, np.float64, writable=True)
+        its, res = C.c_int(), C.c_double()
+        ctx._check(ctx.L.aerof_gpu_gmres(ctx.h, bb.ptr, xx.ptr, self.krylov, self.maxits, self.eps,
+                                         int(transpose), C.byref(its), C.byref(res)))
+        return xx.obj, its.value, res.value
+
+    def solveT(self, b):
+        return self.solve(b, transpose=True)
+
+
+class ImplicitSteadySolver:
+    """Pseudo-transient backward-Euler Newton with GMRES + block-Jacobi."""
+
+    def __init__(self, ctx: Context, precision: int = PREC_FP32, cfl0: float = 10.0, cfl_min: float = 0.0,
+                 cfl_max: float = 1e4, ser: float = 0.7, ksp_eps: float = 1e-2, krylov: int = 30,
+                 maxits: int = 30, tol: float = 1e-8, max_steps: int = 500):
+        self.ctx = ctx
+        self.p = NewtonParams(cfl0, cfl_min, cfl_max, ser, ksp_eps, tol, krylov, maxits, max_steps, precision)
+
+    def solve(self, U):
+        ctx = self.ctx
+        out = U.clone() if _is_torch(U) else np.array(U, dtype=np.float64, copy=True, order="C")
+        a = _Arg(out, np.float64, (ctx.N, 5), writable=True)
+        hist = np.zeros(self.p.max_steps + 1)
+        res = NewtonResult()
+        ctx._check(ctx.L.aerof_gpu_newton(ctx.h, a.ptr, C.byref(self.p), C.byref(res),
+                                          C.c_void_p(hist.ctypes.data)))
+        return a.obj, {"steps": res.steps, "linear_its": res.linear_its, "rel_residual": res.rel_residual,
+                       "seconds": res.seconds, "history": hist[: res.steps + 1]}
+
+
+class Sensitivity:
+    """Exact linearisation of the residual and its transpose."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+
+    def _call(self, fn, U, x, width_in, width_out):
+        ctx = self.ctx
+        u = _Arg(U, np.float64, (ctx.N, 5))
+        a = _Arg(x, np.float64, (ctx.N, width_in))
+        y = _like(x, (ctx.N, width_out))
+        b = _Arg(y, np.float64, writable=True)
+        ctx._check(fn(ctx.h, u.ptr, a.ptr, b.ptr))
+        return b.obj
+
+    def jvp(self, U, v):
+        return self._call(self.ctx.L.aerof_gpu_jvp, U, v, 5, 5)
+
+    def vjp(self, U, w):
+        return self._call(self.ctx.L.aerof_gpu_vjp, U, w, 5, 5)
+
+    def dRdX(self, U, Xdot):
+        return self._call(self.ctx.L.aerof_gpu_dRdX, U, Xdot, 3, 5)
+
+    def dRdX_T(self, U, lam):
+        return self._call(self.ctx.L.aerof_gpu_dRdX_T, U, lam, 5, 3)

@@ -1,0 +1,90 @@
+// capi.cu -- context lifetime, stream selection and host/device staging of
+// the C ABI declared in include/aerof_gpu.h.
+#include <cstring>
+
+#include "common.cuh"
+
+namespace aerof {
+
+bool is_device_ptr(const void* p) {
+  cudaPointerAttributes a;
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+const double* in_dev(aerof_gpu_ctx* c, const double* p, size_t count, DBuf<double>& stage) {
+  if (is_device_ptr(p)) return p;
+  stage.ensure(count);
+  AEROF_CUDA(cudaMemcpyAsync(stage.p, p, count * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  return stage.p;
+}
+
+double* out_dev(aerof_gpu_ctx* c, double* p, size_t count, DBuf<double>& stage) {
+  (void)c;
+  if (is_device_ptr(p)) return p;
+  stage.ensure(count);
+  return stage.p;
+}
+
+void out_finish(aerof_gpu_ctx* c, double* user, const double* dev, size_t count) {
+  if (user != dev)
+    AEROF_CUDA(cudaMemcpyAsync(user, dev, count * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  AEROF_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+}  // namespace aerof
+
+using namespace aerof;
+
+extern "C" int aerof_gpu_create(const aerof_gpu_config* cfg, aerof_gpu_ctx** out) {
+  if (!cfg || !out) return AEROF_EINVAL;
+  *out = nullptr;
+  if (!(cfg->gamma > 1.0) || cfg->beta < 0.0 || cfg->beta > 0.5 ||
+      (cfg->reconstruction != AEROF_REC_CONSTANT && cfg->reconstruction != AEROF_REC_VANALBADA &&
+       cfg->reconstruction != AEROF_REC_LINEAR))
+    return AEROF_EINVAL;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device < 0 || cfg->device >= ndev) {
+    cudaGetLastError();
+    return AEROF_ECUDA;
+  }
+  aerof_gpu_ctx* c = new aerof_gpu_ctx();
+  c->cfg = *cfg;
+  c->dev = cfg->device;
+  if (cudaSetDevice(c->dev) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return AEROF_ECUDA;
+  }
+  c->stream = c->own_stream;
+  *out = c;
+  return AEROF_OK;
+}
+
+extern "C" int aerof_gpu_destroy(aerof_gpu_ctx* c) {
+  if (!c) return AEROF_EINVAL;
+  cudaSetDevice(c->dev);
+  cudaStreamSynchronize(c->stream);
+  cudaStream_t own = c->own_stream;
+  delete c;  // releases every device buffer
+  if (own) cudaStreamDestroy(own);
+  return AEROF_OK;
+}
+
+extern "C" int aerof_gpu_set_stream(aerof_gpu_ctx* c, void* stream) {
+  if (!c) return AEROF_EINVAL;
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return AEROF_OK;
+}
+
+extern "C" int aerof_gpu_last_error(aerof_gpu_ctx* c, char* buf, int len) {
+  if (!c || !buf || len <= 0) return AEROF_EINVAL;
+  std::strncpy(buf, c->last_error.c_str(), (size_t)len - 1);
+  buf[len - 1] = 0;
+  return AEROF_OK;
+}

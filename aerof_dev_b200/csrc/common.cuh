@@ -1,0 +1,210 @@
+// common.cuh -- context, device buffers and error plumbing shared by the
+// kernels of the edge-based FV path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/aerof_gpu.h"
+#include "physics.cuh"
+
+namespace aerof {
+
+// ------------------------------------------------------------------ errors
+struct CudaError {
+  cudaError_t err;
+  const char* where;
+};
+
+#define AEROF_CUDA(call)                                                  \
+  do {                                                                    \
+    cudaError_t e_ = (call);                                              \
+    if (e_ != cudaSuccess) throw ::aerof::CudaError{e_, #call};           \
+  } while (0)
+
+#define AEROF_LAUNCH_CHECK() AEROF_CUDA(cudaGetLastError())
+
+struct ApiError {
+  int code;
+  std::string msg;
+};
+
+// ------------------------------------------------------------------ buffers
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count == n && p) return;
+    release();
+    if (count == 0) return;
+    cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();
+      throw ApiError{AEROF_ENOMEM, "cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes failed"};
+    }
+    n = count;
+  }
+  void ensure(size_t count) {
+    if (count > n) alloc(count);
+  }
+  void upload(const T* h, size_t count, cudaStream_t s) {
+    alloc(count);
+    if (count) AEROF_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void zero(cudaStream_t s) {
+    if (n) AEROF_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// ------------------------------------------------------------------ mesh
+// Device-resident mesh in the kernels' numbering.  Nodes are kept in the
+// caller's numbering; edges are the reference's lexicographic list.
+struct DeviceMesh {
+  int N = 0, T = 0, F = 0, E = 0;
+  double Ub[5] = {0, 0, 0, 0, 0};
+  DBuf<double> Ubd;        // [5] free-stream conservative state on the device
+  // node record: V (5) + X (3), 64 bytes per node
+  DBuf<double> P;
+  DBuf<double> X;          // [N][3] (copy used by geometry/derivative kernels)
+  DBuf<int> tets;          // [T][4]
+  DBuf<int> tet_edge;      // [T][6]
+  DBuf<int2> edges;        // [E] (i, j), i < j
+  DBuf<double> en;         // [3][E] edge normals, SoA
+  DBuf<double> fnrm;       // [3][F] face normals, SoA
+  DBuf<int> faces;         // [F][3]
+  DBuf<int> fcode;         // [F]
+  DBuf<double> vol;        // [N]
+  DBuf<double> lsqR;       // [6][N] Cholesky factors (r11 r12 r13 r22 r23 r33)
+  DBuf<double> lsqW;       // [6][N] or11 or22 or33 r12or11 r23or22 psi
+  // node -> incident edges in the reference's accumulation order (neighbour
+  // ascending).  nbr_edge holds edge id, sign bit set when the node is the
+  // edge's second endpoint.
+  DBuf<int> nbr_ptr;       // [N+1]
+  DBuf<int> nbr_node;      // [2E]
+  DBuf<int> nbr_edge;      // [2E]  (edge id) | (0x80000000 if node is j)
+  DBuf<int> nbr_tpos;      // [2E]  position of the mirrored entry (row nbr, col node)
+  DBuf<int2> edge_pos;     // [E]   CSR positions of (i,j) in row i and (j,i) in row j
+  // node -> incident boundary faces, ascending face id
+  DBuf<int> nf_ptr;        // [N+1]
+  DBuf<int> nf_face;       // [3F]
+  // edge -> incident tets (ascending) with local edge index
+  DBuf<int> et_ptr;        // [E+1]
+  DBuf<int> et_tet;        // [6T]  tet*8 + local edge
+  // node -> incident tets (ascending) with local vertex index
+  DBuf<int> nt_ptr;        // [N+1]
+  DBuf<int> nt_tet;        // [4T]  tet*4 + local vertex
+  // host copies for queries
+  std::vector<int> h_edges;
+};
+
+struct Scratch {
+  DBuf<double> G;          // [N][16] gradients ddx(5) ddy(5) ddz(5) pad
+  DBuf<double> flux;       // [5][E] per-edge fluxes
+  DBuf<double> Ustage, Rstage, Vstage, Xstage;  // staging for host arrays
+  DBuf<double> dt, k1, k2, U0;
+  DBuf<int> tag;           // [N] failsafe tags
+  DBuf<int> counters;      // [8] device counters
+  DBuf<double> red;        // reduction partials
+  DBuf<double> redout;     // reduction results
+};
+
+// Implicit operator: BSR-by-rows of the H1 Jacobian.
+struct Implicit {
+  int precision = 0;       // 32 or 64, 0 = not assembled
+  DBuf<double> diag64, off64, dinv64;   // [N][25], [2E][25], [N][25]
+  DBuf<float> diag32, off32, dinv32;
+  DBuf<double> diagscr;    // [E][2][25] per-edge diagonal contributions
+  bool prec_ready = false;
+  // Krylov workspace
+  DBuf<double> basis;      // [(m+1)][5N]
+  DBuf<double> w, r, x, b, t;
+  DBuf<double> hcol;       // device scratch for one Hessenberg column
+};
+
+// Dual-number work arrays of the forward-mode linearisation.
+struct DualWork {
+  DBuf<Dual> XD, PD, GD, WD, RD, volD, enD, fnD, fluxD;
+};
+
+// Reverse-mode work arrays.
+struct AdjWork {
+  DBuf<double> edge;       // [E][20] per-edge cotangent contributions
+  DBuf<double> gG;         // [N][16] gradient cotangents
+  DBuf<double> gV;         // [N][5] direct state cotangents
+  DBuf<double> lam;        // [N][5] w / vol
+};
+
+}  // namespace aerof
+
+struct aerof_gpu_ctx {
+  aerof_gpu_config cfg;
+  int dev = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  bool has_mesh = false;
+  aerof::DeviceMesh mesh;
+  aerof::Scratch s;
+  aerof::Implicit imp;
+  aerof::DualWork dual;
+  aerof::AdjWork adj;
+  std::string last_error;
+};
+
+namespace aerof {
+
+// Staging: return a device pointer holding the contents of `p` (count
+// doubles); host arrays are copied into `stage`.
+bool is_device_ptr(const void* p);
+const double* in_dev(aerof_gpu_ctx* c, const double* p, size_t count, DBuf<double>& stage);
+double* out_dev(aerof_gpu_ctx* c, double* p, size_t count, DBuf<double>& stage);
+void out_finish(aerof_gpu_ctx* c, double* user, const double* dev, size_t count);
+
+template <class F>
+int guard(aerof_gpu_ctx* c, F&& f) {
+  if (!c) return AEROF_EINVAL;
+  try {
+    cudaSetDevice(c->dev);
+    return f();
+  } catch (const CudaError& e) {
+    c->last_error = std::string(e.where) + ": " + cudaGetErrorString(e.err);
+    return AEROF_ECUDA;
+  } catch (const ApiError& e) {
+    c->last_error = e.msg;
+    return e.code;
+  } catch (const std::exception& e) {
+    c->last_error = e.what();
+    return AEROF_EINVAL;
+  }
+}
+
+inline int grid_for(size_t n, int block) { return (int)((n + block - 1) / block); }
+
+// implemented in mesh.cu: geometry of coordinates XD ([N][3]) in dual
+// numbers, same kernels and order as the primal set-up
+void geometry_dual(aerof_gpu_ctx* c, const Dual* XD, Dual* volD, Dual* enD, Dual* fnD, Dual* RD);
+
+// implemented in residual.cu (used by implicit.cu and adjoint.cu)
+int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR);
+void prim_dev(aerof_gpu_ctx* c, const double* dU);
+void gradients_dev(aerof_gpu_ctx* c);
+void timestep_dev(aerof_gpu_ctx* c, const double* dU, double cfl, double* ddt);
+double norm2_dev(aerof_gpu_ctx* c, const double* x, size_t n);
+double dot_dev(aerof_gpu_ctx* c, const double* x, const double* y, size_t n);
+
+}  // namespace aerof

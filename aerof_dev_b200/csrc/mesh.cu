@@ -1,0 +1,369 @@
+// mesh.cu -- mesh set-up: integer preprocessing on the host (edge list,
+// incidence lists; all bit-exact integer work) and the static geometry on
+// the device (control volumes, dual-cell edge normals, boundary face
+// normals, least-squares factors), each accumulated per output item in the
+// reference's element/edge order so the sums are deterministic.
+#include <algorithm>
+#include <numeric>
+
+#include "common.cuh"
+#include "physics.cuh"
+
+namespace aerof {
+
+constexpr int kMBlock = 256;
+
+// ElemTet tables (ElemTetCore.C:19-21)
+__constant__ int c_edgeEnd[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+__constant__ int c_edgeFace[6][2] = {{0, 1}, {2, 0}, {1, 2}, {0, 3}, {3, 1}, {2, 3}};
+static const int h_edgeEnd[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+
+template <class T>
+struct Vec3 {
+  T x, y, z;
+};
+template <class T> __device__ __forceinline__ Vec3<T> v3(T a, T b, T c) { return Vec3<T>{a, b, c}; }
+template <class T> __device__ __forceinline__ Vec3<T> operator+(Vec3<T> a, Vec3<T> b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+template <class T> __device__ __forceinline__ Vec3<T> operator-(Vec3<T> a, Vec3<T> b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+template <class T> __device__ __forceinline__ Vec3<T> scale(double c, Vec3<T> a) { return v3(c * a.x, c * a.y, c * a.z); }
+// Vec3D::operator^ (Vector3D.h:266-274)
+template <class T> __device__ __forceinline__ Vec3<T> cross(Vec3<T> a, Vec3<T> b) {
+  return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+template <class T> __device__ __forceinline__ Vec3<T> node_x(const T* X, int n) {
+  return v3(X[3 * (size_t)n], X[3 * (size_t)n + 1], X[3 * (size_t)n + 2]);
+}
+
+// Signed tet volume (ElemTetCore.C:24-39): sixth * v3 . (v1 ^ v2)
+template <class T>
+__device__ __forceinline__ T tet_volume(const T* X, const int* nd) {
+  Vec3<T> x0 = node_x(X, nd[0]);
+  Vec3<T> v1 = node_x(X, nd[1]) - x0, v2 = node_x(X, nd[2]) - x0, v3_ = node_x(X, nd[3]) - x0;
+  Vec3<T> c = cross(v1, v2);
+  const double sixth = 1.0 / 6.0;
+  return sixth * (v3_.x * c.x + v3_.y * c.y + v3_.z * c.z);
+}
+
+// Dual-cell facet normal of local edge l of a tet, oriented from the lower
+// to the higher global node id: ElemTet::computeEdgeNormalsGCL1
+// (ElemTetCore.C:281-330) with Xn = Xnp1.
+template <class T>
+__device__ __forceinline__ Vec3<T> tet_edge_normal(const T* X, const int* nd, int l) {
+  const double third = 1.0 / 3.0;
+  Vec3<T> x[4] = {node_x(X, nd[0]), node_x(X, nd[1]), node_x(X, nd[2]), node_x(X, nd[3])};
+  Vec3<T> f[4];
+  f[0] = scale(third, x[0] + x[1] + x[2]);
+  f[1] = scale(third, x[0] + x[1] + x[3]);
+  f[2] = scale(third, x[0] + x[2] + x[3]);
+  f[3] = scale(third, x[1] + x[2] + x[3]);
+  Vec3<T> g = scale(0.25, x[0] + x[1] + x[2] + x[3]);
+  Vec3<T> xg0 = f[c_edgeFace[l][0]] - g;
+  Vec3<T> xg1 = f[c_edgeFace[l][1]] - g;
+  Vec3<T> c = cross(xg1, xg0);
+  Vec3<T> n = scale(0.5, c + c) + scale(0.25, c + c);
+  if (nd[c_edgeEnd[l][0]] < nd[c_edgeEnd[l][1]]) return n;
+  return v3(-n.x, -n.y, -n.z);
+}
+
+// FaceTria::computeNormalGCL1 (FaceTriaCore.C:65-82) with Xn = Xnp1:
+// twelfth * ((3 x02) ^ x01 + (3 x02) ^ x01), outward for the face ordering.
+template <class T>
+__device__ __forceinline__ Vec3<T> face_normal(const T* X, const int* nd) {
+  const double twelfth = 1.0 / 12.0;
+  Vec3<T> x0 = node_x(X, nd[0]);
+  Vec3<T> x01 = node_x(X, nd[1]) - x0, x02 = node_x(X, nd[2]) - x0;
+  Vec3<T> a = scale(2.0, x02) + x02;
+  Vec3<T> s = cross(a, x01) + cross(a, x01);
+  return scale(twelfth, s);
+}
+
+template <class T>
+__global__ void k_ctrl_vol(int N, const T* __restrict__ X, const int* __restrict__ tets,
+                           const int* __restrict__ nt_ptr, const int* __restrict__ nt_tet, T* __restrict__ vol) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  T v(0.0);
+  for (int p = nt_ptr[i]; p < nt_ptr[i + 1]; ++p) {
+    int t = nt_tet[p] >> 2;
+    v += 0.25 * tet_volume(X, tets + 4 * (size_t)t);
+  }
+  vol[i] = v;
+}
+
+template <class T>
+__global__ void k_edge_normals(int E, const T* __restrict__ X, const int* __restrict__ tets,
+                               const int* __restrict__ et_ptr, const int* __restrict__ et_tet, T* __restrict__ en) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  T a(0.0), b(0.0), c(0.0);
+  for (int p = et_ptr[e]; p < et_ptr[e + 1]; ++p) {
+    int t = et_tet[p] >> 3, l = et_tet[p] & 7;
+    Vec3<T> n = tet_edge_normal(X, tets + 4 * (size_t)t, l);
+    a += n.x; b += n.y; c += n.z;
+  }
+  en[e] = a; en[(size_t)E + e] = b; en[2 * (size_t)E + e] = c;
+}
+
+template <class T>
+__global__ void k_face_normals(int F, const T* __restrict__ X, const int* __restrict__ faces, T* __restrict__ fn) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= F) return;
+  Vec3<T> n = face_normal(X, faces + 3 * (size_t)f);
+  fn[f] = n.x; fn[(size_t)F + f] = n.y; fn[2 * (size_t)F + f] = n.z;
+}
+
+// SubDomain::computeWeightsLeastSquaresEdgePart/NodePart
+// (SubDomainCore.C:1334-1381, 1755-1777), per node over its neighbours in
+// ascending order (the reference's edge order for that node).
+template <class T>
+__global__ void k_lsq_R(int N, const T* __restrict__ X, const int* __restrict__ nbr_ptr,
+                        const int* __restrict__ nbr_node, T* __restrict__ R) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  T s[6] = {T(0.0), T(0.0), T(0.0), T(0.0), T(0.0), T(0.0)};
+  Vec3<T> xi = node_x(X, i);
+  for (int p = nbr_ptr[i]; p < nbr_ptr[i + 1]; ++p) {
+    Vec3<T> d = node_x(X, nbr_node[p]) - xi;
+    s[0] += d.x * d.x; s[1] += d.x * d.y; s[2] += d.x * d.z;
+    s[3] += d.y * d.y; s[4] += d.y * d.z; s[5] += d.z * d.z;
+  }
+  T r11 = dsqrt(s[0]);
+  T or11 = 1.0 / r11;
+  T r12 = s[1] * or11;
+  T r13 = s[2] * or11;
+  T r22 = dsqrt(s[3] - r12 * r12);
+  T r23 = (s[4] - r12 * r13) / r22;
+  T r33 = dsqrt(s[5] - (r13 * r13 + r23 * r23));
+  R[i] = r11; R[(size_t)N + i] = r12; R[2 * (size_t)N + i] = r13;
+  R[3 * (size_t)N + i] = r22; R[4 * (size_t)N + i] = r23; R[5 * (size_t)N + i] = r33;
+}
+
+__global__ void k_lsq_W(int N, const double* __restrict__ R, double* __restrict__ W) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double r[6], w[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) r[k] = R[(size_t)k * N + i];
+  lsq_node_constants(r, w);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) W[(size_t)k * N + i] = w[k];
+}
+
+__global__ void k_setX(int N, const double* __restrict__ X, double* __restrict__ P) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  P[8 * (size_t)i + 5] = X[3 * (size_t)i];
+  P[8 * (size_t)i + 6] = X[3 * (size_t)i + 1];
+  P[8 * (size_t)i + 7] = X[3 * (size_t)i + 2];
+}
+
+
+// ------------------------------------------------------------------ host
+struct HostMesh {
+  std::vector<int> edge_pos;
+  std::vector<int> edges, tet_edge, nbr_ptr, nbr_node, nbr_edge, nbr_tpos, nf_ptr, nf_face, et_ptr, et_tet,
+      nt_ptr, nt_tet;
+};
+
+// EdgeSet::find + createPointers (EdgeCore.C:55-117): unique (min,max)
+// pairs of the tet edges, numbered lexicographically.
+static void build_host(int N, int T, int F, const int* tets, const int* faces, HostMesh& h, int& E) {
+  std::vector<uint64_t> keys((size_t)T * 6);
+  for (int t = 0; t < T; ++t)
+    for (int l = 0; l < 6; ++l) {
+      uint64_t a = (uint32_t)tets[4 * (size_t)t + h_edgeEnd[l][0]];
+      uint64_t b = (uint32_t)tets[4 * (size_t)t + h_edgeEnd[l][1]];
+      if (a > b) std::swap(a, b);
+      keys[6 * (size_t)t + l] = (a << 32) | b;
+    }
+  std::vector<uint64_t> u(keys);
+  std::sort(u.begin(), u.end());
+  u.erase(std::unique(u.begin(), u.end()), u.end());
+  if (u.size() > (size_t)0x3fffffff) throw ApiError{AEROF_EINVAL, "too many edges"};
+  E = (int)u.size();
+  h.edges.resize(2 * (size_t)E);
+  for (int l = 0; l < E; ++l) {
+    h.edges[2 * (size_t)l] = (int)(u[l] >> 32);
+    h.edges[2 * (size_t)l + 1] = (int)(u[l] & 0xffffffffu);
+  }
+  h.tet_edge.resize((size_t)T * 6);
+  for (size_t k = 0; k < keys.size(); ++k)
+    h.tet_edge[k] = (int)(std::lower_bound(u.begin(), u.end(), keys[k]) - u.begin());
+  // node -> neighbours ascending: appending edges in lexicographic order
+  // gives, per node, incoming edges (k<i) by k then outgoing (i<j) by j.
+  h.nbr_ptr.assign(N + 1, 0);
+  for (int l = 0; l < E; ++l) { h.nbr_ptr[h.edges[2 * l] + 1]++; h.nbr_ptr[h.edges[2 * l + 1] + 1]++; }
+  for (int i = 0; i < N; ++i) h.nbr_ptr[i + 1] += h.nbr_ptr[i];
+  h.nbr_node.resize(2 * (size_t)E);
+  h.nbr_edge.resize(2 * (size_t)E);
+  h.nbr_tpos.resize(2 * (size_t)E);
+  h.edge_pos.resize(2 * (size_t)E);
+  std::vector<int> pos(h.nbr_ptr.begin(), h.nbr_ptr.end() - 1);
+  for (int l = 0; l < E; ++l) {
+    int i = h.edges[2 * l], j = h.edges[2 * l + 1];
+    int pi = pos[i]++, pj = pos[j]++;
+    h.nbr_node[pi] = j; h.nbr_edge[pi] = l;
+    h.nbr_node[pj] = i; h.nbr_edge[pj] = (int)((unsigned)l | 0x80000000u);
+    h.nbr_tpos[pi] = pj; h.nbr_tpos[pj] = pi;
+    h.edge_pos[2 * (size_t)l] = pi; h.edge_pos[2 * (size_t)l + 1] = pj;
+  }
+  // node -> faces (ascending face id)
+  h.nf_ptr.assign(N + 1, 0);
+  for (size_t q = 0; q < 3 * (size_t)F; ++q) h.nf_ptr[faces[q] + 1]++;
+  for (int i = 0; i < N; ++i) h.nf_ptr[i + 1] += h.nf_ptr[i];
+  h.nf_face.resize(3 * (size_t)F);
+  pos.assign(h.nf_ptr.begin(), h.nf_ptr.end() - 1);
+  for (int f = 0; f < F; ++f)
+    for (int l = 0; l < 3; ++l) h.nf_face[pos[faces[3 * (size_t)f + l]]++] = f;
+  // edge -> tets (ascending tet id)
+  h.et_ptr.assign(E + 1, 0);
+  for (size_t k = 0; k < h.tet_edge.size(); ++k) h.et_ptr[h.tet_edge[k] + 1]++;
+  for (int l = 0; l < E; ++l) h.et_ptr[l + 1] += h.et_ptr[l];
+  h.et_tet.resize((size_t)T * 6);
+  pos.assign(h.et_ptr.begin(), h.et_ptr.end() - 1);
+  for (int t = 0; t < T; ++t)
+    for (int l = 0; l < 6; ++l) h.et_tet[pos[h.tet_edge[6 * (size_t)t + l]]++] = t * 8 + l;
+  // node -> tets (ascending tet id)
+  h.nt_ptr.assign(N + 1, 0);
+  for (size_t q = 0; q < 4 * (size_t)T; ++q) h.nt_ptr[tets[q] + 1]++;
+  for (int i = 0; i < N; ++i) h.nt_ptr[i + 1] += h.nt_ptr[i];
+  h.nt_tet.resize(4 * (size_t)T);
+  pos.assign(h.nt_ptr.begin(), h.nt_ptr.end() - 1);
+  for (int t = 0; t < T; ++t)
+    for (int l = 0; l < 4; ++l) h.nt_tet[pos[tets[4 * (size_t)t + l]]++] = t * 4 + l;
+}
+
+void compute_geometry(aerof_gpu_ctx* c) {
+  DeviceMesh& m = c->mesh;
+  cudaStream_t s = c->stream;
+  m.vol.alloc(m.N);
+  m.en.alloc(3 * (size_t)m.E);
+  m.fnrm.alloc(3 * (size_t)std::max(m.F, 1));
+  m.lsqR.alloc(6 * (size_t)m.N);
+  m.lsqW.alloc(6 * (size_t)m.N);
+  k_ctrl_vol<double><<<grid_for(m.N, kMBlock), kMBlock, 0, s>>>(m.N, m.X.p, m.tets.p, m.nt_ptr.p, m.nt_tet.p, m.vol.p);
+  AEROF_LAUNCH_CHECK();
+  k_edge_normals<double><<<grid_for(m.E, kMBlock), kMBlock, 0, s>>>(m.E, m.X.p, m.tets.p, m.et_ptr.p, m.et_tet.p, m.en.p);
+  AEROF_LAUNCH_CHECK();
+  if (m.F) {
+    k_face_normals<double><<<grid_for(m.F, kMBlock), kMBlock, 0, s>>>(m.F, m.X.p, m.faces.p, m.fnrm.p);
+    AEROF_LAUNCH_CHECK();
+  }
+  k_lsq_R<double><<<grid_for(m.N, kMBlock), kMBlock, 0, s>>>(m.N, m.X.p, m.nbr_ptr.p, m.nbr_node.p, m.lsqR.p);
+  AEROF_LAUNCH_CHECK();
+  k_lsq_W<<<grid_for(m.N, kMBlock), kMBlock, 0, s>>>(m.N, m.lsqR.p, m.lsqW.p);
+  AEROF_LAUNCH_CHECK();
+  k_setX<<<grid_for(m.N, kMBlock), kMBlock, 0, s>>>(m.N, m.X.p, m.P.p);
+  AEROF_LAUNCH_CHECK();
+}
+
+void geometry_dual(aerof_gpu_ctx* c, const Dual* XD, Dual* volD, Dual* enD, Dual* fnD, Dual* RD) {
+  DeviceMesh& m = c->mesh;
+  cudaStream_t s = c->stream;
+  k_ctrl_vol<Dual><<<grid_for(m.N, kMBlock), kMBlock, 0, s>>>(m.N, XD, m.tets.p, m.nt_ptr.p, m.nt_tet.p, volD);
+  AEROF_LAUNCH_CHECK();
+  k_edge_normals<Dual><<<grid_for(m.E, kMBlock), kMBlock, 0, s>>>(m.E, XD, m.tets.p, m.et_ptr.p, m.et_tet.p, enD);
+  AEROF_LAUNCH_CHECK();
+  if (m.F) {
+    k_face_normals<Dual><<<grid_for(m.F, kMBlock), kMBlock, 0, s>>>(m.F, XD, m.faces.p, fnD);
+    AEROF_LAUNCH_CHECK();
+  }
+  k_lsq_R<Dual><<<grid_for(m.N, kMBlock), kMBlock, 0, s>>>(m.N, XD, m.nbr_ptr.p, m.nbr_node.p, RD);
+  AEROF_LAUNCH_CHECK();
+}
+
+}  // namespace aerof
+
+using namespace aerof;
+
+extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const double* X, const int* tets,
+                                  const int* faces, const int* codes, const double* Ub) {
+  return guard(c, [&]() -> int {
+    if (N <= 0 || T <= 0 || F < 0 || !X || !tets || (F && (!faces || !codes)) || !Ub) return AEROF_EINVAL;
+    for (size_t q = 0; q < 4 * (size_t)T; ++q)
+      if (tets[q] < 0 || tets[q] >= N) { c->last_error = "tet node index out of range"; return AEROF_EINVAL; }
+    for (size_t q = 0; q < 3 * (size_t)F; ++q)
+      if (faces[q] < 0 || faces[q] >= N) { c->last_error = "face node index out of range"; return AEROF_EINVAL; }
+    for (int f = 0; f < F; ++f)
+      if (codes[f] != AEROF_BC_SLIP_WALL_MOVING && codes[f] != AEROF_BC_INLET_MOVING &&
+          codes[f] != AEROF_BC_OUTLET_MOVING) {
+        c->last_error = "unsupported boundary code " + std::to_string(codes[f]);
+        return AEROF_EINVAL;
+      }
+    c->has_mesh = false;
+    c->imp.precision = 0;
+    c->imp.prec_ready = false;
+    HostMesh h;
+    int E = 0;
+    build_host(N, T, F, tets, faces, h, E);
+    DeviceMesh& m = c->mesh;
+    cudaStream_t s = c->stream;
+    m.N = N; m.T = T; m.F = F; m.E = E;
+    for (int k = 0; k < 5; ++k) m.Ub[k] = Ub[k];
+    m.Ubd.upload(Ub, 5, s);
+    m.X.upload(X, 3 * (size_t)N, s);
+    m.P.alloc(8 * (size_t)N);
+    m.P.zero(s);
+    m.tets.upload(tets, 4 * (size_t)T, s);
+    m.tet_edge.upload(h.tet_edge.data(), h.tet_edge.size(), s);
+    m.edges.upload(reinterpret_cast<const int2*>(h.edges.data()), (size_t)E, s);
+    if (F) {
+      m.faces.upload(faces, 3 * (size_t)F, s);
+      m.fcode.upload(codes, (size_t)F, s);
+    } else {
+      m.faces.alloc(3); m.fcode.alloc(1);
+    }
+    m.nbr_ptr.upload(h.nbr_ptr.data(), h.nbr_ptr.size(), s);
+    m.nbr_node.upload(h.nbr_node.data(), h.nbr_node.size(), s);
+    m.nbr_edge.upload(h.nbr_edge.data(), h.nbr_edge.size(), s);
+    m.nbr_tpos.upload(h.nbr_tpos.data(), h.nbr_tpos.size(), s);
+    m.edge_pos.upload(reinterpret_cast<const int2*>(h.edge_pos.data()), (size_t)E, s);
+    m.nf_ptr.upload(h.nf_ptr.data(), h.nf_ptr.size(), s);
+    if (F) m.nf_face.upload(h.nf_face.data(), h.nf_face.size(), s);
+    else m.nf_face.alloc(1);
+    m.et_ptr.upload(h.et_ptr.data(), h.et_ptr.size(), s);
+    m.et_tet.upload(h.et_tet.data(), h.et_tet.size(), s);
+    m.nt_ptr.upload(h.nt_ptr.data(), h.nt_ptr.size(), s);
+    m.nt_tet.upload(h.nt_tet.data(), h.nt_tet.size(), s);
+    m.h_edges.swap(h.edges);
+    compute_geometry(c);
+    AEROF_CUDA(cudaStreamSynchronize(s));
+    c->has_mesh = true;
+    return AEROF_OK;
+  });
+}
+
+extern "C" int aerof_gpu_mesh_sizes(aerof_gpu_ctx* c, int* N, int* E, int* F) {
+  if (!c) return AEROF_EINVAL;
+  if (N) *N = c->mesh.N;
+  if (E) *E = c->mesh.E;
+  if (F) *F = c->mesh.F;
+  return c->has_mesh ? AEROF_OK : AEROF_ESTATE;
+}
+
+extern "C" int aerof_gpu_get_edges(aerof_gpu_ctx* c, int* edges) {
+  if (!c || !edges) return AEROF_EINVAL;
+  if (!c->has_mesh) return AEROF_ESTATE;
+  std::copy(c->mesh.h_edges.begin(), c->mesh.h_edges.end(), edges);
+  return AEROF_OK;
+}
+
+extern "C" int aerof_gpu_get_geometry(aerof_gpu_ctx* c, double* edge_normal, double* face_normal, double* ctrl_vol,
+                                      double* lsq_R) {
+  return guard(c, [&]() -> int {
+    if (!c->has_mesh) return AEROF_ESTATE;
+    DeviceMesh& m = c->mesh;
+    auto soa_to_aos = [&](const DBuf<double>& src, int n, int w, double* dst) {
+      std::vector<double> h((size_t)n * w);
+      AEROF_CUDA(cudaMemcpyAsync(h.data(), src.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      AEROF_CUDA(cudaStreamSynchronize(c->stream));
+      for (int i = 0; i < n; ++i)
+        for (int k = 0; k < w; ++k) dst[(size_t)w * i + k] = h[(size_t)k * n + i];
+    };
+    if (edge_normal) soa_to_aos(m.en, m.E, 3, edge_normal);
+    if (face_normal && m.F) soa_to_aos(m.fnrm, m.F, 3, face_normal);
+    if (ctrl_vol) soa_to_aos(m.vol, m.N, 1, ctrl_vol);
+    if (lsq_R) soa_to_aos(m.lsqR, m.N, 6, lsq_R);
+    return AEROF_OK;
+  });
+}

@@ -1,0 +1,469 @@
+// physics.cuh -- pointwise device functions of the Euler finite-volume path.
+//
+// Each function states the reference routine whose arithmetic it keeps
+// (file:line in the AERO-F tree).  They are templated on the scalar type so
+// the same source yields the primal kernels (double) and the exact
+// forward-mode linearisation (Dual, adjoint.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace aerof {
+
+#define AEROF_HD __host__ __device__ __forceinline__
+
+// ------------------------------------------------------------ dual numbers
+struct Dual {
+  double v, d;
+  AEROF_HD Dual() : v(0), d(0) {}
+  AEROF_HD Dual(double a) : v(a), d(0) {}
+  AEROF_HD Dual(double a, double b) : v(a), d(b) {}
+};
+AEROF_HD Dual operator+(Dual a, Dual b) { return Dual(a.v + b.v, a.d + b.d); }
+AEROF_HD Dual operator-(Dual a, Dual b) { return Dual(a.v - b.v, a.d - b.d); }
+AEROF_HD Dual operator-(Dual a) { return Dual(-a.v, -a.d); }
+AEROF_HD Dual operator*(Dual a, Dual b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
+AEROF_HD Dual operator/(Dual a, Dual b) {
+  double q = a.v / b.v;
+  return Dual(q, (a.d - q * b.d) / b.v);
+}
+AEROF_HD Dual& operator+=(Dual& a, Dual b) { a = a + b; return a; }
+AEROF_HD Dual& operator-=(Dual& a, Dual b) { a = a - b; return a; }
+AEROF_HD Dual& operator*=(Dual& a, Dual b) { a = a * b; return a; }
+AEROF_HD Dual dsqrt(Dual a) { double s = sqrt(a.v); return Dual(s, a.d / (2.0 * s)); }
+AEROF_HD double dsqrt(double a) { return sqrt(a); }
+AEROF_HD double vof(double a) { return a; }
+AEROF_HD double vof(Dual a) { return a.v; }
+template <class T> AEROF_HD T tmax0(T a) { return vof(a) < 0.0 ? T(0.0) : a; }
+template <class T> AEROF_HD T tmin0(T a) { return vof(a) > 0.0 ? T(0.0) : a; }
+template <class T> AEROF_HD T tabs(T a) { return vof(a) < 0.0 ? -a : a; }
+
+// ------------------------------------------------------------ gas model
+struct Gas {
+  double gam, gam1, invgam1;
+};
+AEROF_HD Gas make_gas(double gam) {
+  Gas g;
+  g.gam = gam;
+  g.gam1 = gam - 1.0;
+  g.invgam1 = 1.0 / g.gam1;
+  return g;
+}
+
+// VarFcnSGEuler::conservativeToPrimitive (VarFcnSGEuler.h:307-327), Pstiff=0
+template <class T>
+AEROF_HD void cons2prim(const Gas& g, const T* U, T* V) {
+  V[0] = U[0];
+  T invRho = 1.0 / U[0];
+  V[1] = U[1] * invRho;
+  V[2] = U[2] * invRho;
+  V[3] = U[3] * invRho;
+  T vel2 = V[1] * V[1] + V[2] * V[2] + V[3] * V[3];
+  V[4] = g.gam1 * (U[4] - 0.5 * U[0] * vel2);
+}
+
+// ------------------------------------------------------------ least squares
+// Per-node constants of computeLocalWeightsLeastSquares (SubDomain.C:137-159):
+// they depend on R_i only, so they are formed once per mesh:
+// w = (or11, or22, or33, r12or11, r23or22, psi).
+AEROF_HD void lsq_node_constants(const double* R, double* w) {
+  double or11 = 1.0 / R[0];
+  double or22 = 1.0 / R[3];
+  double or33 = 1.0 / R[5];
+  w[0] = or11;
+  w[1] = or22;
+  w[2] = or33;
+  w[3] = R[1] * or11;
+  w[4] = R[4] * or22;
+  w[5] = (R[1] * R[4] - R[2] * R[3]) * or11 * or22;
+}
+// W(dx) from the per-node constants (same operations as the reference).
+template <class T>
+AEROF_HD void lsq_weights(const T* w, T dx0, T dx1, T dx2, T& W0, T& W1, T& W2) {
+  T alpha1 = dx0 * w[0] * w[0];
+  T alpha2 = (dx1 - w[3] * dx0) * w[1] * w[1];
+  T alpha3 = (dx2 - w[4] * dx1 + w[5] * dx0) * w[2] * w[2];
+  W0 = alpha1 - w[3] * alpha2 + w[5] * alpha3;
+  W1 = alpha2 - w[4] * alpha3;
+  W2 = alpha3;
+}
+
+// ------------------------------------------------------------ reconstruction
+// RecFcn::computeVanAlbadaFcn (RecFcn.h:268-281)
+template <class T>
+AEROF_HD T vanalbada_fcn(T a, T b) {
+  const double eps = 1.e-16;
+  T a2 = a * a;
+  T b2 = b * b;
+  double ab = vof(a * b);
+  if (ab > 0.0) return (a * (b2 + eps) + b * (a2 + eps)) / (a2 + b2 + 2.0 * eps);
+  if (ab == 0.0) return 0.5 * eps * (a + b) / (a2 + b2 + 2.0 * eps);
+  return T(0.0);
+}
+// RecFcn::vanalbada (RecFcn.h:432-446); beta2 = 1-2 beta
+template <class T>
+AEROF_HD void vanalbada(double beta, T Vi, T ddVij, T Vj, T ddVji, T& Vij, T& Vji) {
+  const double beta2 = 1.0 - 2.0 * beta;
+  T dVji = Vj - Vi;
+  T dV = beta2 * dVji;
+  T dVi = dV + 2.0 * beta * ddVij;
+  T dVj = dV + 2.0 * beta * ddVji;
+  Vij = Vi + 0.5 * vanalbada_fcn(dVi, dVji);
+  Vji = Vj - 0.5 * vanalbada_fcn(dVj, dVji);
+}
+// RecFcn::linear (RecFcn.h:240-249); beta1 = 1/2 - beta
+template <class T>
+AEROF_HD void linear_rec(double beta, T Vi, T ddVij, T Vj, T ddVji, T& Vij, T& Vji) {
+  const double beta1 = 0.5 - beta;
+  T dV = beta1 * (Vj - Vi);
+  Vij = Vi + dV + beta * ddVij;
+  Vji = Vj - dV - beta * ddVji;
+}
+
+// ------------------------------------------------------------ fluxes
+// roeflux7.f:1-202 (type 0, pstiff = 0, static mesh vitno = 0): Roe-averaged
+// upwind selection of the physical flux plus the one-wave dissipation term.
+template <class T>
+AEROF_HD void roe_flux(const Gas& g, T n0, T n1, T n2, const T* Ug, const T* Ud, T* phi) {
+  const double gam = g.gam, gam1 = g.gam1, invgam1 = g.invgam1;
+  T rnorm = dsqrt(n0 * n0 + n1 * n1 + n2 * n2);
+  T invnorm = 1.0 / rnorm;
+  T nx = n0 * invnorm, ny = n1 * invnorm, nz = n2 * invnorm;
+  T vitg2 = Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3];
+  T vitd2 = Ud[1] * Ud[1] + Ud[2] * Ud[2] + Ud[3] * Ud[3];
+  T squsr1 = dsqrt(Ug[0]);
+  T squsr2 = dsqrt(Ud[0]);
+  T ener1 = Ug[4] * invgam1 + 0.5 * Ug[0] * vitg2;
+  T ener2 = Ud[4] * invgam1 + 0.5 * Ud[0] * vitd2;
+  T usro = 1.0 / (squsr1 + squsr2);
+  T uar2 = (squsr1 * Ug[1] + squsr2 * Ud[1]) * usro;
+  T uar3 = (squsr1 * Ug[2] + squsr2 * Ud[2]) * usro;
+  T uar4 = (squsr1 * Ug[3] + squsr2 * Ud[3]) * usro;
+  T uar5 = ((ener1 + Ug[4]) / squsr1 + (ener2 + Ud[4]) / squsr2) * usro;
+  T VdotN = nx * uar2 + ny * uar3 + nz * uar4;
+  const bool left = vof(VdotN) > 0.0;
+  // centred (upwind-side physical) flux
+  const T* Us = left ? Ug : Ud;
+  T vits2 = left ? vitg2 : vitd2;
+  T vn = Us[1] * nx + Us[2] * ny + Us[3] * nz;
+  T H = gam * Us[4] + 0.5 * gam1 * Us[0] * vits2;
+  H = H / (gam1 * Us[0]);
+  T f0 = Us[0] * vn;
+  T f1 = f0 * Us[1] + Us[4] * nx;
+  T f2 = f0 * Us[2] + Us[4] * ny;
+  T f3 = f0 * Us[3] + Us[4] * nz;
+  T f4 = f0 * H;
+  // dissipation
+  T qir = 0.5 * (uar2 * uar2 + uar3 * uar3 + uar4 * uar4);
+  T cr2 = gam1 * (uar5 - qir);
+  T cr = dsqrt(cr2);
+  cr2 = 1.0 / cr2;
+  T dif1 = Ud[0] - Ug[0];
+  T dif2 = -Ug[0] * Ug[1] + Ud[0] * Ud[1];
+  T dif3 = -Ug[0] * Ug[2] + Ud[0] * Ud[2];
+  T dif4 = -Ug[0] * Ug[3] + Ud[0] * Ud[3];
+  T dif5 = ener2 - ener1;
+  T invtbeta2 = -1.0 / cr;
+  T A = VdotN * dif1 - nx * dif2 - ny * dif3 - nz * dif4;
+  T B = qir * dif1 - uar2 * dif2 - uar3 * dif3 - uar4 * dif4 + dif5;
+  // flur4 (left==false) or flur5 (left==true); the other is zero.
+  T fl, rs;
+  if (!left) {
+    fl = tmax0(VdotN + cr) * ((-cr) * A + gam1 * (-cr) * invtbeta2 * B);
+    rs = cr * fl;  // r * flur4
+  } else {
+    fl = -tmin0(VdotN - cr) * (cr * A + (-gam1 * cr * invtbeta2 * B));
+    rs = (-cr) * fl;  // s * flur5
+  }
+  phi[0] = f0 - 0.5 * fl * cr2;
+  phi[1] = f1 - (nx * rs + uar2 * fl) * 0.5 * cr2;
+  phi[2] = f2 - (ny * rs + uar3 * fl) * 0.5 * cr2;
+  phi[3] = f3 - (nz * rs + uar4 * fl) * 0.5 * cr2;
+  phi[4] = f4 - (VdotN * rs + uar5 * fl) * 0.5 * cr2;
+  phi[0] = phi[0] * rnorm;
+  phi[1] = phi[1] * rnorm;
+  phi[2] = phi[2] * rnorm;
+  phi[3] = phi[3] * rnorm;
+  phi[4] = phi[4] * rnorm;
+}
+
+// boundflux5.f:1-111 (type 0, sig = 0): Steger-Warming far-field flux
+// A+(V) U(V) + A-(V) Ub with V primitive and Ub conservative.
+template <class T>
+AEROF_HD void sw_flux(const Gas& g, T vnx, T vny, T vnz, const T* ua, const double* ub, T* flux) {
+  const double gam = g.gam, gam1 = g.gam1;
+  T cap = dsqrt(vnx * vnx + vny * vny + vnz * vnz);
+  T capd1 = vnx / cap, capd2 = vny / cap, capd3 = vnz / cap;
+  T ro = ua[0];
+  T usro = 1.0 / ro;
+  T u = ua[1], v = ua[2], w = ua[3];
+  T vit = u * u + v * v + w * w;
+  T pm = ua[4];
+  T rhoE = pm / gam1 + 0.5 * ro * vit;
+  T c2 = gam * pm * usro;
+  T c = dsqrt(c2);
+  T usc = 1.0 / c;
+  T cc = 0.5 * vit + c2 / gam1;
+  T unx = capd1 * u + capd2 * v + capd3 * w;
+  T l1 = cap * unx, l4 = cap * (unx + c), l5 = cap * (unx - c);
+  T vp1 = tmax0(l1), vp4 = tmax0(l4), vp5 = tmax0(l5);
+  T vpp = vp4 + vp5;
+  T vpm = vp4 - vp5;
+  T fgp0 = (gam1 * ro * vp1 + 0.5 * ro * vpp) / gam;
+  T fgp1 = fgp0 * u + 0.5 * pm * usc * capd1 * vpm;
+  T fgp2 = fgp0 * v + 0.5 * pm * usc * capd2 * vpm;
+  T fgp3 = fgp0 * w + 0.5 * pm * usc * capd3 * vpm;
+  T fgp4 = 0.5 * ((gam1 / gam) * ro * vit * (vp1 - 0.5 * vpp) + rhoE * vpp + ro * unx * c * vpm / gam);
+  vp1 = tmin0(l1); vp4 = tmin0(l4); vp5 = tmin0(l5);
+  vpp = vp1 - 0.5 * (vp4 + vp5);
+  vpm = 0.5 * (vp5 - vp4);
+  T xn1 = gam1 * usc * (-(0.5 * vit * ub[0]) + u * ub[1] + v * ub[2] + w * ub[3] - ub[4]);
+  T xn2 = unx * ub[0] - capd1 * ub[1] - capd2 * ub[2] - capd3 * ub[3];
+  T ff = usc * (vpp * xn1 + vpm * xn2);
+  T gg = vpm * xn1 + vpp * xn2;
+  flux[0] = fgp0 + (vp1 * ub[0] + ff);
+  flux[1] = fgp1 + (vp1 * ub[1] + u * ff + capd1 * gg);
+  flux[2] = fgp2 + (vp1 * ub[2] + v * ff + capd2 * gg);
+  flux[3] = fgp3 + (vp1 * ub[3] + w * ff + capd3 * gg);
+  flux[4] = fgp4 + (vp1 * ub[4] + cc * ff + unx * gg);
+}
+
+// FluxFcnSGWallEuler3D::compute (FluxFcnDescSG.C:779-789), ndot = 0
+template <class T>
+AEROF_HD void wall_flux(T nx, T ny, T nz, const T* V, T* flux) {
+  flux[0] = T(0.0);
+  flux[1] = V[4] * nx;
+  flux[2] = V[4] * ny;
+  flux[3] = V[4] * nz;
+  flux[4] = T(0.0);
+}
+
+template <class T>
+AEROF_HD void face_flux(const Gas& g, int code, T nx, T ny, T nz, const T* V, const double* Ub, T* f) {
+  if (code == AEROF_BC_SLIP_WALL_MOVING) wall_flux(nx, ny, nz, V, f);
+  else sw_flux(g, nx, ny, nz, V, Ub, f);
+}
+
+// ------------------------------------------------------------ Jacobians
+// VarFcnBase::postMultiplyBydVdU (VarFcnBase.h:372-400) with
+// VarFcnSGEuler::computedVdU (VarFcnSGEuler.h:588-603): res = mat * dV/dU.
+AEROF_HD void post_dVdU(const Gas& g, const double* V, const double* mat, double* res) {
+  double invrho = 1.0 / V[0];
+  double d5 = -invrho * V[1], d10 = -invrho * V[2], d15 = -invrho * V[3];
+  double d20 = g.gam1 * 0.5 * (V[1] * V[1] + V[2] * V[2] + V[3] * V[3]);
+  double d21 = -g.gam1 * V[1], d22 = -g.gam1 * V[2], d23 = -g.gam1 * V[3], d24 = g.gam1;
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+    const double* m = mat + 5 * r;
+    double* o = res + 5 * r;
+    o[0] = m[0] + m[1] * d5 + m[2] * d10 + m[3] * d15 + m[4] * d20;
+    o[1] = m[1] * invrho + m[4] * d21;
+    o[2] = m[2] * invrho + m[4] * d22;
+    o[3] = m[3] * invrho + m[4] * d23;
+    o[4] = m[4] * d24;
+  }
+}
+
+// roejac6.f:1-316 (type 0, prec 0 -> beta 1, dissipation coefficient 1):
+// approximate Jacobian of the Roe flux w.r.t. the conservative state Ug,
+// sw = +1 adds the dissipation matrix, sw = -1 subtracts it.
+AEROF_HD void roe_jac(const Gas& g, double n0, double n1, double n2, const double* Ug, const double* Ud,
+                      double sw, double* jac) {
+  const double gam = g.gam, gam1 = g.gam1;
+  double rnorm = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+  double invnorm = 1.0 / rnorm;
+  double n[3] = {n0 * invnorm, n1 * invnorm, n2 * invnorm};
+  double VdotN = Ug[1] * n[0] + Ug[2] * n[1] + Ug[3] * n[2];
+  double qir = 0.5 * (Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3]);
+  double enth = (gam * Ug[4] + gam1 * Ug[0] * qir) / (gam1 * Ug[0]);
+  double H[25];
+  H[0] = 0.0; H[1] = n[0]; H[2] = n[1]; H[3] = n[2]; H[4] = 0.0;
+  H[5] = gam1 * n[0] * qir - Ug[1] * VdotN;
+  H[6] = (1.0 - gam1) * n[0] * Ug[1] + VdotN;
+  H[7] = -gam1 * n[0] * Ug[2] + Ug[1] * n[1];
+  H[8] = -gam1 * n[0] * Ug[3] + Ug[1] * n[2];
+  H[9] = gam1 * n[0];
+  H[10] = gam1 * n[1] * qir - Ug[2] * VdotN;
+  H[11] = -gam1 * n[1] * Ug[1] + Ug[2] * n[0];
+  H[12] = (1.0 - gam1) * n[1] * Ug[2] + VdotN;
+  H[13] = -gam1 * n[1] * Ug[3] + Ug[2] * n[2];
+  H[14] = gam1 * n[1];
+  H[15] = gam1 * n[2] * qir - Ug[3] * VdotN;
+  H[16] = -gam1 * n[2] * Ug[1] + Ug[3] * n[0];
+  H[17] = -gam1 * n[2] * Ug[2] + Ug[3] * n[1];
+  H[18] = (1.0 - gam1) * n[2] * Ug[3] + VdotN;
+  H[19] = gam1 * n[2];
+  H[20] = (gam1 * qir - enth) * VdotN;
+  H[21] = enth * n[0] - gam1 * Ug[1] * VdotN;
+  H[22] = enth * n[1] - gam1 * Ug[2] * VdotN;
+  H[23] = enth * n[2] - gam1 * Ug[3] * VdotN;
+  H[24] = (1.0 + gam1) * VdotN;
+  // Roe average
+  double squsr1 = sqrt(Ug[0]), squsr2 = sqrt(Ud[0]);
+  double ener1 = Ug[4] / gam1 + 0.5 * Ug[0] * (Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3]);
+  double ener2 = Ud[4] / gam1 + 0.5 * Ud[0] * (Ud[1] * Ud[1] + Ud[2] * Ud[2] + Ud[3] * Ud[3]);
+  double usro = 1.0 / (squsr1 + squsr2);
+  double uar2 = (squsr1 * Ug[1] + squsr2 * Ud[1]) * usro;
+  double uar3 = (squsr1 * Ug[2] + squsr2 * Ud[2]) * usro;
+  double uar4 = (squsr1 * Ug[3] + squsr2 * Ud[3]) * usro;
+  double uar5 = ((ener1 + Ug[4]) / squsr1 + (ener2 + Ud[4]) / squsr2) * usro;
+  enth = uar5;
+  VdotN = n[0] * uar2 + n[1] * uar3 + n[2] * uar4;
+  qir = 0.5 * (uar2 * uar2 + uar3 * uar3 + uar4 * uar4);
+  double cr = sqrt(gam1 * (uar5 - qir));
+  double crsq = cr * cr;
+  double gc = gam1 / crsq;
+  double usc2 = 0.5 / crsq;
+  // beta = 1: vp4,vp5 = VdotN +- cr written as the reference's general form
+  double sq = sqrt(0.0 * VdotN * (0.0 * VdotN) + 4.0 * crsq);
+  double vp4 = 0.5 * (2.0 * VdotN + sq);
+  double vp5 = 0.5 * (2.0 * VdotN - sq);
+  double rRT = vp4 - VdotN;
+  double sRT = vp5 - VdotN;
+  double tRT = 0.5 * (vp5 - vp4);
+  double vp1 = fabs(VdotN);
+  vp4 = fabs(vp4);
+  vp5 = fabs(vp5);
+  double tmw[25];
+  tmw[0] = n[0] + n[1] * uar4 - uar3 * n[2] - gc * n[0] * qir;
+  tmw[1] = gc * n[0] * uar2;
+  tmw[2] = gc * n[0] * uar3 + n[2];
+  tmw[3] = gc * n[0] * uar4 - n[1];
+  tmw[4] = -gc * n[0];
+  tmw[5] = n[1] + n[2] * uar2 - uar4 * n[0] - gc * n[1] * qir;
+  tmw[6] = gc * n[1] * uar2 - n[2];
+  tmw[7] = gc * n[1] * uar3;
+  tmw[8] = gc * n[1] * uar4 + n[0];
+  tmw[9] = -gc * n[1];
+  tmw[10] = n[2] + n[0] * uar3 - uar2 * n[1] - gc * n[2] * qir;
+  tmw[11] = gc * n[2] * uar2 + n[1];
+  tmw[12] = gc * n[2] * uar3 - n[0];
+  tmw[13] = gc * n[2] * uar4;
+  tmw[14] = -gc * n[2];
+  tmw[15] = gam1 * qir * sRT / tRT + VdotN * crsq / tRT;
+  tmw[16] = -gam1 * uar2 * sRT / tRT - crsq * n[0] / tRT;
+  tmw[17] = -gam1 * uar3 * sRT / tRT - crsq * n[1] / tRT;
+  tmw[18] = -gam1 * uar4 * sRT / tRT - crsq * n[2] / tRT;
+  tmw[19] = gam1 * sRT / tRT;
+  tmw[20] = -gam1 * qir * rRT / tRT - VdotN * crsq / tRT;
+  tmw[21] = gam1 * uar2 * rRT / tRT + crsq * n[0] / tRT;
+  tmw[22] = gam1 * uar3 * rRT / tRT + crsq * n[1] / tRT;
+  tmw[23] = gam1 * uar4 * rRT / tRT + crsq * n[2] / tRT;
+  tmw[24] = -gam1 * rRT / tRT;
+  const double half_rn = 0.5 * rnorm;
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    double t0 = tmw[j], t1 = tmw[5 + j], t2 = tmw[10 + j], t3 = tmw[15 + j], t4 = tmw[20 + j];
+    double d0 = vp1 * (n[0] * t0 + n[1] * t1 + n[2] * t2) + vp4 * usc2 * t3 + vp5 * usc2 * t4;
+    double d1 = vp1 * (n[0] * uar2 * t0 + (n[1] * uar2 - n[2]) * t1 + (n[2] * uar2 + n[1]) * t2) +
+                vp4 * (usc2 * (uar2 + rRT * n[0])) * t3 + vp5 * (usc2 * (uar2 + sRT * n[0])) * t4;
+    double d2 = vp1 * (n[1] * uar3 * t1 + (n[0] * uar3 + n[2]) * t0 + (n[2] * uar3 - n[0]) * t2) +
+                vp4 * (usc2 * (uar3 + rRT * n[1])) * t3 + vp5 * (usc2 * (uar3 + sRT * n[1])) * t4;
+    double d3 = vp1 * (n[2] * uar4 * t2 + (n[0] * uar4 - n[1]) * t0 + (n[1] * uar4 + n[0]) * t1) +
+                vp4 * (usc2 * (uar4 + rRT * n[2])) * t3 + vp5 * (usc2 * (uar4 + sRT * n[2])) * t4;
+    double d4 = vp1 * ((n[0] * qir + (n[2] * uar3 - n[1] * uar4)) * t0 +
+                       (n[1] * qir + (n[0] * uar4 - n[2] * uar2)) * t1 +
+                       (n[2] * qir + (n[1] * uar2 - n[0] * uar3)) * t2) +
+                vp4 * (usc2 * (enth + VdotN * rRT)) * t3 + vp5 * (usc2 * (enth + VdotN * sRT)) * t4;
+    jac[j] = (H[j] + sw * d0) * half_rn;
+    jac[5 + j] = (H[5 + j] + sw * d1) * half_rn;
+    jac[10 + j] = (H[10 + j] + sw * d2) * half_rn;
+    jac[15 + j] = (H[15 + j] + sw * d3) * half_rn;
+    jac[20 + j] = (H[20 + j] + sw * d4) * half_rn;
+  }
+}
+
+// Face blocks: FluxFcnFD<5>::computeJacobian (FluxFcnBase.h:112-159) for the
+// Steger-Warming faces, FluxFcnSGWallEuler3D::computeJacobian
+// (FluxFcnDescSG.C:838-886) for slip walls, both post-multiplied by dV/dU.
+AEROF_HD void face_jac(const Gas& g, int code, double nx, double ny, double nz, const double* V,
+                       const double* Ub, double* jac) {
+  double dfdV[25];
+  if (code == AEROF_BC_SLIP_WALL_MOVING) {
+#pragma unroll
+    for (int k = 0; k < 25; ++k) dfdV[k] = 0.0;
+    dfdV[9] = nx; dfdV[14] = ny; dfdV[19] = nz; dfdV[24] = 0.0;
+  } else {
+    const double eps0 = 1.e-6;
+    double f0[5], fe[5], Ve[5];
+    sw_flux(g, nx, ny, nz, V, Ub, f0);
+    for (int k = 0; k < 5; ++k) {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) Ve[q] = V[q];
+      double eps = (fabs(V[k]) < 1.e-10) ? eps0 : eps0 * V[k];
+      double inveps = 1.0 / eps;
+      Ve[k] += eps;
+      sw_flux(g, nx, ny, nz, Ve, Ub, fe);
+#pragma unroll
+      for (int j = 0; j < 5; ++j) dfdV[5 * j + k] = (fe[j] - f0[j]) * inveps;
+    }
+  }
+  post_dVdU(g, V, dfdV, jac);
+}
+
+// ------------------------------------------------------------ 5x5 inverse
+// invertDenseMatrix (DenseMatrixOps.h:1006-1185): LINPACK dgefa (partial
+// pivoting) + dgedi, here on a row-major block viewed as column-major
+// transpose.  Returns 0 or the 1-based step with a zero pivot.
+template <class S>
+AEROF_HD int invert5(S* a) {
+  // t(r,c) = a[c*5 + r] : the transpose in column-major is a itself read
+  // row-major, so operate on a directly with A(r,c) = a[r + 5*c]^T ...
+  S t[25];
+#pragma unroll
+  for (int r = 0; r < 5; ++r)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) t[r + 5 * c] = a[5 * r + c];
+#define AEROF_A(r, c) t[(r) + 5 * (c)]
+  int ipvt[5];
+  for (int k = 0; k < 4; ++k) {
+    int l = k;
+    S mx = AEROF_A(k, k) < S(0) ? -AEROF_A(k, k) : AEROF_A(k, k);
+    for (int r = k + 1; r < 5; ++r) {
+      S v = AEROF_A(r, k) < S(0) ? -AEROF_A(r, k) : AEROF_A(r, k);
+      if (v > mx) { mx = v; l = r; }
+    }
+    ipvt[k] = l;
+    if (AEROF_A(l, k) == S(0)) return k + 1;
+    if (l != k) { S tmp = AEROF_A(l, k); AEROF_A(l, k) = AEROF_A(k, k); AEROF_A(k, k) = tmp; }
+    S tt = S(-1.0) / AEROF_A(k, k);
+    for (int r = k + 1; r < 5; ++r) AEROF_A(r, k) *= tt;
+    for (int j = k + 1; j < 5; ++j) {
+      S u = AEROF_A(l, j);
+      if (l != k) { AEROF_A(l, j) = AEROF_A(k, j); AEROF_A(k, j) = u; }
+      for (int r = k + 1; r < 5; ++r) AEROF_A(r, j) += u * AEROF_A(r, k);
+    }
+  }
+  ipvt[4] = 4;
+  if (AEROF_A(4, 4) == S(0)) return 5;
+  for (int k = 0; k < 5; ++k) {
+    AEROF_A(k, k) = S(1.0) / AEROF_A(k, k);
+    S tt = -AEROF_A(k, k);
+    for (int r = 0; r < k; ++r) AEROF_A(r, k) *= tt;
+    for (int j = k + 1; j < 5; ++j) {
+      S u = AEROF_A(k, j);
+      AEROF_A(k, j) = S(0);
+      for (int r = 0; r <= k; ++r) AEROF_A(r, j) += u * AEROF_A(r, k);
+    }
+  }
+  S work[5];
+  for (int kb = 1; kb <= 4; ++kb) {
+    int k = 4 - kb;
+    for (int i = k + 1; i < 5; ++i) { work[i] = AEROF_A(i, k); AEROF_A(i, k) = S(0); }
+    for (int j = k + 1; j < 5; ++j) {
+      S u = work[j];
+      for (int r = 0; r < 5; ++r) AEROF_A(r, k) += u * AEROF_A(r, j);
+    }
+    int l = ipvt[k];
+    if (l != k)
+      for (int r = 0; r < 5; ++r) { S tmp = AEROF_A(r, k); AEROF_A(r, k) = AEROF_A(r, l); AEROF_A(r, l) = tmp; }
+  }
+#undef AEROF_A
+#pragma unroll
+  for (int r = 0; r < 5; ++r)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) a[5 * r + c] = t[r + 5 * c];
+  return 0;
+}
+
+}  // namespace aerof

@@ -175,12 +175,17 @@ def smooth_state(X: np.ndarray, mach: float, amp: float = 0.02, gamma: float = 1
     p = 1.0 / (gamma * mach * mach)
     s = np.sin(np.pi * X[:, 0]) * np.sin(np.pi * X[:, 1]) * np.sin(np.pi * X[:, 2])
     c = np.cos(2.0 * np.pi * X[:, 0]) * np.sin(np.pi * X[:, 2])
+    # a generic linear ramp per component keeps every edge difference away
+    # from exactly zero (van Albada switches branch at a*b == 0)
+    d = np.array([[1.0, 0.37, 0.61], [0.43, 1.0, 0.29], [0.71, 0.23, 1.0], [0.19, 0.83, 0.47],
+                  [0.57, 0.31, 0.89]])
+    lin = X @ d.T
     V = np.empty((X.shape[0], 5))
-    V[:, 0] = 1.0 + amp * s
-    V[:, 1] = 1.0 + amp * c
-    V[:, 2] = 0.5 * amp * s
-    V[:, 3] = -0.5 * amp * c
-    V[:, 4] = p * (1.0 + amp * (s + 0.5 * c))
+    V[:, 0] = 1.0 + amp * (s + 0.3 * lin[:, 0])
+    V[:, 1] = 1.0 + amp * (c + 0.3 * lin[:, 1])
+    V[:, 2] = amp * (0.5 * s + 0.3 * lin[:, 2])
+    V[:, 3] = amp * (-0.5 * c + 0.3 * lin[:, 3])
+    V[:, 4] = p * (1.0 + amp * (s + 0.5 * c + 0.3 * lin[:, 4]))
     return prim_to_cons(V, gamma)
 
 

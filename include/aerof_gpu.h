@@ -1,0 +1,190 @@
+/*
+ * aerof_gpu.h -- C ABI of the B200 (sm_100a) implementation of AERO-F's
+ * implicit edge-based finite-volume hot path.
+ *
+ * AERO-F has no plugin or FFI layer: the hot path is reached through C++
+ * template classes (SpaceOperator<dim>, MatVecProd<dim,neq>,
+ * KspPrec<dim,Scalar>, KspSolver<...>).  Each entry point below replaces one
+ * member of that call surface; the citation names the reference function
+ * (file:line in the AERO-F tree) whose contract it keeps.  A C++ shim that
+ * subclasses those classes and forwards here is shown in INTEGRATION.md.
+ *
+ * Conventions
+ *  - Every function returns int: 0 = AEROF_OK, > 0 = number of unphysical
+ *    states detected (a warning, the result is still written), < 0 = error.
+ *  - State and residual vectors use the reference's layout: double[N][5]
+ *    (AoS, one node after the other, node numbering of the mesh passed to
+ *    aerof_gpu_set_mesh), conservative (rho, rho u, rho v, rho w, E) for U.
+ *  - Any array argument may be host memory (pageable or pinned) or device
+ *    memory of the context's GPU; the library detects which and stages host
+ *    arrays through its own device buffers on the context's stream.  All
+ *    calls are synchronous with respect to the host on return.
+ *  - One context is used by one host thread at a time.
+ *  - No call spins on device flags; device-side failures are counted into a
+ *    device error word and returned as status codes.
+ */
+#ifndef AEROF_GPU_H
+#define AEROF_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AEROF_OK 0
+#define AEROF_EINVAL -1    /* bad argument */
+#define AEROF_ENOMEM -2    /* device allocation failed */
+#define AEROF_ECUDA -3     /* CUDA runtime error */
+#define AEROF_ETIMEDOUT -4 /* bounded wait expired */
+#define AEROF_ESINGULAR -5 /* zero pivot in a 5x5 diagonal block */
+#define AEROF_ESTATE -6    /* call order violated (e.g. no mesh set) */
+
+/* Boundary codes (BcDef.h:5-28) understood by the face kernels. */
+#define AEROF_BC_SLIP_WALL_MOVING -2
+#define AEROF_BC_INLET_MOVING -4
+#define AEROF_BC_OUTLET_MOVING -5
+
+/* Reconstruction (SchemeData, IoDataCore.C:2415-2435). */
+#define AEROF_REC_CONSTANT 1  /* first order: RecFcnConstant                     */
+#define AEROF_REC_VANALBADA 2 /* LSQ gradients + van Albada, RecFcnVanAlbada<5>   */
+#define AEROF_REC_LINEAR 3    /* LSQ gradients + unlimited MUSCL, RecFcnLinear<5> */
+
+/* Precision of the assembled H1 Jacobian and block-Jacobi preconditioner. */
+#define AEROF_PREC_FP64 64
+#define AEROF_PREC_FP32 32 /* FP32 blocks, FP64 vectors and accumulation */
+
+typedef struct aerof_gpu_ctx aerof_gpu_ctx;
+
+/* The few IoData fields the path uses (IoDataCore.C:2415-2435, 3160). */
+typedef struct aerof_gpu_config {
+  double gamma;      /* ratio of specific heats (GasModelData), 1.4        */
+  double beta;       /* MUSCL beta (SchemeData::beta), 1/3                 */
+  int reconstruction;/* AEROF_REC_*                                          */
+  int failsafe;      /* 1: tag nodes with non-positive reconstructed rho/p,
+                        zero their gradients and recompute (Domain.C:876-918) */
+  int device;        /* CUDA device ordinal                                  */
+  int reserved[5];
+} aerof_gpu_config;
+
+/* Steady pseudo-transient Newton-Krylov parameters (TsData/CFLData/KspData,
+ * IoDataCore.C:2896-2911, 3067-3089; IoData.C:9-20). */
+typedef struct aerof_newton_params {
+  double cfl0, cfl_min, cfl_max, ser; /* RESIDUAL CFL law (TsParameters.C:211-217) */
+  double ksp_eps;                     /* GMRES relative tolerance (1e-2)            */
+  double tol;                         /* stop at ||R(Q)||/||R(Q0)|| <= tol          */
+  int ksp_krylov;                     /* GMRES restart length (30)                  */
+  int ksp_maxits;                     /* GMRES max iterations (30)                  */
+  int max_steps;                      /* pseudo-time steps                          */
+  int precision;                      /* AEROF_PREC_FP32 or AEROF_PREC_FP64         */
+  int reserved[4];
+} aerof_newton_params;
+
+typedef struct aerof_newton_result {
+  int steps;            /* pseudo-time steps taken                   */
+  int linear_its;       /* total GMRES iterations                    */
+  double rel_residual;  /* final ||R||/||R0||                        */
+  double seconds;       /* device time of the solve (CUDA events)    */
+} aerof_newton_result;
+
+/* ---- context ---------------------------------------------------------- */
+int aerof_gpu_create(const aerof_gpu_config* cfg, aerof_gpu_ctx** out);
+int aerof_gpu_destroy(aerof_gpu_ctx* ctx);
+/* Run subsequent work on this cudaStream_t (NULL: the context's own stream). */
+int aerof_gpu_set_stream(aerof_gpu_ctx* ctx, void* stream);
+/* Last error message of this context (NUL-terminated, truncated to len). */
+int aerof_gpu_last_error(aerof_gpu_ctx* ctx, char* buf, int len);
+
+/* ---- mesh -------------------------------------------------------------
+ * Replaces GeoSource/SubDomain construction plus the static-mesh geometry
+ * DistGeoState::compute (DistGeoState.C:542-600): edges are the unique node
+ * pairs of the tets numbered lexicographically (EdgeSet::createPointers,
+ * EdgeCore.C:92-117); edge normals ElemTet::computeEdgeNormalsGCL1
+ * (ElemTetCore.C:281-330), face normals FaceTria::computeNormalGCL1
+ * (FaceTriaCore.C:65-82), control volumes (ElemTetCore.C:102-112) and the
+ * least-squares factors (SubDomainCore.C:1334-1381, 1755-1777).
+ * X[N][3], tets[T][4] (positively oriented), faces[F][3] (outward by
+ * 0.5*((x2-x0)^(x1-x0))), codes[F] (AEROF_BC_*), Ub[5] the conservative
+ * free-stream state of every far-field face (DistBcData.C:652-730).       */
+int aerof_gpu_set_mesh(aerof_gpu_ctx* ctx, int N, int T, int F, const double* X, const int* tets,
+                       const int* faces, const int* codes, const double* Ub);
+int aerof_gpu_mesh_sizes(aerof_gpu_ctx* ctx, int* N, int* E, int* F);
+/* Edge list [E][2] (i<j), lexicographic: EdgeSet::getPtr (Edge.h). */
+int aerof_gpu_get_edges(aerof_gpu_ctx* ctx, int* edges);
+/* Geometry in reference numbering: edge normals [E][3], face normals [F][3],
+ * control volumes [N], least-squares factors [N][6] (r11 r12 r13 r22 r23 r33). */
+int aerof_gpu_get_geometry(aerof_gpu_ctx* ctx, double* edge_normal, double* face_normal,
+                           double* ctrl_vol, double* lsq_R);
+
+/* ---- residual ---------------------------------------------------------
+ * SpaceOperator<5>::computeResidual(X, ctrlVol, U, R, timeState)
+ * (SpaceOperator.h:171-173, SpaceOperator.C:524-634): R = (sum of Roe edge
+ * fluxes + boundary fluxes)/ctrlVol for the configured reconstruction.
+ * Returns the number of non-positive reconstructed densities/pressures
+ * (EdgeCore.C:137-168) -- 0 on a healthy state.                          */
+int aerof_gpu_residual(aerof_gpu_ctx* ctx, const double* U, double* R);
+/* DistNodalGrad::compute, least squares (DistNodalGrad.C:790-806,
+ * SubDomain.C:297-374) of primitive V[N][5]; ddx/ddy/ddz [N][5].        */
+int aerof_gpu_gradients(aerof_gpu_ctx* ctx, const double* V, double* ddx, double* ddy, double* ddz);
+/* DistTimeState::computeTimeStep with local time stepping
+ * (DistTimeState.C:746-801, Domain.C:30-100, Edge.C:87-143, Face.C:242-289):
+ * dt[N] = cfl*vol/(-sum of wave-speed terms).                             */
+int aerof_gpu_timestep(aerof_gpu_ctx* ctx, const double* U, double cfl, double* dt);
+/* ExplicitTsDesc::computeRKSecondOrder (ExplicitTsDesc.C:98-117), nsteps
+ * local-time-step Heun steps at fixed cfl, U[N][5] updated in place.     */
+int aerof_gpu_rk2(aerof_gpu_ctx* ctx, double* U, double cfl, int nsteps);
+
+/* ---- implicit operator ------------------------------------------------
+ * MatVecProdH1<5,MatScalar,5>::evaluate (MatVecProd.C:1074-1160) =
+ * SpaceOperator::computeJacobian (SpaceOperator.C:2088-2150) +
+ * TimeState::addToJacobian (TimeState.C:731-756): first-order approximate
+ * Roe Jacobian (roejac6.f), FD far-field and analytic wall face blocks,
+ * diag/ctrlVol, + I/dt.  dt may be NULL (no time term).  precision selects
+ * FP32 or FP64 block storage.                                              */
+int aerof_gpu_jacobian(aerof_gpu_ctx* ctx, const double* U, const double* dt, int precision);
+/* The assembled H1 operator in MvpMat layout a[N+2E][25] (MvpMatrix.h:10-80),
+ * reference numbering, as double.                                          */
+int aerof_gpu_get_jacobian(aerof_gpu_ctx* ctx, double* A);
+/* MatVecProdH1::apply / applyTranspose (MatVecProd.C:1165-1208,
+ * SubDomain.C:3916-3995): y = A p or A^T p, p,y [N][5].                   */
+int aerof_gpu_matvec(aerof_gpu_ctx* ctx, const double* p, double* y, int transpose);
+/* JacobiPrec::getData + setup (KspPrec.C:75-82,115-124; DiagMatrix.C:44-80):
+ * invert the 5x5 diagonal blocks (LINPACK dgefa/dgedi) in the Jacobian's
+ * precision.  Returns AEROF_ESINGULAR on a zero pivot.                    */
+int aerof_gpu_prec_setup(aerof_gpu_ctx* ctx);
+/* JacobiPrec::apply / applyT (KspPrec.C:86-111): y = D^-1 x or D^-T x.    */
+int aerof_gpu_prec_apply(aerof_gpu_ctx* ctx, const double* x, double* y, int transpose);
+/* GmresSolver::solve / solveT (KspSolver.C:351-492, 752-915): right-
+ * preconditioned GMRES(krylov) with modified Gram-Schmidt in FP64, x0 = 0.
+ * its receives the iteration count (== maxits means saturation, the
+ * reference's SATURATED_LS), res the final estimated residual norm.       */
+int aerof_gpu_gmres(aerof_gpu_ctx* ctx, const double* b, double* x, int krylov, int maxits,
+                    double eps, int transpose, int* its, double* res);
+/* TsSolver::resolve + NewtonSolver::solve (maxIts=1) for a steady problem
+ * (TsSolver.h:231-380, NewtonSolver.h:70-231, ImplicitCoupledTsDesc.C:
+ * 85-300): U[N][5] updated in place; history (optional, max_steps+1
+ * entries) receives ||R||/||R0|| per step.                                 */
+int aerof_gpu_newton(aerof_gpu_ctx* ctx, double* U, const aerof_newton_params* p,
+                     aerof_newton_result* out, double* history);
+
+/* ---- sensitivities ----------------------------------------------------
+ * Exact linearisation of the configured residual (the operator
+ * MatVecProdH2 applies, MatVecProd.C:1462-1704; derivative routines
+ * Edge.C:1451-1573, RecFcn.h:451-526, g_roeflux*.f, g_boundflux5.f):     */
+/* Jv = dR/dU . v                                                            */
+int aerof_gpu_jvp(aerof_gpu_ctx* ctx, const double* U, const double* v, double* Jv);
+/* JTw = (dR/dU)^T . w  (MatVecProdH2::applyTranspose, MatVecProd.C:1685-1704) */
+int aerof_gpu_vjp(aerof_gpu_ctx* ctx, const double* U, const double* w, double* JTw);
+/* dR = dR/dX . Xdot, Xdot[N][3] (SpaceOperator::computeDerivativeOfResidual
+ * through normals, ctrlVol, LSQ factors and dx; fsoAnalytical,
+ * FluidShapeOptimizationHandler.C:1368-1430)                               */
+int aerof_gpu_dRdX(aerof_gpu_ctx* ctx, const double* U, const double* Xdot, double* dR);
+/* gX = (dR/dX)^T . lambda, gX[N][3] (fsoApply_dFdXtranspose,
+ * FluidShapeOptimizationHandler.C:1434-1448)                               */
+int aerof_gpu_dRdX_T(aerof_gpu_ctx* ctx, const double* U, const double* lambda, double* gX);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AEROF_GPU_H */

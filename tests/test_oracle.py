@@ -1,0 +1,194 @@
+"""CPU tests of the oracle: pinned against golden vectors produced by the
+reference's own header code, plus the self-consistency properties that pin
+the Fortran-derived kernels (no Fortran compiler is available)."""
+import os
+
+import numpy as np
+import pytest
+
+from aerof_dev_b200 import workloads as W
+from conftest import rel_l2
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "reference_pointwise.npz")
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(GOLD)
+
+
+def test_vanalbada_and_linear_bitwise(oracle_mod, gold):
+    ri = gold["rec_in"]
+    for r, va, li in zip(ri, gold["vanalbada_out"], gold["linear_out"]):
+        a, b = oracle_mod.vanalbada(r[0], r[1:6], r[6:11], r[11:16], r[16:21])
+        assert np.array_equal(np.concatenate([a, b]), va)
+        a, b = oracle_mod.linear_rec(r[0], r[1:6], r[6:11], r[11:16], r[16:21])
+        assert np.array_equal(np.concatenate([a, b]), li)
+
+
+def test_cons2prim_bitwise(oracle_mod, gold):
+    for u, v in zip(gold["cons_in"], gold["cons2prim_out"]):
+        assert np.array_equal(oracle_mod.cons2prim(1.4, u), v)
+
+
+def test_post_dVdU_bitwise(oracle_mod, gold):
+    for r, o in zip(gold["dVdU_in"], gold["dVdU_out"]):
+        assert np.array_equal(oracle_mod.post_dVdU(1.4, r[:5], r[5:]).reshape(-1), o)
+
+
+def test_invert5_bitwise(oracle_mod, gold):
+    for a, o in zip(gold["invert_in"], gold["invert_out"]):
+        b, info = oracle_mod.invert5(a.reshape(5, 5))
+        assert info == int(o[0])
+        assert np.array_equal(b.reshape(-1), o[1:])
+
+
+def test_positivity_check_matches_reference(gold):
+    # VarFcnSGEuler::checkReconstructedValues: rho <= 0 or p <= 0 is an error
+    for v, bad in zip(gold["check_in"], gold["check_out"][:, 0]):
+        assert bool(v[0] <= 0.0 or v[4] <= 0.0) == bool(bad)
+
+
+@pytest.fixture(scope="module")
+def small(oracle_mod):
+    m = W.make_lattice_mesh(7, jitter=0.2, codes="channel")
+    return m, oracle_mod.Oracle(m)
+
+
+def test_mesh_sizes_and_edges(small):
+    m, o = small
+    s = W.lattice_sizes(7)
+    assert o.E == s["E"]
+    e = o.edges()
+    assert np.all(e[:, 0] < e[:, 1])
+    key = e[:, 0].astype(np.int64) * o.N + e[:, 1]
+    assert np.all(np.diff(key) > 0)  # lexicographic, unique
+
+
+def test_dual_cell_closure(small):
+    m, o = small
+    g = o.geometry()
+    e = o.edges()
+    s = np.zeros((o.N, 3))
+    np.add.at(s, e[:, 0], g["edge_normal"])
+    np.add.at(s, e[:, 1], -g["edge_normal"])
+    for l in range(3):
+        np.add.at(s, m["faces"][:, l], g["face_normal"] / 3)
+    assert np.abs(s).max() < 1e-15
+    assert abs(g["ctrl_vol"].sum() - 1.0) < 1e-13
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+def test_freestream_preserved(small, order):
+    m, o = small
+    Ub = W.freestream(0.8)
+    U = np.tile(Ub, (o.N, 1))
+    R, ierr = o.residual(U, Ub, order)
+    assert ierr == 0
+    assert np.abs(R).max() < 1e-11
+
+
+def test_lsq_gradient_exact_for_linear_field(small):
+    m, o = small
+    X = m["X"]
+    a = np.array([[1.0 + k, 2.0 - k, 0.5 * k] for k in range(5)])
+    V = 1.0 + X @ a.T
+    gx, gy, gz = o.gradients(V)
+    assert np.abs(gx - a[:, 0]).max() < 1e-12
+    assert np.abs(gy - a[:, 1]).max() < 1e-12
+    assert np.abs(gz - a[:, 2]).max() < 1e-12
+
+
+def test_roe_flux_consistency_and_antisymmetry(oracle_mod):
+    rng = np.random.default_rng(3)
+    for _ in range(50):
+        Vi = np.array([1 + 0.1 * rng.random(), *(0.5 * rng.standard_normal(3)), 1 + rng.random()])
+        Vj = Vi * (1 + 0.05 * rng.standard_normal(5))
+        n = rng.standard_normal(3)
+        f = oracle_mod.roeflux7(1.4, n, Vi, Vj)
+        g = oracle_mod.roeflux7(1.4, -n, Vj, Vi)
+        assert np.abs(f + g).max() <= 1e-14 * np.abs(f).max()
+        rho, u, v, w, p = Vi
+        un = u * n[0] + v * n[1] + w * n[2]
+        E = p / 0.4 + 0.5 * rho * (u * u + v * v + w * w)
+        phys = np.array([rho * un, rho * u * un + p * n[0], rho * v * un + p * n[1], rho * w * un + p * n[2],
+                         (E + p) * un])
+        assert np.abs(oracle_mod.roeflux7(1.4, n, Vi, Vi) - phys).max() < 1e-13 * (1 + np.abs(phys).max())
+
+
+def test_steger_warming_freestream_consistency(oracle_mod):
+    # A+(V)U(V) + A-(V)U(V) = F(V): the far-field flux of the free stream
+    # against itself is the physical flux
+    Ub = W.freestream(0.8)
+    V = oracle_mod.cons2prim(1.4, Ub)
+    n = np.array([0.2, -0.7, 0.4])
+    f = oracle_mod.boundflux5(1.4, n, V, Ub)
+    rho, u, v, w, p = V
+    un = u * n[0] + v * n[1] + w * n[2]
+    phys = np.array([rho * un, rho * u * un + p * n[0], rho * v * un + p * n[1], rho * w * un + p * n[2],
+                     (Ub[4] + p) * un])
+    assert np.abs(f - phys).max() < 1e-13
+
+
+def test_roejac6_matches_fd_on_equal_states(oracle_mod):
+    # with Ug == Ud the two approximate Jacobians are 1/2 (A +- |A|) |n|, so
+    # dF/dU_L + dF/dU_R is the exact physical-flux Jacobian A |n|
+    Vi = np.array([1.1, 0.6, 0.1, -0.2, 1.3])
+    n = np.array([0.3, 0.5, -0.2])
+    jl, jr = oracle_mod.roejac6(1.4, n, Vi, Vi)
+    U = W.prim_to_cons(Vi[None])[0]
+
+    def phys(U):
+        V = oracle_mod.cons2prim(1.4, U)
+        rho, u, v, w, p = V
+        un = u * n[0] + v * n[1] + w * n[2]
+        return np.array([rho * un, rho * u * un + p * n[0], rho * v * un + p * n[1], rho * w * un + p * n[2],
+                         (U[4] + p) * un])
+
+    J = np.empty((5, 5))
+    for k in range(5):
+        h = 1e-6 * max(1.0, abs(U[k]))
+        e = np.zeros(5); e[k] = h
+        J[:, k] = (phys(U + e) - phys(U - e)) / (2 * h)
+    assert np.abs((jl + jr) - J).max() < 1e-7
+
+
+def test_threaded_baseline_matches_sequential(small):
+    m, o = small
+    Ub = W.freestream(0.8)
+    U = W.perturbed_state(o.N, 0.8)
+    R, _ = o.residual(U, Ub, 2)
+    Rt = o.residual_threaded(U, Ub, 2, nthreads=3)
+    assert rel_l2(Rt, R) < 1e-13
+
+
+def test_jvp_matches_central_fd(small):
+    m, o = small
+    Ub = W.freestream(0.8)
+    U = W.smooth_state(m["X"], 0.8)
+    rng = np.random.default_rng(5)
+    v = rng.standard_normal(U.shape) * np.array([1e-2, 1e-2, 1e-2, 1e-2, 1e-2])
+    Jv = o.jvp(U, Ub, v, order=2)
+    h = 1e-6
+    fd = (o.residual(U + h * v, Ub, 2)[0] - o.residual(U - h * v, Ub, 2)[0]) / (2 * h)
+    assert rel_l2(Jv, fd) < 1e-6
+
+
+def test_dRdX_matches_central_fd(small):
+    m, o = small
+    Ub = W.freestream(0.8)
+    U = W.smooth_state(m["X"], 0.8)
+    Xdot = W.shape_modes(m["X"], 1)[0]
+    dR, R = o.dRdX(U, Ub, Xdot, order=2)
+    h = 1e-6
+    fd = (o.residual_at(m["X"] + h * Xdot, U, Ub, 2) - o.residual_at(m["X"] - h * Xdot, U, Ub, 2)) / (2 * h)
+    assert rel_l2(dR, fd) < 1e-6
+
+
+def test_newton_converges_small(oracle_mod):
+    m = W.make_lattice_mesh(5, jitter=0.1, codes="channel")
+    o = oracle_mod.Oracle(m)
+    Ub = W.freestream(0.8)
+    U = W.perturbed_state(o.N, 0.8, amp=0.02)
+    U2, hist, lits = o.newton(U, Ub, order=2, tol=1e-8, max_steps=300)
+    assert hist[-1] <= 1e-8

@@ -44,7 +44,10 @@ EXPORTS = [
     "aerof_gpu_jacobian", "aerof_gpu_get_jacobian", "aerof_gpu_matvec", "aerof_gpu_prec_setup",
     "aerof_gpu_prec_apply", "aerof_gpu_gmres", "aerof_gpu_newton",
     "aerof_gpu_jvp", "aerof_gpu_vjp", "aerof_gpu_dRdX", "aerof_gpu_dRdX_T",
+    "aerof_gpu_residual_async", "aerof_gpu_status", "aerof_gpu_profile", "aerof_gpu_timers",
+    "aerof_gpu_update_coordinates", "aerof_gpu_linearized_solve",
 ]
+TIMER_NAMES = ["nodal_grad", "fv_term", "time_step", "fv_jac", "prec_setup", "ksp_matvec", "ksp_other", "other"]
 
 
 class AerofError(RuntimeError):
@@ -107,6 +110,13 @@ def library(path: str | None = None):
             "aerof_gpu_vjp": [vp, dp, dp, dp],
             "aerof_gpu_dRdX": [vp, dp, dp, dp],
             "aerof_gpu_dRdX_T": [vp, dp, dp, dp],
+            "aerof_gpu_residual_async": [vp, dp, dp],
+            "aerof_gpu_status": [vp],
+            "aerof_gpu_profile": [vp, C.c_int],
+            "aerof_gpu_timers": [vp, dp, dp, C.c_int],
+            "aerof_gpu_update_coordinates": [vp, dp],
+            "aerof_gpu_linearized_solve": [vp, dp, dp, dp, C.c_int, C.c_int, C.c_double, C.c_int,
+                                           C.POINTER(C.c_int), C.POINTER(C.c_double)],
         }
         for name, args in sig.items():
             if hasattr(L, name):
@@ -206,10 +216,27 @@ class Context:
         self.N, self.E, self.F = n.value, e.value, ff.value
         return self
 
+    def status(self) -> int:
+        """Wait for the stream; unphysical count of async calls since last status."""
+        return self._check(self.L.aerof_gpu_status(self.h))
+
+    def profile(self, enable: bool = True):
+        self._check(self.L.aerof_gpu_profile(self.h, int(enable)))
+
+    def timers(self) -> dict:
+        """Per-category device milliseconds and interval counts (resets them)."""
+        ms = np.zeros(8); cnt = np.zeros(8, dtype=np.int64)
+        self._check(self.L.aerof_gpu_timers(self.h, C.c_void_p(ms.ctypes.data), C.c_void_p(cnt.ctypes.data), 8))
+        return {n: (float(m), int(c)) for n, m, c in zip(TIMER_NAMES, ms, cnt)}
+
     @classmethod
     def from_mesh(cls, mesh: dict, Ub, **kw) -> "Context":
         ctx = cls(**kw)
         return ctx.set_mesh(mesh["X"], mesh["tets"], mesh["faces"], mesh["codes"], Ub)
+
+    def update_coordinates(self, X):
+        x = _Arg(X, np.float64, (self.N, 3))
+        self._check(self.L.aerof_gpu_update_coordinates(self.h, x.ptr))
 
     def edges(self) -> np.ndarray:
         e = np.empty((self.E, 2), dtype=np.int32)
@@ -238,6 +265,14 @@ class SpaceOperator:
         r = _Arg(R, np.float64, (ctx.N, 5), writable=True)
         bad = ctx._check(ctx.L.aerof_gpu_residual(ctx.h, u.ptr, r.ptr))
         return r.obj, bad
+
+    def computeResidualAsync(self, U, R):
+        """Enqueue R = residual(U) for device tensors without waiting."""
+        ctx = self.ctx
+        u = _Arg(U, np.float64, (ctx.N, 5))
+        r = _Arg(R, np.float64, (ctx.N, 5), writable=True)
+        ctx._check(ctx.L.aerof_gpu_residual_async(ctx.h, u.ptr, r.ptr))
+        return r.obj
 
     def computeGradients(self, V):
         ctx = self.ctx
@@ -392,3 +427,15 @@ class Sensitivity:
 
     def dRdX_T(self, U, lam):
         return self._call(self.ctx.L.aerof_gpu_dRdX_T, U, lam, 5, 3)
+
+    def solve(self, U, b, transpose=False, krylov=30, maxits=300, eps=1e-10):
+        """Solve J x = b (direct) or J^T x = b (adjoint) with the exact operator."""
+        ctx = self.ctx
+        u = _Arg(U, np.float64, (ctx.N, 5))
+        bb = _Arg(b, np.float64, (ctx.N, 5))
+        x = _like(b, (ctx.N, 5))
+        xx = _Arg(x, np.float64, writable=True)
+        its, res = C.c_int(), C.c_double()
+        ctx._check(ctx.L.aerof_gpu_linearized_solve(ctx.h, u.ptr, bb.ptr, xx.ptr, krylov, maxits, eps,
+                                                    int(transpose), C.byref(its), C.byref(res)))
+        return xx.obj, its.value, res.value

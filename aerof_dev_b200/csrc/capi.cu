@@ -36,9 +36,66 @@ void out_finish(aerof_gpu_ctx* c, double* user, const double* dev, size_t count)
   AEROF_CUDA(cudaStreamSynchronize(c->stream));
 }
 
+int timer_begin(aerof_gpu_ctx* c, int cat) {
+  Timers& t = c->timers;
+  if (!t.on) return -1;
+  cudaEvent_t e[2];
+  for (int k = 0; k < 2; ++k) {
+    if (!t.pool.empty()) { e[k] = t.pool.back(); t.pool.pop_back(); }
+    else AEROF_CUDA(cudaEventCreate(&e[k]));
+  }
+  AEROF_CUDA(cudaEventRecord(e[0], c->stream));
+  t.recs.push_back({cat, e[0], e[1]});
+  return (int)t.recs.size() - 1;
+}
+
+void timer_end(aerof_gpu_ctx* c, int h) {
+  if (h < 0) return;
+  cudaEventRecord(c->timers.recs[h].b, c->stream);
+}
+
+static void timers_collect(aerof_gpu_ctx* c) {
+  Timers& t = c->timers;
+  if (t.recs.empty()) return;
+  AEROF_CUDA(cudaStreamSynchronize(c->stream));
+  for (auto& r : t.recs) {
+    float ms = 0.f;
+    AEROF_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+    t.ms[r.cat] += ms;
+    t.cnt[r.cat] += 1;
+    t.pool.push_back(r.a);
+    t.pool.push_back(r.b);
+  }
+  t.recs.clear();
+}
+
 }  // namespace aerof
 
 using namespace aerof;
+
+extern "C" int aerof_gpu_profile(aerof_gpu_ctx* c, int enable) {
+  return guard(c, [&]() -> int {
+    if (!enable) timers_collect(c);
+    c->timers.on = enable != 0;
+    return AEROF_OK;
+  });
+}
+
+extern "C" int aerof_gpu_timers(aerof_gpu_ctx* c, double* ms, long long* count, int n) {
+  return guard(c, [&]() -> int {
+    if (n < 0) return AEROF_EINVAL;
+    timers_collect(c);
+    for (int k = 0; k < AEROF_T_COUNT; ++k) {
+      if (k < n) {
+        if (ms) ms[k] = c->timers.ms[k];
+        if (count) count[k] = c->timers.cnt[k];
+      }
+      c->timers.ms[k] = 0.0;
+      c->timers.cnt[k] = 0;
+    }
+    return AEROF_OK;
+  });
+}
 
 extern "C" int aerof_gpu_create(const aerof_gpu_config* cfg, aerof_gpu_ctx** out) {
   if (!cfg || !out) return AEROF_EINVAL;

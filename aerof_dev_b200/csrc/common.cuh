@@ -140,6 +140,7 @@ struct Implicit {
 // Dual-number work arrays of the forward-mode linearisation.
 struct DualWork {
   DBuf<Dual> XD, PD, GD, WD, RD, volD, enD, fnD, fluxD;
+  bool geom_static = false;  // dual geometry holds the primal with zero tangents
 };
 
 // Reverse-mode work arrays.
@@ -148,6 +149,23 @@ struct AdjWork {
   DBuf<double> gG;         // [N][16] gradient cotangents
   DBuf<double> gV;         // [N][5] direct state cotangents
   DBuf<double> lam;        // [N][5] w / vol
+  DBuf<double> gd;         // [2E][3] least-squares offset cotangents
+  DBuf<double> gvol;       // [N] control-volume cotangents
+  DBuf<double> gfn;        // [F][3] face-normal cotangents
+};
+
+// CUDA-event timers per category (AEROF_T_*), recorded without host sync.
+struct Timers {
+  bool on = false;
+  struct Rec { int cat; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  double ms[AEROF_T_COUNT] = {0};
+  long long cnt[AEROF_T_COUNT] = {0};
+  ~Timers() {
+    for (auto& r : recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (auto e : pool) cudaEventDestroy(e);
+  }
 };
 
 }  // namespace aerof
@@ -163,6 +181,7 @@ struct aerof_gpu_ctx {
   aerof::Implicit imp;
   aerof::DualWork dual;
   aerof::AdjWork adj;
+  aerof::Timers timers;
   std::string last_error;
 };
 
@@ -199,12 +218,30 @@ inline int grid_for(size_t n, int block) { return (int)((n + block - 1) / block)
 // numbers, same kernels and order as the primal set-up
 void geometry_dual(aerof_gpu_ctx* c, const Dual* XD, Dual* volD, Dual* enD, Dual* fnD, Dual* RD);
 
-// implemented in residual.cu (used by implicit.cu and adjoint.cu)
-int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR);
+// Timer scope: records start/stop events around the enclosed launches.
+int timer_begin(aerof_gpu_ctx* c, int cat);
+void timer_end(aerof_gpu_ctx* c, int handle);
+struct TimerScope {
+  aerof_gpu_ctx* c;
+  int h;
+  TimerScope(aerof_gpu_ctx* cc, int cat) : c(cc), h(timer_begin(cc, cat)) {}
+  ~TimerScope() { timer_end(c, h); }
+};
+
+// implemented in residual.cu (used by implicit.cu and adjoint.cu).  With
+// sync == false the unphysical count is left on the device (counters[2]).
+int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync = true);
 void prim_dev(aerof_gpu_ctx* c, const double* dU);
 void gradients_dev(aerof_gpu_ctx* c);
 void timestep_dev(aerof_gpu_ctx* c, const double* dU, double cfl, double* ddt);
 double norm2_dev(aerof_gpu_ctx* c, const double* x, size_t n);
 double dot_dev(aerof_gpu_ctx* c, const double* x, const double* y, size_t n);
+
+// implemented in adjoint.cu
+int residual_forward(aerof_gpu_ctx* c, const double* dU, const double* dv, const double* dXdot, double* ddR,
+                     bool sync = true);
+void vjp_dev(aerof_gpu_ctx* c, const double* dU, const double* dw, double* dout);
+// implemented in mesh.cu: recompute the geometry for new coordinates
+void compute_geometry(aerof_gpu_ctx* c);
 
 }  // namespace aerof

@@ -280,6 +280,7 @@ void jacobian_dev(aerof_gpu_ctx* c, const double* dU, const double* ddt, int pre
   DeviceMesh& m = c->mesh;
   Implicit& J = c->imp;
   const Gas g = make_gas(c->cfg.gamma);
+  TimerScope tj(c, AEROF_T_FV_JAC);
   prim_dev(c, dU);
   J.diagscr.ensure(25 * 2 * (size_t)m.E);
   const int ge = grid_for(m.E, kIB), gn = grid_for(m.N, kIB);
@@ -310,6 +311,7 @@ void jacobian_dev(aerof_gpu_ctx* c, const double* dU, const double* ddt, int pre
 
 void matvec_dev(aerof_gpu_ctx* c, const double* p, double* y, int trans) {
   DeviceMesh& m = c->mesh;
+  TimerScope tm(c, AEROF_T_KSP_MATVEC);
   Implicit& J = c->imp;
   const int gn = grid_for(m.N, kIB);
   if (J.precision == AEROF_PREC_FP32) {
@@ -325,6 +327,7 @@ void matvec_dev(aerof_gpu_ctx* c, const double* p, double* y, int trans) {
 int prec_setup_dev(aerof_gpu_ctx* c) {
   DeviceMesh& m = c->mesh;
   Implicit& J = c->imp;
+  TimerScope tp(c, AEROF_T_PREC_SETUP);
   c->s.counters.ensure(8);
   int* bad = c->s.counters.p + 4;
   AEROF_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
@@ -346,6 +349,7 @@ int prec_setup_dev(aerof_gpu_ctx* c) {
 
 void prec_apply_dev(aerof_gpu_ctx* c, const double* x, double* z, int trans) {
   DeviceMesh& m = c->mesh;
+  TimerScope tp(c, AEROF_T_KSP_OTHER);
   Implicit& J = c->imp;
   const int gn = grid_for(m.N, kIB);
   if (J.precision == AEROF_PREC_FP32) k_bj_apply<float><<<gn, kIB, 0, c->stream>>>(m.N, J.dinv32.p, x, z, trans);
@@ -357,7 +361,16 @@ void prec_apply_dev(aerof_gpu_ctx* c, const double* x, double* z, int trans) {
 // preconditioning), MGS, Givens rotations and back substitution on the host
 // (KspSolver.C:917-982).  x = 0 on entry.  Returns iterations.
 int gmres_dev(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int maxits, double eps, int trans,
-              double* final_res) {
+              double* final_res, const double* exactU) {
+  // operator: the assembled H1 matrix, or (exactU != null) the exact
+  // linearisation at state exactU applied matrix-free (MatVecProdH2,
+  // MatVecProd.C:1462-1704): J p by forward mode, J^T p by reverse mode.
+  auto op = [&](const double* p, double* y) {
+    if (!exactU) { matvec_dev(c, p, y, trans); return; }
+    TimerScope t(c, AEROF_T_KSP_MATVEC);
+    if (trans) vjp_dev(c, exactU, p, y);
+    else residual_forward(c, exactU, p, nullptr, y, false);
+  };
   DeviceMesh& m = c->mesh;
   Implicit& J = c->imp;
   const size_t n = 5 * (size_t)m.N;
@@ -387,7 +400,7 @@ int gmres_dev(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int maxi
   double target = 0.0, l2res = 0.0;
   do {
     // r = b - A x ; beta = ||r||  (x == 0 on the first cycle)
-    matvec_dev(c, x, w, trans);
+    op(x, w);
     k_sub<<<gv, kIB, 0, s>>>(n, b, w, r);
     AEROF_LAUNCH_CHECK();
     double beta = norm2_dev(c, r, n);
@@ -400,7 +413,7 @@ int gmres_dev(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int maxi
     int j;
     for (j = 0; j < numVec; ++j) {
       prec_apply_dev(c, Vb + (size_t)j * n, r, trans);
-      matvec_dev(c, r, w, trans);
+      op(r, w);
       // h_ij = w . V_i ; w -= h_ij V_i   (i = 0..j), then ||w||
       for (int i = 0; i <= j; ++i)
         dot_to(i ? hd + (i - 1) : nullptr, i ? Vb + (size_t)(i - 1) * n : nullptr, Vb + (size_t)i * n, hd + i);
@@ -554,7 +567,7 @@ extern "C" int aerof_gpu_gmres(aerof_gpu_ctx* c, const double* b, double* x, int
     const double* db = in_dev(c, b, n, c->s.Ustage);
     double* dx = out_dev(c, x, n, c->s.Rstage);
     double r = 0.0;
-    int it = gmres_dev(c, db, dx, krylov, maxits, eps, transpose, &r);
+    int it = gmres_dev(c, db, dx, krylov, maxits, eps, transpose, &r, nullptr);
     out_finish(c, x, dx, n);
     if (its) *its = it;
     if (res) *res = r;
@@ -613,7 +626,7 @@ extern "C" int aerof_gpu_newton(aerof_gpu_ctx* c, double* U, const aerof_newton_
       }
       k_scale<<<gv, kIB, 0, s>>>(n, -1.0, R, rhs);
       AEROF_LAUNCH_CHECK();
-      lits += gmres_dev(c, rhs, dQ, p->ksp_krylov, p->ksp_maxits, p->ksp_eps, 0, nullptr);
+      lits += gmres_dev(c, rhs, dQ, p->ksp_krylov, p->ksp_maxits, p->ksp_eps, 0, nullptr, nullptr);
       k_add<<<gv, kIB, 0, s>>>(n, dQ, dU);
       AEROF_LAUNCH_CHECK();
     }
@@ -632,5 +645,37 @@ extern "C" int aerof_gpu_newton(aerof_gpu_ctx* c, double* U, const aerof_newton_
       out->seconds = ms * 1e-3;
     }
     return bad;
+  });
+}
+
+// Linearised steady systems with the exact operator (sensitivity analysis,
+// FluidShapeOptimizationHandler.C:1557-1624): transpose = 0 solves
+// J x = b (direct), transpose = 1 solves J^T x = b (adjoint, GmresSolver::
+// solveT, KspSolver.C:752-915).  Preconditioner: block-Jacobi of the
+// first-order H1 operator at U without time term, in FP64.
+extern "C" int aerof_gpu_linearized_solve(aerof_gpu_ctx* c, const double* U, const double* b, double* x, int krylov,
+                                          int maxits, double eps, int transpose, int* its, double* res) {
+  return guard(c, [&]() -> int {
+    need_mesh_or_throw(c);
+    if (!U || !b || !x || krylov < 1 || maxits < 1 || !(eps >= 0.0)) return AEROF_EINVAL;
+    const size_t n = 5 * (size_t)c->mesh.N;
+    c->imp.t.ensure(n);
+    const double* dU0 = in_dev(c, U, n, c->s.Ustage);
+    if (dU0 != c->imp.t.p)
+      AEROF_CUDA(cudaMemcpyAsync(c->imp.t.p, dU0, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    const double* dU = c->imp.t.p;
+    const double* db = in_dev(c, b, n, c->s.Vstage);
+    double* dx = out_dev(c, x, n, c->s.Rstage);
+    jacobian_dev(c, dU, nullptr, AEROF_PREC_FP64);
+    if (int nb = prec_setup_dev(c)) {
+      c->last_error = std::to_string(nb) + " singular diagonal block(s)";
+      return AEROF_ESINGULAR;
+    }
+    double r = 0.0;
+    int it = gmres_dev(c, db, dx, krylov, maxits, eps, transpose, &r, dU);
+    out_finish(c, x, dx, n);
+    if (its) *its = it;
+    if (res) *res = r;
+    return AEROF_OK;
   });
 }

@@ -8,74 +8,13 @@
 
 #include "common.cuh"
 #include "physics.cuh"
+#include "geometry.cuh"
 
 namespace aerof {
 
 constexpr int kMBlock = 256;
 
-// ElemTet tables (ElemTetCore.C:19-21)
-__constant__ int c_edgeEnd[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
-__constant__ int c_edgeFace[6][2] = {{0, 1}, {2, 0}, {1, 2}, {0, 3}, {3, 1}, {2, 3}};
 static const int h_edgeEnd[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
-
-template <class T>
-struct Vec3 {
-  T x, y, z;
-};
-template <class T> __device__ __forceinline__ Vec3<T> v3(T a, T b, T c) { return Vec3<T>{a, b, c}; }
-template <class T> __device__ __forceinline__ Vec3<T> operator+(Vec3<T> a, Vec3<T> b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
-template <class T> __device__ __forceinline__ Vec3<T> operator-(Vec3<T> a, Vec3<T> b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
-template <class T> __device__ __forceinline__ Vec3<T> scale(double c, Vec3<T> a) { return v3(c * a.x, c * a.y, c * a.z); }
-// Vec3D::operator^ (Vector3D.h:266-274)
-template <class T> __device__ __forceinline__ Vec3<T> cross(Vec3<T> a, Vec3<T> b) {
-  return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
-}
-template <class T> __device__ __forceinline__ Vec3<T> node_x(const T* X, int n) {
-  return v3(X[3 * (size_t)n], X[3 * (size_t)n + 1], X[3 * (size_t)n + 2]);
-}
-
-// Signed tet volume (ElemTetCore.C:24-39): sixth * v3 . (v1 ^ v2)
-template <class T>
-__device__ __forceinline__ T tet_volume(const T* X, const int* nd) {
-  Vec3<T> x0 = node_x(X, nd[0]);
-  Vec3<T> v1 = node_x(X, nd[1]) - x0, v2 = node_x(X, nd[2]) - x0, v3_ = node_x(X, nd[3]) - x0;
-  Vec3<T> c = cross(v1, v2);
-  const double sixth = 1.0 / 6.0;
-  return sixth * (v3_.x * c.x + v3_.y * c.y + v3_.z * c.z);
-}
-
-// Dual-cell facet normal of local edge l of a tet, oriented from the lower
-// to the higher global node id: ElemTet::computeEdgeNormalsGCL1
-// (ElemTetCore.C:281-330) with Xn = Xnp1.
-template <class T>
-__device__ __forceinline__ Vec3<T> tet_edge_normal(const T* X, const int* nd, int l) {
-  const double third = 1.0 / 3.0;
-  Vec3<T> x[4] = {node_x(X, nd[0]), node_x(X, nd[1]), node_x(X, nd[2]), node_x(X, nd[3])};
-  Vec3<T> f[4];
-  f[0] = scale(third, x[0] + x[1] + x[2]);
-  f[1] = scale(third, x[0] + x[1] + x[3]);
-  f[2] = scale(third, x[0] + x[2] + x[3]);
-  f[3] = scale(third, x[1] + x[2] + x[3]);
-  Vec3<T> g = scale(0.25, x[0] + x[1] + x[2] + x[3]);
-  Vec3<T> xg0 = f[c_edgeFace[l][0]] - g;
-  Vec3<T> xg1 = f[c_edgeFace[l][1]] - g;
-  Vec3<T> c = cross(xg1, xg0);
-  Vec3<T> n = scale(0.5, c + c) + scale(0.25, c + c);
-  if (nd[c_edgeEnd[l][0]] < nd[c_edgeEnd[l][1]]) return n;
-  return v3(-n.x, -n.y, -n.z);
-}
-
-// FaceTria::computeNormalGCL1 (FaceTriaCore.C:65-82) with Xn = Xnp1:
-// twelfth * ((3 x02) ^ x01 + (3 x02) ^ x01), outward for the face ordering.
-template <class T>
-__device__ __forceinline__ Vec3<T> face_normal(const T* X, const int* nd) {
-  const double twelfth = 1.0 / 12.0;
-  Vec3<T> x0 = node_x(X, nd[0]);
-  Vec3<T> x01 = node_x(X, nd[1]) - x0, x02 = node_x(X, nd[2]) - x0;
-  Vec3<T> a = scale(2.0, x02) + x02;
-  Vec3<T> s = cross(a, x01) + cross(a, x01);
-  return scale(twelfth, s);
-}
 
 template <class T>
 __global__ void k_ctrl_vol(int N, const T* __restrict__ X, const int* __restrict__ tets,
@@ -327,8 +266,27 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
     m.nt_tet.upload(h.nt_tet.data(), h.nt_tet.size(), s);
     m.h_edges.swap(h.edges);
     compute_geometry(c);
+    c->dual.geom_static = false;
     AEROF_CUDA(cudaStreamSynchronize(s));
     c->has_mesh = true;
+    return AEROF_OK;
+  });
+}
+
+extern "C" int aerof_gpu_update_coordinates(aerof_gpu_ctx* c, const double* X) {
+  return guard(c, [&]() -> int {
+    if (!c->has_mesh) return AEROF_ESTATE;
+    if (!X) return AEROF_EINVAL;
+    DeviceMesh& m = c->mesh;
+    if (is_device_ptr(X))
+      AEROF_CUDA(cudaMemcpyAsync(m.X.p, X, 3 * (size_t)m.N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    else
+      AEROF_CUDA(cudaMemcpyAsync(m.X.p, X, 3 * (size_t)m.N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    compute_geometry(c);
+    c->dual.geom_static = false;
+    c->imp.precision = 0;
+    c->imp.prec_ready = false;
+    AEROF_CUDA(cudaStreamSynchronize(c->stream));
     return AEROF_OK;
   });
 }

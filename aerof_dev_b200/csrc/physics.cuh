@@ -467,3 +467,241 @@ AEROF_HD int invert5(S* a) {
 }
 
 }  // namespace aerof
+
+namespace aerof {
+
+// ------------------------------------------------------------ adjoints
+// Reverse mode of roe_flux: recomputes the forward values, then
+// accumulates the cotangents gUg += (dphi/dUg)^T gphi, gUd += (dphi/dUd)^T
+// gphi and gn += (dphi/dn)^T gphi.  The dissipation term is differentiated
+// in its algebraically simplified form fl = lam (s cr A + gam1 B), s = -1
+// (right side upwind) or +1 (left side), which is the same function as the
+// reference's cr2byt / invtbeta2 form.
+__device__ __forceinline__ void roe_flux_adj(const Gas& g, double n0, double n1, double n2, const double* Ug,
+                                             const double* Ud, const double* gphi, double* gUg, double* gUd,
+                                             double* gn) {
+  const double gam = g.gam, gam1 = g.gam1, invgam1 = g.invgam1;
+  // ---- forward
+  const double s2 = n0 * n0 + n1 * n1 + n2 * n2;
+  const double rnorm = sqrt(s2);
+  const double invnorm = 1.0 / rnorm;
+  const double nx = n0 * invnorm, ny = n1 * invnorm, nz = n2 * invnorm;
+  const double vitg2 = Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3];
+  const double vitd2 = Ud[1] * Ud[1] + Ud[2] * Ud[2] + Ud[3] * Ud[3];
+  const double sq1 = sqrt(Ug[0]), sq2 = sqrt(Ud[0]);
+  const double ener1 = Ug[4] * invgam1 + 0.5 * Ug[0] * vitg2;
+  const double ener2 = Ud[4] * invgam1 + 0.5 * Ud[0] * vitd2;
+  const double usro = 1.0 / (sq1 + sq2);
+  const double m2 = sq1 * Ug[1] + sq2 * Ud[1], m3 = sq1 * Ug[2] + sq2 * Ud[2], m4 = sq1 * Ug[3] + sq2 * Ud[3];
+  const double uar2 = m2 * usro, uar3 = m3 * usro, uar4 = m4 * usro;
+  const double a1 = (ener1 + Ug[4]) / sq1, a2 = (ener2 + Ud[4]) / sq2;
+  const double uar5 = (a1 + a2) * usro;
+  const double VdotN = nx * uar2 + ny * uar3 + nz * uar4;
+  const bool left = VdotN > 0.0;
+  const double* Us = left ? Ug : Ud;
+  const double vits2 = left ? vitg2 : vitd2;
+  const double vn = Us[1] * nx + Us[2] * ny + Us[3] * nz;
+  const double H = (gam * Us[4] + 0.5 * gam1 * Us[0] * vits2) / (gam1 * Us[0]);
+  const double f0 = Us[0] * vn;
+  const double f1 = f0 * Us[1] + Us[4] * nx, f2 = f0 * Us[2] + Us[4] * ny, f3 = f0 * Us[3] + Us[4] * nz;
+  const double f4 = f0 * H;
+  const double qir = 0.5 * (uar2 * uar2 + uar3 * uar3 + uar4 * uar4);
+  const double c2 = gam1 * (uar5 - qir);
+  const double cr = sqrt(c2);
+  const double cr2 = 1.0 / c2;
+  const double dif1 = Ud[0] - Ug[0];
+  const double dif2 = Ud[0] * Ud[1] - Ug[0] * Ug[1];
+  const double dif3 = Ud[0] * Ud[2] - Ug[0] * Ug[2];
+  const double dif4 = Ud[0] * Ud[3] - Ug[0] * Ug[3];
+  const double dif5 = ener2 - ener1;
+  const double A = VdotN * dif1 - nx * dif2 - ny * dif3 - nz * dif4;
+  const double B = qir * dif1 - uar2 * dif2 - uar3 * dif3 - uar4 * dif4 + dif5;
+  const double sg = left ? 1.0 : -1.0;
+  const double lamarg = cr - sg * VdotN;
+  const bool lam_on = lamarg > 0.0;
+  const double lam = lam_on ? lamarg : 0.0;
+  const double K = sg * cr * A + gam1 * B;
+  const double fl = lam * K;
+  const double rs = -sg * cr * fl;
+  const double t1 = nx * rs + uar2 * fl, t2 = ny * rs + uar3 * fl, t3 = nz * rs + uar4 * fl;
+  const double t4 = VdotN * rs + uar5 * fl;
+  const double q0 = f0 - 0.5 * fl * cr2;
+  const double q1 = f1 - t1 * 0.5 * cr2, q2 = f2 - t2 * 0.5 * cr2, q3 = f3 - t3 * 0.5 * cr2;
+  const double q4 = f4 - t4 * 0.5 * cr2;
+  // ---- reverse
+  double g_rnorm = gphi[0] * q0 + gphi[1] * q1 + gphi[2] * q2 + gphi[3] * q3 + gphi[4] * q4;
+  const double gq0 = gphi[0] * rnorm, gq1 = gphi[1] * rnorm, gq2 = gphi[2] * rnorm, gq3 = gphi[3] * rnorm,
+               gq4 = gphi[4] * rnorm;
+  double g_f0 = gq0, g_f1 = gq1, g_f2 = gq2, g_f3 = gq3, g_f4 = gq4;
+  double g_fl = -0.5 * cr2 * gq0;
+  double g_cr2 = -0.5 * (fl * gq0 + t1 * gq1 + t2 * gq2 + t3 * gq3 + t4 * gq4);
+  const double gt1 = -0.5 * cr2 * gq1, gt2 = -0.5 * cr2 * gq2, gt3 = -0.5 * cr2 * gq3, gt4 = -0.5 * cr2 * gq4;
+  double g_nx = rs * gt1, g_ny = rs * gt2, g_nz = rs * gt3;
+  double g_rs = nx * gt1 + ny * gt2 + nz * gt3 + VdotN * gt4;
+  double g_uar2 = fl * gt1, g_uar3 = fl * gt2, g_uar4 = fl * gt3, g_uar5 = fl * gt4;
+  double g_VdotN = rs * gt4;
+  g_fl += uar2 * gt1 + uar3 * gt2 + uar4 * gt3 + uar5 * gt4;
+  // rs = -sg cr fl
+  double g_cr = -sg * fl * g_rs;
+  g_fl += -sg * cr * g_rs;
+  // fl = lam K
+  const double g_lam = K * g_fl;
+  const double g_K = lam * g_fl;
+  g_cr += sg * A * g_K;
+  const double g_A = sg * cr * g_K;
+  const double g_B = gam1 * g_K;
+  if (lam_on) {
+    g_cr += g_lam;
+    g_VdotN += -sg * g_lam;
+  }
+  // A, B
+  g_VdotN += dif1 * g_A;
+  double g_dif1 = VdotN * g_A + qir * g_B;
+  double g_dif2 = -nx * g_A - uar2 * g_B;
+  double g_dif3 = -ny * g_A - uar3 * g_B;
+  double g_dif4 = -nz * g_A - uar4 * g_B;
+  const double g_dif5 = g_B;
+  g_nx -= dif2 * g_A; g_ny -= dif3 * g_A; g_nz -= dif4 * g_A;
+  double g_qir = dif1 * g_B;
+  g_uar2 -= dif2 * g_B; g_uar3 -= dif3 * g_B; g_uar4 -= dif4 * g_B;
+  // cr2 = 1/c2 ; cr = sqrt(c2) ; c2 = gam1 (uar5 - qir)
+  double g_c2 = -cr2 * cr2 * g_cr2 + 0.5 / cr * g_cr;
+  g_uar5 += gam1 * g_c2;
+  g_qir -= gam1 * g_c2;
+  g_uar2 += uar2 * g_qir; g_uar3 += uar3 * g_qir; g_uar4 += uar4 * g_qir;
+  // differences
+  double gL[5] = {0, 0, 0, 0, 0}, gR[5] = {0, 0, 0, 0, 0};
+  gR[0] += g_dif1 + Ud[1] * g_dif2 + Ud[2] * g_dif3 + Ud[3] * g_dif4;
+  gL[0] -= g_dif1 + Ug[1] * g_dif2 + Ug[2] * g_dif3 + Ug[3] * g_dif4;
+  gR[1] += Ud[0] * g_dif2; gR[2] += Ud[0] * g_dif3; gR[3] += Ud[0] * g_dif4;
+  gL[1] -= Ug[0] * g_dif2; gL[2] -= Ug[0] * g_dif3; gL[3] -= Ug[0] * g_dif4;
+  double g_ener2 = g_dif5, g_ener1 = -g_dif5;
+  // centred flux of the upwind side
+  {
+    double gs[5] = {0, 0, 0, 0, 0};
+    const double g_f0t = g_f0 + Us[1] * g_f1 + Us[2] * g_f2 + Us[3] * g_f3 + H * g_f4;
+    gs[1] += f0 * g_f1; gs[2] += f0 * g_f2; gs[3] += f0 * g_f3;
+    gs[4] += nx * g_f1 + ny * g_f2 + nz * g_f3;
+    g_nx += Us[4] * g_f1; g_ny += Us[4] * g_f2; g_nz += Us[4] * g_f3;
+    const double g_H = f0 * g_f4;
+    gs[0] += vn * g_f0t;
+    const double g_vn = Us[0] * g_f0t;
+    gs[4] += gam / (gam1 * Us[0]) * g_H;
+    gs[0] += -gam * Us[4] / (gam1 * Us[0] * Us[0]) * g_H;
+    const double g_vits2 = 0.5 * g_H;
+    gs[1] += 2.0 * Us[1] * g_vits2 + nx * g_vn;
+    gs[2] += 2.0 * Us[2] * g_vits2 + ny * g_vn;
+    gs[3] += 2.0 * Us[3] * g_vits2 + nz * g_vn;
+    g_nx += Us[1] * g_vn; g_ny += Us[2] * g_vn; g_nz += Us[3] * g_vn;
+    double* gt = left ? gL : gR;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) gt[k] += gs[k];
+  }
+  // VdotN = n . uar
+  g_nx += uar2 * g_VdotN; g_ny += uar3 * g_VdotN; g_nz += uar4 * g_VdotN;
+  g_uar2 += nx * g_VdotN; g_uar3 += ny * g_VdotN; g_uar4 += nz * g_VdotN;
+  // Roe averages
+  const double g_S = usro * g_uar5;
+  double g_usro = (a1 + a2) * g_uar5;
+  g_ener1 += g_S / sq1; gL[4] += g_S / sq1;
+  g_ener2 += g_S / sq2; gR[4] += g_S / sq2;
+  double g_sq1 = -a1 / sq1 * g_S, g_sq2 = -a2 / sq2 * g_S;
+  const double gm2 = usro * g_uar2, gm3 = usro * g_uar3, gm4 = usro * g_uar4;
+  g_usro += m2 * g_uar2 + m3 * g_uar3 + m4 * g_uar4;
+  g_sq1 += Ug[1] * gm2 + Ug[2] * gm3 + Ug[3] * gm4;
+  g_sq2 += Ud[1] * gm2 + Ud[2] * gm3 + Ud[3] * gm4;
+  gL[1] += sq1 * gm2; gL[2] += sq1 * gm3; gL[3] += sq1 * gm4;
+  gR[1] += sq2 * gm2; gR[2] += sq2 * gm3; gR[3] += sq2 * gm4;
+  g_sq1 += -usro * usro * g_usro;
+  g_sq2 += -usro * usro * g_usro;
+  // energies
+  gL[4] += invgam1 * g_ener1; gL[0] += 0.5 * vitg2 * g_ener1;
+  const double g_vitg2 = 0.5 * Ug[0] * g_ener1;
+  gR[4] += invgam1 * g_ener2; gR[0] += 0.5 * vitd2 * g_ener2;
+  const double g_vitd2 = 0.5 * Ud[0] * g_ener2;
+  gL[1] += 2.0 * Ug[1] * g_vitg2; gL[2] += 2.0 * Ug[2] * g_vitg2; gL[3] += 2.0 * Ug[3] * g_vitg2;
+  gR[1] += 2.0 * Ud[1] * g_vitd2; gR[2] += 2.0 * Ud[2] * g_vitd2; gR[3] += 2.0 * Ud[3] * g_vitd2;
+  gL[0] += 0.5 / sq1 * g_sq1;
+  gR[0] += 0.5 / sq2 * g_sq2;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) { gUg[k] += gL[k]; gUd[k] += gR[k]; }
+  if (gn) {
+    // nx = n0 / rnorm ...
+    const double g_inv = n0 * g_nx + n1 * g_ny + n2 * g_nz;
+    g_rnorm += -invnorm * invnorm * g_inv;
+    const double g_s2 = 0.5 / rnorm * g_rnorm;
+    gn[0] += invnorm * g_nx + 2.0 * n0 * g_s2;
+    gn[1] += invnorm * g_ny + 2.0 * n1 * g_s2;
+    gn[2] += invnorm * g_nz + 2.0 * n2 * g_s2;
+  }
+}
+
+// Partial derivatives of RecFcn::computeVanAlbadaFcn (RecFcn.h:268-281)
+// w.r.t. its two arguments, branch by branch.
+__device__ __forceinline__ void vanalbada_fcn_partials(double a, double b, double& da, double& db) {
+  const double eps = 1.e-16;
+  const double ab = a * b;
+  const double D = a * a + b * b + 2.0 * eps;
+  if (ab > 0.0) {
+    const double Nn = a * (b * b + eps) + b * (a * a + eps);
+    da = ((b * b + eps) + 2.0 * a * b) / D - Nn * 2.0 * a / (D * D);
+    db = (2.0 * a * b + (a * a + eps)) / D - Nn * 2.0 * b / (D * D);
+  } else if (ab == 0.0) {
+    const double Nn = 0.5 * eps * (a + b);
+    da = 0.5 * eps / D - Nn * 2.0 * a / (D * D);
+    db = 0.5 * eps / D - Nn * 2.0 * b / (D * D);
+  } else {
+    da = 0.0;
+    db = 0.0;
+  }
+}
+
+// Reverse of the per-component reconstruction (vanalbada / linear /
+// constant): given cotangents of (Vij, Vji), accumulate those of Vi, Vj and
+// of the projected slopes ddVij, ddVji.
+__device__ __forceinline__ void reconstruct_adj(int rec, double beta, double Vi, double ddVij, double Vj,
+                                                double ddVji, double gVij, double gVji, double& gVi, double& gVj,
+                                                double& gddij, double& gddji) {
+  if (rec == AEROF_REC_CONSTANT) {
+    gVi += gVij; gVj += gVji; gddij = 0.0; gddji = 0.0;
+    return;
+  }
+  if (rec == AEROF_REC_LINEAR) {
+    const double b1 = 0.5 - beta;
+    gVi += gVij * (1.0 - b1) + gVji * b1;
+    gVj += gVij * b1 + gVji * (1.0 - b1);
+    gddij = beta * gVij;
+    gddji = -beta * gVji;
+    return;
+  }
+  const double b2 = 1.0 - 2.0 * beta;
+  const double dVji = Vj - Vi;
+  const double dV = b2 * dVji;
+  const double dVi = dV + 2.0 * beta * ddVij;
+  const double dVj = dV + 2.0 * beta * ddVji;
+  double A1, B1, A2, B2;
+  vanalbada_fcn_partials(dVi, dVji, A1, B1);
+  vanalbada_fcn_partials(dVj, dVji, A2, B2);
+  const double g_dVi = 0.5 * A1 * gVij;
+  const double g_dVj = -0.5 * A2 * gVji;
+  double g_dVji = 0.5 * B1 * gVij - 0.5 * B2 * gVji;
+  const double g_dV = g_dVi + g_dVj;
+  gddij = 2.0 * beta * g_dVi;
+  gddji = 2.0 * beta * g_dVj;
+  g_dVji += b2 * g_dV;
+  gVi += gVij - g_dVji;
+  gVj += gVji + g_dVji;
+}
+
+// (dV/dU)^T gV for V = prim(U) (VarFcnSGEuler.h:307-327)
+__device__ __forceinline__ void prim_adj(const Gas& g, const double* U, const double* gV, double* gU) {
+  const double ir = 1.0 / U[0];
+  const double u = U[1] * ir, v = U[2] * ir, w = U[3] * ir;
+  gU[0] = gV[0] - (u * gV[1] + v * gV[2] + w * gV[3]) * ir + g.gam1 * 0.5 * (u * u + v * v + w * w) * gV[4];
+  gU[1] = gV[1] * ir - g.gam1 * u * gV[4];
+  gU[2] = gV[2] * ir - g.gam1 * v * gV[4];
+  gU[3] = gV[3] * ir - g.gam1 * w * gV[4];
+  gU[4] = g.gam1 * gV[4];
+}
+
+}  // namespace aerof

@@ -286,30 +286,41 @@ static int* counters(aerof_gpu_ctx* c) {
 }
 
 // Residual of device state dU into device dR (both [N][5]).  Returns the
-// number of non-positive reconstructed states of the first pass.
-int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR) {
+// number of non-positive reconstructed states of the first pass (sync), or
+// 0 with the count accumulated in counters[2] (no sync, failsafe off).
+int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
   DeviceMesh& m = c->mesh;
   const Gas g = make_gas(c->cfg.gamma);
   const int rec = c->cfg.reconstruction;
   int* cnt = counters(c);
-  AEROF_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * 8, c->stream));
-  prim_dev(c, dU);
+  if (sync) AEROF_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * 2, c->stream));
+  int* ecnt = sync ? cnt : cnt + 2;
   c->s.flux.ensure(5 * (size_t)m.E);
   c->s.G.ensure(16 * (size_t)m.N);
   if (c->cfg.failsafe) {
     c->s.tag.ensure(m.N);
     c->s.tag.zero(c->stream);
   }
-  if (rec != AEROF_REC_CONSTANT) gradients_dev(c);
-  k_edge_flux<<<grid_for(m.E, kBlock), kBlock, 0, c->stream>>>(
-      m.E, g, rec, c->cfg.beta, c->cfg.failsafe, m.edges.p, m.en.p, m.P.p, c->s.G.p, c->s.flux.p,
-      c->s.tag.p, cnt);
-  AEROF_LAUNCH_CHECK();
+  {
+    TimerScope t(c, AEROF_T_NODAL_GRAD);
+    prim_dev(c, dU);
+    if (rec != AEROF_REC_CONSTANT) gradients_dev(c);
+  }
+  {
+    TimerScope t(c, AEROF_T_FV_TERM);
+    k_edge_flux<<<grid_for(m.E, kBlock), kBlock, 0, c->stream>>>(
+        m.E, g, rec, c->cfg.beta, c->cfg.failsafe, m.edges.p, m.en.p, m.P.p, c->s.G.p, c->s.flux.p,
+        c->s.tag.p, ecnt);
+    AEROF_LAUNCH_CHECK();
+  }
   int bad = 0;
-  AEROF_CUDA(cudaMemcpyAsync(&bad, cnt, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  AEROF_CUDA(cudaStreamSynchronize(c->stream));
+  if (sync) {
+    AEROF_CUDA(cudaMemcpyAsync(&bad, cnt, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    AEROF_CUDA(cudaStreamSynchronize(c->stream));
+  }
   if (bad && c->cfg.failsafe && rec != AEROF_REC_CONSTANT) {
     // Domain.C:886-918: zero the gradients of tagged nodes and recompute.
+    TimerScope t(c, AEROF_T_FV_TERM);
     k_grad<<<grid_for(m.N, kBlock), kBlock, 0, c->stream>>>(m.N, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p,
                                                             c->s.tag.p, c->s.G.p);
     AEROF_LAUNCH_CHECK();
@@ -317,15 +328,19 @@ int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR) {
         m.E, g, rec, c->cfg.beta, 0, m.edges.p, m.en.p, m.P.p, c->s.G.p, c->s.flux.p, c->s.tag.p, cnt + 1);
     AEROF_LAUNCH_CHECK();
   }
-  k_node_residual<<<grid_for(m.N, kBlock), kBlock, 0, c->stream>>>(
-      m.N, m.E, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_edge.p,
-      c->s.flux.p, m.nf_ptr.p, m.nf_face.p, m.fcode.p, m.fnrm.p, m.F, m.P.p, m.vol.p, dR);
-  AEROF_LAUNCH_CHECK();
+  {
+    TimerScope t(c, AEROF_T_FV_TERM);
+    k_node_residual<<<grid_for(m.N, kBlock), kBlock, 0, c->stream>>>(
+        m.N, m.E, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_edge.p,
+        c->s.flux.p, m.nf_ptr.p, m.nf_face.p, m.fcode.p, m.fnrm.p, m.F, m.P.p, m.vol.p, dR);
+    AEROF_LAUNCH_CHECK();
+  }
   return bad;
 }
 
 void timestep_dev(aerof_gpu_ctx* c, const double* dU, double cfl, double* ddt) {
   DeviceMesh& m = c->mesh;
+  TimerScope t(c, AEROF_T_TIME_STEP);
   prim_dev(c, dU);
   k_timestep<<<grid_for(m.N, kBlock), kBlock, 0, c->stream>>>(
       m.N, m.E, m.F, make_gas(c->cfg.gamma), cfl, m.edges.p, m.en.p, m.nbr_ptr.p, m.nbr_edge.p, m.nf_ptr.p,
@@ -369,6 +384,35 @@ extern "C" int aerof_gpu_residual(aerof_gpu_ctx* c, const double* U, double* R) 
     double* dR = out_dev(c, R, n5, c->s.Rstage);
     int bad = residual_dev(c, dU, dR);
     out_finish(c, R, dR, n5);
+    return bad;
+  });
+}
+
+extern "C" int aerof_gpu_residual_async(aerof_gpu_ctx* c, const double* U, double* R) {
+  return guard(c, [&]() -> int {
+    if (int e = need_mesh(c)) return e;
+    if (!U || !R || c->cfg.failsafe) return AEROF_EINVAL;
+    if (!is_device_ptr(U) || !is_device_ptr(R)) {
+      c->last_error = "aerof_gpu_residual_async needs device pointers";
+      return AEROF_EINVAL;
+    }
+    if (c->s.counters.n == 0) {
+      counters(c);
+      AEROF_CUDA(cudaMemsetAsync(c->s.counters.p, 0, sizeof(int) * 8, c->stream));
+    }
+    residual_dev(c, U, R, false);
+    return AEROF_OK;
+  });
+}
+
+extern "C" int aerof_gpu_status(aerof_gpu_ctx* c) {
+  return guard(c, [&]() -> int {
+    int bad = 0;
+    if (c->s.counters.n) {
+      AEROF_CUDA(cudaMemcpyAsync(&bad, c->s.counters.p + 2, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      AEROF_CUDA(cudaMemsetAsync(c->s.counters.p + 2, 0, sizeof(int), c->stream));
+    }
+    AEROF_CUDA(cudaStreamSynchronize(c->stream));
     return bad;
   });
 }

@@ -1,0 +1,329 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 edge-based finite-volume hot path.
+
+Workload (one "step" = one evaluation): the FP64 second-order residual of
+AERO-F's SpaceOperator::computeResidual on a 101^3-node jittered Kuhn tet
+mesh (N=1,030,301, E=7,090,300, F_b=120,000), LSQ gradients + van Albada
+MUSCL + Roe flux, slip walls on y/z, Steger-Warming far field on x, Mach 0.8,
+seeded 1% perturbation of the free stream.  Synthetic, seeded inputs stand in
+for the reference's sower meshes (no public dataset is involved).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value   = residual evaluations x E / device time (Medges/s), inputs resident
+          in HBM, K back-to-back asynchronous calls timed with CUDA events.
+e2e     = the same through the public API with pinned host buffers: each
+          step copies U host->device, evaluates, copies R device->host.
+roofline: the finite-volume-term pass (edge fluxes + assembly), algorithmic
+          bytes 32E + 232N + 40F_b per launch, against the measured HBM copy
+          bandwidth; roofline_residual: the whole evaluation against
+          B_res2 = 40E + 464N + 40F_b.
+--impl reference: the CPU oracle (a C++ restatement of the reference's
+          loops; the reference itself needs Fortran/MPI and cannot be built)
+          timed with all host threads on the same workload.
+Multi-GPU (torchrun): independent replicas, one per GPU, weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "residual Medges/s, %HBM peak; mixed vs FP64 Newton time-to-1e-8; adjoint cost"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": FALLBACK_HBM_GBS, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"]
+        if self.gpu_id:
+            cmd += ["-i", self.gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def build_workload(n: int):
+    from aerof_dev_b200 import workloads as W
+    mesh = W.make_lattice_mesh(n, jitter=0.2, codes="channel")
+    Ub = W.freestream(0.8)
+    U = W.perturbed_state(mesh["X"].shape[0], 0.8)
+    return W, mesh, Ub, U
+
+
+def cpu_baseline(mesh, Ub, U, E: int, budget_s: float = 20.0, max_evals: int = 20) -> dict:
+    """CPU oracle (restatement of the reference's loops), all host threads,
+    on a bounded number of full evaluations of the same workload."""
+    from oracle.oracle import Oracle
+    o = Oracle(mesh)
+    cores = os.cpu_count() or 1
+    out = np.empty_like(U)
+    o.residual_threaded(U, Ub, 2, nthreads=cores, out=out)  # warm-up
+    t0 = time.perf_counter()
+    k = 0
+    while k < max_evals:
+        o.residual_threaded(U, Ub, 2, nthreads=cores, out=out)
+        k += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": E * k / dt / 1e6, "unit": "Medges/s", "cores": cores, "kind": "port",
+            "sample": f"{k} full second-order residual evaluations of the 101^3 mesh after 1 warm-up "
+                      f"({dt:.1f} s), OpenMP over {cores} threads, g++ -O3 -march=native"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    W, mesh, Ub, U = build_workload(args.n)
+    s = W.lattice_sizes(args.n)
+    from oracle.oracle import Oracle
+    o = Oracle(mesh)
+    cores = os.cpu_count() or 1
+    out = np.empty_like(U)
+    for _ in range(max(args.warmup, 1)):
+        o.residual_threaded(U, Ub, 2, nthreads=cores, out=out)
+        break  # one warm-up evaluation is enough on the CPU
+    # each step is one full evaluation; the number of timed steps is capped
+    # so the run stays within a few minutes
+    t0 = time.perf_counter()
+    k = 0
+    while k < args.steps:
+        o.residual_threaded(U, Ub, 2, nthreads=cores, out=out)
+        k += 1
+        if time.perf_counter() - t0 > args.ref_budget:
+            break
+    dt = time.perf_counter() - t0
+    value = s["E"] * k / dt / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Medges/s", "n_gpus": args.gpus,
+        "steps": k, "requested_steps": args.steps, "warmup": 1, "ms_per_step": dt / k * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(args, s),
+        "cpu_baseline": {"value": value, "unit": "Medges/s", "cores": cores, "kind": "port",
+                         "sample": f"{k} full evaluations (capped at {args.ref_budget:.0f} s of the "
+                                   f"{args.steps} requested), OpenMP over {cores} threads"},
+        "e2e": {"value": value, "unit": "Medges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config_dict(args, s) -> dict:
+    return {"workload": f"FP64 second-order residual (LSQ + van Albada + Roe), {args.n}^3 jittered Kuhn tet mesh "
+                        f"N={s['N']} E={s['E']} F_b={s['F']}, slip walls y/z, far field x, Mach 0.8",
+            "mesh_n": args.n, "N": s["N"], "E": s["E"], "F_b": s["F"], "evals_per_step": 1,
+            "l2": "working set > 126 MB L2 (node data 0.2 GB + edge data 0.5 GB); no flush",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+def run_ours(args):
+    import torch
+    import aerof_dev_b200 as A
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    W, mesh, Ub, U = build_workload(args.n)
+    s = W.lattice_sizes(args.n)
+    ctx = A.Context.from_mesh(mesh, Ub, reconstruction=A.REC_VANALBADA, device=local)
+    assert ctx.E == s["E"]
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    sp = A.SpaceOperator(ctx)
+    Ud = torch.from_numpy(U).cuda()
+    Rd = torch.empty_like(Ud)
+    for _ in range(args.warmup):
+        sp.computeResidualAsync(Ud, Rd)
+    bad = ctx.status()
+    ctx.timers()
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    time.sleep(0.3)
+    ctx.profile(True)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        sp.computeResidualAsync(Ud, Rd)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if pg:
+        pg.barrier()
+    bad += ctx.status()
+    tm = ctx.timers()
+    ctx.profile(False)
+    clk = clocks.stop()
+    if pg:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    value = s["E"] * args.steps * world / (ms * 1e-3) / 1e6
+
+    # end to end through the public API with pinned host buffers
+    ctx.set_stream(stream.cuda_stream)
+    Uh = torch.from_numpy(U).pin_memory()
+    Rh = torch.empty_like(Uh).pin_memory()
+    k2 = max(1, min(args.steps, args.e2e_steps))
+    sp.computeResidual(Uh, Rh)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(k2):
+        sp.computeResidual(Uh, Rh)
+    a1.record(stream)
+    torch.cuda.synchronize()
+    ms2 = a0.elapsed_time(a1)
+    if pg:
+        t = torch.tensor([ms2], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms2 = float(t.item())
+    e2e = s["E"] * k2 * world / (ms2 * 1e-3) / 1e6
+
+    peaks = measured_peaks()
+    fv_ms, fv_n = tm["fv_term"]
+    t_fv = fv_ms / max(fv_n, 1) * 1e-3
+    B_fv = 32 * s["E"] + 232 * s["N"] + 40 * s["F"]
+    ach = B_fv / t_fv / 1e9
+    B_res = 40 * s["E"] + 464 * s["N"] + 40 * s["F"]
+    t_eval = ms * 1e-3 / args.steps
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get("fv_term_bytes_per_launch")
+    line = {
+        "metric": METRIC, "value": value, "unit": "Medges/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_dict(args, s),
+        "roofline": {"bound": "hbm", "kernel": "finite-volume term (edge fluxes + assembly)",
+                     "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": ach / peaks["hbm_gbs"],
+                     "traffic": traffic, "algorithmic_bytes": B_fv, "ms_per_launch": t_fv * 1e3,
+                     "peak_source": peaks["source"]},
+        "roofline_residual": {"bound": "hbm", "achieved": B_res / t_eval / 1e9, "peak": peaks["hbm_gbs"],
+                              "unit": "GB/s", "frac": B_res / t_eval / 1e9 / peaks["hbm_gbs"],
+                              "algorithmic_bytes": B_res},
+        "timers_ms_per_eval": {k: (v[0] / max(v[1], 1)) for k, v in tm.items() if v[1]},
+        "e2e": {"value": e2e, "unit": "Medges/s", "h2d_bytes_per_step": U.nbytes, "d2h_bytes_per_step": U.nbytes,
+                "steps": k2},
+        "gpu_launches": 4 * args.steps,
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
+                   "samples": clk["samples"]},
+        "unphysical_states": bad,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(mesh, Ub, U, s["E"])
+    ctx.close()
+    if pg:
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=101, help="lattice nodes per side")
+    ap.add_argument("--e2e-steps", type=int, default=200)
+    ap.add_argument("--ref-budget", type=float, default=120.0, help="seconds of timed CPU work (reference arm)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -108,6 +108,11 @@ int aerof_gpu_last_error(aerof_gpu_ctx* ctx, char* buf, int len);
  * free-stream state of every far-field face (DistBcData.C:652-730).       */
 int aerof_gpu_set_mesh(aerof_gpu_ctx* ctx, int N, int T, int F, const double* X, const int* tets,
                        const int* faces, const int* codes, const double* Ub);
+/* New node coordinates X[N][3] for the same topology: recomputes the
+ * static geometry (DistGeoState::compute with a moved mesh, as the shape
+ * finite differences of fsoSemiAnalytical do, FluidShapeOptimizationHandler.C:
+ * 1216-1363).                                                               */
+int aerof_gpu_update_coordinates(aerof_gpu_ctx* ctx, const double* X);
 int aerof_gpu_mesh_sizes(aerof_gpu_ctx* ctx, int* N, int* E, int* F);
 /* Edge list [E][2] (i<j), lexicographic: EdgeSet::getPtr (Edge.h). */
 int aerof_gpu_get_edges(aerof_gpu_ctx* ctx, int* edges);
@@ -123,6 +128,16 @@ int aerof_gpu_get_geometry(aerof_gpu_ctx* ctx, double* edge_normal, double* face
  * Returns the number of non-positive reconstructed densities/pressures
  * (EdgeCore.C:137-168) -- 0 on a healthy state.                          */
 int aerof_gpu_residual(aerof_gpu_ctx* ctx, const double* U, double* R);
+/* Same as aerof_gpu_residual for device-resident U and R, without waiting
+ * for the GPU: the call only enqueues work on the context's stream.  The
+ * count of non-positive reconstructed states accumulates on the device and
+ * is returned (and reset) by aerof_gpu_status.  Requires failsafe == 0
+ * (the failsafe re-run needs the count on the host), AEROF_EINVAL otherwise. */
+int aerof_gpu_residual_async(aerof_gpu_ctx* ctx, const double* U, double* R);
+/* Waits for the context's stream; returns the accumulated unphysical count
+ * of asynchronous calls since the previous aerof_gpu_status (>= 0) or an
+ * error code.                                                              */
+int aerof_gpu_status(aerof_gpu_ctx* ctx);
 /* DistNodalGrad::compute, least squares (DistNodalGrad.C:790-806,
  * SubDomain.C:297-374) of primitive V[N][5]; ddx/ddy/ddz [N][5].        */
 int aerof_gpu_gradients(aerof_gpu_ctx* ctx, const double* V, double* ddx, double* ddy, double* ddz);
@@ -167,6 +182,24 @@ int aerof_gpu_gmres(aerof_gpu_ctx* ctx, const double* b, double* x, int krylov, 
 int aerof_gpu_newton(aerof_gpu_ctx* ctx, double* U, const aerof_newton_params* p,
                      aerof_newton_result* out, double* history);
 
+/* ---- timers ------------------------------------------------------------
+ * The reference's Timer categories (Timer.h:12-70: addNodalGradTime,
+ * addFiniteVolumeTermTime, addTimeStepTime, addFiniteVolumeJacTime,
+ * addPrecSetupTime, addKspTime) measured with CUDA events on the context's
+ * stream while profiling is enabled.                                        */
+#define AEROF_T_NODAL_GRAD 0    /* conservative->primitive + LSQ gradients   */
+#define AEROF_T_FV_TERM 1       /* edge fluxes + boundary fluxes + assembly  */
+#define AEROF_T_TIME_STEP 2
+#define AEROF_T_FV_JAC 3
+#define AEROF_T_PREC_SETUP 4
+#define AEROF_T_KSP_MATVEC 5
+#define AEROF_T_KSP_OTHER 6     /* orthogonalisation, preconditioner apply   */
+#define AEROF_T_COUNT 8
+int aerof_gpu_profile(aerof_gpu_ctx* ctx, int enable);
+/* Waits for the stream, then returns per category the summed device time
+ * in milliseconds and the number of timed intervals, and resets them.     */
+int aerof_gpu_timers(aerof_gpu_ctx* ctx, double* ms, long long* count, int n);
+
 /* ---- sensitivities ----------------------------------------------------
  * Exact linearisation of the configured residual (the operator
  * MatVecProdH2 applies, MatVecProd.C:1462-1704; derivative routines
@@ -182,6 +215,14 @@ int aerof_gpu_dRdX(aerof_gpu_ctx* ctx, const double* U, const double* Xdot, doub
 /* gX = (dR/dX)^T . lambda, gX[N][3] (fsoApply_dFdXtranspose,
  * FluidShapeOptimizationHandler.C:1434-1448)                               */
 int aerof_gpu_dRdX_T(aerof_gpu_ctx* ctx, const double* U, const double* lambda, double* gX);
+
+/* Linearised steady solves with the exact Jacobian applied matrix-free
+ * (fsoLinearSolver / fsoAdjointLinearSolver, FluidShapeOptimizationHandler.C:
+ * 1557-1624; GmresSolver::solve / solveT): transpose = 0 solves J x = b,
+ * transpose = 1 solves J^T x = b, GMRES(krylov) right-preconditioned by the
+ * block-Jacobi of the FP64 first-order operator at U (no time term).       */
+int aerof_gpu_linearized_solve(aerof_gpu_ctx* ctx, const double* U, const double* b, double* x, int krylov,
+                               int maxits, double eps, int transpose, int* its, double* res);
 
 #ifdef __cplusplus
 }

@@ -34,6 +34,7 @@ LIB_PATH = os.path.join(HERE, "libaerof_gpu.so")
 AEROF_OK = 0
 ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ETIMEDOUT", -5: "ESINGULAR", -6: "ESTATE"}
 REC_CONSTANT, REC_VANALBADA, REC_LINEAR = 1, 2, 3
+KERNEL_BLOCKED, KERNEL_EDGE = 0, 1
 PREC_FP32, PREC_FP64 = 32, 64
 
 # every entry point of include/aerof_gpu.h
@@ -58,7 +59,8 @@ class AerofError(RuntimeError):
 
 class Config(C.Structure):
     _fields_ = [("gamma", C.c_double), ("beta", C.c_double), ("reconstruction", C.c_int),
-                ("failsafe", C.c_int), ("device", C.c_int), ("reserved", C.c_int * 5)]
+                ("failsafe", C.c_int), ("device", C.c_int), ("residual_kernel", C.c_int),
+                ("reserved", C.c_int * 4)]
 
 
 class NewtonParams(C.Structure):
@@ -169,9 +171,9 @@ class Context:
     """One GPU context: ``aerof_gpu_create`` + ``aerof_gpu_set_mesh``."""
 
     def __init__(self, reconstruction: int = REC_VANALBADA, gamma: float = 1.4, beta: float = 1.0 / 3.0,
-                 failsafe: int = 0, device: int = 0):
+                 failsafe: int = 0, device: int = 0, residual_kernel: int = KERNEL_BLOCKED):
         self.L = library()
-        cfg = Config(gamma, beta, reconstruction, failsafe, device)
+        cfg = Config(gamma, beta, reconstruction, failsafe, device, residual_kernel)
         h = C.c_void_p()
         self._check(self.L.aerof_gpu_create(C.byref(cfg), C.byref(h)), None)
         self.h = h

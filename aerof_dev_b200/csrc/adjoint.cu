@@ -260,9 +260,11 @@ __global__ void k_a_edges(int E, Gas g, int rec, double beta, const int2* __rest
     o[5 + k] = gvj;
     o[10 + k] = gdi;
     o[15 + k] = gdj;
-    gdx0 += gi[k] * gdi + gj[k] * gdj;
-    gdx1 += gi[5 + k] * gdi + gj[5 + k] * gdj;
-    gdx2 += gi[10 + k] * gdi + gj[10 + k] * gdj;
+    if (rec != AEROF_REC_CONSTANT) {
+      gdx0 += gi[k] * gdi + gj[k] * gdj;
+      gdx1 += gi[5 + k] * gdi + gj[5 + k] * gdj;
+      gdx2 += gi[10 + k] * gdi + gj[10 + k] * gdj;
+    }
   }
   o[20] = gn[0]; o[21] = gn[1]; o[22] = gn[2];
   o[23] = gdx0; o[24] = gdx1; o[25] = gdx2;

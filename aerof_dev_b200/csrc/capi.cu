@@ -102,7 +102,8 @@ extern "C" int aerof_gpu_create(const aerof_gpu_config* cfg, aerof_gpu_ctx** out
   *out = nullptr;
   if (!(cfg->gamma > 1.0) || cfg->beta < 0.0 || cfg->beta > 0.5 ||
       (cfg->reconstruction != AEROF_REC_CONSTANT && cfg->reconstruction != AEROF_REC_VANALBADA &&
-       cfg->reconstruction != AEROF_REC_LINEAR))
+       cfg->reconstruction != AEROF_REC_LINEAR) ||
+      (cfg->residual_kernel != AEROF_KERNEL_BLOCKED && cfg->residual_kernel != AEROF_KERNEL_EDGE))
     return AEROF_EINVAL;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device < 0 || cfg->device >= ndev) {

@@ -111,11 +111,31 @@ struct DeviceMesh {
   DBuf<int> nt_tet;        // [4T]  tet*4 + local vertex
   // host copies for queries
   std::vector<int> h_edges;
+
+  // ---- blocked residual: Morton-renumbered copy of the node data ----
+  int NB = 256;            // nodes per block
+  int nblk = 0, maxE = 0, nX = 0;
+  DBuf<int> n2o, o2n;      // [N] new -> old and old -> new node ids
+  DBuf<double> P2;         // [N][8] node records in new numbering
+  DBuf<double> W2;         // [6][N] LSQ constants, new numbering
+  DBuf<double> vol2;       // [N]
+  DBuf<int> nb2_ptr, nb2_node;  // neighbour CSR in new numbering (ascending)
+  DBuf<int2> bedges;       // [E] (first, second) new ids, sorted, first < second
+  DBuf<int> bsrc;          // [E] reference edge id | (1<<31 if reversed)
+  DBuf<double> bnorm;      // [3][E] normals oriented first -> second
+  DBuf<int> beptr;         // [nblk+1] owned-edge range of each block
+  DBuf<int> lptr, lidx;    // per node (new): owned local edge slots, sign bit = second endpoint
+  DBuf<int> xslot;         // [E] spill slot of a block-crossing edge, -1 otherwise
+  DBuf<int> xin_ptr, xin_slot;  // per node (new): incoming spill slots
 };
 
 struct Scratch {
   DBuf<double> G;          // [N][16] gradients ddx(5) ddy(5) ddz(5) pad
   DBuf<double> flux;       // [5][E] per-edge fluxes
+  DBuf<double> fbuf;       // [3F][5] boundary subface fluxes
+  DBuf<double> G2;         // [N][16] gradients, blocked numbering
+  DBuf<double> part;       // [N][5] block-local flux sums, blocked numbering
+  DBuf<double> spill;      // [nX][5] fluxes of block-crossing edges
   DBuf<double> Ustage, Rstage, Vstage, Xstage;  // staging for host arrays
   DBuf<double> dt, k1, k2, U0;
   DBuf<int> tag;           // [N] failsafe tags

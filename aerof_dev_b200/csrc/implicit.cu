@@ -106,11 +106,11 @@ __global__ void k_jac_diag(int N, int F, Gas g, const double* __restrict__ Ub0, 
 // neighbours in ascending order (SubDomain::computeMatVecProdH1 and
 // H1transpose, SubDomain.C:3916-3995).  Blocks in S (float or double),
 // vectors and accumulation in double.
-template <class S>
-__device__ __forceinline__ void gemv_add(const S* __restrict__ a, const double* __restrict__ x, double* y, bool trans) {
+template <class S, class TX>
+__device__ __forceinline__ void gemv_add(const S* __restrict__ a, const TX* __restrict__ x, double* y, bool trans) {
   double xv[5];
 #pragma unroll
-  for (int k = 0; k < 5; ++k) xv[k] = x[k];
+  for (int k = 0; k < 5; ++k) xv[k] = (double)x[k];
   if (!trans) {
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
@@ -130,10 +130,10 @@ __device__ __forceinline__ void gemv_add(const S* __restrict__ a, const double* 
   }
 }
 
-template <class S, bool TRANS>
+template <class S, bool TRANS, class TI, class TO>
 __global__ void k_spmv(int N, const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_node,
                        const int* __restrict__ nbr_tpos, const S* __restrict__ diag, const S* __restrict__ off,
-                       const double* __restrict__ p, double* __restrict__ y) {
+                       const TI* __restrict__ p, TO* __restrict__ y) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double acc[5] = {0, 0, 0, 0, 0};
@@ -143,7 +143,7 @@ __global__ void k_spmv(int N, const int* __restrict__ nbr_ptr, const int* __rest
     gemv_add(off + 25 * b, p + 5 * (size_t)nbr_node[q], acc, TRANS);
   }
 #pragma unroll
-  for (int k = 0; k < 5; ++k) y[5 * (size_t)i + k] = acc[k];
+  for (int k = 0; k < 5; ++k) y[5 * (size_t)i + k] = (TO)acc[k];
 }
 
 // Block-Jacobi set-up (JacobiPrec::setup -> DiagMat::invert, DiagMatrix.C:
@@ -166,15 +166,15 @@ __global__ void k_bj_invert(int N, const S* __restrict__ diag, S* __restrict__ d
 }
 
 // z = D^-1 x (or D^-T x): JacobiPrec::apply/applyT (KspPrec.C:86-111)
-template <class S>
-__global__ void k_bj_apply(int N, const S* __restrict__ dinv, const double* __restrict__ x, double* __restrict__ z,
+template <class S, class TI, class TO>
+__global__ void k_bj_apply(int N, const S* __restrict__ dinv, const TI* __restrict__ x, TO* __restrict__ z,
                            int trans) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double acc[5] = {0, 0, 0, 0, 0};
   gemv_add(dinv + 25 * (size_t)i, x + 5 * (size_t)i, acc, trans != 0);
 #pragma unroll
-  for (int k = 0; k < 5; ++k) z[5 * (size_t)i + k] = acc[k];
+  for (int k = 0; k < 5; ++k) z[5 * (size_t)i + k] = (TO)acc[k];
 }
 
 // ------------------------------------------------------------ vector ops
@@ -183,30 +183,34 @@ __global__ void k_axpby(size_t n, double a, const double* __restrict__ x, double
   size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q < n) z[q] = a * x[q] + b * y[q];
 }
-__global__ void k_scale(size_t n, double a, const double* __restrict__ x, double* __restrict__ z) {
+template <class TI, class TO>
+__global__ void k_scale(size_t n, double a, const TI* __restrict__ x, TO* __restrict__ z) {
   size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < n) z[q] = a * x[q];
+  if (q < n) z[q] = (TO)(a * (double)x[q]);
 }
 // z = b - w
-__global__ void k_sub(size_t n, const double* __restrict__ b, const double* __restrict__ w, double* __restrict__ z) {
+template <class TW, class TO>
+__global__ void k_sub(size_t n, const double* __restrict__ b, const TW* __restrict__ w, TO* __restrict__ z) {
   size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < n) z[q] = b[q] - w[q];
+  if (q < n) z[q] = (TO)(b[q] - (double)w[q]);
 }
 // Modified Gram-Schmidt step i with the projection of step i-1 fused in:
 //   w -= hprev * Vprev   (hprev read from device memory, skipped if null)
 //   part[b] = partial sums of w . Vcur      (deterministic block tree)
-__global__ void k_mgs_step(size_t n, const double* __restrict__ hprev, const double* __restrict__ Vprev,
-                           const double* __restrict__ Vcur, double* __restrict__ w, double* __restrict__ part) {
+template <class TV>
+__global__ void k_mgs_step(size_t n, const double* __restrict__ hprev, const TV* __restrict__ Vprev,
+                           const TV* __restrict__ Vcur, TV* __restrict__ w, double* __restrict__ part) {
   __shared__ double sh[kIB];
   const double h = hprev ? *hprev : 0.0;
   double s = 0.0;
   for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-    double wq = w[q];
+    double wq = (double)w[q];
     if (hprev) {
-      wq = wq - h * Vprev[q];
-      w[q] = wq;
+      wq = wq - h * (double)Vprev[q];
+      w[q] = (TV)wq;
+      wq = (double)(TV)wq;
     }
-    s += wq * Vcur[q];
+    s += wq * (double)Vcur[q];
   }
   sh[threadIdx.x] = s;
   __syncthreads();
@@ -229,14 +233,16 @@ __global__ void k_sum_partials(int nb, const double* __restrict__ part, double* 
   if (threadIdx.x == 0) out[0] = sh[0];
 }
 // last projection of the column, then w . w
-__global__ void k_mgs_last(size_t n, const double* __restrict__ hprev, const double* __restrict__ Vprev,
-                           double* __restrict__ w, double* __restrict__ part) {
+template <class TV>
+__global__ void k_mgs_last(size_t n, const double* __restrict__ hprev, const TV* __restrict__ Vprev,
+                           TV* __restrict__ w, double* __restrict__ part) {
   __shared__ double sh[kIB];
   const double h = *hprev;
   double s = 0.0;
   for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-    double wq = w[q] - h * Vprev[q];
-    w[q] = wq;
+    const TV wt = (TV)((double)w[q] - h * (double)Vprev[q]);
+    w[q] = wt;
+    const double wq = (double)wt;
     s += wq * wq;
   }
   sh[threadIdx.x] = s;
@@ -248,17 +254,34 @@ __global__ void k_mgs_last(size_t n, const double* __restrict__ hprev, const dou
   if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 // x += sum_m y_m V_m   (y on the device, k terms)
-__global__ void k_combine(size_t n, int k, const double* __restrict__ y, const double* __restrict__ V, size_t ld,
-                          double* __restrict__ out) {
+template <class TV>
+__global__ void k_combine(size_t n, int k, const double* __restrict__ y, const TV* __restrict__ V, size_t ld,
+                          TV* __restrict__ out) {
   size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   double s = 0.0;
-  for (int m = 0; m < k; ++m) s += y[m] * V[(size_t)m * ld + q];
-  out[q] = s;
+  for (int m = 0; m < k; ++m) s += y[m] * (double)V[(size_t)m * ld + q];
+  out[q] = (TV)s;
 }
-__global__ void k_add(size_t n, const double* __restrict__ a, double* __restrict__ x) {
+template <class TA>
+__global__ void k_add(size_t n, const TA* __restrict__ a, double* __restrict__ x) {
   size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < n) x[q] += a[q];
+  if (q < n) x[q] += (double)a[q];
+}
+// deterministic dot / squared norm of TV vectors, FP64 accumulation
+template <class TV>
+__global__ void k_dot_tv(size_t n, const TV* __restrict__ x, const TV* __restrict__ y, double* __restrict__ part) {
+  __shared__ double sh[kIB];
+  double s = 0.0;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+    s += (double)x[q] * (double)y[q];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if (threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
 }  // namespace aerof
@@ -309,20 +332,22 @@ void jacobian_dev(aerof_gpu_ctx* c, const double* dU, const double* ddt, int pre
   J.prec_ready = false;
 }
 
-void matvec_dev(aerof_gpu_ctx* c, const double* p, double* y, int trans) {
+template <class TI, class TO>
+void matvec_t(aerof_gpu_ctx* c, const TI* p, TO* y, int trans) {
   DeviceMesh& m = c->mesh;
   TimerScope tm(c, AEROF_T_KSP_MATVEC);
   Implicit& J = c->imp;
   const int gn = grid_for(m.N, kIB);
   if (J.precision == AEROF_PREC_FP32) {
-    if (trans) k_spmv<float, true><<<gn, kIB, 0, c->stream>>>(m.N, m.nbr_ptr.p, m.nbr_node.p, m.nbr_tpos.p, J.diag32.p, J.off32.p, p, y);
-    else k_spmv<float, false><<<gn, kIB, 0, c->stream>>>(m.N, m.nbr_ptr.p, m.nbr_node.p, m.nbr_tpos.p, J.diag32.p, J.off32.p, p, y);
+    if (trans) k_spmv<float, true, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, m.nbr_ptr.p, m.nbr_node.p, m.nbr_tpos.p, J.diag32.p, J.off32.p, p, y);
+    else k_spmv<float, false, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, m.nbr_ptr.p, m.nbr_node.p, m.nbr_tpos.p, J.diag32.p, J.off32.p, p, y);
   } else {
-    if (trans) k_spmv<double, true><<<gn, kIB, 0, c->stream>>>(m.N, m.nbr_ptr.p, m.nbr_node.p, m.nbr_tpos.p, J.diag64.p, J.off64.p, p, y);
-    else k_spmv<double, false><<<gn, kIB, 0, c->stream>>>(m.N, m.nbr_ptr.p, m.nbr_node.p, m.nbr_tpos.p, J.diag64.p, J.off64.p, p, y);
+    if (trans) k_spmv<double, true, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, m.nbr_ptr.p, m.nbr_node.p, m.nbr_tpos.p, J.diag64.p, J.off64.p, p, y);
+    else k_spmv<double, false, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, m.nbr_ptr.p, m.nbr_node.p, m.nbr_tpos.p, J.diag64.p, J.off64.p, p, y);
   }
   AEROF_LAUNCH_CHECK();
 }
+void matvec_dev(aerof_gpu_ctx* c, const double* p, double* y, int trans) { matvec_t<double, double>(c, p, y, trans); }
 
 int prec_setup_dev(aerof_gpu_ctx* c) {
   DeviceMesh& m = c->mesh;
@@ -347,77 +372,111 @@ int prec_setup_dev(aerof_gpu_ctx* c) {
   return h;
 }
 
-void prec_apply_dev(aerof_gpu_ctx* c, const double* x, double* z, int trans) {
+template <class TI, class TO>
+void prec_apply_t(aerof_gpu_ctx* c, const TI* x, TO* z, int trans) {
   DeviceMesh& m = c->mesh;
   TimerScope tp(c, AEROF_T_KSP_OTHER);
   Implicit& J = c->imp;
   const int gn = grid_for(m.N, kIB);
-  if (J.precision == AEROF_PREC_FP32) k_bj_apply<float><<<gn, kIB, 0, c->stream>>>(m.N, J.dinv32.p, x, z, trans);
-  else k_bj_apply<double><<<gn, kIB, 0, c->stream>>>(m.N, J.dinv64.p, x, z, trans);
+  if (J.precision == AEROF_PREC_FP32)
+    k_bj_apply<float, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, J.dinv32.p, x, z, trans);
+  else
+    k_bj_apply<double, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, J.dinv64.p, x, z, trans);
   AEROF_LAUNCH_CHECK();
+}
+void prec_apply_dev(aerof_gpu_ctx* c, const double* x, double* z, int trans) {
+  prec_apply_t<double, double>(c, x, z, trans);
 }
 
 // GmresSolver::solve (KspSolver.C:351-492), typePrec = 2 (right
 // preconditioning), MGS, Givens rotations and back substitution on the host
 // (KspSolver.C:917-982).  x = 0 on entry.  Returns iterations.
-int gmres_dev(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int maxits, double eps, int trans,
-              double* final_res, const double* exactU) {
-  // operator: the assembled H1 matrix, or (exactU != null) the exact
-  // linearisation at state exactU applied matrix-free (MatVecProdH2,
-  // MatVecProd.C:1462-1704): J p by forward mode, J^T p by reverse mode.
-  auto op = [&](const double* p, double* y) {
-    if (!exactU) { matvec_dev(c, p, y, trans); return; }
-    TimerScope t(c, AEROF_T_KSP_MATVEC);
-    if (trans) vjp_dev(c, exactU, p, y);
-    else residual_forward(c, exactU, p, nullptr, y, false);
-  };
+// TV is the storage type of the Krylov vectors: double, or float for the
+// mixed-precision solver (dots, norms and the Hessenberg system stay FP64;
+// b and x stay FP64).  exactU != null selects the exact operator (TV =
+// double only).
+template <class TV>
+static int gmres_t(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int maxits, double eps, int trans,
+                   double* final_res, const double* exactU) {
   DeviceMesh& m = c->mesh;
   Implicit& J = c->imp;
   const size_t n = 5 * (size_t)m.N;
   const int gv = grid_for(n, kIB);
   cudaStream_t s = c->stream;
-  J.basis.ensure((size_t)(numVec + 1) * n);
-  J.w.ensure(n); J.r.ensure(n);
+  const size_t vbytes = (size_t)(numVec + 1) * n * sizeof(TV);
+  J.basis.ensure((vbytes + 7) / 8);
+  J.w.ensure((n * sizeof(TV) + 7) / 8);
+  J.r.ensure((n * sizeof(TV) + 7) / 8);
   J.hcol.ensure((size_t)numVec + 2 + (size_t)numVec + 1);
   c->s.red.ensure(kGB);
-  double* Vb = J.basis.p;
-  double* w = J.w.p;
-  double* r = J.r.p;
+  TV* Vb = reinterpret_cast<TV*>(J.basis.p);
+  TV* w = reinterpret_cast<TV*>(J.w.p);
+  TV* r = reinterpret_cast<TV*>(J.r.p);
   double* hd = J.hcol.p;              // [numVec + 2] Hessenberg column
   double* yd = J.hcol.p + numVec + 2;  // [numVec + 1] solution coefficients
   double* part = c->s.red.p;
+  auto op = [&](const TV* p, TV* y) {
+    if (!exactU) { matvec_t<TV, TV>(c, p, y, trans); return; }
+    TimerScope t(c, AEROF_T_KSP_MATVEC);
+    const double* pd = reinterpret_cast<const double*>(p);
+    double* yy = reinterpret_cast<double*>(y);
+    if (trans) vjp_dev(c, exactU, pd, yy);
+    else residual_forward(c, exactU, pd, nullptr, yy, false);
+  };
+  auto norm2 = [&](const TV* v) -> double {
+    k_dot_tv<TV><<<kGB, kIB, 0, s>>>(n, v, v, part);
+    AEROF_LAUNCH_CHECK();
+    k_sum_partials<<<1, kIB, 0, s>>>(kGB, part, hd);
+    AEROF_LAUNCH_CHECK();
+    double h = 0.0;
+    AEROF_CUDA(cudaMemcpyAsync(&h, hd, sizeof(double), cudaMemcpyDeviceToHost, s));
+    AEROF_CUDA(cudaStreamSynchronize(s));
+    return std::sqrt(h);
+  };
   AEROF_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
   std::vector<double> H((size_t)(numVec + 1) * numVec, 0.0), cs(2 * (size_t)numVec), g(numVec + 1), y(numVec),
       hcol(numVec + 2);
   auto h = [&](int i, int j) -> double& { return H[(size_t)i * numVec + j]; };
-  auto dot_to = [&](const double* hp, const double* vprev, const double* vcur, double* out) {
-    k_mgs_step<<<kGB, kIB, 0, s>>>(n, hp, vprev, vcur, w, part);
+  auto dot_to = [&](const double* hp, const TV* vprev, const TV* vcur, double* out) {
+    k_mgs_step<TV><<<kGB, kIB, 0, s>>>(n, hp, vprev, vcur, w, part);
     AEROF_LAUNCH_CHECK();
     k_sum_partials<<<1, kIB, 0, s>>>(kGB, part, out);
     AEROF_LAUNCH_CHECK();
   };
   int iter = 0, exitLoop = 0;
   double target = 0.0, l2res = 0.0;
+  const double bnorm = norm2_dev(c, b, n);
   do {
-    // r = b - A x ; beta = ||r||  (x == 0 on the first cycle)
-    op(x, w);
-    k_sub<<<gv, kIB, 0, s>>>(n, b, w, r);
-    AEROF_LAUNCH_CHECK();
-    double beta = norm2_dev(c, r, n);
-    if (iter == 0) target = eps * norm2_dev(c, b, n);
+    // r = b - A x  (x == 0 on the first cycle)
+    if (iter == 0) {
+      k_scale<double, TV><<<gv, kIB, 0, s>>>(n, 1.0, b, r);
+      AEROF_LAUNCH_CHECK();
+    } else {
+      k_scale<double, TV><<<gv, kIB, 0, s>>>(n, 1.0, x, r);
+      AEROF_LAUNCH_CHECK();
+      op(r, w);
+      k_sub<TV, TV><<<gv, kIB, 0, s>>>(n, b, w, r);
+      AEROF_LAUNCH_CHECK();
+    }
+    const double beta = norm2(r);
+    if (iter == 0) target = eps * bnorm;
     if (beta == 0.0) { if (final_res) *final_res = 0.0; return iter; }
-    k_scale<<<gv, kIB, 0, s>>>(n, 1.0 / beta, r, Vb);
+    k_scale<TV, TV><<<gv, kIB, 0, s>>>(n, 1.0 / beta, r, Vb);
     AEROF_LAUNCH_CHECK();
     std::fill(g.begin(), g.end(), 0.0);
     g[0] = beta;
     int j;
     for (j = 0; j < numVec; ++j) {
-      prec_apply_dev(c, Vb + (size_t)j * n, r, trans);
+      {
+        TimerScope t(c, AEROF_T_KSP_OTHER);
+        prec_apply_t<TV, TV>(c, Vb + (size_t)j * n, r, trans);
+      }
       op(r, w);
       // h_ij = w . V_i ; w -= h_ij V_i   (i = 0..j), then ||w||
+      TimerScope t(c, AEROF_T_KSP_OTHER);
       for (int i = 0; i <= j; ++i)
         dot_to(i ? hd + (i - 1) : nullptr, i ? Vb + (size_t)(i - 1) * n : nullptr, Vb + (size_t)i * n, hd + i);
-      k_mgs_last<<<kGB, kIB, 0, s>>>(n, hd + j, Vb + (size_t)j * n, w, part);
+      k_mgs_last<TV><<<kGB, kIB, 0, s>>>(n, hd + j, Vb + (size_t)j * n, w, part);
       AEROF_LAUNCH_CHECK();
       k_sum_partials<<<1, kIB, 0, s>>>(kGB, part, hd + j + 1);
       AEROF_LAUNCH_CHECK();
@@ -427,7 +486,7 @@ int gmres_dev(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int maxi
       h(j + 1, j) = std::sqrt(hcol[j + 1]);
       const bool breakdown = (h(j + 1, j) == 0.0);
       if (!breakdown) {
-        k_scale<<<gv, kIB, 0, s>>>(n, 1. / h(j + 1, j), w, Vb + (size_t)(j + 1) * n);
+        k_scale<TV, TV><<<gv, kIB, 0, s>>>(n, 1. / h(j + 1, j), w, Vb + (size_t)(j + 1) * n);
         AEROF_LAUNCH_CHECK();
       }
       for (int i = 0; i < j; ++i) {
@@ -457,15 +516,22 @@ int gmres_dev(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int maxi
       y[i] /= h(i, i);
     }
     AEROF_CUDA(cudaMemcpyAsync(yd, y.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
-    k_combine<<<gv, kIB, 0, s>>>(n, j + 1, yd, Vb, n, w);
+    k_combine<TV><<<gv, kIB, 0, s>>>(n, j + 1, yd, Vb, n, w);
     AEROF_LAUNCH_CHECK();
-    prec_apply_dev(c, w, r, trans);
-    k_add<<<gv, kIB, 0, s>>>(n, r, x);
+    prec_apply_t<TV, TV>(c, w, r, trans);
+    k_add<TV><<<gv, kIB, 0, s>>>(n, r, x);
     AEROF_LAUNCH_CHECK();
   } while (exitLoop == 0);
   AEROF_CUDA(cudaStreamSynchronize(s));
   if (final_res) *final_res = l2res;
   return iter;
+}
+
+int gmres_dev(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int maxits, double eps, int trans,
+              double* final_res, const double* exactU) {
+  if (!exactU && c->imp.precision == AEROF_PREC_FP32)
+    return gmres_t<float>(c, b, x, numVec, maxits, eps, trans, final_res, nullptr);
+  return gmres_t<double>(c, b, x, numVec, maxits, eps, trans, final_res, exactU);
 }
 
 }  // namespace aerof
@@ -624,10 +690,10 @@ extern "C" int aerof_gpu_newton(aerof_gpu_ctx* c, double* U, const aerof_newton_
         c->last_error = std::to_string(nb) + " singular diagonal block(s) at Newton step " + std::to_string(k);
         return AEROF_ESINGULAR;
       }
-      k_scale<<<gv, kIB, 0, s>>>(n, -1.0, R, rhs);
+      k_scale<double, double><<<gv, kIB, 0, s>>>(n, -1.0, R, rhs);
       AEROF_LAUNCH_CHECK();
       lits += gmres_dev(c, rhs, dQ, p->ksp_krylov, p->ksp_maxits, p->ksp_eps, 0, nullptr, nullptr);
-      k_add<<<gv, kIB, 0, s>>>(n, dQ, dU);
+      k_add<double><<<gv, kIB, 0, s>>>(n, dQ, dU);
       AEROF_LAUNCH_CHECK();
     }
     AEROF_CUDA(cudaEventRecord(e1, s));

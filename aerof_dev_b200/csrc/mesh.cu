@@ -4,7 +4,9 @@
 // normals, least-squares factors), each accumulated per output item in the
 // reference's element/edge order so the sums are deterministic.
 #include <algorithm>
+#include <cstdlib>
 #include <numeric>
+#include <utility>
 
 #include "common.cuh"
 #include "physics.cuh"
@@ -172,6 +174,147 @@ static void build_host(int N, int T, int F, const int* tets, const int* faces, H
     for (int l = 0; l < 4; ++l) h.nt_tet[pos[tets[4 * (size_t)t + l]]++] = t * 4 + l;
 }
 
+// ------------------------------------------------------------------ blocked
+// Morton (Z-order) renumbering of the nodes and the per-block edge lists of
+// the blocked residual kernel.  Integer work only; deterministic.
+struct HostBlocked {
+  std::vector<int> n2o, o2n, nb2_ptr, nb2_node, bsrc, beptr, lptr, lidx, xslot, xin_ptr, xin_slot;
+  std::vector<int2> bedges;
+  int nblk = 0, maxE = 0, nX = 0;
+};
+
+static inline uint64_t spread3(uint64_t v) {
+  v &= 0x1fffff;
+  v = (v | v << 32) & 0x1f00000000ffffULL;
+  v = (v | v << 16) & 0x1f0000ff0000ffULL;
+  v = (v | v << 8) & 0x100f00f00f00f00fULL;
+  v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+  v = (v | v << 2) & 0x1249249249249249ULL;
+  return v;
+}
+
+static void build_blocked(int N, int E, int NB, const double* X, const std::vector<int>& edges, HostBlocked& b) {
+  double lo[3] = {X[0], X[1], X[2]}, hi[3] = {X[0], X[1], X[2]};
+  for (int i = 0; i < N; ++i)
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], X[3 * (size_t)i + k]);
+      hi[k] = std::max(hi[k], X[3 * (size_t)i + k]);
+    }
+  double ext = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
+  double sc = ext > 0 ? (double)((1 << 21) - 1) / ext : 0.0;
+  std::vector<std::pair<uint64_t, int>> key(N);
+  for (int i = 0; i < N; ++i) {
+    uint64_t q[3];
+    for (int k = 0; k < 3; ++k) q[k] = (uint64_t)((X[3 * (size_t)i + k] - lo[k]) * sc);
+    key[i] = {spread3(q[0]) | spread3(q[1]) << 1 | spread3(q[2]) << 2, i};
+  }
+  std::sort(key.begin(), key.end());
+  b.n2o.resize(N);
+  b.o2n.resize(N);
+  for (int n = 0; n < N; ++n) { b.n2o[n] = key[n].second; b.o2n[key[n].second] = n; }
+  // edges in the new numbering, oriented first < second, sorted
+  std::vector<std::pair<uint64_t, int>> ek(E);
+  for (int l = 0; l < E; ++l) {
+    uint32_t a = (uint32_t)b.o2n[edges[2 * (size_t)l]], c = (uint32_t)b.o2n[edges[2 * (size_t)l + 1]];
+    const bool rev = a > c;
+    if (rev) std::swap(a, c);
+    ek[l] = {((uint64_t)a << 32) | c, (int)((unsigned)l | (rev ? 0x80000000u : 0u))};
+  }
+  std::sort(ek.begin(), ek.end());
+  b.bedges.resize(E);
+  b.bsrc.resize(E);
+  for (int q = 0; q < E; ++q) {
+    b.bedges[q] = make_int2((int)(ek[q].first >> 32), (int)(ek[q].first & 0xffffffffu));
+    b.bsrc[q] = ek[q].second;
+  }
+  ek.clear();
+  ek.shrink_to_fit();
+  b.nblk = (N + NB - 1) / NB;
+  b.beptr.assign(b.nblk + 1, E);
+  {
+    int q = 0;
+    for (int blk = 0; blk < b.nblk; ++blk) {
+      while (q < E && b.bedges[q].x < blk * NB) ++q;
+      b.beptr[blk] = q;
+    }
+    b.beptr[b.nblk] = E;
+  }
+  b.maxE = 0;
+  for (int blk = 0; blk < b.nblk; ++blk) b.maxE = std::max(b.maxE, b.beptr[blk + 1] - b.beptr[blk]);
+  // neighbour CSR (ascending new ids), local assembly lists, spill slots
+  b.nb2_ptr.assign(N + 1, 0);
+  b.lptr.assign(N + 1, 0);
+  b.xin_ptr.assign(N + 1, 0);
+  b.xslot.assign(E, -1);
+  b.nX = 0;
+  for (int q = 0; q < E; ++q) {
+    const int f = b.bedges[q].x, sd = b.bedges[q].y;
+    b.nb2_ptr[f + 1]++; b.nb2_ptr[sd + 1]++;
+    b.lptr[f + 1]++;
+    if (sd / NB == f / NB) b.lptr[sd + 1]++;
+    else { b.xslot[q] = b.nX++; b.xin_ptr[sd + 1]++; }
+  }
+  for (int n = 0; n < N; ++n) {
+    b.nb2_ptr[n + 1] += b.nb2_ptr[n];
+    b.lptr[n + 1] += b.lptr[n];
+    b.xin_ptr[n + 1] += b.xin_ptr[n];
+  }
+  b.nb2_node.resize(2 * (size_t)E);
+  b.lidx.resize(b.lptr[N]);
+  b.xin_slot.resize(b.nX);
+  std::vector<int> pn(b.nb2_ptr.begin(), b.nb2_ptr.end() - 1), pl(b.lptr.begin(), b.lptr.end() - 1),
+      px(b.xin_ptr.begin(), b.xin_ptr.end() - 1);
+  for (int q = 0; q < E; ++q) {
+    const int f = b.bedges[q].x, sd = b.bedges[q].y;
+    const int blk = f / NB, slot = q - b.beptr[blk];
+    b.nb2_node[pn[f]++] = sd;
+    b.nb2_node[pn[sd]++] = f;
+    b.lidx[pl[f]++] = slot;
+    if (b.xslot[q] < 0) b.lidx[pl[sd]++] = (int)((unsigned)slot | 0x80000000u);
+    else b.xin_slot[px[sd]++] = b.xslot[q];
+  }
+}
+
+// blocked copies of the node geometry and oriented edge normals
+__global__ void k_blocked_nodes(int N, const int* __restrict__ n2o, const double* __restrict__ X,
+                                const double* __restrict__ W, const double* __restrict__ vol,
+                                double* __restrict__ P2, double* __restrict__ W2, double* __restrict__ vol2) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int o = n2o[n];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) P2[8 * (size_t)n + k] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) P2[8 * (size_t)n + 5 + k] = X[3 * (size_t)o + k];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) W2[(size_t)k * N + n] = W[(size_t)k * N + o];
+  vol2[n] = vol[o];
+}
+__global__ void k_blocked_normals(int E, const int* __restrict__ bsrc, const double* __restrict__ en,
+                                  double* __restrict__ bn) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= E) return;
+  const int src = bsrc[q];
+  const size_t l = (size_t)(src & 0x7fffffff);
+  const double sg = src < 0 ? -1.0 : 1.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) bn[(size_t)k * E + q] = sg * en[(size_t)k * E + l];
+}
+
+void compute_blocked_geometry(aerof_gpu_ctx* c) {
+  DeviceMesh& m = c->mesh;
+  cudaStream_t s = c->stream;
+  m.P2.alloc(8 * (size_t)m.N);
+  m.W2.alloc(6 * (size_t)m.N);
+  m.vol2.alloc(m.N);
+  m.bnorm.alloc(3 * (size_t)m.E);
+  k_blocked_nodes<<<grid_for(m.N, kMBlock), kMBlock, 0, s>>>(m.N, m.n2o.p, m.X.p, m.lsqW.p, m.vol.p, m.P2.p, m.W2.p,
+                                                              m.vol2.p);
+  AEROF_LAUNCH_CHECK();
+  k_blocked_normals<<<grid_for(m.E, kMBlock), kMBlock, 0, s>>>(m.E, m.bsrc.p, m.en.p, m.bnorm.p);
+  AEROF_LAUNCH_CHECK();
+}
+
 void compute_geometry(aerof_gpu_ctx* c) {
   DeviceMesh& m = c->mesh;
   cudaStream_t s = c->stream;
@@ -194,6 +337,7 @@ void compute_geometry(aerof_gpu_ctx* c) {
   AEROF_LAUNCH_CHECK();
   k_setX<<<grid_for(m.N, kMBlock), kMBlock, 0, s>>>(m.N, m.X.p, m.P.p);
   AEROF_LAUNCH_CHECK();
+  compute_blocked_geometry(c);
 }
 
 void geometry_dual(aerof_gpu_ctx* c, const Dual* XD, Dual* volD, Dual* enD, Dual* fnD, Dual* RD) {
@@ -264,6 +408,32 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
     m.et_tet.upload(h.et_tet.data(), h.et_tet.size(), s);
     m.nt_ptr.upload(h.nt_ptr.data(), h.nt_ptr.size(), s);
     m.nt_tet.upload(h.nt_tet.data(), h.nt_tet.size(), s);
+    {
+      // nodes per block of the blocked residual kernel (tuning knob; the
+      // shared-memory footprint is NB*192 B + owned edges * 40 B)
+      m.NB = 128;
+      if (const char* env = std::getenv("AEROF_BLOCK_NODES")) {
+        const int v = std::atoi(env);
+        if (v == 64 || v == 128 || v == 256) m.NB = v;
+      }
+      HostBlocked hb;
+      build_blocked(N, E, m.NB, X, h.edges, hb);
+      m.nblk = hb.nblk; m.maxE = hb.maxE; m.nX = hb.nX;
+      m.n2o.upload(hb.n2o.data(), N, s);
+      m.o2n.upload(hb.o2n.data(), N, s);
+      m.nb2_ptr.upload(hb.nb2_ptr.data(), N + 1, s);
+      m.nb2_node.upload(hb.nb2_node.data(), hb.nb2_node.size(), s);
+      m.bedges.upload(hb.bedges.data(), (size_t)E, s);
+      m.bsrc.upload(hb.bsrc.data(), (size_t)E, s);
+      m.beptr.upload(hb.beptr.data(), hb.beptr.size(), s);
+      m.lptr.upload(hb.lptr.data(), N + 1, s);
+      m.lidx.upload(hb.lidx.data(), std::max<size_t>(hb.lidx.size(), 1), s);
+      m.xslot.upload(hb.xslot.data(), (size_t)E, s);
+      m.xin_ptr.upload(hb.xin_ptr.data(), N + 1, s);
+      if (hb.nX) m.xin_slot.upload(hb.xin_slot.data(), hb.xin_slot.size(), s);
+      else m.xin_slot.alloc(1);
+      AEROF_CUDA(cudaStreamSynchronize(s));  // host vectors die at scope end
+    }
     m.h_edges.swap(h.edges);
     compute_geometry(c);
     c->dual.geom_static = false;

@@ -38,6 +38,42 @@ template <class T> AEROF_HD T tmax0(T a) { return vof(a) < 0.0 ? T(0.0) : a; }
 template <class T> AEROF_HD T tmin0(T a) { return vof(a) > 0.0 ? T(0.0) : a; }
 template <class T> AEROF_HD T tabs(T a) { return vof(a) < 0.0 ? -a : a; }
 
+// ------------------------------------------------------------ fast reciprocals
+// Reciprocal and reciprocal square root for the primal double kernels: the
+// hardware approximation (PTX rcp.approx.ftz.f64 / rsqrt.approx.ftz.f64,
+// about 23 correct bits) refined by Newton-Raphson iteration: for 1/x the
+// third-order step r <- r + r (e + e^2), e = 1 - x r (one step takes 23
+// correct bits past double precision); for 1/sqrt x two second-order steps
+// y <- y + y/2 (1 - x y^2).  Results are within a few ulp of the correctly
+// rounded value.  Inputs are positive normal numbers (densities,
+// pressures, squared norms, positive denominators).  The dual-number
+// instantiation keeps exact division and square root.
+AEROF_HD double rcp_(double x) {
+#ifdef __CUDA_ARCH__
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  const double e = fma(-x, r, 1.0);
+  return fma(r, fma(e, e, e), r);
+#else
+  return 1.0 / x;
+#endif
+}
+AEROF_HD double rsqrt_(double x) {
+#ifdef __CUDA_ARCH__
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x * y, y, 1.0);
+  y = fma(0.5 * y, e, y);
+  e = fma(-x * y, y, 1.0);
+  return fma(0.5 * y, e, y);
+#else
+  return 1.0 / sqrt(x);
+#endif
+}
+AEROF_HD Dual rcp_(Dual x) { return 1.0 / x; }
+AEROF_HD Dual rsqrt_(Dual x) { return 1.0 / dsqrt(x); }
+template <class T> AEROF_HD T sel(bool c, T a, T b) { return c ? a : b; }
+
 // ------------------------------------------------------------ gas model
 struct Gas {
   double gam, gam1, invgam1;
@@ -89,16 +125,19 @@ AEROF_HD void lsq_weights(const T* w, T dx0, T dx1, T dx2, T& W0, T& W1, T& W2) 
 }
 
 // ------------------------------------------------------------ reconstruction
-// RecFcn::computeVanAlbadaFcn (RecFcn.h:268-281)
+// RecFcn::computeVanAlbadaFcn (RecFcn.h:268-281).  For a*b > 0 the
+// numerator a(b^2+eps) + b(a^2+eps) equals (a+b)(ab+eps); for a*b == 0 the
+// reference's 0.5 eps (a+b) is the same expression with ab+eps replaced by
+// eps/2; otherwise the result is 0.  One reciprocal of the denominator,
+// branch-free selection.
 template <class T>
 AEROF_HD T vanalbada_fcn(T a, T b) {
   const double eps = 1.e-16;
-  T a2 = a * a;
-  T b2 = b * b;
-  double ab = vof(a * b);
-  if (ab > 0.0) return (a * (b2 + eps) + b * (a2 + eps)) / (a2 + b2 + 2.0 * eps);
-  if (ab == 0.0) return 0.5 * eps * (a + b) / (a2 + b2 + 2.0 * eps);
-  return T(0.0);
+  T ab = a * b;
+  const double abv = vof(ab);
+  T den = a * a + (b * b + 2.0 * eps);
+  T t = sel(abv > 0.0, ab + eps, sel(abv == 0.0, T(0.5 * eps), T(0.0)));
+  return (a + b) * t * rcp_(den);
 }
 // RecFcn::vanalbada (RecFcn.h:432-446); beta2 = 1-2 beta
 template <class T>
@@ -125,66 +164,63 @@ AEROF_HD void linear_rec(double beta, T Vi, T ddVij, T Vj, T ddVji, T& Vij, T& V
 // upwind selection of the physical flux plus the one-wave dissipation term.
 template <class T>
 AEROF_HD void roe_flux(const Gas& g, T n0, T n1, T n2, const T* Ug, const T* Ud, T* phi) {
-  const double gam = g.gam, gam1 = g.gam1, invgam1 = g.invgam1;
-  T rnorm = dsqrt(n0 * n0 + n1 * n1 + n2 * n2);
-  T invnorm = 1.0 / rnorm;
+  const double gam1 = g.gam1, invgam1 = g.invgam1, gog1 = g.gam * g.invgam1;
+  T s2 = n0 * n0 + n1 * n1 + n2 * n2;
+  T invnorm = rsqrt_(s2);
+  T rnorm = s2 * invnorm;
   T nx = n0 * invnorm, ny = n1 * invnorm, nz = n2 * invnorm;
   T vitg2 = Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3];
   T vitd2 = Ud[1] * Ud[1] + Ud[2] * Ud[2] + Ud[3] * Ud[3];
-  T squsr1 = dsqrt(Ug[0]);
-  T squsr2 = dsqrt(Ud[0]);
+  // sqrt(rho) and 1/sqrt(rho) of both sides
+  T rs1 = rsqrt_(Ug[0]), rs2 = rsqrt_(Ud[0]);
+  T squsr1 = Ug[0] * rs1;
+  T squsr2 = Ud[0] * rs2;
   T ener1 = Ug[4] * invgam1 + 0.5 * Ug[0] * vitg2;
   T ener2 = Ud[4] * invgam1 + 0.5 * Ud[0] * vitd2;
-  T usro = 1.0 / (squsr1 + squsr2);
+  T usro = rcp_(squsr1 + squsr2);
   T uar2 = (squsr1 * Ug[1] + squsr2 * Ud[1]) * usro;
   T uar3 = (squsr1 * Ug[2] + squsr2 * Ud[2]) * usro;
   T uar4 = (squsr1 * Ug[3] + squsr2 * Ud[3]) * usro;
-  T uar5 = ((ener1 + Ug[4]) / squsr1 + (ener2 + Ud[4]) / squsr2) * usro;
+  T uar5 = ((ener1 + Ug[4]) * rs1 + (ener2 + Ud[4]) * rs2) * usro;
   T VdotN = nx * uar2 + ny * uar3 + nz * uar4;
   const bool left = vof(VdotN) > 0.0;
-  // centred (upwind-side physical) flux
-  const T* Us = left ? Ug : Ud;
-  T vits2 = left ? vitg2 : vitd2;
-  T vn = Us[1] * nx + Us[2] * ny + Us[3] * nz;
-  T H = gam * Us[4] + 0.5 * gam1 * Us[0] * vits2;
-  H = H / (gam1 * Us[0]);
-  T f0 = Us[0] * vn;
-  T f1 = f0 * Us[1] + Us[4] * nx;
-  T f2 = f0 * Us[2] + Us[4] * ny;
-  T f3 = f0 * Us[3] + Us[4] * nz;
+  // centred flux of the upwind side (roeflux7.f:79-98):
+  // H = (gam p + 0.5 gam1 rho |u|^2) / (gam1 rho) = gam/gam1 p/rho + |u|^2/2
+  T Us0 = sel(left, Ug[0], Ud[0]), Us1 = sel(left, Ug[1], Ud[1]), Us2 = sel(left, Ug[2], Ud[2]);
+  T Us3 = sel(left, Ug[3], Ud[3]), Us4 = sel(left, Ug[4], Ud[4]);
+  T rss = sel(left, rs1, rs2);
+  T vits2 = sel(left, vitg2, vitd2);
+  T vn = Us1 * nx + Us2 * ny + Us3 * nz;
+  T H = gog1 * Us4 * (rss * rss) + 0.5 * vits2;
+  T f0 = Us0 * vn;
+  T f1 = f0 * Us1 + Us4 * nx;
+  T f2 = f0 * Us2 + Us4 * ny;
+  T f3 = f0 * Us3 + Us4 * nz;
   T f4 = f0 * H;
-  // dissipation
+  // one-wave dissipation (roeflux7.f:107-181) with cr2byt = -cr,
+  // invtbeta2 = -1/cr: flur4 = max(VdotN+cr,0) (-cr A + gam1 B) when the
+  // right side is upwind, flur5 = max(cr-VdotN,0) (cr A + gam1 B) otherwise.
   T qir = 0.5 * (uar2 * uar2 + uar3 * uar3 + uar4 * uar4);
-  T cr2 = gam1 * (uar5 - qir);
-  T cr = dsqrt(cr2);
-  cr2 = 1.0 / cr2;
+  T c2 = gam1 * (uar5 - qir);
+  T rc = rsqrt_(c2);
+  T cr = c2 * rc;
+  T cr2 = rc * rc;
   T dif1 = Ud[0] - Ug[0];
-  T dif2 = -Ug[0] * Ug[1] + Ud[0] * Ud[1];
-  T dif3 = -Ug[0] * Ug[2] + Ud[0] * Ud[2];
-  T dif4 = -Ug[0] * Ug[3] + Ud[0] * Ud[3];
+  T dif2 = Ud[0] * Ud[1] - Ug[0] * Ug[1];
+  T dif3 = Ud[0] * Ud[2] - Ug[0] * Ug[2];
+  T dif4 = Ud[0] * Ud[3] - Ug[0] * Ug[3];
   T dif5 = ener2 - ener1;
-  T invtbeta2 = -1.0 / cr;
   T A = VdotN * dif1 - nx * dif2 - ny * dif3 - nz * dif4;
   T B = qir * dif1 - uar2 * dif2 - uar3 * dif3 - uar4 * dif4 + dif5;
-  // flur4 (left==false) or flur5 (left==true); the other is zero.
-  T fl, rs;
-  if (!left) {
-    fl = tmax0(VdotN + cr) * ((-cr) * A + gam1 * (-cr) * invtbeta2 * B);
-    rs = cr * fl;  // r * flur4
-  } else {
-    fl = -tmin0(VdotN - cr) * (cr * A + (-gam1 * cr * invtbeta2 * B));
-    rs = (-cr) * fl;  // s * flur5
-  }
-  phi[0] = f0 - 0.5 * fl * cr2;
-  phi[1] = f1 - (nx * rs + uar2 * fl) * 0.5 * cr2;
-  phi[2] = f2 - (ny * rs + uar3 * fl) * 0.5 * cr2;
-  phi[3] = f3 - (nz * rs + uar4 * fl) * 0.5 * cr2;
-  phi[4] = f4 - (VdotN * rs + uar5 * fl) * 0.5 * cr2;
-  phi[0] = phi[0] * rnorm;
-  phi[1] = phi[1] * rnorm;
-  phi[2] = phi[2] * rnorm;
-  phi[3] = phi[3] * rnorm;
-  phi[4] = phi[4] * rnorm;
+  T scr = sel(left, cr, -cr);
+  T fl = tmax0(cr - (left ? VdotN : -VdotN)) * (scr * A + gam1 * B);
+  T rs = -scr * fl;
+  T hc = 0.5 * cr2;
+  phi[0] = (f0 - hc * fl) * rnorm;
+  phi[1] = (f1 - (nx * rs + uar2 * fl) * hc) * rnorm;
+  phi[2] = (f2 - (ny * rs + uar3 * fl) * hc) * rnorm;
+  phi[3] = (f3 - (nz * rs + uar4 * fl) * hc) * rnorm;
+  phi[4] = (f4 - (VdotN * rs + uar5 * fl) * hc) * rnorm;
 }
 
 // boundflux5.f:1-111 (type 0, sig = 0): Steger-Warming far-field flux

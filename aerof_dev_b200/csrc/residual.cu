@@ -38,65 +38,83 @@ __global__ void k_setV(int N, const double* __restrict__ V, double* __restrict__
 }
 
 // Least-squares gradients, one thread per node gathering its neighbours in
-// ascending order: ddV_i = sum_j W_i(X_j - X_i) (V_j - V_i).
-__global__ void k_grad(int N, const double* __restrict__ P, const double* __restrict__ lsqW,
-                       const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_node,
-                       const int* __restrict__ tag, double* __restrict__ G) {
+// ascending order: ddV_i = sum_j W_i(X_j - X_i) (V_j - V_i).  Two neighbour
+// records (64 B each, four 16 B loads) are fetched before either is used.
+__device__ __forceinline__ void load_rec(const double* __restrict__ P, int j, double* r) {
+  const double2* q = reinterpret_cast<const double2*>(P + 8 * (size_t)j);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    double2 v = __ldg(q + k);
+    r[2 * k] = v.x;
+    r[2 * k + 1] = v.y;
+  }
+}
+__device__ __forceinline__ void grad_acc(const double* w, const double* vi, const double* xi, const double* pj,
+                                         double* gx, double* gy, double* gz) {
+  double W0, W1, W2;
+  lsq_weights(w, pj[5] - xi[0], pj[6] - xi[1], pj[7] - xi[2], W0, W1, W2);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    double dv = pj[k] - vi[k];
+    gx[k] += W0 * dv;
+    gy[k] += W1 * dv;
+    gz[k] += W2 * dv;
+  }
+}
+__global__ void k_grad(int N, const double* __restrict__ P, const double* __restrict__ lsqW, const int* __restrict__ nbr_ptr,
+       const int* __restrict__ nbr_node, const int* __restrict__ tag, double* __restrict__ G) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double w[6];
 #pragma unroll
   for (int k = 0; k < 6; ++k) w[k] = lsqW[(size_t)k * N + i];
-  const double* pi = P + 8 * (size_t)i;
-  double vi[5], xi[3];
-#pragma unroll
-  for (int k = 0; k < 5; ++k) vi[k] = pi[k];
-  xi[0] = pi[5]; xi[1] = pi[6]; xi[2] = pi[7];
+  double pi[8];
+  load_rec(P, i, pi);
   double gx[5] = {0, 0, 0, 0, 0}, gy[5] = {0, 0, 0, 0, 0}, gz[5] = {0, 0, 0, 0, 0};
+  int p = nbr_ptr[i];
   const int p1 = nbr_ptr[i + 1];
-  for (int p = nbr_ptr[i]; p < p1; ++p) {
-    const double* pj = P + 8 * (size_t)nbr_node[p];
-    double W0, W1, W2;
-    lsq_weights(w, pj[5] - xi[0], pj[6] - xi[1], pj[7] - xi[2], W0, W1, W2);
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      double dv = pj[k] - vi[k];
-      gx[k] += W0 * dv;
-      gy[k] += W1 * dv;
-      gz[k] += W2 * dv;
-    }
+  for (; p + 1 < p1; p += 2) {
+    double pa[8], pb[8];
+    const int ja = nbr_node[p], jb = nbr_node[p + 1];
+    load_rec(P, ja, pa);
+    load_rec(P, jb, pb);
+    grad_acc(w, pi, pi + 5, pa, gx, gy, gz);
+    grad_acc(w, pi, pi + 5, pb, gx, gy, gz);
+  }
+  if (p < p1) {
+    double pa[8];
+    load_rec(P, nbr_node[p], pa);
+    grad_acc(w, pi, pi + 5, pa, gx, gy, gz);
   }
   const bool zero = tag && tag[i];
-  double* gi = G + 16 * (size_t)i;
+  double2* gi = reinterpret_cast<double2*>(G + 16 * (size_t)i);
+  double o[16];
 #pragma unroll
   for (int k = 0; k < 5; ++k) {
-    gi[k] = zero ? 0.0 : gx[k];
-    gi[5 + k] = zero ? 0.0 : gy[k];
-    gi[10 + k] = zero ? 0.0 : gz[k];
+    o[k] = zero ? 0.0 : gx[k];
+    o[5 + k] = zero ? 0.0 : gy[k];
+    o[10 + k] = zero ? 0.0 : gz[k];
   }
+  o[15] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) gi[k] = make_double2(o[2 * k], o[2 * k + 1]);
 }
 
-// Roe flux of every edge into flux[5][E].  Non-positive reconstructed
-// density/pressure (VarFcnSGEuler::checkReconstructedValues,
-// VarFcnSGEuler.h:90-110) skips the edge, counts into counters[0] and, with
-// failsafe, tags the offending node (EdgeCore.C:137-168).
-__global__ void k_edge_flux(int E, Gas g, int rec, double beta, int failsafe, const int2* __restrict__ edges,
-                            const double* __restrict__ en, const double* __restrict__ P,
-                            const double* __restrict__ G, double* __restrict__ flux, int* __restrict__ tag,
-                            int* __restrict__ counters) {
-  int l = blockIdx.x * blockDim.x + threadIdx.x;
-  if (l >= E) return;
-  const int2 ij = edges[l];
-  const double* pi = P + 8 * (size_t)ij.x;
-  const double* pj = P + 8 * (size_t)ij.y;
+// Flux of one edge (i = first, j = second endpoint): reconstruction from the
+// node records and gradients, positivity check (VarFcnSGEuler::
+// checkReconstructedValues, VarFcnSGEuler.h:90-110; on failure the edge is
+// skipped as in Edge.C:414-421, counted, and with failsafe the offending
+// node tagged, EdgeCore.C:137-168), then the Roe flux.
+__device__ __forceinline__ void edge_flux_rec(const Gas& g, int rec, double beta, int failsafe, int i, int j,
+                                              double n0, double n1, double n2, const double* pi, const double* gi,
+                                              const double* pj, const double* gj, int* __restrict__ tag,
+                                              int* __restrict__ counter, double* f) {
   double Vi[5], Vj[5];
   if (rec == AEROF_REC_CONSTANT) {
 #pragma unroll
     for (int k = 0; k < 5; ++k) { Vi[k] = pi[k]; Vj[k] = pj[k]; }
   } else {
     const double dx0 = pj[5] - pi[5], dx1 = pj[6] - pi[6], dx2 = pj[7] - pi[7];
-    const double* gi = G + 16 * (size_t)ij.x;
-    const double* gj = G + 16 * (size_t)ij.y;
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
       double ddVij = dx0 * gi[k] + dx1 * gi[5 + k] + dx2 * gi[10 + k];
@@ -107,31 +125,197 @@ __global__ void k_edge_flux(int E, Gas g, int rec, double beta, int failsafe, co
   }
   const bool bi = Vi[0] <= 0.0 || Vi[4] <= 0.0;
   const bool bj = Vj[0] <= 0.0 || Vj[4] <= 0.0;
-  double f[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+  for (int k = 0; k < 5; ++k) f[k] = 0.0;
   if (bi || bj) {
-    atomicAdd(&counters[0], (int)bi + (int)bj);
+    atomicAdd(counter, (int)bi + (int)bj);
     if (failsafe) {
-      if (bi) tag[ij.x] = 1;
-      if (bj) tag[ij.y] = 1;
+      if (bi) tag[i] = 1;
+      if (bj) tag[j] = 1;
     }
-  } else {
-    const double n0 = en[l], n1 = en[(size_t)E + l], n2 = en[2 * (size_t)E + l];
-    if (sqrt(n0 * n0 + n1 * n1 + n2 * n2) >= 1e-18) roe_flux(g, n0, n1, n2, Vi, Vj, f);
+  } else if (n0 * n0 + n1 * n1 + n2 * n2 >= 1e-36) {
+    roe_flux(g, n0, n1, n2, Vi, Vj, f);
   }
+}
+__device__ __forceinline__ void edge_flux_eval(const Gas& g, int rec, double beta, int failsafe, int i, int j,
+                                               double n0, double n1, double n2, const double* __restrict__ P,
+                                               const double* __restrict__ G, int* __restrict__ tag,
+                                               int* __restrict__ counter, double* f) {
+  edge_flux_rec(g, rec, beta, failsafe, i, j, n0, n1, n2, P + 8 * (size_t)i, G + 16 * (size_t)i, P + 8 * (size_t)j,
+                G + 16 * (size_t)j, tag, counter, f);
+}
+
+// Roe flux of every edge into flux[5][E] (EDGE organisation).
+__global__ void k_edge_flux(int E, Gas g, int rec, double beta, int failsafe, const int2* __restrict__ edges,
+                            const double* __restrict__ en, const double* __restrict__ P,
+                            const double* __restrict__ G, double* __restrict__ flux, int* __restrict__ tag,
+                            int* __restrict__ counters) {
+  int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= E) return;
+  const int2 ij = edges[l];
+  double f[5];
+  edge_flux_eval(g, rec, beta, failsafe, ij.x, ij.y, en[l], en[(size_t)E + l], en[2 * (size_t)E + l], P, G, tag,
+                 counters, f);
 #pragma unroll
   for (int k = 0; k < 5; ++k) flux[(size_t)k * E + l] = f[k];
 }
 
+// BLOCKED organisation: one thread block per NB consecutive (Morton
+// ordered) nodes.  Phase 0: the block's node records (V, X) and gradients
+// are copied to shared memory.  Phase 1: the block's threads evaluate the
+// fluxes of the edges whose first endpoint is in the block (endpoint data
+// from shared memory when the node is in the block, from global memory
+// otherwise) into shared memory; fluxes of edges whose second endpoint lies
+// in a later block also go to spill[].  Phase 2: thread t sums, for node
+// blk*NB+t, its edges held in shared memory in ascending edge order (+ as
+// first endpoint, - as second) into part[].
+__global__ void __launch_bounds__(256) k_fv_blocked(int N, int E, int NB, Gas g, int rec, double beta, int failsafe,
+                                                    const int2* __restrict__ bedges, const double* __restrict__ bn,
+                                                    const int* __restrict__ beptr, const double* __restrict__ P,
+                                                    const double* __restrict__ G, const int* __restrict__ lptr,
+                                                    const int* __restrict__ lidx, const int* __restrict__ xslot,
+                                                    double* __restrict__ part, double* __restrict__ spill,
+                                                    int* __restrict__ tag, int* __restrict__ counters) {
+  extern __shared__ double sm[];
+  double* Pn = sm;                 // [NB][8]
+  double* Gn = sm + 8 * NB;        // [NB][16]
+  double* Fs = sm + 24 * NB;       // [owned edges][5]
+  const int blk = blockIdx.x;
+  const int n0 = blk * NB;
+  const int nn = min(NB, N - n0);
+  {
+    const double2* ps = reinterpret_cast<const double2*>(P + 8 * (size_t)n0);
+    const double2* gs = reinterpret_cast<const double2*>(G + 16 * (size_t)n0);
+    double2* pd = reinterpret_cast<double2*>(Pn);
+    double2* gd = reinterpret_cast<double2*>(Gn);
+    for (int k = threadIdx.x; k < 4 * nn; k += blockDim.x) pd[k] = ps[k];
+    if (rec != AEROF_REC_CONSTANT)
+      for (int k = threadIdx.x; k < 8 * nn; k += blockDim.x) gd[k] = gs[k];
+  }
+  __syncthreads();
+  const int e0 = beptr[blk], e1 = beptr[blk + 1];
+  for (int q = e0 + threadIdx.x; q < e1; q += blockDim.x) {
+    const int2 ij = bedges[q];
+    const int li = ij.x - n0, lj = ij.y - n0;
+    const double* pi = Pn + 8 * li;
+    const double* gi = Gn + 16 * li;
+    const bool jin = lj < nn;
+    const double* pj = jin ? Pn + 8 * lj : P + 8 * (size_t)ij.y;
+    const double* gj = jin ? Gn + 16 * lj : G + 16 * (size_t)ij.y;
+    double f[5];
+    edge_flux_rec(g, rec, beta, failsafe, ij.x, ij.y, bn[q], bn[(size_t)E + q], bn[2 * (size_t)E + q], pi, gi, pj,
+                  gj, tag, counters, f);
+    double* fs = Fs + 5 * (q - e0);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) fs[k] = f[k];
+    const int xs = xslot[q];
+    if (xs >= 0) {
+#pragma unroll
+      for (int k = 0; k < 5; ++k) spill[5 * (size_t)xs + k] = f[k];
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nn; t += blockDim.x) {
+    const int n = n0 + t;
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int k = lptr[n]; k < lptr[n + 1]; ++k) {
+      const int e = lidx[k];
+      const double* fs = Fs + 5 * (e & 0x7fffffff);
+      const double sg = e < 0 ? -1.0 : 1.0;
+#pragma unroll
+      for (int c = 0; c < 5; ++c) acc[c] += sg * fs[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 5; ++c) part[5 * (size_t)n + c] = acc[c];
+  }
+}
+
+// BLOCKED organisation, per node (new numbering): block-local sum, minus the
+// spilled fluxes of incoming block-crossing edges, plus the boundary faces
+// of the node (face order), times 1/ctrlVol; written to R in the caller's
+// numbering.
+__global__ void k_fv_nodes(int N, const int* __restrict__ n2o, const double* __restrict__ part,
+                           const int* __restrict__ xin_ptr, const int* __restrict__ xin_slot,
+                           const double* __restrict__ spill, const int* __restrict__ nf_ptr,
+                           const int* __restrict__ nf_face, const int* __restrict__ faces,
+                           const double* __restrict__ fbuf, const double* __restrict__ vol2, double* __restrict__ R) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double acc[5];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) acc[c] = part[5 * (size_t)n + c];
+  for (int k = xin_ptr[n]; k < xin_ptr[n + 1]; ++k) {
+    const double* sp = spill + 5 * (size_t)xin_slot[k];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) acc[c] -= sp[c];
+  }
+  const int o = n2o[n];
+  for (int q = nf_ptr[o]; q < nf_ptr[o + 1]; ++q) {
+    const int f = nf_face[q];
+    const int* fd = faces + 3 * (size_t)f;
+    const int l = fd[0] == o ? 0 : (fd[1] == o ? 1 : 2);
+    const double* ff = fbuf + 5 * (3 * (size_t)f + l);
+#pragma unroll
+    for (int c = 0; c < 5; ++c) acc[c] += ff[c];
+  }
+  const double invcv = 1.0 / vol2[n];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) R[5 * (size_t)o + c] = acc[c] * invcv;
+}
+
+// U[N][5] (caller numbering) -> blocked node records P2[n].V
+__global__ void k_prim_blocked(int N, Gas g, const int* __restrict__ n2o, const double* __restrict__ U,
+                               double* __restrict__ P2) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int o = n2o[n];
+  double u[5], v[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) u[k] = U[5 * (size_t)o + k];
+  cons2prim(g, u, v);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) P2[8 * (size_t)n + k] = v[k];
+}
+
+// Boundary fluxes, one thread per face, the three subface fluxes with
+// normal n_f/3 (FaceTriaCore.C:288-308) into fbuf[3F][5].
+__global__ void k_face_flux(int F, Gas g, const double* __restrict__ Ub0, const int* __restrict__ faces,
+                            const int* __restrict__ fcode, const double* __restrict__ fn,
+                            const double* __restrict__ P, const int* __restrict__ o2n, double* __restrict__ fbuf) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= F) return;
+  const double third = 1.0 / 3.0;
+  double Ub[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) Ub[k] = Ub0[k];
+  const double nx = third * fn[f], ny = third * fn[(size_t)F + f], nz = third * fn[2 * (size_t)F + f];
+  const int code = fcode[f];
+  for (int l = 0; l < 3; ++l) {
+    const int nd0 = faces[3 * (size_t)f + l];
+    const int nd = o2n ? o2n[nd0] : nd0;
+    double V[5], ff[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) V[k] = P[8 * (size_t)nd + k];
+    face_flux(g, code, nx, ny, nz, V, Ub, ff);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) fbuf[5 * (3 * (size_t)f + l) + k] = ff[k];
+  }
+}
+
 // Per-node assembly: edges in ascending-neighbour order (+flux when the node
-// is the edge's first endpoint, -flux otherwise), then boundary faces with
-// subface normals n_f/3 (FaceTriaCore.C:288-308), then R *= 1/ctrlVol
-// (SpaceOperator.C:614-620).  R is written in the caller's [N][5] layout.
-__global__ void k_node_residual(int N, int E, Gas g, const double* __restrict__ Ub0,
-                                const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_edge,
-                                const double* __restrict__ flux, const int* __restrict__ nf_ptr,
-                                const int* __restrict__ nf_face, const int* __restrict__ fcode,
-                                const double* __restrict__ fn, int F, const double* __restrict__ P,
-                                const double* __restrict__ vol, double* __restrict__ R) {
+// is the edge's first endpoint, -flux otherwise), then boundary faces in
+// face order (Face.C:1185-1215), then R *= 1/ctrlVol (SpaceOperator.C:
+// 614-620).  R is written in the caller's [N][5] layout.  FACEBUF: the face
+// fluxes come precomputed from k_face_flux; otherwise they are evaluated
+// here.
+template <bool FACEBUF>
+__global__ void k_node_residual_t(int N, int E, Gas g, const double* __restrict__ Ub0,
+                                  const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_edge,
+                                  const double* __restrict__ flux, const int* __restrict__ nf_ptr,
+                                  const int* __restrict__ nf_face, const int* __restrict__ fcode,
+                                  const double* __restrict__ fn, int F, const int* __restrict__ faces,
+                                  const double* __restrict__ fbuf, const double* __restrict__ P,
+                                  const double* __restrict__ vol, double* __restrict__ R) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double acc[5] = {0, 0, 0, 0, 0};
@@ -139,16 +323,21 @@ __global__ void k_node_residual(int N, int E, Gas g, const double* __restrict__ 
   for (int p = nbr_ptr[i]; p < p1; ++p) {
     const int e = nbr_edge[p];
     const size_t l = (size_t)(e & 0x7fffffff);
-    if (e < 0) {
+    const double sg = e < 0 ? -1.0 : 1.0;
 #pragma unroll
-      for (int k = 0; k < 5; ++k) acc[k] -= flux[k * (size_t)E + l];
-    } else {
-#pragma unroll
-      for (int k = 0; k < 5; ++k) acc[k] += flux[k * (size_t)E + l];
-    }
+    for (int k = 0; k < 5; ++k) acc[k] += sg * flux[k * (size_t)E + l];
   }
   const int q1 = nf_ptr[i + 1];
-  if (nf_ptr[i] < q1) {
+  if (FACEBUF) {
+    for (int q = nf_ptr[i]; q < q1; ++q) {
+      const int f = nf_face[q];
+      const int* fd = faces + 3 * (size_t)f;
+      const int l = fd[0] == i ? 0 : (fd[1] == i ? 1 : 2);
+      const double* ff = fbuf + 5 * (3 * (size_t)f + l);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) acc[k] += ff[k];
+    }
+  } else if (nf_ptr[i] < q1) {
     double V[5], Ub[5];
 #pragma unroll
     for (int k = 0; k < 5; ++k) { V[k] = P[8 * (size_t)i + k]; Ub[k] = Ub0[k]; }
@@ -288,8 +477,76 @@ static int* counters(aerof_gpu_ctx* c) {
 // Residual of device state dU into device dR (both [N][5]).  Returns the
 // number of non-positive reconstructed states of the first pass (sync), or
 // 0 with the count accumulated in counters[2] (no sync, failsafe off).
+// BLOCKED organisation of residual_dev (see k_fv_blocked).
+static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
+  DeviceMesh& m = c->mesh;
+  const Gas g = make_gas(c->cfg.gamma);
+  const int rec = c->cfg.reconstruction;
+  cudaStream_t s = c->stream;
+  int* cnt = counters(c);
+  if (sync) AEROF_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * 2, s));
+  int* ecnt = sync ? cnt : cnt + 2;
+  c->s.G2.ensure(16 * (size_t)m.N);
+  c->s.part.ensure(5 * (size_t)m.N);
+  c->s.spill.ensure(5 * (size_t)std::max(m.nX, 1));
+  c->s.fbuf.ensure(15 * (size_t)std::max(m.F, 1));
+  if (c->cfg.failsafe) {
+    c->s.tag.ensure(m.N);
+    c->s.tag.zero(s);
+  }
+  const size_t smem = ((size_t)24 * m.NB + (size_t)m.maxE * 5) * sizeof(double);
+  AEROF_CUDA(cudaFuncSetAttribute(k_fv_blocked, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  {
+    TimerScope t(c, AEROF_T_NODAL_GRAD);
+    k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
+    AEROF_LAUNCH_CHECK();
+    if (rec != AEROF_REC_CONSTANT) {
+      k_grad<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.P2.p, m.W2.p, m.nb2_ptr.p, m.nb2_node.p, nullptr,
+                                                      c->s.G2.p);
+      AEROF_LAUNCH_CHECK();
+    }
+  }
+  auto fv = [&](int fs, int* counter) {
+    k_fv_blocked<<<m.nblk, 256, smem, s>>>(m.N, m.E, m.NB, g, rec, c->cfg.beta, fs, m.bedges.p, m.bnorm.p,
+                                            m.beptr.p, m.P2.p, c->s.G2.p, m.lptr.p, m.lidx.p, m.xslot.p,
+                                            c->s.part.p, c->s.spill.p, c->s.tag.p, counter);
+    AEROF_LAUNCH_CHECK();
+  };
+  {
+    TimerScope t(c, AEROF_T_FV_TERM);
+    fv(c->cfg.failsafe, ecnt);
+  }
+  int bad = 0;
+  if (sync) {
+    AEROF_CUDA(cudaMemcpyAsync(&bad, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
+    AEROF_CUDA(cudaStreamSynchronize(s));
+  }
+  if (bad && c->cfg.failsafe && rec != AEROF_REC_CONSTANT) {
+    TimerScope t(c, AEROF_T_FV_TERM);
+    k_grad<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.P2.p, m.W2.p, m.nb2_ptr.p, m.nb2_node.p, c->s.tag.p,
+                                                    c->s.G2.p);
+    AEROF_LAUNCH_CHECK();
+    fv(0, cnt + 1);
+  }
+  {
+    TimerScope t(c, AEROF_T_FV_TERM);
+    if (m.F) {
+      k_face_flux<<<grid_for(m.F, kBlock), kBlock, 0, s>>>(m.F, g, m.Ubd.p, m.faces.p, m.fcode.p, m.fnrm.p, m.P2.p,
+                                                           m.o2n.p, c->s.fbuf.p);
+      AEROF_LAUNCH_CHECK();
+    }
+    k_fv_nodes<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.n2o.p, c->s.part.p, m.xin_ptr.p, m.xin_slot.p,
+                                                        c->s.spill.p, m.nf_ptr.p, m.nf_face.p, m.faces.p, c->s.fbuf.p,
+                                                        m.vol2.p, dR);
+    AEROF_LAUNCH_CHECK();
+  }
+  return bad;
+}
+
 int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
   DeviceMesh& m = c->mesh;
+  if (c->cfg.residual_kernel == AEROF_KERNEL_BLOCKED && ((size_t)24 * m.NB + (size_t)m.maxE * 5) * 8 <= 200 * 1024)
+    return residual_blocked_dev(c, dU, dR, sync);
   const Gas g = make_gas(c->cfg.gamma);
   const int rec = c->cfg.reconstruction;
   int* cnt = counters(c);
@@ -330,9 +587,15 @@ int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
   }
   {
     TimerScope t(c, AEROF_T_FV_TERM);
-    k_node_residual<<<grid_for(m.N, kBlock), kBlock, 0, c->stream>>>(
-        m.N, m.E, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_edge.p,
-        c->s.flux.p, m.nf_ptr.p, m.nf_face.p, m.fcode.p, m.fnrm.p, m.F, m.P.p, m.vol.p, dR);
+    c->s.fbuf.ensure(15 * (size_t)std::max(m.F, 1));
+    if (m.F) {
+      k_face_flux<<<grid_for(m.F, kBlock), kBlock, 0, c->stream>>>(m.F, g, m.Ubd.p, m.faces.p, m.fcode.p, m.fnrm.p,
+                                                                   m.P.p, nullptr, c->s.fbuf.p);
+      AEROF_LAUNCH_CHECK();
+    }
+    k_node_residual_t<true><<<grid_for(m.N, kBlock), kBlock, 0, c->stream>>>(
+        m.N, m.E, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_edge.p, c->s.flux.p, m.nf_ptr.p, m.nf_face.p, m.fcode.p, m.fnrm.p,
+        m.F, m.faces.p, c->s.fbuf.p, m.P.p, m.vol.p, dR);
     AEROF_LAUNCH_CHECK();
   }
   return bad;

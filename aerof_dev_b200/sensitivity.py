@@ -121,16 +121,27 @@ def direct_gradient(ctx, U, X, functional: ZForce, modes, eps=1e-10, krylov=30, 
 
 
 def fd_gradient(ctx, U, X, functional: ZForce, modes, h=1e-6, **conv):
-    """Central finite differences with the flow re-converged at X +- h Xdot."""
-    out = []
-    for Xd in modes:
+    """Central finite differences with the flow re-converged at X +- h Xdot.
+
+    h may be a pair (h1, h2 = h1/2): Richardson extrapolation
+    (4 D(h2) - D(h1)) / 3 of the two central differences, O(h^4)."""
+    def central(Xd, step):
         vals = []
         for sgn in (1.0, -1.0):
-            Xp = X + sgn * h * Xd
+            Xp = X + sgn * step * Xd
             ctx.update_coordinates(Xp)
             Up, _ = converge(ctx, U, **conv)
             vals.append(functional.value(Up, Xp))
-        out.append((vals[0] - vals[1]) / (2 * h))
+        return (vals[0] - vals[1]) / (2 * step)
+
+    out = []
+    for Xd in modes:
+        if isinstance(h, (tuple, list)):
+            d1, d2 = central(Xd, h[0]), central(Xd, h[1])
+            ratio = (h[0] / h[1]) ** 2
+            out.append((ratio * d2 - d1) / (ratio - 1.0))
+        else:
+            out.append(central(Xd, h))
     ctx.update_coordinates(X)
     return np.array(out)
 

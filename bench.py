@@ -184,7 +184,7 @@ def config_dict(args, s) -> dict:
                         f"N={s['N']} E={s['E']} F_b={s['F']}, slip walls y/z, far field x, Mach 0.8",
             "mesh_n": args.n, "N": s["N"], "E": s["E"], "F_b": s["F"], "evals_per_step": 1,
             "l2": "working set > 126 MB L2 (node data 0.2 GB + edge data 0.5 GB); no flush",
-            "parallelism": f"replicas x{args.gpus}"}
+            "parallelism": f"replicas x{args.gpus}", "kernel": getattr(args, "kernel", "blocked")}
 
 
 def run_ours(args):
@@ -200,7 +200,8 @@ def run_ours(args):
         pg = dist
     W, mesh, Ub, U = build_workload(args.n)
     s = W.lattice_sizes(args.n)
-    ctx = A.Context.from_mesh(mesh, Ub, reconstruction=A.REC_VANALBADA, device=local)
+    kern = {"blocked": A.KERNEL_BLOCKED, "edge": A.KERNEL_EDGE}[args.kernel]
+    ctx = A.Context.from_mesh(mesh, Ub, reconstruction=A.REC_VANALBADA, device=local, residual_kernel=kern)
     assert ctx.E == s["E"]
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
@@ -292,7 +293,7 @@ def run_ours(args):
         "timers_ms_per_eval": {k: (v[0] / max(v[1], 1)) for k, v in tm.items() if v[1]},
         "e2e": {"value": e2e, "unit": "Medges/s", "h2d_bytes_per_step": U.nbytes, "d2h_bytes_per_step": U.nbytes,
                 "steps": k2},
-        "gpu_launches": 4 * args.steps,
+        "gpu_launches": (5 if args.kernel == "blocked" else 5) * args.steps,
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
                    "samples": clk["samples"]},
         "unphysical_states": bad,
@@ -307,6 +308,106 @@ def run_ours(args):
     return 0
 
 
+def run_newton(args):
+    """Mixed-precision vs all-FP64 pseudo-transient Newton-GMRES, relative
+    residual 1e-8 (CFL 10 -> 1e4, RESIDUAL law ser 0.7, GMRES(30) eps 1e-2,
+    block-Jacobi).  Times are device time of aerof_gpu_newton (CUDA events)."""
+    import torch
+    import aerof_dev_b200 as A
+    torch.cuda.set_device(0)
+    W, mesh, Ub, U = build_workload(args.n)
+    s = W.lattice_sizes(args.n)
+    t0 = time.perf_counter()
+    ctx = A.Context.from_mesh(mesh, Ub, reconstruction=A.REC_VANALBADA)
+    setup_s = time.perf_counter() - t0
+    res = {}
+    states = {}
+    for name, prec in (("mixed", A.PREC_FP32), ("fp64", A.PREC_FP64)):
+        sol = A.ImplicitSteadySolver(ctx, precision=prec, cfl0=10.0, cfl_max=1e4, ser=0.7, ksp_eps=1e-2,
+                                     krylov=30, maxits=30, tol=1e-8, max_steps=args.max_steps)
+        ctx.profile(True)
+        Uo, info = sol.solve(torch.from_numpy(U).cuda())
+        tm = ctx.timers()
+        ctx.profile(False)
+        states[name] = Uo
+        res[name] = {"seconds": info["seconds"], "steps": info["steps"], "gmres_its": info["linear_its"],
+                     "rel_residual": info["rel_residual"],
+                     "timers_s": {k: v[0] / 1e3 for k, v in tm.items() if v[1]}}
+    d = (torch.linalg.norm(states["mixed"] - states["fp64"]) / torch.linalg.norm(states["fp64"])).item()
+    line = {"metric": METRIC, "workload": "newton", "value": res["fp64"]["seconds"] / res["mixed"]["seconds"],
+            "unit": "x (FP64 time / mixed time to ||R||/||R0|| <= 1e-8)", "higher_is_better": True,
+            "config": {"workload": f"steady Newton-GMRES, {args.n}^3 jittered Kuhn tet mesh N={s['N']} E={s['E']}, "
+                                   "second-order FP64 residual, first-order H1 Jacobian, block-Jacobi, GMRES(30)",
+                       "mesh_setup_s": setup_s},
+            "mixed": res["mixed"], "fp64": res["fp64"], "state_rel_l2_mixed_vs_fp64": d}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
+def run_adjoint(args):
+    """Adjoint shape sensitivities of the z-force on z=0 (32 Gaussian-bump
+    modes) on a converged Mach 0.8 flow, checked against finite differences;
+    cost of (J^T v + dR/dX^T lambda) against one primal residual."""
+    import torch
+    import aerof_dev_b200 as A
+    from aerof_dev_b200 import sensitivity as S
+    torch.cuda.set_device(0)
+    W = __import__("aerof_dev_b200.workloads", fromlist=["x"])
+    mesh = W.make_lattice_mesh(args.n, jitter=0.2, codes="channel")
+    X = mesh["X"] + W.shape_modes(mesh["X"], 1, sigma=0.25, amplitude=0.04, seed=7)[0]
+    mesh = dict(mesh, X=X)
+    Ub = W.freestream(0.8)
+    ctx = A.Context.from_mesh(mesh, Ub)
+    N = X.shape[0]
+    U0 = torch.from_numpy(np.tile(Ub, (N, 1))).cuda()
+    t0 = time.perf_counter()
+    U, info = S.converge(ctx, U0, tol=1e-10, max_steps=args.max_steps)
+    conv_s = time.perf_counter() - t0
+    zf = np.nonzero(mesh["sides"] == 4)[0]
+    F = S.ZForce(mesh["faces"], zf)
+    modes = W.shape_modes(X, args.modes, seed=11, amplitude=1.0)
+    Uh = U.cpu().numpy()
+    # cost ratio, device-resident, CUDA events
+    sp, sens = A.SpaceOperator(ctx), A.Sensitivity(ctx)
+    lam = torch.from_numpy(np.random.default_rng(3).standard_normal((N, 5))).cuda()
+    R = torch.empty_like(U)
+
+    def timed(fn, k=10):
+        fn(); torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(k):
+            fn()
+        e1.record(); torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    t_res = timed(lambda: sp.computeResidual(U, R))
+    t_vjp = timed(lambda: sens.vjp(U, lam))
+    t_dxt = timed(lambda: sens.dRdX_T(U, lam))
+    t_jvp = timed(lambda: sens.jvp(U, lam))
+    t1 = time.perf_counter()
+    ga, ainfo = S.adjoint_gradient(ctx, U, X, F, modes)
+    adj_s = time.perf_counter() - t1
+    nfd = min(args.fd_modes, args.modes)
+    gr = S.fd_gradient(ctx, Uh, X, F, modes[:nfd], h=(2e-4, 1e-4), tol=1e-10, max_steps=args.max_steps)
+    g6 = S.fd_gradient(ctx, Uh, X, F, modes[:nfd], h=1e-6, tol=1e-10, max_steps=args.max_steps)
+    line = {"metric": METRIC, "workload": "adjoint", "value": (t_vjp + t_dxt) / t_res,
+            "unit": "x one primal residual (J^T v + dR/dX^T lambda)", "higher_is_better": False,
+            "config": {"workload": f"adjoint z-force sensitivities, {args.n}^3 jittered mesh with a base bump, "
+                                   f"{args.modes} Gaussian-bump modes, Mach 0.8", "N": N},
+            "ms": {"residual": t_res, "vjp": t_vjp, "dRdX_T": t_dxt, "jvp": t_jvp},
+            "converge_s": conv_s, "adjoint_gradient_s": adj_s, "adjoint": ainfo,
+            "J": F.value(Uh, X), "grad": ga.tolist(),
+            "fd_richardson": gr.tolist(), "fd_step_1e-6": g6.tolist(),
+            "max_rel_err_vs_richardson": float(np.abs(ga[:nfd] - gr).max() / np.abs(gr).max()),
+            "max_rel_err_vs_fd_1e-6": float(np.abs(ga[:nfd] - g6).max() / np.abs(g6).max()),
+            "newton": {k: v for k, v in info.items() if k != "history"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -317,11 +418,21 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=200)
     ap.add_argument("--ref-budget", type=float, default=120.0, help="seconds of timed CPU work (reference arm)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["residual", "newton", "adjoint"], default="residual")
+    ap.add_argument("--max-steps", type=int, default=400)
+    ap.add_argument("--modes", type=int, default=32)
+    ap.add_argument("--fd-modes", type=int, default=4)
+    ap.add_argument("--kernel", choices=["blocked", "edge"], default="blocked",
+                    help="residual kernel organisation (see include/aerof_gpu.h)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "newton":
+        return run_newton(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
     return run_ours(args)
 
 

@@ -64,8 +64,19 @@ typedef struct aerof_gpu_config {
   int failsafe;      /* 1: tag nodes with non-positive reconstructed rho/p,
                         zero their gradients and recompute (Domain.C:876-918) */
   int device;        /* CUDA device ordinal                                  */
-  int reserved[5];
+  int residual_kernel;/* AEROF_KERNEL_* (0: blocked, the default)           */
+  int reserved[4];
 } aerof_gpu_config;
+
+/* Residual kernel organisation (same result within rounding):
+ * BLOCKED: nodes renumbered along a Morton curve, one thread block per 256
+ *   nodes evaluates the fluxes of the edges it owns into shared memory and
+ *   assembles them there; only edges that cross blocks go through global
+ *   memory.  Per-node sums run in a fixed order, not the reference's.
+ * EDGE: one thread per edge writes its flux to global memory, every node
+ *   then sums its edges in the reference's order (ascending neighbour).   */
+#define AEROF_KERNEL_BLOCKED 0
+#define AEROF_KERNEL_EDGE 1
 
 /* Steady pseudo-transient Newton-Krylov parameters (TsData/CFLData/KspData,
  * IoDataCore.C:2896-2911, 3067-3089; IoData.C:9-20). */

@@ -21,8 +21,11 @@ def case(request, gpu_lib, oracle_mod):
     return m, Ub, o
 
 
-def ctx_for(A, m, Ub, rec=2, failsafe=0):
-    return A.Context.from_mesh(m, Ub, reconstruction=rec, failsafe=failsafe)
+KERNELS = [0, 1]  # blocked, edge
+
+
+def ctx_for(A, m, Ub, rec=2, failsafe=0, kernel=0):
+    return A.Context.from_mesh(m, Ub, reconstruction=rec, failsafe=failsafe, residual_kernel=kernel)
 
 
 def test_edges_bit_exact(gpu_lib, case):
@@ -51,10 +54,11 @@ def test_gradients_parity(gpu_lib, case):
         assert rel_l2(a, b) < TOL
 
 
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("rec", [1, 2, 3])
-def test_residual_parity(gpu_lib, case, rec):
+def test_residual_parity(gpu_lib, case, rec, kernel):
     m, Ub, o = case
-    ctx = ctx_for(gpu_lib, m, Ub, rec=rec)
+    ctx = ctx_for(gpu_lib, m, Ub, rec=rec, kernel=kernel)
     U = W.perturbed_state(o.N, 0.8)
     R, bad = gpu_lib.SpaceOperator(ctx).computeResidual(U)
     Rr, badr = o.residual(U, Ub, rec)
@@ -62,10 +66,11 @@ def test_residual_parity(gpu_lib, case, rec):
     assert rel_l2(R, Rr) < TOL
 
 
-def test_residual_device_pointers_and_determinism(gpu_lib, case):
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_residual_device_pointers_and_determinism(gpu_lib, case, kernel):
     import torch
     m, Ub, o = case
-    ctx = ctx_for(gpu_lib, m, Ub)
+    ctx = ctx_for(gpu_lib, m, Ub, kernel=kernel)
     U = W.perturbed_state(o.N, 0.8)
     Ut = torch.from_numpy(U).cuda()
     sp = gpu_lib.SpaceOperator(ctx)
@@ -77,9 +82,10 @@ def test_residual_device_pointers_and_determinism(gpu_lib, case):
     assert np.array_equal(R1.cpu().numpy(), Rh)
 
 
-def test_freestream_preserved_gpu(gpu_lib, case):
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_freestream_preserved_gpu(gpu_lib, case, kernel):
     m, Ub, o = case
-    ctx = ctx_for(gpu_lib, m, Ub)
+    ctx = ctx_for(gpu_lib, m, Ub, kernel=kernel)
     U = np.tile(Ub, (o.N, 1))
     R, bad = gpu_lib.SpaceOperator(ctx).computeResidual(U)
     assert bad == 0 and np.abs(R).max() < 1e-11
@@ -93,13 +99,14 @@ def test_timestep_parity(gpu_lib, case):
     assert rel_l2(dt, o.timestep(U, 0.8)) < TOL
 
 
-def test_rk2_parity(gpu_lib, oracle_mod):
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_rk2_parity(gpu_lib, oracle_mod, kernel):
     # CPU-runnable case: first order, far field, Mach 0.5, 10 RK2 steps, CFL 0.8
     m = W.make_lattice_mesh(11, codes="farfield")
     Ub = W.freestream(0.5)
     o = oracle_mod.Oracle(m)
     U = W.perturbed_state(o.N, 0.5)
-    ctx = ctx_for(gpu_lib, m, Ub, rec=1)
+    ctx = ctx_for(gpu_lib, m, Ub, rec=1, kernel=kernel)
     Ug, bad = gpu_lib.ExplicitRK2(ctx, 0.8).run(U, 10)
     Ur = o.rk2(U, Ub, 1, 0.8, 10)
     assert bad == 0
@@ -107,7 +114,8 @@ def test_rk2_parity(gpu_lib, oracle_mod):
     assert rel_l2(Ug - U, Ur - U) < 1e-10
 
 
-def test_unphysical_state_counted_and_failsafe(gpu_lib, oracle_mod):
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_unphysical_state_counted_and_failsafe(gpu_lib, oracle_mod, kernel):
     m = W.make_lattice_mesh(7, jitter=0.2, codes="channel")
     Ub = W.freestream(0.8)
     o = oracle_mod.Oracle(m)
@@ -121,11 +129,11 @@ def test_unphysical_state_counted_and_failsafe(gpu_lib, oracle_mod):
     U = W.prim_to_cons(V)
     _, bad_ref = o.residual(U, Ub, 3)
     assert bad_ref > 0
-    ctx = ctx_for(gpu_lib, m, Ub, rec=3)
+    ctx = ctx_for(gpu_lib, m, Ub, rec=3, kernel=kernel)
     _, bad = gpu_lib.SpaceOperator(ctx).computeResidual(U)
     assert bad == bad_ref
     # failsafe: tagged nodes fall back to zero gradients, result matches oracle
-    ctx = ctx_for(gpu_lib, m, Ub, rec=3, failsafe=1)
+    ctx = ctx_for(gpu_lib, m, Ub, rec=3, failsafe=1, kernel=kernel)
     R, bad = gpu_lib.SpaceOperator(ctx).computeResidual(U)
     Rr, bad_r = o.residual(U, Ub, 3, failsafe=1)
     assert bad == bad_r
@@ -144,3 +152,13 @@ def test_bad_arguments_rejected(gpu_lib):
     with pytest.raises(A.AerofError) as e:
         ctx.set_mesh(m["X"], bad_tets, m["faces"], m["codes"], W.freestream(0.5))
     assert e.value.code == -1
+
+
+def test_blocked_numbering_is_a_permutation(gpu_lib, case):
+    # the Morton renumbering must not change the result beyond rounding:
+    # both organisations agree with each other as closely as with the oracle
+    m, Ub, o = case
+    U = W.perturbed_state(o.N, 0.8)
+    Rb, _ = gpu_lib.SpaceOperator(ctx_for(gpu_lib, m, Ub, kernel=0)).computeResidual(U)
+    Re, _ = gpu_lib.SpaceOperator(ctx_for(gpu_lib, m, Ub, kernel=1)).computeResidual(U)
+    assert rel_l2(Rb, Re) < 1e-13

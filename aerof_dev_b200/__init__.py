@@ -46,7 +46,7 @@ EXPORTS = [
     "aerof_gpu_prec_apply", "aerof_gpu_gmres", "aerof_gpu_newton",
     "aerof_gpu_jvp", "aerof_gpu_vjp", "aerof_gpu_dRdX", "aerof_gpu_dRdX_T",
     "aerof_gpu_residual_async", "aerof_gpu_status", "aerof_gpu_profile", "aerof_gpu_timers",
-    "aerof_gpu_update_coordinates", "aerof_gpu_linearized_solve",
+    "aerof_gpu_update_coordinates", "aerof_gpu_linearized_solve", "aerof_gpu_residual_noalloc",
 ]
 TIMER_NAMES = ["nodal_grad", "fv_term", "time_step", "fv_jac", "prec_setup", "ksp_matvec", "ksp_other", "other"]
 
@@ -117,6 +117,7 @@ def library(path: str | None = None):
             "aerof_gpu_profile": [vp, C.c_int],
             "aerof_gpu_timers": [vp, dp, dp, C.c_int],
             "aerof_gpu_update_coordinates": [vp, dp],
+            "aerof_gpu_residual_noalloc": [vp, dp, dp],
             "aerof_gpu_linearized_solve": [vp, dp, dp, dp, C.c_int, C.c_int, C.c_double, C.c_int,
                                            C.POINTER(C.c_int), C.POINTER(C.c_double)],
         }
@@ -275,6 +276,15 @@ class SpaceOperator:
         r = _Arg(R, np.float64, (ctx.N, 5), writable=True)
         ctx._check(ctx.L.aerof_gpu_residual_async(ctx.h, u.ptr, r.ptr))
         return r.obj
+
+    def computeResidualNoAlloc(self, U, R):
+        """R = residual(U) for device tensors through the entry point that
+        allocates nothing (fixed 16 MiB scratch, meshes up to ~40k nodes)."""
+        ctx = self.ctx
+        u = _Arg(U, np.float64, (ctx.N, 5))
+        r = _Arg(R, np.float64, (ctx.N, 5), writable=True)
+        bad = ctx._check(ctx.L.aerof_gpu_residual_noalloc(ctx.h, u.ptr, r.ptr))
+        return r.obj, bad
 
     def computeGradients(self, V):
         ctx = self.ctx

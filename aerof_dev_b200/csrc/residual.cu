@@ -8,6 +8,8 @@
 // the order the reference's lexicographic edge loop visits them,
 // Edge.C:391-435, SubDomain.C:341-370), then its boundary faces in face
 // order (Face.C:1185-1215).  No floating-point atomics are used.
+#include <mutex>
+
 #include "common.cuh"
 #include "physics.cuh"
 
@@ -755,6 +757,107 @@ extern "C" int aerof_gpu_rk2(aerof_gpu_ctx* c, double* U, double cfl, int nsteps
     if (dU != U)
       AEROF_CUDA(cudaMemcpyAsync(U, dU, n5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     AEROF_CUDA(cudaStreamSynchronize(c->stream));
+    return bad;
+  });
+}
+
+// ====================================================================
+// Residual without any allocation.
+//
+// Who needs it: callers that may not allocate device memory once they are
+// running -- an application that has reserved all of the GPU's memory for
+// its own pool before it calls us, or a host thread that must not take the
+// device allocator's locks.  aerof_gpu_residual grows its scratch buffers
+// (per-edge fluxes, gradients, counters) on first use; this variant keeps
+// that scratch in one fixed array of device memory that is part of the
+// library image instead, so the call itself allocates nothing.  The first
+// call on a device looks up the array's device address (once per device,
+// with that device current); make that first call before any stream
+// capture.  All calls share the one array: two calls that overlap on the
+// GPU (other streams, other contexts on the same device) race on it.
+//
+// Limit: the scratch holds 5E + 16N doubles (fluxes, gradients) plus N ints
+// (failsafe tags) plus 8 ints (counters), at most kNoAllocScratchDoubles =
+// 2,097,152 doubles (16 MiB), i.e. meshes up to roughly 40,000 nodes (a 34^3
+// lattice).  Every GPU that loads the library holds these 16 MiB until the
+// process exits.
+namespace aerof {
+
+constexpr size_t kNoAllocScratchDoubles = 2u * 1024u * 1024u;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+// Device address of g_noalloc_scratch per device, looked up once per device
+// with that device current (host code cannot use the symbol itself).
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_addr[128] = {nullptr};
+
+static double* noalloc_scratch(int dev) {
+  if (dev < 0 || dev >= 128) throw ApiError{AEROF_EINVAL, "device ordinal out of range"};
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      throw ApiError{AEROF_ECUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e)};
+    }
+    g_noalloc_addr[dev] = static_cast<double*>(p);
+  }
+  return g_noalloc_addr[dev];
+}
+
+}  // namespace aerof
+
+extern "C" int aerof_gpu_residual_noalloc(aerof_gpu_ctx* c, const double* U, double* R) {
+  return guard(c, [&]() -> int {
+    if (int e = need_mesh(c)) return e;
+    if (!U || !R) return AEROF_EINVAL;
+    if (!is_device_ptr(U) || !is_device_ptr(R)) {
+      c->last_error = "aerof_gpu_residual_noalloc needs device pointers for U and R";
+      return AEROF_EINVAL;
+    }
+    DeviceMesh& m = c->mesh;
+    const size_t need = 5 * (size_t)m.E + 16 * (size_t)m.N + ((size_t)m.N + 1) / 2 + 4;
+    if (need > kNoAllocScratchDoubles) {
+      c->last_error = "mesh too large for aerof_gpu_residual_noalloc: needs " + std::to_string(need) +
+                      " doubles of scratch (5E + 16N + N/2 + 4), the fixed array holds " +
+                      std::to_string(kNoAllocScratchDoubles);
+      return AEROF_EINVAL;
+    }
+    double* base = noalloc_scratch(c->dev);
+    double* flux = base;
+    double* G = flux + 5 * (size_t)m.E;
+    int* cnt = reinterpret_cast<int*>(G + 16 * (size_t)m.N);
+    int* tag = cnt + 8;
+    cudaStream_t s = c->stream;
+    const Gas g = make_gas(c->cfg.gamma);
+    const int rec = c->cfg.reconstruction;
+    // the array keeps the previous call's contents: clear the counters and tags
+    AEROF_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (8 + (size_t)m.N), s));
+    k_prim<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, U, m.P.p);
+    AEROF_LAUNCH_CHECK();
+    if (rec != AEROF_REC_CONSTANT) {
+      k_grad<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, nullptr, G);
+      AEROF_LAUNCH_CHECK();
+    }
+    k_edge_flux<<<grid_for(m.E, kBlock), kBlock, 0, s>>>(m.E, g, rec, c->cfg.beta, c->cfg.failsafe, m.edges.p,
+                                                         m.en.p, m.P.p, G, flux, tag, cnt);
+    AEROF_LAUNCH_CHECK();
+    int bad = 0;
+    AEROF_CUDA(cudaMemcpyAsync(&bad, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
+    AEROF_CUDA(cudaStreamSynchronize(s));
+    if (bad && c->cfg.failsafe && rec != AEROF_REC_CONSTANT) {
+      k_grad<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, tag, G);
+      AEROF_LAUNCH_CHECK();
+      k_edge_flux<<<grid_for(m.E, kBlock), kBlock, 0, s>>>(m.E, g, rec, c->cfg.beta, 0, m.edges.p, m.en.p, m.P.p, G,
+                                                           flux, tag, cnt + 1);
+      AEROF_LAUNCH_CHECK();
+    }
+    k_node_residual_t<false><<<grid_for(m.N, kBlock), kBlock, 0, s>>>(
+        m.N, m.E, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_edge.p, flux, m.nf_ptr.p, m.nf_face.p, m.fcode.p, m.fnrm.p, m.F,
+        m.faces.p, nullptr, m.P.p, m.vol.p, R);
+    AEROF_LAUNCH_CHECK();
+    AEROF_CUDA(cudaStreamSynchronize(s));
     return bad;
   });
 }

@@ -149,6 +149,24 @@ int aerof_gpu_residual_async(aerof_gpu_ctx* ctx, const double* U, double* R);
  * of asynchronous calls since the previous aerof_gpu_status (>= 0) or an
  * error code.                                                              */
 int aerof_gpu_status(aerof_gpu_ctx* ctx);
+/* Same result as aerof_gpu_residual, but the call allocates no memory: it is
+ * for callers that cannot allocate device memory while they run (an
+ * application that has handed all device memory to its own pool, a thread
+ * that must not take the allocator's locks).  This entry point has no
+ * counterpart in the reference; it is an addition of this library.
+ * - U and R must be device pointers (host arrays would need staging buffers).
+ * - Scratch (per-edge fluxes, gradients, tags, counters) lives in one fixed
+ *   16 MiB array of device memory inside the library, held by every GPU that
+ *   loads it until the process exits.  Meshes needing more than
+ *   5E + 16N + N/2 + 4 <= 2,097,152 doubles (about 40,000 nodes) are rejected
+ *   with AEROF_EINVAL and a message in aerof_gpu_last_error.
+ * - The first call on a device looks up the array's device address; make
+ *   that first call before any stream capture.
+ * - Every call shares the array and the previous call's contents stay in it
+ *   (the call clears what must start at zero).  Calls that overlap on the GPU
+ *   -- on other streams or from other contexts on the same device -- race.
+ * Returns the unphysical-state count like aerof_gpu_residual.              */
+int aerof_gpu_residual_noalloc(aerof_gpu_ctx* ctx, const double* U, double* R);
 /* DistNodalGrad::compute, least squares (DistNodalGrad.C:790-806,
  * SubDomain.C:297-374) of primitive V[N][5]; ddx/ddy/ddz [N][5].        */
 int aerof_gpu_gradients(aerof_gpu_ctx* ctx, const double* V, double* ddx, double* ddy, double* ddz);

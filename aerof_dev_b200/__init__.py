@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import sys
 
 import numpy as np
 
@@ -39,7 +40,8 @@ PREC_FP32, PREC_FP64 = 32, 64
 
 # every entry point of include/aerof_gpu.h
 EXPORTS = [
-    "aerof_gpu_create", "aerof_gpu_destroy", "aerof_gpu_set_stream", "aerof_gpu_last_error",
+    "aerof_gpu_create", "aerof_gpu_destroy", "aerof_gpu_set_stream", "aerof_gpu_launch_count",
+    "aerof_gpu_last_error",
     "aerof_gpu_set_mesh", "aerof_gpu_mesh_sizes", "aerof_gpu_get_edges", "aerof_gpu_get_geometry",
     "aerof_gpu_residual", "aerof_gpu_gradients", "aerof_gpu_timestep", "aerof_gpu_rk2",
     "aerof_gpu_jacobian", "aerof_gpu_get_jacobian", "aerof_gpu_matvec", "aerof_gpu_prec_setup",
@@ -91,6 +93,7 @@ def library(path: str | None = None):
             "aerof_gpu_create": [C.POINTER(Config), C.POINTER(C.c_void_p)],
             "aerof_gpu_destroy": [vp],
             "aerof_gpu_set_stream": [vp, vp],
+            "aerof_gpu_launch_count": [vp],
             "aerof_gpu_last_error": [vp, C.c_char_p, C.c_int],
             "aerof_gpu_set_mesh": [vp, C.c_int, C.c_int, C.c_int, dp, ip, ip, ip, dp],
             "aerof_gpu_mesh_sizes": [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
@@ -118,7 +121,7 @@ def library(path: str | None = None):
             "aerof_gpu_timers": [vp, dp, dp, C.c_int],
             "aerof_gpu_update_coordinates": [vp, dp],
             "aerof_gpu_residual_noalloc": [vp, dp, dp],
-            "aerof_gpu_linearized_solve": [vp, dp, dp, dp, C.c_int, C.c_int, C.c_double, C.c_int,
+            "aerof_gpu_linearized_solve": [vp, dp, dp, dp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
                                            C.POINTER(C.c_int), C.POINTER(C.c_double)],
         }
         for name, args in sig.items():
@@ -168,18 +171,66 @@ def _like(a, shape, dtype=np.float64):
     return np.empty(shape, dtype=dtype)
 
 
+_CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
+
+
+def launch_count() -> int:
+    """Kernels the library launched since the previous call (process-wide)."""
+    n = C.c_longlong(0)
+    rc = library().aerof_gpu_launch_count(C.byref(n))
+    if rc != 0:
+        raise AerofError(rc, "aerof_gpu_launch_count")
+    return int(n.value)
+
+
+class _StreamOrdered:
+    """The library's entry points, each called after the context has been
+    put on torch's current stream (see ``Context._follow_torch``)."""
+
+    def __init__(self, ctx, lib):
+        self._ctx, self._lib = ctx, lib
+
+    def __getattr__(self, name):
+        fn = getattr(self._lib, name)
+        ctx = self._ctx
+
+        def call(*args):
+            ctx._follow_torch()
+            return fn(*args)
+        return call
+
+
 class Context:
-    """One GPU context: ``aerof_gpu_create`` + ``aerof_gpu_set_mesh``."""
+    """One GPU context: ``aerof_gpu_create`` + ``aerof_gpu_set_mesh``.
+
+    Unless ``set_stream`` chose a stream, the context's work is ordered on
+    torch's current stream whenever torch has initialised CUDA, so device
+    tensors produced by torch are complete before the library reads them."""
 
     def __init__(self, reconstruction: int = REC_VANALBADA, gamma: float = 1.4, beta: float = 1.0 / 3.0,
                  failsafe: int = 0, device: int = 0, residual_kernel: int = KERNEL_BLOCKED):
-        self.L = library()
+        self._raw = library()
+        self._explicit_stream = False
+        self._torch_stream = None
+        self.h = None
+        self.L = _StreamOrdered(self, self._raw)
         cfg = Config(gamma, beta, reconstruction, failsafe, device, residual_kernel)
         h = C.c_void_p()
-        self._check(self.L.aerof_gpu_create(C.byref(cfg), C.byref(h)), None)
+        self._check(self._raw.aerof_gpu_create(C.byref(cfg), C.byref(h)), None)
         self.h = h
         self.cfg = cfg
         self.N = self.E = self.F = 0
+
+    def _follow_torch(self):
+        if self._explicit_stream or not self.h:
+            return
+        torch = sys.modules.get("torch")
+        if torch is None or not torch.cuda.is_initialized():
+            return
+        hs = torch.cuda.current_stream(self.cfg.device).cuda_stream or _CUDA_STREAM_LEGACY
+        if hs != self._torch_stream:
+            self._raw.aerof_gpu_set_stream(self.h, C.c_void_p(hs))
+            self._torch_stream = hs
 
     def _check(self, rc: int, h=0):
         if rc < 0:
@@ -187,14 +238,14 @@ class Context:
             hh = self.h if h == 0 else h
             if hh:
                 buf = C.create_string_buffer(512)
-                self.L.aerof_gpu_last_error(hh, buf, 512)
+                self._raw.aerof_gpu_last_error(hh, buf, 512)
                 msg = buf.value.decode()
             raise AerofError(rc, msg)
         return rc
 
     def close(self):
         if getattr(self, "h", None):
-            self.L.aerof_gpu_destroy(self.h)
+            self._raw.aerof_gpu_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -203,8 +254,18 @@ class Context:
         except Exception:
             pass
 
-    def set_stream(self, stream_ptr: int | None):
-        self._check(self.L.aerof_gpu_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
+    def set_stream(self, stream):
+        """Run the context's work on a CUDA stream: a ``torch.cuda.Stream``, a
+        raw ``cudaStream_t`` handle, or None for the context's own stream.  A
+        handle of 0 is the legacy default stream (torch reports its default
+        stream as 0), passed to the library as ``cudaStreamLegacy``."""
+        if stream is None:
+            h = 0
+        else:
+            h = getattr(stream, "cuda_stream", stream) or _CUDA_STREAM_LEGACY
+        self._explicit_stream = stream is not None
+        self._torch_stream = None
+        self._check(self._raw.aerof_gpu_set_stream(self.h, C.c_void_p(h)))
 
     def set_mesh(self, X, tets, faces, codes, Ub):
         X = _Arg(X, np.float64)
@@ -440,8 +501,10 @@ class Sensitivity:
     def dRdX_T(self, U, lam):
         return self._call(self.ctx.L.aerof_gpu_dRdX_T, U, lam, 5, 3)
 
-    def solve(self, U, b, transpose=False, krylov=30, maxits=300, eps=1e-10):
-        """Solve J x = b (direct) or J^T x = b (adjoint) with the exact operator."""
+    def solve(self, U, b, transpose=False, krylov=30, maxits=300, eps=1e-10, inner_its=0):
+        """Solve J x = b (direct) or J^T x = b (adjoint) with the exact
+        operator.  inner_its > 0: flexible GMRES preconditioned by that many
+        mixed-precision GMRES iterations on the first-order operator."""
         ctx = self.ctx
         u = _Arg(U, np.float64, (ctx.N, 5))
         bb = _Arg(b, np.float64, (ctx.N, 5))
@@ -449,5 +512,5 @@ class Sensitivity:
         xx = _Arg(x, np.float64, writable=True)
         its, res = C.c_int(), C.c_double()
         ctx._check(ctx.L.aerof_gpu_linearized_solve(ctx.h, u.ptr, bb.ptr, xx.ptr, krylov, maxits, eps,
-                                                    int(transpose), C.byref(its), C.byref(res)))
+                                                    int(transpose), int(inner_its), C.byref(its), C.byref(res)))
         return xx.obj, its.value, res.value

@@ -134,6 +134,14 @@ extern "C" int aerof_gpu_destroy(aerof_gpu_ctx* c) {
   return AEROF_OK;
 }
 
+std::atomic<long long> aerof::g_launch_count{0};
+
+extern "C" int aerof_gpu_launch_count(long long* count) {
+  if (!count) return AEROF_EINVAL;
+  *count = aerof::g_launch_count.exchange(0);
+  return AEROF_OK;
+}
+
 extern "C" int aerof_gpu_set_stream(aerof_gpu_ctx* c, void* stream) {
   if (!c) return AEROF_EINVAL;
   c->stream = stream ? (cudaStream_t)stream : c->own_stream;

@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <cstdio>
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -13,6 +14,7 @@
 #include "physics.cuh"
 
 namespace aerof {
+extern std::atomic<long long> g_launch_count;
 
 // ------------------------------------------------------------------ errors
 struct CudaError {
@@ -26,7 +28,13 @@ struct CudaError {
     if (e_ != cudaSuccess) throw ::aerof::CudaError{e_, #call};           \
   } while (0)
 
-#define AEROF_LAUNCH_CHECK() AEROF_CUDA(cudaGetLastError())
+// Every kernel launch of the library is followed by this check, which also
+// counts the launch (aerof_gpu_launch_count).
+#define AEROF_LAUNCH_CHECK()                                            \
+  do {                                                                  \
+    ::aerof::g_launch_count.fetch_add(1, std::memory_order_relaxed);    \
+    AEROF_CUDA(cudaGetLastError());                                     \
+  } while (0)
 
 struct ApiError {
   int code;
@@ -111,22 +119,34 @@ struct DeviceMesh {
   DBuf<int> nt_tet;        // [4T]  tet*4 + local vertex
   // host copies for queries
   std::vector<int> h_edges;
+  // Sliced block layout of the H1 operator (rows in slices of 32; block k of
+  // row r = 32 s + l stored element-interleaved: element e at
+  // ((sptr[s] + k) * 25 + e) * 32 + l; diagonal and its inverse at
+  // (s * 25 + e) * 32 + l).  scol: column of block (s, k, l); rows with
+  // fewer than ks[s] blocks are padded with their own index.
+  int nsl = 0;
+  DBuf<int> sptr;          // [nsl+1] block columns before slice s
+  DBuf<int> scol;          // [sptr[nsl] * 32]
+  std::vector<int> h_sptr, h_nbr_ptr;
 
   // ---- blocked residual: Morton-renumbered copy of the node data ----
   int NB = 256;            // nodes per block
-  int nblk = 0, maxE = 0, nX = 0;
+  int nblk = 0, maxE = 0, nX = 0, maxH = 0, maxL = 0, maxHf = 0;
   DBuf<int> n2o, o2n;      // [N] new -> old and old -> new node ids
   DBuf<double> P2;         // [N][8] node records in new numbering
   DBuf<double> W2;         // [6][N] LSQ constants, new numbering
   DBuf<double> vol2;       // [N]
   DBuf<int> nb2_ptr, nb2_node;  // neighbour CSR in new numbering (ascending)
-  DBuf<int2> bedges;       // [E] (first, second) new ids, sorted, first < second
+  DBuf<int> hptr, hnode;        // per block: halo nodes (outside the block, ascending)
+  DBuf<unsigned short> lnb;     // nb2_node entries as slots of the block's staged nodes
+  DBuf<int> hfptr, hfnode;      // per block: forward halo (second endpoints in later blocks)
+  DBuf<ushort2> bl;             // per blocked edge: (first, second) as slots of the staged nodes
   DBuf<int> bsrc;          // [E] reference edge id | (1<<31 if reversed)
   DBuf<double> bnorm;      // [3][E] normals oriented first -> second
   DBuf<int> beptr;         // [nblk+1] owned-edge range of each block
   DBuf<int> lptr, lidx;    // per node (new): owned local edge slots, sign bit = second endpoint
   DBuf<int> xslot;         // [E] spill slot of a block-crossing edge, -1 otherwise
-  DBuf<int> xin_ptr, xin_slot;  // per node (new): incoming spill slots
+  DBuf<int> xin_ptr;       // per node (new): its incoming spill slots [xin_ptr[n], xin_ptr[n+1])
 };
 
 struct Scratch {
@@ -147,14 +167,17 @@ struct Scratch {
 // Implicit operator: BSR-by-rows of the H1 Jacobian.
 struct Implicit {
   int precision = 0;       // 32 or 64, 0 = not assembled
+  bool transposed = false; // blocks hold H1^T (row r = column r of H1)
   DBuf<double> diag64, off64, dinv64;   // [N][25], [2E][25], [N][25]
   DBuf<float> diag32, off32, dinv32;
-  DBuf<double> diagscr;    // [E][2][25] per-edge diagonal contributions
   bool prec_ready = false;
   // Krylov workspace
   DBuf<double> basis;      // [(m+1)][5N]
   DBuf<double> w, r, x, b, t;
   DBuf<double> hcol;       // device scratch for one Hessenberg column
+  DBuf<unsigned> ticket;   // grid-reduction ticket of the fused Gram-Schmidt kernels
+  // flexible GMRES on the exact linearisation (outer FP64 vectors)
+  DBuf<double> fV, fZ, fw, fr, fh;
 };
 
 // Dual-number work arrays of the forward-mode linearisation.

@@ -22,128 +22,201 @@ namespace aerof {
 constexpr int kIB = 256;
 constexpr int kGB = 1184;  // reduction grid: 8 x 148 SMs
 
-template <class S> __device__ __forceinline__ void store_block(S* dst, const double* v, double scale) {
+// Sliced block layout (SELL-32): rows in slices of 32; element e of block k
+// of row r = 32 s + l at ((sptr[s] + k) * 25 + e) * 32 + l, so the 32 rows of
+// a warp read each block element as one 128-byte (FP32) line; diagonal
+// blocks and their inverses at (s * 25 + e) * 32 + l.
+__device__ __forceinline__ size_t sl_off(const int* __restrict__ sptr, int r, int k, int e) {
+  return (((size_t)sptr[r >> 5] + k) * 25 + e) * 32 + (r & 31);
+}
+__device__ __forceinline__ size_t sl_diag(int r, int e) { return ((size_t)(r >> 5) * 25 + e) * 32 + (r & 31); }
+
+// v * scale rounded to S, written as block k of row r (TR: the transposed
+// block), and the same for a diagonal block
+template <class S, bool TR>
+__device__ __forceinline__ void store_off(S* __restrict__ off, const int* __restrict__ sptr, int r, int k,
+                                          const double* v, double scale) {
+  const size_t b = sl_off(sptr, r, k, 0);
 #pragma unroll
-  for (int k = 0; k < 25; ++k) dst[k] = (S)(v[k] * scale);
+  for (int e = 0; e < 25; ++e) off[b + (size_t)32 * e] = (S)(v[TR ? 5 * (e % 5) + e / 5 : e] * scale);
+}
+template <class S, bool TR>
+__device__ __forceinline__ void store_diag(S* __restrict__ diag, int r, const double* v) {
+  const size_t b = sl_diag(r, 0);
+#pragma unroll
+  for (int e = 0; e < 25; ++e) diag[b + (size_t)32 * e] = (S)v[TR ? 5 * (e % 5) + e / 5 : e];
 }
 
-// One thread per edge: approximate Roe Jacobians at the un-reconstructed
-// states (roejacappr3Dgas, FluxFcnDescSG.C:155-262), off-diagonal blocks
-// A_ij = dF/dU_j / vol_i and A_ji = -dF/dU_i / vol_j (Edge.C:4503-4523),
-// and the diagonal contributions +dF/dU_i (row i) and -dF/dU_j (row j) into
-// dscr at the same CSR positions, summed per row afterwards.
-template <class S>
-__global__ void k_jac_edges(int E, Gas g, const int2* __restrict__ edges, const int2* __restrict__ epos,
-                            const double* __restrict__ en, const double* __restrict__ P,
-                            const double* __restrict__ vol, S* __restrict__ off, double* __restrict__ dscr) {
-  int l = blockIdx.x * blockDim.x + threadIdx.x;
-  if (l >= E) return;
-  const int2 ij = edges[l];
-  const int2 pp = epos[l];
-  const double n0 = en[l], n1 = en[(size_t)E + l], n2 = en[2 * (size_t)E + l];
-  double Vi[5], Vj[5];
-#pragma unroll
-  for (int k = 0; k < 5; ++k) { Vi[k] = P[8 * (size_t)ij.x + k]; Vj[k] = P[8 * (size_t)ij.y + k]; }
-  double ji[25], jj[25];
-  if (sqrt(n0 * n0 + n1 * n1 + n2 * n2) < 1e-18) {
-#pragma unroll
-    for (int k = 0; k < 25; ++k) ji[k] = jj[k] = 0.0;
-  } else {
-    roe_jac(g, n0, n1, n2, Vi, Vj, 1.0, ji);
-    roe_jac(g, n0, n1, n2, Vj, Vi, -1.0, jj);
-  }
-  const double voli = 1.0 / vol[ij.x], volj = 1.0 / vol[ij.y];
-  store_block(off + 25 * (size_t)pp.x, jj, voli);
-  store_block(off + 25 * (size_t)pp.y, ji, -volj);
-  store_block(dscr + 25 * (size_t)pp.x, ji, 1.0);
-  store_block(dscr + 25 * (size_t)pp.y, jj, -1.0);
-}
-
-// One thread per node: diagonal block = sum of the row's edge contributions
-// (neighbour order), + face blocks (face order, Face.C:814-847), times
-// 1/vol (SubDomain.C:1760-1765), + I/dt (TimeState.C:731-756).
-template <class S>
-__global__ void k_jac_diag(int N, int F, Gas g, const double* __restrict__ Ub0, const int* __restrict__ nbr_ptr,
-                           const double* __restrict__ dscr, const int* __restrict__ nf_ptr,
-                           const int* __restrict__ nf_face, const int* __restrict__ fcode,
-                           const double* __restrict__ fn, const double* __restrict__ P,
-                           const double* __restrict__ vol, const double* __restrict__ dt, S* __restrict__ diag) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+// Half a warp per row r: lane l takes the row's neighbours s at positions
+// l, l+16, ... of its ascending neighbour list.  For the edge e = (r, s)
+// (r first endpoint, sg = +1) or (s, r) (r second, sg = -1) it evaluates the
+// approximate Roe Jacobians at the un-reconstructed states
+// (roejacappr3Dgas, FluxFcnDescSG.C:155-262; roe_jac(n, Va, Vb, +1) is
+// dF/dU of the first endpoint a, roe_jac(n, Va, Vb, -1) of the second): the
+// off-diagonal block A_rs = sg dF/dU_s / vol_r and the contribution
+// sg dF/dU_r to the diagonal block (Edge.C:4503-4523).  The lanes then take
+// the row's boundary faces (Face.C:814-847) the same way; the 16 partial
+// diagonal sums are added in a fixed xor tree, times 1/vol
+// (SubDomain.C:1760-1765), + I/dt (TimeState.C:731-756).  Every edge's two
+// Jacobians are evaluated once by each of its two rows, which costs twice
+// the arithmetic of an edge loop but needs no scratch for the diagonal.
+// TR: the transpose H1^T is stored instead (block k of row r = A_sr^T, with
+// A_sr = -sg dF/dU_r / vol_s, the Jacobian already formed for the
+// diagonal), for products with the transpose that read coalesced.
+template <class S, bool TR>
+__global__ void __launch_bounds__(256) k_jac_rows(int N, int E, int F, Gas g, const double* __restrict__ Ub0,
+                                                  const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_node,
+                                                  const int* __restrict__ nbr_edge, const double* __restrict__ en,
+                                                  const double* __restrict__ P, const double* __restrict__ vol,
+                                                  const int* __restrict__ nf_ptr, const int* __restrict__ nf_face,
+                                                  const int* __restrict__ fcode, const double* __restrict__ fn,
+                                                  const double* __restrict__ dt, const int* __restrict__ sptr,
+                                                  S* __restrict__ off, S* __restrict__ diag) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = t >> 4, l = t & 15;
+  const bool act = r < N;
   double a[25];
 #pragma unroll
   for (int k = 0; k < 25; ++k) a[k] = 0.0;
-  for (int p = nbr_ptr[i]; p < nbr_ptr[i + 1]; ++p) {
-    const double* d = dscr + 25 * (size_t)p;
+  if (act) {
+    double Vr[5];
 #pragma unroll
-    for (int k = 0; k < 25; ++k) a[k] += d[k];
-  }
-  const int q1 = nf_ptr[i + 1];
-  if (nf_ptr[i] < q1) {
-    double V[5], Ub[5], jac[25];
+    for (int k = 0; k < 5; ++k) Vr[k] = P[8 * (size_t)r + k];
+    const double volr = 1.0 / vol[r];
+    const int p0 = nbr_ptr[r], p1 = nbr_ptr[r + 1];
+    for (int p = p0 + l; p < p1; p += 16) {
+      const int s = nbr_node[p];
+      const int er = nbr_edge[p];
+      const size_t e = (size_t)(er & 0x7fffffff);
+      const double sg = er < 0 ? -1.0 : 1.0;
+      const double n0 = en[e], n1 = en[(size_t)E + e], n2 = en[2 * (size_t)E + e];
+      double Vs[5];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) { V[k] = P[8 * (size_t)i + k]; Ub[k] = Ub0[k]; }
-    const double third = 1.0 / 3.0;
-    for (int q = nf_ptr[i]; q < q1; ++q) {
-      const int f = nf_face[q];
-      face_jac(g, fcode[f], third * fn[f], third * fn[(size_t)F + f], third * fn[2 * (size_t)F + f], V, Ub, jac);
+      for (int k = 0; k < 5; ++k) Vs[k] = P[8 * (size_t)s + k];
+      const double rnorm = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+      const bool zero = rnorm < 1e-18;
+      // roe_jac(n, Vs, Vr, -sg) and roe_jac(n, Vr, Vs, sg) share the
+      // dissipation matrix D: form it once, then (H(V) +- D) |n| / 2
+      double jac[25];
+      double D[25], H[25];
+      double un[3];
+      const double invnorm = 1.0 / rnorm;
+      un[0] = n0 * invnorm; un[1] = n1 * invnorm; un[2] = n2 * invnorm;
+      const double half_rn = 0.5 * rnorm;
+      if (!zero) roe_jac_D(g, un, Vr, Vs, D);
+      if (!TR) {
+        if (zero) {
 #pragma unroll
-      for (int k = 0; k < 25; ++k) a[k] += jac[k];
+          for (int k = 0; k < 25; ++k) jac[k] = 0.0;
+        } else {
+          roe_jac_H(g, un, Vs, H);
+#pragma unroll
+          for (int k = 0; k < 25; ++k) jac[k] = (H[k] + (-sg) * D[k]) * half_rn;
+        }
+        store_off<S, false>(off, sptr, r, p - p0, jac, sg * volr);
+      }
+      if (zero) {
+#pragma unroll
+        for (int k = 0; k < 25; ++k) jac[k] = 0.0;
+      } else {
+        roe_jac_H(g, un, Vr, H);
+#pragma unroll
+        for (int k = 0; k < 25; ++k) {
+          jac[k] = (H[k] + sg * D[k]) * half_rn;
+          a[k] += sg * jac[k];
+        }
+      }
+      if (TR) store_off<S, true>(off, sptr, r, p - p0, jac, -sg * (1.0 / vol[s]));
+    }
+    const int q1 = nf_ptr[r + 1];
+    if (nf_ptr[r] + l < q1) {
+      double Ub[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) Ub[k] = Ub0[k];
+      const double third = 1.0 / 3.0;
+      for (int q = nf_ptr[r] + l; q < q1; q += 16) {
+        const int f = nf_face[q];
+        double jac[25];
+        face_jac(g, fcode[f], third * fn[f], third * fn[(size_t)F + f], third * fn[2 * (size_t)F + f], Vr, Ub, jac);
+#pragma unroll
+        for (int k = 0; k < 25; ++k) a[k] += jac[k];
+      }
     }
   }
-  const double voli = 1.0 / vol[i];
+#pragma unroll
+  for (int k = 0; k < 25; ++k) {
+    a[k] += __shfl_xor_sync(0xffffffffu, a[k], 8);
+    a[k] += __shfl_xor_sync(0xffffffffu, a[k], 4);
+    a[k] += __shfl_xor_sync(0xffffffffu, a[k], 2);
+    a[k] += __shfl_xor_sync(0xffffffffu, a[k], 1);
+  }
+  if (!act || l != 0) return;
+  const double voli = 1.0 / vol[r];
 #pragma unroll
   for (int k = 0; k < 25; ++k) a[k] *= voli;
   if (dt) {
-    const double c = 1.0 / dt[i];
+    const double c = 1.0 / dt[r];
 #pragma unroll
     for (int k = 0; k < 5; ++k) a[6 * k] += c;
   }
-  store_block(diag + 25 * (size_t)i, a, 1.0);
+  store_diag<S, TR>(diag, r, a);
 }
 
-// y = A p (or A^T p): per row, diagonal block first, then the row's
-// neighbours in ascending order (SubDomain::computeMatVecProdH1 and
-// H1transpose, SubDomain.C:3916-3995).  Blocks in S (float or double),
-// vectors and accumulation in double.
+// y += A x for a 5x5 block of the sliced layout (element e at b + 32 e),
+// or A^T x; FP64 accumulation in the order of a row-major gemv
 template <class S, class TX>
-__device__ __forceinline__ void gemv_add(const S* __restrict__ a, const TX* __restrict__ x, double* y, bool trans) {
+__device__ __forceinline__ void gemv_sl(const S* __restrict__ a, size_t b, const TX* __restrict__ x, double* y,
+                                        bool trans) {
   double xv[5];
 #pragma unroll
   for (int k = 0; k < 5; ++k) xv[k] = (double)x[k];
   if (!trans) {
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
-      double s = (double)a[5 * r] * xv[0];
+      double s = (double)a[b + 32 * (5 * r)] * xv[0];
 #pragma unroll
-      for (int c = 1; c < 5; ++c) s += (double)a[5 * r + c] * xv[c];
+      for (int c = 1; c < 5; ++c) s += (double)a[b + 32 * (5 * r + c)] * xv[c];
       y[r] += s;
     }
   } else {
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
-      double s = (double)a[r] * xv[0];
+      double s = (double)a[b + 32 * r] * xv[0];
 #pragma unroll
-      for (int c = 1; c < 5; ++c) s += (double)a[5 * c + r] * xv[c];
+      for (int c = 1; c < 5; ++c) s += (double)a[b + 32 * (5 * c + r)] * xv[c];
       y[r] += s;
     }
   }
 }
 
+// y = A p (or A^T p): per row, diagonal block first, then the row's
+// neighbours in ascending order (SubDomain::computeMatVecProdH1 and
+// H1transpose, SubDomain.C:3916-3995).  Blocks in S (float or double),
+// vectors and accumulation in double.  One thread per row; a warp is one
+// slice, so every block element is read as one coalesced line.  TRANS
+// (stored blocks not transposed): block A_sr is read from row s's slice.
 template <class S, bool TRANS, class TI, class TO>
-__global__ void k_spmv(int N, const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_node,
-                       const int* __restrict__ nbr_tpos, const S* __restrict__ diag, const S* __restrict__ off,
-                       const TI* __restrict__ p, TO* __restrict__ y) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+__global__ void __launch_bounds__(256) k_spmv(int N, const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_tpos,
+                                              const int* __restrict__ sptr, const int* __restrict__ scol,
+                                              const S* __restrict__ diag, const S* __restrict__ off,
+                                              const TI* __restrict__ p, TO* __restrict__ y) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= N) return;
   double acc[5] = {0, 0, 0, 0, 0};
-  gemv_add(diag + 25 * (size_t)i, p + 5 * (size_t)i, acc, TRANS);
-  for (int q = nbr_ptr[i]; q < nbr_ptr[i + 1]; ++q) {
-    const size_t b = TRANS ? (size_t)nbr_tpos[q] : (size_t)q;
-    gemv_add(off + 25 * b, p + 5 * (size_t)nbr_node[q], acc, TRANS);
+  gemv_sl(diag, sl_diag(r, 0), p + 5 * (size_t)r, acc, TRANS);
+  const int p0 = nbr_ptr[r], cnt = nbr_ptr[r + 1] - p0;
+  const size_t cb = (size_t)sptr[r >> 5] * 32 + (r & 31);
+  for (int k = 0; k < cnt; ++k) {
+    const int s = scol[cb + (size_t)32 * k];
+    if (!TRANS) {
+      gemv_sl(off, sl_off(sptr, r, k, 0), p + 5 * (size_t)s, acc, false);
+    } else {
+      const int kt = nbr_tpos[p0 + k] - nbr_ptr[s];
+      gemv_sl(off, sl_off(sptr, s, kt, 0), p + 5 * (size_t)s, acc, true);
+    }
   }
 #pragma unroll
-  for (int k = 0; k < 5; ++k) y[5 * (size_t)i + k] = (TO)acc[k];
+  for (int k = 0; k < 5; ++k) y[5 * (size_t)r + k] = (TO)acc[k];
 }
 
 // Block-Jacobi set-up (JacobiPrec::setup -> DiagMat::invert, DiagMatrix.C:
@@ -153,16 +226,17 @@ template <class S>
 __global__ void k_bj_invert(int N, const S* __restrict__ diag, S* __restrict__ dinv, int* __restrict__ bad) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
+  const size_t b = sl_diag(i, 0);
   S a[25];
 #pragma unroll
-  for (int k = 0; k < 25; ++k) a[k] = diag[25 * (size_t)i + k];
+  for (int k = 0; k < 25; ++k) a[k] = diag[b + (size_t)32 * k];
   bool inv = true;
 #pragma unroll
   for (int k = 0; k < 5; ++k)
     if (a[6 * k] == S(0)) inv = false;
   if (inv && invert5<S>(a)) atomicAdd(bad, 1);
 #pragma unroll
-  for (int k = 0; k < 25; ++k) dinv[25 * (size_t)i + k] = a[k];
+  for (int k = 0; k < 25; ++k) dinv[b + (size_t)32 * k] = a[k];
 }
 
 // z = D^-1 x (or D^-T x): JacobiPrec::apply/applyT (KspPrec.C:86-111)
@@ -172,7 +246,7 @@ __global__ void k_bj_apply(int N, const S* __restrict__ dinv, const TI* __restri
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double acc[5] = {0, 0, 0, 0, 0};
-  gemv_add(dinv + 25 * (size_t)i, x + 5 * (size_t)i, acc, trans != 0);
+  gemv_sl(dinv, sl_diag(i, 0), x + 5 * (size_t)i, acc, trans != 0);
 #pragma unroll
   for (int k = 0; k < 5; ++k) z[5 * (size_t)i + k] = (TO)acc[k];
 }
@@ -194,64 +268,92 @@ __global__ void k_sub(size_t n, const double* __restrict__ b, const TW* __restri
   size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q < n) z[q] = (TO)(b[q] - (double)w[q]);
 }
-// Modified Gram-Schmidt step i with the projection of step i-1 fused in:
-//   w -= hprev * Vprev   (hprev read from device memory, skipped if null)
-//   part[b] = partial sums of w . Vcur      (deterministic block tree)
-template <class TV>
-__global__ void k_mgs_step(size_t n, const double* __restrict__ hprev, const TV* __restrict__ Vprev,
-                           const TV* __restrict__ Vcur, TV* __restrict__ w, double* __restrict__ part) {
-  __shared__ double sh[kIB];
+// Deterministic grid reduction finished by the last block: every block
+// writes its partial sum (warp xor trees, then the warps in order), takes a
+// ticket, and the block that takes the last ticket adds the partials in
+// block order, writes *out and re-arms the ticket.
+__device__ __forceinline__ double block_sum(double v, double* ws) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += ws[k];
+  return t;
+}
+__device__ __forceinline__ void grid_sum_last_block(double v, double* __restrict__ part,
+                                                    unsigned* __restrict__ ticket, double* __restrict__ out) {
+  __shared__ double ws[32];
+  __shared__ bool last;
+  const double b = block_sum(v, ws);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = b;
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double t = 0.0;
+  for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) t += __ldcg(part + k);
+  t = block_sum(t, ws);
+  if (threadIdx.x == 0) {
+    *out = t;
+    *ticket = 0u;
+  }
+}
+
+template <class TV> struct Vec16;
+template <> struct Vec16<float> { using T = float4; static constexpr int W = 4; };
+template <> struct Vec16<double> { using T = double2; static constexpr int W = 2; };
+
+// Modified Gram-Schmidt step with the projection of the previous step fused
+// in, 16-byte loads, and the reduction finished in the same launch:
+//   w -= hprev * Vprev    (skipped when hprev is null)
+//   *out = w . Vcur       (NORM: *out = w . w)
+// w is rounded to TV after the projection, before the product, as the
+// stored vector is.  All vectors 16-byte aligned.
+template <class TV, bool NORM>
+__global__ void __launch_bounds__(kIB) k_mgs(size_t n, const double* __restrict__ hprev, const TV* __restrict__ Vprev,
+                                             const TV* __restrict__ Vcur, TV* __restrict__ w,
+                                             double* __restrict__ part, unsigned* __restrict__ ticket,
+                                             double* __restrict__ out) {
+  using VT = typename Vec16<TV>::T;
+  constexpr int W = Vec16<TV>::W;
   const double h = hprev ? *hprev : 0.0;
+  const size_t nv = n / W;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
   double s = 0.0;
-  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < nv; q += stride) {
+    VT wv = reinterpret_cast<const VT*>(w)[q];
+    TV* wp = reinterpret_cast<TV*>(&wv);
+    if (hprev) {
+      const VT pv = reinterpret_cast<const VT*>(Vprev)[q];
+      const TV* pp = reinterpret_cast<const TV*>(&pv);
+#pragma unroll
+      for (int k = 0; k < W; ++k) wp[k] = (TV)((double)wp[k] - h * (double)pp[k]);
+      reinterpret_cast<VT*>(w)[q] = wv;
+    }
+    if (NORM) {
+#pragma unroll
+      for (int k = 0; k < W; ++k) s += (double)wp[k] * (double)wp[k];
+    } else {
+      const VT cv = reinterpret_cast<const VT*>(Vcur)[q];
+      const TV* cp = reinterpret_cast<const TV*>(&cv);
+#pragma unroll
+      for (int k = 0; k < W; ++k) s += (double)wp[k] * (double)cp[k];
+    }
+  }
+  for (size_t q = nv * W + (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
     double wq = (double)w[q];
     if (hprev) {
-      wq = wq - h * (double)Vprev[q];
-      w[q] = (TV)wq;
-      wq = (double)(TV)wq;
+      w[q] = (TV)(wq - h * (double)Vprev[q]);
+      wq = (double)w[q];
     }
-    s += wq * (double)Vcur[q];
+    s += wq * (NORM ? wq : (double)Vcur[q]);
   }
-  sh[threadIdx.x] = s;
-  __syncthreads();
-  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
-    if (threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
-}
-__global__ void k_sum_partials(int nb, const double* __restrict__ part, double* __restrict__ out) {
-  __shared__ double sh[kIB];
-  double s = 0.0;
-  for (int b = threadIdx.x; b < nb; b += blockDim.x) s += part[b];
-  sh[threadIdx.x] = s;
-  __syncthreads();
-  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
-    if (threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) out[0] = sh[0];
-}
-// last projection of the column, then w . w
-template <class TV>
-__global__ void k_mgs_last(size_t n, const double* __restrict__ hprev, const TV* __restrict__ Vprev,
-                           TV* __restrict__ w, double* __restrict__ part) {
-  __shared__ double sh[kIB];
-  const double h = *hprev;
-  double s = 0.0;
-  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-    const TV wt = (TV)((double)w[q] - h * (double)Vprev[q]);
-    w[q] = wt;
-    const double wq = (double)wt;
-    s += wq * wq;
-  }
-  sh[threadIdx.x] = s;
-  __syncthreads();
-  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
-    if (threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+  grid_sum_last_block(s, part, ticket, out);
 }
 // x += sum_m y_m V_m   (y on the device, k terms)
 template <class TV>
@@ -267,21 +369,6 @@ template <class TA>
 __global__ void k_add(size_t n, const TA* __restrict__ a, double* __restrict__ x) {
   size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q < n) x[q] += (double)a[q];
-}
-// deterministic dot / squared norm of TV vectors, FP64 accumulation
-template <class TV>
-__global__ void k_dot_tv(size_t n, const TV* __restrict__ x, const TV* __restrict__ y, double* __restrict__ part) {
-  __shared__ double sh[kIB];
-  double s = 0.0;
-  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
-    s += (double)x[q] * (double)y[q];
-  sh[threadIdx.x] = s;
-  __syncthreads();
-  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
-    if (threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
 }  // namespace aerof
@@ -299,53 +386,61 @@ static void need_jac(aerof_gpu_ctx* c) {
 
 // Assemble the H1 operator at device state dU with device time steps ddt
 // (may be null).
-void jacobian_dev(aerof_gpu_ctx* c, const double* dU, const double* ddt, int precision) {
+// sizes of the sliced arrays (elements)
+static size_t sl_diag_size(const DeviceMesh& m) { return (size_t)m.nsl * 25 * 32; }
+static size_t sl_off_size(const DeviceMesh& m) { return std::max<size_t>((size_t)m.h_sptr.back() * 25 * 32, 1); }
+
+void jacobian_dev(aerof_gpu_ctx* c, const double* dU, const double* ddt, int precision, bool transposed) {
   DeviceMesh& m = c->mesh;
   Implicit& J = c->imp;
   const Gas g = make_gas(c->cfg.gamma);
   TimerScope tj(c, AEROF_T_FV_JAC);
   prim_dev(c, dU);
-  J.diagscr.ensure(25 * 2 * (size_t)m.E);
-  const int ge = grid_for(m.E, kIB), gn = grid_for(m.N, kIB);
+  const int gr = grid_for(16 * (size_t)m.N, kIB);
+  auto rows = [&](auto* off, auto* diag, auto kern) {
+    kern<<<gr, kIB, 0, c->stream>>>(m.N, m.E, m.F, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_node.p, m.nbr_edge.p, m.en.p,
+                                    m.P.p, m.vol.p, m.nf_ptr.p, m.nf_face.p, m.fcode.p, m.fnrm.p, ddt, m.sptr.p, off,
+                                    diag);
+    AEROF_LAUNCH_CHECK();
+  };
   if (precision == AEROF_PREC_FP32) {
     J.diag64.release(); J.off64.release(); J.dinv64.release();
-    J.diag32.alloc(25 * (size_t)m.N);
-    J.off32.alloc(25 * 2 * (size_t)m.E);
-    k_jac_edges<float><<<ge, kIB, 0, c->stream>>>(m.E, g, m.edges.p, m.edge_pos.p, m.en.p, m.P.p, m.vol.p, J.off32.p,
-                                                  J.diagscr.p);
-    AEROF_LAUNCH_CHECK();
-    k_jac_diag<float><<<gn, kIB, 0, c->stream>>>(m.N, m.F, g, m.Ubd.p, m.nbr_ptr.p, J.diagscr.p, m.nf_ptr.p,
-                                                 m.nf_face.p, m.fcode.p, m.fnrm.p, m.P.p, m.vol.p, ddt, J.diag32.p);
-    AEROF_LAUNCH_CHECK();
+    J.diag32.alloc(sl_diag_size(m));
+    J.off32.alloc(sl_off_size(m));
+    if (transposed) rows(J.off32.p, J.diag32.p, k_jac_rows<float, true>);
+    else rows(J.off32.p, J.diag32.p, k_jac_rows<float, false>);
   } else {
     J.diag32.release(); J.off32.release(); J.dinv32.release();
-    J.diag64.alloc(25 * (size_t)m.N);
-    J.off64.alloc(25 * 2 * (size_t)m.E);
-    k_jac_edges<double><<<ge, kIB, 0, c->stream>>>(m.E, g, m.edges.p, m.edge_pos.p, m.en.p, m.P.p, m.vol.p,
-                                                   J.off64.p, J.diagscr.p);
-    AEROF_LAUNCH_CHECK();
-    k_jac_diag<double><<<gn, kIB, 0, c->stream>>>(m.N, m.F, g, m.Ubd.p, m.nbr_ptr.p, J.diagscr.p, m.nf_ptr.p,
-                                                  m.nf_face.p, m.fcode.p, m.fnrm.p, m.P.p, m.vol.p, ddt, J.diag64.p);
-    AEROF_LAUNCH_CHECK();
+    J.diag64.alloc(sl_diag_size(m));
+    J.off64.alloc(sl_off_size(m));
+    if (transposed) rows(J.off64.p, J.diag64.p, k_jac_rows<double, true>);
+    else rows(J.off64.p, J.diag64.p, k_jac_rows<double, false>);
   }
   J.precision = precision;
+  J.transposed = transposed;
   J.prec_ready = false;
 }
 
+// products with H1 (trans = 0) or H1^T (trans = 1); the stored blocks may
+// hold either, so the kernel reads them plainly or transposed
 template <class TI, class TO>
 void matvec_t(aerof_gpu_ctx* c, const TI* p, TO* y, int trans) {
   DeviceMesh& m = c->mesh;
   TimerScope tm(c, AEROF_T_KSP_MATVEC);
   Implicit& J = c->imp;
   const int gn = grid_for(m.N, kIB);
+  const bool tr = (trans != 0) != J.transposed;
+  auto go = [&](auto kern, auto* diag, auto* off) {
+    kern<<<gn, kIB, 0, c->stream>>>(m.N, m.nbr_ptr.p, m.nbr_tpos.p, m.sptr.p, m.scol.p, diag, off, p, y);
+    AEROF_LAUNCH_CHECK();
+  };
   if (J.precision == AEROF_PREC_FP32) {
-    if (trans) k_spmv<float, true, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, m.nbr_ptr.p, m.nbr_node.p, m.nbr_tpos.p, J.diag32.p, J.off32.p, p, y);
-    else k_spmv<float, false, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, m.nbr_ptr.p, m.nbr_node.p, m.nbr_tpos.p, J.diag32.p, J.off32.p, p, y);
+    if (tr) go(k_spmv<float, true, TI, TO>, J.diag32.p, J.off32.p);
+    else go(k_spmv<float, false, TI, TO>, J.diag32.p, J.off32.p);
   } else {
-    if (trans) k_spmv<double, true, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, m.nbr_ptr.p, m.nbr_node.p, m.nbr_tpos.p, J.diag64.p, J.off64.p, p, y);
-    else k_spmv<double, false, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, m.nbr_ptr.p, m.nbr_node.p, m.nbr_tpos.p, J.diag64.p, J.off64.p, p, y);
+    if (tr) go(k_spmv<double, true, TI, TO>, J.diag64.p, J.off64.p);
+    else go(k_spmv<double, false, TI, TO>, J.diag64.p, J.off64.p);
   }
-  AEROF_LAUNCH_CHECK();
 }
 void matvec_dev(aerof_gpu_ctx* c, const double* p, double* y, int trans) { matvec_t<double, double>(c, p, y, trans); }
 
@@ -358,10 +453,10 @@ int prec_setup_dev(aerof_gpu_ctx* c) {
   AEROF_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
   const int gn = grid_for(m.N, kIB);
   if (J.precision == AEROF_PREC_FP32) {
-    J.dinv32.alloc(25 * (size_t)m.N);
+    J.dinv32.alloc(sl_diag_size(m));
     k_bj_invert<float><<<gn, kIB, 0, c->stream>>>(m.N, J.diag32.p, J.dinv32.p, bad);
   } else {
-    J.dinv64.alloc(25 * (size_t)m.N);
+    J.dinv64.alloc(sl_diag_size(m));
     k_bj_invert<double><<<gn, kIB, 0, c->stream>>>(m.N, J.diag64.p, J.dinv64.p, bad);
   }
   AEROF_LAUNCH_CHECK();
@@ -372,16 +467,19 @@ int prec_setup_dev(aerof_gpu_ctx* c) {
   return h;
 }
 
+// z = D^-1 x or D^-T x; with transposed storage the inverted blocks are
+// those of D^T, so the roles swap
 template <class TI, class TO>
 void prec_apply_t(aerof_gpu_ctx* c, const TI* x, TO* z, int trans) {
   DeviceMesh& m = c->mesh;
   TimerScope tp(c, AEROF_T_KSP_OTHER);
   Implicit& J = c->imp;
   const int gn = grid_for(m.N, kIB);
+  const int tr = ((trans != 0) != J.transposed) ? 1 : 0;
   if (J.precision == AEROF_PREC_FP32)
-    k_bj_apply<float, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, J.dinv32.p, x, z, trans);
+    k_bj_apply<float, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, J.dinv32.p, x, z, tr);
   else
-    k_bj_apply<double, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, J.dinv64.p, x, z, trans);
+    k_bj_apply<double, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, J.dinv64.p, x, z, tr);
   AEROF_LAUNCH_CHECK();
 }
 void prec_apply_dev(aerof_gpu_ctx* c, const double* x, double* z, int trans) {
@@ -403,8 +501,12 @@ static int gmres_t(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int
   const size_t n = 5 * (size_t)m.N;
   const int gv = grid_for(n, kIB);
   cudaStream_t s = c->stream;
-  const size_t vbytes = (size_t)(numVec + 1) * n * sizeof(TV);
+  const size_t ld = (n + 63) / 64 * 64;  // basis leading dimension: 256-byte aligned vectors
+  const size_t vbytes = (size_t)(numVec + 1) * ld * sizeof(TV);
   J.basis.ensure((vbytes + 7) / 8);
+  J.ticket.ensure(1);
+  AEROF_CUDA(cudaMemsetAsync(J.ticket.p, 0, sizeof(unsigned), s));
+  unsigned* ticket = J.ticket.p;
   J.w.ensure((n * sizeof(TV) + 7) / 8);
   J.r.ensure((n * sizeof(TV) + 7) / 8);
   J.hcol.ensure((size_t)numVec + 2 + (size_t)numVec + 1);
@@ -423,10 +525,8 @@ static int gmres_t(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int
     if (trans) vjp_dev(c, exactU, pd, yy);
     else residual_forward(c, exactU, pd, nullptr, yy, false);
   };
-  auto norm2 = [&](const TV* v) -> double {
-    k_dot_tv<TV><<<kGB, kIB, 0, s>>>(n, v, v, part);
-    AEROF_LAUNCH_CHECK();
-    k_sum_partials<<<1, kIB, 0, s>>>(kGB, part, hd);
+  auto norm2 = [&](TV* v) -> double {
+    k_mgs<TV, true><<<kGB, kIB, 0, s>>>(n, nullptr, nullptr, nullptr, v, part, ticket, hd);
     AEROF_LAUNCH_CHECK();
     double h = 0.0;
     AEROF_CUDA(cudaMemcpyAsync(&h, hd, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -438,9 +538,7 @@ static int gmres_t(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int
       hcol(numVec + 2);
   auto h = [&](int i, int j) -> double& { return H[(size_t)i * numVec + j]; };
   auto dot_to = [&](const double* hp, const TV* vprev, const TV* vcur, double* out) {
-    k_mgs_step<TV><<<kGB, kIB, 0, s>>>(n, hp, vprev, vcur, w, part);
-    AEROF_LAUNCH_CHECK();
-    k_sum_partials<<<1, kIB, 0, s>>>(kGB, part, out);
+    k_mgs<TV, false><<<kGB, kIB, 0, s>>>(n, hp, vprev, vcur, w, part, ticket, out);
     AEROF_LAUNCH_CHECK();
   };
   int iter = 0, exitLoop = 0;
@@ -469,16 +567,14 @@ static int gmres_t(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int
     for (j = 0; j < numVec; ++j) {
       {
         TimerScope t(c, AEROF_T_KSP_OTHER);
-        prec_apply_t<TV, TV>(c, Vb + (size_t)j * n, r, trans);
+        prec_apply_t<TV, TV>(c, Vb + (size_t)j * ld, r, trans);
       }
       op(r, w);
       // h_ij = w . V_i ; w -= h_ij V_i   (i = 0..j), then ||w||
       TimerScope t(c, AEROF_T_KSP_OTHER);
       for (int i = 0; i <= j; ++i)
-        dot_to(i ? hd + (i - 1) : nullptr, i ? Vb + (size_t)(i - 1) * n : nullptr, Vb + (size_t)i * n, hd + i);
-      k_mgs_last<TV><<<kGB, kIB, 0, s>>>(n, hd + j, Vb + (size_t)j * n, w, part);
-      AEROF_LAUNCH_CHECK();
-      k_sum_partials<<<1, kIB, 0, s>>>(kGB, part, hd + j + 1);
+        dot_to(i ? hd + (i - 1) : nullptr, i ? Vb + (size_t)(i - 1) * ld : nullptr, Vb + (size_t)i * ld, hd + i);
+      k_mgs<TV, true><<<kGB, kIB, 0, s>>>(n, hd + j, Vb + (size_t)j * ld, nullptr, w, part, ticket, hd + j + 1);
       AEROF_LAUNCH_CHECK();
       AEROF_CUDA(cudaMemcpyAsync(hcol.data(), hd, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, s));
       AEROF_CUDA(cudaStreamSynchronize(s));
@@ -486,7 +582,7 @@ static int gmres_t(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int
       h(j + 1, j) = std::sqrt(hcol[j + 1]);
       const bool breakdown = (h(j + 1, j) == 0.0);
       if (!breakdown) {
-        k_scale<TV, TV><<<gv, kIB, 0, s>>>(n, 1. / h(j + 1, j), w, Vb + (size_t)(j + 1) * n);
+        k_scale<TV, TV><<<gv, kIB, 0, s>>>(n, 1. / h(j + 1, j), w, Vb + (size_t)(j + 1) * ld);
         AEROF_LAUNCH_CHECK();
       }
       for (int i = 0; i < j; ++i) {
@@ -516,10 +612,135 @@ static int gmres_t(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int
       y[i] /= h(i, i);
     }
     AEROF_CUDA(cudaMemcpyAsync(yd, y.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
-    k_combine<TV><<<gv, kIB, 0, s>>>(n, j + 1, yd, Vb, n, w);
+    k_combine<TV><<<gv, kIB, 0, s>>>(n, j + 1, yd, Vb, ld, w);
     AEROF_LAUNCH_CHECK();
     prec_apply_t<TV, TV>(c, w, r, trans);
     k_add<TV><<<gv, kIB, 0, s>>>(n, r, x);
+    AEROF_LAUNCH_CHECK();
+  } while (exitLoop == 0);
+  AEROF_CUDA(cudaStreamSynchronize(s));
+  if (final_res) *final_res = l2res;
+  return iter;
+}
+
+// Flexible GMRES(m) on the exact linearisation at exactU (J or J^T by
+// forward or reverse mode, FP64 vectors) whose preconditioner is itself a
+// solve: z_j = (approximately) H1^{-1} v_j by inner_its iterations of the
+// mixed-precision GMRES on the assembled first-order operator (FP32 blocks
+// and Krylov vectors, block-Jacobi).  The corrections are kept (Z) and
+// x = Z y, so the changing inner solve does not spoil the minimisation.
+// x = 0 on entry.  Returns outer iterations.
+static int fgmres_exact(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int maxits, double eps, int trans,
+                        double* final_res, const double* exactU, int inner_m, int inner_its, double inner_eps) {
+  DeviceMesh& m = c->mesh;
+  Implicit& J = c->imp;
+  const size_t n = 5 * (size_t)m.N;
+  const size_t ld = (n + 63) / 64 * 64;
+  const int gv = grid_for(n, kIB);
+  cudaStream_t s = c->stream;
+  J.fV.ensure((size_t)(numVec + 1) * ld);
+  J.fZ.ensure((size_t)numVec * ld);
+  J.fw.ensure(ld);
+  J.fr.ensure(ld);
+  J.fh.ensure((size_t)numVec + 2 + (size_t)numVec + 1);
+  J.ticket.ensure(1);
+  c->s.red.ensure(kGB);
+  double* V = J.fV.p;
+  double* Z = J.fZ.p;
+  double* w = J.fw.p;
+  double* r = J.fr.p;
+  double* hd = J.fh.p;
+  double* yd = J.fh.p + numVec + 2;
+  double* part = c->s.red.p;
+  unsigned* ticket = J.ticket.p;
+  AEROF_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), s));
+  auto op = [&](const double* p, double* y) {
+    TimerScope t(c, AEROF_T_KSP_MATVEC);
+    if (trans) vjp_dev(c, exactU, p, y);
+    else residual_forward(c, exactU, p, nullptr, y, false);
+  };
+  auto norm2 = [&](double* v) -> double {
+    k_mgs<double, true><<<kGB, kIB, 0, s>>>(n, nullptr, nullptr, nullptr, v, part, ticket, hd);
+    AEROF_LAUNCH_CHECK();
+    double h = 0.0;
+    AEROF_CUDA(cudaMemcpyAsync(&h, hd, sizeof(double), cudaMemcpyDeviceToHost, s));
+    AEROF_CUDA(cudaStreamSynchronize(s));
+    return std::sqrt(h);
+  };
+  AEROF_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
+  std::vector<double> H((size_t)(numVec + 1) * numVec, 0.0), cs(2 * (size_t)numVec), g(numVec + 1), y(numVec),
+      hcol(numVec + 2);
+  auto h = [&](int i, int j) -> double& { return H[(size_t)i * numVec + j]; };
+  int iter = 0, exitLoop = 0;
+  double target = 0.0, l2res = 0.0;
+  const double bnorm = norm2_dev(c, b, n);
+  do {
+    if (iter == 0) {
+      AEROF_CUDA(cudaMemcpyAsync(r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    } else {
+      op(x, w);
+      k_sub<double, double><<<gv, kIB, 0, s>>>(n, b, w, r);
+      AEROF_LAUNCH_CHECK();
+    }
+    const double beta = norm2(r);
+    if (iter == 0) target = eps * bnorm;
+    if (beta == 0.0) { if (final_res) *final_res = 0.0; return iter; }
+    k_scale<double, double><<<gv, kIB, 0, s>>>(n, 1.0 / beta, r, V);
+    AEROF_LAUNCH_CHECK();
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int j;
+    for (j = 0; j < numVec; ++j) {
+      double* zj = Z + (size_t)j * ld;
+      gmres_t<float>(c, V + (size_t)j * ld, zj, inner_m, inner_its, inner_eps, trans, nullptr, nullptr);
+      op(zj, w);
+      TimerScope t(c, AEROF_T_KSP_OTHER);
+      for (int i = 0; i <= j; ++i) {
+        k_mgs<double, false><<<kGB, kIB, 0, s>>>(n, i ? hd + (i - 1) : nullptr, i ? V + (size_t)(i - 1) * ld : nullptr,
+                                                 V + (size_t)i * ld, w, part, ticket, hd + i);
+        AEROF_LAUNCH_CHECK();
+      }
+      k_mgs<double, true><<<kGB, kIB, 0, s>>>(n, hd + j, V + (size_t)j * ld, nullptr, w, part, ticket, hd + j + 1);
+      AEROF_LAUNCH_CHECK();
+      AEROF_CUDA(cudaMemcpyAsync(hcol.data(), hd, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, s));
+      AEROF_CUDA(cudaStreamSynchronize(s));
+      for (int i = 0; i <= j; ++i) h(i, j) = hcol[i];
+      h(j + 1, j) = std::sqrt(hcol[j + 1]);
+      const bool breakdown = (h(j + 1, j) == 0.0);
+      if (!breakdown) {
+        k_scale<double, double><<<gv, kIB, 0, s>>>(n, 1. / h(j + 1, j), w, V + (size_t)(j + 1) * ld);
+        AEROF_LAUNCH_CHECK();
+      }
+      for (int i = 0; i < j; ++i) {
+        double hj = cs[2 * i + 1] * h(i, j) + cs[2 * i] * h(i + 1, j);
+        double hjp1 = -cs[2 * i] * h(i, j) + cs[2 * i + 1] * h(i + 1, j);
+        h(i, j) = hj; h(i + 1, j) = hjp1;
+      }
+      if (h(j, j) * h(j, j) == 0.0) { cs[2 * j + 1] = 0.0; cs[2 * j] = 1.0; }
+      else {
+        double coef = 1.0 / std::sqrt(h(j, j) * h(j, j) + h(j + 1, j) * h(j + 1, j));
+        cs[2 * j + 1] = std::sqrt(h(j, j) * h(j, j)) * coef;
+        cs[2 * j] = cs[2 * j + 1] * h(j + 1, j) / h(j, j);
+      }
+      h(j, j) = cs[2 * j + 1] * h(j, j) + cs[2 * j] * h(j + 1, j);
+      h(j + 1, j) = 0.0;
+      g[j + 1] = -cs[2 * j] * g[j];
+      g[j] = cs[2 * j + 1] * g[j];
+      ++iter;
+      if (breakdown) { exitLoop = 1; break; }
+      l2res = std::fabs(g[j + 1]);
+      if (l2res <= target || iter >= maxits) { exitLoop = 1; break; }
+    }
+    if (j == numVec) --j;
+    for (int i = j; i >= 0; --i) {
+      y[i] = g[i];
+      for (int k = j; k >= i + 1; --k) y[i] -= h(i, k) * y[k];
+      y[i] /= h(i, i);
+    }
+    AEROF_CUDA(cudaMemcpyAsync(yd, y.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
+    k_combine<double><<<gv, kIB, 0, s>>>(n, j + 1, yd, Z, ld, w);
+    AEROF_LAUNCH_CHECK();
+    k_add<double><<<gv, kIB, 0, s>>>(n, w, x);
     AEROF_LAUNCH_CHECK();
   } while (exitLoop == 0);
   AEROF_CUDA(cudaStreamSynchronize(s));
@@ -546,7 +767,7 @@ extern "C" int aerof_gpu_jacobian(aerof_gpu_ctx* c, const double* U, const doubl
     const size_t N = c->mesh.N;
     const double* dU = in_dev(c, U, 5 * N, c->s.Ustage);
     const double* ddt = dt ? in_dev(c, dt, N, c->s.Vstage) : nullptr;
-    jacobian_dev(c, dU, ddt, precision);
+    jacobian_dev(c, dU, ddt, precision, false);
     AEROF_CUDA(cudaStreamSynchronize(c->stream));
     return AEROF_OK;
   });
@@ -558,7 +779,7 @@ extern "C" int aerof_gpu_get_jacobian(aerof_gpu_ctx* c, double* A) {
     if (!A) return AEROF_EINVAL;
     DeviceMesh& m = c->mesh;
     Implicit& J = c->imp;
-    const size_t nd = 25 * (size_t)m.N, no = 25 * 2 * (size_t)m.E;
+    const size_t nd = sl_diag_size(m), no = sl_off_size(m);
     std::vector<double> diag(nd), off(no);
     if (J.precision == AEROF_PREC_FP32) {
       std::vector<float> d32(nd), o32(no);
@@ -572,13 +793,39 @@ extern "C" int aerof_gpu_get_jacobian(aerof_gpu_ctx* c, double* A) {
       AEROF_CUDA(cudaMemcpyAsync(off.data(), J.off64.p, no * 8, cudaMemcpyDeviceToHost, c->stream));
       AEROF_CUDA(cudaStreamSynchronize(c->stream));
     }
+    // MvpMat layout: a[N] diagonal blocks, then per edge l the blocks
+    // (i, j) and (j, i); the sliced storage is read back (transposed when
+    // it holds H1^T)
+    const std::vector<int>& sp = m.h_sptr;
+    const std::vector<int>& np = m.h_nbr_ptr;
+    const bool T = J.transposed;
+    auto el = [&](int e) { return T ? 5 * (e % 5) + e / 5 : e; };
+    for (int r = 0; r < m.N; ++r)
+      for (int e = 0; e < 25; ++e) A[25 * (size_t)r + e] = diag[((size_t)(r >> 5) * 25 + el(e)) * 32 + (r & 31)];
+    auto block = [&](int r, int p, double* dst) {
+      // block at CSR position p of row r of H1; with H1^T stored it is the
+      // transpose of the mirrored block
+      for (int e = 0; e < 25; ++e) dst[e] = off[(((size_t)sp[r >> 5] + (p - np[r])) * 25 + e) * 32 + (r & 31)];
+    };
     std::vector<int2> epos(m.E);
     AEROF_CUDA(cudaMemcpyAsync(epos.data(), m.edge_pos.p, sizeof(int2) * m.E, cudaMemcpyDeviceToHost, c->stream));
     AEROF_CUDA(cudaStreamSynchronize(c->stream));
-    std::copy(diag.begin(), diag.end(), A);
+    const size_t nA = 25 * (size_t)m.N;
+    double tmp[25];
     for (int l = 0; l < m.E; ++l) {
-      std::copy(&off[25 * (size_t)epos[l].x], &off[25 * (size_t)epos[l].x] + 25, A + nd + 50 * (size_t)l);
-      std::copy(&off[25 * (size_t)epos[l].y], &off[25 * (size_t)epos[l].y] + 25, A + nd + 50 * (size_t)l + 25);
+      const int i = m.h_edges[2 * (size_t)l], j = m.h_edges[2 * (size_t)l + 1];
+      double* aij = A + nA + 50 * (size_t)l;
+      double* aji = aij + 25;
+      if (!T) {
+        block(i, epos[l].x, aij);
+        block(j, epos[l].y, aji);
+      } else {
+        // stored row i, position of j holds A_ji^T; row j, position of i holds A_ij^T
+        block(i, epos[l].x, tmp);
+        for (int e = 0; e < 25; ++e) aji[e] = tmp[el(e)];
+        block(j, epos[l].y, tmp);
+        for (int e = 0; e < 25; ++e) aij[e] = tmp[el(e)];
+      }
     }
     return AEROF_OK;
   });
@@ -685,7 +932,7 @@ extern "C" int aerof_gpu_newton(aerof_gpu_ctx* c, double* U, const aerof_newton_
       if (k > 0) cfl = std::min(std::max(cfl * std::pow(rel_prev / rel, p->ser), p->cfl_min), p->cfl_max);
       rel_prev = rel;
       timestep_dev(c, dU, cfl, dt);
-      jacobian_dev(c, dU, dt, p->precision);
+      jacobian_dev(c, dU, dt, p->precision, false);
       if (int nb = prec_setup_dev(c)) {
         c->last_error = std::to_string(nb) + " singular diagonal block(s) at Newton step " + std::to_string(k);
         return AEROF_ESINGULAR;
@@ -720,10 +967,11 @@ extern "C" int aerof_gpu_newton(aerof_gpu_ctx* c, double* U, const aerof_newton_
 // solveT, KspSolver.C:752-915).  Preconditioner: block-Jacobi of the
 // first-order H1 operator at U without time term, in FP64.
 extern "C" int aerof_gpu_linearized_solve(aerof_gpu_ctx* c, const double* U, const double* b, double* x, int krylov,
-                                          int maxits, double eps, int transpose, int* its, double* res) {
+                                          int maxits, double eps, int transpose, int inner_its, int* its,
+                                          double* res) {
   return guard(c, [&]() -> int {
     need_mesh_or_throw(c);
-    if (!U || !b || !x || krylov < 1 || maxits < 1 || !(eps >= 0.0)) return AEROF_EINVAL;
+    if (!U || !b || !x || krylov < 1 || maxits < 1 || !(eps >= 0.0) || inner_its < 0) return AEROF_EINVAL;
     const size_t n = 5 * (size_t)c->mesh.N;
     c->imp.t.ensure(n);
     const double* dU0 = in_dev(c, U, n, c->s.Ustage);
@@ -732,13 +980,15 @@ extern "C" int aerof_gpu_linearized_solve(aerof_gpu_ctx* c, const double* U, con
     const double* dU = c->imp.t.p;
     const double* db = in_dev(c, b, n, c->s.Vstage);
     double* dx = out_dev(c, x, n, c->s.Rstage);
-    jacobian_dev(c, dU, nullptr, AEROF_PREC_FP64);
+    jacobian_dev(c, dU, nullptr, inner_its ? AEROF_PREC_FP32 : AEROF_PREC_FP64, inner_its && transpose);
     if (int nb = prec_setup_dev(c)) {
       c->last_error = std::to_string(nb) + " singular diagonal block(s)";
       return AEROF_ESINGULAR;
     }
     double r = 0.0;
-    int it = gmres_dev(c, db, dx, krylov, maxits, eps, transpose, &r, dU);
+    const int it = inner_its ? fgmres_exact(c, db, dx, krylov, maxits, eps, transpose, &r, dU, std::min(inner_its, 30),
+                                            inner_its, 1e-3)
+                             : gmres_dev(c, db, dx, krylov, maxits, eps, transpose, &r, dU);
     out_finish(c, x, dx, n);
     if (its) *its = it;
     if (res) *res = r;

@@ -178,9 +178,12 @@ static void build_host(int N, int T, int F, const int* tets, const int* faces, H
 // Morton (Z-order) renumbering of the nodes and the per-block edge lists of
 // the blocked residual kernel.  Integer work only; deterministic.
 struct HostBlocked {
-  std::vector<int> n2o, o2n, nb2_ptr, nb2_node, bsrc, beptr, lptr, lidx, xslot, xin_ptr, xin_slot;
+  std::vector<int> n2o, o2n, nb2_ptr, nb2_node, bsrc, beptr, lptr, lidx, xslot, xin_ptr, hptr, hnode,
+      hfptr, hfnode;
+  std::vector<unsigned short> lnb;
+  std::vector<ushort2> bl;
   std::vector<int2> bedges;
-  int nblk = 0, maxE = 0, nX = 0;
+  int nblk = 0, maxE = 0, nX = 0, maxH = 0, maxL = 0, maxHf = 0;
 };
 
 static inline uint64_t spread3(uint64_t v) {
@@ -252,7 +255,7 @@ static void build_blocked(int N, int E, int NB, const double* X, const std::vect
     b.nb2_ptr[f + 1]++; b.nb2_ptr[sd + 1]++;
     b.lptr[f + 1]++;
     if (sd / NB == f / NB) b.lptr[sd + 1]++;
-    else { b.xslot[q] = b.nX++; b.xin_ptr[sd + 1]++; }
+    else { b.xslot[q] = 0; b.nX++; b.xin_ptr[sd + 1]++; }
   }
   for (int n = 0; n < N; ++n) {
     b.nb2_ptr[n + 1] += b.nb2_ptr[n];
@@ -261,7 +264,6 @@ static void build_blocked(int N, int E, int NB, const double* X, const std::vect
   }
   b.nb2_node.resize(2 * (size_t)E);
   b.lidx.resize(b.lptr[N]);
-  b.xin_slot.resize(b.nX);
   std::vector<int> pn(b.nb2_ptr.begin(), b.nb2_ptr.end() - 1), pl(b.lptr.begin(), b.lptr.end() - 1),
       px(b.xin_ptr.begin(), b.xin_ptr.end() - 1);
   for (int q = 0; q < E; ++q) {
@@ -270,8 +272,61 @@ static void build_blocked(int N, int E, int NB, const double* X, const std::vect
     b.nb2_node[pn[f]++] = sd;
     b.nb2_node[pn[sd]++] = f;
     b.lidx[pl[f]++] = slot;
+    // spill slots numbered by destination node (then edge), so the
+    // destination's incoming fluxes are contiguous
     if (b.xslot[q] < 0) b.lidx[pl[sd]++] = (int)((unsigned)slot | 0x80000000u);
-    else b.xin_slot[px[sd]++] = b.xslot[q];
+    else b.xslot[q] = px[sd]++;
+  }
+  // halo of every block (neighbours outside it, ascending) and each
+  // neighbour-CSR entry as a slot of the block's staged node set: slots
+  // [0, nn) are the block's own nodes, [nn, nn + halo) its halo.
+  b.hptr.assign(b.nblk + 1, 0);
+  b.hnode.clear();
+  b.lnb.assign(2 * (size_t)E, 0);
+  b.maxH = 0;
+  std::vector<int> h;
+  for (int blk = 0; blk < b.nblk; ++blk) {
+    const int n0 = blk * NB, n1 = std::min(N, n0 + NB), nn = n1 - n0;
+    h.clear();
+    for (int p = b.nb2_ptr[n0]; p < b.nb2_ptr[n1]; ++p) {
+      const int j = b.nb2_node[p];
+      if (j < n0 || j >= n1) h.push_back(j);
+    }
+    std::sort(h.begin(), h.end());
+    h.erase(std::unique(h.begin(), h.end()), h.end());
+    if (nn + h.size() > 65535) throw ApiError{AEROF_EINVAL, "a node block's halo exceeds 65535 nodes"};
+    b.maxH = std::max(b.maxH, (int)h.size());
+    b.maxL = std::max(b.maxL, b.nb2_ptr[n1] - b.nb2_ptr[n0]);
+    for (int p = b.nb2_ptr[n0]; p < b.nb2_ptr[n1]; ++p) {
+      const int j = b.nb2_node[p];
+      b.lnb[p] = (unsigned short)(j >= n0 && j < n1 ? j - n0
+                                                    : nn + (std::lower_bound(h.begin(), h.end(), j) - h.begin()));
+    }
+    b.hnode.insert(b.hnode.end(), h.begin(), h.end());
+    b.hptr[blk + 1] = (int)b.hnode.size();
+  }
+  // forward halo of every block (second endpoints of its edges lying in
+  // later blocks, ascending) and each edge's endpoints as staged slots
+  b.hfptr.assign(b.nblk + 1, 0);
+  b.hfnode.clear();
+  b.bl.resize(E);
+  b.maxHf = 0;
+  for (int blk = 0; blk < b.nblk; ++blk) {
+    const int n0 = blk * NB, n1 = std::min(N, n0 + NB), nn = n1 - n0;
+    h.clear();
+    for (int q = b.beptr[blk]; q < b.beptr[blk + 1]; ++q)
+      if (b.bedges[q].y >= n1) h.push_back(b.bedges[q].y);
+    std::sort(h.begin(), h.end());
+    h.erase(std::unique(h.begin(), h.end()), h.end());
+    if (nn + h.size() > 65535) throw ApiError{AEROF_EINVAL, "a node block's forward halo exceeds 65535 nodes"};
+    b.maxHf = std::max(b.maxHf, (int)h.size());
+    for (int q = b.beptr[blk]; q < b.beptr[blk + 1]; ++q) {
+      const int j = b.bedges[q].y;
+      const int lj = j < n1 ? j - n0 : nn + (int)(std::lower_bound(h.begin(), h.end(), j) - h.begin());
+      b.bl[q] = make_ushort2((unsigned short)(b.bedges[q].x - n0), (unsigned short)lj);
+    }
+    b.hfnode.insert(b.hfnode.end(), h.begin(), h.end());
+    b.hfptr[blk + 1] = (int)b.hfnode.size();
   }
 }
 
@@ -418,21 +473,56 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
       }
       HostBlocked hb;
       build_blocked(N, E, m.NB, X, h.edges, hb);
-      m.nblk = hb.nblk; m.maxE = hb.maxE; m.nX = hb.nX;
+      m.nblk = hb.nblk; m.maxE = hb.maxE; m.nX = hb.nX; m.maxH = hb.maxH; m.maxL = hb.maxL; m.maxHf = hb.maxHf;
+      m.hfptr.upload(hb.hfptr.data(), hb.hfptr.size(), s);
+      if (hb.hfnode.empty()) m.hfnode.alloc(1);
+      else m.hfnode.upload(hb.hfnode.data(), hb.hfnode.size(), s);
+      if (hb.bl.empty()) m.bl.alloc(1);
+      else m.bl.upload(hb.bl.data(), hb.bl.size(), s);
+      m.hptr.upload(hb.hptr.data(), hb.hptr.size(), s);
+      if (hb.hnode.empty()) m.hnode.alloc(1);
+      else m.hnode.upload(hb.hnode.data(), hb.hnode.size(), s);
+      if (hb.lnb.empty()) m.lnb.alloc(1);
+      else m.lnb.upload(hb.lnb.data(), hb.lnb.size(), s);
       m.n2o.upload(hb.n2o.data(), N, s);
       m.o2n.upload(hb.o2n.data(), N, s);
       m.nb2_ptr.upload(hb.nb2_ptr.data(), N + 1, s);
       m.nb2_node.upload(hb.nb2_node.data(), hb.nb2_node.size(), s);
-      m.bedges.upload(hb.bedges.data(), (size_t)E, s);
       m.bsrc.upload(hb.bsrc.data(), (size_t)E, s);
       m.beptr.upload(hb.beptr.data(), hb.beptr.size(), s);
       m.lptr.upload(hb.lptr.data(), N + 1, s);
-      m.lidx.upload(hb.lidx.data(), std::max<size_t>(hb.lidx.size(), 1), s);
+      if (hb.lidx.empty()) m.lidx.alloc(1);
+      else m.lidx.upload(hb.lidx.data(), hb.lidx.size(), s);
       m.xslot.upload(hb.xslot.data(), (size_t)E, s);
       m.xin_ptr.upload(hb.xin_ptr.data(), N + 1, s);
-      if (hb.nX) m.xin_slot.upload(hb.xin_slot.data(), hb.xin_slot.size(), s);
-      else m.xin_slot.alloc(1);
       AEROF_CUDA(cudaStreamSynchronize(s));  // host vectors die at scope end
+    }
+    // sliced layout of the implicit operator
+    {
+      const int nsl = (N + 31) / 32;
+      std::vector<int> sp(nsl + 1, 0);
+      for (int sl = 0; sl < nsl; ++sl) {
+        int ks = 0;
+        for (int r = 32 * sl; r < std::min(N, 32 * sl + 32); ++r) ks = std::max(ks, h.nbr_ptr[r + 1] - h.nbr_ptr[r]);
+        sp[sl + 1] = sp[sl] + ks;
+      }
+      std::vector<int> sc((size_t)sp[nsl] * 32);
+      for (int r = 0; r < N; ++r) {
+        const int sl = r >> 5, l = r & 31, cnt = h.nbr_ptr[r + 1] - h.nbr_ptr[r];
+        for (int k = 0; k < sp[sl + 1] - sp[sl]; ++k)
+          sc[((size_t)sp[sl] + k) * 32 + l] = k < cnt ? h.nbr_node[h.nbr_ptr[r] + k] : r;
+      }
+      for (int r = N; r < 32 * nsl; ++r) {
+        const int sl = r >> 5, l = r & 31;
+        for (int k = 0; k < sp[sl + 1] - sp[sl]; ++k) sc[((size_t)sp[sl] + k) * 32 + l] = 32 * sl;
+      }
+      m.nsl = nsl;
+      m.sptr.upload(sp.data(), sp.size(), s);
+      if (sc.empty()) m.scol.alloc(1);
+      else m.scol.upload(sc.data(), sc.size(), s);
+      AEROF_CUDA(cudaStreamSynchronize(s));
+      m.h_sptr.swap(sp);
+      m.h_nbr_ptr = h.nbr_ptr;
     }
     m.h_edges.swap(h.edges);
     compute_geometry(c);

@@ -303,16 +303,14 @@ AEROF_HD void post_dVdU(const Gas& g, const double* V, const double* mat, double
 // roejac6.f:1-316 (type 0, prec 0 -> beta 1, dissipation coefficient 1):
 // approximate Jacobian of the Roe flux w.r.t. the conservative state Ug,
 // sw = +1 adds the dissipation matrix, sw = -1 subtracts it.
-AEROF_HD void roe_jac(const Gas& g, double n0, double n1, double n2, const double* Ug, const double* Ud,
-                      double sw, double* jac) {
+//
+// Convective part of roejac6: the exact flux Jacobian H(U) of state U along
+// the unit normal n (roejac6.f, first block).
+AEROF_HD void roe_jac_H(const Gas& g, const double* n, const double* Ug, double* H) {
   const double gam = g.gam, gam1 = g.gam1;
-  double rnorm = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
-  double invnorm = 1.0 / rnorm;
-  double n[3] = {n0 * invnorm, n1 * invnorm, n2 * invnorm};
-  double VdotN = Ug[1] * n[0] + Ug[2] * n[1] + Ug[3] * n[2];
-  double qir = 0.5 * (Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3]);
-  double enth = (gam * Ug[4] + gam1 * Ug[0] * qir) / (gam1 * Ug[0]);
-  double H[25];
+  const double VdotN = Ug[1] * n[0] + Ug[2] * n[1] + Ug[3] * n[2];
+  const double qir = 0.5 * (Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3]);
+  const double enth = (gam * Ug[4] + gam1 * Ug[0] * qir) / (gam1 * Ug[0]);
   H[0] = 0.0; H[1] = n[0]; H[2] = n[1]; H[3] = n[2]; H[4] = 0.0;
   H[5] = gam1 * n[0] * qir - Ug[1] * VdotN;
   H[6] = (1.0 - gam1) * n[0] * Ug[1] + VdotN;
@@ -334,7 +332,14 @@ AEROF_HD void roe_jac(const Gas& g, double n0, double n1, double n2, const doubl
   H[22] = enth * n[1] - gam1 * Ug[2] * VdotN;
   H[23] = enth * n[2] - gam1 * Ug[3] * VdotN;
   H[24] = (1.0 + gam1) * VdotN;
-  // Roe average
+}
+
+// Dissipation part of roejac6: |A| at the Roe average of the two states,
+// written through its eigenvectors (roejac6.f, second block).  The Roe
+// average is symmetric in (Ug, Ud), bit for bit (every sum of the two sides
+// is a commutative two-term addition), so one D serves both endpoints.
+AEROF_HD void roe_jac_D(const Gas& g, const double* n, const double* Ug, const double* Ud, double* D) {
+  const double gam1 = g.gam1;
   double squsr1 = sqrt(Ug[0]), squsr2 = sqrt(Ud[0]);
   double ener1 = Ug[4] / gam1 + 0.5 * Ug[0] * (Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3]);
   double ener2 = Ud[4] / gam1 + 0.5 * Ud[0] * (Ud[1] * Ud[1] + Ud[2] * Ud[2] + Ud[3] * Ud[3]);
@@ -343,9 +348,9 @@ AEROF_HD void roe_jac(const Gas& g, double n0, double n1, double n2, const doubl
   double uar3 = (squsr1 * Ug[2] + squsr2 * Ud[2]) * usro;
   double uar4 = (squsr1 * Ug[3] + squsr2 * Ud[3]) * usro;
   double uar5 = ((ener1 + Ug[4]) / squsr1 + (ener2 + Ud[4]) / squsr2) * usro;
-  enth = uar5;
-  VdotN = n[0] * uar2 + n[1] * uar3 + n[2] * uar4;
-  qir = 0.5 * (uar2 * uar2 + uar3 * uar3 + uar4 * uar4);
+  const double enth = uar5;
+  const double VdotN = n[0] * uar2 + n[1] * uar3 + n[2] * uar4;
+  const double qir = 0.5 * (uar2 * uar2 + uar3 * uar3 + uar4 * uar4);
   double cr = sqrt(gam1 * (uar5 - qir));
   double crsq = cr * cr;
   double gc = gam1 / crsq;
@@ -386,27 +391,37 @@ AEROF_HD void roe_jac(const Gas& g, double n0, double n1, double n2, const doubl
   tmw[22] = gam1 * uar3 * rRT / tRT + crsq * n[1] / tRT;
   tmw[23] = gam1 * uar4 * rRT / tRT + crsq * n[2] / tRT;
   tmw[24] = -gam1 * rRT / tRT;
-  const double half_rn = 0.5 * rnorm;
 #pragma unroll
   for (int j = 0; j < 5; ++j) {
     double t0 = tmw[j], t1 = tmw[5 + j], t2 = tmw[10 + j], t3 = tmw[15 + j], t4 = tmw[20 + j];
-    double d0 = vp1 * (n[0] * t0 + n[1] * t1 + n[2] * t2) + vp4 * usc2 * t3 + vp5 * usc2 * t4;
-    double d1 = vp1 * (n[0] * uar2 * t0 + (n[1] * uar2 - n[2]) * t1 + (n[2] * uar2 + n[1]) * t2) +
-                vp4 * (usc2 * (uar2 + rRT * n[0])) * t3 + vp5 * (usc2 * (uar2 + sRT * n[0])) * t4;
-    double d2 = vp1 * (n[1] * uar3 * t1 + (n[0] * uar3 + n[2]) * t0 + (n[2] * uar3 - n[0]) * t2) +
+    D[j] = vp1 * (n[0] * t0 + n[1] * t1 + n[2] * t2) + vp4 * usc2 * t3 + vp5 * usc2 * t4;
+    D[5 + j] = vp1 * (n[0] * uar2 * t0 + (n[1] * uar2 - n[2]) * t1 + (n[2] * uar2 + n[1]) * t2) +
+               vp4 * (usc2 * (uar2 + rRT * n[0])) * t3 + vp5 * (usc2 * (uar2 + sRT * n[0])) * t4;
+    D[10 + j] = vp1 * (n[1] * uar3 * t1 + (n[0] * uar3 + n[2]) * t0 + (n[2] * uar3 - n[0]) * t2) +
                 vp4 * (usc2 * (uar3 + rRT * n[1])) * t3 + vp5 * (usc2 * (uar3 + sRT * n[1])) * t4;
-    double d3 = vp1 * (n[2] * uar4 * t2 + (n[0] * uar4 - n[1]) * t0 + (n[1] * uar4 + n[0]) * t1) +
+    D[15 + j] = vp1 * (n[2] * uar4 * t2 + (n[0] * uar4 - n[1]) * t0 + (n[1] * uar4 + n[0]) * t1) +
                 vp4 * (usc2 * (uar4 + rRT * n[2])) * t3 + vp5 * (usc2 * (uar4 + sRT * n[2])) * t4;
-    double d4 = vp1 * ((n[0] * qir + (n[2] * uar3 - n[1] * uar4)) * t0 +
+    D[20 + j] = vp1 * ((n[0] * qir + (n[2] * uar3 - n[1] * uar4)) * t0 +
                        (n[1] * qir + (n[0] * uar4 - n[2] * uar2)) * t1 +
                        (n[2] * qir + (n[1] * uar2 - n[0] * uar3)) * t2) +
                 vp4 * (usc2 * (enth + VdotN * rRT)) * t3 + vp5 * (usc2 * (enth + VdotN * sRT)) * t4;
-    jac[j] = (H[j] + sw * d0) * half_rn;
-    jac[5 + j] = (H[5 + j] + sw * d1) * half_rn;
-    jac[10 + j] = (H[10 + j] + sw * d2) * half_rn;
-    jac[15 + j] = (H[15 + j] + sw * d3) * half_rn;
-    jac[20 + j] = (H[20 + j] + sw * d4) * half_rn;
   }
+}
+
+// jac = (H(Ug) + sw |A|_Roe) |n| / 2: the derivative of the Roe flux with
+// respect to the first state (sw = +1) or, called with the states swapped,
+// the second (sw = -1).
+AEROF_HD void roe_jac(const Gas& g, double n0, double n1, double n2, const double* Ug, const double* Ud,
+                      double sw, double* jac) {
+  double rnorm = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+  double invnorm = 1.0 / rnorm;
+  double n[3] = {n0 * invnorm, n1 * invnorm, n2 * invnorm};
+  double H[25], D[25];
+  roe_jac_H(g, n, Ug, H);
+  roe_jac_D(g, n, Ug, Ud, D);
+  const double half_rn = 0.5 * rnorm;
+#pragma unroll
+  for (int k = 0; k < 25; ++k) jac[k] = (H[k] + sw * D[k]) * half_rn;
 }
 
 // Face blocks: FluxFcnFD<5>::computeJacobian (FluxFcnBase.h:112-159) for the

@@ -8,6 +8,7 @@
 // the order the reference's lexicographic edge loop visits them,
 // Edge.C:391-435, SubDomain.C:341-370), then its boundary faces in face
 // order (Face.C:1185-1215).  No floating-point atomics are used.
+#include <cstdlib>
 #include <mutex>
 
 #include "common.cuh"
@@ -39,9 +40,10 @@ __global__ void k_setV(int N, const double* __restrict__ V, double* __restrict__
   for (int k = 0; k < 5; ++k) P[8 * (size_t)i + k] = V[5 * (size_t)i + k];
 }
 
-// Least-squares gradients, one thread per node gathering its neighbours in
-// ascending order: ddV_i = sum_j W_i(X_j - X_i) (V_j - V_i).  Two neighbour
-// records (64 B each, four 16 B loads) are fetched before either is used.
+// Least-squares gradients, ddV_i = sum_j W_i(X_j - X_i) (V_j - V_i), with
+// four lanes per node: lane r of a node's group takes the neighbours at
+// positions r, r+4, ... of the node's ascending neighbour list, then the
+// four partial sums are added in a fixed tree (lanes 0+1, 2+3, then both).
 __device__ __forceinline__ void load_rec(const double* __restrict__ P, int j, double* r) {
   const double2* q = reinterpret_cast<const double2*>(P + 8 * (size_t)j);
 #pragma unroll
@@ -63,43 +65,188 @@ __device__ __forceinline__ void grad_acc(const double* w, const double* vi, cons
     gz[k] += W2 * dv;
   }
 }
-__global__ void k_grad(int N, const double* __restrict__ P, const double* __restrict__ lsqW, const int* __restrict__ nbr_ptr,
-       const int* __restrict__ nbr_node, const int* __restrict__ tag, double* __restrict__ G) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  double w[6];
+__global__ void __launch_bounds__(256) k_grad(int N, const double* __restrict__ P, const double* __restrict__ lsqW,
+                                              const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_node,
+                                              const int* __restrict__ tag, double* __restrict__ G) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t >> 2, r = t & 3;
+  const bool act = i < N;
+  double g[15];
 #pragma unroll
-  for (int k = 0; k < 6; ++k) w[k] = lsqW[(size_t)k * N + i];
-  double pi[8];
-  load_rec(P, i, pi);
-  double gx[5] = {0, 0, 0, 0, 0}, gy[5] = {0, 0, 0, 0, 0}, gz[5] = {0, 0, 0, 0, 0};
-  int p = nbr_ptr[i];
-  const int p1 = nbr_ptr[i + 1];
-  for (; p + 1 < p1; p += 2) {
-    double pa[8], pb[8];
-    const int ja = nbr_node[p], jb = nbr_node[p + 1];
-    load_rec(P, ja, pa);
-    load_rec(P, jb, pb);
-    grad_acc(w, pi, pi + 5, pa, gx, gy, gz);
-    grad_acc(w, pi, pi + 5, pb, gx, gy, gz);
+  for (int k = 0; k < 15; ++k) g[k] = 0.0;
+  if (act) {
+    double w[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) w[k] = lsqW[(size_t)k * N + i];
+    double pi[8];
+    load_rec(P, i, pi);
+    const int p1 = nbr_ptr[i + 1];
+    for (int p = nbr_ptr[i] + r; p < p1; p += 4) {
+      double pj[8];
+      load_rec(P, nbr_node[p], pj);
+      grad_acc(w, pi, pi + 5, pj, g, g + 5, g + 10);
+    }
   }
-  if (p < p1) {
-    double pa[8];
-    load_rec(P, nbr_node[p], pa);
-    grad_acc(w, pi, pi + 5, pa, gx, gy, gz);
+  // fixed-order combination of the four partial sums
+#pragma unroll
+  for (int k = 0; k < 15; ++k) {
+    g[k] += __shfl_xor_sync(0xffffffffu, g[k], 1);
+    g[k] += __shfl_xor_sync(0xffffffffu, g[k], 2);
   }
+  if (!act) return;
   const bool zero = tag && tag[i];
-  double2* gi = reinterpret_cast<double2*>(G + 16 * (size_t)i);
-  double o[16];
+  // lane r stores doubles 4r..4r+3 of the node's 128-byte record (the
+  // selection uses constant indices only, so g stays in registers)
+  double o[4];
 #pragma unroll
-  for (int k = 0; k < 5; ++k) {
-    o[k] = zero ? 0.0 : gx[k];
-    o[5 + k] = zero ? 0.0 : gy[k];
-    o[10 + k] = zero ? 0.0 : gz[k];
+  for (int q = 0; q < 4; ++q) {
+    double v = 0.0;
+#pragma unroll
+    for (int rr = 0; rr < 4; ++rr)
+      if (4 * rr + q < 15 && r == rr) v = g[4 * rr + q < 15 ? 4 * rr + q : 0];
+    o[q] = zero ? 0.0 : v;
   }
-  o[15] = 0.0;
+  double2* gi = reinterpret_cast<double2*>(G + 16 * (size_t)i);
+  gi[2 * r] = make_double2(o[0], o[1]);
+  gi[2 * r + 1] = make_double2(o[2], o[3]);
+}
+
+// Strides (in doubles) of the node records staged in shared memory: 80 B
+// for (V, X) and 144 B for the gradients, so that the 16-byte loads of 8
+// lanes reading 8 different records fall into disjoint banks.
+constexpr int kPS = 10;
+constexpr int kGS = 18;
+
+// 16-byte global -> shared copy that completes asynchronously (cp.async,
+// cached in L2 only); cp_async_wait_all() waits for this thread's copies.
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// BLOCKED organisation: least-squares gradients of one Morton block of NB
+// nodes per CTA.  The CTA stages the node records (V, X) of its own nodes
+// and of its halo (every neighbour outside the block) in shared memory,
+// then forms the gradients of its own nodes from shared memory only.
+// FUSED: the records are built from U (caller numbering) by the primitive
+// conversion, and V of the own nodes is written to P2 for the flux kernels;
+// otherwise P2 already holds V and the records are copied with cp.async.
+// L = blockDim / NB lanes share a node and take the neighbours at positions
+// r, r+L, ...; their partial sums are added in a fixed shuffle tree.
+// Staging is one pass of independent loads, so the gather latency is paid
+// once per block instead of once per neighbour.
+// P2 is read (X, never written here) and written (V of own nodes only).
+__device__ __forceinline__ void stage_record(Gas g, const int* __restrict__ n2o, const double* __restrict__ U,
+                                             double* P2, int j, double* rec, bool own) {
+  const int o = n2o[j];
+  double u[5], v[5];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) gi[k] = make_double2(o[2 * k], o[2 * k + 1]);
+  for (int k = 0; k < 5; ++k) u[k] = __ldg(U + 5 * (size_t)o + k);
+  const double x0 = P2[8 * (size_t)j + 5], x1 = P2[8 * (size_t)j + 6], x2 = P2[8 * (size_t)j + 7];
+  cons2prim(g, u, v);
+  double2* r2 = reinterpret_cast<double2*>(rec);
+  r2[0] = make_double2(v[0], v[1]);
+  r2[1] = make_double2(v[2], v[3]);
+  r2[2] = make_double2(v[4], x0);
+  r2[3] = make_double2(x1, x2);
+  if (own) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) P2[8 * (size_t)j + k] = v[k];
+  }
+}
+
+template <int L, bool FUSED>
+__global__ void __launch_bounds__(256, 3) k_grad_staged(int N, int NB, Gas g, const int* __restrict__ n2o,
+                                                     const double* __restrict__ U, double* P2,
+                                                     const double* __restrict__ W2, const int* __restrict__ nb2_ptr,
+                                                     const unsigned short* __restrict__ lnb,
+                                                     const int* __restrict__ hptr, const int* __restrict__ hnode,
+                                                     const int* __restrict__ tag, double* __restrict__ G2) {
+  extern __shared__ double sm[];
+  const int blk = blockIdx.x;
+  const int n0 = blk * NB;
+  const int nn = min(NB, N - n0);
+  const int h0 = hptr[blk], nh = hptr[blk + 1] - h0;
+  const int c0 = nb2_ptr[n0], nc = nb2_ptr[n0 + nn] - c0;
+  double* rec = sm;                                                        // [nn + nh][kPS]
+  unsigned short* ls = reinterpret_cast<unsigned short*>(rec + kPS * (size_t)(nn + nh));  // [nc]
+  const int t = threadIdx.x / L, r = threadIdx.x % L;
+  const bool act = t < nn;
+  // the thread's own node data is requested before the staging completes
+  double w[6];
+  int pb = 0, pe = 0;
+  if (act) {
+    const int i = n0 + t;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) w[k] = W2[(size_t)k * N + i];
+    pb = nb2_ptr[i] - c0;
+    pe = nb2_ptr[i + 1] - c0;
+  }
+  for (int k = threadIdx.x; k < nc; k += blockDim.x) ls[k] = lnb[c0 + k];
+  if (FUSED) {
+    for (int t = threadIdx.x; t < nn + nh; t += blockDim.x) {
+      const bool own = t < nn;
+      stage_record(g, n2o, U, P2, own ? n0 + t : hnode[h0 + t - nn], rec + kPS * t, own);
+    }
+  } else {
+    const double2* ps = reinterpret_cast<const double2*>(P2 + 8 * (size_t)n0);
+    double2* pd = reinterpret_cast<double2*>(rec);
+    for (int k = threadIdx.x; k < 4 * nn; k += blockDim.x) cp_async16(pd + (kPS / 2) * (k >> 2) + (k & 3), ps + k);
+    for (int k = threadIdx.x; k < 4 * nh; k += blockDim.x) {
+      const int j = hnode[h0 + (k >> 2)];
+      cp_async16(pd + (kPS / 2) * (nn + (k >> 2)) + (k & 3), reinterpret_cast<const double2*>(P2 + 8 * (size_t)j) + (k & 3));
+    }
+    cp_async_wait_all();
+  }
+  __syncthreads();
+  double gs[15];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) gs[k] = 0.0;
+  if (act) {
+    double pi[8];
+    const double2* qi = reinterpret_cast<const double2*>(rec + kPS * t);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double2 v = qi[k];
+      pi[2 * k] = v.x;
+      pi[2 * k + 1] = v.y;
+    }
+#pragma unroll 1
+    for (int p = pb + r; p < pe; p += L) {
+      double pj[8];
+      const double2* qj = reinterpret_cast<const double2*>(rec + kPS * (int)ls[p]);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const double2 v = qj[k];
+        pj[2 * k] = v.x;
+        pj[2 * k + 1] = v.y;
+      }
+      grad_acc(w, pi, pi + 5, pj, gs, gs + 5, gs + 10);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 15; ++k) {
+    if (L > 1) gs[k] += __shfl_xor_sync(0xffffffffu, gs[k], 1);
+    if (L > 2) gs[k] += __shfl_xor_sync(0xffffffffu, gs[k], 2);
+  }
+  if (!act) return;
+  const int i = n0 + t;
+  const bool zero = tag && tag[i];
+  // lane r stores doubles (16/L) r .. (16/L)(r+1)-1 of the 128-byte record
+  constexpr int S = 16 / L;
+  double o[S];
+#pragma unroll
+  for (int q = 0; q < S; ++q) {
+    double v = 0.0;
+#pragma unroll
+    for (int rr = 0; rr < L; ++rr)
+      if (S * rr + q < 15 && r == rr) v = gs[S * rr + q < 15 ? S * rr + q : 0];
+    o[q] = zero ? 0.0 : v;
+  }
+  double2* gi = reinterpret_cast<double2*>(G2 + 16 * (size_t)i + S * r);
+#pragma unroll
+  for (int q = 0; q < S / 2; ++q) gi[q] = make_double2(o[2 * q], o[2 * q + 1]);
 }
 
 // Flux of one edge (i = first, j = second endpoint): reconstruction from the
@@ -163,70 +310,123 @@ __global__ void k_edge_flux(int E, Gas g, int rec, double beta, int failsafe, co
 }
 
 // BLOCKED organisation: one thread block per NB consecutive (Morton
-// ordered) nodes.  Phase 0: the block's node records (V, X) and gradients
-// are copied to shared memory.  Phase 1: the block's threads evaluate the
-// fluxes of the edges whose first endpoint is in the block (endpoint data
-// from shared memory when the node is in the block, from global memory
-// otherwise) into shared memory; fluxes of edges whose second endpoint lies
-// in a later block also go to spill[].  Phase 2: thread t sums, for node
-// blk*NB+t, its edges held in shared memory in ascending edge order (+ as
-// first endpoint, - as second) into part[].
-__global__ void __launch_bounds__(256) k_fv_blocked(int N, int E, int NB, Gas g, int rec, double beta, int failsafe,
-                                                    const int2* __restrict__ bedges, const double* __restrict__ bn,
-                                                    const int* __restrict__ beptr, const double* __restrict__ P,
+// ordered) nodes.  Phase 0: the node records (V, X) and gradients of the
+// block's nodes and of its forward halo (second endpoints of the block's
+// edges that lie in later blocks) are copied to shared memory with
+// asynchronous 16-byte copies.  Phase 1: the block's threads evaluate the
+// fluxes of the edges whose first endpoint is in the block, every operand
+// from shared memory (bl[q] = the two endpoints as staged slots), into
+// shared memory; fluxes of edges whose second endpoint lies in a later
+// block also go to spill[].  Phase 2: thread t sums, for node blk*NB+t, its
+// edges held in shared memory in ascending edge order (+ as first endpoint,
+// - as second) into part[].
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_fv_blocked(int N, int E, int NB, Gas g, int rec, double beta, int failsafe,
+                                                    const ushort2* __restrict__ bl, const double* __restrict__ bn,
+                                                    const int* __restrict__ beptr, const int* __restrict__ hfptr,
+                                                    const int* __restrict__ hfnode, const double* __restrict__ P,
                                                     const double* __restrict__ G, const int* __restrict__ lptr,
                                                     const int* __restrict__ lidx, const int* __restrict__ xslot,
                                                     double* __restrict__ part, double* __restrict__ spill,
                                                     int* __restrict__ tag, int* __restrict__ counters) {
   extern __shared__ double sm[];
-  double* Pn = sm;                 // [NB][8]
-  double* Gn = sm + 8 * NB;        // [NB][16]
-  double* Fs = sm + 24 * NB;       // [owned edges][5]
   const int blk = blockIdx.x;
   const int n0 = blk * NB;
   const int nn = min(NB, N - n0);
+  const int h0 = hfptr[blk], nh = hfptr[blk + 1] - h0;
+  const int ns = nn + nh;
+  const int e0 = beptr[blk], e1 = beptr[blk + 1];
+  double* Pn = sm;                      // [ns][kPS]
+  double* Gn = sm + kPS * ns;           // [ns][kGS]
+  double* Fs = sm + (kPS + kGS) * ns;   // [e1 - e0][5]
+  int* hs = reinterpret_cast<int*>(Fs + 5 * (e1 - e0));  // [nh] halo node ids
+  for (int k = threadIdx.x; k < nh; k += blockDim.x) hs[k] = hfnode[h0 + k];
   {
+    const bool grad = rec != AEROF_REC_CONSTANT;
+    // own nodes: contiguous records
     const double2* ps = reinterpret_cast<const double2*>(P + 8 * (size_t)n0);
     const double2* gs = reinterpret_cast<const double2*>(G + 16 * (size_t)n0);
     double2* pd = reinterpret_cast<double2*>(Pn);
     double2* gd = reinterpret_cast<double2*>(Gn);
-    for (int k = threadIdx.x; k < 4 * nn; k += blockDim.x) pd[k] = ps[k];
-    if (rec != AEROF_REC_CONSTANT)
-      for (int k = threadIdx.x; k < 8 * nn; k += blockDim.x) gd[k] = gs[k];
+    for (int k = threadIdx.x; k < 4 * nn; k += blockDim.x) cp_async16(pd + (kPS / 2) * (k >> 2) + (k & 3), ps + k);
+    if (grad)
+      for (int k = threadIdx.x; k < 8 * nn; k += blockDim.x)
+        cp_async16(gd + (kGS / 2) * (k >> 3) + (k & 7), gs + k);
+    // forward halo: one 64 B and one 128 B record per node
+    for (int k = threadIdx.x; k < 4 * nh; k += blockDim.x) {
+      const int j = hfnode[h0 + (k >> 2)];
+      cp_async16(pd + (kPS / 2) * (nn + (k >> 2)) + (k & 3), reinterpret_cast<const double2*>(P + 8 * (size_t)j) + (k & 3));
+    }
+    if (grad)
+      for (int k = threadIdx.x; k < 8 * nh; k += blockDim.x) {
+        const int j = hfnode[h0 + (k >> 3)];
+        cp_async16(gd + (kGS / 2) * (nn + (k >> 3)) + (k & 7),
+                   reinterpret_cast<const double2*>(G + 16 * (size_t)j) + (k & 7));
+      }
   }
+  // the edge data of each iteration is requested one iteration ahead (the
+  // first before the staging completes)
+  int q = e0 + threadIdx.x;
+  ushort2 lq = make_ushort2(0, 0);
+  double nx = 0.0, ny = 0.0, nz = 0.0;
+  int xs = -1;
+  if (q < e1) {
+    lq = bl[q];
+    nx = bn[q]; ny = bn[(size_t)E + q]; nz = bn[2 * (size_t)E + q];
+    xs = xslot[q];
+  }
+  cp_async_wait_all();
   __syncthreads();
-  const int e0 = beptr[blk], e1 = beptr[blk + 1];
-  for (int q = e0 + threadIdx.x; q < e1; q += blockDim.x) {
-    const int2 ij = bedges[q];
-    const int li = ij.x - n0, lj = ij.y - n0;
-    const double* pi = Pn + 8 * li;
-    const double* gi = Gn + 16 * li;
-    const bool jin = lj < nn;
-    const double* pj = jin ? Pn + 8 * lj : P + 8 * (size_t)ij.y;
-    const double* gj = jin ? Gn + 16 * lj : G + 16 * (size_t)ij.y;
+  for (; q < e1; q += blockDim.x) {
+    const int qn = q + blockDim.x;
+    ushort2 lqn = make_ushort2(0, 0);
+    double nxn = 0.0, nyn = 0.0, nzn = 0.0;
+    int xsn = -1;
+    if (qn < e1) {
+      lqn = bl[qn];
+      nxn = bn[qn]; nyn = bn[(size_t)E + qn]; nzn = bn[2 * (size_t)E + qn];
+      xsn = xslot[qn];
+    }
+    const int li = lq.x, lj = lq.y;
     double f[5];
-    edge_flux_rec(g, rec, beta, failsafe, ij.x, ij.y, bn[q], bn[(size_t)E + q], bn[2 * (size_t)E + q], pi, gi, pj,
-                  gj, tag, counters, f);
+    // global node ids are needed only to tag unphysical states
+    const int gi = n0 + li, gj = lj < nn ? n0 + lj : hs[lj - nn];
+    edge_flux_rec(g, rec, beta, failsafe, gi, gj, nx, ny, nz, Pn + kPS * li, Gn + kGS * li, Pn + kPS * lj,
+                  Gn + kGS * lj, tag, counters, f);
     double* fs = Fs + 5 * (q - e0);
 #pragma unroll
     for (int k = 0; k < 5; ++k) fs[k] = f[k];
-    const int xs = xslot[q];
     if (xs >= 0) {
 #pragma unroll
       for (int k = 0; k < 5; ++k) spill[5 * (size_t)xs + k] = f[k];
     }
+    lq = lqn; nx = nxn; ny = nyn; nz = nzn; xs = xsn;
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < nn; t += blockDim.x) {
-    const int n = n0 + t;
-    double acc[5] = {0, 0, 0, 0, 0};
-    for (int k = lptr[n]; k < lptr[n + 1]; ++k) {
+  // L = blockDim / NB lanes per node take entries r, r+L, ... of its list;
+  // the partial sums are combined in a fixed xor tree
+  const int L = blockDim.x / NB;
+  const int t = threadIdx.x / L, r = threadIdx.x % L;
+  const int n = n0 + t;
+  double acc[5] = {0, 0, 0, 0, 0};
+  if (t < nn) {
+    for (int k = lptr[n] + r; k < lptr[n + 1]; k += L) {
       const int e = lidx[k];
       const double* fs = Fs + 5 * (e & 0x7fffffff);
-      const double sg = e < 0 ? -1.0 : 1.0;
+      if (e < 0) {
 #pragma unroll
-      for (int c = 0; c < 5; ++c) acc[c] += sg * fs[c];
+        for (int c = 0; c < 5; ++c) acc[c] -= fs[c];
+      } else {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) acc[c] += fs[c];
+      }
     }
+  }
+  for (int o = 1; o < L; o <<= 1) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+  }
+  if (t < nn && r == 0) {
 #pragma unroll
     for (int c = 0; c < 5; ++c) part[5 * (size_t)n + c] = acc[c];
   }
@@ -237,8 +437,7 @@ __global__ void __launch_bounds__(256) k_fv_blocked(int N, int E, int NB, Gas g,
 // of the node (face order), times 1/ctrlVol; written to R in the caller's
 // numbering.
 __global__ void k_fv_nodes(int N, const int* __restrict__ n2o, const double* __restrict__ part,
-                           const int* __restrict__ xin_ptr, const int* __restrict__ xin_slot,
-                           const double* __restrict__ spill, const int* __restrict__ nf_ptr,
+                           const int* __restrict__ xin_ptr, const double* __restrict__ spill, const int* __restrict__ nf_ptr,
                            const int* __restrict__ nf_face, const int* __restrict__ faces,
                            const double* __restrict__ fbuf, const double* __restrict__ vol2, double* __restrict__ R) {
   int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -247,7 +446,7 @@ __global__ void k_fv_nodes(int N, const int* __restrict__ n2o, const double* __r
 #pragma unroll
   for (int c = 0; c < 5; ++c) acc[c] = part[5 * (size_t)n + c];
   for (int k = xin_ptr[n]; k < xin_ptr[n + 1]; ++k) {
-    const double* sp = spill + 5 * (size_t)xin_slot[k];
+    const double* sp = spill + 5 * (size_t)k;
 #pragma unroll
     for (int c = 0; c < 5; ++c) acc[c] -= sp[c];
   }
@@ -466,7 +665,7 @@ void prim_dev(aerof_gpu_ctx* c, const double* dU) {
 void gradients_dev(aerof_gpu_ctx* c) {
   DeviceMesh& m = c->mesh;
   c->s.G.ensure(16 * (size_t)m.N);
-  k_grad<<<grid_for(m.N, kBlock), kBlock, 0, c->stream>>>(m.N, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p,
+  k_grad<<<grid_for(4 * (size_t)m.N, kBlock), kBlock, 0, c->stream>>>(m.N, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p,
                                                           nullptr, c->s.G.p);
   AEROF_LAUNCH_CHECK();
 }
@@ -479,6 +678,49 @@ static int* counters(aerof_gpu_ctx* c) {
 // Residual of device state dU into device dR (both [N][5]).  Returns the
 // number of non-positive reconstructed states of the first pass (sync), or
 // 0 with the count accumulated in counters[2] (no sync, failsafe off).
+constexpr size_t kMaxStagedSmem = 160 * 1024;
+
+static int grad_kernel_choice() {
+  static const int v = [] {
+    const char* e = std::getenv("AEROF_GRAD_KERNEL");
+    const int k = e ? std::atoi(e) : 0;
+    return k >= 0 && k <= 2 ? k : 0;
+  }();
+  return v;
+}
+
+// dynamic shared memory of k_fv_blocked: staged records of the block's
+// nodes and forward halo, the fluxes of its edges, the halo node ids
+static size_t fv_blocked_smem(const DeviceMesh& m) {
+  return ((size_t)(kPS + kGS) * (m.NB + m.maxHf) + (size_t)5 * m.maxE) * sizeof(double) + (size_t)4 * m.maxHf;
+}
+
+// fused: prim conversion inside the gradient kernel; otherwise
+// k_prim_blocked writes P2 first
+static void launch_grad_staged(const DeviceMesh& m, const Gas& g, const double* dU, const int* tag, double* G2,
+                               size_t smem, bool fused, cudaStream_t s) {
+  const int L = kBlock / m.NB;
+  if (!fused) {
+    k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
+    AEROF_LAUNCH_CHECK();
+  }
+  auto go = [&](auto kern) {
+    AEROF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<m.nblk, kBlock, smem, s>>>(m.N, m.NB, g, m.n2o.p, dU, m.P2.p, m.W2.p, m.nb2_ptr.p, m.lnb.p, m.hptr.p,
+                                      m.hnode.p, tag, G2);
+    AEROF_LAUNCH_CHECK();
+  };
+  if (fused) {
+    if (L == 4) go(k_grad_staged<4, true>);
+    else if (L == 2) go(k_grad_staged<2, true>);
+    else go(k_grad_staged<1, true>);
+  } else {
+    if (L == 4) go(k_grad_staged<4, false>);
+    else if (L == 2) go(k_grad_staged<2, false>);
+    else go(k_grad_staged<1, false>);
+  }
+}
+
 // BLOCKED organisation of residual_dev (see k_fv_blocked).
 static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
   DeviceMesh& m = c->mesh;
@@ -496,22 +738,43 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
     c->s.tag.ensure(m.N);
     c->s.tag.zero(s);
   }
-  const size_t smem = ((size_t)24 * m.NB + (size_t)m.maxE * 5) * sizeof(double);
-  AEROF_CUDA(cudaFuncSetAttribute(k_fv_blocked, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const size_t smem = fv_blocked_smem(m);
+  // register budget from the CTAs per SM that shared memory allows
+  // (228 KB per SM, 1 KB reserved per CTA)
+  const int by_smem = (int)std::min<size_t>(4, (228 * 1024) / (smem + 1024));
+  auto fvk = by_smem >= 4 ? k_fv_blocked<4> : by_smem == 3 ? k_fv_blocked<3> : k_fv_blocked<2>;
+  AEROF_CUDA(cudaFuncSetAttribute(fvk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const size_t gsmem = ((size_t)8 * kPS * (m.NB + m.maxH) + (size_t)2 * m.maxL + 15) / 16 * 16;
+  // gradient organisation (tuning knob AEROF_GRAD_KERNEL): 0 staged from
+  // P2, 1 staged with the primitive conversion fused, 2 node-parallel
+  const int gk = grad_kernel_choice();
+  const bool staged = gsmem <= kMaxStagedSmem && gk != 2;
+  // prim + gradients: staged per block when the block's halo fits, else
+  // the node-parallel kernels on the blocked arrays
+  auto grad = [&](const int* tg) {
+    if (staged) {
+      launch_grad_staged(m, g, dU, tg, c->s.G2.p, gsmem, gk == 1, s);
+    } else {
+      k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
+      AEROF_LAUNCH_CHECK();
+      k_grad<<<grid_for(4 * (size_t)m.N, kBlock), kBlock, 0, s>>>(m.N, m.P2.p, m.W2.p, m.nb2_ptr.p, m.nb2_node.p, tg,
+                                                                  c->s.G2.p);
+      AEROF_LAUNCH_CHECK();
+    }
+  };
   {
     TimerScope t(c, AEROF_T_NODAL_GRAD);
-    k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
-    AEROF_LAUNCH_CHECK();
     if (rec != AEROF_REC_CONSTANT) {
-      k_grad<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.P2.p, m.W2.p, m.nb2_ptr.p, m.nb2_node.p, nullptr,
-                                                      c->s.G2.p);
+      grad(nullptr);
+    } else {
+      k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
       AEROF_LAUNCH_CHECK();
     }
   }
   auto fv = [&](int fs, int* counter) {
-    k_fv_blocked<<<m.nblk, 256, smem, s>>>(m.N, m.E, m.NB, g, rec, c->cfg.beta, fs, m.bedges.p, m.bnorm.p,
-                                            m.beptr.p, m.P2.p, c->s.G2.p, m.lptr.p, m.lidx.p, m.xslot.p,
-                                            c->s.part.p, c->s.spill.p, c->s.tag.p, counter);
+    fvk<<<m.nblk, 256, smem, s>>>(m.N, m.E, m.NB, g, rec, c->cfg.beta, fs, m.bl.p, m.bnorm.p, m.beptr.p,
+                                            m.hfptr.p, m.hfnode.p, m.P2.p, c->s.G2.p, m.lptr.p, m.lidx.p,
+                                            m.xslot.p, c->s.part.p, c->s.spill.p, c->s.tag.p, counter);
     AEROF_LAUNCH_CHECK();
   };
   {
@@ -525,9 +788,7 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
   }
   if (bad && c->cfg.failsafe && rec != AEROF_REC_CONSTANT) {
     TimerScope t(c, AEROF_T_FV_TERM);
-    k_grad<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.P2.p, m.W2.p, m.nb2_ptr.p, m.nb2_node.p, c->s.tag.p,
-                                                    c->s.G2.p);
-    AEROF_LAUNCH_CHECK();
+    grad(c->s.tag.p);
     fv(0, cnt + 1);
   }
   {
@@ -537,9 +798,8 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
                                                            m.o2n.p, c->s.fbuf.p);
       AEROF_LAUNCH_CHECK();
     }
-    k_fv_nodes<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.n2o.p, c->s.part.p, m.xin_ptr.p, m.xin_slot.p,
-                                                        c->s.spill.p, m.nf_ptr.p, m.nf_face.p, m.faces.p, c->s.fbuf.p,
-                                                        m.vol2.p, dR);
+    k_fv_nodes<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.n2o.p, c->s.part.p, m.xin_ptr.p, c->s.spill.p,
+                                                        m.nf_ptr.p, m.nf_face.p, m.faces.p, c->s.fbuf.p, m.vol2.p, dR);
     AEROF_LAUNCH_CHECK();
   }
   return bad;
@@ -547,7 +807,7 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
 
 int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
   DeviceMesh& m = c->mesh;
-  if (c->cfg.residual_kernel == AEROF_KERNEL_BLOCKED && ((size_t)24 * m.NB + (size_t)m.maxE * 5) * 8 <= 200 * 1024)
+  if (c->cfg.residual_kernel == AEROF_KERNEL_BLOCKED && fv_blocked_smem(m) <= 200 * 1024)
     return residual_blocked_dev(c, dU, dR, sync);
   const Gas g = make_gas(c->cfg.gamma);
   const int rec = c->cfg.reconstruction;
@@ -580,7 +840,7 @@ int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
   if (bad && c->cfg.failsafe && rec != AEROF_REC_CONSTANT) {
     // Domain.C:886-918: zero the gradients of tagged nodes and recompute.
     TimerScope t(c, AEROF_T_FV_TERM);
-    k_grad<<<grid_for(m.N, kBlock), kBlock, 0, c->stream>>>(m.N, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p,
+    k_grad<<<grid_for(4 * (size_t)m.N, kBlock), kBlock, 0, c->stream>>>(m.N, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p,
                                                             c->s.tag.p, c->s.G.p);
     AEROF_LAUNCH_CHECK();
     k_edge_flux<<<grid_for(m.E, kBlock), kBlock, 0, c->stream>>>(
@@ -837,7 +1097,7 @@ extern "C" int aerof_gpu_residual_noalloc(aerof_gpu_ctx* c, const double* U, dou
     k_prim<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, U, m.P.p);
     AEROF_LAUNCH_CHECK();
     if (rec != AEROF_REC_CONSTANT) {
-      k_grad<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, nullptr, G);
+      k_grad<<<grid_for(4 * (size_t)m.N, kBlock), kBlock, 0, s>>>(m.N, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, nullptr, G);
       AEROF_LAUNCH_CHECK();
     }
     k_edge_flux<<<grid_for(m.E, kBlock), kBlock, 0, s>>>(m.E, g, rec, c->cfg.beta, c->cfg.failsafe, m.edges.p,
@@ -847,7 +1107,7 @@ extern "C" int aerof_gpu_residual_noalloc(aerof_gpu_ctx* c, const double* U, dou
     AEROF_CUDA(cudaMemcpyAsync(&bad, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
     AEROF_CUDA(cudaStreamSynchronize(s));
     if (bad && c->cfg.failsafe && rec != AEROF_REC_CONSTANT) {
-      k_grad<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, tag, G);
+      k_grad<<<grid_for(4 * (size_t)m.N, kBlock), kBlock, 0, s>>>(m.N, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, tag, G);
       AEROF_LAUNCH_CHECK();
       k_edge_flux<<<grid_for(m.E, kBlock), kBlock, 0, s>>>(m.E, g, rec, c->cfg.beta, 0, m.edges.p, m.en.p, m.P.p, G,
                                                            flux, tag, cnt + 1);

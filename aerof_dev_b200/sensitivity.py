@@ -77,44 +77,59 @@ class ZForce:
         return g
 
 
-def converge(ctx, U, precision=32, tol=1e-10, max_steps=2000, exact_steps=3, krylov=30):
+def _norm(x) -> float:
+    if type(x).__module__.startswith("torch"):
+        return float(x.norm().item())
+    return float(np.linalg.norm(x))
+
+
+def _host(x):
+    if type(x).__module__.startswith("torch"):
+        return x.detach().cpu().numpy()
+    return np.asarray(x)
+
+
+def converge(ctx, U, precision=32, tol=1e-10, max_steps=2000, exact_steps=3, krylov=30, inner_its=20):
     """Steady solve: pseudo-transient Newton (H1 operator) to ``tol``, then a
-    few exact Newton steps with the matrix-free exact Jacobian."""
+    few exact Newton steps with the matrix-free exact Jacobian (flexible
+    GMRES preconditioned by inner_its mixed-precision H1 iterations)."""
     import aerof_dev_b200 as A
     sol = A.ImplicitSteadySolver(ctx, precision=precision, tol=tol, max_steps=max_steps)
     U, info = sol.solve(U)
     sp = A.SpaceOperator(ctx)
     S = A.Sensitivity(ctx)
-    hist = [float(np.linalg.norm(sp.computeResidual(U)[0]))]
+    hist = [_norm(sp.computeResidual(U)[0])]
     for _ in range(exact_steps):
         R, _ = sp.computeResidual(U)
-        dU, its, res = S.solve(U, -R, transpose=False, krylov=krylov, maxits=600, eps=1e-8)
+        dU, its, res = S.solve(U, -R, transpose=False, krylov=krylov, maxits=600, eps=1e-8, inner_its=inner_its)
         U = U + dU
-        hist.append(float(np.linalg.norm(sp.computeResidual(U)[0])))
+        hist.append(_norm(sp.computeResidual(U)[0]))
     info["exact_newton_residuals"] = hist
     return U, info
 
 
-def adjoint_gradient(ctx, U, X, functional: ZForce, modes, eps=1e-10, krylov=30, maxits=2000):
+def adjoint_gradient(ctx, U, X, functional: ZForce, modes, eps=1e-10, krylov=30, maxits=2000, inner_its=20):
     """dJ/ds_k for every mode by the adjoint method."""
     import aerof_dev_b200 as A
     S = A.Sensitivity(ctx)
+    U = _host(U)
     gU = functional.dU(U, X)
-    lam, its, res = S.solve(U, gU, transpose=True, krylov=krylov, maxits=maxits, eps=eps)
+    lam, its, res = S.solve(U, gU, transpose=True, krylov=krylov, maxits=maxits, eps=eps, inner_its=inner_its)
     gX = functional.dX(U, X) - S.dRdX_T(U, lam)
     return np.einsum("kni,ni->k", modes, gX), {"adjoint_its": its, "adjoint_res": res}
 
 
-def direct_gradient(ctx, U, X, functional: ZForce, modes, eps=1e-10, krylov=30, maxits=2000):
+def direct_gradient(ctx, U, X, functional: ZForce, modes, eps=1e-10, krylov=30, maxits=2000, inner_its=20):
     """dJ/ds_k for every mode by the direct method (one solve per mode)."""
     import aerof_dev_b200 as A
     S = A.Sensitivity(ctx)
+    U = _host(U)
     gU = functional.dU(U, X)
     gX = functional.dX(U, X)
     out, its_all = [], []
     for Xd in modes:
         rhs = -S.dRdX(U, Xd)
-        x, its, res = S.solve(U, rhs, transpose=False, krylov=krylov, maxits=maxits, eps=eps)
+        x, its, res = S.solve(U, rhs, transpose=False, krylov=krylov, maxits=maxits, eps=eps, inner_its=inner_its)
         out.append(float(np.sum(gX * Xd) + np.sum(gU * x)))
         its_all.append(its)
     return np.array(out), {"direct_its": its_all}
@@ -131,7 +146,7 @@ def fd_gradient(ctx, U, X, functional: ZForce, modes, h=1e-6, **conv):
             Xp = X + sgn * step * Xd
             ctx.update_coordinates(Xp)
             Up, _ = converge(ctx, U, **conv)
-            vals.append(functional.value(Up, Xp))
+            vals.append(functional.value(_host(Up), Xp))
         return (vals[0] - vals[1]) / (2 * step)
 
     out = []

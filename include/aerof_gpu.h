@@ -103,6 +103,10 @@ int aerof_gpu_create(const aerof_gpu_config* cfg, aerof_gpu_ctx** out);
 int aerof_gpu_destroy(aerof_gpu_ctx* ctx);
 /* Run subsequent work on this cudaStream_t (NULL: the context's own stream). */
 int aerof_gpu_set_stream(aerof_gpu_ctx* ctx, void* stream);
+/* Number of kernels the library has launched (all contexts of the process)
+ * since the previous call; the counter restarts at 0.  Diagnostics only, no
+ * reference counterpart. */
+int aerof_gpu_launch_count(long long* count);
 /* Last error message of this context (NUL-terminated, truncated to len). */
 int aerof_gpu_last_error(aerof_gpu_ctx* ctx, char* buf, int len);
 
@@ -248,10 +252,15 @@ int aerof_gpu_dRdX_T(aerof_gpu_ctx* ctx, const double* U, const double* lambda, 
 /* Linearised steady solves with the exact Jacobian applied matrix-free
  * (fsoLinearSolver / fsoAdjointLinearSolver, FluidShapeOptimizationHandler.C:
  * 1557-1624; GmresSolver::solve / solveT): transpose = 0 solves J x = b,
- * transpose = 1 solves J^T x = b, GMRES(krylov) right-preconditioned by the
- * block-Jacobi of the FP64 first-order operator at U (no time term).       */
+ * transpose = 1 solves J^T x = b to ||r|| <= eps ||b||.
+ * inner_its = 0: GMRES(krylov) right-preconditioned by the block-Jacobi of
+ * the FP64 first-order operator at U (no time term).
+ * inner_its > 0: flexible GMRES(krylov) whose preconditioner is inner_its
+ * iterations of the mixed-precision GMRES on the first-order operator (FP32
+ * blocks and Krylov vectors, block-Jacobi); the outer iteration and the
+ * exact products stay FP64.  its = outer iterations.                       */
 int aerof_gpu_linearized_solve(aerof_gpu_ctx* ctx, const double* U, const double* b, double* x, int krylov,
-                               int maxits, double eps, int transpose, int* its, double* res);
+                               int maxits, double eps, int transpose, int inner_its, int* its, double* res);
 
 #ifdef __cplusplus
 }

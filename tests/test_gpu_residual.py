@@ -162,3 +162,41 @@ def test_blocked_numbering_is_a_permutation(gpu_lib, case):
     Rb, _ = gpu_lib.SpaceOperator(ctx_for(gpu_lib, m, Ub, kernel=0)).computeResidual(U)
     Re, _ = gpu_lib.SpaceOperator(ctx_for(gpu_lib, m, Ub, kernel=1)).computeResidual(U)
     assert rel_l2(Rb, Re) < 1e-13
+
+
+@pytest.mark.parametrize("nb", ["64", "256"])
+def test_block_sizes(gpu_lib, oracle_mod, monkeypatch, nb):
+    # the staged gradient kernel runs 4, 2 or 1 lanes per node depending on
+    # the block size; every block size gives the oracle's residual, also on
+    # the failsafe path that recomputes tagged gradients
+    monkeypatch.setenv("AEROF_BLOCK_NODES", nb)
+    m = W.make_lattice_mesh(13, jitter=0.25, codes="channel")
+    Ub = W.freestream(0.8)
+    o = oracle_mod.Oracle(m)
+    U = W.perturbed_state(o.N, 0.8)
+    for rec in (2, 3):
+        R, bad = gpu_lib.SpaceOperator(ctx_for(gpu_lib, m, Ub, rec=rec)).computeResidual(U)
+        Rr, badr = o.residual(U, Ub, rec)
+        assert bad == badr == 0
+        assert rel_l2(R, Rr) < TOL
+    V = o.prim(U)
+    i = 5 * 169 + 5 * 13 + 5
+    V[i, 4] *= 40.0
+    V[i + 1, 4] *= 0.02
+    U2 = W.prim_to_cons(V)
+    R, bad = gpu_lib.SpaceOperator(ctx_for(gpu_lib, m, Ub, rec=3, failsafe=1)).computeResidual(U2)
+    Rr, badr = o.residual(U2, Ub, 3, failsafe=1)
+    assert bad == badr > 0
+    assert rel_l2(R, Rr) < TOL
+
+
+def test_launch_count(gpu_lib, case):
+    m, Ub, o = case
+    ctx = ctx_for(gpu_lib, m, Ub)
+    U = W.perturbed_state(o.N, 0.8)
+    sp = gpu_lib.SpaceOperator(ctx)
+    sp.computeResidual(U)
+    gpu_lib.launch_count()
+    sp.computeResidual(U)
+    n = gpu_lib.launch_count()
+    assert 3 <= n <= 6

@@ -131,7 +131,7 @@ struct DeviceMesh {
 
   // ---- blocked residual: Morton-renumbered copy of the node data ----
   int NB = 256;            // nodes per block
-  int nblk = 0, maxE = 0, nX = 0, maxH = 0, maxL = 0, maxHf = 0;
+  int nblk = 0, maxE = 0, nX = 0, maxH = 0, maxL = 0, maxHf = 0, maxLp = 0;
   DBuf<int> n2o, o2n;      // [N] new -> old and old -> new node ids
   DBuf<double> P2;         // [N][8] node records in new numbering
   DBuf<double> W2;         // [6][N] LSQ constants, new numbering
@@ -139,7 +139,10 @@ struct DeviceMesh {
   DBuf<int> nb2_ptr, nb2_node;  // neighbour CSR in new numbering (ascending)
   DBuf<int> hptr, hnode;        // per block: halo nodes (outside the block, ascending)
   DBuf<unsigned short> lnb;     // nb2_node entries as slots of the block's staged nodes
+  DBuf<int> hpad;               // [nblk][maxH] halo ids, -1 padded
+  DBuf<unsigned short> lpad;    // [nblk][maxLp] the block's lnb segment, 0 padded
   DBuf<int> hfptr, hfnode;      // per block: forward halo (second endpoints in later blocks)
+  DBuf<int> hfpad;              // [nblk][maxHf] forward halo ids, -1 padded
   DBuf<ushort2> bl;             // per blocked edge: (first, second) as slots of the staged nodes
   DBuf<int> bsrc;          // [E] reference edge id | (1<<31 if reversed)
   DBuf<double> bnorm;      // [3][E] normals oriented first -> second

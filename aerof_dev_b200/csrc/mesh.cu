@@ -180,10 +180,11 @@ static void build_host(int N, int T, int F, const int* tets, const int* faces, H
 struct HostBlocked {
   std::vector<int> n2o, o2n, nb2_ptr, nb2_node, bsrc, beptr, lptr, lidx, xslot, xin_ptr, hptr, hnode,
       hfptr, hfnode;
-  std::vector<unsigned short> lnb;
+  std::vector<unsigned short> lnb, lpad;
+  std::vector<int> hpad, hfpad;
   std::vector<ushort2> bl;
   std::vector<int2> bedges;
-  int nblk = 0, maxE = 0, nX = 0, maxH = 0, maxL = 0, maxHf = 0;
+  int nblk = 0, maxE = 0, nX = 0, maxH = 0, maxL = 0, maxHf = 0, maxLp = 0;
 };
 
 static inline uint64_t spread3(uint64_t v) {
@@ -305,6 +306,17 @@ static void build_blocked(int N, int E, int NB, const double* X, const std::vect
     b.hnode.insert(b.hnode.end(), h.begin(), h.end());
     b.hptr[blk + 1] = (int)b.hnode.size();
   }
+  // the same in fixed-stride per-block segments (halo ids padded with -1 to
+  // maxH, local slots padded to a multiple of 8 entries), so a block's
+  // staging addresses follow from its index alone
+  b.maxLp = (b.maxL + 7) / 8 * 8;
+  b.hpad.assign((size_t)b.nblk * std::max(b.maxH, 1), -1);
+  b.lpad.assign((size_t)b.nblk * std::max(b.maxLp, 8), 0);
+  for (int blk = 0; blk < b.nblk; ++blk) {
+    const int n0 = blk * NB, n1 = std::min(N, n0 + NB);
+    std::copy(b.hnode.begin() + b.hptr[blk], b.hnode.begin() + b.hptr[blk + 1], b.hpad.begin() + (size_t)blk * b.maxH);
+    std::copy(b.lnb.begin() + b.nb2_ptr[n0], b.lnb.begin() + b.nb2_ptr[n1], b.lpad.begin() + (size_t)blk * b.maxLp);
+  }
   // forward halo of every block (second endpoints of its edges lying in
   // later blocks, ascending) and each edge's endpoints as staged slots
   b.hfptr.assign(b.nblk + 1, 0);
@@ -328,6 +340,11 @@ static void build_blocked(int N, int E, int NB, const double* X, const std::vect
     b.hfnode.insert(b.hfnode.end(), h.begin(), h.end());
     b.hfptr[blk + 1] = (int)b.hfnode.size();
   }
+  // fixed-stride copy of the forward halo ids (-1 padded to maxHf)
+  b.hfpad.assign((size_t)b.nblk * std::max(b.maxHf, 1), -1);
+  for (int blk = 0; blk < b.nblk; ++blk)
+    std::copy(b.hfnode.begin() + b.hfptr[blk], b.hfnode.begin() + b.hfptr[blk + 1],
+              b.hfpad.begin() + (size_t)blk * b.maxHf);
 }
 
 // blocked copies of the node geometry and oriented edge normals
@@ -473,7 +490,10 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
       }
       HostBlocked hb;
       build_blocked(N, E, m.NB, X, h.edges, hb);
-      m.nblk = hb.nblk; m.maxE = hb.maxE; m.nX = hb.nX; m.maxH = hb.maxH; m.maxL = hb.maxL; m.maxHf = hb.maxHf;
+      m.nblk = hb.nblk; m.maxE = hb.maxE; m.nX = hb.nX; m.maxH = hb.maxH; m.maxL = hb.maxL; m.maxHf = hb.maxHf; m.maxLp = hb.maxLp;
+      m.hpad.upload(hb.hpad.data(), hb.hpad.size(), s);
+      m.lpad.upload(hb.lpad.data(), hb.lpad.size(), s);
+      m.hfpad.upload(hb.hfpad.data(), hb.hfpad.size(), s);
       m.hfptr.upload(hb.hfptr.data(), hb.hfptr.size(), s);
       if (hb.hfnode.empty()) m.hfnode.alloc(1);
       else m.hfnode.upload(hb.hfnode.data(), hb.hfnode.size(), s);
@@ -486,7 +506,9 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
       else m.lnb.upload(hb.lnb.data(), hb.lnb.size(), s);
       m.n2o.upload(hb.n2o.data(), N, s);
       m.o2n.upload(hb.o2n.data(), N, s);
-      m.nb2_ptr.upload(hb.nb2_ptr.data(), N + 1, s);
+      const int last = hb.nb2_ptr[N];
+      hb.nb2_ptr.resize(N + 1 + 4, last);  // padding read by the 16-byte staging of the last block
+      m.nb2_ptr.upload(hb.nb2_ptr.data(), hb.nb2_ptr.size(), s);
       m.nb2_node.upload(hb.nb2_node.data(), hb.nb2_node.size(), s);
       m.bsrc.upload(hb.bsrc.data(), (size_t)E, s);
       m.beptr.upload(hb.beptr.data(), hb.beptr.size(), s);

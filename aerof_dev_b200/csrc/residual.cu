@@ -249,6 +249,138 @@ __global__ void __launch_bounds__(256, 3) k_grad_staged(int N, int NB, Gas g, co
   for (int q = 0; q < S / 2; ++q) gi[q] = make_double2(o[2 * q], o[2 * q + 1]);
 }
 
+// 8-byte variant of cp_async16 (cached in L1 and L2)
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Shared-memory stage of the pipelined gradient kernel (offsets in doubles,
+// all even so that every part is 16-byte aligned).
+struct GradStage {
+  int rec, w, ptr, ls, size;
+};
+
+// Persistent, software-pipelined form of the staged gradient kernel: each
+// CTA walks the blocks blockIdx.x, + gridDim.x, ... and, while it forms the
+// gradients of one block from shared memory, the asynchronous copies of the
+// next block's node records (own and halo), LSQ constants, neighbour
+// pointers and local neighbour slots are in flight into the other stage.
+// The halo ids of the block after that are loaded into registers one
+// iteration ahead, so no copy waits on a dependent load.  Halo of at most
+// 512 nodes (two records per thread).
+template <int L>
+__global__ void __launch_bounds__(256, 2) k_grad_pipe(int N, int NB, int nblk, int maxH, int maxLp, GradStage st,
+                                                      const double* __restrict__ P2, const double* __restrict__ W2,
+                                                      const int* __restrict__ nb2_ptr,
+                                                      const unsigned short* __restrict__ lpad,
+                                                      const int* __restrict__ hpad, const int* __restrict__ tag,
+                                                      double* __restrict__ G2) {
+  extern __shared__ double sm[];
+  const int tid = threadIdx.x;
+  auto load_ids = [&](int b, int& a0, int& a1) {
+    a0 = tid < maxH ? hpad[(size_t)b * maxH + tid] : -1;
+    a1 = tid + 256 < maxH ? hpad[(size_t)b * maxH + tid + 256] : -1;
+  };
+  auto issue = [&](int b, double* S, int a0, int a1) {
+    const int n0 = b * NB, nn = min(NB, N - n0);
+    double2* rec = reinterpret_cast<double2*>(S + st.rec);
+    const double2* ps = reinterpret_cast<const double2*>(P2 + 8 * (size_t)n0);
+    for (int k = tid; k < 4 * nn; k += blockDim.x) cp_async16(rec + (kPS / 2) * (k >> 2) + (k & 3), ps + k);
+    if (a0 >= 0) {
+      const double2* src = reinterpret_cast<const double2*>(P2 + 8 * (size_t)a0);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) cp_async16(rec + (kPS / 2) * (nn + tid) + c, src + c);
+    }
+    if (a1 >= 0) {
+      const double2* src = reinterpret_cast<const double2*>(P2 + 8 * (size_t)a1);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) cp_async16(rec + (kPS / 2) * (nn + tid + 256) + c, src + c);
+    }
+    if (tid < nn) {
+#pragma unroll
+      for (int a = 0; a < 6; ++a) cp_async8(S + st.w + a * NB + tid, W2 + (size_t)a * N + n0 + tid);
+    }
+    if (4 * tid < nn + 1) cp_async16(S + st.ptr + 2 * tid, nb2_ptr + n0 + 4 * tid);
+    if (8 * tid < maxLp) cp_async16(S + st.ls + 2 * tid, lpad + (size_t)b * maxLp + 8 * tid);
+  };
+  int b = blockIdx.x;
+  if (b >= nblk) return;
+  int a0, a1;
+  load_ids(b, a0, a1);
+  issue(b, sm, a0, a1);
+  cp_async_commit();
+  if (b + (int)gridDim.x < nblk) load_ids(b + gridDim.x, a0, a1);
+  for (int k = 0; b < nblk; ++k, b += gridDim.x) {
+    const int bn = b + gridDim.x;
+    if (bn < nblk) issue(bn, sm + ((k + 1) & 1) * st.size, a0, a1);
+    cp_async_commit();
+    if (bn + (int)gridDim.x < nblk) load_ids(bn + gridDim.x, a0, a1);
+    cp_async_wait_prev();
+    __syncthreads();
+    const double* S = sm + (k & 1) * st.size;
+    const double* rec = S + st.rec;
+    const int* ptr = reinterpret_cast<const int*>(S + st.ptr);
+    const unsigned short* ls = reinterpret_cast<const unsigned short*>(S + st.ls);
+    const int n0 = b * NB, nn = min(NB, N - n0);
+    const int t = tid / L, r = tid % L;
+    const bool act = t < nn;
+    double gs[15];
+#pragma unroll
+    for (int q = 0; q < 15; ++q) gs[q] = 0.0;
+    if (act) {
+      double w[6], pi[8];
+#pragma unroll
+      for (int a = 0; a < 6; ++a) w[a] = S[st.w + a * NB + t];
+      const double2* qi = reinterpret_cast<const double2*>(rec + kPS * t);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double2 v = qi[q];
+        pi[2 * q] = v.x;
+        pi[2 * q + 1] = v.y;
+      }
+      const int c0 = ptr[0], pe = ptr[t + 1] - c0;
+#pragma unroll 1
+      for (int p = ptr[t] - c0 + r; p < pe; p += L) {
+        double pj[8];
+        const double2* qj = reinterpret_cast<const double2*>(rec + kPS * (int)ls[p]);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double2 v = qj[q];
+          pj[2 * q] = v.x;
+          pj[2 * q + 1] = v.y;
+        }
+        grad_acc(w, pi, pi + 5, pj, gs, gs + 5, gs + 10);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 15; ++q) {
+      if (L > 1) gs[q] += __shfl_xor_sync(0xffffffffu, gs[q], 1);
+      if (L > 2) gs[q] += __shfl_xor_sync(0xffffffffu, gs[q], 2);
+    }
+    if (act) {
+      const int i = n0 + t;
+      const bool zero = tag && tag[i];
+      constexpr int SL = 16 / L;
+      double o[SL];
+#pragma unroll
+      for (int q = 0; q < SL; ++q) {
+        double v = 0.0;
+#pragma unroll
+        for (int rr = 0; rr < L; ++rr)
+          if (SL * rr + q < 15 && r == rr) v = gs[SL * rr + q < 15 ? SL * rr + q : 0];
+        o[q] = zero ? 0.0 : v;
+      }
+      double2* gi = reinterpret_cast<double2*>(G2 + 16 * (size_t)i + SL * r);
+#pragma unroll
+      for (int q = 0; q < SL / 2; ++q) gi[q] = make_double2(o[2 * q], o[2 * q + 1]);
+    }
+    __syncthreads();
+  }
+}
+
 // Flux of one edge (i = first, j = second endpoint): reconstruction from the
 // node records and gradients, positivity check (VarFcnSGEuler::
 // checkReconstructedValues, VarFcnSGEuler.h:90-110; on failure the edge is
@@ -324,7 +456,8 @@ template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_fv_blocked(int N, int E, int NB, Gas g, int rec, double beta, int failsafe,
                                                     const ushort2* __restrict__ bl, const double* __restrict__ bn,
                                                     const int* __restrict__ beptr, const int* __restrict__ hfptr,
-                                                    const int* __restrict__ hfnode, const double* __restrict__ P,
+                                                    const int* __restrict__ hfpad, int maxHf,
+                                                    const double* __restrict__ P,
                                                     const double* __restrict__ G, const int* __restrict__ lptr,
                                                     const int* __restrict__ lidx, const int* __restrict__ xslot,
                                                     double* __restrict__ part, double* __restrict__ spill,
@@ -340,7 +473,8 @@ __global__ void __launch_bounds__(256, MINB) k_fv_blocked(int N, int E, int NB, 
   double* Gn = sm + kPS * ns;           // [ns][kGS]
   double* Fs = sm + (kPS + kGS) * ns;   // [e1 - e0][5]
   int* hs = reinterpret_cast<int*>(Fs + 5 * (e1 - e0));  // [nh] halo node ids
-  for (int k = threadIdx.x; k < nh; k += blockDim.x) hs[k] = hfnode[h0 + k];
+  const int* hf = hfpad + (size_t)blk * maxHf;            // addresses from the block index alone
+  for (int k = threadIdx.x; k < nh; k += blockDim.x) hs[k] = hf[k];
   {
     const bool grad = rec != AEROF_REC_CONSTANT;
     // own nodes: contiguous records
@@ -354,12 +488,12 @@ __global__ void __launch_bounds__(256, MINB) k_fv_blocked(int N, int E, int NB, 
         cp_async16(gd + (kGS / 2) * (k >> 3) + (k & 7), gs + k);
     // forward halo: one 64 B and one 128 B record per node
     for (int k = threadIdx.x; k < 4 * nh; k += blockDim.x) {
-      const int j = hfnode[h0 + (k >> 2)];
+      const int j = hf[k >> 2];
       cp_async16(pd + (kPS / 2) * (nn + (k >> 2)) + (k & 3), reinterpret_cast<const double2*>(P + 8 * (size_t)j) + (k & 3));
     }
     if (grad)
       for (int k = threadIdx.x; k < 8 * nh; k += blockDim.x) {
-        const int j = hfnode[h0 + (k >> 3)];
+        const int j = hf[k >> 3];
         cp_async16(gd + (kGS / 2) * (nn + (k >> 3)) + (k & 7),
                    reinterpret_cast<const double2*>(G + 16 * (size_t)j) + (k & 7));
       }
@@ -683,8 +817,8 @@ constexpr size_t kMaxStagedSmem = 160 * 1024;
 static int grad_kernel_choice() {
   static const int v = [] {
     const char* e = std::getenv("AEROF_GRAD_KERNEL");
-    const int k = e ? std::atoi(e) : 0;
-    return k >= 0 && k <= 2 ? k : 0;
+    const int k = e ? std::atoi(e) : 3;
+    return k >= 0 && k <= 3 ? k : 3;
   }();
   return v;
 }
@@ -693,6 +827,44 @@ static int grad_kernel_choice() {
 // nodes and forward halo, the fluxes of its edges, the halo node ids
 static size_t fv_blocked_smem(const DeviceMesh& m) {
   return ((size_t)(kPS + kGS) * (m.NB + m.maxHf) + (size_t)5 * m.maxE) * sizeof(double) + (size_t)4 * m.maxHf;
+}
+
+static GradStage grad_stage(const DeviceMesh& m) {
+  GradStage st;
+  st.rec = 0;
+  st.w = kPS * (m.NB + m.maxH);
+  st.w += st.w & 1;
+  st.ptr = st.w + 6 * m.NB;
+  st.ls = st.ptr + (m.NB + 8) / 2;
+  st.ls += st.ls & 1;
+  st.size = st.ls + std::max(m.maxLp, 8) / 4;
+  st.size += st.size & 1;
+  return st;
+}
+
+// persistent pipelined gradients (k_prim_blocked writes P2 first)
+static void launch_grad_pipe(aerof_gpu_ctx* c, const Gas& g, const double* dU, const int* tag, double* G2,
+                             cudaStream_t s) {
+  const DeviceMesh& m = c->mesh;
+  k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
+  AEROF_LAUNCH_CHECK();
+  const GradStage st = grad_stage(m);
+  const size_t smem = (size_t)2 * st.size * sizeof(double);
+  const int L = kBlock / m.NB;
+  auto go = [&](auto kern) {
+    AEROF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    AEROF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, smem));
+    int sms = 0;
+    AEROF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
+    const int grid = std::max(1, std::min(m.nblk, std::max(per_sm, 1) * sms));
+    kern<<<grid, kBlock, smem, s>>>(m.N, m.NB, m.nblk, m.maxH, m.maxLp, st, m.P2.p, m.W2.p, m.nb2_ptr.p, m.lpad.p,
+                                    m.hpad.p, tag, G2);
+    AEROF_LAUNCH_CHECK();
+  };
+  if (L == 4) go(k_grad_pipe<4>);
+  else if (L == 2) go(k_grad_pipe<2>);
+  else go(k_grad_pipe<1>);
 }
 
 // fused: prim conversion inside the gradient kernel; otherwise
@@ -746,13 +918,17 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
   AEROF_CUDA(cudaFuncSetAttribute(fvk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const size_t gsmem = ((size_t)8 * kPS * (m.NB + m.maxH) + (size_t)2 * m.maxL + 15) / 16 * 16;
   // gradient organisation (tuning knob AEROF_GRAD_KERNEL): 0 staged from
-  // P2, 1 staged with the primitive conversion fused, 2 node-parallel
+  // P2, 1 staged with the primitive conversion fused, 2 node-parallel,
+  // 3 (default) staged, persistent and software pipelined
   const int gk = grad_kernel_choice();
   const bool staged = gsmem <= kMaxStagedSmem && gk != 2;
+  const bool piped = gk == 3 && m.maxH <= 512 && 2 * grad_stage(m).size * sizeof(double) <= kMaxStagedSmem;
   // prim + gradients: staged per block when the block's halo fits, else
   // the node-parallel kernels on the blocked arrays
   auto grad = [&](const int* tg) {
-    if (staged) {
+    if (piped) {
+      launch_grad_pipe(c, g, dU, tg, c->s.G2.p, s);
+    } else if (staged) {
       launch_grad_staged(m, g, dU, tg, c->s.G2.p, gsmem, gk == 1, s);
     } else {
       k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
@@ -773,7 +949,7 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
   }
   auto fv = [&](int fs, int* counter) {
     fvk<<<m.nblk, 256, smem, s>>>(m.N, m.E, m.NB, g, rec, c->cfg.beta, fs, m.bl.p, m.bnorm.p, m.beptr.p,
-                                            m.hfptr.p, m.hfnode.p, m.P2.p, c->s.G2.p, m.lptr.p, m.lidx.p,
+                                            m.hfptr.p, m.hfpad.p, m.maxHf, m.P2.p, c->s.G2.p, m.lptr.p, m.lidx.p,
                                             m.xslot.p, c->s.part.p, c->s.spill.p, c->s.tag.p, counter);
     AEROF_LAUNCH_CHECK();
   };

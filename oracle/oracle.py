@@ -23,7 +23,7 @@ _fp = C.POINTER(C.c_float)
 def build(force: bool = False) -> str:
     """Compile the oracle (g++ -O3 -fopenmp -ffp-contract=off)."""
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
-        cmd = ["g++", "-O3", "-march=native", "-fopenmp", "-ffp-contract=off", "-std=c++17",
+        cmd = ["g++", "-O3", "-march=x86-64-v3", "-fopenmp", "-ffp-contract=off", "-std=c++17",
                "-shared", "-fPIC", SRC, "-o", LIB]
         subprocess.check_call(cmd)
     return LIB

@@ -46,7 +46,7 @@ EXPORTS = [
     "aerof_gpu_residual", "aerof_gpu_gradients", "aerof_gpu_timestep", "aerof_gpu_rk2",
     "aerof_gpu_jacobian", "aerof_gpu_get_jacobian", "aerof_gpu_matvec", "aerof_gpu_prec_setup",
     "aerof_gpu_prec_apply", "aerof_gpu_gmres", "aerof_gpu_newton",
-    "aerof_gpu_jvp", "aerof_gpu_vjp", "aerof_gpu_dRdX", "aerof_gpu_dRdX_T",
+    "aerof_gpu_jvp", "aerof_gpu_vjp", "aerof_gpu_dRdX", "aerof_gpu_dRdX_T", "aerof_gpu_adjoint_products",
     "aerof_gpu_residual_async", "aerof_gpu_status", "aerof_gpu_profile", "aerof_gpu_timers",
     "aerof_gpu_update_coordinates", "aerof_gpu_linearized_solve", "aerof_gpu_residual_noalloc",
 ]
@@ -115,6 +115,7 @@ def library(path: str | None = None):
             "aerof_gpu_vjp": [vp, dp, dp, dp],
             "aerof_gpu_dRdX": [vp, dp, dp, dp],
             "aerof_gpu_dRdX_T": [vp, dp, dp, dp],
+            "aerof_gpu_adjoint_products": [vp, dp, dp, dp, dp],
             "aerof_gpu_residual_async": [vp, dp, dp],
             "aerof_gpu_status": [vp],
             "aerof_gpu_profile": [vp, C.c_int],
@@ -500,6 +501,16 @@ class Sensitivity:
 
     def dRdX_T(self, U, lam):
         return self._call(self.ctx.L.aerof_gpu_dRdX_T, U, lam, 5, 3)
+
+    def adjoint_products(self, U, lam):
+        """(J^T lam, (dR/dX)^T lam) from one reverse sweep."""
+        ctx = self.ctx
+        u = _Arg(U, np.float64, (ctx.N, 5))
+        l = _Arg(lam, np.float64, (ctx.N, 5))
+        a = _Arg(_like(lam, (ctx.N, 5)), np.float64, writable=True)
+        b = _Arg(_like(lam, (ctx.N, 3)), np.float64, writable=True)
+        ctx._check(ctx.L.aerof_gpu_adjoint_products(ctx.h, u.ptr, l.ptr, a.ptr, b.ptr))
+        return a.obj, b.obj
 
     def solve(self, U, b, transpose=False, krylov=30, maxits=300, eps=1e-10, inner_its=0):
         """Solve J x = b (direct) or J^T x = b (adjoint) with the exact

@@ -624,8 +624,9 @@ __global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const
   gX[3 * (size_t)q + 2] = gx[2];
 }
 
-// (dR/dX)^T lambda for device state dU, cotangent dlam, into dgX [N][3].
-void dRdX_T_dev(aerof_gpu_ctx* c, const double* dU, const double* dlam, double* dgX) {
+// (dR/dX)^T lambda for device state dU, cotangent dlam, into dgX [N][3];
+// with dJT also J^T lambda into dJT [N][5] from the same reverse sweep.
+void dRdX_T_dev(aerof_gpu_ctx* c, const double* dU, const double* dlam, double* dgX, double* dJT = nullptr) {
   DeviceMesh& m = c->mesh;
   AdjWork& a = c->adj;
   cudaStream_t s = c->stream;
@@ -635,7 +636,12 @@ void dRdX_T_dev(aerof_gpu_ctx* c, const double* dU, const double* dlam, double* 
   const size_t n5 = 5 * (size_t)m.N;
   c->s.k2.ensure(n5);
   double* R = c->s.k2.p;
-  residual_dev(c, dU, R);  // also leaves P (V, X) and G (gradients) current
+  residual_dev(c, dU, R);
+  // the node records P and gradients G in the caller's numbering (the
+  // blocked residual keeps its own copies)
+  prim_dev(c, dU);
+  c->s.G.ensure(16 * (size_t)m.N);
+  if (rec != AEROF_REC_CONSTANT) gradients_dev(c);
   a.lam.ensure(n5);
   a.edge.ensure(32 * (size_t)m.E);
   a.gV.ensure(n5);
@@ -654,11 +660,18 @@ void dRdX_T_dev(aerof_gpu_ctx* c, const double* dU, const double* dlam, double* 
                                                          a.lam.p, a.gfn.p);
     AEROF_LAUNCH_CHECK();
   }
-  if (rec != AEROF_REC_CONSTANT) {
+  if (rec != AEROF_REC_CONSTANT || dJT) {
     k_a_node<<<gn, kAB, 0, s>>>(m.N, m.F, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_node.p, m.nbr_edge.p, a.edge.p, m.nf_ptr.p,
                                 m.nf_face.p, m.fcode.p, m.fnrm.p, m.P.p, a.lam.p, a.gV.p, a.gG.p);
     AEROF_LAUNCH_CHECK();
+  }
+  if (rec != AEROF_REC_CONSTANT) {
     k_a_lsq_x<<<gn, kAB, 0, s>>>(m.N, m.P.p, m.lsqR.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, a.gG.p, a.gd.p);
+    AEROF_LAUNCH_CHECK();
+  }
+  if (dJT) {
+    k_a_lsq_prim<<<gn, kAB, 0, s>>>(m.N, g, rec, dU, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, a.gV.p, a.gG.p,
+                                    dJT);
     AEROF_LAUNCH_CHECK();
   }
   k_a_gather_x<<<gn, kAB, 0, s>>>(m.N, rec, m.X.p, m.tets.p, m.tet_edge.p, m.faces.p, m.nbr_ptr.p, m.nbr_edge.p,
@@ -718,6 +731,23 @@ extern "C" int aerof_gpu_vjp(aerof_gpu_ctx* c, const double* U, const double* w,
     double* dout = out_dev(c, JTw, n, c->s.Rstage);
     vjp_dev(c, dU, dw, dout);
     out_finish(c, JTw, dout, n);
+    return AEROF_OK;
+  });
+}
+
+extern "C" int aerof_gpu_adjoint_products(aerof_gpu_ctx* c, const double* U, const double* lambda, double* JTl,
+                                          double* gX) {
+  return guard(c, [&]() -> int {
+    if (int e = need(c)) return e;
+    if (!U || !lambda || !JTl || !gX) return AEROF_EINVAL;
+    const size_t N = c->mesh.N;
+    const double* dU = in_dev(c, U, 5 * N, c->s.Ustage);
+    const double* dl = in_dev(c, lambda, 5 * N, c->s.Vstage);
+    double* dJ = out_dev(c, JTl, 5 * N, c->s.Rstage);
+    double* dg = out_dev(c, gX, 3 * N, c->s.Xstage);
+    dRdX_T_dev(c, dU, dl, dg, dJ);
+    out_finish(c, JTl, dJ, 5 * N);
+    out_finish(c, gX, dg, 3 * N);
     return AEROF_OK;
   });
 }

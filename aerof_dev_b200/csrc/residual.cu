@@ -299,12 +299,15 @@ __global__ void __launch_bounds__(256, 2) k_grad_pipe(int N, int NB, int nblk, i
 #pragma unroll
       for (int c = 0; c < 4; ++c) cp_async16(rec + (kPS / 2) * (nn + tid + 256) + c, src + c);
     }
-    if (tid < nn) {
+    // every copy below loops over the block's extent: a segment may be
+    // longer than one copy per thread (the local slots of a 256-node block
+    // are ~3600 entries, 16-byte copies carry 8)
+    for (int k = tid; k < nn; k += blockDim.x) {
 #pragma unroll
-      for (int a = 0; a < 6; ++a) cp_async8(S + st.w + a * NB + tid, W2 + (size_t)a * N + n0 + tid);
+      for (int a = 0; a < 6; ++a) cp_async8(S + st.w + a * NB + k, W2 + (size_t)a * N + n0 + k);
     }
-    if (4 * tid < nn + 1) cp_async16(S + st.ptr + 2 * tid, nb2_ptr + n0 + 4 * tid);
-    if (8 * tid < maxLp) cp_async16(S + st.ls + 2 * tid, lpad + (size_t)b * maxLp + 8 * tid);
+    for (int k = tid; 4 * k < nn + 1; k += blockDim.x) cp_async16(S + st.ptr + 2 * k, nb2_ptr + n0 + 4 * k);
+    for (int k = tid; 8 * k < maxLp; k += blockDim.x) cp_async16(S + st.ls + 2 * k, lpad + (size_t)b * maxLp + 8 * k);
   };
   int b = blockIdx.x;
   if (b >= nblk) return;

@@ -248,6 +248,12 @@ int aerof_gpu_dRdX(aerof_gpu_ctx* ctx, const double* U, const double* Xdot, doub
 /* gX = (dR/dX)^T . lambda, gX[N][3] (fsoApply_dFdXtranspose,
  * FluidShapeOptimizationHandler.C:1434-1448)                               */
 int aerof_gpu_dRdX_T(aerof_gpu_ctx* ctx, const double* U, const double* lambda, double* gX);
+/* Both products of the adjoint gradient from one reverse sweep over the
+ * edges: JTl = (dR/dU)^T . lambda and gX = (dR/dX)^T . lambda (the two
+ * operators fsoComputeAdjoint and fsoApply_dFdXtranspose apply,
+ * FluidShapeOptimizationHandler.C:1434-1448, 2475-2502).                  */
+int aerof_gpu_adjoint_products(aerof_gpu_ctx* ctx, const double* U, const double* lambda, double* JTl,
+                               double* gX);
 
 /* Linearised steady solves with the exact Jacobian applied matrix-free
  * (fsoLinearSolver / fsoAdjointLinearSolver, FluidShapeOptimizationHandler.C:

@@ -109,3 +109,23 @@ def test_transposed_assembly_is_the_transpose(gpu_lib, case):
     assert np.array_equal(GT, mv.blocks())
     assert rel_l2(mv.apply(p, transpose=True), yT) < 1e-15
     assert rel_l2(mv.apply(p), y) < 1e-15
+
+
+def test_dRdX_T_fresh_context_and_fused_products(gpu_lib, case):
+    # a fresh context whose first call is the reverse product (no earlier
+    # call has left node records or gradients behind), and the fused sweep
+    # returning both adjoint products
+    rec, m, Ub, o, U, _ = case
+    ctx = gpu_lib.Context.from_mesh(m, Ub, reconstruction=rec)
+    S = gpu_lib.Sensitivity(ctx)
+    rng = np.random.default_rng(19)
+    lam = rng.standard_normal(U.shape)
+    Xdot = rng.standard_normal(m["X"].shape)
+    gX = S.dRdX_T(U, lam)
+    ref, _ = o.dRdX(U, Ub, Xdot, order=rec)
+    a, b = np.sum(lam * ref), np.sum(gX * Xdot)
+    assert abs(a - b) <= 1e-10 * max(abs(a), 1e-300)
+    ctx2 = gpu_lib.Context.from_mesh(m, Ub, reconstruction=rec)
+    JTl, gX2 = gpu_lib.Sensitivity(ctx2).adjoint_products(U, lam)
+    assert rel_l2(gX2, gX) < 1e-14
+    assert rel_l2(JTl, S.vjp(U, lam)) < 1e-14

@@ -22,49 +22,82 @@ namespace aerof {
 constexpr int kIB = 256;
 constexpr int kGB = 1184;  // reduction grid: 8 x 148 SMs
 
-// Sliced block layout (SELL-32): rows in slices of 32; element e of block k
-// of row r = 32 s + l at ((sptr[s] + k) * 25 + e) * 32 + l, so the 32 rows of
-// a warp read each block element as one 128-byte (FP32) line; diagonal
-// blocks and their inverses at (s * 25 + e) * 32 + l.
-__device__ __forceinline__ size_t sl_off(const int* __restrict__ sptr, int r, int k, int e) {
-  return (((size_t)sptr[r >> 5] + k) * 25 + e) * 32 + (r & 31);
+// Sliced block layout (SELL-32): rows in slices of 32 (row r = 32 s + l);
+// block k of the rows of slice s occupies 800 consecutive elements at
+// (sptr[s] + k) * 800 (the diagonal blocks and their inverses at s * 800).
+// Inside, elements 0..23 of lane l are stored as W-wide vectors (W = 4 for
+// FP32, 2 for FP64: 16 bytes) at ((e / W) * 32 + l) * W + e % W and element
+// 24 at 768 + l, so a warp reads a block as 16-byte loads of consecutive
+// lanes, one coalesced 512-byte line per vector, with no padding.
+template <class S> struct SlW { static constexpr int W = 16 / (int)sizeof(S); };
+template <class S>
+__host__ __device__ __forceinline__ size_t sl_el(int e, int l) {
+  constexpr int W = SlW<S>::W;
+  return e < 24 ? ((size_t)(e / W) * 32 + l) * W + e % W : (size_t)768 + l;
 }
-__device__ __forceinline__ size_t sl_diag(int r, int e) { return ((size_t)(r >> 5) * 25 + e) * 32 + (r & 31); }
+__device__ __forceinline__ size_t sl_blk(const int* __restrict__ sptr, int r, int k) {
+  return ((size_t)sptr[r >> 5] + k) * 800;
+}
+__device__ __forceinline__ size_t sl_dblk(int r) { return (size_t)(r >> 5) * 800; }
+
+// the 25 elements of lane l's block at base b, as doubles
+template <class S>
+__device__ __forceinline__ void load_block(const S* __restrict__ a, size_t b, int l, double* v);
+template <>
+__device__ __forceinline__ void load_block<float>(const float* __restrict__ a, size_t b, int l, double* v) {
+  const float4* q = reinterpret_cast<const float4*>(a + b) + l;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    const float4 t = q[32 * i];
+    v[4 * i] = t.x; v[4 * i + 1] = t.y; v[4 * i + 2] = t.z; v[4 * i + 3] = t.w;
+  }
+  v[24] = a[b + 768 + l];
+}
+template <>
+__device__ __forceinline__ void load_block<double>(const double* __restrict__ a, size_t b, int l, double* v) {
+  const double2* q = reinterpret_cast<const double2*>(a + b) + l;
+#pragma unroll
+  for (int i = 0; i < 12; ++i) {
+    const double2 t = q[32 * i];
+    v[2 * i] = t.x; v[2 * i + 1] = t.y;
+  }
+  v[24] = a[b + 768 + l];
+}
 
 // v * scale rounded to S, written as block k of row r (TR: the transposed
 // block), and the same for a diagonal block
 template <class S, bool TR>
 __device__ __forceinline__ void store_off(S* __restrict__ off, const int* __restrict__ sptr, int r, int k,
                                           const double* v, double scale) {
-  const size_t b = sl_off(sptr, r, k, 0);
+  const size_t b = sl_blk(sptr, r, k);
 #pragma unroll
-  for (int e = 0; e < 25; ++e) off[b + (size_t)32 * e] = (S)(v[TR ? 5 * (e % 5) + e / 5 : e] * scale);
+  for (int e = 0; e < 25; ++e) off[b + sl_el<S>(e, r & 31)] = (S)(v[TR ? 5 * (e % 5) + e / 5 : e] * scale);
 }
 template <class S, bool TR>
 __device__ __forceinline__ void store_diag(S* __restrict__ diag, int r, const double* v) {
-  const size_t b = sl_diag(r, 0);
+  const size_t b = sl_dblk(r);
 #pragma unroll
-  for (int e = 0; e < 25; ++e) diag[b + (size_t)32 * e] = (S)v[TR ? 5 * (e % 5) + e / 5 : e];
+  for (int e = 0; e < 25; ++e) diag[b + sl_el<S>(e, r & 31)] = (S)v[TR ? 5 * (e % 5) + e / 5 : e];
 }
 
-// Half a warp per row r: lane l takes the row's neighbours s at positions
-// l, l+16, ... of its ascending neighbour list.  For the edge e = (r, s)
-// (r first endpoint, sg = +1) or (s, r) (r second, sg = -1) it evaluates the
-// approximate Roe Jacobians at the un-reconstructed states
-// (roejacappr3Dgas, FluxFcnDescSG.C:155-262; roe_jac(n, Va, Vb, +1) is
-// dF/dU of the first endpoint a, roe_jac(n, Va, Vb, -1) of the second): the
-// off-diagonal block A_rs = sg dF/dU_s / vol_r and the contribution
-// sg dF/dU_r to the diagonal block (Edge.C:4503-4523).  The lanes then take
-// the row's boundary faces (Face.C:814-847) the same way; the 16 partial
-// diagonal sums are added in a fixed xor tree, times 1/vol
-// (SubDomain.C:1760-1765), + I/dt (TimeState.C:731-756).  Every edge's two
-// Jacobians are evaluated once by each of its two rows, which costs twice
-// the arithmetic of an edge loop but needs no scratch for the diagonal.
-// TR: the transpose H1^T is stored instead (block k of row r = A_sr^T, with
-// A_sr = -sg dF/dU_r / vol_s, the Jacobian already formed for the
-// diagonal), for products with the transpose that read coalesced.
+// One thread per row r; a warp is one slice of the sliced layout, so for
+// each neighbour position k the 32 rows write every block element as one
+// coalesced line.  For the edge e = (r, s) (r first endpoint, sg = +1) or
+// (s, r) (r second, sg = -1) the approximate Roe Jacobians at the
+// un-reconstructed states (roejacappr3Dgas, FluxFcnDescSG.C:155-262;
+// roejac(n, Va, Vb, +1) = dF/dU of the first endpoint a, (.., -1) of the
+// second) give the off-diagonal block A_rs = sg dF/dU_s / vol_r and the
+// contribution sg dF/dU_r to the diagonal block (Edge.C:4503-4523).  Both
+// Jacobians share the Roe dissipation matrix D, formed one column at a
+// time with the convective parts H(V_s), H(V_r), so no 25-element block is
+// held in registers besides the diagonal sum.  Then the row's boundary
+// faces (Face.C:814-847), times 1/vol (SubDomain.C:1760-1765), + I/dt
+// (TimeState.C:731-756).  Every edge's Jacobians are evaluated once by each
+// of its two rows.  TR: the transpose H1^T is stored instead (block k of
+// row r = A_sr^T with A_sr = -sg dF/dU_r / vol_s, the Jacobian formed for
+// the diagonal), for products with the transpose that read coalesced.
 template <class S, bool TR>
-__global__ void __launch_bounds__(256) k_jac_rows(int N, int E, int F, Gas g, const double* __restrict__ Ub0,
+__global__ void __launch_bounds__(128) k_jac_rows(int N, int E, int F, Gas g, const double* __restrict__ Ub0,
                                                   const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_node,
                                                   const int* __restrict__ nbr_edge, const double* __restrict__ en,
                                                   const double* __restrict__ P, const double* __restrict__ vol,
@@ -72,118 +105,112 @@ __global__ void __launch_bounds__(256) k_jac_rows(int N, int E, int F, Gas g, co
                                                   const int* __restrict__ fcode, const double* __restrict__ fn,
                                                   const double* __restrict__ dt, const int* __restrict__ sptr,
                                                   S* __restrict__ off, S* __restrict__ diag) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int r = t >> 4, l = t & 15;
-  const bool act = r < N;
-  double a[25];
+  // the diagonal sum lives in shared memory (element k of this thread at
+  // a[128 k], conflict-free), which keeps the register count low enough
+  // for several CTAs per SM
+  __shared__ double sdiag[25 * 128];
+  double* a = sdiag + threadIdx.x;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= N) return;
 #pragma unroll
-  for (int k = 0; k < 25; ++k) a[k] = 0.0;
-  if (act) {
-    double Vr[5];
+  for (int k = 0; k < 25; ++k) a[128 * k] = 0.0;
+  double Vr[5];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) Vr[k] = P[8 * (size_t)r + k];
-    const double volr = 1.0 / vol[r];
-    const int p0 = nbr_ptr[r], p1 = nbr_ptr[r + 1];
-    for (int p = p0 + l; p < p1; p += 16) {
-      const int s = nbr_node[p];
-      const int er = nbr_edge[p];
-      const size_t e = (size_t)(er & 0x7fffffff);
-      const double sg = er < 0 ? -1.0 : 1.0;
-      const double n0 = en[e], n1 = en[(size_t)E + e], n2 = en[2 * (size_t)E + e];
-      double Vs[5];
+  for (int k = 0; k < 5; ++k) Vr[k] = P[8 * (size_t)r + k];
+  const double volr = 1.0 / vol[r];
+  const int p0 = nbr_ptr[r], p1 = nbr_ptr[r + 1];
+  for (int p = p0; p < p1; ++p) {
+    const int s = nbr_node[p];
+    const int er = nbr_edge[p];
+    const size_t e = (size_t)(er & 0x7fffffff);
+    const double sg = er < 0 ? -1.0 : 1.0;
+    const double n0 = en[e], n1 = en[(size_t)E + e], n2 = en[2 * (size_t)E + e];
+    double Vs[5];
 #pragma unroll
-      for (int k = 0; k < 5; ++k) Vs[k] = P[8 * (size_t)s + k];
-      const double rnorm = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
-      const bool zero = rnorm < 1e-18;
-      // roe_jac(n, Vs, Vr, -sg) and roe_jac(n, Vr, Vs, sg) share the
-      // dissipation matrix D: form it once, then (H(V) +- D) |n| / 2
-      double jac[25];
-      double D[25], H[25];
-      double un[3];
-      const double invnorm = 1.0 / rnorm;
-      un[0] = n0 * invnorm; un[1] = n1 * invnorm; un[2] = n2 * invnorm;
-      const double half_rn = 0.5 * rnorm;
-      if (!zero) roe_jac_D(g, un, Vr, Vs, D);
-      if (!TR) {
-        if (zero) {
+    for (int k = 0; k < 5; ++k) Vs[k] = P[8 * (size_t)s + k];
+    const double rnorm = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+    const size_t b = sl_blk(sptr, r, p - p0);
+    const int lane = r & 31;
+    if (rnorm < 1e-18) {
 #pragma unroll
-          for (int k = 0; k < 25; ++k) jac[k] = 0.0;
+      for (int k = 0; k < 25; ++k) off[b + sl_el<S>(k, lane)] = (S)0.0;
+      continue;
+    }
+    const double invnorm = 1.0 / rnorm;
+    const double un[3] = {n0 * invnorm, n1 * invnorm, n2 * invnorm};
+    const double half_rn = 0.5 * rnorm;
+    const double sco = TR ? -sg * (1.0 / vol[s]) : sg * volr;
+    const RoeAvg A = roe_avg(g, un, Vr, Vs);
+    const HState hr = h_state(g, un, Vr), hs = h_state(g, un, Vs);
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      double d[5];
+      D_col(g, A, un, j, d);
+#pragma unroll
+      for (int m = 0; m < 5; ++m) {
+        const int el = 5 * m + j;
+        // diagonal contribution: roejac(n, Vr, Vs, sg)
+        const double jd = (H_elem(g, hr, un, el) + sg * d[m]) * half_rn;
+        a[128 * el] += sg * jd;
+        if (TR) {
+          off[b + sl_el<S>(5 * j + m, lane)] = (S)(jd * sco);
         } else {
-          roe_jac_H(g, un, Vs, H);
-#pragma unroll
-          for (int k = 0; k < 25; ++k) jac[k] = (H[k] + (-sg) * D[k]) * half_rn;
+          // off-diagonal block: roejac(n, Vs, Vr, -sg)
+          const double jo = (H_elem(g, hs, un, el) + (-sg) * d[m]) * half_rn;
+          off[b + sl_el<S>(el, lane)] = (S)(jo * sco);
         }
-        store_off<S, false>(off, sptr, r, p - p0, jac, sg * volr);
-      }
-      if (zero) {
-#pragma unroll
-        for (int k = 0; k < 25; ++k) jac[k] = 0.0;
-      } else {
-        roe_jac_H(g, un, Vr, H);
-#pragma unroll
-        for (int k = 0; k < 25; ++k) {
-          jac[k] = (H[k] + sg * D[k]) * half_rn;
-          a[k] += sg * jac[k];
-        }
-      }
-      if (TR) store_off<S, true>(off, sptr, r, p - p0, jac, -sg * (1.0 / vol[s]));
-    }
-    const int q1 = nf_ptr[r + 1];
-    if (nf_ptr[r] + l < q1) {
-      double Ub[5];
-#pragma unroll
-      for (int k = 0; k < 5; ++k) Ub[k] = Ub0[k];
-      const double third = 1.0 / 3.0;
-      for (int q = nf_ptr[r] + l; q < q1; q += 16) {
-        const int f = nf_face[q];
-        double jac[25];
-        face_jac(g, fcode[f], third * fn[f], third * fn[(size_t)F + f], third * fn[2 * (size_t)F + f], Vr, Ub, jac);
-#pragma unroll
-        for (int k = 0; k < 25; ++k) a[k] += jac[k];
       }
     }
   }
+  const int q1 = nf_ptr[r + 1];
+  if (nf_ptr[r] < q1) {
+    double Ub[5];
 #pragma unroll
-  for (int k = 0; k < 25; ++k) {
-    a[k] += __shfl_xor_sync(0xffffffffu, a[k], 8);
-    a[k] += __shfl_xor_sync(0xffffffffu, a[k], 4);
-    a[k] += __shfl_xor_sync(0xffffffffu, a[k], 2);
-    a[k] += __shfl_xor_sync(0xffffffffu, a[k], 1);
+    for (int k = 0; k < 5; ++k) Ub[k] = Ub0[k];
+    const double third = 1.0 / 3.0;
+    for (int q = nf_ptr[r]; q < q1; ++q) {
+      const int f = nf_face[q];
+      double jac[25];
+      face_jac(g, fcode[f], third * fn[f], third * fn[(size_t)F + f], third * fn[2 * (size_t)F + f], Vr, Ub, jac);
+#pragma unroll
+      for (int k = 0; k < 25; ++k) a[128 * k] += jac[k];
+    }
   }
-  if (!act || l != 0) return;
-  const double voli = 1.0 / vol[r];
+  double v[25];
 #pragma unroll
-  for (int k = 0; k < 25; ++k) a[k] *= voli;
+  for (int k = 0; k < 25; ++k) v[k] = a[128 * k] * volr;
   if (dt) {
     const double c = 1.0 / dt[r];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) a[6 * k] += c;
+    for (int k = 0; k < 5; ++k) v[6 * k] += c;
   }
-  store_diag<S, TR>(diag, r, a);
+  store_diag<S, TR>(diag, r, v);
 }
 
-// y += A x for a 5x5 block of the sliced layout (element e at b + 32 e),
-// or A^T x; FP64 accumulation in the order of a row-major gemv
+// y += A x (or A^T x) for the block of lane l at base b of the sliced
+// layout; FP64 accumulation in the order of a row-major gemv
 template <class S, class TX>
-__device__ __forceinline__ void gemv_sl(const S* __restrict__ a, size_t b, const TX* __restrict__ x, double* y,
+__device__ __forceinline__ void gemv_sl(const S* __restrict__ a, size_t b, int l, const TX* __restrict__ x, double* y,
                                         bool trans) {
+  double av[25];
+  load_block<S>(a, b, l, av);
   double xv[5];
 #pragma unroll
   for (int k = 0; k < 5; ++k) xv[k] = (double)x[k];
   if (!trans) {
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
-      double s = (double)a[b + 32 * (5 * r)] * xv[0];
+      double s = av[5 * r] * xv[0];
 #pragma unroll
-      for (int c = 1; c < 5; ++c) s += (double)a[b + 32 * (5 * r + c)] * xv[c];
+      for (int c = 1; c < 5; ++c) s += av[5 * r + c] * xv[c];
       y[r] += s;
     }
   } else {
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
-      double s = (double)a[b + 32 * r] * xv[0];
+      double s = av[r] * xv[0];
 #pragma unroll
-      for (int c = 1; c < 5; ++c) s += (double)a[b + 32 * (5 * c + r)] * xv[c];
+      for (int c = 1; c < 5; ++c) s += av[5 * c + r] * xv[c];
       y[r] += s;
     }
   }
@@ -203,16 +230,16 @@ __global__ void __launch_bounds__(256) k_spmv(int N, const int* __restrict__ nbr
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= N) return;
   double acc[5] = {0, 0, 0, 0, 0};
-  gemv_sl(diag, sl_diag(r, 0), p + 5 * (size_t)r, acc, TRANS);
+  gemv_sl(diag, sl_dblk(r), r & 31, p + 5 * (size_t)r, acc, TRANS);
   const int p0 = nbr_ptr[r], cnt = nbr_ptr[r + 1] - p0;
   const size_t cb = (size_t)sptr[r >> 5] * 32 + (r & 31);
   for (int k = 0; k < cnt; ++k) {
     const int s = scol[cb + (size_t)32 * k];
     if (!TRANS) {
-      gemv_sl(off, sl_off(sptr, r, k, 0), p + 5 * (size_t)s, acc, false);
+      gemv_sl(off, sl_blk(sptr, r, k), r & 31, p + 5 * (size_t)s, acc, false);
     } else {
       const int kt = nbr_tpos[p0 + k] - nbr_ptr[s];
-      gemv_sl(off, sl_off(sptr, s, kt, 0), p + 5 * (size_t)s, acc, true);
+      gemv_sl(off, sl_blk(sptr, s, kt), s & 31, p + 5 * (size_t)s, acc, true);
     }
   }
 #pragma unroll
@@ -226,17 +253,17 @@ template <class S>
 __global__ void k_bj_invert(int N, const S* __restrict__ diag, S* __restrict__ dinv, int* __restrict__ bad) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  const size_t b = sl_diag(i, 0);
+  const size_t b = sl_dblk(i);
   S a[25];
 #pragma unroll
-  for (int k = 0; k < 25; ++k) a[k] = diag[b + (size_t)32 * k];
+  for (int k = 0; k < 25; ++k) a[k] = diag[b + sl_el<S>(k, i & 31)];
   bool inv = true;
 #pragma unroll
   for (int k = 0; k < 5; ++k)
     if (a[6 * k] == S(0)) inv = false;
   if (inv && invert5<S>(a)) atomicAdd(bad, 1);
 #pragma unroll
-  for (int k = 0; k < 25; ++k) dinv[b + (size_t)32 * k] = a[k];
+  for (int k = 0; k < 25; ++k) dinv[b + sl_el<S>(k, i & 31)] = a[k];
 }
 
 // z = D^-1 x (or D^-T x): JacobiPrec::apply/applyT (KspPrec.C:86-111)
@@ -246,7 +273,7 @@ __global__ void k_bj_apply(int N, const S* __restrict__ dinv, const TI* __restri
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double acc[5] = {0, 0, 0, 0, 0};
-  gemv_sl(dinv, sl_diag(i, 0), x + 5 * (size_t)i, acc, trans != 0);
+  gemv_sl(dinv, sl_dblk(i), i & 31, x + 5 * (size_t)i, acc, trans != 0);
 #pragma unroll
   for (int k = 0; k < 5; ++k) z[5 * (size_t)i + k] = (TO)acc[k];
 }
@@ -387,8 +414,8 @@ static void need_jac(aerof_gpu_ctx* c) {
 // Assemble the H1 operator at device state dU with device time steps ddt
 // (may be null).
 // sizes of the sliced arrays (elements)
-static size_t sl_diag_size(const DeviceMesh& m) { return (size_t)m.nsl * 25 * 32; }
-static size_t sl_off_size(const DeviceMesh& m) { return std::max<size_t>((size_t)m.h_sptr.back() * 25 * 32, 1); }
+static size_t sl_diag_size(const DeviceMesh& m) { return (size_t)m.nsl * 800; }
+static size_t sl_off_size(const DeviceMesh& m) { return std::max<size_t>((size_t)m.h_sptr.back() * 800, 1); }
 
 void jacobian_dev(aerof_gpu_ctx* c, const double* dU, const double* ddt, int precision, bool transposed) {
   DeviceMesh& m = c->mesh;
@@ -396,9 +423,9 @@ void jacobian_dev(aerof_gpu_ctx* c, const double* dU, const double* ddt, int pre
   const Gas g = make_gas(c->cfg.gamma);
   TimerScope tj(c, AEROF_T_FV_JAC);
   prim_dev(c, dU);
-  const int gr = grid_for(16 * (size_t)m.N, kIB);
+  const int gr = grid_for((size_t)m.N, 128);
   auto rows = [&](auto* off, auto* diag, auto kern) {
-    kern<<<gr, kIB, 0, c->stream>>>(m.N, m.E, m.F, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_node.p, m.nbr_edge.p, m.en.p,
+    kern<<<gr, 128, 0, c->stream>>>(m.N, m.E, m.F, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_node.p, m.nbr_edge.p, m.en.p,
                                     m.P.p, m.vol.p, m.nf_ptr.p, m.nf_face.p, m.fcode.p, m.fnrm.p, ddt, m.sptr.p, off,
                                     diag);
     AEROF_LAUNCH_CHECK();
@@ -800,12 +827,14 @@ extern "C" int aerof_gpu_get_jacobian(aerof_gpu_ctx* c, double* A) {
     const std::vector<int>& np = m.h_nbr_ptr;
     const bool T = J.transposed;
     auto el = [&](int e) { return T ? 5 * (e % 5) + e / 5 : e; };
+    const bool f32 = J.precision == AEROF_PREC_FP32;
+    auto elo = [&](int e, int l) { return f32 ? sl_el<float>(e, l) : sl_el<double>(e, l); };
     for (int r = 0; r < m.N; ++r)
-      for (int e = 0; e < 25; ++e) A[25 * (size_t)r + e] = diag[((size_t)(r >> 5) * 25 + el(e)) * 32 + (r & 31)];
+      for (int e = 0; e < 25; ++e) A[25 * (size_t)r + e] = diag[(size_t)(r >> 5) * 800 + elo(el(e), r & 31)];
     auto block = [&](int r, int p, double* dst) {
       // block at CSR position p of row r of H1; with H1^T stored it is the
       // transpose of the mirrored block
-      for (int e = 0; e < 25; ++e) dst[e] = off[(((size_t)sp[r >> 5] + (p - np[r])) * 25 + e) * 32 + (r & 31)];
+      for (int e = 0; e < 25; ++e) dst[e] = off[((size_t)sp[r >> 5] + (p - np[r])) * 800 + elo(e, r & 31)];
     };
     std::vector<int2> epos(m.E);
     AEROF_CUDA(cudaMemcpyAsync(epos.data(), m.edge_pos.p, sizeof(int2) * m.E, cudaMemcpyDeviceToHost, c->stream));

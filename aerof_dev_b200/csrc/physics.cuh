@@ -338,73 +338,142 @@ AEROF_HD void roe_jac_H(const Gas& g, const double* n, const double* Ug, double*
 // written through its eigenvectors (roejac6.f, second block).  The Roe
 // average is symmetric in (Ug, Ud), bit for bit (every sum of the two sides
 // is a commutative two-term addition), so one D serves both endpoints.
-AEROF_HD void roe_jac_D(const Gas& g, const double* n, const double* Ug, const double* Ud, double* D) {
+// RoeAvg holds the scalars of the average; tmw_elem and D_col form the
+// eigenvector matrix and D one column at a time, so a caller can stream
+// the 5x5 blocks without holding 25-element arrays.
+struct RoeAvg {
+  double uar2, uar3, uar4, enth, VdotN, qir, crsq, gc, usc2, rRT, sRT, tRT, vp1, vp4, vp5;
+};
+AEROF_HD RoeAvg roe_avg(const Gas& g, const double* n, const double* Ug, const double* Ud) {
   const double gam1 = g.gam1;
+  RoeAvg A;
   double squsr1 = sqrt(Ug[0]), squsr2 = sqrt(Ud[0]);
   double ener1 = Ug[4] / gam1 + 0.5 * Ug[0] * (Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3]);
   double ener2 = Ud[4] / gam1 + 0.5 * Ud[0] * (Ud[1] * Ud[1] + Ud[2] * Ud[2] + Ud[3] * Ud[3]);
   double usro = 1.0 / (squsr1 + squsr2);
-  double uar2 = (squsr1 * Ug[1] + squsr2 * Ud[1]) * usro;
-  double uar3 = (squsr1 * Ug[2] + squsr2 * Ud[2]) * usro;
-  double uar4 = (squsr1 * Ug[3] + squsr2 * Ud[3]) * usro;
+  A.uar2 = (squsr1 * Ug[1] + squsr2 * Ud[1]) * usro;
+  A.uar3 = (squsr1 * Ug[2] + squsr2 * Ud[2]) * usro;
+  A.uar4 = (squsr1 * Ug[3] + squsr2 * Ud[3]) * usro;
   double uar5 = ((ener1 + Ug[4]) / squsr1 + (ener2 + Ud[4]) / squsr2) * usro;
-  const double enth = uar5;
-  const double VdotN = n[0] * uar2 + n[1] * uar3 + n[2] * uar4;
-  const double qir = 0.5 * (uar2 * uar2 + uar3 * uar3 + uar4 * uar4);
-  double cr = sqrt(gam1 * (uar5 - qir));
-  double crsq = cr * cr;
-  double gc = gam1 / crsq;
-  double usc2 = 0.5 / crsq;
+  A.enth = uar5;
+  A.VdotN = n[0] * A.uar2 + n[1] * A.uar3 + n[2] * A.uar4;
+  A.qir = 0.5 * (A.uar2 * A.uar2 + A.uar3 * A.uar3 + A.uar4 * A.uar4);
+  double cr = sqrt(gam1 * (uar5 - A.qir));
+  A.crsq = cr * cr;
+  A.gc = gam1 / A.crsq;
+  A.usc2 = 0.5 / A.crsq;
   // beta = 1: vp4,vp5 = VdotN +- cr written as the reference's general form
-  double sq = sqrt(0.0 * VdotN * (0.0 * VdotN) + 4.0 * crsq);
-  double vp4 = 0.5 * (2.0 * VdotN + sq);
-  double vp5 = 0.5 * (2.0 * VdotN - sq);
-  double rRT = vp4 - VdotN;
-  double sRT = vp5 - VdotN;
-  double tRT = 0.5 * (vp5 - vp4);
-  double vp1 = fabs(VdotN);
-  vp4 = fabs(vp4);
-  vp5 = fabs(vp5);
-  double tmw[25];
-  tmw[0] = n[0] + n[1] * uar4 - uar3 * n[2] - gc * n[0] * qir;
-  tmw[1] = gc * n[0] * uar2;
-  tmw[2] = gc * n[0] * uar3 + n[2];
-  tmw[3] = gc * n[0] * uar4 - n[1];
-  tmw[4] = -gc * n[0];
-  tmw[5] = n[1] + n[2] * uar2 - uar4 * n[0] - gc * n[1] * qir;
-  tmw[6] = gc * n[1] * uar2 - n[2];
-  tmw[7] = gc * n[1] * uar3;
-  tmw[8] = gc * n[1] * uar4 + n[0];
-  tmw[9] = -gc * n[1];
-  tmw[10] = n[2] + n[0] * uar3 - uar2 * n[1] - gc * n[2] * qir;
-  tmw[11] = gc * n[2] * uar2 + n[1];
-  tmw[12] = gc * n[2] * uar3 - n[0];
-  tmw[13] = gc * n[2] * uar4;
-  tmw[14] = -gc * n[2];
-  tmw[15] = gam1 * qir * sRT / tRT + VdotN * crsq / tRT;
-  tmw[16] = -gam1 * uar2 * sRT / tRT - crsq * n[0] / tRT;
-  tmw[17] = -gam1 * uar3 * sRT / tRT - crsq * n[1] / tRT;
-  tmw[18] = -gam1 * uar4 * sRT / tRT - crsq * n[2] / tRT;
-  tmw[19] = gam1 * sRT / tRT;
-  tmw[20] = -gam1 * qir * rRT / tRT - VdotN * crsq / tRT;
-  tmw[21] = gam1 * uar2 * rRT / tRT + crsq * n[0] / tRT;
-  tmw[22] = gam1 * uar3 * rRT / tRT + crsq * n[1] / tRT;
-  tmw[23] = gam1 * uar4 * rRT / tRT + crsq * n[2] / tRT;
-  tmw[24] = -gam1 * rRT / tRT;
+  double sq = sqrt(0.0 * A.VdotN * (0.0 * A.VdotN) + 4.0 * A.crsq);
+  double vp4 = 0.5 * (2.0 * A.VdotN + sq);
+  double vp5 = 0.5 * (2.0 * A.VdotN - sq);
+  A.rRT = vp4 - A.VdotN;
+  A.sRT = vp5 - A.VdotN;
+  A.tRT = 0.5 * (vp5 - vp4);
+  A.vp1 = fabs(A.VdotN);
+  A.vp4 = fabs(vp4);
+  A.vp5 = fabs(vp5);
+  return A;
+}
+// element e (row-major) of the left eigenvector matrix tmw
+AEROF_HD double tmw_elem(const Gas& g, const RoeAvg& A, const double* n, int e) {
+  const double gam1 = g.gam1;
+  switch (e) {
+    case 0: return n[0] + n[1] * A.uar4 - A.uar3 * n[2] - A.gc * n[0] * A.qir;
+    case 1: return A.gc * n[0] * A.uar2;
+    case 2: return A.gc * n[0] * A.uar3 + n[2];
+    case 3: return A.gc * n[0] * A.uar4 - n[1];
+    case 4: return -A.gc * n[0];
+    case 5: return n[1] + n[2] * A.uar2 - A.uar4 * n[0] - A.gc * n[1] * A.qir;
+    case 6: return A.gc * n[1] * A.uar2 - n[2];
+    case 7: return A.gc * n[1] * A.uar3;
+    case 8: return A.gc * n[1] * A.uar4 + n[0];
+    case 9: return -A.gc * n[1];
+    case 10: return n[2] + n[0] * A.uar3 - A.uar2 * n[1] - A.gc * n[2] * A.qir;
+    case 11: return A.gc * n[2] * A.uar2 + n[1];
+    case 12: return A.gc * n[2] * A.uar3 - n[0];
+    case 13: return A.gc * n[2] * A.uar4;
+    case 14: return -A.gc * n[2];
+    case 15: return gam1 * A.qir * A.sRT / A.tRT + A.VdotN * A.crsq / A.tRT;
+    case 16: return -gam1 * A.uar2 * A.sRT / A.tRT - A.crsq * n[0] / A.tRT;
+    case 17: return -gam1 * A.uar3 * A.sRT / A.tRT - A.crsq * n[1] / A.tRT;
+    case 18: return -gam1 * A.uar4 * A.sRT / A.tRT - A.crsq * n[2] / A.tRT;
+    case 19: return gam1 * A.sRT / A.tRT;
+    case 20: return -gam1 * A.qir * A.rRT / A.tRT - A.VdotN * A.crsq / A.tRT;
+    case 21: return gam1 * A.uar2 * A.rRT / A.tRT + A.crsq * n[0] / A.tRT;
+    case 22: return gam1 * A.uar3 * A.rRT / A.tRT + A.crsq * n[1] / A.tRT;
+    case 23: return gam1 * A.uar4 * A.rRT / A.tRT + A.crsq * n[2] / A.tRT;
+    default: return -gam1 * A.rRT / A.tRT;
+  }
+}
+// column j of D: d[m] = D[5 m + j]
+AEROF_HD void D_col(const Gas& g, const RoeAvg& A, const double* n, int j, double* d) {
+  const double t0 = tmw_elem(g, A, n, j), t1 = tmw_elem(g, A, n, 5 + j), t2 = tmw_elem(g, A, n, 10 + j);
+  const double t3 = tmw_elem(g, A, n, 15 + j), t4 = tmw_elem(g, A, n, 20 + j);
+  const double uar2 = A.uar2, uar3 = A.uar3, uar4 = A.uar4, qir = A.qir, usc2 = A.usc2, rRT = A.rRT, sRT = A.sRT;
+  const double vp1 = A.vp1, vp4 = A.vp4, vp5 = A.vp5, enth = A.enth, VdotN = A.VdotN;
+  d[0] = vp1 * (n[0] * t0 + n[1] * t1 + n[2] * t2) + vp4 * usc2 * t3 + vp5 * usc2 * t4;
+  d[1] = vp1 * (n[0] * uar2 * t0 + (n[1] * uar2 - n[2]) * t1 + (n[2] * uar2 + n[1]) * t2) +
+         vp4 * (usc2 * (uar2 + rRT * n[0])) * t3 + vp5 * (usc2 * (uar2 + sRT * n[0])) * t4;
+  d[2] = vp1 * (n[1] * uar3 * t1 + (n[0] * uar3 + n[2]) * t0 + (n[2] * uar3 - n[0]) * t2) +
+         vp4 * (usc2 * (uar3 + rRT * n[1])) * t3 + vp5 * (usc2 * (uar3 + sRT * n[1])) * t4;
+  d[3] = vp1 * (n[2] * uar4 * t2 + (n[0] * uar4 - n[1]) * t0 + (n[1] * uar4 + n[0]) * t1) +
+         vp4 * (usc2 * (uar4 + rRT * n[2])) * t3 + vp5 * (usc2 * (uar4 + sRT * n[2])) * t4;
+  d[4] = vp1 * ((n[0] * qir + (n[2] * uar3 - n[1] * uar4)) * t0 + (n[1] * qir + (n[0] * uar4 - n[2] * uar2)) * t1 +
+                (n[2] * qir + (n[1] * uar2 - n[0] * uar3)) * t2) +
+         vp4 * (usc2 * (enth + VdotN * rRT)) * t3 + vp5 * (usc2 * (enth + VdotN * sRT)) * t4;
+}
+AEROF_HD void roe_jac_D(const Gas& g, const double* n, const double* Ug, const double* Ud, double* D) {
+  const RoeAvg A = roe_avg(g, n, Ug, Ud);
 #pragma unroll
   for (int j = 0; j < 5; ++j) {
-    double t0 = tmw[j], t1 = tmw[5 + j], t2 = tmw[10 + j], t3 = tmw[15 + j], t4 = tmw[20 + j];
-    D[j] = vp1 * (n[0] * t0 + n[1] * t1 + n[2] * t2) + vp4 * usc2 * t3 + vp5 * usc2 * t4;
-    D[5 + j] = vp1 * (n[0] * uar2 * t0 + (n[1] * uar2 - n[2]) * t1 + (n[2] * uar2 + n[1]) * t2) +
-               vp4 * (usc2 * (uar2 + rRT * n[0])) * t3 + vp5 * (usc2 * (uar2 + sRT * n[0])) * t4;
-    D[10 + j] = vp1 * (n[1] * uar3 * t1 + (n[0] * uar3 + n[2]) * t0 + (n[2] * uar3 - n[0]) * t2) +
-                vp4 * (usc2 * (uar3 + rRT * n[1])) * t3 + vp5 * (usc2 * (uar3 + sRT * n[1])) * t4;
-    D[15 + j] = vp1 * (n[2] * uar4 * t2 + (n[0] * uar4 - n[1]) * t0 + (n[1] * uar4 + n[0]) * t1) +
-                vp4 * (usc2 * (uar4 + rRT * n[2])) * t3 + vp5 * (usc2 * (uar4 + sRT * n[2])) * t4;
-    D[20 + j] = vp1 * ((n[0] * qir + (n[2] * uar3 - n[1] * uar4)) * t0 +
-                       (n[1] * qir + (n[0] * uar4 - n[2] * uar2)) * t1 +
-                       (n[2] * qir + (n[1] * uar2 - n[0] * uar3)) * t2) +
-                vp4 * (usc2 * (enth + VdotN * rRT)) * t3 + vp5 * (usc2 * (enth + VdotN * sRT)) * t4;
+    double d[5];
+    D_col(g, A, n, j, d);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) D[5 * m + j] = d[m];
+  }
+}
+
+// Scalars of the convective Jacobian H(U) (see roe_jac_H) and its element
+// e (row-major), for streaming use.
+struct HState {
+  double U1, U2, U3, VdotN, qir, enth;
+};
+AEROF_HD HState h_state(const Gas& g, const double* n, const double* Ug) {
+  HState h;
+  h.U1 = Ug[1]; h.U2 = Ug[2]; h.U3 = Ug[3];
+  h.VdotN = Ug[1] * n[0] + Ug[2] * n[1] + Ug[3] * n[2];
+  h.qir = 0.5 * (Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3]);
+  h.enth = (g.gam * Ug[4] + g.gam1 * Ug[0] * h.qir) / (g.gam1 * Ug[0]);
+  return h;
+}
+AEROF_HD double H_elem(const Gas& g, const HState& h, const double* n, int e) {
+  const double gam1 = g.gam1;
+  switch (e) {
+    case 0: return 0.0;
+    case 1: return n[0];
+    case 2: return n[1];
+    case 3: return n[2];
+    case 4: return 0.0;
+    case 5: return gam1 * n[0] * h.qir - h.U1 * h.VdotN;
+    case 6: return (1.0 - gam1) * n[0] * h.U1 + h.VdotN;
+    case 7: return -gam1 * n[0] * h.U2 + h.U1 * n[1];
+    case 8: return -gam1 * n[0] * h.U3 + h.U1 * n[2];
+    case 9: return gam1 * n[0];
+    case 10: return gam1 * n[1] * h.qir - h.U2 * h.VdotN;
+    case 11: return -gam1 * n[1] * h.U1 + h.U2 * n[0];
+    case 12: return (1.0 - gam1) * n[1] * h.U2 + h.VdotN;
+    case 13: return -gam1 * n[1] * h.U3 + h.U2 * n[2];
+    case 14: return gam1 * n[1];
+    case 15: return gam1 * n[2] * h.qir - h.U3 * h.VdotN;
+    case 16: return -gam1 * n[2] * h.U1 + h.U3 * n[0];
+    case 17: return -gam1 * n[2] * h.U2 + h.U3 * n[1];
+    case 18: return (1.0 - gam1) * n[2] * h.U3 + h.VdotN;
+    case 19: return gam1 * n[2];
+    case 20: return (gam1 * h.qir - h.enth) * h.VdotN;
+    case 21: return h.enth * n[0] - gam1 * h.U1 * h.VdotN;
+    case 22: return h.enth * n[1] - gam1 * h.U2 * h.VdotN;
+    case 23: return h.enth * n[2] - gam1 * h.U3 * h.VdotN;
+    default: return (1.0 + gam1) * h.VdotN;
   }
 }
 

@@ -455,8 +455,8 @@ __global__ void k_edge_flux(int E, Gas g, int rec, double beta, int failsafe, co
 // block also go to spill[].  Phase 2: thread t sums, for node blk*NB+t, its
 // edges held in shared memory in ascending edge order (+ as first endpoint,
 // - as second) into part[].
-template <int MINB>
-__global__ void __launch_bounds__(256, MINB) k_fv_blocked(int N, int E, int NB, Gas g, int rec, double beta, int failsafe,
+template <int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) k_fv_blocked(int N, int E, int NB, Gas g, int rec, double beta, int failsafe,
                                                     const ushort2* __restrict__ bl, const double* __restrict__ bn,
                                                     const int* __restrict__ beptr, const int* __restrict__ hfptr,
                                                     const int* __restrict__ hfpad, int maxHf,
@@ -472,6 +472,13 @@ __global__ void __launch_bounds__(256, MINB) k_fv_blocked(int N, int E, int NB, 
   const int h0 = hfptr[blk], nh = hfptr[blk + 1] - h0;
   const int ns = nn + nh;
   const int e0 = beptr[blk], e1 = beptr[blk + 1];
+  // phase 2: L lanes per node (the largest power of two with NB L <= the
+  // block's threads); the node's list bounds are requested now
+  int L = 1;
+  while (2 * L * NB <= (int)blockDim.x) L *= 2;
+  const int t2 = threadIdx.x / L, r2 = threadIdx.x % L;
+  const bool act2 = t2 < nn && (int)threadIdx.x < L * NB;
+  const int lb = act2 ? lptr[n0 + t2] : 0, le = act2 ? lptr[n0 + t2 + 1] : 0;
   double* Pn = sm;                      // [ns][kPS]
   double* Gn = sm + kPS * ns;           // [ns][kGS]
   double* Fs = sm + (kPS + kGS) * ns;   // [e1 - e0][5]
@@ -539,31 +546,39 @@ __global__ void __launch_bounds__(256, MINB) k_fv_blocked(int N, int E, int NB, 
     }
     lq = lqn; nx = nxn; ny = nyn; nz = nzn; xs = xsn;
   }
-  __syncthreads();
-  // L = blockDim / NB lanes per node take entries r, r+L, ... of its list;
-  // the partial sums are combined in a fixed xor tree
-  const int L = blockDim.x / NB;
-  const int t = threadIdx.x / L, r = threadIdx.x % L;
-  const int n = n0 + t;
-  double acc[5] = {0, 0, 0, 0, 0};
-  if (t < nn) {
-    for (int k = lptr[n] + r; k < lptr[n + 1]; k += L) {
-      const int e = lidx[k];
-      const double* fs = Fs + 5 * (e & 0x7fffffff);
-      if (e < 0) {
+  // the first kLI entries of this lane's part of the node's list are
+  // requested before the barrier, the rest (long lists only) after it
+  constexpr int kLI = 8;
+  int li_pre[kLI];
 #pragma unroll
-        for (int c = 0; c < 5; ++c) acc[c] -= fs[c];
-      } else {
-#pragma unroll
-        for (int c = 0; c < 5; ++c) acc[c] += fs[c];
-      }
-    }
+  for (int m = 0; m < kLI; ++m) {
+    const int k = lb + r2 + m * L;
+    li_pre[m] = k < le ? lidx[k] : 0;
   }
+  __syncthreads();
+  // L lanes per node take entries r, r+L, ... of its list; the partial sums
+  // are combined in a fixed xor tree
+  const int n = n0 + t2;
+  double acc[5] = {0, 0, 0, 0, 0};
+  auto add = [&](int e) {
+    const double* fs = Fs + 5 * (e & 0x7fffffff);
+    if (e < 0) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) acc[c] -= fs[c];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) acc[c] += fs[c];
+    }
+  };
+#pragma unroll
+  for (int m = 0; m < kLI; ++m)
+    if (lb + r2 + m * L < le) add(li_pre[m]);
+  for (int k = lb + r2 + kLI * L; k < le; k += L) add(lidx[k]);
   for (int o = 1; o < L; o <<= 1) {
 #pragma unroll
     for (int c = 0; c < 5; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
   }
-  if (t < nn && r == 0) {
+  if (act2 && r2 == 0) {
 #pragma unroll
     for (int c = 0; c < 5; ++c) part[5 * (size_t)n + c] = acc[c];
   }
@@ -917,7 +932,10 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
   // register budget from the CTAs per SM that shared memory allows
   // (228 KB per SM, 1 KB reserved per CTA)
   const int by_smem = (int)std::min<size_t>(4, (228 * 1024) / (smem + 1024));
-  auto fvk = by_smem >= 4 ? k_fv_blocked<4> : by_smem == 3 ? k_fv_blocked<3> : k_fv_blocked<2>;
+  // 256 threads with the register budget of the CTAs that fit (384
+  // threads at two CTAs per SM measured slower)
+  const int fv_threads = 256;
+  auto fvk = by_smem >= 4 ? k_fv_blocked<256, 4> : by_smem == 3 ? k_fv_blocked<256, 3> : k_fv_blocked<256, 2>;
   AEROF_CUDA(cudaFuncSetAttribute(fvk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const size_t gsmem = ((size_t)8 * kPS * (m.NB + m.maxH) + (size_t)2 * m.maxL + 15) / 16 * 16;
   // gradient organisation (tuning knob AEROF_GRAD_KERNEL): 0 staged from
@@ -951,7 +969,7 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
     }
   }
   auto fv = [&](int fs, int* counter) {
-    fvk<<<m.nblk, 256, smem, s>>>(m.N, m.E, m.NB, g, rec, c->cfg.beta, fs, m.bl.p, m.bnorm.p, m.beptr.p,
+    fvk<<<m.nblk, fv_threads, smem, s>>>(m.N, m.E, m.NB, g, rec, c->cfg.beta, fs, m.bl.p, m.bnorm.p, m.beptr.p,
                                             m.hfptr.p, m.hfpad.p, m.maxHf, m.P2.p, c->s.G2.p, m.lptr.p, m.lidx.p,
                                             m.xslot.p, c->s.part.p, c->s.spill.p, c->s.tag.p, counter);
     AEROF_LAUNCH_CHECK();

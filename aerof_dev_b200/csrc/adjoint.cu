@@ -270,17 +270,69 @@ __global__ void k_a_edges(int E, Gas g, int rec, double beta, const int2* __rest
   o[23] = gdx0; o[24] = gdx1; o[25] = gdx2;
 }
 
-// Face flux cotangents by forward mode (5 state directions), g_V += J^T lam
+// Dual number with five tangents (the five state directions of a face
+// flux in one evaluation).  Division through one reciprocal of the divisor.
+struct Dual5 {
+  double v, d[5];
+  __device__ Dual5() : v(0.0), d{0.0, 0.0, 0.0, 0.0, 0.0} {}
+  __device__ Dual5(double a) : v(a), d{0.0, 0.0, 0.0, 0.0, 0.0} {}
+};
+__device__ __forceinline__ Dual5 operator+(const Dual5& a, const Dual5& b) {
+  Dual5 r(a.v + b.v);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) r.d[k] = a.d[k] + b.d[k];
+  return r;
+}
+__device__ __forceinline__ Dual5 operator-(const Dual5& a, const Dual5& b) {
+  Dual5 r(a.v - b.v);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) r.d[k] = a.d[k] - b.d[k];
+  return r;
+}
+__device__ __forceinline__ Dual5 operator-(const Dual5& a) {
+  Dual5 r(-a.v);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) r.d[k] = -a.d[k];
+  return r;
+}
+__device__ __forceinline__ Dual5 operator*(const Dual5& a, const Dual5& b) {
+  Dual5 r(a.v * b.v);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
+  return r;
+}
+__device__ __forceinline__ Dual5 operator/(const Dual5& a, const Dual5& b) {
+  const double ib = 1.0 / b.v;
+  Dual5 r(a.v * ib);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) * ib;
+  return r;
+}
+__device__ __forceinline__ Dual5 dsqrt(const Dual5& a) {
+  Dual5 r(sqrt(a.v));
+  const double h = 0.5 / r.v;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) r.d[k] = a.d[k] * h;
+  return r;
+}
+__device__ __forceinline__ double vof(const Dual5& a) { return a.v; }
+
+// Face flux cotangents, g_V += (d flux / d V)^T lam, the five state
+// directions in one forward-mode evaluation
 __device__ void face_vjp_V(const Gas& g, int code, double nx, double ny, double nz, const double* V, const double* Ub,
                            const double* lam, double* gV) {
-  for (int d = 0; d < 5; ++d) {
-    Dual Vd[5], f[5];
+  Dual5 Vd[5], f[5];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) Vd[k] = Dual(V[k], k == d ? 1.0 : 0.0);
-    face_flux(g, code, Dual(nx), Dual(ny), Dual(nz), Vd, Ub, f);
+  for (int k = 0; k < 5; ++k) {
+    Vd[k] = Dual5(V[k]);
+    Vd[k].d[k] = 1.0;
+  }
+  face_flux(g, code, Dual5(nx), Dual5(ny), Dual5(nz), Vd, Ub, f);
+#pragma unroll
+  for (int d = 0; d < 5; ++d) {
     double s = 0.0;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) s += f[k].d * lam[k];
+    for (int k = 0; k < 5; ++k) s += f[k].d[d] * lam[k];
     gV[d] += s;
   }
 }
@@ -377,6 +429,295 @@ __global__ void k_a_lsq_prim(int N, Gas g, int rec, const double* __restrict__ U
   for (int k = 0; k < 5; ++k) out[5 * (size_t)q + k] = gu[k];
 }
 
+// ---------------------------------------------------------------------
+// BLOCKED reverse sweep (Morton blocks of the residual's blocked
+// organisation).  lam2[n] = w[n2o[n]] / vol: the cotangent of the unscaled
+// flux sum, as 48-byte records.
+__global__ void k_a_lam2(int N, const int* __restrict__ n2o, const double* __restrict__ w,
+                         const double* __restrict__ vol2, double* __restrict__ lam2) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int o = n2o[n];
+  const double iv = 1.0 / vol2[n];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) lam2[6 * (size_t)n + k] = w[5 * (size_t)o + k] * iv;
+  lam2[6 * (size_t)n + 5] = 0.0;
+}
+
+// One CTA per block.  Phase 0: node records, gradients and lam of the
+// block's nodes and forward halo are staged in shared memory (cp.async).
+// Phase 1, thread per edge: the reconstruction is recomputed, the Roe flux
+// reversed (gF = lam_i - lam_j), and the cotangents (gL, gR) of the two
+// reconstructed states kept in shared memory; for a block-crossing edge the
+// second endpoint's part (g_Vj, g_ddji, dx) goes to spill; with GEO the
+// cotangents of the oriented edge normal and of dx go to geo in the
+// original edge numbering and orientation.  Phase 2, L lanes per node: the
+// node's edges in edge order, each reversed through the reconstruction for
+// the node's side: g_V += g_Vside, g_grad += dx (x) g_ddside; xor-tree lane
+// sum; written to gVp / gGp.
+template <bool GEO>
+__global__ void __launch_bounds__(256, 1) k_a_fv_blocked(int N, int E, int NB, Gas g, int rec, double beta,
+                                                         const ushort2* __restrict__ bl, const double* __restrict__ bn,
+                                                         const int* __restrict__ beptr, const int* __restrict__ hfptr,
+                                                         const int* __restrict__ hfpad, int maxHf,
+                                                         const double* __restrict__ P, const double* __restrict__ G,
+                                                         const double* __restrict__ lam2, const int* __restrict__ lptr,
+                                                         const int* __restrict__ lidx, const int* __restrict__ xslot,
+                                                         const int* __restrict__ bsrc, double* __restrict__ gVp,
+                                                         double* __restrict__ gGp, double* __restrict__ spill,
+                                                         double* __restrict__ geo) {
+  extern __shared__ double sm[];
+  const int blk = blockIdx.x;
+  const int n0 = blk * NB;
+  const int nn = min(NB, N - n0);
+  const int nh = hfptr[blk + 1] - hfptr[blk];
+  const int ns = nn + nh;
+  const int e0 = beptr[blk], e1 = beptr[blk + 1];
+  int L = 1;
+  while (2 * L * NB <= (int)blockDim.x) L *= 2;
+  const int t2 = threadIdx.x / L, r2 = threadIdx.x % L;
+  const bool act2 = t2 < nn && (int)threadIdx.x < L * NB;
+  const int lb = act2 ? lptr[n0 + t2] : 0, le = act2 ? lptr[n0 + t2 + 1] : 0;
+  double* Pn = sm;                           // [ns][kPS]
+  double* Gn = sm + kPS * ns;                // [ns][kGS]
+  double* Ln = sm + (kPS + kGS) * ns;        // [ns][6]
+  double* Es = sm + (kPS + kGS + 6) * ns;    // [e1 - e0][10]: gL, gR
+  const bool grad = rec != AEROF_REC_CONSTANT;
+  {
+    const int* hf = hfpad + (size_t)blk * maxHf;
+    double2* pd = reinterpret_cast<double2*>(Pn);
+    double2* gd = reinterpret_cast<double2*>(Gn);
+    double2* ld = reinterpret_cast<double2*>(Ln);
+    const double2* ps = reinterpret_cast<const double2*>(P + 8 * (size_t)n0);
+    const double2* gs = reinterpret_cast<const double2*>(G + 16 * (size_t)n0);
+    const double2* ls = reinterpret_cast<const double2*>(lam2 + 6 * (size_t)n0);
+    for (int k = threadIdx.x; k < 4 * nn; k += blockDim.x) cp_async16(pd + (kPS / 2) * (k >> 2) + (k & 3), ps + k);
+    for (int k = threadIdx.x; k < 3 * nn; k += blockDim.x) cp_async16(ld + k, ls + k);
+    if (grad)
+      for (int k = threadIdx.x; k < 8 * nn; k += blockDim.x) cp_async16(gd + (kGS / 2) * (k >> 3) + (k & 7), gs + k);
+    for (int k = threadIdx.x; k < 4 * nh; k += blockDim.x) {
+      const int j = hf[k >> 2];
+      cp_async16(pd + (kPS / 2) * (nn + (k >> 2)) + (k & 3), reinterpret_cast<const double2*>(P + 8 * (size_t)j) + (k & 3));
+    }
+    for (int k = threadIdx.x; k < 3 * nh; k += blockDim.x) {
+      const int j = hf[k / 3];
+      cp_async16(ld + 3 * nn + k, reinterpret_cast<const double2*>(lam2 + 6 * (size_t)j) + k % 3);
+    }
+    if (grad)
+      for (int k = threadIdx.x; k < 8 * nh; k += blockDim.x) {
+        const int j = hf[k >> 3];
+        cp_async16(gd + (kGS / 2) * (nn + (k >> 3)) + (k & 7), reinterpret_cast<const double2*>(G + 16 * (size_t)j) + (k & 7));
+      }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  for (int q = e0 + threadIdx.x; q < e1; q += blockDim.x) {
+    const ushort2 lq = bl[q];
+    const double n0_ = bn[q], n1_ = bn[(size_t)E + q], n2_ = bn[2 * (size_t)E + q];
+    const double* pi = Pn + kPS * lq.x;
+    const double* pj = Pn + kPS * lq.y;
+    const double* gi = Gn + kGS * lq.x;
+    const double* gj = Gn + kGS * lq.y;
+    const double dx0 = pj[5] - pi[5], dx1 = pj[6] - pi[6], dx2 = pj[7] - pi[7];
+    double Vi[5], Vj[5], ddij[5], ddji[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      if (!grad) {
+        ddij[k] = ddji[k] = 0.0;
+        Vi[k] = pi[k]; Vj[k] = pj[k];
+      } else {
+        ddij[k] = dx0 * gi[k] + dx1 * gi[5 + k] + dx2 * gi[10 + k];
+        ddji[k] = dx0 * gj[k] + dx1 * gj[5 + k] + dx2 * gj[10 + k];
+        if (rec == AEROF_REC_VANALBADA) vanalbada(beta, pi[k], ddij[k], pj[k], ddji[k], Vi[k], Vj[k]);
+        else linear_rec(beta, pi[k], ddij[k], pj[k], ddji[k], Vi[k], Vj[k]);
+      }
+    }
+    double gF[5], gL[5] = {0, 0, 0, 0, 0}, gR[5] = {0, 0, 0, 0, 0}, gn[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 5; ++k) gF[k] = Ln[6 * lq.x + k] - Ln[6 * lq.y + k];
+    if (sqrt(n0_ * n0_ + n1_ * n1_ + n2_ * n2_) >= 1e-18) roe_flux_adj(g, n0_, n1_, n2_, Vi, Vj, gF, gL, gR, gn);
+    double* es = Es + 10 * (q - e0);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) { es[k] = gL[k]; es[5 + k] = gR[k]; }
+    const int xs = xslot[q];
+    if (GEO || xs >= 0) {
+      double gdx0 = 0.0, gdx1 = 0.0, gdx2 = 0.0;
+      double* sp = xs >= 0 ? spill + 13 * (size_t)xs : nullptr;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        double gvi = 0.0, gvj = 0.0, gdi, gdj;
+        reconstruct_adj(rec, beta, pi[k], ddij[k], pj[k], ddji[k], gL[k], gR[k], gvi, gvj, gdi, gdj);
+        if (grad) {
+          gdx0 += gi[k] * gdi + gj[k] * gdj;
+          gdx1 += gi[5 + k] * gdi + gj[5 + k] * gdj;
+          gdx2 += gi[10 + k] * gdi + gj[10 + k] * gdj;
+        }
+        if (sp) { sp[k] = gvj; sp[5 + k] = gdj; }
+      }
+      if (sp) { sp[10] = dx0; sp[11] = dx1; sp[12] = dx2; }
+      if (GEO) {
+        const int src = bsrc[q];
+        const size_t l = (size_t)(src & 0x7fffffff);
+        const double sg = src < 0 ? -1.0 : 1.0;
+        geo[l] = sg * gn[0];
+        geo[(size_t)E + l] = sg * gn[1];
+        geo[2 * (size_t)E + l] = sg * gn[2];
+        geo[3 * (size_t)E + l] = sg * gdx0;
+        geo[4 * (size_t)E + l] = sg * gdx1;
+        geo[5 * (size_t)E + l] = sg * gdx2;
+      }
+    }
+  }
+  __syncthreads();
+  double av[5] = {0, 0, 0, 0, 0}, ag[15];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) ag[k] = 0.0;
+  for (int k = lb + r2; k < le; k += L) {
+    const int e = lidx[k];
+    const int slot = e & 0x7fffffff;
+    const bool second = e < 0;
+    const ushort2 lq = bl[e0 + slot];
+    const double* pi = Pn + kPS * lq.x;
+    const double* pj = Pn + kPS * lq.y;
+    const double* gi = Gn + kGS * lq.x;
+    const double* gj = Gn + kGS * lq.y;
+    const double dx0 = pj[5] - pi[5], dx1 = pj[6] - pi[6], dx2 = pj[7] - pi[7];
+    const double* es = Es + 10 * slot;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      double ddij = 0.0, ddji = 0.0;
+      if (grad) {
+        ddij = dx0 * gi[c] + dx1 * gi[5 + c] + dx2 * gi[10 + c];
+        ddji = dx0 * gj[c] + dx1 * gj[5 + c] + dx2 * gj[10 + c];
+      }
+      double gvi = 0.0, gvj = 0.0, gdi, gdj;
+      reconstruct_adj(rec, beta, pi[c], ddij, pj[c], ddji, es[c], es[5 + c], gvi, gvj, gdi, gdj);
+      const double gd = second ? gdj : gdi;
+      av[c] += second ? gvj : gvi;
+      ag[c] += dx0 * gd;
+      ag[5 + c] += dx1 * gd;
+      ag[10 + c] += dx2 * gd;
+    }
+  }
+  for (int o = 1; o < L; o <<= 1) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) av[c] += __shfl_xor_sync(0xffffffffu, av[c], o);
+#pragma unroll
+    for (int c = 0; c < 15; ++c) ag[c] += __shfl_xor_sync(0xffffffffu, ag[c], o);
+  }
+  if (act2 && r2 == 0) {
+    const size_t n = (size_t)(n0 + t2);
+#pragma unroll
+    for (int c = 0; c < 5; ++c) gVp[5 * n + c] = av[c];
+#pragma unroll
+    for (int c = 0; c < 15; ++c) gGp[16 * n + c] = ag[c];
+    gGp[16 * n + 15] = 0.0;
+  }
+}
+
+// Per node (blocked numbering): in-block sums + the spilled parts of the
+// incoming block-crossing edges (contiguous slots), written to the caller's
+// numbering.
+__global__ void k_a_fv_nodes(int N, const int* __restrict__ n2o, const double* __restrict__ gVp,
+                             const double* __restrict__ gGp, const int* __restrict__ xin_ptr,
+                             const double* __restrict__ spill, double* __restrict__ gV, double* __restrict__ gG) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double av[5], ag[15];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) av[c] = gVp[5 * (size_t)n + c];
+#pragma unroll
+  for (int c = 0; c < 15; ++c) ag[c] = gGp[16 * (size_t)n + c];
+  for (int k = xin_ptr[n]; k < xin_ptr[n + 1]; ++k) {
+    const double* sp = spill + 13 * (size_t)k;
+    const double dx0 = sp[10], dx1 = sp[11], dx2 = sp[12];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      av[c] += sp[c];
+      ag[c] += dx0 * sp[5 + c];
+      ag[5 + c] += dx1 * sp[5 + c];
+      ag[10 + c] += dx2 * sp[5 + c];
+    }
+  }
+  const size_t o = (size_t)n2o[n];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) gV[5 * o + c] = av[c];
+#pragma unroll
+  for (int c = 0; c < 15; ++c) gG[16 * o + c] = ag[c];
+  gG[16 * o + 15] = 0.0;
+}
+
+// Boundary faces of node i (face order), added to g_V[i]: the face flux
+// Jacobian transposed applied to lam_i = w_i / vol_i (forward mode in the
+// 5 state directions).
+__global__ void k_a_faces(int N, int F, Gas g, const double* __restrict__ Ub0, const int* __restrict__ nf_ptr,
+                          const int* __restrict__ nf_face, const int* __restrict__ fcode,
+                          const double* __restrict__ fn, const double* __restrict__ P, const double* __restrict__ w,
+                          const double* __restrict__ vol, double* __restrict__ gV) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N || nf_ptr[i] == nf_ptr[i + 1]) return;
+  double V[5], Ub[5], lm[5], gv[5];
+  const double iv = 1.0 / vol[i];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    V[k] = P[8 * (size_t)i + k];
+    Ub[k] = Ub0[k];
+    lm[k] = w[5 * (size_t)i + k] * iv;
+    gv[k] = gV[5 * (size_t)i + k];
+  }
+  const double third = 1.0 / 3.0;
+  for (int q = nf_ptr[i]; q < nf_ptr[i + 1]; ++q) {
+    const int f = nf_face[q];
+    face_vjp_V(g, fcode[f], third * fn[f], third * fn[(size_t)F + f], third * fn[2 * (size_t)F + f], V, Ub, lm, gv);
+  }
+#pragma unroll
+  for (int k = 0; k < 5; ++k) gV[5 * (size_t)i + k] = gv[k];
+}
+
+// Blocked reverse sweep over the edges and faces: a.gV, a.gG (caller
+// numbering) from the cotangent dw; with geo, also the cotangents of the
+// edge normals and dx.  Needs P (caller numbering) and P2/G2 current.
+static void reverse_sweep_blocked(aerof_gpu_ctx* c, const double* dw, bool geo) {
+  DeviceMesh& m = c->mesh;
+  AdjWork& a = c->adj;
+  cudaStream_t s = c->stream;
+  const Gas g = make_gas(c->cfg.gamma);
+  const int rec = c->cfg.reconstruction;
+  const int gn = grid_for(m.N, kAB);
+  a.lam2.ensure(6 * (size_t)m.N);
+  a.gVp.ensure(5 * (size_t)m.N);
+  a.gGp.ensure(16 * (size_t)m.N);
+  a.spill.ensure(13 * (size_t)std::max(m.nX, 1));
+  a.gV.ensure(5 * (size_t)m.N);
+  a.gG.ensure(16 * (size_t)m.N);
+  if (geo) a.geo.ensure(6 * (size_t)std::max(m.E, 1));
+  k_a_lam2<<<gn, kAB, 0, s>>>(m.N, m.n2o.p, dw, m.vol2.p, a.lam2.p);
+  AEROF_LAUNCH_CHECK();
+  const size_t smem = ((size_t)(kPS + kGS + 6) * (m.NB + m.maxHf) + (size_t)10 * m.maxE) * sizeof(double);
+  auto go = [&](auto kern) {
+    AEROF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<m.nblk, 256, smem, s>>>(m.N, m.E, m.NB, g, rec, c->cfg.beta, m.bl.p, m.bnorm.p, m.beptr.p, m.hfptr.p,
+                                   m.hfpad.p, m.maxHf, m.P2.p, c->s.G2.p, a.lam2.p, m.lptr.p, m.lidx.p, m.xslot.p,
+                                   m.bsrc.p, a.gVp.p, a.gGp.p, a.spill.p, geo ? a.geo.p : nullptr);
+    AEROF_LAUNCH_CHECK();
+  };
+  if (geo) go(k_a_fv_blocked<true>);
+  else go(k_a_fv_blocked<false>);
+  k_a_fv_nodes<<<gn, kAB, 0, s>>>(m.N, m.n2o.p, a.gVp.p, a.gGp.p, m.xin_ptr.p, a.spill.p, a.gV.p, a.gG.p);
+  AEROF_LAUNCH_CHECK();
+  if (m.F) {
+    k_a_faces<<<gn, kAB, 0, s>>>(m.N, m.F, g, m.Ubd.p, m.nf_ptr.p, m.nf_face.p, m.fcode.p, m.fnrm.p, m.P.p, dw,
+                                 m.vol.p, a.gV.p);
+    AEROF_LAUNCH_CHECK();
+  }
+}
+
+// whether the blocked reverse sweep's shared memory fits
+static bool reverse_blocked_fits(const DeviceMesh& m) {
+  return m.nblk > 0 &&
+         ((size_t)(kPS + kGS + 6) * (m.NB + m.maxHf) + (size_t)10 * m.maxE) * sizeof(double) <= 200 * 1024;
+}
+
 // J^T w for device state dU and cotangent dw, into dout ([N][5]).
 void vjp_dev(aerof_gpu_ctx* c, const double* dU, const double* dw, double* dout) {
   DeviceMesh& m = c->mesh;
@@ -386,19 +727,24 @@ void vjp_dev(aerof_gpu_ctx* c, const double* dU, const double* dw, double* dout)
   const int rec = c->cfg.reconstruction;
   const int gn = grid_for(m.N, kAB), ge = grid_for(m.E, kAB);
   prim_dev(c, dU);
-  c->s.G.ensure(16 * (size_t)m.N);
-  if (rec != AEROF_REC_CONSTANT) gradients_dev(c);
-  a.lam.ensure(5 * (size_t)m.N);
-  a.edge.ensure(32 * (size_t)m.E);
   a.gV.ensure(5 * (size_t)m.N);
   a.gG.ensure(16 * (size_t)m.N);
-  k_a_lam<<<gn, kAB, 0, s>>>(m.N, dw, m.vol.p, a.lam.p);
-  AEROF_LAUNCH_CHECK();
-  k_a_edges<<<ge, kAB, 0, s>>>(m.E, g, rec, c->cfg.beta, m.edges.p, m.en.p, m.P.p, c->s.G.p, a.lam.p, a.edge.p);
-  AEROF_LAUNCH_CHECK();
-  k_a_node<<<gn, kAB, 0, s>>>(m.N, m.F, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_node.p, m.nbr_edge.p, a.edge.p, m.nf_ptr.p,
-                              m.nf_face.p, m.fcode.p, m.fnrm.p, m.P.p, a.lam.p, a.gV.p, a.gG.p);
-  AEROF_LAUNCH_CHECK();
+  if (reverse_blocked_fits(m)) {
+    prim_grad_blocked_dev(c, dU, nullptr);
+    reverse_sweep_blocked(c, dw, false);
+  } else {
+    c->s.G.ensure(16 * (size_t)m.N);
+    if (rec != AEROF_REC_CONSTANT) gradients_dev(c);
+    a.lam.ensure(5 * (size_t)m.N);
+    a.edge.ensure(32 * (size_t)m.E);
+    k_a_lam<<<gn, kAB, 0, s>>>(m.N, dw, m.vol.p, a.lam.p);
+    AEROF_LAUNCH_CHECK();
+    k_a_edges<<<ge, kAB, 0, s>>>(m.E, g, rec, c->cfg.beta, m.edges.p, m.en.p, m.P.p, c->s.G.p, a.lam.p, a.edge.p);
+    AEROF_LAUNCH_CHECK();
+    k_a_node<<<gn, kAB, 0, s>>>(m.N, m.F, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_node.p, m.nbr_edge.p, a.edge.p, m.nf_ptr.p,
+                                m.nf_face.p, m.fcode.p, m.fnrm.p, m.P.p, a.lam.p, a.gV.p, a.gG.p);
+    AEROF_LAUNCH_CHECK();
+  }
   k_a_lsq_prim<<<gn, kAB, 0, s>>>(m.N, g, rec, dU, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, a.gV.p, a.gG.p, dout);
   AEROF_LAUNCH_CHECK();
 }
@@ -546,7 +892,7 @@ __global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const
                              const int* __restrict__ tet_edge, const int* __restrict__ faces,
                              const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_edge,
                              const int* __restrict__ nbr_tpos, const double* __restrict__ gd,
-                             const double* __restrict__ erec, const int* __restrict__ nt_ptr,
+                             const double* __restrict__ geo, int E, const int* __restrict__ nt_ptr,
                              const int* __restrict__ nt_tet, const int* __restrict__ nf_ptr,
                              const int* __restrict__ nf_face, const double* __restrict__ gvol,
                              const double* __restrict__ gfn, double* __restrict__ gX);
@@ -555,11 +901,30 @@ __global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const
 
 namespace aerof {
 
+// Dual number with three tangents: the x, y, z derivatives of the tet and
+// face geometry with respect to one vertex in a single evaluation.
+struct Dual3 {
+  double v, d[3];
+};
+__device__ __forceinline__ Dual3 operator+(const Dual3& a, const Dual3& b) {
+  return Dual3{a.v + b.v, {a.d[0] + b.d[0], a.d[1] + b.d[1], a.d[2] + b.d[2]}};
+}
+__device__ __forceinline__ Dual3 operator-(const Dual3& a, const Dual3& b) {
+  return Dual3{a.v - b.v, {a.d[0] - b.d[0], a.d[1] - b.d[1], a.d[2] - b.d[2]}};
+}
+__device__ __forceinline__ Dual3 operator-(const Dual3& a) { return Dual3{-a.v, {-a.d[0], -a.d[1], -a.d[2]}}; }
+__device__ __forceinline__ Dual3 operator*(const Dual3& a, const Dual3& b) {
+  return Dual3{a.v * b.v, {a.d[0] * b.v + a.v * b.d[0], a.d[1] * b.v + a.v * b.d[1], a.d[2] * b.v + a.v * b.d[2]}};
+}
+__device__ __forceinline__ Dual3 operator*(double c, const Dual3& a) {
+  return Dual3{c * a.v, {c * a.d[0], c * a.d[1], c * a.d[2]}};
+}
+
 __global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const int* __restrict__ tets,
                              const int* __restrict__ tet_edge, const int* __restrict__ faces,
                              const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_edge,
                              const int* __restrict__ nbr_tpos, const double* __restrict__ gd,
-                             const double* __restrict__ erec, const int* __restrict__ nt_ptr,
+                             const double* __restrict__ geo, int E, const int* __restrict__ nt_ptr,
                              const int* __restrict__ nt_tet, const int* __restrict__ nf_ptr,
                              const int* __restrict__ nf_face, const double* __restrict__ gvol,
                              const double* __restrict__ gfn, double* __restrict__ gX) {
@@ -568,60 +933,78 @@ __global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const
   double gx[3] = {0, 0, 0};
   for (int p = nbr_ptr[q]; p < nbr_ptr[q + 1]; ++p) {
     const int e = nbr_edge[p];
-    const double* o = erec + 32 * (size_t)(e & 0x7fffffff);
+    const size_t el = (size_t)(e & 0x7fffffff);
     const double s = e < 0 ? 1.0 : -1.0;  // dx = X_second - X_first
 #pragma unroll
-    for (int c = 0; c < 3; ++c) gx[c] += s * o[23 + c];
+    for (int c = 0; c < 3; ++c) gx[c] += s * geo[(3 + c) * (size_t)E + el];
     if (rec != AEROF_REC_CONSTANT) {
       const size_t tp = (size_t)nbr_tpos[p];
 #pragma unroll
       for (int c = 0; c < 3; ++c) gx[c] += gd[3 * tp + c] - gd[3 * (size_t)p + c];
     }
   }
-  // tets: control volumes and dual-cell normals
+  // tets: control volumes and dual-cell normals, the three derivatives
+  // with respect to this vertex in one pass
   for (int p = nt_ptr[q]; p < nt_ptr[q + 1]; ++p) {
     const int t = nt_tet[p] >> 2, a = nt_tet[p] & 3;
     const int* nd = tets + 4 * (size_t)t;
     const double gvt = 0.25 * (gvol[nd[0]] + gvol[nd[1]] + gvol[nd[2]] + gvol[nd[3]]);
-    int ed[6];
+    Dual3 xs[12];
 #pragma unroll
-    for (int l = 0; l < 6; ++l) ed[l] = tet_edge[6 * (size_t)t + l];
-    for (int c = 0; c < 3; ++c) {
-      Dual xs[12];
+    for (int v = 0; v < 4; ++v)
 #pragma unroll
-      for (int v = 0; v < 4; ++v)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) xs[3 * v + k] = Dual(X[3 * (size_t)nd[v] + k], (v == a && k == c) ? 1.0 : 0.0);
-      const int loc[4] = {0, 1, 2, 3};
-      double acc = tet_volume(xs, loc).d * gvt;
-      for (int l = 0; l < 6; ++l) {
-        // orientation by global node ids, as in the set-up
-        Vec3<Dual> n = tet_edge_normal_local(xs, nd, l);
-        const double* gn = erec + 32 * (size_t)ed[l] + 20;
-        acc += n.x.d * gn[0] + n.y.d * gn[1] + n.z.d * gn[2];
+      for (int k = 0; k < 3; ++k) {
+        Dual3 z{X[3 * (size_t)nd[v] + k], {0.0, 0.0, 0.0}};
+        if (v == a) z.d[k] = 1.0;
+        xs[3 * v + k] = z;
       }
-      gx[c] += acc;
+    const int loc[4] = {0, 1, 2, 3};
+    const Dual3 vol = tet_volume(xs, loc);
+    double acc[3] = {vol.d[0] * gvt, vol.d[1] * gvt, vol.d[2] * gvt};
+#pragma unroll
+    for (int l = 0; l < 6; ++l) {
+      // orientation by global node ids, as in the set-up
+      const Vec3<Dual3> n = tet_edge_normal_local(xs, nd, l);
+      const size_t el = (size_t)tet_edge[6 * (size_t)t + l];
+      const double g0 = geo[el], g1 = geo[(size_t)E + el], g2 = geo[2 * (size_t)E + el];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) acc[c] += n.x.d[c] * g0 + n.y.d[c] * g1 + n.z.d[c] * g2;
     }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gx[c] += acc[c];
   }
   // boundary faces: face normals
   for (int p = nf_ptr[q]; p < nf_ptr[q + 1]; ++p) {
     const int f = nf_face[p];
     const int* nd = faces + 3 * (size_t)f;
     const int a = nd[0] == q ? 0 : (nd[1] == q ? 1 : 2);
-    for (int c = 0; c < 3; ++c) {
-      Dual xs[9];
+    Dual3 xs[9];
 #pragma unroll
-      for (int v = 0; v < 3; ++v)
+    for (int v = 0; v < 3; ++v)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) xs[3 * v + k] = Dual(X[3 * (size_t)nd[v] + k], (v == a && k == c) ? 1.0 : 0.0);
-      const int loc[3] = {0, 1, 2};
-      Vec3<Dual> n = face_normal(xs, loc);
-      gx[c] += n.x.d * gfn[3 * (size_t)f] + n.y.d * gfn[3 * (size_t)f + 1] + n.z.d * gfn[3 * (size_t)f + 2];
-    }
+      for (int k = 0; k < 3; ++k) {
+        Dual3 z{X[3 * (size_t)nd[v] + k], {0.0, 0.0, 0.0}};
+        if (v == a) z.d[k] = 1.0;
+        xs[3 * v + k] = z;
+      }
+    const int loc[3] = {0, 1, 2};
+    const Vec3<Dual3> n = face_normal(xs, loc);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      gx[c] += n.x.d[c] * gfn[3 * (size_t)f] + n.y.d[c] * gfn[3 * (size_t)f + 1] + n.z.d[c] * gfn[3 * (size_t)f + 2];
   }
   gX[3 * (size_t)q] = gx[0];
   gX[3 * (size_t)q + 1] = gx[1];
   gX[3 * (size_t)q + 2] = gx[2];
+}
+
+// cotangents of the edge normals and dx out of the per-edge records of the
+// edge-parallel reverse sweep, in the layout of the blocked one
+__global__ void k_a_geo_from_rec(int E, const double* __restrict__ erec, double* __restrict__ geo) {
+  int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= E) return;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) geo[(size_t)k * E + l] = erec[32 * (size_t)l + 20 + k];
 }
 
 // (dR/dX)^T lambda for device state dU, cotangent dlam, into dgX [N][3];
@@ -637,32 +1020,37 @@ void dRdX_T_dev(aerof_gpu_ctx* c, const double* dU, const double* dlam, double* 
   c->s.k2.ensure(n5);
   double* R = c->s.k2.p;
   residual_dev(c, dU, R);
-  // the node records P and gradients G in the caller's numbering (the
-  // blocked residual keeps its own copies)
+  // node records P in the caller's numbering for the node and face passes
   prim_dev(c, dU);
-  c->s.G.ensure(16 * (size_t)m.N);
-  if (rec != AEROF_REC_CONSTANT) gradients_dev(c);
   a.lam.ensure(n5);
-  a.edge.ensure(32 * (size_t)m.E);
   a.gV.ensure(n5);
   a.gG.ensure(16 * (size_t)m.N);
   a.gd.ensure(3 * 2 * (size_t)m.E);
   a.gvol.ensure(m.N);
   a.gfn.ensure(3 * (size_t)std::max(m.F, 1));
+  a.geo.ensure(6 * (size_t)std::max(m.E, 1));
   k_a_lam<<<gn, kAB, 0, s>>>(m.N, dlam, m.vol.p, a.lam.p);
   AEROF_LAUNCH_CHECK();
   k_a_gvol<<<gn, kAB, 0, s>>>(m.N, dlam, R, m.vol.p, a.gvol.p);
   AEROF_LAUNCH_CHECK();
-  k_a_edges<<<ge, kAB, 0, s>>>(m.E, g, rec, c->cfg.beta, m.edges.p, m.en.p, m.P.p, c->s.G.p, a.lam.p, a.edge.p);
-  AEROF_LAUNCH_CHECK();
+  if (reverse_blocked_fits(m)) {
+    prim_grad_blocked_dev(c, dU, nullptr);
+    reverse_sweep_blocked(c, dlam, true);
+  } else {
+    c->s.G.ensure(16 * (size_t)m.N);
+    if (rec != AEROF_REC_CONSTANT) gradients_dev(c);
+    a.edge.ensure(32 * (size_t)m.E);
+    k_a_edges<<<ge, kAB, 0, s>>>(m.E, g, rec, c->cfg.beta, m.edges.p, m.en.p, m.P.p, c->s.G.p, a.lam.p, a.edge.p);
+    AEROF_LAUNCH_CHECK();
+    k_a_node<<<gn, kAB, 0, s>>>(m.N, m.F, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_node.p, m.nbr_edge.p, a.edge.p, m.nf_ptr.p,
+                                m.nf_face.p, m.fcode.p, m.fnrm.p, m.P.p, a.lam.p, a.gV.p, a.gG.p);
+    AEROF_LAUNCH_CHECK();
+    k_a_geo_from_rec<<<ge, kAB, 0, s>>>(m.E, a.edge.p, a.geo.p);
+    AEROF_LAUNCH_CHECK();
+  }
   if (m.F) {
     k_a_face_normal<<<grid_for(m.F, kAB), kAB, 0, s>>>(m.F, g, m.Ubd.p, m.faces.p, m.fcode.p, m.fnrm.p, m.P.p,
                                                          a.lam.p, a.gfn.p);
-    AEROF_LAUNCH_CHECK();
-  }
-  if (rec != AEROF_REC_CONSTANT || dJT) {
-    k_a_node<<<gn, kAB, 0, s>>>(m.N, m.F, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_node.p, m.nbr_edge.p, a.edge.p, m.nf_ptr.p,
-                                m.nf_face.p, m.fcode.p, m.fnrm.p, m.P.p, a.lam.p, a.gV.p, a.gG.p);
     AEROF_LAUNCH_CHECK();
   }
   if (rec != AEROF_REC_CONSTANT) {
@@ -675,8 +1063,8 @@ void dRdX_T_dev(aerof_gpu_ctx* c, const double* dU, const double* dlam, double* 
     AEROF_LAUNCH_CHECK();
   }
   k_a_gather_x<<<gn, kAB, 0, s>>>(m.N, rec, m.X.p, m.tets.p, m.tet_edge.p, m.faces.p, m.nbr_ptr.p, m.nbr_edge.p,
-                                  m.nbr_tpos.p, a.gd.p, a.edge.p, m.nt_ptr.p, m.nt_tet.p, m.nf_ptr.p, m.nf_face.p,
-                                  a.gvol.p, a.gfn.p, dgX);
+                                  m.nbr_tpos.p, a.gd.p, a.geo.p, m.E, m.nt_ptr.p, m.nt_tet.p, m.nf_ptr.p,
+                                  m.nf_face.p, a.gvol.p, a.gfn.p, dgX);
   AEROF_LAUNCH_CHECK();
 }
 

@@ -198,6 +198,11 @@ struct AdjWork {
   DBuf<double> gd;         // [2E][3] least-squares offset cotangents
   DBuf<double> gvol;       // [N] control-volume cotangents
   DBuf<double> gfn;        // [F][3] face-normal cotangents
+  // blocked reverse sweep
+  DBuf<double> lam2;       // [N][6] w / vol in the blocked numbering (16-byte records)
+  DBuf<double> gVp, gGp;   // [N][5], [N][16] in-block partial sums (blocked numbering)
+  DBuf<double> spill;      // [nX][13] second-endpoint parts of block-crossing edges
+  DBuf<double> geo;        // [6][E] cotangents of edge normals and dx (original edge order)
 };
 
 // CUDA-event timers per category (AEROF_T_*), recorded without host sync.
@@ -274,10 +279,33 @@ struct TimerScope {
   ~TimerScope() { timer_end(c, h); }
 };
 
+// ---- shared-memory staging helpers (residual and adjoint kernels)
+// Strides (in doubles) of the node records staged in shared memory: 80 B
+// for (V, X) and 144 B for the gradients, so that the 16-byte loads of 8
+// lanes reading 8 different records fall into disjoint banks.
+constexpr int kPS = 10;
+constexpr int kGS = 18;
+
+// 16-byte global -> shared copy that completes asynchronously (cp.async,
+// cached in L2 only); cp_async_wait_all() waits for this thread's copies.
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+// 8-byte variant (cached in L1 and L2)
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
 // implemented in residual.cu (used by implicit.cu and adjoint.cu).  With
 // sync == false the unphysical count is left on the device (counters[2]).
 int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync = true);
 void prim_dev(aerof_gpu_ctx* c, const double* dU);
+void prim_grad_blocked_dev(aerof_gpu_ctx* c, const double* dU, const int* tag);
 void gradients_dev(aerof_gpu_ctx* c);
 void timestep_dev(aerof_gpu_ctx* c, const double* dU, double cfl, double* ddt);
 double norm2_dev(aerof_gpu_ctx* c, const double* x, size_t n);

@@ -12,6 +12,7 @@
 // reference's accumulation order (SubDomain.C:3916-3995).
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -64,6 +65,26 @@ __device__ __forceinline__ void load_block<double>(const double* __restrict__ a,
   v[24] = a[b + 768 + l];
 }
 
+// the 25 values of lane l's block at base b written as 16-byte vectors
+// (elements 0..23) and one scalar (element 24): one coalesced line per
+// vector for the 32 rows of a warp
+template <class S>
+__device__ __forceinline__ void store_block_vec(S* __restrict__ a, size_t b, int l, const S* v);
+template <>
+__device__ __forceinline__ void store_block_vec<float>(float* __restrict__ a, size_t b, int l, const float* v) {
+  float4* q = reinterpret_cast<float4*>(a + b) + l;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) q[32 * i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+  a[b + 768 + l] = v[24];
+}
+template <>
+__device__ __forceinline__ void store_block_vec<double>(double* __restrict__ a, size_t b, int l, const double* v) {
+  double2* q = reinterpret_cast<double2*>(a + b) + l;
+#pragma unroll
+  for (int i = 0; i < 12; ++i) q[32 * i] = make_double2(v[2 * i], v[2 * i + 1]);
+  a[b + 768 + l] = v[24];
+}
+
 // v * scale rounded to S, written as block k of row r (TR: the transposed
 // block), and the same for a diagonal block
 template <class S, bool TR>
@@ -75,9 +96,10 @@ __device__ __forceinline__ void store_off(S* __restrict__ off, const int* __rest
 }
 template <class S, bool TR>
 __device__ __forceinline__ void store_diag(S* __restrict__ diag, int r, const double* v) {
-  const size_t b = sl_dblk(r);
+  S t[25];
 #pragma unroll
-  for (int e = 0; e < 25; ++e) diag[b + sl_el<S>(e, r & 31)] = (S)v[TR ? 5 * (e % 5) + e / 5 : e];
+  for (int e = 0; e < 25; ++e) t[e] = (S)v[TR ? 5 * (e % 5) + e / 5 : e];
+  store_block_vec<S>(diag, sl_dblk(r), r & 31, t);
 }
 
 // One thread per row r; a warp is one slice of the sliced layout, so for
@@ -96,8 +118,12 @@ __device__ __forceinline__ void store_diag(S* __restrict__ diag, int r, const do
 // of its two rows.  TR: the transpose H1^T is stored instead (block k of
 // row r = A_sr^T with A_sr = -sg dF/dU_r / vol_s, the Jacobian formed for
 // the diagonal), for products with the transpose that read coalesced.
+// block size of k_jac_rows: its shared scratch (two [25][threads] arrays)
+// stays under the 48 KB static limit
+template <class S> struct JacThreads { static constexpr int T = sizeof(S) == 4 ? 128 : 64; };
+
 template <class S, bool TR>
-__global__ void __launch_bounds__(128) k_jac_rows(int N, int E, int F, Gas g, const double* __restrict__ Ub0,
+__global__ void __launch_bounds__(JacThreads<S>::T) k_jac_rows(int N, int E, int F, Gas g, const double* __restrict__ Ub0,
                                                   const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_node,
                                                   const int* __restrict__ nbr_edge, const double* __restrict__ en,
                                                   const double* __restrict__ P, const double* __restrict__ vol,
@@ -108,12 +134,15 @@ __global__ void __launch_bounds__(128) k_jac_rows(int N, int E, int F, Gas g, co
   // the diagonal sum lives in shared memory (element k of this thread at
   // a[128 k], conflict-free), which keeps the register count low enough
   // for several CTAs per SM
-  __shared__ double sdiag[25 * 128];
+  constexpr int T = JacThreads<S>::T;
+  __shared__ double sdiag[25 * T];
+  __shared__ S soff[25 * T];  // the block being formed, written out as vectors
   double* a = sdiag + threadIdx.x;
+  S* so = soff + threadIdx.x;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= N) return;
 #pragma unroll
-  for (int k = 0; k < 25; ++k) a[128 * k] = 0.0;
+  for (int k = 0; k < 25; ++k) a[T * k] = 0.0;
   double Vr[5];
 #pragma unroll
   for (int k = 0; k < 5; ++k) Vr[k] = P[8 * (size_t)r + k];
@@ -131,9 +160,16 @@ __global__ void __launch_bounds__(128) k_jac_rows(int N, int E, int F, Gas g, co
     const double rnorm = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
     const size_t b = sl_blk(sptr, r, p - p0);
     const int lane = r & 31;
+    auto flush = [&]() {
+      S t[25];
+#pragma unroll
+      for (int k = 0; k < 25; ++k) t[k] = so[T * k];
+      store_block_vec<S>(off, b, lane, t);
+    };
     if (rnorm < 1e-18) {
 #pragma unroll
-      for (int k = 0; k < 25; ++k) off[b + sl_el<S>(k, lane)] = (S)0.0;
+      for (int k = 0; k < 25; ++k) so[T * k] = (S)0.0;
+      flush();
       continue;
     }
     const double invnorm = 1.0 / rnorm;
@@ -151,16 +187,17 @@ __global__ void __launch_bounds__(128) k_jac_rows(int N, int E, int F, Gas g, co
         const int el = 5 * m + j;
         // diagonal contribution: roejac(n, Vr, Vs, sg)
         const double jd = (H_elem(g, hr, un, el) + sg * d[m]) * half_rn;
-        a[128 * el] += sg * jd;
+        a[T * el] += sg * jd;
         if (TR) {
-          off[b + sl_el<S>(5 * j + m, lane)] = (S)(jd * sco);
+          so[T * (5 * j + m)] = (S)(jd * sco);
         } else {
           // off-diagonal block: roejac(n, Vs, Vr, -sg)
           const double jo = (H_elem(g, hs, un, el) + (-sg) * d[m]) * half_rn;
-          off[b + sl_el<S>(el, lane)] = (S)(jo * sco);
+          so[T * el] = (S)(jo * sco);
         }
       }
     }
+    flush();
   }
   const int q1 = nf_ptr[r + 1];
   if (nf_ptr[r] < q1) {
@@ -173,12 +210,12 @@ __global__ void __launch_bounds__(128) k_jac_rows(int N, int E, int F, Gas g, co
       double jac[25];
       face_jac(g, fcode[f], third * fn[f], third * fn[(size_t)F + f], third * fn[2 * (size_t)F + f], Vr, Ub, jac);
 #pragma unroll
-      for (int k = 0; k < 25; ++k) a[128 * k] += jac[k];
+      for (int k = 0; k < 25; ++k) a[T * k] += jac[k];
     }
   }
   double v[25];
 #pragma unroll
-  for (int k = 0; k < 25; ++k) v[k] = a[128 * k] * volr;
+  for (int k = 0; k < 25; ++k) v[k] = a[T * k] * volr;
   if (dt) {
     const double c = 1.0 / dt[r];
 #pragma unroll
@@ -255,15 +292,18 @@ __global__ void k_bj_invert(int N, const S* __restrict__ diag, S* __restrict__ d
   if (i >= N) return;
   const size_t b = sl_dblk(i);
   S a[25];
+  {
+    double t[25];
+    load_block<S>(diag, b, i & 31, t);
 #pragma unroll
-  for (int k = 0; k < 25; ++k) a[k] = diag[b + sl_el<S>(k, i & 31)];
+    for (int k = 0; k < 25; ++k) a[k] = (S)t[k];
+  }
   bool inv = true;
 #pragma unroll
   for (int k = 0; k < 5; ++k)
     if (a[6 * k] == S(0)) inv = false;
   if (inv && invert5<S>(a)) atomicAdd(bad, 1);
-#pragma unroll
-  for (int k = 0; k < 25; ++k) dinv[b + sl_el<S>(k, i & 31)] = a[k];
+  store_block_vec<S>(dinv, b, i & 31, a);
 }
 
 // z = D^-1 x (or D^-T x): JacobiPrec::apply/applyT (KspPrec.C:86-111)
@@ -423,9 +463,9 @@ void jacobian_dev(aerof_gpu_ctx* c, const double* dU, const double* ddt, int pre
   const Gas g = make_gas(c->cfg.gamma);
   TimerScope tj(c, AEROF_T_FV_JAC);
   prim_dev(c, dU);
-  const int gr = grid_for((size_t)m.N, 128);
   auto rows = [&](auto* off, auto* diag, auto kern) {
-    kern<<<gr, 128, 0, c->stream>>>(m.N, m.E, m.F, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_node.p, m.nbr_edge.p, m.en.p,
+    constexpr int T = JacThreads<std::remove_pointer_t<decltype(off)>>::T;
+    kern<<<grid_for((size_t)m.N, T), T, 0, c->stream>>>(m.N, m.E, m.F, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_node.p, m.nbr_edge.p, m.en.p,
                                     m.P.p, m.vol.p, m.nf_ptr.p, m.nf_face.p, m.fcode.p, m.fnrm.p, ddt, m.sptr.p, off,
                                     diag);
     AEROF_LAUNCH_CHECK();

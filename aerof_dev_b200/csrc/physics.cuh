@@ -759,21 +759,19 @@ __device__ __forceinline__ void roe_flux_adj(const Gas& g, double n0, double n1,
 // Partial derivatives of RecFcn::computeVanAlbadaFcn (RecFcn.h:268-281)
 // w.r.t. its two arguments, branch by branch.
 __device__ __forceinline__ void vanalbada_fcn_partials(double a, double b, double& da, double& db) {
+  // one reciprocal of the denominator D (rcp_), branch-free selection
   const double eps = 1.e-16;
   const double ab = a * b;
   const double D = a * a + b * b + 2.0 * eps;
-  if (ab > 0.0) {
-    const double Nn = a * (b * b + eps) + b * (a * a + eps);
-    da = ((b * b + eps) + 2.0 * a * b) / D - Nn * 2.0 * a / (D * D);
-    db = (2.0 * a * b + (a * a + eps)) / D - Nn * 2.0 * b / (D * D);
-  } else if (ab == 0.0) {
-    const double Nn = 0.5 * eps * (a + b);
-    da = 0.5 * eps / D - Nn * 2.0 * a / (D * D);
-    db = 0.5 * eps / D - Nn * 2.0 * b / (D * D);
-  } else {
-    da = 0.0;
-    db = 0.0;
-  }
+  const double iD = rcp_(D);
+  const double iD2 = iD * iD;
+  const bool pos = ab > 0.0;
+  const double Nn = pos ? a * (b * b + eps) + b * (a * a + eps) : 0.5 * eps * (a + b);
+  const double ta = pos ? (b * b + eps) + 2.0 * a * b : 0.5 * eps;
+  const double tb = pos ? 2.0 * a * b + (a * a + eps) : 0.5 * eps;
+  const bool live = ab >= 0.0;
+  da = live ? ta * iD - Nn * 2.0 * a * iD2 : 0.0;
+  db = live ? tb * iD - Nn * 2.0 * b * iD2 : 0.0;
 }
 
 // Reverse of the per-component reconstruction (vanalbada / linear /

@@ -111,19 +111,6 @@ __global__ void __launch_bounds__(256) k_grad(int N, const double* __restrict__ 
   gi[2 * r + 1] = make_double2(o[2], o[3]);
 }
 
-// Strides (in doubles) of the node records staged in shared memory: 80 B
-// for (V, X) and 144 B for the gradients, so that the 16-byte loads of 8
-// lanes reading 8 different records fall into disjoint banks.
-constexpr int kPS = 10;
-constexpr int kGS = 18;
-
-// 16-byte global -> shared copy that completes asynchronously (cp.async,
-// cached in L2 only); cp_async_wait_all() waits for this thread's copies.
-__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // BLOCKED organisation: least-squares gradients of one Morton block of NB
 // nodes per CTA.  The CTA stages the node records (V, X) of its own nodes
@@ -249,13 +236,6 @@ __global__ void __launch_bounds__(256, 3) k_grad_staged(int N, int NB, Gas g, co
   for (int q = 0; q < S / 2; ++q) gi[q] = make_double2(o[2 * q], o[2 * q + 1]);
 }
 
-// 8-byte variant of cp_async16 (cached in L1 and L2)
-__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 // Shared-memory stage of the pipelined gradient kernel (offsets in doubles,
 // all even so that every part is 16-byte aligned).
@@ -535,8 +515,30 @@ __global__ void __launch_bounds__(THREADS, MINB) k_fv_blocked(int N, int E, int 
     double f[5];
     // global node ids are needed only to tag unphysical states
     const int gi = n0 + li, gj = lj < nn ? n0 + lj : hs[lj - nn];
-    edge_flux_rec(g, rec, beta, failsafe, gi, gj, nx, ny, nz, Pn + kPS * li, Gn + kGS * li, Pn + kPS * lj,
-                  Gn + kGS * lj, tag, counters, f);
+    // the two records as 16-byte shared loads (the record strides keep
+    // every row 16-byte aligned)
+    double pr[2][8], gr[2][16];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const int sl = side ? lj : li;
+      const double2* pp = reinterpret_cast<const double2*>(Pn + kPS * sl);
+      const double2* gp = reinterpret_cast<const double2*>(Gn + kGS * sl);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const double2 v = pp[k];
+        pr[side][2 * k] = v.x;
+        pr[side][2 * k + 1] = v.y;
+      }
+      if (rec != AEROF_REC_CONSTANT) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const double2 v = gp[k];
+          gr[side][2 * k] = v.x;
+          gr[side][2 * k + 1] = v.y;
+        }
+      }
+    }
+    edge_flux_rec(g, rec, beta, failsafe, gi, gj, nx, ny, nz, pr[0], gr[0], pr[1], gr[1], tag, counters, f);
     double* fs = Fs + 5 * (q - e0);
 #pragma unroll
     for (int k = 0; k < 5; ++k) fs[k] = f[k];
@@ -584,16 +586,19 @@ __global__ void __launch_bounds__(THREADS, MINB) k_fv_blocked(int N, int E, int 
   }
 }
 
-// BLOCKED organisation, per node (new numbering): block-local sum, minus the
+// BLOCKED organisation, per node: block-local sum (new numbering), minus the
 // spilled fluxes of incoming block-crossing edges, plus the boundary faces
 // of the node (face order), times 1/ctrlVol; written to R in the caller's
 // numbering.
-__global__ void k_fv_nodes(int N, const int* __restrict__ n2o, const double* __restrict__ part,
+__global__ void k_fv_nodes(int N, const int* __restrict__ o2n, const double* __restrict__ part,
                            const int* __restrict__ xin_ptr, const double* __restrict__ spill, const int* __restrict__ nf_ptr,
                            const int* __restrict__ nf_face, const int* __restrict__ faces,
-                           const double* __restrict__ fbuf, const double* __restrict__ vol2, double* __restrict__ R) {
-  int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
+                           const double* __restrict__ fbuf, const double* __restrict__ vol, double* __restrict__ R) {
+  // one thread per row of R in the caller's numbering (coalesced writes);
+  // the blocked partial sums and spills are read through o2n
+  int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= N) return;
+  const int n = o2n[o];
   double acc[5];
 #pragma unroll
   for (int c = 0; c < 5; ++c) acc[c] = part[5 * (size_t)n + c];
@@ -602,7 +607,6 @@ __global__ void k_fv_nodes(int N, const int* __restrict__ n2o, const double* __r
 #pragma unroll
     for (int c = 0; c < 5; ++c) acc[c] -= sp[c];
   }
-  const int o = n2o[n];
   for (int q = nf_ptr[o]; q < nf_ptr[o + 1]; ++q) {
     const int f = nf_face[q];
     const int* fd = faces + 3 * (size_t)f;
@@ -611,7 +615,7 @@ __global__ void k_fv_nodes(int N, const int* __restrict__ n2o, const double* __r
 #pragma unroll
     for (int c = 0; c < 5; ++c) acc[c] += ff[c];
   }
-  const double invcv = 1.0 / vol2[n];
+  const double invcv = 1.0 / vol[o];
 #pragma unroll
   for (int c = 0; c < 5; ++c) R[5 * (size_t)o + c] = acc[c] * invcv;
 }
@@ -911,6 +915,38 @@ static void launch_grad_staged(const DeviceMesh& m, const Gas& g, const double* 
   }
 }
 
+// P2 = prim(U) in the blocked numbering and, unless the reconstruction is
+// constant, the gradients G2 (zero at tagged nodes when tag is given).
+void prim_grad_blocked_dev(aerof_gpu_ctx* c, const double* dU, const int* tag) {
+  DeviceMesh& m = c->mesh;
+  const Gas g = make_gas(c->cfg.gamma);
+  cudaStream_t s = c->stream;
+  c->s.G2.ensure(16 * (size_t)m.N);
+  if (c->cfg.reconstruction == AEROF_REC_CONSTANT) {
+    k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
+    AEROF_LAUNCH_CHECK();
+    return;
+  }
+  const size_t gsmem = ((size_t)8 * kPS * (m.NB + m.maxH) + (size_t)2 * m.maxL + 15) / 16 * 16;
+  // gradient organisation (tuning knob AEROF_GRAD_KERNEL): 0 staged from
+  // P2, 1 staged with the primitive conversion fused, 2 node-parallel,
+  // 3 (default) staged, persistent and software pipelined
+  const int gk = grad_kernel_choice();
+  const bool staged = gsmem <= kMaxStagedSmem && gk != 2;
+  const bool piped = gk == 3 && m.maxH <= 512 && 2 * grad_stage(m).size * sizeof(double) <= kMaxStagedSmem;
+  if (piped) {
+    launch_grad_pipe(c, g, dU, tag, c->s.G2.p, s);
+  } else if (staged) {
+    launch_grad_staged(m, g, dU, tag, c->s.G2.p, gsmem, gk == 1, s);
+  } else {
+    k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
+    AEROF_LAUNCH_CHECK();
+    k_grad<<<grid_for(4 * (size_t)m.N, kBlock), kBlock, 0, s>>>(m.N, m.P2.p, m.W2.p, m.nb2_ptr.p, m.nb2_node.p, tag,
+                                                                c->s.G2.p);
+    AEROF_LAUNCH_CHECK();
+  }
+}
+
 // BLOCKED organisation of residual_dev (see k_fv_blocked).
 static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
   DeviceMesh& m = c->mesh;
@@ -937,36 +973,9 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
   const int fv_threads = 256;
   auto fvk = by_smem >= 4 ? k_fv_blocked<256, 4> : by_smem == 3 ? k_fv_blocked<256, 3> : k_fv_blocked<256, 2>;
   AEROF_CUDA(cudaFuncSetAttribute(fvk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const size_t gsmem = ((size_t)8 * kPS * (m.NB + m.maxH) + (size_t)2 * m.maxL + 15) / 16 * 16;
-  // gradient organisation (tuning knob AEROF_GRAD_KERNEL): 0 staged from
-  // P2, 1 staged with the primitive conversion fused, 2 node-parallel,
-  // 3 (default) staged, persistent and software pipelined
-  const int gk = grad_kernel_choice();
-  const bool staged = gsmem <= kMaxStagedSmem && gk != 2;
-  const bool piped = gk == 3 && m.maxH <= 512 && 2 * grad_stage(m).size * sizeof(double) <= kMaxStagedSmem;
-  // prim + gradients: staged per block when the block's halo fits, else
-  // the node-parallel kernels on the blocked arrays
-  auto grad = [&](const int* tg) {
-    if (piped) {
-      launch_grad_pipe(c, g, dU, tg, c->s.G2.p, s);
-    } else if (staged) {
-      launch_grad_staged(m, g, dU, tg, c->s.G2.p, gsmem, gk == 1, s);
-    } else {
-      k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
-      AEROF_LAUNCH_CHECK();
-      k_grad<<<grid_for(4 * (size_t)m.N, kBlock), kBlock, 0, s>>>(m.N, m.P2.p, m.W2.p, m.nb2_ptr.p, m.nb2_node.p, tg,
-                                                                  c->s.G2.p);
-      AEROF_LAUNCH_CHECK();
-    }
-  };
   {
     TimerScope t(c, AEROF_T_NODAL_GRAD);
-    if (rec != AEROF_REC_CONSTANT) {
-      grad(nullptr);
-    } else {
-      k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
-      AEROF_LAUNCH_CHECK();
-    }
+    prim_grad_blocked_dev(c, dU, nullptr);
   }
   auto fv = [&](int fs, int* counter) {
     fvk<<<m.nblk, fv_threads, smem, s>>>(m.N, m.E, m.NB, g, rec, c->cfg.beta, fs, m.bl.p, m.bnorm.p, m.beptr.p,
@@ -985,7 +994,7 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
   }
   if (bad && c->cfg.failsafe && rec != AEROF_REC_CONSTANT) {
     TimerScope t(c, AEROF_T_FV_TERM);
-    grad(c->s.tag.p);
+    prim_grad_blocked_dev(c, dU, c->s.tag.p);
     fv(0, cnt + 1);
   }
   {
@@ -995,8 +1004,8 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
                                                            m.o2n.p, c->s.fbuf.p);
       AEROF_LAUNCH_CHECK();
     }
-    k_fv_nodes<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.n2o.p, c->s.part.p, m.xin_ptr.p, c->s.spill.p,
-                                                        m.nf_ptr.p, m.nf_face.p, m.faces.p, c->s.fbuf.p, m.vol2.p, dR);
+    k_fv_nodes<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.o2n.p, c->s.part.p, m.xin_ptr.p, c->s.spill.p,
+                                                        m.nf_ptr.p, m.nf_face.p, m.faces.p, c->s.fbuf.p, m.vol.p, dR);
     AEROF_LAUNCH_CHECK();
   }
   return bad;

@@ -388,21 +388,23 @@ __global__ void k_a_node(int N, int F, Gas g, const double* __restrict__ Ub0, co
 // Per node q: transpose of the least-squares gradient,
 // g_V_q += sum_{i in nbr(q)} W_i(x_q - x_i) . g_grad_i - sum_{p} W_q(x_p - x_q) . g_grad_q,
 // then (dV/dU)^T.
-__global__ void k_a_lsq_prim(int N, Gas g, int rec, const double* __restrict__ U, const double* __restrict__ P,
-                             const double* __restrict__ lsqW, const int* __restrict__ nbr_ptr,
-                             const int* __restrict__ nbr_node, const double* __restrict__ gV,
-                             const double* __restrict__ gG, double* __restrict__ out) {
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= N) return;
-  double gv[5];
-#pragma unroll
-  for (int k = 0; k < 5; ++k) gv[k] = gV[5 * (size_t)q + k];
-  if (rec != AEROF_REC_CONSTANT) {
+__global__ void __launch_bounds__(256) k_a_lsq_prim(int N, Gas g, int rec, const double* __restrict__ U,
+                                                    const double* __restrict__ P, const double* __restrict__ lsqW,
+                                                    const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_node,
+                                                    const double* __restrict__ gV, const double* __restrict__ gG,
+                                                    double* __restrict__ out) {
+  // four lanes per node share its neighbours (r, r+4, ...); fixed xor tree
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int q = t >> 2, r = t & 3;
+  const bool act = q < N;
+  double gv[5] = {0, 0, 0, 0, 0};
+  double Wsum0 = 0.0, Wsum1 = 0.0, Wsum2 = 0.0;
+  if (act && rec != AEROF_REC_CONSTANT) {
     const double* pq = P + 8 * (size_t)q;
-    double wq[6], Wsum0 = 0.0, Wsum1 = 0.0, Wsum2 = 0.0;
+    double wq[6];
 #pragma unroll
     for (int k = 0; k < 6; ++k) wq[k] = lsqW[(size_t)k * N + q];
-    for (int p = nbr_ptr[q]; p < nbr_ptr[q + 1]; ++p) {
+    for (int p = nbr_ptr[q] + r; p < nbr_ptr[q + 1]; p += 4) {
       const int i = nbr_node[p];
       const double* pi = P + 8 * (size_t)i;
       double wi[6];
@@ -417,6 +419,19 @@ __global__ void k_a_lsq_prim(int N, Gas g, int rec, const double* __restrict__ U
       lsq_weights(wq, pi[5] - pq[5], pi[6] - pq[6], pi[7] - pq[7], V0, V1, V2);
       Wsum0 += V0; Wsum1 += V1; Wsum2 += V2;
     }
+  }
+#pragma unroll
+  for (int o = 1; o < 4; o <<= 1) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) gv[k] += __shfl_xor_sync(0xffffffffu, gv[k], o);
+    Wsum0 += __shfl_xor_sync(0xffffffffu, Wsum0, o);
+    Wsum1 += __shfl_xor_sync(0xffffffffu, Wsum1, o);
+    Wsum2 += __shfl_xor_sync(0xffffffffu, Wsum2, o);
+  }
+  if (!act || r != 0) return;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) gv[k] += gV[5 * (size_t)q + k];
+  if (rec != AEROF_REC_CONSTANT) {
     const double* gq = gG + 16 * (size_t)q;
 #pragma unroll
     for (int k = 0; k < 5; ++k) gv[k] -= Wsum0 * gq[k] + Wsum1 * gq[5 + k] + Wsum2 * gq[10 + k];
@@ -745,7 +760,8 @@ void vjp_dev(aerof_gpu_ctx* c, const double* dU, const double* dw, double* dout)
                                 m.nf_face.p, m.fcode.p, m.fnrm.p, m.P.p, a.lam.p, a.gV.p, a.gG.p);
     AEROF_LAUNCH_CHECK();
   }
-  k_a_lsq_prim<<<gn, kAB, 0, s>>>(m.N, g, rec, dU, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, a.gV.p, a.gG.p, dout);
+  k_a_lsq_prim<<<grid_for(4 * (size_t)m.N, kAB), kAB, 0, s>>>(m.N, g, rec, dU, m.P.p, m.lsqW.p, m.nbr_ptr.p,
+                                                              m.nbr_node.p, a.gV.p, a.gG.p, dout);
   AEROF_LAUNCH_CHECK();
 }
 
@@ -792,11 +808,15 @@ __global__ void k_a_face_normal(int F, Gas g, const double* __restrict__ Ub0, co
 // d = x_p - x_i through W(w_i, d), through w_i = f(R_i) and through the
 // Cholesky factor R_i of sum d d^T (SubDomainCore.C:1334-1381, 1755-1777;
 // SubDomain.C:137-159).  gd[p] (3 doubles per neighbour entry).
-__global__ void k_a_lsq_x(int N, const double* __restrict__ P, const double* __restrict__ lsqR,
-                          const double* __restrict__ lsqW, const int* __restrict__ nbr_ptr,
-                          const int* __restrict__ nbr_node, const double* __restrict__ gG, double* __restrict__ gd) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+__global__ void __launch_bounds__(256) k_a_lsq_x(int N, const double* __restrict__ P, const double* __restrict__ lsqR,
+                                                 const double* __restrict__ lsqW, const int* __restrict__ nbr_ptr,
+                                                 const int* __restrict__ nbr_node, const double* __restrict__ gG,
+                                                 double* __restrict__ gd) {
+  // four lanes per node share its neighbours (lane, lane+4, ...) in both passes;
+  // the cotangent of the node's constants is summed in a fixed xor tree
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = min(t >> 2, N - 1), lane = t & 3;
+  const bool act = (t >> 2) < N;
   const double* pi = P + 8 * (size_t)i;
   const double* gg = gG + 16 * (size_t)i;
   double w[6], r[6];
@@ -804,7 +824,7 @@ __global__ void k_a_lsq_x(int N, const double* __restrict__ P, const double* __r
   for (int k = 0; k < 6; ++k) { w[k] = lsqW[(size_t)k * N + i]; r[k] = lsqR[(size_t)k * N + i]; }
   double gw[6] = {0, 0, 0, 0, 0, 0};
   // pass 1: through W(w, d)
-  for (int p = nbr_ptr[i]; p < nbr_ptr[i + 1]; ++p) {
+  for (int p = nbr_ptr[i] + lane; act && p < nbr_ptr[i + 1]; p += 4) {
     const double* pj = P + 8 * (size_t)nbr_node[p];
     const double d0 = pj[5] - pi[5], d1 = pj[6] - pi[6], d2 = pj[7] - pi[7];
     double gW0 = 0.0, gW1 = 0.0, gW2 = 0.0;
@@ -833,6 +853,11 @@ __global__ void k_a_lsq_x(int N, const double* __restrict__ P, const double* __r
     gd2 += ge3; gw[4] += -d1 * ge3; gd1 += -w[4] * ge3; gw[5] += d0 * ge3; gd0 += w[5] * ge3;
     gd[3 * (size_t)p] = gd0; gd[3 * (size_t)p + 1] = gd1; gd[3 * (size_t)p + 2] = gd2;
   }
+#pragma unroll
+  for (int o = 1; o < 4; o <<= 1)
+#pragma unroll
+    for (int k = 0; k < 6; ++k) gw[k] += __shfl_xor_sync(0xffffffffu, gw[k], o);
+  if (!act) return;
   // w = f(R): w0=1/r11 w1=1/r22 w2=1/r33 w3=r12 w0 w4=r23 w1 w5=(r12 r23 - r13 r22) w0 w1
   const double r11 = r[0], r12 = r[1], r13 = r[2], r22 = r[3], r23 = r[4], r33 = r[5];
   const double psi0 = r12 * r23 - r13 * r22;
@@ -863,7 +888,7 @@ __global__ void k_a_lsq_x(int N, const double* __restrict__ P, const double* __r
   gr[0] += -r12 / r11 * gr[1];
   gS[0] = 0.5 / r11 * gr[0];
   // pass 2: S = sum d d^T
-  for (int p = nbr_ptr[i]; p < nbr_ptr[i + 1]; ++p) {
+  for (int p = nbr_ptr[i] + lane; p < nbr_ptr[i + 1]; p += 4) {
     const double* pj = P + 8 * (size_t)nbr_node[p];
     const double d0 = pj[5] - pi[5], d1 = pj[6] - pi[6], d2 = pj[7] - pi[7];
     gd[3 * (size_t)p] += 2.0 * d0 * gS[0] + d1 * gS[1] + d2 * gS[2];
@@ -901,25 +926,6 @@ __global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const
 
 namespace aerof {
 
-// Dual number with three tangents: the x, y, z derivatives of the tet and
-// face geometry with respect to one vertex in a single evaluation.
-struct Dual3 {
-  double v, d[3];
-};
-__device__ __forceinline__ Dual3 operator+(const Dual3& a, const Dual3& b) {
-  return Dual3{a.v + b.v, {a.d[0] + b.d[0], a.d[1] + b.d[1], a.d[2] + b.d[2]}};
-}
-__device__ __forceinline__ Dual3 operator-(const Dual3& a, const Dual3& b) {
-  return Dual3{a.v - b.v, {a.d[0] - b.d[0], a.d[1] - b.d[1], a.d[2] - b.d[2]}};
-}
-__device__ __forceinline__ Dual3 operator-(const Dual3& a) { return Dual3{-a.v, {-a.d[0], -a.d[1], -a.d[2]}}; }
-__device__ __forceinline__ Dual3 operator*(const Dual3& a, const Dual3& b) {
-  return Dual3{a.v * b.v, {a.d[0] * b.v + a.v * b.d[0], a.d[1] * b.v + a.v * b.d[1], a.d[2] * b.v + a.v * b.d[2]}};
-}
-__device__ __forceinline__ Dual3 operator*(double c, const Dual3& a) {
-  return Dual3{c * a.v, {c * a.d[0], c * a.d[1], c * a.d[2]}};
-}
-
 __global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const int* __restrict__ tets,
                              const int* __restrict__ tet_edge, const int* __restrict__ faces,
                              const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_edge,
@@ -943,55 +949,65 @@ __global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const
       for (int c = 0; c < 3; ++c) gx[c] += gd[3 * tp + c] - gd[3 * (size_t)p + c];
     }
   }
-  // tets: control volumes and dual-cell normals, the three derivatives
-  // with respect to this vertex in one pass
+  // tets: control volumes and dual-cell normals, reverse mode in closed
+  // form for this vertex a.  Volume V = (e3 . (e1 x e2)) / 6, e_i = x_i - x_0;
+  // edge normal n = 1.5 s (xg1 x xg0) with xg = face centroid - tet centroid
+  // (ElemTetCore.C:281-330), so g_xg1 = xg0 x g_c, g_xg0 = g_c x xg1 with
+  // g_c = 1.5 s g_n, then a third to each vertex of the face and a quarter
+  // to every vertex (with minus) for the centroid.
   for (int p = nt_ptr[q]; p < nt_ptr[q + 1]; ++p) {
     const int t = nt_tet[p] >> 2, a = nt_tet[p] & 3;
     const int* nd = tets + 4 * (size_t)t;
     const double gvt = 0.25 * (gvol[nd[0]] + gvol[nd[1]] + gvol[nd[2]] + gvol[nd[3]]);
-    Dual3 xs[12];
+    Vec3<double> x[4];
 #pragma unroll
-    for (int v = 0; v < 4; ++v)
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        Dual3 z{X[3 * (size_t)nd[v] + k], {0.0, 0.0, 0.0}};
-        if (v == a) z.d[k] = 1.0;
-        xs[3 * v + k] = z;
-      }
-    const int loc[4] = {0, 1, 2, 3};
-    const Dual3 vol = tet_volume(xs, loc);
-    double acc[3] = {vol.d[0] * gvt, vol.d[1] * gvt, vol.d[2] * gvt};
+    for (int v = 0; v < 4; ++v) x[v] = node_x(X, nd[v]);
+    const Vec3<double> e1 = x[1] - x[0], e2 = x[2] - x[0], e3 = x[3] - x[0];
+    Vec3<double> dV;
+    if (a == 1) dV = cross(e2, e3);
+    else if (a == 2) dV = cross(e3, e1);
+    else if (a == 3) dV = cross(e1, e2);
+    else dV = v3(0.0, 0.0, 0.0) - (cross(e2, e3) + cross(e3, e1) + cross(e1, e2));
+    const double sixth = 1.0 / 6.0;
+    double acc[3] = {sixth * dV.x * gvt, sixth * dV.y * gvt, sixth * dV.z * gvt};
+    const double third = 1.0 / 3.0;
+    Vec3<double> f[4];
+    f[0] = scale(third, x[0] + x[1] + x[2]);
+    f[1] = scale(third, x[0] + x[1] + x[3]);
+    f[2] = scale(third, x[0] + x[2] + x[3]);
+    f[3] = scale(third, x[1] + x[2] + x[3]);
+    const Vec3<double> gc0 = scale(0.25, x[0] + x[1] + x[2] + x[3]);
 #pragma unroll
     for (int l = 0; l < 6; ++l) {
-      // orientation by global node ids, as in the set-up
-      const Vec3<Dual3> n = tet_edge_normal_local(xs, nd, l);
+      const int F0 = tet_edge_face(l, 0), F1 = tet_edge_face(l, 1);
+      const Vec3<double> xg0 = f[F0] - gc0, xg1 = f[F1] - gc0;
       const size_t el = (size_t)tet_edge[6 * (size_t)t + l];
-      const double g0 = geo[el], g1 = geo[(size_t)E + el], g2 = geo[2 * (size_t)E + el];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) acc[c] += n.x.d[c] * g0 + n.y.d[c] * g1 + n.z.d[c] * g2;
+      const double sl = nd[tet_edge_end(l, 0)] < nd[tet_edge_end(l, 1)] ? 1.5 : -1.5;
+      const Vec3<double> gcv = v3(sl * geo[el], sl * geo[(size_t)E + el], sl * geo[2 * (size_t)E + el]);
+      const Vec3<double> g1 = cross(xg0, gcv), g0 = cross(gcv, xg1);
+      // face k holds every vertex but 3 - k
+      const double w0 = (a != 3 - F0 ? third : 0.0) - 0.25, w1 = (a != 3 - F1 ? third : 0.0) - 0.25;
+      acc[0] += w0 * g0.x + w1 * g1.x;
+      acc[1] += w0 * g0.y + w1 * g1.y;
+      acc[2] += w0 * g0.z + w1 * g1.z;
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) gx[c] += acc[c];
   }
-  // boundary faces: face normals
+  // boundary faces: n = (3 x02 x x01 + 3 x02 x x01) / 12 (FaceTriaCore.C:
+  // 65-82) = x02 x x01 / 2, so g_x02 = x01 x g_n / 2, g_x01 = g_n x x02 / 2
   for (int p = nf_ptr[q]; p < nf_ptr[q + 1]; ++p) {
     const int f = nf_face[p];
     const int* nd = faces + 3 * (size_t)f;
     const int a = nd[0] == q ? 0 : (nd[1] == q ? 1 : 2);
-    Dual3 xs[9];
-#pragma unroll
-    for (int v = 0; v < 3; ++v)
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        Dual3 z{X[3 * (size_t)nd[v] + k], {0.0, 0.0, 0.0}};
-        if (v == a) z.d[k] = 1.0;
-        xs[3 * v + k] = z;
-      }
-    const int loc[3] = {0, 1, 2};
-    const Vec3<Dual3> n = face_normal(xs, loc);
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-      gx[c] += n.x.d[c] * gfn[3 * (size_t)f] + n.y.d[c] * gfn[3 * (size_t)f + 1] + n.z.d[c] * gfn[3 * (size_t)f + 2];
+    const Vec3<double> x0 = node_x(X, nd[0]);
+    const Vec3<double> x01 = node_x(X, nd[1]) - x0, x02 = node_x(X, nd[2]) - x0;
+    const Vec3<double> gn = v3(gfn[3 * (size_t)f], gfn[3 * (size_t)f + 1], gfn[3 * (size_t)f + 2]);
+    const Vec3<double> g02 = scale(0.5, cross(x01, gn)), g01 = scale(0.5, cross(gn, x02));
+    const Vec3<double> d = a == 2 ? g02 : (a == 1 ? g01 : v3(0.0, 0.0, 0.0) - (g02 + g01));
+    gx[0] += d.x;
+    gx[1] += d.y;
+    gx[2] += d.z;
   }
   gX[3 * (size_t)q] = gx[0];
   gX[3 * (size_t)q + 1] = gx[1];
@@ -1054,11 +1070,11 @@ void dRdX_T_dev(aerof_gpu_ctx* c, const double* dU, const double* dlam, double* 
     AEROF_LAUNCH_CHECK();
   }
   if (rec != AEROF_REC_CONSTANT) {
-    k_a_lsq_x<<<gn, kAB, 0, s>>>(m.N, m.P.p, m.lsqR.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, a.gG.p, a.gd.p);
+    k_a_lsq_x<<<grid_for(4 * (size_t)m.N, kAB), kAB, 0, s>>>(m.N, m.P.p, m.lsqR.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, a.gG.p, a.gd.p);
     AEROF_LAUNCH_CHECK();
   }
   if (dJT) {
-    k_a_lsq_prim<<<gn, kAB, 0, s>>>(m.N, g, rec, dU, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, a.gV.p, a.gG.p,
+    k_a_lsq_prim<<<grid_for(4 * (size_t)m.N, kAB), kAB, 0, s>>>(m.N, g, rec, dU, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, a.gV.p, a.gG.p,
                                     dJT);
     AEROF_LAUNCH_CHECK();
   }

@@ -125,6 +125,8 @@ struct DeviceMesh {
   // (s * 25 + e) * 32 + l).  scol: column of block (s, k, l); rows with
   // fewer than ks[s] blocks are padded with their own index.
   int nsl = 0;
+  int nbrow = 0;           // rows with boundary faces
+  DBuf<int> brow, blist;   // [N] index among the boundary rows (-1: none); [nbrow] those rows
   DBuf<int> sptr;          // [nsl+1] block columns before slice s
   DBuf<int> scol;          // [sptr[nsl] * 32]
   std::vector<int> h_sptr, h_nbr_ptr;
@@ -179,6 +181,7 @@ struct Implicit {
   DBuf<double> w, r, x, b, t;
   DBuf<double> hcol;       // device scratch for one Hessenberg column
   DBuf<unsigned> ticket;   // grid-reduction ticket of the fused Gram-Schmidt kernels
+  DBuf<double> fsum;       // [nbrow][25] boundary-face blocks of the boundary rows
   // flexible GMRES on the exact linearisation (outer FP64 vectors)
   DBuf<double> fV, fZ, fw, fr, fh;
 };

@@ -118,22 +118,53 @@ __device__ __forceinline__ void store_diag(S* __restrict__ diag, int r, const do
 // of its two rows.  TR: the transpose H1^T is stored instead (block k of
 // row r = A_sr^T with A_sr = -sg dF/dU_r / vol_s, the Jacobian formed for
 // the diagonal), for products with the transpose that read coalesced.
+// Boundary-face blocks of the boundary rows (Face.C:814-847: FD flux
+// Jacobians for far field, the analytic wall block, in face order), summed
+// per row into fsum; k_jac_rows adds them to the diagonal.  Kept apart so
+// that the FD arithmetic does not set the register budget of the edge pass.
+__global__ void k_jac_faces(int nbrow, int F, Gas g, const double* __restrict__ Ub0, const int* __restrict__ blist,
+                            const int* __restrict__ nf_ptr, const int* __restrict__ nf_face,
+                            const int* __restrict__ fcode, const double* __restrict__ fn,
+                            const double* __restrict__ P, double* __restrict__ fsum) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nbrow) return;
+  const int r = blist[t];
+  double V[5], Ub[5], a[25];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) { V[k] = P[8 * (size_t)r + k]; Ub[k] = Ub0[k]; }
+#pragma unroll
+  for (int k = 0; k < 25; ++k) a[k] = 0.0;
+  const double third = 1.0 / 3.0;
+  for (int q = nf_ptr[r]; q < nf_ptr[r + 1]; ++q) {
+    const int f = nf_face[q];
+    double jac[25];
+    face_jac(g, fcode[f], third * fn[f], third * fn[(size_t)F + f], third * fn[2 * (size_t)F + f], V, Ub, jac);
+#pragma unroll
+    for (int k = 0; k < 25; ++k) a[k] += jac[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 25; ++k) fsum[25 * (size_t)t + k] = a[k];
+}
+
 // block size of k_jac_rows: its shared scratch (two [25][threads] arrays)
 // stays under the 48 KB static limit
-template <class S> struct JacThreads { static constexpr int T = sizeof(S) == 4 ? 128 : 64; };
+// and, for FP32, the register budget of 4 CTAs per SM
+template <class S> struct JacThreads {
+  static constexpr int T = sizeof(S) == 4 ? 128 : 64;
+  static constexpr int B = sizeof(S) == 4 ? 4 : 1;
+};
 
 template <class S, bool TR>
-__global__ void __launch_bounds__(JacThreads<S>::T) k_jac_rows(int N, int E, int F, Gas g, const double* __restrict__ Ub0,
+__global__ void __launch_bounds__(JacThreads<S>::T, JacThreads<S>::B) k_jac_rows(int N, int E, int F, Gas g, const double* __restrict__ Ub0,
                                                   const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_node,
                                                   const int* __restrict__ nbr_edge, const double* __restrict__ en,
                                                   const double* __restrict__ P, const double* __restrict__ vol,
-                                                  const int* __restrict__ nf_ptr, const int* __restrict__ nf_face,
-                                                  const int* __restrict__ fcode, const double* __restrict__ fn,
+                                                  const int* __restrict__ brow, const double* __restrict__ fsum,
                                                   const double* __restrict__ dt, const int* __restrict__ sptr,
                                                   S* __restrict__ off, S* __restrict__ diag) {
   // the diagonal sum lives in shared memory (element k of this thread at
-  // a[128 k], conflict-free), which keeps the register count low enough
-  // for several CTAs per SM
+  // a[T k], conflict-free), which keeps the register count low enough for
+  // several CTAs per SM
   constexpr int T = JacThreads<S>::T;
   __shared__ double sdiag[25 * T];
   __shared__ S soff[25 * T];  // the block being formed, written out as vectors
@@ -172,46 +203,44 @@ __global__ void __launch_bounds__(JacThreads<S>::T) k_jac_rows(int N, int E, int
       flush();
       continue;
     }
+    // the Jacobians are formed in the storage precision S (FP32 for the
+    // mixed-precision solver) and summed into the diagonal in FP64
     const double invnorm = 1.0 / rnorm;
-    const double un[3] = {n0 * invnorm, n1 * invnorm, n2 * invnorm};
-    const double half_rn = 0.5 * rnorm;
-    const double sco = TR ? -sg * (1.0 / vol[s]) : sg * volr;
-    const RoeAvg A = roe_avg(g, un, Vr, Vs);
-    const HState hr = h_state(g, un, Vr), hs = h_state(g, un, Vs);
+    const S un[3] = {(S)(n0 * invnorm), (S)(n1 * invnorm), (S)(n2 * invnorm)};
+    const S half_rn = (S)(0.5 * rnorm);
+    const S sco = (S)(TR ? -sg * (1.0 / vol[s]) : sg * volr);
+    const S sgS = (S)sg;
+    S VrS[5], VsS[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) { VrS[k] = (S)Vr[k]; VsS[k] = (S)Vs[k]; }
+    const auto A = roe_avg<S>(g, un, VrS, VsS);
+    const auto hr = h_state<S>(g, un, VrS);
+    const auto hs = h_state<S>(g, un, VsS);
 #pragma unroll
     for (int j = 0; j < 5; ++j) {
-      double d[5];
-      D_col(g, A, un, j, d);
+      S d[5];
+      D_col<S>(g, A, un, j, d);
 #pragma unroll
       for (int m = 0; m < 5; ++m) {
         const int el = 5 * m + j;
         // diagonal contribution: roejac(n, Vr, Vs, sg)
-        const double jd = (H_elem(g, hr, un, el) + sg * d[m]) * half_rn;
-        a[T * el] += sg * jd;
+        const S jd = (H_elem<S>(g, hr, un, el) + sgS * d[m]) * half_rn;
+        a[T * el] += sg * (double)jd;
         if (TR) {
-          so[T * (5 * j + m)] = (S)(jd * sco);
+          so[T * (5 * j + m)] = jd * sco;
         } else {
           // off-diagonal block: roejac(n, Vs, Vr, -sg)
-          const double jo = (H_elem(g, hs, un, el) + (-sg) * d[m]) * half_rn;
-          so[T * el] = (S)(jo * sco);
+          const S jo = (H_elem<S>(g, hs, un, el) + (-sgS) * d[m]) * half_rn;
+          so[T * el] = jo * sco;
         }
       }
     }
     flush();
   }
-  const int q1 = nf_ptr[r + 1];
-  if (nf_ptr[r] < q1) {
-    double Ub[5];
+  const int br = brow[r];
+  if (br >= 0) {
 #pragma unroll
-    for (int k = 0; k < 5; ++k) Ub[k] = Ub0[k];
-    const double third = 1.0 / 3.0;
-    for (int q = nf_ptr[r]; q < q1; ++q) {
-      const int f = nf_face[q];
-      double jac[25];
-      face_jac(g, fcode[f], third * fn[f], third * fn[(size_t)F + f], third * fn[2 * (size_t)F + f], Vr, Ub, jac);
-#pragma unroll
-      for (int k = 0; k < 25; ++k) a[T * k] += jac[k];
-    }
+    for (int k = 0; k < 25; ++k) a[T * k] += fsum[25 * (size_t)br + k];
   }
   double v[25];
 #pragma unroll
@@ -463,11 +492,18 @@ void jacobian_dev(aerof_gpu_ctx* c, const double* dU, const double* ddt, int pre
   const Gas g = make_gas(c->cfg.gamma);
   TimerScope tj(c, AEROF_T_FV_JAC);
   prim_dev(c, dU);
+  J.fsum.ensure(25 * (size_t)std::max(m.nbrow, 1));
+  if (m.nbrow) {
+    k_jac_faces<<<grid_for((size_t)m.nbrow, 128), 128, 0, c->stream>>>(m.nbrow, m.F, g, m.Ubd.p, m.blist.p, m.nf_ptr.p,
+                                                                      m.nf_face.p, m.fcode.p, m.fnrm.p, m.P.p,
+                                                                      J.fsum.p);
+    AEROF_LAUNCH_CHECK();
+  }
   auto rows = [&](auto* off, auto* diag, auto kern) {
     constexpr int T = JacThreads<std::remove_pointer_t<decltype(off)>>::T;
-    kern<<<grid_for((size_t)m.N, T), T, 0, c->stream>>>(m.N, m.E, m.F, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_node.p, m.nbr_edge.p, m.en.p,
-                                    m.P.p, m.vol.p, m.nf_ptr.p, m.nf_face.p, m.fcode.p, m.fnrm.p, ddt, m.sptr.p, off,
-                                    diag);
+    kern<<<grid_for((size_t)m.N, T), T, 0, c->stream>>>(m.N, m.E, m.F, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_node.p,
+                                                        m.nbr_edge.p, m.en.p, m.P.p, m.vol.p, m.brow.p, J.fsum.p, ddt,
+                                                        m.sptr.p, off, diag);
     AEROF_LAUNCH_CHECK();
   };
   if (precision == AEROF_PREC_FP32) {

@@ -519,6 +519,17 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
       m.xin_ptr.upload(hb.xin_ptr.data(), N + 1, s);
       AEROF_CUDA(cudaStreamSynchronize(s));  // host vectors die at scope end
     }
+    // rows with boundary faces (their face blocks are formed apart)
+    {
+      std::vector<int> br(N, -1), bls;
+      for (int r = 0; r < N; ++r)
+        if (h.nf_ptr[r] < h.nf_ptr[r + 1]) { br[r] = (int)bls.size(); bls.push_back(r); }
+      m.nbrow = (int)bls.size();
+      m.brow.upload(br.data(), (size_t)N, s);
+      if (bls.empty()) m.blist.alloc(1);
+      else m.blist.upload(bls.data(), bls.size(), s);
+      AEROF_CUDA(cudaStreamSynchronize(s));
+    }
     // sliced layout of the implicit operator
     {
       const int nsl = (N + 31) / 32;

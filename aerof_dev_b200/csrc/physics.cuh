@@ -341,42 +341,66 @@ AEROF_HD void roe_jac_H(const Gas& g, const double* n, const double* Ug, double*
 // RoeAvg holds the scalars of the average; tmw_elem and D_col form the
 // eigenvector matrix and D one column at a time, so a caller can stream
 // the 5x5 blocks without holding 25-element arrays.
+template <class T = double>
 struct RoeAvg {
-  double uar2, uar3, uar4, enth, VdotN, qir, crsq, gc, usc2, rRT, sRT, tRT, vp1, vp4, vp5;
+  T uar2, uar3, uar4, enth, VdotN, qir, crsq, gc, usc2, rRT, sRT, tRT, vp1, vp4, vp5;
 };
-AEROF_HD RoeAvg roe_avg(const Gas& g, const double* n, const double* Ug, const double* Ud) {
-  const double gam1 = g.gam1;
-  RoeAvg A;
-  double squsr1 = sqrt(Ug[0]), squsr2 = sqrt(Ud[0]);
-  double ener1 = Ug[4] / gam1 + 0.5 * Ug[0] * (Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3]);
-  double ener2 = Ud[4] / gam1 + 0.5 * Ud[0] * (Ud[1] * Ud[1] + Ud[2] * Ud[2] + Ud[3] * Ud[3]);
-  double usro = 1.0 / (squsr1 + squsr2);
-  A.uar2 = (squsr1 * Ug[1] + squsr2 * Ud[1]) * usro;
-  A.uar3 = (squsr1 * Ug[2] + squsr2 * Ud[2]) * usro;
-  A.uar4 = (squsr1 * Ug[3] + squsr2 * Ud[3]) * usro;
-  double uar5 = ((ener1 + Ug[4]) / squsr1 + (ener2 + Ud[4]) / squsr2) * usro;
+// a*b + c*d with both products rounded (no fused multiply-add), so the
+// result does not depend on which pair is named first
+AEROF_HD double sym_dot2(double a, double b, double c, double d) {
+#ifdef __CUDA_ARCH__
+  return __dmul_rn(a, b) + __dmul_rn(c, d);
+#else
+  return a * b + c * d;
+#endif
+}
+AEROF_HD float sym_dot2(float a, float b, float c, float d) {
+#ifdef __CUDA_ARCH__
+  return __fmul_rn(a, b) + __fmul_rn(c, d);
+#else
+  return a * b + c * d;
+#endif
+}
+
+// T = double: the reference arithmetic; T = float: the same formulas in
+// FP32, for the FP32-stored Jacobian of the mixed-precision solver.  The
+// Roe average is formed symmetrically in (Ug, Ud) (sym_dot2), so the two
+// rows of an edge obtain the same dissipation matrix bit for bit.
+template <class T = double>
+AEROF_HD RoeAvg<T> roe_avg(const Gas& g, const T* n, const T* Ug, const T* Ud) {
+  const T gam1 = (T)g.gam1;
+  RoeAvg<T> A;
+  T squsr1 = sqrt(Ug[0]), squsr2 = sqrt(Ud[0]);
+  T ener1 = Ug[4] / gam1 + T(0.5) * Ug[0] * (Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3]);
+  T ener2 = Ud[4] / gam1 + T(0.5) * Ud[0] * (Ud[1] * Ud[1] + Ud[2] * Ud[2] + Ud[3] * Ud[3]);
+  T usro = T(1.0) / (squsr1 + squsr2);
+  A.uar2 = sym_dot2(squsr1, Ug[1], squsr2, Ud[1]) * usro;
+  A.uar3 = sym_dot2(squsr1, Ug[2], squsr2, Ud[2]) * usro;
+  A.uar4 = sym_dot2(squsr1, Ug[3], squsr2, Ud[3]) * usro;
+  T uar5 = ((ener1 + Ug[4]) / squsr1 + (ener2 + Ud[4]) / squsr2) * usro;
   A.enth = uar5;
   A.VdotN = n[0] * A.uar2 + n[1] * A.uar3 + n[2] * A.uar4;
-  A.qir = 0.5 * (A.uar2 * A.uar2 + A.uar3 * A.uar3 + A.uar4 * A.uar4);
-  double cr = sqrt(gam1 * (uar5 - A.qir));
+  A.qir = T(0.5) * (A.uar2 * A.uar2 + A.uar3 * A.uar3 + A.uar4 * A.uar4);
+  T cr = sqrt(gam1 * (uar5 - A.qir));
   A.crsq = cr * cr;
   A.gc = gam1 / A.crsq;
-  A.usc2 = 0.5 / A.crsq;
+  A.usc2 = T(0.5) / A.crsq;
   // beta = 1: vp4,vp5 = VdotN +- cr written as the reference's general form
-  double sq = sqrt(0.0 * A.VdotN * (0.0 * A.VdotN) + 4.0 * A.crsq);
-  double vp4 = 0.5 * (2.0 * A.VdotN + sq);
-  double vp5 = 0.5 * (2.0 * A.VdotN - sq);
+  T sq = sqrt(T(0.0) * A.VdotN * (T(0.0) * A.VdotN) + T(4.0) * A.crsq);
+  T vp4 = T(0.5) * (T(2.0) * A.VdotN + sq);
+  T vp5 = T(0.5) * (T(2.0) * A.VdotN - sq);
   A.rRT = vp4 - A.VdotN;
   A.sRT = vp5 - A.VdotN;
-  A.tRT = 0.5 * (vp5 - vp4);
+  A.tRT = T(0.5) * (vp5 - vp4);
   A.vp1 = fabs(A.VdotN);
   A.vp4 = fabs(vp4);
   A.vp5 = fabs(vp5);
   return A;
 }
 // element e (row-major) of the left eigenvector matrix tmw
-AEROF_HD double tmw_elem(const Gas& g, const RoeAvg& A, const double* n, int e) {
-  const double gam1 = g.gam1;
+template <class T = double>
+AEROF_HD T tmw_elem(const Gas& g, const RoeAvg<T>& A, const T* n, int e) {
+  const T gam1 = (T)g.gam1;
   switch (e) {
     case 0: return n[0] + n[1] * A.uar4 - A.uar3 * n[2] - A.gc * n[0] * A.qir;
     case 1: return A.gc * n[0] * A.uar2;
@@ -406,11 +430,12 @@ AEROF_HD double tmw_elem(const Gas& g, const RoeAvg& A, const double* n, int e) 
   }
 }
 // column j of D: d[m] = D[5 m + j]
-AEROF_HD void D_col(const Gas& g, const RoeAvg& A, const double* n, int j, double* d) {
-  const double t0 = tmw_elem(g, A, n, j), t1 = tmw_elem(g, A, n, 5 + j), t2 = tmw_elem(g, A, n, 10 + j);
-  const double t3 = tmw_elem(g, A, n, 15 + j), t4 = tmw_elem(g, A, n, 20 + j);
-  const double uar2 = A.uar2, uar3 = A.uar3, uar4 = A.uar4, qir = A.qir, usc2 = A.usc2, rRT = A.rRT, sRT = A.sRT;
-  const double vp1 = A.vp1, vp4 = A.vp4, vp5 = A.vp5, enth = A.enth, VdotN = A.VdotN;
+template <class T = double>
+AEROF_HD void D_col(const Gas& g, const RoeAvg<T>& A, const T* n, int j, T* d) {
+  const T t0 = tmw_elem(g, A, n, j), t1 = tmw_elem(g, A, n, 5 + j), t2 = tmw_elem(g, A, n, 10 + j);
+  const T t3 = tmw_elem(g, A, n, 15 + j), t4 = tmw_elem(g, A, n, 20 + j);
+  const T uar2 = A.uar2, uar3 = A.uar3, uar4 = A.uar4, qir = A.qir, usc2 = A.usc2, rRT = A.rRT, sRT = A.sRT;
+  const T vp1 = A.vp1, vp4 = A.vp4, vp5 = A.vp5, enth = A.enth, VdotN = A.VdotN;
   d[0] = vp1 * (n[0] * t0 + n[1] * t1 + n[2] * t2) + vp4 * usc2 * t3 + vp5 * usc2 * t4;
   d[1] = vp1 * (n[0] * uar2 * t0 + (n[1] * uar2 - n[2]) * t1 + (n[2] * uar2 + n[1]) * t2) +
          vp4 * (usc2 * (uar2 + rRT * n[0])) * t3 + vp5 * (usc2 * (uar2 + sRT * n[0])) * t4;
@@ -423,7 +448,7 @@ AEROF_HD void D_col(const Gas& g, const RoeAvg& A, const double* n, int j, doubl
          vp4 * (usc2 * (enth + VdotN * rRT)) * t3 + vp5 * (usc2 * (enth + VdotN * sRT)) * t4;
 }
 AEROF_HD void roe_jac_D(const Gas& g, const double* n, const double* Ug, const double* Ud, double* D) {
-  const RoeAvg A = roe_avg(g, n, Ug, Ud);
+  const RoeAvg<double> A = roe_avg(g, n, Ug, Ud);
 #pragma unroll
   for (int j = 0; j < 5; ++j) {
     double d[5];
@@ -435,45 +460,48 @@ AEROF_HD void roe_jac_D(const Gas& g, const double* n, const double* Ug, const d
 
 // Scalars of the convective Jacobian H(U) (see roe_jac_H) and its element
 // e (row-major), for streaming use.
+template <class T = double>
 struct HState {
-  double U1, U2, U3, VdotN, qir, enth;
+  T U1, U2, U3, VdotN, qir, enth;
 };
-AEROF_HD HState h_state(const Gas& g, const double* n, const double* Ug) {
-  HState h;
+template <class T = double>
+AEROF_HD HState<T> h_state(const Gas& g, const T* n, const T* Ug) {
+  HState<T> h;
   h.U1 = Ug[1]; h.U2 = Ug[2]; h.U3 = Ug[3];
   h.VdotN = Ug[1] * n[0] + Ug[2] * n[1] + Ug[3] * n[2];
-  h.qir = 0.5 * (Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3]);
-  h.enth = (g.gam * Ug[4] + g.gam1 * Ug[0] * h.qir) / (g.gam1 * Ug[0]);
+  h.qir = T(0.5) * (Ug[1] * Ug[1] + Ug[2] * Ug[2] + Ug[3] * Ug[3]);
+  h.enth = ((T)g.gam * Ug[4] + (T)g.gam1 * Ug[0] * h.qir) / ((T)g.gam1 * Ug[0]);
   return h;
 }
-AEROF_HD double H_elem(const Gas& g, const HState& h, const double* n, int e) {
-  const double gam1 = g.gam1;
+template <class T = double>
+AEROF_HD T H_elem(const Gas& g, const HState<T>& h, const T* n, int e) {
+  const T gam1 = (T)g.gam1;
   switch (e) {
-    case 0: return 0.0;
+    case 0: return T(0.0);
     case 1: return n[0];
     case 2: return n[1];
     case 3: return n[2];
-    case 4: return 0.0;
+    case 4: return T(0.0);
     case 5: return gam1 * n[0] * h.qir - h.U1 * h.VdotN;
-    case 6: return (1.0 - gam1) * n[0] * h.U1 + h.VdotN;
+    case 6: return (T(1.0) - gam1) * n[0] * h.U1 + h.VdotN;
     case 7: return -gam1 * n[0] * h.U2 + h.U1 * n[1];
     case 8: return -gam1 * n[0] * h.U3 + h.U1 * n[2];
     case 9: return gam1 * n[0];
     case 10: return gam1 * n[1] * h.qir - h.U2 * h.VdotN;
     case 11: return -gam1 * n[1] * h.U1 + h.U2 * n[0];
-    case 12: return (1.0 - gam1) * n[1] * h.U2 + h.VdotN;
+    case 12: return (T(1.0) - gam1) * n[1] * h.U2 + h.VdotN;
     case 13: return -gam1 * n[1] * h.U3 + h.U2 * n[2];
     case 14: return gam1 * n[1];
     case 15: return gam1 * n[2] * h.qir - h.U3 * h.VdotN;
     case 16: return -gam1 * n[2] * h.U1 + h.U3 * n[0];
     case 17: return -gam1 * n[2] * h.U2 + h.U3 * n[1];
-    case 18: return (1.0 - gam1) * n[2] * h.U3 + h.VdotN;
+    case 18: return (T(1.0) - gam1) * n[2] * h.U3 + h.VdotN;
     case 19: return gam1 * n[2];
     case 20: return (gam1 * h.qir - h.enth) * h.VdotN;
     case 21: return h.enth * n[0] - gam1 * h.U1 * h.VdotN;
     case 22: return h.enth * n[1] - gam1 * h.U2 * h.VdotN;
     case 23: return h.enth * n[2] - gam1 * h.U3 * h.VdotN;
-    default: return (1.0 + gam1) * h.VdotN;
+    default: return (T(1.0) + gam1) * h.VdotN;
   }
 }
 

@@ -515,30 +515,8 @@ __global__ void __launch_bounds__(THREADS, MINB) k_fv_blocked(int N, int E, int 
     double f[5];
     // global node ids are needed only to tag unphysical states
     const int gi = n0 + li, gj = lj < nn ? n0 + lj : hs[lj - nn];
-    // the two records as 16-byte shared loads (the record strides keep
-    // every row 16-byte aligned)
-    double pr[2][8], gr[2][16];
-#pragma unroll
-    for (int side = 0; side < 2; ++side) {
-      const int sl = side ? lj : li;
-      const double2* pp = reinterpret_cast<const double2*>(Pn + kPS * sl);
-      const double2* gp = reinterpret_cast<const double2*>(Gn + kGS * sl);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const double2 v = pp[k];
-        pr[side][2 * k] = v.x;
-        pr[side][2 * k + 1] = v.y;
-      }
-      if (rec != AEROF_REC_CONSTANT) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const double2 v = gp[k];
-          gr[side][2 * k] = v.x;
-          gr[side][2 * k + 1] = v.y;
-        }
-      }
-    }
-    edge_flux_rec(g, rec, beta, failsafe, gi, gj, nx, ny, nz, pr[0], gr[0], pr[1], gr[1], tag, counters, f);
+    edge_flux_rec(g, rec, beta, failsafe, gi, gj, nx, ny, nz, Pn + kPS * li, Gn + kGS * li, Pn + kPS * lj,
+                  Gn + kGS * lj, tag, counters, f);
     double* fs = Fs + 5 * (q - e0);
 #pragma unroll
     for (int k = 0; k < 5; ++k) fs[k] = f[k];

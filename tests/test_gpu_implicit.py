@@ -37,13 +37,19 @@ def test_jacobian_fp64_parity(gpu_lib, setup):
 
 
 def test_jacobian_fp32_storage(gpu_lib, setup):
+    # the FP32 operator of the mixed-precision solver is formed in FP32
+    # arithmetic (edge blocks) and summed into the diagonal in FP64: each
+    # block agrees with the FP64 oracle to FP32 accuracy
     m, Ub, o, U, dt, A = setup
     ctx = gpu_lib.Context.from_mesh(m, Ub)
     mv = gpu_lib.MatVecProdH1(ctx, gpu_lib.PREC_FP32)
     mv.evaluate(U, dt)
     G = mv.blocks()
-    assert np.array_equal(G[o.N:], A[o.N:].astype(np.float32).astype(np.float64))
-    assert rel_l2(G, A) < 1e-7
+    off, ref = G[o.N:].reshape(-1, 25), A[o.N:].reshape(-1, 25)
+    scale = np.abs(ref).max(axis=1, keepdims=True)
+    assert np.abs(off - ref).max() <= 1e-5 * scale.max()
+    assert np.all(np.abs(off - ref) <= 1e-5 * scale + 1e-30)
+    assert rel_l2(G, A) < 1e-6
 
 
 @pytest.mark.parametrize("prec", [64, 32])

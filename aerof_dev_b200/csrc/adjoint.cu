@@ -919,12 +919,71 @@ __global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const
                              const int* __restrict__ nbr_tpos, const double* __restrict__ gd,
                              const double* __restrict__ geo, int E, const int* __restrict__ nt_ptr,
                              const int* __restrict__ nt_tet, const int* __restrict__ nf_ptr,
-                             const int* __restrict__ nf_face, const double* __restrict__ gvol,
+                             const int* __restrict__ nf_face, const double* __restrict__ tg,
                              const double* __restrict__ gfn, double* __restrict__ gX);
 
 }  // namespace aerof
 
 namespace aerof {
+
+// Per tet: cotangents of its four vertices' coordinates through the
+// control volumes and the dual-cell edge normals, reverse mode in closed
+// form.  Volume V = (e3 . (e1 x e2)) / 6, e_i = x_i - x_0; edge normal
+// n = 1.5 s (xg1 x xg0) with xg = face centroid - tet centroid
+// (ElemTetCore.C:281-330), so g_xg1 = xg0 x g_c, g_xg0 = g_c x xg1 with
+// g_c = 1.5 s g_n, then a third to each vertex of the face and minus a
+// quarter to every vertex for the centroid.  tg[t][3 a + c].
+__global__ void k_a_tet_x(int T, const double* __restrict__ X, const int* __restrict__ tets,
+                          const int* __restrict__ tet_edge, const double* __restrict__ geo, int E,
+                          const double* __restrict__ gvol, double* __restrict__ tg) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= T) return;
+  const int* nd = tets + 4 * (size_t)t;
+  const double gvt = 0.25 * (gvol[nd[0]] + gvol[nd[1]] + gvol[nd[2]] + gvol[nd[3]]);
+  Vec3<double> x[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) x[v] = node_x(X, nd[v]);
+  const Vec3<double> e1 = x[1] - x[0], e2 = x[2] - x[0], e3 = x[3] - x[0];
+  const double sv = gvt / 6.0;
+  Vec3<double> g[4];
+  g[1] = scale(sv, cross(e2, e3));
+  g[2] = scale(sv, cross(e3, e1));
+  g[3] = scale(sv, cross(e1, e2));
+  g[0] = v3(0.0, 0.0, 0.0) - (g[1] + g[2] + g[3]);
+  const double third = 1.0 / 3.0;
+  Vec3<double> f[4];
+  f[0] = scale(third, x[0] + x[1] + x[2]);
+  f[1] = scale(third, x[0] + x[1] + x[3]);
+  f[2] = scale(third, x[0] + x[2] + x[3]);
+  f[3] = scale(third, x[1] + x[2] + x[3]);
+  const Vec3<double> gc0 = scale(0.25, x[0] + x[1] + x[2] + x[3]);
+  Vec3<double> gf[4] = {v3(0.0, 0.0, 0.0), v3(0.0, 0.0, 0.0), v3(0.0, 0.0, 0.0), v3(0.0, 0.0, 0.0)};
+  Vec3<double> gcen = v3(0.0, 0.0, 0.0);
+#pragma unroll
+  for (int l = 0; l < 6; ++l) {
+    const int F0 = tet_edge_face(l, 0), F1 = tet_edge_face(l, 1);
+    const Vec3<double> xg0 = f[F0] - gc0, xg1 = f[F1] - gc0;
+    const size_t el = (size_t)tet_edge[6 * (size_t)t + l];
+    const double sl = nd[tet_edge_end(l, 0)] < nd[tet_edge_end(l, 1)] ? 1.5 : -1.5;
+    const Vec3<double> gcv = v3(sl * geo[el], sl * geo[(size_t)E + el], sl * geo[2 * (size_t)E + el]);
+    const Vec3<double> g1 = cross(xg0, gcv), g0 = cross(gcv, xg1);
+    gf[F0] = gf[F0] + g0;
+    gf[F1] = gf[F1] + g1;
+    gcen = gcen + g0 + g1;
+  }
+  // face k holds every vertex but 3 - k
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    Vec3<double> s = v3(0.0, 0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (a != 3 - k) s = s + gf[k];
+    const Vec3<double> d = g[a] + scale(third, s) - scale(0.25, gcen);
+    tg[12 * (size_t)t + 3 * a] = d.x;
+    tg[12 * (size_t)t + 3 * a + 1] = d.y;
+    tg[12 * (size_t)t + 3 * a + 2] = d.z;
+  }
+}
 
 __global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const int* __restrict__ tets,
                              const int* __restrict__ tet_edge, const int* __restrict__ faces,
@@ -932,7 +991,7 @@ __global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const
                              const int* __restrict__ nbr_tpos, const double* __restrict__ gd,
                              const double* __restrict__ geo, int E, const int* __restrict__ nt_ptr,
                              const int* __restrict__ nt_tet, const int* __restrict__ nf_ptr,
-                             const int* __restrict__ nf_face, const double* __restrict__ gvol,
+                             const int* __restrict__ nf_face, const double* __restrict__ tg,
                              const double* __restrict__ gfn, double* __restrict__ gX) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= N) return;
@@ -949,50 +1008,12 @@ __global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const
       for (int c = 0; c < 3; ++c) gx[c] += gd[3 * tp + c] - gd[3 * (size_t)p + c];
     }
   }
-  // tets: control volumes and dual-cell normals, reverse mode in closed
-  // form for this vertex a.  Volume V = (e3 . (e1 x e2)) / 6, e_i = x_i - x_0;
-  // edge normal n = 1.5 s (xg1 x xg0) with xg = face centroid - tet centroid
-  // (ElemTetCore.C:281-330), so g_xg1 = xg0 x g_c, g_xg0 = g_c x xg1 with
-  // g_c = 1.5 s g_n, then a third to each vertex of the face and a quarter
-  // to every vertex (with minus) for the centroid.
+  // tets: the per-tet vertex cotangents of k_a_tet_x
   for (int p = nt_ptr[q]; p < nt_ptr[q + 1]; ++p) {
-    const int t = nt_tet[p] >> 2, a = nt_tet[p] & 3;
-    const int* nd = tets + 4 * (size_t)t;
-    const double gvt = 0.25 * (gvol[nd[0]] + gvol[nd[1]] + gvol[nd[2]] + gvol[nd[3]]);
-    Vec3<double> x[4];
+    const size_t t = (size_t)(nt_tet[p] >> 2);
+    const int a = nt_tet[p] & 3;
 #pragma unroll
-    for (int v = 0; v < 4; ++v) x[v] = node_x(X, nd[v]);
-    const Vec3<double> e1 = x[1] - x[0], e2 = x[2] - x[0], e3 = x[3] - x[0];
-    Vec3<double> dV;
-    if (a == 1) dV = cross(e2, e3);
-    else if (a == 2) dV = cross(e3, e1);
-    else if (a == 3) dV = cross(e1, e2);
-    else dV = v3(0.0, 0.0, 0.0) - (cross(e2, e3) + cross(e3, e1) + cross(e1, e2));
-    const double sixth = 1.0 / 6.0;
-    double acc[3] = {sixth * dV.x * gvt, sixth * dV.y * gvt, sixth * dV.z * gvt};
-    const double third = 1.0 / 3.0;
-    Vec3<double> f[4];
-    f[0] = scale(third, x[0] + x[1] + x[2]);
-    f[1] = scale(third, x[0] + x[1] + x[3]);
-    f[2] = scale(third, x[0] + x[2] + x[3]);
-    f[3] = scale(third, x[1] + x[2] + x[3]);
-    const Vec3<double> gc0 = scale(0.25, x[0] + x[1] + x[2] + x[3]);
-#pragma unroll
-    for (int l = 0; l < 6; ++l) {
-      const int F0 = tet_edge_face(l, 0), F1 = tet_edge_face(l, 1);
-      const Vec3<double> xg0 = f[F0] - gc0, xg1 = f[F1] - gc0;
-      const size_t el = (size_t)tet_edge[6 * (size_t)t + l];
-      const double sl = nd[tet_edge_end(l, 0)] < nd[tet_edge_end(l, 1)] ? 1.5 : -1.5;
-      const Vec3<double> gcv = v3(sl * geo[el], sl * geo[(size_t)E + el], sl * geo[2 * (size_t)E + el]);
-      const Vec3<double> g1 = cross(xg0, gcv), g0 = cross(gcv, xg1);
-      // face k holds every vertex but 3 - k
-      const double w0 = (a != 3 - F0 ? third : 0.0) - 0.25, w1 = (a != 3 - F1 ? third : 0.0) - 0.25;
-      acc[0] += w0 * g0.x + w1 * g1.x;
-      acc[1] += w0 * g0.y + w1 * g1.y;
-      acc[2] += w0 * g0.z + w1 * g1.z;
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) gx[c] += acc[c];
+    for (int c = 0; c < 3; ++c) gx[c] += tg[12 * t + 3 * a + c];
   }
   // boundary faces: n = (3 x02 x x01 + 3 x02 x x01) / 12 (FaceTriaCore.C:
   // 65-82) = x02 x x01 / 2, so g_x02 = x01 x g_n / 2, g_x01 = g_n x x02 / 2
@@ -1078,9 +1099,12 @@ void dRdX_T_dev(aerof_gpu_ctx* c, const double* dU, const double* dlam, double* 
                                     dJT);
     AEROF_LAUNCH_CHECK();
   }
+  a.tg.ensure(12 * (size_t)std::max(m.T, 1));
+  k_a_tet_x<<<grid_for(m.T, kAB), kAB, 0, s>>>(m.T, m.X.p, m.tets.p, m.tet_edge.p, a.geo.p, m.E, a.gvol.p, a.tg.p);
+  AEROF_LAUNCH_CHECK();
   k_a_gather_x<<<gn, kAB, 0, s>>>(m.N, rec, m.X.p, m.tets.p, m.tet_edge.p, m.faces.p, m.nbr_ptr.p, m.nbr_edge.p,
                                   m.nbr_tpos.p, a.gd.p, a.geo.p, m.E, m.nt_ptr.p, m.nt_tet.p, m.nf_ptr.p,
-                                  m.nf_face.p, a.gvol.p, a.gfn.p, dgX);
+                                  m.nf_face.p, a.tg.p, a.gfn.p, dgX);
   AEROF_LAUNCH_CHECK();
 }
 

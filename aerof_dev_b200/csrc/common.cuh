@@ -206,6 +206,7 @@ struct AdjWork {
   DBuf<double> gVp, gGp;   // [N][5], [N][16] in-block partial sums (blocked numbering)
   DBuf<double> spill;      // [nX][13] second-endpoint parts of block-crossing edges
   DBuf<double> geo;        // [6][E] cotangents of edge normals and dx (original edge order)
+  DBuf<double> tg;         // [T][12] per-tet vertex coordinate cotangents
 };
 
 // CUDA-event timers per category (AEROF_T_*), recorded without host sync.

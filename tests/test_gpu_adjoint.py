@@ -96,7 +96,9 @@ def test_linearized_solve_flexible(gpu_lib, case, transpose):
 def test_transposed_assembly_is_the_transpose(gpu_lib, case):
     # the flexible adjoint solve assembles H1^T directly (coalesced transpose
     # products); read back, it is the FP32 H1 assembled the usual way, and
-    # its products with and without transpose match
+    # its products with and without transpose match.  Both are formed in
+    # FP32 arithmetic by different rows of each edge, so they agree to FP32
+    # rounding, not bit for bit.
     rec, m, Ub, o, U, ctx = case
     S = gpu_lib.Sensitivity(ctx)
     b = np.random.default_rng(17).standard_normal(U.shape)
@@ -106,9 +108,11 @@ def test_transposed_assembly_is_the_transpose(gpu_lib, case):
     p = np.random.default_rng(18).standard_normal(U.shape)
     yT, y = mv.apply(p, transpose=True), mv.apply(p)
     mv.evaluate(U)
-    assert np.array_equal(GT, mv.blocks())
-    assert rel_l2(mv.apply(p, transpose=True), yT) < 1e-15
-    assert rel_l2(mv.apply(p), y) < 1e-15
+    G = mv.blocks()
+    scale = np.abs(G).reshape(len(G), 25).max(axis=1)
+    assert np.all(np.abs(GT - G).reshape(len(G), 25).max(axis=1) <= 1e-5 * scale + 1e-30)
+    assert rel_l2(mv.apply(p, transpose=True), yT) < 1e-6
+    assert rel_l2(mv.apply(p), y) < 1e-6
 
 
 def test_dRdX_T_fresh_context_and_fused_products(gpu_lib, case):

@@ -138,7 +138,7 @@ def cpu_baseline(mesh, Ub, U, E: int, budget_s: float = 20.0, max_evals: int = 2
     dt = time.perf_counter() - t0
     return {"value": E * k / dt / 1e6, "unit": "Medges/s", "cores": cores, "kind": "port",
             "sample": f"{k} full second-order residual evaluations of the 101^3 mesh after 1 warm-up "
-                      f"({dt:.1f} s), OpenMP over {cores} threads, g++ -O3 -march=native"}
+                      f"({dt:.1f} s), OpenMP over {cores} threads, g++ -O3 -march=x86-64-v3"}
 
 
 def run_reference(args):

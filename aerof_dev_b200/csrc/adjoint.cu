@@ -512,7 +512,8 @@ __global__ void __launch_bounds__(256, 1) k_a_fv_blocked(int N, int E, int NB, G
       for (int k = threadIdx.x; k < 8 * nn; k += blockDim.x) cp_async16(gd + (kGS / 2) * (k >> 3) + (k & 7), gs + k);
     for (int k = threadIdx.x; k < 4 * nh; k += blockDim.x) {
       const int j = hf[k >> 2];
-      cp_async16(pd + (kPS / 2) * (nn + (k >> 2)) + (k & 3), reinterpret_cast<const double2*>(P + 8 * (size_t)j) + (k & 3));
+      cp_async16(pd + (kPS / 2) * (nn + (k >> 2)) + (k & 3),
+                 reinterpret_cast<const double2*>(P + 8 * (size_t)j) + (k & 3));
     }
     for (int k = threadIdx.x; k < 3 * nh; k += blockDim.x) {
       const int j = hf[k / 3];
@@ -521,7 +522,8 @@ __global__ void __launch_bounds__(256, 1) k_a_fv_blocked(int N, int E, int NB, G
     if (grad)
       for (int k = threadIdx.x; k < 8 * nh; k += blockDim.x) {
         const int j = hf[k >> 3];
-        cp_async16(gd + (kGS / 2) * (nn + (k >> 3)) + (k & 7), reinterpret_cast<const double2*>(G + 16 * (size_t)j) + (k & 7));
+        cp_async16(gd + (kGS / 2) * (nn + (k >> 3)) + (k & 7),
+                   reinterpret_cast<const double2*>(G + 16 * (size_t)j) + (k & 7));
       }
   }
   cp_async_wait_all();
@@ -775,7 +777,8 @@ namespace aerof {
 // (forward mode in the 3 normal directions).
 __global__ void k_a_face_normal(int F, Gas g, const double* __restrict__ Ub0, const int* __restrict__ faces,
                                 const int* __restrict__ fcode, const double* __restrict__ fn,
-                                const double* __restrict__ P, const double* __restrict__ lam, double* __restrict__ gfn) {
+                                const double* __restrict__ P, const double* __restrict__ lam,
+                                double* __restrict__ gfn) {
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= F) return;
   const double third = 1.0 / 3.0;
@@ -1091,12 +1094,13 @@ void dRdX_T_dev(aerof_gpu_ctx* c, const double* dU, const double* dlam, double* 
     AEROF_LAUNCH_CHECK();
   }
   if (rec != AEROF_REC_CONSTANT) {
-    k_a_lsq_x<<<grid_for(4 * (size_t)m.N, kAB), kAB, 0, s>>>(m.N, m.P.p, m.lsqR.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, a.gG.p, a.gd.p);
+    k_a_lsq_x<<<grid_for(4 * (size_t)m.N, kAB), kAB, 0, s>>>(m.N, m.P.p, m.lsqR.p, m.lsqW.p, m.nbr_ptr.p,
+                                                             m.nbr_node.p, a.gG.p, a.gd.p);
     AEROF_LAUNCH_CHECK();
   }
   if (dJT) {
-    k_a_lsq_prim<<<grid_for(4 * (size_t)m.N, kAB), kAB, 0, s>>>(m.N, g, rec, dU, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, a.gV.p, a.gG.p,
-                                    dJT);
+    k_a_lsq_prim<<<grid_for(4 * (size_t)m.N, kAB), kAB, 0, s>>>(m.N, g, rec, dU, m.P.p, m.lsqW.p, m.nbr_ptr.p,
+                                                                m.nbr_node.p, a.gV.p, a.gG.p, dJT);
     AEROF_LAUNCH_CHECK();
   }
   a.tg.ensure(12 * (size_t)std::max(m.T, 1));

@@ -23,9 +23,15 @@ struct Vec3 {
   T x, y, z;
 };
 template <class T> __device__ __forceinline__ Vec3<T> v3(T a, T b, T c) { return Vec3<T>{a, b, c}; }
-template <class T> __device__ __forceinline__ Vec3<T> operator+(Vec3<T> a, Vec3<T> b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
-template <class T> __device__ __forceinline__ Vec3<T> operator-(Vec3<T> a, Vec3<T> b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
-template <class T> __device__ __forceinline__ Vec3<T> scale(double c, Vec3<T> a) { return v3(c * a.x, c * a.y, c * a.z); }
+template <class T> __device__ __forceinline__ Vec3<T> operator+(Vec3<T> a, Vec3<T> b) {
+  return v3(a.x + b.x, a.y + b.y, a.z + b.z);
+}
+template <class T> __device__ __forceinline__ Vec3<T> operator-(Vec3<T> a, Vec3<T> b) {
+  return v3(a.x - b.x, a.y - b.y, a.z - b.z);
+}
+template <class T> __device__ __forceinline__ Vec3<T> scale(double c, Vec3<T> a) {
+  return v3(c * a.x, c * a.y, c * a.z);
+}
 // Vec3D::operator^ (Vector3D.h:266-274)
 template <class T> __device__ __forceinline__ Vec3<T> cross(Vec3<T> a, Vec3<T> b) {
   return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);

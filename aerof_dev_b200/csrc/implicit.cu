@@ -155,7 +155,8 @@ template <class S> struct JacThreads {
 };
 
 template <class S, bool TR>
-__global__ void __launch_bounds__(JacThreads<S>::T, JacThreads<S>::B) k_jac_rows(int N, int E, int F, Gas g, const double* __restrict__ Ub0,
+__global__ void __launch_bounds__(JacThreads<S>::T, JacThreads<S>::B)
+    k_jac_rows(int N, int E, int F, Gas g, const double* __restrict__ Ub0,
                                                   const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_node,
                                                   const int* __restrict__ nbr_edge, const double* __restrict__ en,
                                                   const double* __restrict__ P, const double* __restrict__ vol,

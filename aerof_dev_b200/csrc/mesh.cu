@@ -397,7 +397,8 @@ void compute_geometry(aerof_gpu_ctx* c) {
   m.lsqW.alloc(6 * (size_t)m.N);
   k_ctrl_vol<double><<<grid_for(m.N, kMBlock), kMBlock, 0, s>>>(m.N, m.X.p, m.tets.p, m.nt_ptr.p, m.nt_tet.p, m.vol.p);
   AEROF_LAUNCH_CHECK();
-  k_edge_normals<double><<<grid_for(m.E, kMBlock), kMBlock, 0, s>>>(m.E, m.X.p, m.tets.p, m.et_ptr.p, m.et_tet.p, m.en.p);
+  k_edge_normals<double><<<grid_for(m.E, kMBlock), kMBlock, 0, s>>>(m.E, m.X.p, m.tets.p, m.et_ptr.p, m.et_tet.p,
+                                                                      m.en.p);
   AEROF_LAUNCH_CHECK();
   if (m.F) {
     k_face_normals<double><<<grid_for(m.F, kMBlock), kMBlock, 0, s>>>(m.F, m.X.p, m.faces.p, m.fnrm.p);
@@ -490,7 +491,8 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
       }
       HostBlocked hb;
       build_blocked(N, E, m.NB, X, h.edges, hb);
-      m.nblk = hb.nblk; m.maxE = hb.maxE; m.nX = hb.nX; m.maxH = hb.maxH; m.maxL = hb.maxL; m.maxHf = hb.maxHf; m.maxLp = hb.maxLp;
+      m.nblk = hb.nblk; m.maxE = hb.maxE; m.nX = hb.nX;
+      m.maxH = hb.maxH; m.maxL = hb.maxL; m.maxHf = hb.maxHf; m.maxLp = hb.maxLp;
       m.hpad.upload(hb.hpad.data(), hb.hpad.size(), s);
       m.lpad.upload(hb.lpad.data(), hb.lpad.size(), s);
       m.hfpad.upload(hb.hfpad.data(), hb.hfpad.size(), s);

@@ -182,7 +182,8 @@ __global__ void __launch_bounds__(256, 3) k_grad_staged(int N, int NB, Gas g, co
     for (int k = threadIdx.x; k < 4 * nn; k += blockDim.x) cp_async16(pd + (kPS / 2) * (k >> 2) + (k & 3), ps + k);
     for (int k = threadIdx.x; k < 4 * nh; k += blockDim.x) {
       const int j = hnode[h0 + (k >> 2)];
-      cp_async16(pd + (kPS / 2) * (nn + (k >> 2)) + (k & 3), reinterpret_cast<const double2*>(P2 + 8 * (size_t)j) + (k & 3));
+      cp_async16(pd + (kPS / 2) * (nn + (k >> 2)) + (k & 3),
+                 reinterpret_cast<const double2*>(P2 + 8 * (size_t)j) + (k & 3));
     }
     cp_async_wait_all();
   }
@@ -436,7 +437,8 @@ __global__ void k_edge_flux(int E, Gas g, int rec, double beta, int failsafe, co
 // edges held in shared memory in ascending edge order (+ as first endpoint,
 // - as second) into part[].
 template <int THREADS, int MINB>
-__global__ void __launch_bounds__(THREADS, MINB) k_fv_blocked(int N, int E, int NB, Gas g, int rec, double beta, int failsafe,
+__global__ void __launch_bounds__(THREADS, MINB)
+    k_fv_blocked(int N, int E, int NB, Gas g, int rec, double beta, int failsafe,
                                                     const ushort2* __restrict__ bl, const double* __restrict__ bn,
                                                     const int* __restrict__ beptr, const int* __restrict__ hfptr,
                                                     const int* __restrict__ hfpad, int maxHf,
@@ -479,7 +481,8 @@ __global__ void __launch_bounds__(THREADS, MINB) k_fv_blocked(int N, int E, int 
     // forward halo: one 64 B and one 128 B record per node
     for (int k = threadIdx.x; k < 4 * nh; k += blockDim.x) {
       const int j = hf[k >> 2];
-      cp_async16(pd + (kPS / 2) * (nn + (k >> 2)) + (k & 3), reinterpret_cast<const double2*>(P + 8 * (size_t)j) + (k & 3));
+      cp_async16(pd + (kPS / 2) * (nn + (k >> 2)) + (k & 3),
+                 reinterpret_cast<const double2*>(P + 8 * (size_t)j) + (k & 3));
     }
     if (grad)
       for (int k = threadIdx.x; k < 8 * nh; k += blockDim.x) {
@@ -569,7 +572,8 @@ __global__ void __launch_bounds__(THREADS, MINB) k_fv_blocked(int N, int E, int 
 // of the node (face order), times 1/ctrlVol; written to R in the caller's
 // numbering.
 __global__ void k_fv_nodes(int N, const int* __restrict__ o2n, const double* __restrict__ part,
-                           const int* __restrict__ xin_ptr, const double* __restrict__ spill, const int* __restrict__ nf_ptr,
+                           const int* __restrict__ xin_ptr, const double* __restrict__ spill,
+                           const int* __restrict__ nf_ptr,
                            const int* __restrict__ nf_face, const int* __restrict__ faces,
                            const double* __restrict__ fbuf, const double* __restrict__ vol, double* __restrict__ R) {
   // one thread per row of R in the caller's numbering (coalesced writes);
@@ -948,8 +952,16 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
   const int by_smem = (int)std::min<size_t>(4, (228 * 1024) / (smem + 1024));
   // 256 threads with the register budget of the CTAs that fit (384
   // threads at two CTAs per SM measured slower)
-  const int fv_threads = 256;
-  auto fvk = by_smem >= 4 ? k_fv_blocked<256, 4> : by_smem == 3 ? k_fv_blocked<256, 3> : k_fv_blocked<256, 2>;
+  // tuning knob AEROF_FV_THREADS = 512: two CTAs of 512 threads per SM at
+  // 64 registers (more warps, some spilling) when shared memory allows two
+  static const int fv_env = [] {
+    const char* e = std::getenv("AEROF_FV_THREADS");
+    return e ? std::atoi(e) : 256;
+  }();
+  const bool wide = fv_env == 512 && by_smem >= 2;
+  const int fv_threads = wide ? 512 : 256;
+  auto fvk = wide ? k_fv_blocked<512, 2>
+                  : by_smem >= 4 ? k_fv_blocked<256, 4> : by_smem == 3 ? k_fv_blocked<256, 3> : k_fv_blocked<256, 2>;
   AEROF_CUDA(cudaFuncSetAttribute(fvk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   {
     TimerScope t(c, AEROF_T_NODAL_GRAD);
@@ -1281,7 +1293,8 @@ extern "C" int aerof_gpu_residual_noalloc(aerof_gpu_ctx* c, const double* U, dou
     k_prim<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, U, m.P.p);
     AEROF_LAUNCH_CHECK();
     if (rec != AEROF_REC_CONSTANT) {
-      k_grad<<<grid_for(4 * (size_t)m.N, kBlock), kBlock, 0, s>>>(m.N, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, nullptr, G);
+      k_grad<<<grid_for(4 * (size_t)m.N, kBlock), kBlock, 0, s>>>(m.N, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p,
+                                                                  nullptr, G);
       AEROF_LAUNCH_CHECK();
     }
     k_edge_flux<<<grid_for(m.E, kBlock), kBlock, 0, s>>>(m.E, g, rec, c->cfg.beta, c->cfg.failsafe, m.edges.p,
@@ -1291,7 +1304,8 @@ extern "C" int aerof_gpu_residual_noalloc(aerof_gpu_ctx* c, const double* U, dou
     AEROF_CUDA(cudaMemcpyAsync(&bad, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
     AEROF_CUDA(cudaStreamSynchronize(s));
     if (bad && c->cfg.failsafe && rec != AEROF_REC_CONSTANT) {
-      k_grad<<<grid_for(4 * (size_t)m.N, kBlock), kBlock, 0, s>>>(m.N, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p, tag, G);
+      k_grad<<<grid_for(4 * (size_t)m.N, kBlock), kBlock, 0, s>>>(m.N, m.P.p, m.lsqW.p, m.nbr_ptr.p, m.nbr_node.p,
+                                                                  tag, G);
       AEROF_LAUNCH_CHECK();
       k_edge_flux<<<grid_for(m.E, kBlock), kBlock, 0, s>>>(m.E, g, rec, c->cfg.beta, 0, m.edges.p, m.en.p, m.P.p, G,
                                                            flux, tag, cnt + 1);

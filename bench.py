@@ -190,6 +190,7 @@ def config_dict(args, s) -> dict:
 def run_ours(args):
     import torch
     import aerof_dev_b200 as A
+    from aerof_dev_b200.replicas import aggregate_rate, max_over_ranks
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     pg = None
@@ -243,11 +244,8 @@ def run_ours(args):
     tm = ctx.timers()
     ctx.profile(False)
     clk = clocks.stop()
-    if pg:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
-    value = s["E"] * args.steps * world / (ms * 1e-3) / 1e6
+    ms = max_over_ranks(ms, "cuda")
+    value = aggregate_rate(s["E"] * args.steps, world, ms) / 1e6
 
     # end to end through the public API with pinned host buffers
     Uh = torch.from_numpy(U).pin_memory()
@@ -265,11 +263,8 @@ def run_ours(args):
     a1.record(stream)
     torch.cuda.synchronize()
     ms2 = a0.elapsed_time(a1)
-    if pg:
-        t = torch.tensor([ms2], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms2 = float(t.item())
-    e2e = s["E"] * k2 * world / (ms2 * 1e-3) / 1e6
+    ms2 = max_over_ranks(ms2, "cuda")
+    e2e = aggregate_rate(s["E"] * k2, world, ms2) / 1e6
 
     peaks = measured_peaks()
     # the finite-volume term (edge fluxes, boundary fluxes, node assembly)

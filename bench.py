@@ -413,6 +413,49 @@ def run_adjoint(args):
     return 0
 
 
+def run_adjoint_products(args):
+    """Per-call device times of the residual and of the exact linearised
+    products on a smooth state (no flow solve): J v, J^T w, (dR/dX)^T lam and
+    both adjoint products from one reverse sweep; 3 warm-up + 10 timed calls
+    each, CUDA events on the context's stream."""
+    import torch
+    import aerof_dev_b200 as A
+    from aerof_dev_b200 import workloads as W
+    torch.cuda.set_device(0)
+    mesh = W.make_lattice_mesh(args.n, jitter=0.2, codes="channel")
+    Ub = W.freestream(0.8)
+    ctx = A.Context.from_mesh(mesh, Ub, reconstruction=args.rec)
+    ctx.set_stream(torch.cuda.current_stream())
+    U = torch.from_numpy(W.smooth_state(mesh["X"], 0.8)).cuda()
+    lam = torch.from_numpy(np.random.default_rng(3).standard_normal((ctx.N, 5))).cuda()
+    sp, S = A.SpaceOperator(ctx), A.Sensitivity(ctx)
+    R = torch.empty_like(U)
+    out = {}
+    for name, fn in (("residual", lambda: sp.computeResidual(U, R)), ("jvp", lambda: S.jvp(U, lam)),
+                     ("vjp", lambda: S.vjp(U, lam)), ("dRdX_T", lambda: S.dRdX_T(U, lam)),
+                     ("adjoint_products", lambda: S.adjoint_products(U, lam))):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = e0.elapsed_time(e1) / 10
+    s = W.lattice_sizes(args.n)
+    line = {"metric": METRIC, "workload": "adjoint_products", "value": out["adjoint_products"] / out["residual"],
+            "unit": "x one primal residual (J^T lambda and dR/dX^T lambda, one reverse sweep)",
+            "higher_is_better": False, "ms": out,
+            "config": {"workload": f"{args.n}^3 jittered Kuhn tet mesh N={s['N']} E={s['E']}, smooth Mach 0.8 state",
+                       "reconstruction": {1: "constant", 2: "van Albada", 3: "linear"}[args.rec]}}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -423,7 +466,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=200)
     ap.add_argument("--ref-budget", type=float, default=120.0, help="seconds of timed CPU work (reference arm)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["residual", "newton", "adjoint"], default="residual")
+    ap.add_argument("--workload", choices=["residual", "newton", "adjoint", "adjoint_products"], default="residual")
     ap.add_argument("--max-steps", type=int, default=400)
     ap.add_argument("--modes", type=int, default=32)
     ap.add_argument("--fd-modes", type=int, default=4)
@@ -440,6 +483,8 @@ def main():
         return run_newton(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.workload == "adjoint_products":
+        return run_adjoint_products(args)
     return run_ours(args)
 
 

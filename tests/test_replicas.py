@@ -31,7 +31,7 @@ def test_max_over_ranks_gloo_two_ranks():
     import torch.multiprocessing as mp
     world, port = 2, _free_port()
     values = [3.5, 7.25]
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.spawn(_worker, args=(world, port, values, out), nprocs=world, join=True)
     for r in range(world):

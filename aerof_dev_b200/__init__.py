@@ -49,6 +49,7 @@ EXPORTS = [
     "aerof_gpu_jvp", "aerof_gpu_vjp", "aerof_gpu_dRdX", "aerof_gpu_dRdX_T", "aerof_gpu_adjoint_products",
     "aerof_gpu_residual_async", "aerof_gpu_status", "aerof_gpu_profile", "aerof_gpu_timers",
     "aerof_gpu_update_coordinates", "aerof_gpu_linearized_solve", "aerof_gpu_residual_noalloc",
+    "aerof_gpu_h2_evaluate", "aerof_gpu_h2_apply", "aerof_gpu_h2_release", "aerof_gpu_set_exact_operator",
 ]
 TIMER_NAMES = ["nodal_grad", "fv_term", "time_step", "fv_jac", "prec_setup", "ksp_matvec", "ksp_other", "other"]
 
@@ -124,6 +125,10 @@ def library(path: str | None = None):
             "aerof_gpu_residual_noalloc": [vp, dp, dp],
             "aerof_gpu_linearized_solve": [vp, dp, dp, dp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
                                            C.POINTER(C.c_int), C.POINTER(C.c_double)],
+            "aerof_gpu_h2_evaluate": [vp, dp],
+            "aerof_gpu_h2_apply": [vp, dp, dp, C.c_int],
+            "aerof_gpu_h2_release": [vp],
+            "aerof_gpu_set_exact_operator": [vp, C.c_int],
         }
         for name, args in sig.items():
             if hasattr(L, name):
@@ -511,6 +516,30 @@ class Sensitivity:
         b = _Arg(_like(lam, (ctx.N, 3)), np.float64, writable=True)
         ctx._check(ctx.L.aerof_gpu_adjoint_products(ctx.h, u.ptr, l.ptr, a.ptr, b.ptr))
         return a.obj, b.obj
+
+    def h2_evaluate(self, U):
+        """MatVecProdH2::evaluate: store the exact linearisation at U on the
+        device (560 bytes per edge)."""
+        ctx = self.ctx
+        u = _Arg(U, np.float64, (ctx.N, 5))
+        ctx._check(ctx.L.aerof_gpu_h2_evaluate(ctx.h, u.ptr))
+
+    def h2_apply(self, p, transpose=False):
+        """MatVecProdH2::apply (J p) or applyTranspose (J^T p) with the
+        stored operator."""
+        ctx = self.ctx
+        a = _Arg(p, np.float64, (ctx.N, 5))
+        b = _Arg(_like(p, (ctx.N, 5)), np.float64, writable=True)
+        ctx._check(ctx.L.aerof_gpu_h2_apply(ctx.h, a.ptr, b.ptr, int(transpose)))
+        return b.obj
+
+    def h2_release(self):
+        self.ctx._check(self.ctx.L.aerof_gpu_h2_release(self.ctx.h))
+
+    def set_exact_operator(self, stored: bool):
+        """Exact products of `solve`: re-evaluated per product (False) or
+        from the operator stored once per solve (True)."""
+        self.ctx._check(self.ctx.L.aerof_gpu_set_exact_operator(self.ctx.h, int(bool(stored))))
 
     def solve(self, U, b, transpose=False, krylov=30, maxits=300, eps=1e-10, inner_its=0):
         """Solve J x = b (direct) or J^T x = b (adjoint) with the exact

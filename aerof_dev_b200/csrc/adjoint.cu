@@ -1112,6 +1112,693 @@ void dRdX_T_dev(aerof_gpu_ctx* c, const double* dU, const double* dlam, double* 
   AEROF_LAUNCH_CHECK();
 }
 
+// ---------------------------------------------------------------------
+// STORED EXACT LINEARISATION (MatVecProdH2, MatVecProd.C:1462-1704).  The
+// reference's evaluate keeps per edge the reconstruction coefficients
+// (SubDomain::precomputeRec, SubDomain.C:3836-3865) and the two flux
+// Jacobians (A at numNodes + 2l, + 1, computeH2); apply and applyTranspose
+// (SubDomain::computeMatVecProdH2, SubDomain.C:4076-4190) form the
+// direction's gradients, reconstruct it linearly, apply the blocks and
+// assemble.  Here, per blocked edge, the 50 block entries and the 20
+// reconstruction partials are stored as 35 16-byte pairs, SoA by pair
+// ([35][E] double2, one coalesced 16-byte load per pair):
+//   pair 5 r + c (r, c < 5): (d phi_r / d Vij_c, d phi_r / d Vji_c)
+//   pair 25 + c:             (p1_c, p2_c)
+//   pair 30 + c:             (q1_c, q2_c)
+// and per boundary row the summed face-flux Jacobian; a product is one
+// pass over that data in the blocked organisation plus the gradient
+// (forward) or its transpose (reverse).
+
+// Thread per blocked edge, CTA per block: the reconstruction at the
+// linearisation state, d phi / d Vij and d phi / d Vji by five reverse
+// evaluations of the Roe flux (row r from the unit cotangent e_r), and the
+// partials of the reconstruction of each component.
+__global__ void __launch_bounds__(128) k_h2_edges(int N, int E, int NB, Gas g, int rec, double beta,
+                                                  const ushort2* __restrict__ bl, const double* __restrict__ bn,
+                                                  const int* __restrict__ beptr, const int* __restrict__ hfpad,
+                                                  int maxHf, const double* __restrict__ P2,
+                                                  const double* __restrict__ G2, double2* __restrict__ h2) {
+  const int blk = blockIdx.x;
+  const int n0 = blk * NB;
+  const int nn = min(NB, N - n0);
+  const int e0 = beptr[blk], e1 = beptr[blk + 1];
+  const int* hf = hfpad + (size_t)blk * maxHf;
+  const bool grad = rec != AEROF_REC_CONSTANT;
+  const size_t sE = (size_t)E;
+  for (int q = e0 + threadIdx.x; q < e1; q += blockDim.x) {
+    const ushort2 lq = bl[q];
+    // the first endpoint lies in the block, the second in it or in its
+    // forward halo
+    const size_t ni = (size_t)(n0 + lq.x);
+    const size_t nj = (size_t)(lq.y < nn ? n0 + lq.y : hf[lq.y - nn]);
+    const double* pi = P2 + 8 * ni;
+    const double* pj = P2 + 8 * nj;
+    const double* gi = G2 + 16 * ni;
+    const double* gj = G2 + 16 * nj;
+    const double n0_ = bn[q], n1_ = bn[sE + q], n2_ = bn[2 * sE + q];
+    const double dx0 = pj[5] - pi[5], dx1 = pj[6] - pi[6], dx2 = pj[7] - pi[7];
+    double Vi[5], Vj[5], cp1[5], cp2[5], cq1[5], cq2[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      if (!grad) {
+        Vi[k] = pi[k]; Vj[k] = pj[k];
+        cp1[k] = cp2[k] = cq1[k] = cq2[k] = 0.0;
+        continue;
+      }
+      const double ddij = dx0 * gi[k] + dx1 * gi[5 + k] + dx2 * gi[10 + k];
+      const double ddji = dx0 * gj[k] + dx1 * gj[5 + k] + dx2 * gj[10 + k];
+      if (rec == AEROF_REC_VANALBADA) {
+        vanalbada(beta, pi[k], ddij, pj[k], ddji, Vi[k], Vj[k]);
+        // Vij = Vi + 0.5 f(dVi, dVji), Vji = Vj - 0.5 f(dVj, dVji),
+        // dVji = Vj - Vi, dVi = b2 dVji + 2 beta ddij (RecFcn.h:432-446)
+        const double b2 = 1.0 - 2.0 * beta;
+        const double dVji = pj[k] - pi[k];
+        const double dV = b2 * dVji;
+        double A1, B1, A2, B2;
+        vanalbada_fcn_partials(dV + 2.0 * beta * ddij, dVji, A1, B1);
+        vanalbada_fcn_partials(dV + 2.0 * beta * ddji, dVji, A2, B2);
+        cp1[k] = 0.5 * (B1 + b2 * A1);
+        cp2[k] = 0.5 * (B2 + b2 * A2);
+        cq1[k] = beta * A1;
+        cq2[k] = beta * A2;
+      } else {
+        linear_rec(beta, pi[k], ddij, pj[k], ddji, Vi[k], Vj[k]);
+        cp1[k] = cp2[k] = 0.5 - beta;
+        cq1[k] = cq2[k] = beta;
+      }
+    }
+    const bool live = sqrt(n0_ * n0_ + n1_ * n1_ + n2_ * n2_) >= 1e-18;
+#pragma unroll 1
+    for (int r = 0; r < 5; ++r) {
+      double gF[5], gL[5] = {0, 0, 0, 0, 0}, gR[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+      for (int k = 0; k < 5; ++k) gF[k] = k == r ? 1.0 : 0.0;
+      if (live) roe_flux_adj(g, n0_, n1_, n2_, Vi, Vj, gF, gL, gR, nullptr);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) h2[(size_t)(5 * r + k) * sE + q] = make_double2(gL[k], gR[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      h2[(size_t)(25 + k) * sE + q] = make_double2(cp1[k], cp2[k]);
+      h2[(size_t)(30 + k) * sE + q] = make_double2(cq1[k], cq2[k]);
+    }
+  }
+}
+
+// Per boundary row: the Jacobian d F / d V summed over the row's faces
+// (subface normal n_f / 3), five tangents in one forward evaluation per
+// face; SoA [25][nbrow], element (k, d) = d F_k / d V_d.
+__global__ void k_h2_faces(int nbrow, int F, Gas g, const double* __restrict__ Ub0, const int* __restrict__ blist,
+                           const int* __restrict__ nf_ptr, const int* __restrict__ nf_face,
+                           const int* __restrict__ fcode, const double* __restrict__ fn,
+                           const double* __restrict__ P, double* __restrict__ fj) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbrow) return;
+  const int i = blist[b];
+  double J[25], Ub[5];
+  Dual5 Vd[5];
+#pragma unroll
+  for (int k = 0; k < 25; ++k) J[k] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    Ub[k] = Ub0[k];
+    Vd[k] = Dual5(P[8 * (size_t)i + k]);
+    Vd[k].d[k] = 1.0;
+  }
+  const double third = 1.0 / 3.0;
+  for (int q = nf_ptr[i]; q < nf_ptr[i + 1]; ++q) {
+    const int f = nf_face[q];
+    Dual5 ff[5];
+    face_flux(g, fcode[f], Dual5(third * fn[f]), Dual5(third * fn[(size_t)F + f]), Dual5(third * fn[2 * (size_t)F + f]),
+              Vd, Ub, ff);
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+#pragma unroll
+      for (int d = 0; d < 5; ++d) J[5 * k + d] += ff[k].d[d];
+  }
+#pragma unroll
+  for (int k = 0; k < 25; ++k) fj[(size_t)k * nbrow + b] = J[k];
+}
+
+// (gL, gR) = ((d phi / d Vij)^T gF, (d phi / d Vji)^T gF) of edge q
+__device__ __forceinline__ void h2_transpose_blocks(const double2* __restrict__ h2, size_t sE, int q,
+                                                    const double* gF, double* gL, double* gR) {
+#pragma unroll
+  for (int c = 0; c < 5; ++c) { gL[c] = 0.0; gR[c] = 0.0; }
+#pragma unroll
+  for (int r = 0; r < 5; ++r)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      const double2 a = h2[(size_t)(5 * r + c) * sE + q];
+      gL[c] += a.x * gF[r];
+      gR[c] += a.y * gF[r];
+    }
+}
+
+// J^T of the stored operator, edge part.  CTA per block.  Phase 0: the
+// coordinates and lam2 of the block's nodes and forward halo are staged
+// (cp.async; 32 B of each node record: V4, x, y, z).  Phase 1, thread per
+// edge: gF = lam_i - lam_j, gL = (d phi / d Vij)^T gF, gR = (d phi /
+// d Vji)^T gF kept in shared memory; a block-crossing edge sends the second
+// endpoint's part (g_Vj, g_ddji, dx) to spill.  Phase 2, L lanes per node:
+// the node's edges in edge order through the stored reconstruction
+// partials, g_V += g_Vside, g_grad += dx (x) g_ddside; written to gVp /
+// gGp as k_a_fv_blocked does.
+__global__ void __launch_bounds__(256, 2) k_h2t_blocked(int N, int E, int NB, const ushort2* __restrict__ bl,
+                                                        const int* __restrict__ beptr, const int* __restrict__ hfptr,
+                                                        const int* __restrict__ hfpad, int maxHf,
+                                                        const double* __restrict__ P2, const double* __restrict__ lam2,
+                                                        const int* __restrict__ lptr, const int* __restrict__ lidx,
+                                                        const int* __restrict__ xslot, const double2* __restrict__ h2,
+                                                        double* __restrict__ gVp, double* __restrict__ gGp,
+                                                        double* __restrict__ spill) {
+  extern __shared__ double sm[];
+  const int blk = blockIdx.x;
+  const int n0 = blk * NB;
+  const int nn = min(NB, N - n0);
+  const int nh = hfptr[blk + 1] - hfptr[blk];
+  const int ns = nn + nh;
+  const int e0 = beptr[blk], e1 = beptr[blk + 1];
+  const size_t sE = (size_t)E;
+  int L = 1;
+  while (2 * L * NB <= (int)blockDim.x) L *= 2;
+  const int t2 = threadIdx.x / L, r2 = threadIdx.x % L;
+  const bool act2 = t2 < nn && (int)threadIdx.x < L * NB;
+  const int lb = act2 ? lptr[n0 + t2] : 0, le = act2 ? lptr[n0 + t2 + 1] : 0;
+  double* Xn = sm;             // [ns][4]: V4, x, y, z
+  double* Ln = sm + 4 * ns;    // [ns][6]
+  double* Es = sm + 10 * ns;   // [e1 - e0][10]: gL, gR
+  {
+    const int* hf = hfpad + (size_t)blk * maxHf;
+    double2* xd = reinterpret_cast<double2*>(Xn);
+    double2* ld = reinterpret_cast<double2*>(Ln);
+    const double2* ps = reinterpret_cast<const double2*>(P2 + 8 * (size_t)n0);
+    const double2* ls = reinterpret_cast<const double2*>(lam2 + 6 * (size_t)n0);
+    for (int k = threadIdx.x; k < 2 * nn; k += blockDim.x) cp_async16(xd + k, ps + 4 * (k >> 1) + 2 + (k & 1));
+    for (int k = threadIdx.x; k < 3 * nn; k += blockDim.x) cp_async16(ld + k, ls + k);
+    for (int k = threadIdx.x; k < 2 * nh; k += blockDim.x) {
+      const int j = hf[k >> 1];
+      cp_async16(xd + 2 * nn + k, reinterpret_cast<const double2*>(P2 + 8 * (size_t)j) + 2 + (k & 1));
+    }
+    for (int k = threadIdx.x; k < 3 * nh; k += blockDim.x) {
+      const int j = hf[k / 3];
+      cp_async16(ld + 3 * nn + k, reinterpret_cast<const double2*>(lam2 + 6 * (size_t)j) + k % 3);
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  for (int q = e0 + threadIdx.x; q < e1; q += blockDim.x) {
+    const ushort2 lq = bl[q];
+    double gF[5], gL[5], gR[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) gF[k] = Ln[6 * lq.x + k] - Ln[6 * lq.y + k];
+    h2_transpose_blocks(h2, sE, q, gF, gL, gR);
+    double* es = Es + 10 * (q - e0);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) { es[k] = gL[k]; es[5 + k] = gR[k]; }
+    const int xs = xslot[q];
+    if (xs >= 0) {
+      double* sp = spill + 13 * (size_t)xs;
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        const double2 pp = h2[(size_t)(25 + c) * sE + q];
+        const double q2 = h2[(size_t)(30 + c) * sE + q].y;
+        sp[c] = pp.x * gL[c] + (1.0 - pp.y) * gR[c];
+        sp[5 + c] = -q2 * gR[c];
+      }
+      const double* xi = Xn + 4 * lq.x;
+      const double* xj = Xn + 4 * lq.y;
+      sp[10] = xj[1] - xi[1]; sp[11] = xj[2] - xi[2]; sp[12] = xj[3] - xi[3];
+    }
+  }
+  __syncthreads();
+  double av[5] = {0, 0, 0, 0, 0}, ag[15];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) ag[k] = 0.0;
+  for (int k = lb + r2; k < le; k += L) {
+    const int e = lidx[k];
+    const int slot = e & 0x7fffffff;
+    const bool second = e < 0;
+    const size_t qq = (size_t)(e0 + slot);
+    const ushort2 lq = bl[qq];
+    const double* xi = Xn + 4 * lq.x;
+    const double* xj = Xn + 4 * lq.y;
+    const double dx0 = xj[1] - xi[1], dx1 = xj[2] - xi[2], dx2 = xj[3] - xi[3];
+    const double* es = Es + 10 * slot;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      const double2 pp = h2[(25 + c) * sE + qq], qv = h2[(30 + c) * sE + qq];
+      const double gl = es[c], gr = es[5 + c];
+      const double gv = second ? pp.x * gl + (1.0 - pp.y) * gr : (1.0 - pp.x) * gl + pp.y * gr;
+      const double gd = second ? -qv.y * gr : qv.x * gl;
+      av[c] += gv;
+      ag[c] += dx0 * gd;
+      ag[5 + c] += dx1 * gd;
+      ag[10 + c] += dx2 * gd;
+    }
+  }
+  for (int o = 1; o < L; o <<= 1) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) av[c] += __shfl_xor_sync(0xffffffffu, av[c], o);
+#pragma unroll
+    for (int c = 0; c < 15; ++c) ag[c] += __shfl_xor_sync(0xffffffffu, ag[c], o);
+  }
+  if (act2 && r2 == 0) {
+    const size_t n = (size_t)(n0 + t2);
+#pragma unroll
+    for (int c = 0; c < 5; ++c) gVp[5 * n + c] = av[c];
+#pragma unroll
+    for (int c = 0; c < 15; ++c) gGp[16 * n + c] = ag[c];
+    gGp[16 * n + 15] = 0.0;
+  }
+}
+
+// J^T of the stored operator, edge part, wide form: one CTA of 1024
+// threads per block, used when both endpoints' results of every edge fit in
+// shared memory.  Phase 0 as k_h2t_blocked.  Phase 1 reads each edge's 35
+// pairs once (coalesced) and leaves (g_Vi, g_ddij, g_Vj, g_ddji) in shared
+// memory at a 21-double stride (conflict-free consecutive writes); phase 2
+// gathers from shared memory only.  Same arithmetic as k_h2t_blocked.
+constexpr int kEW = 21;
+__global__ void __launch_bounds__(1024, 1) k_h2t_wide(int N, int E, int NB, const ushort2* __restrict__ bl,
+                                                      const int* __restrict__ beptr, const int* __restrict__ hfptr,
+                                                      const int* __restrict__ hfpad, int maxHf,
+                                                      const double* __restrict__ P2, const double* __restrict__ lam2,
+                                                      const int* __restrict__ lptr, const int* __restrict__ lidx,
+                                                      const int* __restrict__ xslot, const double2* __restrict__ h2,
+                                                      double* __restrict__ gVp, double* __restrict__ gGp,
+                                                      double* __restrict__ spill) {
+  extern __shared__ double sm[];
+  const int blk = blockIdx.x;
+  const int n0 = blk * NB;
+  const int nn = min(NB, N - n0);
+  const int nh = hfptr[blk + 1] - hfptr[blk];
+  const int ns = nn + nh;
+  const int e0 = beptr[blk], e1 = beptr[blk + 1];
+  const size_t sE = (size_t)E;
+  int L = 1;
+  while (2 * L * NB <= (int)blockDim.x) L *= 2;
+  const int t2 = threadIdx.x / L, r2 = threadIdx.x % L;
+  const bool act2 = t2 < nn && (int)threadIdx.x < L * NB;
+  const int lb = act2 ? lptr[n0 + t2] : 0, le = act2 ? lptr[n0 + t2 + 1] : 0;
+  double* Xn = sm;             // [ns][4]: V4, x, y, z
+  double* Ln = sm + 4 * ns;    // [ns][6]
+  double* Es = sm + 10 * ns;   // [e1 - e0][kEW]
+  {
+    const int* hf = hfpad + (size_t)blk * maxHf;
+    double2* xd = reinterpret_cast<double2*>(Xn);
+    double2* ld = reinterpret_cast<double2*>(Ln);
+    const double2* ps = reinterpret_cast<const double2*>(P2 + 8 * (size_t)n0);
+    const double2* ls = reinterpret_cast<const double2*>(lam2 + 6 * (size_t)n0);
+    for (int k = threadIdx.x; k < 2 * nn; k += blockDim.x) cp_async16(xd + k, ps + 4 * (k >> 1) + 2 + (k & 1));
+    for (int k = threadIdx.x; k < 3 * nn; k += blockDim.x) cp_async16(ld + k, ls + k);
+    for (int k = threadIdx.x; k < 2 * nh; k += blockDim.x) {
+      const int j = hf[k >> 1];
+      cp_async16(xd + 2 * nn + k, reinterpret_cast<const double2*>(P2 + 8 * (size_t)j) + 2 + (k & 1));
+    }
+    for (int k = threadIdx.x; k < 3 * nh; k += blockDim.x) {
+      const int j = hf[k / 3];
+      cp_async16(ld + 3 * nn + k, reinterpret_cast<const double2*>(lam2 + 6 * (size_t)j) + k % 3);
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  for (int q = e0 + threadIdx.x; q < e1; q += blockDim.x) {
+    const ushort2 lq = bl[q];
+    double gF[5], gL[5], gR[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) gF[k] = Ln[6 * lq.x + k] - Ln[6 * lq.y + k];
+    h2_transpose_blocks(h2, sE, q, gF, gL, gR);
+    double* es = Es + kEW * (q - e0);
+    const int xs = xslot[q];
+    double* sp = xs >= 0 ? spill + 13 * (size_t)xs : nullptr;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      const double2 pp = h2[(size_t)(25 + c) * sE + q], qv = h2[(size_t)(30 + c) * sE + q];
+      const double gvj = pp.x * gL[c] + (1.0 - pp.y) * gR[c];
+      const double gdj = -qv.y * gR[c];
+      es[c] = (1.0 - pp.x) * gL[c] + pp.y * gR[c];
+      es[5 + c] = qv.x * gL[c];
+      es[10 + c] = gvj;
+      es[15 + c] = gdj;
+      if (sp) { sp[c] = gvj; sp[5 + c] = gdj; }
+    }
+    if (sp) {
+      const double* xi = Xn + 4 * lq.x;
+      const double* xj = Xn + 4 * lq.y;
+      sp[10] = xj[1] - xi[1]; sp[11] = xj[2] - xi[2]; sp[12] = xj[3] - xi[3];
+    }
+  }
+  __syncthreads();
+  double av[5] = {0, 0, 0, 0, 0}, ag[15];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) ag[k] = 0.0;
+  for (int k = lb + r2; k < le; k += L) {
+    const int e = lidx[k];
+    const int slot = e & 0x7fffffff;
+    const ushort2 lq = bl[e0 + slot];
+    const double* xi = Xn + 4 * lq.x;
+    const double* xj = Xn + 4 * lq.y;
+    const double dx0 = xj[1] - xi[1], dx1 = xj[2] - xi[2], dx2 = xj[3] - xi[3];
+    const double* es = Es + kEW * slot + (e < 0 ? 10 : 0);
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      const double gd = es[5 + c];
+      av[c] += es[c];
+      ag[c] += dx0 * gd;
+      ag[5 + c] += dx1 * gd;
+      ag[10 + c] += dx2 * gd;
+    }
+  }
+  for (int o = 1; o < L; o <<= 1) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) av[c] += __shfl_xor_sync(0xffffffffu, av[c], o);
+#pragma unroll
+    for (int c = 0; c < 15; ++c) ag[c] += __shfl_xor_sync(0xffffffffu, ag[c], o);
+  }
+  if (act2 && r2 == 0) {
+    const size_t n = (size_t)(n0 + t2);
+#pragma unroll
+    for (int c = 0; c < 5; ++c) gVp[5 * n + c] = av[c];
+#pragma unroll
+    for (int c = 0; c < 15; ++c) gGp[16 * n + c] = ag[c];
+    gGp[16 * n + 15] = 0.0;
+  }
+}
+
+// J^T of the stored operator, boundary rows: g_V[i] += (d F / d V)^T
+// (w_i / vol_i).
+__global__ void k_h2t_faces(int nbrow, const int* __restrict__ blist, const double* __restrict__ fj,
+                            const double* __restrict__ w, const double* __restrict__ vol, double* __restrict__ gV) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbrow) return;
+  const size_t i = (size_t)blist[b];
+  const double iv = 1.0 / vol[i];
+  double lm[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) lm[k] = w[5 * i + k] * iv;
+#pragma unroll
+  for (int d = 0; d < 5; ++d) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) s += fj[(size_t)(5 * k + d) * nbrow + b] * lm[k];
+    gV[5 * i + d] += s;
+  }
+}
+
+// Tangent records of the forward product: dP2[n] = (dV, X) with dV =
+// (dV/dU) dp at the linearisation state (VarFcnSGEuler.h:307-327), in the
+// blocked numbering.
+__global__ void k_h2_seed(int N, Gas g, const int* __restrict__ n2o, const double* __restrict__ U,
+                          const double* __restrict__ dp, const double* __restrict__ P2, double* __restrict__ dP2) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const size_t o = (size_t)n2o[n];
+  double u[5], du[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) { u[k] = U[5 * o + k]; du[k] = dp[5 * o + k]; }
+  const double ir = 1.0 / u[0];
+  const double a = u[1] * ir, b = u[2] * ir, cc = u[3] * ir;
+  double* d = dP2 + 8 * (size_t)n;
+  d[0] = du[0];
+  d[1] = (du[1] - a * du[0]) * ir;
+  d[2] = (du[2] - b * du[0]) * ir;
+  d[3] = (du[3] - cc * du[0]) * ir;
+  d[4] = g.gam1 * (0.5 * (a * a + b * b + cc * cc) * du[0] - a * du[1] - b * du[2] - cc * du[3] + du[4]);
+  const double* x = P2 + 8 * (size_t)n;
+  d[5] = x[5]; d[6] = x[6]; d[7] = x[7];
+}
+
+// J of the stored operator, edge part: k_fv_blocked's organisation with the
+// flux replaced by its stored linearisation.  Phase 0 stages the tangent
+// records and tangent gradients of the block's nodes and forward halo;
+// phase 1, thread per edge: dVij, dVji through the stored reconstruction
+// partials, dphi = (d phi / d Vij) dVij + (d phi / d Vji) dVji into shared
+// memory (and spill for block-crossing edges); phase 2 sums each node's
+// edges in edge order (+ first endpoint, - second) into part.
+__global__ void __launch_bounds__(512, 2) k_h2_blocked(int N, int E, int NB, int rec, const ushort2* __restrict__ bl,
+                                                       const int* __restrict__ beptr, const int* __restrict__ hfptr,
+                                                       const int* __restrict__ hfpad, int maxHf,
+                                                       const double* __restrict__ dP2, const double* __restrict__ dG2,
+                                                       const int* __restrict__ lptr, const int* __restrict__ lidx,
+                                                       const int* __restrict__ xslot, const double2* __restrict__ h2,
+                                                       double* __restrict__ part, double* __restrict__ spill) {
+  extern __shared__ double sm[];
+  const int blk = blockIdx.x;
+  const int n0 = blk * NB;
+  const int nn = min(NB, N - n0);
+  const int nh = hfptr[blk + 1] - hfptr[blk];
+  const int ns = nn + nh;
+  const int e0 = beptr[blk], e1 = beptr[blk + 1];
+  const size_t sE = (size_t)E;
+  const bool grad = rec != AEROF_REC_CONSTANT;
+  int L = 1;
+  while (2 * L * NB <= (int)blockDim.x) L *= 2;
+  const int t2 = threadIdx.x / L, r2 = threadIdx.x % L;
+  const bool act2 = t2 < nn && (int)threadIdx.x < L * NB;
+  const int lb = act2 ? lptr[n0 + t2] : 0, le = act2 ? lptr[n0 + t2 + 1] : 0;
+  double* Pn = sm;                      // [ns][kPS]
+  double* Gn = sm + kPS * ns;           // [ns][kGS]
+  double* Fs = sm + (kPS + kGS) * ns;   // [e1 - e0][5]
+  {
+    const int* hf = hfpad + (size_t)blk * maxHf;
+    const double2* ps = reinterpret_cast<const double2*>(dP2 + 8 * (size_t)n0);
+    const double2* gs = reinterpret_cast<const double2*>(dG2 + 16 * (size_t)n0);
+    double2* pd = reinterpret_cast<double2*>(Pn);
+    double2* gd = reinterpret_cast<double2*>(Gn);
+    for (int k = threadIdx.x; k < 4 * nn; k += blockDim.x) cp_async16(pd + (kPS / 2) * (k >> 2) + (k & 3), ps + k);
+    if (grad)
+      for (int k = threadIdx.x; k < 8 * nn; k += blockDim.x) cp_async16(gd + (kGS / 2) * (k >> 3) + (k & 7), gs + k);
+    for (int k = threadIdx.x; k < 4 * nh; k += blockDim.x) {
+      const int j = hf[k >> 2];
+      cp_async16(pd + (kPS / 2) * (nn + (k >> 2)) + (k & 3),
+                 reinterpret_cast<const double2*>(dP2 + 8 * (size_t)j) + (k & 3));
+    }
+    if (grad)
+      for (int k = threadIdx.x; k < 8 * nh; k += blockDim.x) {
+        const int j = hf[k >> 3];
+        cp_async16(gd + (kGS / 2) * (nn + (k >> 3)) + (k & 7),
+                   reinterpret_cast<const double2*>(dG2 + 16 * (size_t)j) + (k & 7));
+      }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  for (int q = e0 + threadIdx.x; q < e1; q += blockDim.x) {
+    const ushort2 lq = bl[q];
+    const double* pi = Pn + kPS * lq.x;
+    const double* pj = Pn + kPS * lq.y;
+    const double* gi = Gn + kGS * lq.x;
+    const double* gj = Gn + kGS * lq.y;
+    const double dx0 = pj[5] - pi[5], dx1 = pj[6] - pi[6], dx2 = pj[7] - pi[7];
+    double vl[5], vr[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      const double2 pp = h2[(size_t)(25 + c) * sE + q];
+      double a = (1.0 - pp.x) * pi[c] + pp.x * pj[c];
+      double b = pp.y * pi[c] + (1.0 - pp.y) * pj[c];
+      if (grad) {
+        const double2 qv = h2[(size_t)(30 + c) * sE + q];
+        const double ddij = dx0 * gi[c] + dx1 * gi[5 + c] + dx2 * gi[10 + c];
+        const double ddji = dx0 * gj[c] + dx1 * gj[5 + c] + dx2 * gj[10 + c];
+        a += qv.x * ddij;
+        b -= qv.y * ddji;
+      }
+      vl[c] = a;
+      vr[c] = b;
+    }
+    double* fs = Fs + 5 * (q - e0);
+    const int xs = xslot[q];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      double f = 0.0;
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        const double2 a = h2[(size_t)(5 * r + c) * sE + q];
+        f += a.x * vl[c] + a.y * vr[c];
+      }
+      fs[r] = f;
+      if (xs >= 0) spill[5 * (size_t)xs + r] = f;
+    }
+  }
+  __syncthreads();
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (int k = lb + r2; k < le; k += L) {
+    const int e = lidx[k];
+    const double* fs = Fs + 5 * (e & 0x7fffffff);
+    if (e < 0) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) acc[c] -= fs[c];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) acc[c] += fs[c];
+    }
+  }
+  for (int o = 1; o < L; o <<= 1) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+  }
+  if (act2 && r2 == 0) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) part[5 * (size_t)(n0 + t2) + c] = acc[c];
+  }
+}
+
+// J of the stored operator, per row (caller numbering): block sum minus the
+// spilled tangent fluxes of incoming block-crossing edges, plus the face
+// Jacobian times dV of a boundary row, times 1/ctrlVol.
+__global__ void k_h2_nodes(int N, const int* __restrict__ o2n, const double* __restrict__ part,
+                           const int* __restrict__ xin_ptr, const double* __restrict__ spill,
+                           const int* __restrict__ brow, int nbrow, const double* __restrict__ fj,
+                           const double* __restrict__ dP2, const double* __restrict__ vol, double* __restrict__ y) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= N) return;
+  const int n = o2n[o];
+  double acc[5];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) acc[c] = part[5 * (size_t)n + c];
+  for (int k = xin_ptr[n]; k < xin_ptr[n + 1]; ++k) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) acc[c] -= spill[5 * (size_t)k + c];
+  }
+  const int b = brow[o];
+  if (b >= 0) {
+    double dv[5];
+#pragma unroll
+    for (int d = 0; d < 5; ++d) dv[d] = dP2[8 * (size_t)n + d];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      double s = 0.0;
+#pragma unroll
+      for (int d = 0; d < 5; ++d) s += fj[(size_t)(5 * k + d) * nbrow + b] * dv[d];
+      acc[k] += s;
+    }
+  }
+  const double iv = 1.0 / vol[o];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) y[5 * (size_t)o + c] = acc[c] * iv;
+}
+
+static size_t h2t_smem(const DeviceMesh& m) {
+  return ((size_t)10 * (m.NB + m.maxHf) + (size_t)10 * m.maxE) * sizeof(double);
+}
+static size_t h2t_wide_smem(const DeviceMesh& m) {
+  return ((size_t)10 * (m.NB + m.maxHf) + (size_t)kEW * m.maxE) * sizeof(double);
+}
+static size_t h2f_smem(const DeviceMesh& m) {
+  return ((size_t)(kPS + kGS) * (m.NB + m.maxHf) + (size_t)5 * m.maxE) * sizeof(double);
+}
+
+// whether the stored operator's blocked kernels fit in shared memory
+static bool h2_fits(const DeviceMesh& m) {
+  return m.nblk > 0 && std::max(h2t_smem(m), h2f_smem(m)) <= 200 * 1024;
+}
+
+static double2* h2pairs(H2Op& h) { return reinterpret_cast<double2*>(h.a.p); }
+
+void h2_evaluate_dev(aerof_gpu_ctx* c, const double* dU) {
+  DeviceMesh& m = c->mesh;
+  H2Op& h = c->h2;
+  cudaStream_t s = c->stream;
+  const Gas g = make_gas(c->cfg.gamma);
+  if (!h2_fits(m))
+    throw ApiError{AEROF_ESTATE, "the stored operator needs the blocked organisation within 200 KB of shared memory"};
+  h.ready = false;
+  h.a.ensure((size_t)kH2Rec * std::max(m.E, 1));
+  h.fj.ensure((size_t)25 * std::max(m.nbrow, 1));
+  h.U.ensure(5 * (size_t)m.N);
+  AEROF_CUDA(cudaMemcpyAsync(h.U.p, dU, 5 * (size_t)m.N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  prim_dev(c, dU);
+  prim_grad_blocked_dev(c, dU, nullptr);
+  k_h2_edges<<<m.nblk, 128, 0, s>>>(m.N, m.E, m.NB, g, c->cfg.reconstruction, c->cfg.beta, m.bl.p, m.bnorm.p,
+                                     m.beptr.p, m.hfpad.p, m.maxHf, m.P2.p, c->s.G2.p, h2pairs(h));
+  AEROF_LAUNCH_CHECK();
+  if (m.nbrow) {
+    k_h2_faces<<<grid_for(m.nbrow, kAB), kAB, 0, s>>>(m.nbrow, m.F, g, m.Ubd.p, m.blist.p, m.nf_ptr.p, m.nf_face.p,
+                                                      m.fcode.p, m.fnrm.p, m.P.p, h.fj.p);
+    AEROF_LAUNCH_CHECK();
+  }
+  h.rec = c->cfg.reconstruction;
+  h.ready = true;
+}
+
+// y = J^T w with the stored operator (MatVecProdH2::applyTranspose)
+static void h2_vjp_dev(aerof_gpu_ctx* c, const double* dw, double* dout) {
+  DeviceMesh& m = c->mesh;
+  AdjWork& a = c->adj;
+  H2Op& h = c->h2;
+  cudaStream_t s = c->stream;
+  const Gas g = make_gas(c->cfg.gamma);
+  const int gn = grid_for(m.N, kAB);
+  a.lam2.ensure(6 * (size_t)m.N);
+  a.gVp.ensure(5 * (size_t)m.N);
+  a.gGp.ensure(16 * (size_t)m.N);
+  a.spill.ensure(13 * (size_t)std::max(m.nX, 1));
+  a.gV.ensure(5 * (size_t)m.N);
+  a.gG.ensure(16 * (size_t)m.N);
+  k_a_lam2<<<gn, kAB, 0, s>>>(m.N, m.n2o.p, dw, m.vol2.p, a.lam2.p);
+  AEROF_LAUNCH_CHECK();
+  // wide form when both endpoints' results fit in shared memory (tuning
+  // knob AEROF_H2T_WIDE=0 selects the compact form)
+  const char* wide_var = std::getenv("AEROF_H2T_WIDE");
+  const bool wide_env = !wide_var || std::atoi(wide_var) != 0;
+  const bool wide = wide_env && h2t_wide_smem(m) <= 220 * 1024;
+  const size_t smem = wide ? h2t_wide_smem(m) : h2t_smem(m);
+  auto kern = wide ? k_h2t_wide : k_h2t_blocked;
+  AEROF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<m.nblk, wide ? 1024 : 256, smem, s>>>(m.N, m.E, m.NB, m.bl.p, m.beptr.p, m.hfptr.p, m.hfpad.p, m.maxHf,
+                                               m.P2.p, a.lam2.p, m.lptr.p, m.lidx.p, m.xslot.p, h2pairs(h), a.gVp.p,
+                                               a.gGp.p, a.spill.p);
+  AEROF_LAUNCH_CHECK();
+  k_a_fv_nodes<<<gn, kAB, 0, s>>>(m.N, m.n2o.p, a.gVp.p, a.gGp.p, m.xin_ptr.p, a.spill.p, a.gV.p, a.gG.p);
+  AEROF_LAUNCH_CHECK();
+  if (m.nbrow) {
+    k_h2t_faces<<<grid_for(m.nbrow, kAB), kAB, 0, s>>>(m.nbrow, m.blist.p, h.fj.p, dw, m.vol.p, a.gV.p);
+    AEROF_LAUNCH_CHECK();
+  }
+  k_a_lsq_prim<<<grid_for(4 * (size_t)m.N, kAB), kAB, 0, s>>>(m.N, g, h.rec, h.U.p, m.P.p, m.lsqW.p, m.nbr_ptr.p,
+                                                              m.nbr_node.p, a.gV.p, a.gG.p, dout);
+  AEROF_LAUNCH_CHECK();
+}
+
+// y = J p with the stored operator (MatVecProdH2::apply)
+static void h2_jvp_dev(aerof_gpu_ctx* c, const double* dp, double* dout) {
+  DeviceMesh& m = c->mesh;
+  H2Op& h = c->h2;
+  cudaStream_t s = c->stream;
+  const Gas g = make_gas(c->cfg.gamma);
+  const int gn = grid_for(m.N, kAB);
+  h.dP2.ensure(8 * (size_t)m.N);
+  h.dG2.ensure(16 * (size_t)m.N);
+  h.part.ensure(5 * (size_t)m.N);
+  h.spill.ensure(5 * (size_t)std::max(m.nX, 1));
+  k_h2_seed<<<gn, kAB, 0, s>>>(m.N, g, m.n2o.p, h.U.p, dp, m.P2.p, h.dP2.p);
+  AEROF_LAUNCH_CHECK();
+  if (h.rec != AEROF_REC_CONSTANT) grad_records_blocked_dev(c, h.dP2.p, h.dG2.p);
+  const size_t smem = h2f_smem(m);
+  AEROF_CUDA(cudaFuncSetAttribute(k_h2_blocked, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_h2_blocked<<<m.nblk, 512, smem, s>>>(m.N, m.E, m.NB, h.rec, m.bl.p, m.beptr.p, m.hfptr.p, m.hfpad.p, m.maxHf,
+                                         h.dP2.p, h.dG2.p, m.lptr.p, m.lidx.p, m.xslot.p, h2pairs(h), h.part.p,
+                                         h.spill.p);
+  AEROF_LAUNCH_CHECK();
+  k_h2_nodes<<<gn, kAB, 0, s>>>(m.N, m.o2n.p, h.part.p, m.xin_ptr.p, h.spill.p, m.brow.p, m.nbrow, h.fj.p, h.dP2.p,
+                                m.vol.p, dout);
+  AEROF_LAUNCH_CHECK();
+}
+
+static void h2_apply_dev(aerof_gpu_ctx* c, const double* p, double* y, bool trans) {
+  if (trans) h2_vjp_dev(c, p, y);
+  else h2_jvp_dev(c, p, y);
+}
+
+void exact_product(aerof_gpu_ctx* c, const double* dU, const double* p, double* y, bool trans) {
+  if (c->h2.use && c->h2.ready) {
+    h2_apply_dev(c, p, y, trans);
+    return;
+  }
+  if (trans) vjp_dev(c, dU, p, y);
+  else residual_forward(c, dU, p, nullptr, y, false);
+}
+
 }  // namespace aerof
 
 // ====================================================================== C ABI
@@ -1194,6 +1881,63 @@ extern "C" int aerof_gpu_dRdX_T(aerof_gpu_ctx* c, const double* U, const double*
     double* dg = out_dev(c, gX, 3 * N, c->s.Xstage);
     dRdX_T_dev(c, dU, dl, dg);
     out_finish(c, gX, dg, 3 * N);
+    return AEROF_OK;
+  });
+}
+
+// MatVecProdH2::evaluate (MatVecProd.C:1498-1520): the exact linearisation
+// at U stored in device memory.
+extern "C" int aerof_gpu_h2_evaluate(aerof_gpu_ctx* c, const double* U) {
+  return guard(c, [&]() -> int {
+    if (int e = need(c)) return e;
+    if (!U) return AEROF_EINVAL;
+    const double* dU = in_dev(c, U, 5 * (size_t)c->mesh.N, c->s.Ustage);
+    h2_evaluate_dev(c, dU);
+    AEROF_CUDA(cudaStreamSynchronize(c->stream));
+    return AEROF_OK;
+  });
+}
+
+// MatVecProdH2::apply / applyTranspose (MatVecProd.C:1622-1704) with the
+// stored operator.
+extern "C" int aerof_gpu_h2_apply(aerof_gpu_ctx* c, const double* p, double* y, int transpose) {
+  return guard(c, [&]() -> int {
+    if (int e = need(c)) return e;
+    if (!p || !y) return AEROF_EINVAL;
+    if (!c->h2.ready) {
+      c->last_error = "no stored operator: call aerof_gpu_h2_evaluate first";
+      return AEROF_ESTATE;
+    }
+    const size_t n = 5 * (size_t)c->mesh.N;
+    const double* dp = in_dev(c, p, n, c->s.Vstage);
+    double* dy = out_dev(c, y, n, c->s.Rstage);
+    h2_apply_dev(c, dp, dy, transpose != 0);
+    out_finish(c, y, dy, n);
+    return AEROF_OK;
+  });
+}
+
+extern "C" int aerof_gpu_h2_release(aerof_gpu_ctx* c) {
+  return guard(c, [&]() -> int {
+    AEROF_CUDA(cudaStreamSynchronize(c->stream));
+    H2Op& h = c->h2;
+    h.ready = false;
+    h.use = false;
+    h.a.release();
+    h.fj.release();
+    h.U.release();
+    h.dP2.release();
+    h.dG2.release();
+    h.part.release();
+    h.spill.release();
+    return AEROF_OK;
+  });
+}
+
+extern "C" int aerof_gpu_set_exact_operator(aerof_gpu_ctx* c, int stored) {
+  return guard(c, [&]() -> int {
+    if (stored != 0 && stored != 1) return AEROF_EINVAL;
+    c->h2.in_solves = stored == 1;
     return AEROF_OK;
   });
 }

@@ -209,6 +209,29 @@ struct AdjWork {
   DBuf<double> tg;         // [T][12] per-tet vertex coordinate cotangents
 };
 
+// Stored exact linearisation of the residual (the operator MatVecProdH2
+// holds between evaluate and apply).  Per edge of the blocked organisation,
+// kH2Rec doubles as 16-byte pairs, SoA by pair ([kH2Rec / 2][E] double2):
+// (d phi_r / d Vij_c, d phi_r / d Vji_c) for r, c < 5, then (p1_c, p2_c)
+// and (q1_c, q2_c), the partials of the reconstruction:
+// dVij = (1-p1) dVi + p1 dVj + q1 dddij, dVji = p2 dVi + (1-p2) dVj -
+// q2 dddji.  Per boundary row, SoA [25][nbrow]: the summed face-flux
+// Jacobian d F / d V of its faces.
+constexpr int kH2Rec = 70;
+struct H2Op {
+  bool ready = false;      // evaluated for the current mesh and coordinates
+  bool use = false;        // exact products of linearised solves read it
+  bool in_solves = false;  // linearised solves evaluate and use it
+  int rec = 0;             // reconstruction it was evaluated with
+  DBuf<double> a;          // [kH2Rec / 2][E] pairs
+  DBuf<double> fj;         // [25][nbrow]
+  DBuf<double> U;          // [N][5] state of the linearisation
+  DBuf<double> dP2;        // [N][8] tangent records (dV, X), blocked numbering
+  DBuf<double> dG2;        // [N][16] tangent gradients, blocked numbering
+  DBuf<double> part;       // [N][5] block-local tangent flux sums
+  DBuf<double> spill;      // [nX][5] tangent fluxes of block-crossing edges
+};
+
 // CUDA-event timers per category (AEROF_T_*), recorded without host sync.
 struct Timers {
   bool on = false;
@@ -236,6 +259,7 @@ struct aerof_gpu_ctx {
   aerof::Implicit imp;
   aerof::DualWork dual;
   aerof::AdjWork adj;
+  aerof::H2Op h2;
   aerof::Timers timers;
   std::string last_error;
 };
@@ -310,6 +334,7 @@ __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wa
 int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync = true);
 void prim_dev(aerof_gpu_ctx* c, const double* dU);
 void prim_grad_blocked_dev(aerof_gpu_ctx* c, const double* dU, const int* tag);
+void grad_records_blocked_dev(aerof_gpu_ctx* c, const double* P2src, double* G2dst);
 void gradients_dev(aerof_gpu_ctx* c);
 void timestep_dev(aerof_gpu_ctx* c, const double* dU, double cfl, double* ddt);
 double norm2_dev(aerof_gpu_ctx* c, const double* x, size_t n);
@@ -319,6 +344,11 @@ double dot_dev(aerof_gpu_ctx* c, const double* x, const double* y, size_t n);
 int residual_forward(aerof_gpu_ctx* c, const double* dU, const double* dv, const double* dXdot, double* ddR,
                      bool sync = true);
 void vjp_dev(aerof_gpu_ctx* c, const double* dU, const double* dw, double* dout);
+// exact product of the linearised solves: the stored operator when h2.use,
+// else the matrix-free sweeps at dU
+void exact_product(aerof_gpu_ctx* c, const double* dU, const double* p, double* y, bool trans);
+// the stored operator at dU (h2.ready on return)
+void h2_evaluate_dev(aerof_gpu_ctx* c, const double* dU);
 // implemented in mesh.cu: recompute the geometry for new coordinates
 void compute_geometry(aerof_gpu_ctx* c);
 

@@ -624,10 +624,7 @@ static int gmres_t(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int
   auto op = [&](const TV* p, TV* y) {
     if (!exactU) { matvec_t<TV, TV>(c, p, y, trans); return; }
     TimerScope t(c, AEROF_T_KSP_MATVEC);
-    const double* pd = reinterpret_cast<const double*>(p);
-    double* yy = reinterpret_cast<double*>(y);
-    if (trans) vjp_dev(c, exactU, pd, yy);
-    else residual_forward(c, exactU, pd, nullptr, yy, false);
+    exact_product(c, exactU, reinterpret_cast<const double*>(p), reinterpret_cast<double*>(y), trans);
   };
   auto norm2 = [&](TV* v) -> double {
     k_mgs<TV, true><<<kGB, kIB, 0, s>>>(n, nullptr, nullptr, nullptr, v, part, ticket, hd);
@@ -760,8 +757,7 @@ static int fgmres_exact(aerof_gpu_ctx* c, const double* b, double* x, int numVec
   AEROF_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), s));
   auto op = [&](const double* p, double* y) {
     TimerScope t(c, AEROF_T_KSP_MATVEC);
-    if (trans) vjp_dev(c, exactU, p, y);
-    else residual_forward(c, exactU, p, nullptr, y, false);
+    exact_product(c, exactU, p, y, trans);
   };
   auto norm2 = [&](double* v) -> double {
     k_mgs<double, true><<<kGB, kIB, 0, s>>>(n, nullptr, nullptr, nullptr, v, part, ticket, hd);
@@ -1086,6 +1082,16 @@ extern "C" int aerof_gpu_linearized_solve(aerof_gpu_ctx* c, const double* U, con
     const double* dU = c->imp.t.p;
     const double* db = in_dev(c, b, n, c->s.Vstage);
     double* dx = out_dev(c, x, n, c->s.Rstage);
+    // with the stored operator selected, the exact linearisation at U is
+    // evaluated once and every exact product of the solve reads it
+    struct UseStored {
+      H2Op& h;
+      ~UseStored() { h.use = false; }
+    } use_stored{c->h2};
+    if (c->h2.in_solves) {
+      h2_evaluate_dev(c, dU);
+      c->h2.use = true;
+    }
     jacobian_dev(c, dU, nullptr, inner_its ? AEROF_PREC_FP32 : AEROF_PREC_FP64, inner_its && transpose);
     if (int nb = prec_setup_dev(c)) {
       c->last_error = std::to_string(nb) + " singular diagonal block(s)";

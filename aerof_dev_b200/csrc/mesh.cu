@@ -449,6 +449,7 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
     c->has_mesh = false;
     c->imp.precision = 0;
     c->imp.prec_ready = false;
+    c->h2.ready = false;
     HostMesh h;
     int E = 0;
     build_host(N, T, F, tets, faces, h, E);
@@ -581,6 +582,7 @@ extern "C" int aerof_gpu_update_coordinates(aerof_gpu_ctx* c, const double* X) {
     c->dual.geom_static = false;
     c->imp.precision = 0;
     c->imp.prec_ready = false;
+    c->h2.ready = false;
     AEROF_CUDA(cudaStreamSynchronize(c->stream));
     return AEROF_OK;
   });

@@ -846,12 +846,16 @@ static GradStage grad_stage(const DeviceMesh& m) {
   return st;
 }
 
-// persistent pipelined gradients (k_prim_blocked writes P2 first)
+// persistent pipelined gradients of the records P2src (with dU,
+// k_prim_blocked writes the mesh's P2 first and P2src is that)
 static void launch_grad_pipe(aerof_gpu_ctx* c, const Gas& g, const double* dU, const int* tag, double* G2,
-                             cudaStream_t s) {
+                             cudaStream_t s, const double* P2src = nullptr) {
   const DeviceMesh& m = c->mesh;
-  k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
-  AEROF_LAUNCH_CHECK();
+  if (dU) {
+    k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
+    AEROF_LAUNCH_CHECK();
+  }
+  if (!P2src) P2src = m.P2.p;
   const GradStage st = grad_stage(m);
   const size_t smem = (size_t)2 * st.size * sizeof(double);
   const int L = kBlock / m.NB;
@@ -862,7 +866,7 @@ static void launch_grad_pipe(aerof_gpu_ctx* c, const Gas& g, const double* dU, c
     int sms = 0;
     AEROF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
     const int grid = std::max(1, std::min(m.nblk, std::max(per_sm, 1) * sms));
-    kern<<<grid, kBlock, smem, s>>>(m.N, m.NB, m.nblk, m.maxH, m.maxLp, st, m.P2.p, m.W2.p, m.nb2_ptr.p, m.lpad.p,
+    kern<<<grid, kBlock, smem, s>>>(m.N, m.NB, m.nblk, m.maxH, m.maxLp, st, P2src, m.W2.p, m.nb2_ptr.p, m.lpad.p,
                                     m.hpad.p, tag, G2);
     AEROF_LAUNCH_CHECK();
   };
@@ -925,6 +929,23 @@ void prim_grad_blocked_dev(aerof_gpu_ctx* c, const double* dU, const int* tag) {
     AEROF_LAUNCH_CHECK();
     k_grad<<<grid_for(4 * (size_t)m.N, kBlock), kBlock, 0, s>>>(m.N, m.P2.p, m.W2.p, m.nb2_ptr.p, m.nb2_node.p, tag,
                                                                 c->s.G2.p);
+    AEROF_LAUNCH_CHECK();
+  }
+}
+
+// Least-squares gradients G2dst of the records P2src ([N][8] = (V, X),
+// blocked numbering): the linear map the residual applies to V, here for
+// tangent records.
+void grad_records_blocked_dev(aerof_gpu_ctx* c, const double* P2src, double* G2dst) {
+  const DeviceMesh& m = c->mesh;
+  const Gas g = make_gas(c->cfg.gamma);
+  cudaStream_t s = c->stream;
+  const bool piped = grad_kernel_choice() == 3 && m.maxH <= 512 && 2 * grad_stage(m).size * sizeof(double) <= kMaxStagedSmem;
+  if (piped) {
+    launch_grad_pipe(c, g, nullptr, nullptr, G2dst, s, P2src);
+  } else {
+    k_grad<<<grid_for(4 * (size_t)m.N, kBlock), kBlock, 0, s>>>(m.N, P2src, m.W2.p, m.nb2_ptr.p, m.nb2_node.p, nullptr,
+                                                                G2dst);
     AEROF_LAUNCH_CHECK();
   }
 }

@@ -108,13 +108,22 @@ def converge(ctx, U, precision=32, tol=1e-10, max_steps=2000, exact_steps=3, kry
     return U, info
 
 
-def adjoint_gradient(ctx, U, X, functional: ZForce, modes, eps=1e-10, krylov=30, maxits=2000, inner_its=20):
-    """dJ/ds_k for every mode by the adjoint method."""
+def adjoint_gradient(ctx, U, X, functional: ZForce, modes, eps=1e-10, krylov=30, maxits=2000, inner_its=20,
+                     stored_operator=False):
+    """dJ/ds_k for every mode by the adjoint method.  stored_operator: the
+    adjoint solve applies the stored exact linearisation (evaluated once)
+    instead of re-evaluating it per product."""
     import aerof_dev_b200 as A
     S = A.Sensitivity(ctx)
     U = _host(U)
     gU = functional.dU(U, X)
-    lam, its, res = S.solve(U, gU, transpose=True, krylov=krylov, maxits=maxits, eps=eps, inner_its=inner_its)
+    S.set_exact_operator(stored_operator)
+    try:
+        lam, its, res = S.solve(U, gU, transpose=True, krylov=krylov, maxits=maxits, eps=eps, inner_its=inner_its)
+    finally:
+        S.set_exact_operator(False)
+        if stored_operator:
+            S.h2_release()
     gX = functional.dX(U, X) - S.dRdX_T(U, lam)
     return np.einsum("kni,ni->k", modes, gX), {"adjoint_its": its, "adjoint_res": res}
 

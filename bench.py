@@ -389,9 +389,16 @@ def run_adjoint(args):
     t_dxt = timed(lambda: sens.dRdX_T(U, lam))
     t_jvp = timed(lambda: sens.jvp(U, lam))
     t_both = timed(lambda: sens.adjoint_products(U, lam))
+    sens.h2_evaluate(U)
+    t_h2t = timed(lambda: sens.h2_apply(lam, transpose=True))
+    t_h2 = timed(lambda: sens.h2_apply(lam))
+    sens.h2_release()
     t1 = time.perf_counter()
     ga, ainfo = S.adjoint_gradient(ctx, U, X, F, modes)
     adj_s = time.perf_counter() - t1
+    t1 = time.perf_counter()
+    gs, sinfo = S.adjoint_gradient(ctx, U, X, F, modes, stored_operator=True)
+    adj_stored_s = time.perf_counter() - t1
     nfd = min(args.fd_modes, args.modes)
     gr = S.fd_gradient(ctx, Uh, X, F, modes[:nfd], h=(2e-4, 1e-4), tol=1e-10, max_steps=args.max_steps)
     g6 = S.fd_gradient(ctx, Uh, X, F, modes[:nfd], h=1e-6, tol=1e-10, max_steps=args.max_steps)
@@ -402,8 +409,12 @@ def run_adjoint(args):
             "config": {"workload": f"adjoint z-force sensitivities, {args.n}^3 jittered mesh with a base bump, "
                                    f"{args.modes} Gaussian-bump modes, Mach 0.8",
                        "reconstruction": {1: "constant", 2: "van Albada", 3: "linear"}[args.rec], "N": N},
-            "ms": {"residual": t_res, "vjp": t_vjp, "dRdX_T": t_dxt, "jvp": t_jvp, "adjoint_products": t_both},
+            "ms": {"residual": t_res, "vjp": t_vjp, "dRdX_T": t_dxt, "jvp": t_jvp, "adjoint_products": t_both,
+                   "h2_vjp": t_h2t, "h2_jvp": t_h2},
+            "h2_vjp_over_residual": t_h2t / t_res,
             "converge_s": conv_s, "adjoint_gradient_s": adj_s, "adjoint": ainfo,
+            "adjoint_gradient_stored_operator_s": adj_stored_s, "adjoint_stored_operator": sinfo,
+            "stored_vs_matrix_free_grad_max_rel": float(np.abs(gs - ga).max() / np.abs(ga).max()),
             "J": F.value(Uh, X), "grad": ga.tolist(),
             "fd_richardson": gr.tolist(), "fd_step_1e-6": g6.tolist(),
             "max_rel_err_vs_richardson": float(np.abs(ga[:nfd] - gr).max() / np.abs(gr).max()),
@@ -431,24 +442,32 @@ def run_adjoint_products(args):
     sp, S = A.SpaceOperator(ctx), A.Sensitivity(ctx)
     R = torch.empty_like(U)
     out = {}
-    for name, fn in (("residual", lambda: sp.computeResidual(U, R)), ("jvp", lambda: S.jvp(U, lam)),
-                     ("vjp", lambda: S.vjp(U, lam)), ("dRdX_T", lambda: S.dRdX_T(U, lam)),
-                     ("adjoint_products", lambda: S.adjoint_products(U, lam))):
+    calls = (("residual", lambda: sp.computeResidual(U, R)), ("jvp", lambda: S.jvp(U, lam)),
+             ("vjp", lambda: S.vjp(U, lam)), ("dRdX_T", lambda: S.dRdX_T(U, lam)),
+             ("adjoint_products", lambda: S.adjoint_products(U, lam)),
+             # the stored operator (MatVecProdH2): one evaluation, then products
+             ("h2_evaluate", lambda: S.h2_evaluate(U)), ("h2_vjp", lambda: S.h2_apply(lam, transpose=True)),
+             ("h2_jvp", lambda: S.h2_apply(lam)))
+    for name, fn in calls:
+        reps = 3 if name == "h2_evaluate" else 10
         for _ in range(3):
             fn()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(10):
+        for _ in range(reps):
             fn()
         e1.record()
         torch.cuda.synchronize()
-        out[name] = e0.elapsed_time(e1) / 10
+        out[name] = e0.elapsed_time(e1) / reps
+    S.h2_release()
     s = W.lattice_sizes(args.n)
     line = {"metric": METRIC, "workload": "adjoint_products", "value": out["adjoint_products"] / out["residual"],
             "unit": "x one primal residual (J^T lambda and dR/dX^T lambda, one reverse sweep)",
             "higher_is_better": False, "ms": out,
+            "h2_vjp_over_residual": out["h2_vjp"] / out["residual"],
+            "h2_jvp_over_residual": out["h2_jvp"] / out["residual"],
             "config": {"workload": f"{args.n}^3 jittered Kuhn tet mesh N={s['N']} E={s['E']}, smooth Mach 0.8 state",
                        "reconstruction": {1: "constant", 2: "van Albada", 3: "linear"}[args.rec]}}
     print(json.dumps(line), flush=True)

@@ -255,6 +255,27 @@ int aerof_gpu_dRdX_T(aerof_gpu_ctx* ctx, const double* U, const double* lambda, 
 int aerof_gpu_adjoint_products(aerof_gpu_ctx* ctx, const double* U, const double* lambda, double* JTl,
                                double* gX);
 
+/* Stored exact linearisation (MatVecProdH2, MatVecProd.C:1462-1704).
+ * evaluate (MatVecProd.C:1498-1520; SubDomain::precomputeRec
+ * SubDomain.C:3836-3865 and computeH2): linearises the residual at U and
+ * keeps, per edge, the flux Jacobians with respect to both reconstructed
+ * states and the partials of the reconstruction, and per boundary node the
+ * face-flux Jacobian: 560 bytes per edge + 200 per boundary node + 40 per
+ * node of device memory.  apply (transpose = 0: y = J p) and
+ * applyTranspose (transpose = 1: y = J^T p) (MatVecProd.C:1622-1704;
+ * SubDomain::computeMatVecProdH2, SubDomain.C:4076-4190) read it; the
+ * results equal aerof_gpu_jvp / aerof_gpu_vjp at U within rounding.  The
+ * operator stays valid until the mesh or its coordinates change.         */
+int aerof_gpu_h2_evaluate(aerof_gpu_ctx* ctx, const double* U);
+int aerof_gpu_h2_apply(aerof_gpu_ctx* ctx, const double* p, double* y, int transpose);
+/* Frees the stored operator's device memory.                              */
+int aerof_gpu_h2_release(aerof_gpu_ctx* ctx);
+/* Exact products of aerof_gpu_linearized_solve: stored = 0 (default)
+ * re-evaluates the linearisation per product (no operator storage);
+ * stored = 1 evaluates the stored operator at U once per solve and applies
+ * it to every Krylov vector (the reference's MatVecProdH2 path).          */
+int aerof_gpu_set_exact_operator(aerof_gpu_ctx* ctx, int stored);
+
 /* Linearised steady solves with the exact Jacobian applied matrix-free
  * (fsoLinearSolver / fsoAdjointLinearSolver, FluidShapeOptimizationHandler.C:
  * 1557-1624; GmresSolver::solve / solveT): transpose = 0 solves J x = b,

@@ -691,10 +691,226 @@ __global__ void k_a_faces(int N, int F, Gas g, const double* __restrict__ Ub0, c
   for (int k = 0; k < 5; ++k) gV[5 * (size_t)i + k] = gv[k];
 }
 
+// Per node in the blocked numbering: in-block sums + the spilled parts of
+// the incoming block-crossing edges (+ the boundary faces from the stored
+// face Jacobians fj when given: g_V += (d F / d V)^T w / vol), kept in the
+// blocked numbering for k_a_lsq_blocked.
+__global__ void k_a_nodes_b(int N, const int* __restrict__ n2o, const double* __restrict__ gVp,
+                            const double* __restrict__ gGp, const int* __restrict__ xin_ptr,
+                            const double* __restrict__ spill, const int* __restrict__ brow, int nbrow,
+                            const double* __restrict__ fj, const double* __restrict__ w,
+                            const double* __restrict__ vol, double* __restrict__ gV2, double* __restrict__ gG2) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double av[5], ag[15];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) av[c] = gVp[5 * (size_t)n + c];
+#pragma unroll
+  for (int c = 0; c < 15; ++c) ag[c] = gGp[16 * (size_t)n + c];
+  for (int k = xin_ptr[n]; k < xin_ptr[n + 1]; ++k) {
+    const double* sp = spill + 13 * (size_t)k;
+    const double dx0 = sp[10], dx1 = sp[11], dx2 = sp[12];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      av[c] += sp[c];
+      ag[c] += dx0 * sp[5 + c];
+      ag[5 + c] += dx1 * sp[5 + c];
+      ag[10 + c] += dx2 * sp[5 + c];
+    }
+  }
+  const size_t o = (size_t)n2o[n];
+  if (fj) {
+    const int b = brow[o];
+    if (b >= 0) {
+      const double iv = 1.0 / vol[o];
+      double lm[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) lm[k] = w[5 * o + k] * iv;
+#pragma unroll
+      for (int d = 0; d < 5; ++d) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) s += fj[(size_t)(5 * k + d) * nbrow + b] * lm[k];
+        av[d] += s;
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 5; ++c) gV2[5 * (size_t)n + c] = av[c];
+  double2* gg = reinterpret_cast<double2*>(gG2 + 16 * (size_t)n);
+#pragma unroll
+  for (int c = 0; c < 7; ++c) gg[c] = make_double2(ag[2 * c], ag[2 * c + 1]);
+  gg[7] = make_double2(ag[14], 0.0);
+}
+
+// Boundary rows (blocked numbering of gV2): g_V += (d F / d V)^T w / vol
+// by forward mode per face, in face order (as k_a_faces).
+__global__ void k_a_faces_b(int nbrow, int F, Gas g, const double* __restrict__ Ub0, const int* __restrict__ blist,
+                            const int* __restrict__ o2n, const int* __restrict__ nf_ptr,
+                            const int* __restrict__ nf_face, const int* __restrict__ fcode,
+                            const double* __restrict__ fn, const double* __restrict__ P,
+                            const double* __restrict__ w, const double* __restrict__ vol, double* __restrict__ gV2) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbrow) return;
+  const size_t i = (size_t)blist[b];
+  const size_t n = (size_t)o2n[i];
+  double V[5], Ub[5], lm[5], gv[5];
+  const double iv = 1.0 / vol[i];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    V[k] = P[8 * i + k];
+    Ub[k] = Ub0[k];
+    lm[k] = w[5 * i + k] * iv;
+    gv[k] = gV2[5 * n + k];
+  }
+  const double third = 1.0 / 3.0;
+  for (int q = nf_ptr[i]; q < nf_ptr[i + 1]; ++q) {
+    const int f = nf_face[q];
+    face_vjp_V(g, fcode[f], third * fn[f], third * fn[(size_t)F + f], third * fn[2 * (size_t)F + f], V, Ub, lm, gv);
+  }
+#pragma unroll
+  for (int k = 0; k < 5; ++k) gV2[5 * n + k] = gv[k];
+}
+
+// Transpose of the least-squares gradients and of V(U) in the blocked
+// numbering (same sums as k_a_lsq_prim): CTA per Morton block; the node
+// coordinates, LSQ constants and gradient cotangents of the block's nodes
+// and of its halo (all neighbours outside the block) are staged in shared
+// memory (26-double records: V4 x y z | 6 constants | 16 cotangents), then
+// L lanes per node take its neighbours r, r + L, ...:
+// g_V_q += sum_i W_i(x_q - x_i) . g_grad_i - (sum_i W_q(x_i - x_q)) . g_grad_q,
+// fixed xor-tree lane sum, (dV/dU)^T, written in the caller's numbering.
+constexpr int kLR = 26;
+template <int L>
+__global__ void __launch_bounds__(256, 2) k_a_lsq_blocked(int N, int NB, Gas g, int rec, const int* __restrict__ n2o,
+                                                          const double* __restrict__ U, const double* __restrict__ P2,
+                                                          const double* __restrict__ W2,
+                                                          const int* __restrict__ nb2_ptr,
+                                                          const unsigned short* __restrict__ lnb,
+                                                          const int* __restrict__ hptr, const int* __restrict__ hnode,
+                                                          const double* __restrict__ gV2,
+                                                          const double* __restrict__ gG2, double* __restrict__ out) {
+  extern __shared__ double sm[];
+  const int blk = blockIdx.x;
+  const int n0 = blk * NB;
+  const int nn = min(NB, N - n0);
+  const int h0 = hptr[blk], nh = hptr[blk + 1] - h0;
+  const int ns = nn + nh;
+  const int c0 = nb2_ptr[n0], nc = nb2_ptr[n0 + nn] - c0;
+  const bool grad = rec != AEROF_REC_CONSTANT;
+  double* rs = sm;                                                                       // [ns][kLR]
+  unsigned short* ls = reinterpret_cast<unsigned short*>(rs + kLR * (size_t)ns);         // [nc]
+  const int t = threadIdx.x / L, r = threadIdx.x % L;
+  const bool act = t < nn;
+  if (grad) {
+    for (int k = threadIdx.x; k < nc; k += blockDim.x) ls[k] = lnb[c0 + k];
+    double2* rd = reinterpret_cast<double2*>(rs);
+    for (int k = threadIdx.x; k < 2 * ns; k += blockDim.x) {
+      const int q = k >> 1;
+      const int j = q < nn ? n0 + q : hnode[h0 + q - nn];
+      cp_async16(rd + (kLR / 2) * q + (k & 1), reinterpret_cast<const double2*>(P2 + 8 * (size_t)j) + 2 + (k & 1));
+    }
+    for (int k = threadIdx.x; k < 8 * ns; k += blockDim.x) {
+      const int q = k >> 3;
+      const int j = q < nn ? n0 + q : hnode[h0 + q - nn];
+      cp_async16(rd + (kLR / 2) * q + 5 + (k & 7), reinterpret_cast<const double2*>(gG2 + 16 * (size_t)j) + (k & 7));
+    }
+    for (int k = threadIdx.x; k < 6 * ns; k += blockDim.x) {
+      const int q = k / 6, a = k % 6;
+      const int j = q < nn ? n0 + q : hnode[h0 + q - nn];
+      cp_async8(rs + kLR * q + 4 + a, W2 + (size_t)a * N + j);
+    }
+    cp_async_wait_all();
+  }
+  __syncthreads();
+  double gv[5] = {0, 0, 0, 0, 0};
+  double ws0 = 0.0, ws1 = 0.0, ws2 = 0.0;
+  if (act && grad) {
+    const double* pq = rs + kLR * t;
+    const int pb = nb2_ptr[n0 + t] - c0, pe = nb2_ptr[n0 + t + 1] - c0;
+#pragma unroll 1
+    for (int p = pb + r; p < pe; p += L) {
+      const double* pi = rs + kLR * (int)ls[p];
+      double W0, W1, W2_;
+      lsq_weights(pi + 4, pq[1] - pi[1], pq[2] - pi[2], pq[3] - pi[3], W0, W1, W2_);
+      const double* gi = pi + 10;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) gv[k] += W0 * gi[k] + W1 * gi[5 + k] + W2_ * gi[10 + k];
+      double V0, V1, V2;
+      lsq_weights(pq + 4, pi[1] - pq[1], pi[2] - pq[2], pi[3] - pq[3], V0, V1, V2);
+      ws0 += V0; ws1 += V1; ws2 += V2;
+    }
+  }
+#pragma unroll
+  for (int o = 1; o < L; o <<= 1) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) gv[k] += __shfl_xor_sync(0xffffffffu, gv[k], o);
+    ws0 += __shfl_xor_sync(0xffffffffu, ws0, o);
+    ws1 += __shfl_xor_sync(0xffffffffu, ws1, o);
+    ws2 += __shfl_xor_sync(0xffffffffu, ws2, o);
+  }
+  if (!act || r != 0) return;
+  const size_t n = (size_t)(n0 + t);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) gv[k] += gV2[5 * n + k];
+  if (grad) {
+    const double* gq = rs + kLR * t + 10;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) gv[k] -= ws0 * gq[k] + ws1 * gq[5 + k] + ws2 * gq[10 + k];
+  }
+  const size_t o = (size_t)n2o[n];
+  double u[5], gu[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) u[k] = U[5 * o + k];
+  prim_adj(g, u, gv, gu);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) out[5 * o + k] = gu[k];
+}
+
+static size_t lsq_blocked_smem(const DeviceMesh& m) {
+  return ((size_t)8 * kLR * (m.NB + m.maxH) + (size_t)2 * m.maxL + 15) / 16 * 16;
+}
+
+// After a blocked edge sweep (gVp, gGp, spill current): node assembly with
+// the faces, the LSQ transpose and (dV/dU)^T at dU into dout, all in the
+// blocked organisation.  fj: stored face Jacobians, or null for forward mode
+// per face (needs P at dU).  False (nothing launched) when the staging does
+// not fit in shared memory.
+static bool assemble_lsq_blocked(aerof_gpu_ctx* c, const double* dU, const double* dw, const double* fj, int rec,
+                                 double* dout) {
+  DeviceMesh& m = c->mesh;
+  AdjWork& a = c->adj;
+  cudaStream_t s = c->stream;
+  const Gas g = make_gas(c->cfg.gamma);
+  const size_t smem = lsq_blocked_smem(m);
+  const int L = kAB / m.NB;
+  if (smem > 200 * 1024 || L < 1 || L > 4 || L * m.NB != kAB) return false;
+  a.gV2.ensure(5 * (size_t)m.N);
+  a.gG2.ensure(16 * (size_t)m.N);
+  k_a_nodes_b<<<grid_for(m.N, kAB), kAB, 0, s>>>(m.N, m.n2o.p, a.gVp.p, a.gGp.p, m.xin_ptr.p, a.spill.p, m.brow.p,
+                                                 m.nbrow, fj, dw, m.vol.p, a.gV2.p, a.gG2.p);
+  AEROF_LAUNCH_CHECK();
+  if (!fj && m.nbrow) {
+    k_a_faces_b<<<grid_for(m.nbrow, kAB), kAB, 0, s>>>(m.nbrow, m.F, g, m.Ubd.p, m.blist.p, m.o2n.p, m.nf_ptr.p,
+                                                       m.nf_face.p, m.fcode.p, m.fnrm.p, m.P.p, dw, m.vol.p, a.gV2.p);
+    AEROF_LAUNCH_CHECK();
+  }
+  auto go = [&](auto kern) {
+    AEROF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<m.nblk, kAB, smem, s>>>(m.N, m.NB, g, rec, m.n2o.p, dU, m.P2.p, m.W2.p, m.nb2_ptr.p, m.lnb.p, m.hptr.p,
+                                   m.hnode.p, a.gV2.p, a.gG2.p, dout);
+    AEROF_LAUNCH_CHECK();
+  };
+  if (L == 4) go(k_a_lsq_blocked<4>);
+  else if (L == 2) go(k_a_lsq_blocked<2>);
+  else go(k_a_lsq_blocked<1>);
+  return true;
+}
+
 // Blocked reverse sweep over the edges and faces: a.gV, a.gG (caller
 // numbering) from the cotangent dw; with geo, also the cotangents of the
 // edge normals and dx.  Needs P (caller numbering) and P2/G2 current.
-static void reverse_sweep_blocked(aerof_gpu_ctx* c, const double* dw, bool geo) {
+static void reverse_sweep_blocked(aerof_gpu_ctx* c, const double* dw, bool geo, bool assemble = true) {
   DeviceMesh& m = c->mesh;
   AdjWork& a = c->adj;
   cudaStream_t s = c->stream;
@@ -720,6 +936,7 @@ static void reverse_sweep_blocked(aerof_gpu_ctx* c, const double* dw, bool geo) 
   };
   if (geo) go(k_a_fv_blocked<true>);
   else go(k_a_fv_blocked<false>);
+  if (!assemble) return;
   k_a_fv_nodes<<<gn, kAB, 0, s>>>(m.N, m.n2o.p, a.gVp.p, a.gGp.p, m.xin_ptr.p, a.spill.p, a.gV.p, a.gG.p);
   AEROF_LAUNCH_CHECK();
   if (m.F) {
@@ -748,7 +965,21 @@ void vjp_dev(aerof_gpu_ctx* c, const double* dU, const double* dw, double* dout)
   a.gG.ensure(16 * (size_t)m.N);
   if (reverse_blocked_fits(m)) {
     prim_grad_blocked_dev(c, dU, nullptr);
-    reverse_sweep_blocked(c, dw, false);
+    if (lsq_blocked_smem(m) <= 200 * 1024 && kAB % m.NB == 0) {
+      // edges, then assembly, faces, LSQ transpose and (dV/dU)^T in the
+      // blocked organisation
+      reverse_sweep_blocked(c, dw, false, false);
+      if (assemble_lsq_blocked(c, dU, dw, nullptr, rec, dout)) return;
+      k_a_fv_nodes<<<gn, kAB, 0, s>>>(m.N, m.n2o.p, a.gVp.p, a.gGp.p, m.xin_ptr.p, a.spill.p, a.gV.p, a.gG.p);
+      AEROF_LAUNCH_CHECK();
+      if (m.F) {
+        k_a_faces<<<gn, kAB, 0, s>>>(m.N, m.F, g, m.Ubd.p, m.nf_ptr.p, m.nf_face.p, m.fcode.p, m.fnrm.p, m.P.p, dw,
+                                     m.vol.p, a.gV.p);
+        AEROF_LAUNCH_CHECK();
+      }
+    } else {
+      reverse_sweep_blocked(c, dw, false);
+    }
   } else {
     c->s.G.ensure(16 * (size_t)m.N);
     if (rec != AEROF_REC_CONSTANT) gradients_dev(c);
@@ -1749,6 +1980,7 @@ static void h2_vjp_dev(aerof_gpu_ctx* c, const double* dw, double* dout) {
                                                m.P2.p, a.lam2.p, m.lptr.p, m.lidx.p, m.xslot.p, h2pairs(h), a.gVp.p,
                                                a.gGp.p, a.spill.p);
   AEROF_LAUNCH_CHECK();
+  if (assemble_lsq_blocked(c, h.U.p, dw, h.fj.p, h.rec, dout)) return;
   k_a_fv_nodes<<<gn, kAB, 0, s>>>(m.N, m.n2o.p, a.gVp.p, a.gGp.p, m.xin_ptr.p, a.spill.p, a.gV.p, a.gG.p);
   AEROF_LAUNCH_CHECK();
   if (m.nbrow) {

@@ -207,6 +207,7 @@ struct AdjWork {
   DBuf<double> spill;      // [nX][13] second-endpoint parts of block-crossing edges
   DBuf<double> geo;        // [6][E] cotangents of edge normals and dx (original edge order)
   DBuf<double> tg;         // [T][12] per-tet vertex coordinate cotangents
+  DBuf<double> gV2, gG2;   // [N][5], [N][16] assembled cotangents, blocked numbering
 };
 
 // Stored exact linearisation of the residual (the operator MatVecProdH2

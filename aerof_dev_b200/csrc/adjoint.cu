@@ -20,6 +20,9 @@
 namespace aerof {
 
 constexpr int kAB = 256;
+// doubles per spill slot of the blocked reverse sweeps: g_Vj (5), g_ddji
+// (5), dx (3), padding to a 128-byte record read with 16-byte loads
+constexpr int kSP = 16;
 
 
 __global__ void k_d_seed(int N, Gas g, const double* __restrict__ U, const double* __restrict__ v,
@@ -559,7 +562,7 @@ __global__ void __launch_bounds__(256, 1) k_a_fv_blocked(int N, int E, int NB, G
     const int xs = xslot[q];
     if (GEO || xs >= 0) {
       double gdx0 = 0.0, gdx1 = 0.0, gdx2 = 0.0;
-      double* sp = xs >= 0 ? spill + 13 * (size_t)xs : nullptr;
+      double* sp = xs >= 0 ? spill + kSP * (size_t)xs : nullptr;
 #pragma unroll
       for (int k = 0; k < 5; ++k) {
         double gvi = 0.0, gvj = 0.0, gdi, gdj;
@@ -640,13 +643,27 @@ __global__ void k_a_fv_nodes(int N, const int* __restrict__ n2o, const double* _
                              const double* __restrict__ spill, double* __restrict__ gV, double* __restrict__ gG) {
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
-  double av[5], ag[15];
+  double av[5], ag[16];
 #pragma unroll
   for (int c = 0; c < 5; ++c) av[c] = gVp[5 * (size_t)n + c];
+  {
+    const double2* g2 = reinterpret_cast<const double2*>(gGp + 16 * (size_t)n);
 #pragma unroll
-  for (int c = 0; c < 15; ++c) ag[c] = gGp[16 * (size_t)n + c];
+    for (int c = 0; c < 8; ++c) {
+      const double2 v = g2[c];
+      ag[2 * c] = v.x;
+      ag[2 * c + 1] = v.y;
+    }
+  }
   for (int k = xin_ptr[n]; k < xin_ptr[n + 1]; ++k) {
-    const double* sp = spill + 13 * (size_t)k;
+    double sp[14];
+    const double2* s2 = reinterpret_cast<const double2*>(spill + kSP * (size_t)k);
+#pragma unroll
+    for (int c = 0; c < 7; ++c) {
+      const double2 v = s2[c];
+      sp[2 * c] = v.x;
+      sp[2 * c + 1] = v.y;
+    }
     const double dx0 = sp[10], dx1 = sp[11], dx2 = sp[12];
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
@@ -702,13 +719,27 @@ __global__ void k_a_nodes_b(int N, const int* __restrict__ n2o, const double* __
                             const double* __restrict__ vol, double* __restrict__ gV2, double* __restrict__ gG2) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
-  double av[5], ag[15];
+  double av[5], ag[16];
 #pragma unroll
   for (int c = 0; c < 5; ++c) av[c] = gVp[5 * (size_t)n + c];
+  {
+    const double2* g2 = reinterpret_cast<const double2*>(gGp + 16 * (size_t)n);
 #pragma unroll
-  for (int c = 0; c < 15; ++c) ag[c] = gGp[16 * (size_t)n + c];
+    for (int c = 0; c < 8; ++c) {
+      const double2 v = g2[c];
+      ag[2 * c] = v.x;
+      ag[2 * c + 1] = v.y;
+    }
+  }
   for (int k = xin_ptr[n]; k < xin_ptr[n + 1]; ++k) {
-    const double* sp = spill + 13 * (size_t)k;
+    double sp[14];
+    const double2* s2 = reinterpret_cast<const double2*>(spill + kSP * (size_t)k);
+#pragma unroll
+    for (int c = 0; c < 7; ++c) {
+      const double2 v = s2[c];
+      sp[2 * c] = v.x;
+      sp[2 * c + 1] = v.y;
+    }
     const double dx0 = sp[10], dx1 = sp[11], dx2 = sp[12];
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
@@ -781,8 +812,9 @@ __global__ void k_a_faces_b(int nbrow, int F, Gas g, const double* __restrict__ 
 // g_V_q += sum_i W_i(x_q - x_i) . g_grad_i - (sum_i W_q(x_i - x_q)) . g_grad_q,
 // fixed xor-tree lane sum, (dV/dU)^T, written in the caller's numbering.
 constexpr int kLR = 26;
+constexpr int kLsqThreads = 512;
 template <int L>
-__global__ void __launch_bounds__(256, 2) k_a_lsq_blocked(int N, int NB, Gas g, int rec, const int* __restrict__ n2o,
+__global__ void __launch_bounds__(kLsqThreads, 2) k_a_lsq_blocked(int N, int NB, Gas g, int rec, const int* __restrict__ n2o,
                                                           const double* __restrict__ U, const double* __restrict__ P2,
                                                           const double* __restrict__ W2,
                                                           const int* __restrict__ nb2_ptr,
@@ -803,23 +835,27 @@ __global__ void __launch_bounds__(256, 2) k_a_lsq_blocked(int N, int NB, Gas g, 
   const int t = threadIdx.x / L, r = threadIdx.x % L;
   const bool act = t < nn;
   if (grad) {
-    for (int k = threadIdx.x; k < nc; k += blockDim.x) ls[k] = lnb[c0 + k];
+    // thread per staged node, all its copies together; the first two node
+    // ids of each thread are loaded before any copy is issued
     double2* rd = reinterpret_cast<double2*>(rs);
-    for (int k = threadIdx.x; k < 2 * ns; k += blockDim.x) {
-      const int q = k >> 1;
-      const int j = q < nn ? n0 + q : hnode[h0 + q - nn];
-      cp_async16(rd + (kLR / 2) * q + (k & 1), reinterpret_cast<const double2*>(P2 + 8 * (size_t)j) + 2 + (k & 1));
-    }
-    for (int k = threadIdx.x; k < 8 * ns; k += blockDim.x) {
-      const int q = k >> 3;
-      const int j = q < nn ? n0 + q : hnode[h0 + q - nn];
-      cp_async16(rd + (kLR / 2) * q + 5 + (k & 7), reinterpret_cast<const double2*>(gG2 + 16 * (size_t)j) + (k & 7));
-    }
-    for (int k = threadIdx.x; k < 6 * ns; k += blockDim.x) {
-      const int q = k / 6, a = k % 6;
-      const int j = q < nn ? n0 + q : hnode[h0 + q - nn];
-      cp_async8(rs + kLR * q + 4 + a, W2 + (size_t)a * N + j);
-    }
+    auto stage = [&](int q, int j) {
+      const double2* px = reinterpret_cast<const double2*>(P2 + 8 * (size_t)j) + 2;
+      const double2* pg = reinterpret_cast<const double2*>(gG2 + 16 * (size_t)j);
+      cp_async16(rd + (kLR / 2) * q, px);
+      cp_async16(rd + (kLR / 2) * q + 1, px + 1);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) cp_async16(rd + (kLR / 2) * q + 5 + c, pg + c);
+#pragma unroll
+      for (int a = 0; a < 6; ++a) cp_async8(rs + kLR * q + 4 + a, W2 + (size_t)a * N + j);
+    };
+    auto node_id = [&](int q) { return q < nn ? n0 + q : hnode[h0 + q - nn]; };
+    const int q0 = threadIdx.x, q1 = threadIdx.x + blockDim.x;
+    const int j0 = q0 < ns ? node_id(q0) : -1;
+    const int j1 = q1 < ns ? node_id(q1) : -1;
+    if (j0 >= 0) stage(q0, j0);
+    if (j1 >= 0) stage(q1, j1);
+    for (int q = threadIdx.x + 2 * blockDim.x; q < ns; q += blockDim.x) stage(q, node_id(q));
+    for (int k = threadIdx.x; k < nc; k += blockDim.x) ls[k] = lnb[c0 + k];
     cp_async_wait_all();
   }
   __syncthreads();
@@ -883,8 +919,8 @@ static bool assemble_lsq_blocked(aerof_gpu_ctx* c, const double* dU, const doubl
   cudaStream_t s = c->stream;
   const Gas g = make_gas(c->cfg.gamma);
   const size_t smem = lsq_blocked_smem(m);
-  const int L = kAB / m.NB;
-  if (smem > 200 * 1024 || L < 1 || L > 4 || L * m.NB != kAB) return false;
+  const int L = kLsqThreads / m.NB;
+  if (smem > 200 * 1024 || L < 2 || L > 8 || L * m.NB != kLsqThreads) return false;
   a.gV2.ensure(5 * (size_t)m.N);
   a.gG2.ensure(16 * (size_t)m.N);
   k_a_nodes_b<<<grid_for(m.N, kAB), kAB, 0, s>>>(m.N, m.n2o.p, a.gVp.p, a.gGp.p, m.xin_ptr.p, a.spill.p, m.brow.p,
@@ -897,13 +933,13 @@ static bool assemble_lsq_blocked(aerof_gpu_ctx* c, const double* dU, const doubl
   }
   auto go = [&](auto kern) {
     AEROF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<m.nblk, kAB, smem, s>>>(m.N, m.NB, g, rec, m.n2o.p, dU, m.P2.p, m.W2.p, m.nb2_ptr.p, m.lnb.p, m.hptr.p,
-                                   m.hnode.p, a.gV2.p, a.gG2.p, dout);
+    kern<<<m.nblk, kLsqThreads, smem, s>>>(m.N, m.NB, g, rec, m.n2o.p, dU, m.P2.p, m.W2.p, m.nb2_ptr.p, m.lnb.p,
+                                           m.hptr.p, m.hnode.p, a.gV2.p, a.gG2.p, dout);
     AEROF_LAUNCH_CHECK();
   };
-  if (L == 4) go(k_a_lsq_blocked<4>);
-  else if (L == 2) go(k_a_lsq_blocked<2>);
-  else go(k_a_lsq_blocked<1>);
+  if (L == 8) go(k_a_lsq_blocked<8>);
+  else if (L == 4) go(k_a_lsq_blocked<4>);
+  else go(k_a_lsq_blocked<2>);
   return true;
 }
 
@@ -920,7 +956,7 @@ static void reverse_sweep_blocked(aerof_gpu_ctx* c, const double* dw, bool geo, 
   a.lam2.ensure(6 * (size_t)m.N);
   a.gVp.ensure(5 * (size_t)m.N);
   a.gGp.ensure(16 * (size_t)m.N);
-  a.spill.ensure(13 * (size_t)std::max(m.nX, 1));
+  a.spill.ensure(kSP * (size_t)std::max(m.nX, 1));
   a.gV.ensure(5 * (size_t)m.N);
   a.gG.ensure(16 * (size_t)m.N);
   if (geo) a.geo.ensure(6 * (size_t)std::max(m.E, 1));
@@ -965,7 +1001,7 @@ void vjp_dev(aerof_gpu_ctx* c, const double* dU, const double* dw, double* dout)
   a.gG.ensure(16 * (size_t)m.N);
   if (reverse_blocked_fits(m)) {
     prim_grad_blocked_dev(c, dU, nullptr);
-    if (lsq_blocked_smem(m) <= 200 * 1024 && kAB % m.NB == 0) {
+    if (lsq_blocked_smem(m) <= 200 * 1024 && kLsqThreads % m.NB == 0) {
       // edges, then assembly, faces, LSQ transpose and (dV/dU)^T in the
       // blocked organisation
       reverse_sweep_blocked(c, dw, false, false);
@@ -1549,7 +1585,7 @@ __global__ void __launch_bounds__(256, 2) k_h2t_blocked(int N, int E, int NB, co
     for (int k = 0; k < 5; ++k) { es[k] = gL[k]; es[5 + k] = gR[k]; }
     const int xs = xslot[q];
     if (xs >= 0) {
-      double* sp = spill + 13 * (size_t)xs;
+      double* sp = spill + kSP * (size_t)xs;
 #pragma unroll
       for (int c = 0; c < 5; ++c) {
         const double2 pp = h2[(size_t)(25 + c) * sE + q];
@@ -1609,9 +1645,13 @@ __global__ void __launch_bounds__(256, 2) k_h2t_blocked(int N, int E, int NB, co
 // shared memory.  Phase 0 as k_h2t_blocked.  Phase 1 reads each edge's 35
 // pairs once (coalesced) and leaves (g_Vi, g_ddij, g_Vj, g_ddji) in shared
 // memory at a 21-double stride (conflict-free consecutive writes); phase 2
-// gathers from shared memory only.  Same arithmetic as k_h2t_blocked.
+// gathers from shared memory only.  Same arithmetic as k_h2t_blocked.  The
+// streamed pairs are in flight through L1, so the kernel is faster the less
+// shared memory it holds: a second staging buffer (for a persistent,
+// prefetching form) costs more than its latency hiding gains.
 constexpr int kEW = 21;
-__global__ void __launch_bounds__(1024, 1) k_h2t_wide(int N, int E, int NB, const ushort2* __restrict__ bl,
+constexpr int kWideThreads = 1024;
+__global__ void __launch_bounds__(kWideThreads, 1) k_h2t_wide(int N, int E, int NB, const ushort2* __restrict__ bl,
                                                       const int* __restrict__ beptr, const int* __restrict__ hfptr,
                                                       const int* __restrict__ hfpad, int maxHf,
                                                       const double* __restrict__ P2, const double* __restrict__ lam2,
@@ -1662,7 +1702,7 @@ __global__ void __launch_bounds__(1024, 1) k_h2t_wide(int N, int E, int NB, cons
     h2_transpose_blocks(h2, sE, q, gF, gL, gR);
     double* es = Es + kEW * (q - e0);
     const int xs = xslot[q];
-    double* sp = xs >= 0 ? spill + 13 * (size_t)xs : nullptr;
+    double* sp = xs >= 0 ? spill + kSP * (size_t)xs : nullptr;
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
       const double2 pp = h2[(size_t)(25 + c) * sE + q], qv = h2[(size_t)(30 + c) * sE + q];
@@ -1767,7 +1807,8 @@ __global__ void k_h2_seed(int N, Gas g, const int* __restrict__ n2o, const doubl
 // partials, dphi = (d phi / d Vij) dVij + (d phi / d Vji) dVji into shared
 // memory (and spill for block-crossing edges); phase 2 sums each node's
 // edges in edge order (+ first endpoint, - second) into part.
-__global__ void __launch_bounds__(512, 2) k_h2_blocked(int N, int E, int NB, int rec, const ushort2* __restrict__ bl,
+template <int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) k_h2_blocked(int N, int E, int NB, int rec, const ushort2* __restrict__ bl,
                                                        const int* __restrict__ beptr, const int* __restrict__ hfptr,
                                                        const int* __restrict__ hfpad, int maxHf,
                                                        const double* __restrict__ dP2, const double* __restrict__ dG2,
@@ -1963,7 +2004,7 @@ static void h2_vjp_dev(aerof_gpu_ctx* c, const double* dw, double* dout) {
   a.lam2.ensure(6 * (size_t)m.N);
   a.gVp.ensure(5 * (size_t)m.N);
   a.gGp.ensure(16 * (size_t)m.N);
-  a.spill.ensure(13 * (size_t)std::max(m.nX, 1));
+  a.spill.ensure(kSP * (size_t)std::max(m.nX, 1));
   a.gV.ensure(5 * (size_t)m.N);
   a.gG.ensure(16 * (size_t)m.N);
   k_a_lam2<<<gn, kAB, 0, s>>>(m.N, m.n2o.p, dw, m.vol2.p, a.lam2.p);
@@ -1971,14 +2012,20 @@ static void h2_vjp_dev(aerof_gpu_ctx* c, const double* dw, double* dout) {
   // wide form when both endpoints' results fit in shared memory (tuning
   // knob AEROF_H2T_WIDE=0 selects the compact form)
   const char* wide_var = std::getenv("AEROF_H2T_WIDE");
-  const bool wide_env = !wide_var || std::atoi(wide_var) != 0;
-  const bool wide = wide_env && h2t_wide_smem(m) <= 220 * 1024;
-  const size_t smem = wide ? h2t_wide_smem(m) : h2t_smem(m);
-  auto kern = wide ? k_h2t_wide : k_h2t_blocked;
-  AEROF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<m.nblk, wide ? 1024 : 256, smem, s>>>(m.N, m.E, m.NB, m.bl.p, m.beptr.p, m.hfptr.p, m.hfpad.p, m.maxHf,
-                                               m.P2.p, a.lam2.p, m.lptr.p, m.lidx.p, m.xslot.p, h2pairs(h), a.gVp.p,
-                                               a.gGp.p, a.spill.p);
+  const bool wide = (!wide_var || std::atoi(wide_var) != 0) && h2t_wide_smem(m) <= 220 * 1024;
+  if (wide) {
+    const size_t smem = h2t_wide_smem(m);
+    AEROF_CUDA(cudaFuncSetAttribute(k_h2t_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_h2t_wide<<<m.nblk, kWideThreads, smem, s>>>(m.N, m.E, m.NB, m.bl.p, m.beptr.p, m.hfptr.p, m.hfpad.p, m.maxHf,
+                                                  m.P2.p, a.lam2.p, m.lptr.p, m.lidx.p, m.xslot.p, h2pairs(h),
+                                                  a.gVp.p, a.gGp.p, a.spill.p);
+  } else {
+    const size_t smem = h2t_smem(m);
+    AEROF_CUDA(cudaFuncSetAttribute(k_h2t_blocked, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_h2t_blocked<<<m.nblk, 256, smem, s>>>(m.N, m.E, m.NB, m.bl.p, m.beptr.p, m.hfptr.p, m.hfpad.p, m.maxHf,
+                                            m.P2.p, a.lam2.p, m.lptr.p, m.lidx.p, m.xslot.p, h2pairs(h), a.gVp.p,
+                                            a.gGp.p, a.spill.p);
+  }
   AEROF_LAUNCH_CHECK();
   if (assemble_lsq_blocked(c, h.U.p, dw, h.fj.p, h.rec, dout)) return;
   k_a_fv_nodes<<<gn, kAB, 0, s>>>(m.N, m.n2o.p, a.gVp.p, a.gGp.p, m.xin_ptr.p, a.spill.p, a.gV.p, a.gG.p);
@@ -2007,8 +2054,14 @@ static void h2_jvp_dev(aerof_gpu_ctx* c, const double* dp, double* dout) {
   AEROF_LAUNCH_CHECK();
   if (h.rec != AEROF_REC_CONSTANT) grad_records_blocked_dev(c, h.dP2.p, h.dG2.p);
   const size_t smem = h2f_smem(m);
-  AEROF_CUDA(cudaFuncSetAttribute(k_h2_blocked, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_h2_blocked<<<m.nblk, 512, smem, s>>>(m.N, m.E, m.NB, h.rec, m.bl.p, m.beptr.p, m.hfptr.p, m.hfpad.p, m.maxHf,
+  // one CTA of 1024 threads per SM by default: the streamed pairs are in
+  // flight through L1, which two CTAs' shared memory would leave small
+  // (tuning knob AEROF_H2F_THREADS = 512 or 256: two CTAs per SM)
+  const char* fvar = std::getenv("AEROF_H2F_THREADS");
+  const int fthreads = fvar && std::atoi(fvar) == 512 ? 512 : fvar && std::atoi(fvar) == 256 ? 256 : 1024;
+  auto kf = fthreads == 512 ? k_h2_blocked<512, 2> : fthreads == 256 ? k_h2_blocked<256, 2> : k_h2_blocked<1024, 1>;
+  AEROF_CUDA(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kf<<<m.nblk, fthreads, smem, s>>>(m.N, m.E, m.NB, h.rec, m.bl.p, m.beptr.p, m.hfptr.p, m.hfpad.p, m.maxHf,
                                          h.dP2.p, h.dG2.p, m.lptr.p, m.lidx.p, m.xslot.p, h2pairs(h), h.part.p,
                                          h.spill.p);
   AEROF_LAUNCH_CHECK();

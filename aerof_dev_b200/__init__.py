@@ -50,6 +50,7 @@ EXPORTS = [
     "aerof_gpu_residual_async", "aerof_gpu_status", "aerof_gpu_profile", "aerof_gpu_timers",
     "aerof_gpu_update_coordinates", "aerof_gpu_linearized_solve", "aerof_gpu_residual_noalloc",
     "aerof_gpu_h2_evaluate", "aerof_gpu_h2_apply", "aerof_gpu_h2_release", "aerof_gpu_set_exact_operator",
+    "aerof_gpu_linearized_solve_batch",
 ]
 TIMER_NAMES = ["nodal_grad", "fv_term", "time_step", "fv_jac", "prec_setup", "ksp_matvec", "ksp_other", "other"]
 
@@ -129,6 +130,8 @@ def library(path: str | None = None):
             "aerof_gpu_h2_apply": [vp, dp, dp, C.c_int],
             "aerof_gpu_h2_release": [vp],
             "aerof_gpu_set_exact_operator": [vp, C.c_int],
+            "aerof_gpu_linearized_solve_batch": [vp, dp, C.c_int, dp, dp, C.c_int, C.c_int, C.c_double, C.c_int,
+                                                 C.c_int, dp, dp],
         }
         for name, args in sig.items():
             if hasattr(L, name):
@@ -540,6 +543,22 @@ class Sensitivity:
         """Exact products of `solve`: re-evaluated per product (False) or
         from the operator stored once per solve (True)."""
         self.ctx._check(self.ctx.L.aerof_gpu_set_exact_operator(self.ctx.h, int(bool(stored))))
+
+    def solve_batch(self, U, B, transpose=False, krylov=30, maxits=300, eps=1e-10, inner_its=20):
+        """Solve J x_k = b_k (or J^T x_k = b_k) for every B[k] ([nrhs, N, 5])
+        with one operator set-up (stored exact linearisation).  Returns X,
+        iterations and final residual norms per right-hand side."""
+        ctx = self.ctx
+        u = _Arg(U, np.float64, (ctx.N, 5))
+        nrhs = int(B.shape[0])
+        bb = _Arg(B, np.float64, (nrhs, ctx.N, 5))
+        xx = _Arg(_like(B, (nrhs, ctx.N, 5)), np.float64, writable=True)
+        its = np.zeros(nrhs, dtype=np.int32)
+        res = np.zeros(nrhs, dtype=np.float64)
+        ctx._check(ctx.L.aerof_gpu_linearized_solve_batch(ctx.h, u.ptr, nrhs, bb.ptr, xx.ptr, krylov, maxits, eps,
+                                                          int(transpose), int(inner_its),
+                                                          C.c_void_p(its.ctypes.data), C.c_void_p(res.ctypes.data)))
+        return xx.obj, its, res
 
     def solve(self, U, b, transpose=False, krylov=30, maxits=300, eps=1e-10, inner_its=0):
         """Solve J x = b (direct) or J^T x = b (adjoint) with the exact

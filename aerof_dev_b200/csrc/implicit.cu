@@ -1107,3 +1107,50 @@ extern "C" int aerof_gpu_linearized_solve(aerof_gpu_ctx* c, const double* U, con
     return AEROF_OK;
   });
 }
+
+// Several linearised solves sharing one operator set-up (the batched
+// direct-sensitivity right-hand sides of a shape optimisation,
+// FluidShapeOptimizationHandler.C:2362-2433, one fsoLinearSolver per mode):
+// the exact linearisation at U is stored once (MatVecProdH2::evaluate), the
+// first-order operator and its block-Jacobi are assembled once, and each
+// right-hand side B[k] ([nrhs][N][5]) is solved as aerof_gpu_linearized_solve
+// does, its exact products read from the stored operator.
+extern "C" int aerof_gpu_linearized_solve_batch(aerof_gpu_ctx* c, const double* U, int nrhs, const double* B,
+                                                double* X, int krylov, int maxits, double eps, int transpose,
+                                                int inner_its, int* its, double* res) {
+  return guard(c, [&]() -> int {
+    need_mesh_or_throw(c);
+    if (!U || !B || !X || nrhs < 0 || krylov < 1 || maxits < 1 || !(eps >= 0.0) || inner_its < 0)
+      return AEROF_EINVAL;
+    if (nrhs == 0) return AEROF_OK;
+    const size_t n = 5 * (size_t)c->mesh.N;
+    c->imp.t.ensure(n);
+    const double* dU0 = in_dev(c, U, n, c->s.Ustage);
+    if (dU0 != c->imp.t.p)
+      AEROF_CUDA(cudaMemcpyAsync(c->imp.t.p, dU0, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    const double* dU = c->imp.t.p;
+    struct UseStored {
+      H2Op& h;
+      ~UseStored() { h.use = false; }
+    } use_stored{c->h2};
+    h2_evaluate_dev(c, dU);
+    c->h2.use = true;
+    jacobian_dev(c, dU, nullptr, inner_its ? AEROF_PREC_FP32 : AEROF_PREC_FP64, inner_its && transpose);
+    if (int nb = prec_setup_dev(c)) {
+      c->last_error = std::to_string(nb) + " singular diagonal block(s)";
+      return AEROF_ESINGULAR;
+    }
+    for (int k = 0; k < nrhs; ++k) {
+      const double* db = in_dev(c, B + (size_t)k * n, n, c->s.Vstage);
+      double* dx = out_dev(c, X + (size_t)k * n, n, c->s.Rstage);
+      double r = 0.0;
+      const int it = inner_its ? fgmres_exact(c, db, dx, krylov, maxits, eps, transpose, &r, dU,
+                                              std::min(inner_its, 30), inner_its, 1e-3)
+                               : gmres_dev(c, db, dx, krylov, maxits, eps, transpose, &r, dU);
+      out_finish(c, X + (size_t)k * n, dx, n);
+      if (its) its[k] = it;
+      if (res) res[k] = r;
+    }
+    return AEROF_OK;
+  });
+}

@@ -144,6 +144,22 @@ def direct_gradient(ctx, U, X, functional: ZForce, modes, eps=1e-10, krylov=30, 
     return np.array(out), {"direct_its": its_all}
 
 
+def direct_gradient_batch(ctx, U, X, functional: ZForce, modes, eps=1e-10, krylov=30, maxits=2000, inner_its=20):
+    """dJ/ds_k for every mode by the direct method, all right-hand sides in
+    one batched solve (the exact linearisation stored once)."""
+    import aerof_dev_b200 as A
+    S = A.Sensitivity(ctx)
+    U = _host(U)
+    gU = functional.dU(U, X)
+    gX = functional.dX(U, X)
+    rhs = np.stack([-S.dRdX(U, Xd) for Xd in modes])
+    x, its, res = S.solve_batch(U, rhs, transpose=False, krylov=krylov, maxits=maxits, eps=eps,
+                                inner_its=inner_its)
+    S.h2_release()
+    out = np.einsum("kni,ni->k", modes, gX) + np.einsum("kni,ni->k", x, gU)
+    return out, {"direct_its": its.tolist(), "direct_res": res.tolist()}
+
+
 def fd_gradient(ctx, U, X, functional: ZForce, modes, h=1e-6, **conv):
     """Central finite differences with the flow re-converged at X +- h Xdot.
 

@@ -109,3 +109,21 @@ def test_h2_block_sizes(gpu_lib, monkeypatch, nb, wide):
     w = rng.standard_normal(U.shape)
     assert rel_l2(S.h2_apply(v), S.jvp(U, v)) < 1e-12
     assert rel_l2(S.h2_apply(w, transpose=True), S.vjp(U, w)) < 1e-12
+
+
+def test_batched_solve_matches_single_solves(case):
+    rec, m, Ub, o, U, ctx, S = case
+    if m["X"].shape[0] > 400:
+        pytest.skip("small mesh only")
+    rng = np.random.default_rng(27)
+    B = rng.standard_normal((3,) + U.shape)
+    for transpose in (False, True):
+        X, its, res = S.solve_batch(U, B, transpose=transpose, krylov=30, maxits=600, eps=1e-10, inner_its=10)
+        assert X.shape == B.shape and len(its) == 3
+        for k in range(3):
+            Ax = S.vjp(U, X[k]) if transpose else S.jvp(U, X[k])
+            assert np.linalg.norm(Ax - B[k]) <= 1e-9 * np.linalg.norm(B[k])
+            assert res[k] <= 1.01e-10 * np.linalg.norm(B[k])
+    # the stored operator stays evaluated at U after the batch
+    v = rng.standard_normal(U.shape)
+    assert rel_l2(S.h2_apply(v), S.jvp(U, v)) < 1e-12

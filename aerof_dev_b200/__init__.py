@@ -37,6 +37,7 @@ ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ETIMEDOUT", -5: "ESINGUL
 REC_CONSTANT, REC_VANALBADA, REC_LINEAR = 1, 2, 3
 KERNEL_BLOCKED, KERNEL_EDGE = 0, 1
 PREC_FP32, PREC_FP64 = 32, 64
+PC_JACOBI, PC_ILU0 = 0, 1
 
 # every entry point of include/aerof_gpu.h
 EXPORTS = [
@@ -50,7 +51,7 @@ EXPORTS = [
     "aerof_gpu_residual_async", "aerof_gpu_status", "aerof_gpu_profile", "aerof_gpu_timers",
     "aerof_gpu_update_coordinates", "aerof_gpu_linearized_solve", "aerof_gpu_residual_noalloc",
     "aerof_gpu_h2_evaluate", "aerof_gpu_h2_apply", "aerof_gpu_h2_release", "aerof_gpu_set_exact_operator",
-    "aerof_gpu_linearized_solve_batch",
+    "aerof_gpu_linearized_solve_batch", "aerof_gpu_set_preconditioner",
 ]
 TIMER_NAMES = ["nodal_grad", "fv_term", "time_step", "fv_jac", "prec_setup", "ksp_matvec", "ksp_other", "other"]
 
@@ -132,6 +133,7 @@ def library(path: str | None = None):
             "aerof_gpu_set_exact_operator": [vp, C.c_int],
             "aerof_gpu_linearized_solve_batch": [vp, dp, C.c_int, dp, dp, C.c_int, C.c_int, C.c_double, C.c_int,
                                                  C.c_int, dp, dp],
+            "aerof_gpu_set_preconditioner": [vp, C.c_int],
         }
         for name, args in sig.items():
             if hasattr(L, name):
@@ -292,6 +294,10 @@ class Context:
     def status(self) -> int:
         """Wait for the stream; unphysical count of async calls since last status."""
         return self._check(self.L.aerof_gpu_status(self.h))
+
+    def set_preconditioner(self, pc: int):
+        """Preconditioner of the Krylov solvers: PC_JACOBI or PC_ILU0."""
+        self._check(self.L.aerof_gpu_set_preconditioner(self.h, int(pc)))
 
     def profile(self, enable: bool = True):
         self._check(self.L.aerof_gpu_profile(self.h, int(enable)))

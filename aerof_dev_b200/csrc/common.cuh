@@ -127,6 +127,15 @@ struct DeviceMesh {
   int nsl = 0;
   int nbrow = 0;           // rows with boundary faces
   DBuf<int> brow, blist;   // [N] index among the boundary rows (-1: none); [nbrow] those rows
+  // multicolour ordering for the block ILU(0) preconditioner: greedy
+  // colouring of the node graph (ascending node order, smallest free
+  // colour), rows sorted by (colour, node).  ILU pattern in that order:
+  // row i holds its diagonal and its neighbours, columns ascending.
+  int ncolor = 0;
+  std::vector<int> h_cptr;       // [ncolor+1] first row of each colour
+  DBuf<int> cperm;               // [N] colour-order row -> caller row
+  DBuf<int> ia, ja, ju;          // [N+1], [N+2E] colour-order columns, [N] diagonal position
+  DBuf<int> isrc;                // [N+2E] neighbour slot in the caller row's list, -1 for the diagonal
   DBuf<int> sptr;          // [nsl+1] block columns before slice s
   DBuf<int> scol;          // [sptr[nsl] * 32]
   std::vector<int> h_sptr, h_nbr_ptr;
@@ -182,6 +191,15 @@ struct Implicit {
   DBuf<double> hcol;       // device scratch for one Hessenberg column
   DBuf<unsigned> ticket;   // grid-reduction ticket of the fused Gram-Schmidt kernels
   DBuf<double> fsum;       // [nbrow][25] boundary-face blocks of the boundary rows
+  // preconditioner: AEROF_PC_JACOBI or AEROF_PC_ILU0 (block ILU(0) in the
+  // multicolour ordering, blocks at a padded stride of 16-byte multiples,
+  // inverted diagonal; factored for the operator read plainly (ilu_tr = 0)
+  // or transposed (1))
+  int pc = 0;
+  bool ilu_ready = false;
+  int ilu_tr = 0;
+  DBuf<double> ilu64, iluw;
+  DBuf<float> ilu32;
   // flexible GMRES on the exact linearisation (outer FP64 vectors)
   DBuf<double> fV, fZ, fw, fr, fh;
 };

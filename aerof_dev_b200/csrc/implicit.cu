@@ -523,6 +523,7 @@ void jacobian_dev(aerof_gpu_ctx* c, const double* dU, const double* ddt, int pre
   J.precision = precision;
   J.transposed = transposed;
   J.prec_ready = false;
+  J.ilu_ready = false;
 }
 
 // products with H1 (trans = 0) or H1^T (trans = 1); the stored blocks may
@@ -548,10 +549,269 @@ void matvec_t(aerof_gpu_ctx* c, const TI* p, TO* y, int trans) {
 }
 void matvec_dev(aerof_gpu_ctx* c, const double* p, double* y, int trans) { matvec_t<double, double>(c, p, y, trans); }
 
-int prec_setup_dev(aerof_gpu_ctx* c) {
+// ---------------------------------------------------------------------
+// Block ILU(0) (IluPrec, KspPrec.C:138-330; SparseMat::numericILU and
+// lusol, SparseMatrix.C:353-450) in the multicolour ordering: the
+// reference's algorithm (IKJ elimination, multiplier A_ik U_kk^-1, updates
+// of the row's own pattern only, inverted diagonal; forward solve with the
+// unit lower part, backward solve with the upper part and the inverted
+// diagonal) on rows sorted by colour instead of the reference's RCM order,
+// so the rows of one colour, which are never neighbours, factor and solve
+// in parallel: one launch per colour.  Blocks are stored row after row at a
+// padded stride (28 floats / 26 doubles: 16-byte multiples).
+template <class S> struct IluP { static constexpr int P = sizeof(S) == 4 ? 28 : 26; };
+template <class S>
+__device__ __forceinline__ void ilu_load(const S* __restrict__ a, size_t q, double* v);
+template <>
+__device__ __forceinline__ void ilu_load<float>(const float* __restrict__ a, size_t q, double* v) {
+  const float4* p = reinterpret_cast<const float4*>(a + 28 * q);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    const float4 t = p[i];
+    v[4 * i] = t.x; v[4 * i + 1] = t.y; v[4 * i + 2] = t.z; v[4 * i + 3] = t.w;
+  }
+  v[24] = a[28 * q + 24];
+}
+template <>
+__device__ __forceinline__ void ilu_load<double>(const double* __restrict__ a, size_t q, double* v) {
+  const double2* p = reinterpret_cast<const double2*>(a + 26 * q);
+#pragma unroll
+  for (int i = 0; i < 12; ++i) {
+    const double2 t = p[i];
+    v[2 * i] = t.x; v[2 * i + 1] = t.y;
+  }
+  v[24] = a[26 * q + 24];
+}
+template <class S>
+__device__ __forceinline__ void ilu_store(S* __restrict__ a, size_t q, const double* v) {
+  constexpr int P = IluP<S>::P;
+#pragma unroll
+  for (int e = 0; e < 25; ++e) a[P * q + e] = (S)v[e];
+}
+
+// the operator's blocks (tr: transposed) copied into the colour-ordered
+// ILU pattern, thread per row
+template <class S>
+__global__ void k_ilu_gather(int N, int tr, const int* __restrict__ cperm, const int* __restrict__ ia,
+                             const int* __restrict__ isrc, const int* __restrict__ nbr_ptr,
+                             const int* __restrict__ nbr_node, const int* __restrict__ nbr_tpos,
+                             const int* __restrict__ sptr, const S* __restrict__ diag, const S* __restrict__ off,
+                             S* __restrict__ lu) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int r = cperm[i];
+  for (int q = ia[i]; q < ia[i + 1]; ++q) {
+    const int k = isrc[q];
+    double v[25], t[25];
+    bool flip = tr != 0;
+    if (k < 0) {
+      load_block<S>(diag, sl_dblk(r), r & 31, v);
+    } else if (!tr) {
+      load_block<S>(off, sl_blk(sptr, r, k), r & 31, v);
+    } else {
+      const int p = nbr_ptr[r] + k;
+      const int sn = nbr_node[p];
+      load_block<S>(off, sl_blk(sptr, sn, nbr_tpos[p] - nbr_ptr[sn]), sn & 31, v);
+    }
+    if (flip) {
+#pragma unroll
+      for (int e = 0; e < 25; ++e) t[e] = v[5 * (e % 5) + e / 5];
+      ilu_store<S>(lu, (size_t)q, t);
+    } else {
+      ilu_store<S>(lu, (size_t)q, v);
+    }
+  }
+}
+
+// numericILU for the rows [i0, i1) of one colour (all their lower
+// neighbours belong to earlier colours, already factored)
+template <class S>
+__global__ void k_ilu_factor(int i0, int i1, const int* __restrict__ ia, const int* __restrict__ ja,
+                             const int* __restrict__ ju, S* __restrict__ lu, int* __restrict__ bad) {
+  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= i1) return;
+  const int qd = ju[i], qe = ia[i + 1];
+  for (int k = ia[i]; k < qd; ++k) {
+    const int l = ja[k];
+    double a[25], u[25], mult[25];
+    ilu_load<S>(lu, (size_t)k, a);
+    ilu_load<S>(lu, (size_t)ju[l], u);
+#pragma unroll
+    for (int r = 0; r < 5; ++r)
+#pragma unroll
+      for (int cc = 0; cc < 5; ++cc) {
+        double t = 0.0;
+#pragma unroll
+        for (int x = 0; x < 5; ++x) t += a[5 * r + x] * u[5 * x + cc];
+        mult[5 * r + cc] = t;
+      }
+    ilu_store<S>(lu, (size_t)k, mult);
+    // a[m] -= mult a[j] for the upper entries j of row l whose column is
+    // in row i (both column lists ascending)
+    int m = k + 1;
+    for (int j = ju[l] + 1; j < ia[l + 1]; ++j) {
+      const int cj = ja[j];
+      while (m < qe && ja[m] < cj) ++m;
+      if (m >= qe) break;
+      if (ja[m] != cj) continue;
+      double b[25], am[25];
+      ilu_load<S>(lu, (size_t)j, b);
+      ilu_load<S>(lu, (size_t)m, am);
+#pragma unroll
+      for (int r = 0; r < 5; ++r)
+#pragma unroll
+        for (int cc = 0; cc < 5; ++cc) {
+          double t = am[5 * r + cc];
+#pragma unroll
+          for (int x = 0; x < 5; ++x) t -= mult[5 * r + x] * b[5 * x + cc];
+          am[5 * r + cc] = t;
+        }
+      ilu_store<S>(lu, (size_t)m, am);
+    }
+  }
+  double d[25];
+  ilu_load<S>(lu, (size_t)qd, d);
+  if (invert5<double>(d)) atomicAdd(bad, 1);
+  ilu_store<S>(lu, (size_t)qd, d);
+}
+
+// lusol forward sweep for one colour: w_i = x_(perm i) - sum_{k<i} L_ik w_k
+template <class S, class TI>
+__global__ void k_ilu_fwd(int i0, int i1, const int* __restrict__ cperm, const int* __restrict__ ia,
+                          const int* __restrict__ ja, const int* __restrict__ ju, const S* __restrict__ lu,
+                          const TI* __restrict__ x, double* __restrict__ w) {
+  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= i1) return;
+  const size_t r = (size_t)cperm[i];
+  double acc[5];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) acc[c] = (double)x[5 * r + c];
+  for (int k = ia[i]; k < ju[i]; ++k) {
+    double a[25];
+    ilu_load<S>(lu, (size_t)k, a);
+    const double* wk = w + 5 * (size_t)ja[k];
+    double v[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) v[c] = wk[c];
+#pragma unroll
+    for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+      for (int c = 0; c < 5; ++c) acc[rr] -= a[5 * rr + c] * v[c];
+  }
+#pragma unroll
+  for (int c = 0; c < 5; ++c) w[5 * (size_t)i + c] = acc[c];
+}
+
+// lusol backward sweep for one colour: w_i = U_ii^-1 (w_i - sum_{j>i}
+// U_ij w_j), written to z in the caller's numbering as well
+template <class S, class TO>
+__global__ void k_ilu_bwd(int i0, int i1, const int* __restrict__ cperm, const int* __restrict__ ia,
+                          const int* __restrict__ ja, const int* __restrict__ ju, const S* __restrict__ lu,
+                          double* __restrict__ w, TO* __restrict__ z) {
+  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= i1) return;
+  double acc[5];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) acc[c] = w[5 * (size_t)i + c];
+  for (int k = ju[i] + 1; k < ia[i + 1]; ++k) {
+    double a[25];
+    ilu_load<S>(lu, (size_t)k, a);
+    const double* wk = w + 5 * (size_t)ja[k];
+    double v[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) v[c] = wk[c];
+#pragma unroll
+    for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+      for (int c = 0; c < 5; ++c) acc[rr] -= a[5 * rr + c] * v[c];
+  }
+  double d[25], res[5];
+  ilu_load<S>(lu, (size_t)ju[i], d);
+#pragma unroll
+  for (int rr = 0; rr < 5; ++rr) {
+    double t = 0.0;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) t += d[5 * rr + c] * acc[c];
+    res[rr] = t;
+  }
+  const size_t r = (size_t)cperm[i];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) {
+    w[5 * (size_t)i + c] = res[c];
+    z[5 * r + c] = (TO)res[c];
+  }
+}
+
+// gather + factorisation of the operator read with orientation tr;
+// returns the number of singular diagonal blocks (waits for the stream)
+static int ilu_setup(aerof_gpu_ctx* c, int tr) {
+  DeviceMesh& m = c->mesh;
+  Implicit& J = c->imp;
+  cudaStream_t s = c->stream;
+  c->s.counters.ensure(8);
+  int* bad = c->s.counters.p + 5;
+  AEROF_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
+  const size_t nnz = (size_t)m.N + 2 * (size_t)m.E;
+  const int gn = grid_for(m.N, kIB);
+  auto run = [&](auto* lu, auto* diag, auto* off) {
+    using S = std::remove_pointer_t<decltype(lu)>;
+    k_ilu_gather<S><<<gn, kIB, 0, s>>>(m.N, tr, m.cperm.p, m.ia.p, m.isrc.p, m.nbr_ptr.p, m.nbr_node.p,
+                                       m.nbr_tpos.p, m.sptr.p, diag, off, lu);
+    AEROF_LAUNCH_CHECK();
+    for (int col = 0; col < m.ncolor; ++col) {
+      const int i0 = m.h_cptr[col], i1 = m.h_cptr[col + 1];
+      k_ilu_factor<S><<<grid_for(i1 - i0, kIB), kIB, 0, s>>>(i0, i1, m.ia.p, m.ja.p, m.ju.p, lu, bad);
+      AEROF_LAUNCH_CHECK();
+    }
+  };
+  if (J.precision == AEROF_PREC_FP32) {
+    J.ilu32.ensure(28 * nnz);
+    run(J.ilu32.p, J.diag32.p, J.off32.p);
+  } else {
+    J.ilu64.ensure(26 * nnz);
+    run(J.ilu64.p, J.diag64.p, J.off64.p);
+  }
+  int h = 0;
+  AEROF_CUDA(cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+  AEROF_CUDA(cudaStreamSynchronize(s));
+  J.ilu_ready = true;
+  J.ilu_tr = tr;
+  return h;
+}
+
+template <class TI, class TO>
+static void ilu_apply(aerof_gpu_ctx* c, const TI* x, TO* z) {
+  DeviceMesh& m = c->mesh;
+  Implicit& J = c->imp;
+  cudaStream_t s = c->stream;
+  J.iluw.ensure(5 * (size_t)m.N);
+  double* w = J.iluw.p;
+  auto run = [&](const auto* lu) {
+    using S = std::remove_const_t<std::remove_pointer_t<decltype(lu)>>;
+    for (int col = 0; col < m.ncolor; ++col) {
+      const int i0 = m.h_cptr[col], i1 = m.h_cptr[col + 1];
+      k_ilu_fwd<S, TI><<<grid_for(i1 - i0, kIB), kIB, 0, s>>>(i0, i1, m.cperm.p, m.ia.p, m.ja.p, m.ju.p, lu, x, w);
+      AEROF_LAUNCH_CHECK();
+    }
+    for (int col = m.ncolor - 1; col >= 0; --col) {
+      const int i0 = m.h_cptr[col], i1 = m.h_cptr[col + 1];
+      k_ilu_bwd<S, TO><<<grid_for(i1 - i0, kIB), kIB, 0, s>>>(i0, i1, m.cperm.p, m.ia.p, m.ja.p, m.ju.p, lu, w, z);
+      AEROF_LAUNCH_CHECK();
+    }
+  };
+  if (J.precision == AEROF_PREC_FP32) run((const float*)J.ilu32.p);
+  else run((const double*)J.ilu64.p);
+}
+
+int prec_setup_dev(aerof_gpu_ctx* c, int trans = 0) {
   DeviceMesh& m = c->mesh;
   Implicit& J = c->imp;
   TimerScope tp(c, AEROF_T_PREC_SETUP);
+  if (J.pc == AEROF_PC_ILU0) {
+    const int h = ilu_setup(c, ((trans != 0) != J.transposed) ? 1 : 0);
+    J.prec_ready = true;
+    return h;
+  }
   c->s.counters.ensure(8);
   int* bad = c->s.counters.p + 4;
   AEROF_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
@@ -580,6 +840,15 @@ void prec_apply_t(aerof_gpu_ctx* c, const TI* x, TO* z, int trans) {
   Implicit& J = c->imp;
   const int gn = grid_for(m.N, kIB);
   const int tr = ((trans != 0) != J.transposed) ? 1 : 0;
+  if (J.pc == AEROF_PC_ILU0) {
+    // factored for the other orientation (or not yet): factor this one
+    if (!J.ilu_ready || J.ilu_tr != tr) {
+      if (int nb = ilu_setup(c, tr))
+        throw ApiError{AEROF_ESINGULAR, std::to_string(nb) + " singular diagonal block(s) in the ILU(0) factors"};
+    }
+    ilu_apply(c, x, z);
+    return;
+  }
   if (J.precision == AEROF_PREC_FP32)
     k_bj_apply<float, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, J.dinv32.p, x, z, tr);
   else
@@ -1093,7 +1362,7 @@ extern "C" int aerof_gpu_linearized_solve(aerof_gpu_ctx* c, const double* U, con
       c->h2.use = true;
     }
     jacobian_dev(c, dU, nullptr, inner_its ? AEROF_PREC_FP32 : AEROF_PREC_FP64, inner_its && transpose);
-    if (int nb = prec_setup_dev(c)) {
+    if (int nb = prec_setup_dev(c, transpose)) {
       c->last_error = std::to_string(nb) + " singular diagonal block(s)";
       return AEROF_ESINGULAR;
     }
@@ -1136,7 +1405,7 @@ extern "C" int aerof_gpu_linearized_solve_batch(aerof_gpu_ctx* c, const double* 
     h2_evaluate_dev(c, dU);
     c->h2.use = true;
     jacobian_dev(c, dU, nullptr, inner_its ? AEROF_PREC_FP32 : AEROF_PREC_FP64, inner_its && transpose);
-    if (int nb = prec_setup_dev(c)) {
+    if (int nb = prec_setup_dev(c, transpose)) {
       c->last_error = std::to_string(nb) + " singular diagonal block(s)";
       return AEROF_ESINGULAR;
     }
@@ -1150,6 +1419,18 @@ extern "C" int aerof_gpu_linearized_solve_batch(aerof_gpu_ctx* c, const double* 
       out_finish(c, X + (size_t)k * n, dx, n);
       if (its) its[k] = it;
       if (res) res[k] = r;
+    }
+    return AEROF_OK;
+  });
+}
+
+extern "C" int aerof_gpu_set_preconditioner(aerof_gpu_ctx* c, int type) {
+  return guard(c, [&]() -> int {
+    if (type != AEROF_PC_JACOBI && type != AEROF_PC_ILU0) return AEROF_EINVAL;
+    if (c->imp.pc != type) {
+      c->imp.pc = type;
+      c->imp.prec_ready = false;
+      c->imp.ilu_ready = false;
     }
     return AEROF_OK;
   });

@@ -449,6 +449,7 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
     c->has_mesh = false;
     c->imp.precision = 0;
     c->imp.prec_ready = false;
+    c->imp.ilu_ready = false;
     c->h2.ready = false;
     HostMesh h;
     int E = 0;
@@ -531,6 +532,57 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
       m.brow.upload(br.data(), (size_t)N, s);
       if (bls.empty()) m.blist.alloc(1);
       else m.blist.upload(bls.data(), bls.size(), s);
+      AEROF_CUDA(cudaStreamSynchronize(s));
+    }
+    // multicolour ordering and the ILU(0) pattern in it
+    {
+      std::vector<int> col(N, -1), seen;
+      int nc = 0;
+      for (int r = 0; r < N; ++r) {
+        seen.assign(nc + 1, 0);
+        for (int q = h.nbr_ptr[r]; q < h.nbr_ptr[r + 1]; ++q) {
+          const int cq = col[h.nbr_node[q]];
+          if (cq >= 0) seen[cq] = 1;
+        }
+        int c0 = 0;
+        while (seen[c0]) ++c0;
+        col[r] = c0;
+        nc = std::max(nc, c0 + 1);
+      }
+      std::vector<int> cptr(nc + 1, 0), perm(N), iperm(N);
+      for (int r = 0; r < N; ++r) ++cptr[col[r] + 1];
+      for (int c0 = 0; c0 < nc; ++c0) cptr[c0 + 1] += cptr[c0];
+      {
+        std::vector<int> fill(cptr.begin(), cptr.end() - 1);
+        for (int r = 0; r < N; ++r) perm[fill[col[r]]++] = r;
+      }
+      for (int i = 0; i < N; ++i) iperm[perm[i]] = i;
+      const size_t nnz = (size_t)N + h.nbr_ptr[N];
+      std::vector<int> ia(N + 1), ja(nnz), isrc(nnz), ju(N);
+      std::vector<std::pair<int, int>> row;
+      size_t q0 = 0;
+      for (int i = 0; i < N; ++i) {
+        const int r = perm[i];
+        row.clear();
+        row.emplace_back(i, -1);
+        for (int q = h.nbr_ptr[r]; q < h.nbr_ptr[r + 1]; ++q) row.emplace_back(iperm[h.nbr_node[q]], q - h.nbr_ptr[r]);
+        std::sort(row.begin(), row.end());
+        ia[i] = (int)q0;
+        for (const auto& e : row) {
+          if (e.second < 0) ju[i] = (int)q0;
+          ja[q0] = e.first;
+          isrc[q0] = e.second;
+          ++q0;
+        }
+      }
+      ia[N] = (int)q0;
+      m.ncolor = nc;
+      m.h_cptr.swap(cptr);
+      m.cperm.upload(perm.data(), (size_t)N, s);
+      m.ia.upload(ia.data(), ia.size(), s);
+      m.ja.upload(ja.data(), ja.size(), s);
+      m.ju.upload(ju.data(), ju.size(), s);
+      m.isrc.upload(isrc.data(), isrc.size(), s);
       AEROF_CUDA(cudaStreamSynchronize(s));
     }
     // sliced layout of the implicit operator

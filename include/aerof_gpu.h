@@ -50,6 +50,15 @@ extern "C" {
 #define AEROF_REC_VANALBADA 2 /* LSQ gradients + van Albada, RecFcnVanAlbada<5>   */
 #define AEROF_REC_LINEAR 3    /* LSQ gradients + unlimited MUSCL, RecFcnLinear<5> */
 
+/* Preconditioner of the Krylov solvers (PcData::type, IoDataCore.C:2735-2760):
+ * block-Jacobi (JacobiPrec), or block ILU(0) (IluPrec with fill 0,
+ * SparseMat::numericILU / lusol, SparseMatrix.C:353-450) of the same
+ * operator on a colour-major node ordering (greedy colouring of the node
+ * graph) instead of the reference's RCM order, so that every colour
+ * factors and solves in parallel.                                         */
+#define AEROF_PC_JACOBI 0
+#define AEROF_PC_ILU0 1
+
 /* Precision of the assembled H1 Jacobian and block-Jacobi preconditioner. */
 #define AEROF_PREC_FP64 64
 #define AEROF_PREC_FP32 32 /* FP32 blocks, FP64 vectors and accumulation */
@@ -200,8 +209,14 @@ int aerof_gpu_matvec(aerof_gpu_ctx* ctx, const double* p, double* y, int transpo
  * invert the 5x5 diagonal blocks (LINPACK dgefa/dgedi) in the Jacobian's
  * precision.  Returns AEROF_ESINGULAR on a zero pivot.                    */
 int aerof_gpu_prec_setup(aerof_gpu_ctx* ctx);
-/* JacobiPrec::apply / applyT (KspPrec.C:86-111): y = D^-1 x or D^-T x.    */
+/* JacobiPrec::apply / applyT (KspPrec.C:86-111): y = D^-1 x or D^-T x;
+ * with AEROF_PC_ILU0, IluPrec::apply (y = (LU)^-1 x, factors of H1 or, for
+ * transpose = 1, of H1^T).                                                 */
 int aerof_gpu_prec_apply(aerof_gpu_ctx* ctx, const double* x, double* y, int transpose);
+/* Selects the preconditioner of aerof_gpu_prec_setup / _apply, the GMRES,
+ * Newton and linearised solves: AEROF_PC_JACOBI (default) or
+ * AEROF_PC_ILU0 (IluPrec::setup / apply, KspPrec.C:220-260).               */
+int aerof_gpu_set_preconditioner(aerof_gpu_ctx* ctx, int type);
 /* GmresSolver::solve / solveT (KspSolver.C:351-492, 752-915): right-
  * preconditioned GMRES(krylov) with modified Gram-Schmidt in FP64, x0 = 0.
  * its receives the iteration count (== maxits means saturation, the

@@ -1261,6 +1261,142 @@ int orc_bj_invert(void* h, const double* A, double* Dinv, int fp32) {
   return bad;
 }
 
+// Block ILU(0) preconditioner (IluPrec, KspPrec.C:138-330, fill 0):
+// SparseMat::numericILU and lusol (SparseMatrix.C:353-450) restated on the
+// multicolour node ordering the GPU uses: greedy colouring of the node
+// graph in ascending node order (smallest colour not taken by an already
+// coloured neighbour), rows sorted by (colour, node), columns of each row
+// ascending in that order.  A is the MvpMat layout a[N + 2E][25]; the
+// factored operator is A (transpose = 0) or A^T (1).  fp32 != 0 rounds every
+// stored block to float (PrecScalar = float), arithmetic in double.  y =
+// (LU)^-1 x in the caller's numbering.  Returns the number of singular
+// diagonal blocks, or -1 when ncolor / colour are requested and too small.
+int orc_ilu0(void* h, const double* A, int fp32, int transpose, const double* x, double* y, int* ncolor_out,
+             int* colour_out) {
+  Mesh* m = (Mesh*)h;
+  const int N = m->N;
+  // neighbours ascending (edges are lexicographic: node -> incident edges
+  // ascending gives ascending neighbours)
+  std::vector<int> col(N, -1);
+  int nc = 0;
+  auto nbr = [&](int i, int k) {
+    const int l = m->nodeEdgeIdx[k];
+    return m->edges[2 * l] == i ? m->edges[2 * l + 1] : m->edges[2 * l];
+  };
+  for (int i = 0; i < N; ++i) {
+    std::vector<char> seen(nc + 1, 0);
+    for (int k = m->nodeEdgePtr[i]; k < m->nodeEdgePtr[i + 1]; ++k) {
+      const int c = col[nbr(i, k)];
+      if (c >= 0) seen[c] = 1;
+    }
+    int c = 0;
+    while (seen[c]) ++c;
+    col[i] = c;
+    nc = std::max(nc, c + 1);
+  }
+  if (ncolor_out) *ncolor_out = nc;
+  if (colour_out) std::memcpy(colour_out, col.data(), sizeof(int) * N);
+  std::vector<int> perm, iperm(N);
+  for (int c = 0; c < nc; ++c)
+    for (int i = 0; i < N; ++i)
+      if (col[i] == c) perm.push_back(i);
+  for (int i = 0; i < N; ++i) iperm[perm[i]] = i;
+  // pattern and blocks in colour order
+  std::vector<int> ia(N + 1), ja, ju(N);
+  std::vector<double> a;
+  auto block = [&](int r, int cnode, double* out) {
+    // block (r, cnode) of the operator
+    const double* src;
+    bool tr = transpose != 0;
+    int rr = r, cc = cnode;
+    if (tr) std::swap(rr, cc);
+    if (rr == cc) {
+      src = &A[25 * (size_t)rr];
+    } else {
+      const int lo = std::min(rr, cc), hi = std::max(rr, cc);
+      int l = -1;
+      for (int k = m->nodeEdgePtr[lo]; k < m->nodeEdgePtr[lo + 1]; ++k)
+        if (nbr(lo, k) == hi) l = m->nodeEdgeIdx[k];
+      src = &A[25 * ((size_t)N + 2 * (size_t)l + (rr < cc ? 0 : 1))];
+    }
+    for (int e = 0; e < 25; ++e) {
+      double v = tr ? src[5 * (e % 5) + e / 5] : src[e];
+      out[e] = fp32 ? (double)(float)v : v;
+    }
+  };
+  for (int i = 0; i < N; ++i) {
+    const int r = perm[i];
+    std::vector<int> cols{i};
+    for (int k = m->nodeEdgePtr[r]; k < m->nodeEdgePtr[r + 1]; ++k) cols.push_back(iperm[nbr(r, k)]);
+    std::sort(cols.begin(), cols.end());
+    ia[i] = (int)ja.size();
+    for (int c : cols) {
+      if (c == i) ju[i] = (int)ja.size();
+      ja.push_back(c);
+      a.resize(a.size() + 25);
+      block(r, perm[c], &a[a.size() - 25]);
+    }
+  }
+  ia[N] = (int)ja.size();
+  auto rnd = [&](double v) { return fp32 ? (double)(float)v : v; };
+  // numericILU
+  int bad = 0;
+  std::vector<int> marker(N, -1);
+  for (int i = 0; i < N; ++i) {
+    for (int k = ia[i]; k < ia[i + 1]; ++k) marker[ja[k]] = k;
+    for (int k = ia[i]; k < ju[i]; ++k) {
+      const int l = ja[k];
+      double mult[25];
+      for (int r = 0; r < 5; ++r)
+        for (int c = 0; c < 5; ++c) {
+          double t = 0.0;
+          for (int q = 0; q < 5; ++q) t += a[25 * (size_t)k + 5 * r + q] * a[25 * (size_t)ju[l] + 5 * q + c];
+          mult[5 * r + c] = t;
+        }
+      for (int e = 0; e < 25; ++e) a[25 * (size_t)k + e] = rnd(mult[e]);
+      for (int j = ju[l] + 1; j < ia[l + 1]; ++j) {
+        const int mm = marker[ja[j]];
+        if (mm == -1) continue;
+        for (int r = 0; r < 5; ++r)
+          for (int c = 0; c < 5; ++c) {
+            double t = a[25 * (size_t)mm + 5 * r + c];
+            for (int q = 0; q < 5; ++q) t -= mult[5 * r + q] * a[25 * (size_t)j + 5 * q + c];
+            a[25 * (size_t)mm + 5 * r + c] = rnd(t);
+          }
+      }
+    }
+    for (int k = ia[i]; k < ia[i + 1]; ++k) marker[ja[k]] = -1;
+    double d[25];
+    for (int e = 0; e < 25; ++e) d[e] = a[25 * (size_t)ju[i] + e];
+    if (invert5<double>(d)) ++bad;
+    for (int e = 0; e < 25; ++e) a[25 * (size_t)ju[i] + e] = rnd(d[e]);
+  }
+  // lusol
+  std::vector<double> w(5 * (size_t)N);
+  for (int i = 0; i < N; ++i) {
+    double acc[5];
+    for (int c = 0; c < 5; ++c) acc[c] = x[5 * (size_t)perm[i] + c];
+    for (int k = ia[i]; k < ju[i]; ++k)
+      for (int r = 0; r < 5; ++r)
+        for (int c = 0; c < 5; ++c) acc[r] -= a[25 * (size_t)k + 5 * r + c] * w[5 * (size_t)ja[k] + c];
+    for (int c = 0; c < 5; ++c) w[5 * (size_t)i + c] = acc[c];
+  }
+  for (int i = N - 1; i >= 0; --i) {
+    double acc[5];
+    for (int c = 0; c < 5; ++c) acc[c] = w[5 * (size_t)i + c];
+    for (int k = ju[i] + 1; k < ia[i + 1]; ++k)
+      for (int r = 0; r < 5; ++r)
+        for (int c = 0; c < 5; ++c) acc[r] -= a[25 * (size_t)k + 5 * r + c] * w[5 * (size_t)ja[k] + c];
+    for (int r = 0; r < 5; ++r) {
+      double t = 0.0;
+      for (int c = 0; c < 5; ++c) t += a[25 * (size_t)ju[i] + 5 * r + c] * acc[c];
+      w[5 * (size_t)i + r] = t;
+      y[5 * (size_t)perm[i] + r] = t;
+    }
+  }
+  return bad;
+}
+
 int orc_gmres(void* h, const double* A, const double* Dinv, const double* b, double* x, int numVec,
               int maxits, double eps, int transpose, double* final_res) {
   Mesh* m = (Mesh*)h;

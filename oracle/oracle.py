@@ -64,6 +64,8 @@ def lib():
         L.orc_matvec.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_int]
         L.orc_bj_invert.argtypes = [C.c_void_p, _dp, _dp, C.c_int]
         L.orc_gmres.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.c_int, C.c_int, C.c_double, C.c_int, _dp]
+        L.orc_ilu0.restype = C.c_int
+        L.orc_ilu0.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, _dp, _dp, C.POINTER(C.c_int), _ip]
         L.orc_newton.argtypes = [C.c_void_p, _dp, _dp, C.c_int, C.c_double, C.c_double, C.c_double,
                                  C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
                                  _dp, _ip]
@@ -180,6 +182,15 @@ class Oracle:
         D = np.empty((self.N, 5, 5))
         bad = self.L.orc_bj_invert(self.h, _d(f64(A)), _d(D), int(fp32))
         return D, bad
+
+    def ilu0(self, A, x, fp32=True, transpose=False):
+        """(LU)^-1 x with the block ILU(0) of A (or A^T) in the multicolour
+        ordering; also returns the colour of every node."""
+        x = f64(x); y = np.empty_like(x)
+        nc = C.c_int(0); colour = np.empty(self.N, dtype=np.int32)
+        bad = self.L.orc_ilu0(self.h, _d(f64(A)), int(fp32), int(transpose), _d(x), _d(y), C.byref(nc),
+                              _i(colour))
+        return y, bad, nc.value, colour
 
     def gmres(self, A, Dinv, b, numVec=30, maxits=30, eps=1e-2, transpose=False):
         b = f64(b); x = np.empty_like(b); res = C.c_double(0)

@@ -130,12 +130,22 @@ struct DeviceMesh {
   // multicolour ordering for the block ILU(0) preconditioner: greedy
   // colouring of the node graph (ascending node order, smallest free
   // colour), rows sorted by (colour, node).  ILU pattern in that order:
-  // row i holds its diagonal and its neighbours, columns ascending.
+  // row i holds its diagonal and its neighbours, columns ascending, in a
+  // sliced layout as H1's: each colour's rows in slices of 32 (a slice never
+  // spans two colours), entry k of the slice's rows at block (isp[s] + k).
   int ncolor = 0;
+  size_t ilu_blocks = 0;         // isp[number of slices]
   std::vector<int> h_cptr;       // [ncolor+1] first row of each colour
+  std::vector<int> h_cslice;     // [ncolor+1] first slice of each colour
   DBuf<int> cperm;               // [N] colour-order row -> caller row
-  DBuf<int> ia, ja, ju;          // [N+1], [N+2E] colour-order columns, [N] diagonal position
-  DBuf<int> isrc;                // [N+2E] neighbour slot in the caller row's list, -1 for the diagonal
+  DBuf<int> rlen, rju, rsl;      // [N] entries of the row, diagonal position, slice
+  DBuf<int> sr0, isp;            // [slices] first row, [slices+1] blocks before the slice
+  DBuf<int> jc, jsrc;            // [ilu_blocks*32] column (colour order; -1 padding), neighbour slot (-1 diagonal)
+  // factorisation schedule, as entry ids (block * 32 + lane): per row its
+  // lower entries (A_ik, inverted U_kk) and, per lower entry, the updates
+  // (U_kj, A_ij) of numericILU
+  DBuf<int> lo_ptr, up_ptr;      // [N+1], [lower entries + 1]
+  DBuf<int2> lo, up;
   DBuf<int> sptr;          // [nsl+1] block columns before slice s
   DBuf<int> scol;          // [sptr[nsl] * 32]
   std::vector<int> h_sptr, h_nbr_ptr;

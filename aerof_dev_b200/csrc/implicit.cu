@@ -557,182 +557,193 @@ void matvec_dev(aerof_gpu_ctx* c, const double* p, double* y, int trans) { matve
 // unit lower part, backward solve with the upper part and the inverted
 // diagonal) on rows sorted by colour instead of the reference's RCM order,
 // so the rows of one colour, which are never neighbours, factor and solve
-// in parallel: one launch per colour.  Blocks are stored row after row at a
-// padded stride (28 floats / 26 doubles: 16-byte multiples).
-template <class S> struct IluP { static constexpr int P = sizeof(S) == 4 ? 28 : 26; };
-template <class S>
-__device__ __forceinline__ void ilu_load(const S* __restrict__ a, size_t q, double* v);
-template <>
-__device__ __forceinline__ void ilu_load<float>(const float* __restrict__ a, size_t q, double* v) {
-  const float4* p = reinterpret_cast<const float4*>(a + 28 * q);
-#pragma unroll
-  for (int i = 0; i < 6; ++i) {
-    const float4 t = p[i];
-    v[4 * i] = t.x; v[4 * i + 1] = t.y; v[4 * i + 2] = t.z; v[4 * i + 3] = t.w;
-  }
-  v[24] = a[28 * q + 24];
-}
-template <>
-__device__ __forceinline__ void ilu_load<double>(const double* __restrict__ a, size_t q, double* v) {
-  const double2* p = reinterpret_cast<const double2*>(a + 26 * q);
-#pragma unroll
-  for (int i = 0; i < 12; ++i) {
-    const double2 t = p[i];
-    v[2 * i] = t.x; v[2 * i + 1] = t.y;
-  }
-  v[24] = a[26 * q + 24];
-}
-template <class S>
-__device__ __forceinline__ void ilu_store(S* __restrict__ a, size_t q, const double* v) {
-  constexpr int P = IluP<S>::P;
-#pragma unroll
-  for (int e = 0; e < 25; ++e) a[P * q + e] = (S)v[e];
-}
+// in parallel: one launch per colour.  The factors live in H1's sliced
+// layout (slices of 32 rows of one colour, entry k of a slice as one
+// lane-interleaved block), so a warp reads entry k of its 32 rows as
+// coalesced 16-byte vectors.
 
-// the operator's blocks (tr: transposed) copied into the colour-ordered
-// ILU pattern, thread per row
+// the operator's blocks (tr: transposed) copied into the sliced ILU
+// pattern, thread per colour-order row
 template <class S>
-__global__ void k_ilu_gather(int N, int tr, const int* __restrict__ cperm, const int* __restrict__ ia,
-                             const int* __restrict__ isrc, const int* __restrict__ nbr_ptr,
+__global__ void k_ilu_gather(int N, int tr, const int* __restrict__ cperm, const int* __restrict__ rlen,
+                             const int* __restrict__ rsl, const int* __restrict__ sr0, const int* __restrict__ isp,
+                             const int* __restrict__ jsrc, const int* __restrict__ nbr_ptr,
                              const int* __restrict__ nbr_node, const int* __restrict__ nbr_tpos,
                              const int* __restrict__ sptr, const S* __restrict__ diag, const S* __restrict__ off,
                              S* __restrict__ lu) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const int r = cperm[i];
-  for (int q = ia[i]; q < ia[i + 1]; ++q) {
-    const int k = isrc[q];
-    double v[25], t[25];
-    bool flip = tr != 0;
-    if (k < 0) {
+  const int ws = rsl[i], wl = i - sr0[ws];
+  for (int k = 0; k < rlen[i]; ++k) {
+    const size_t e = (size_t)isp[ws] + k;
+    const int src = jsrc[e * 32 + wl];
+    double v[25];
+    if (src < 0) {
       load_block<S>(diag, sl_dblk(r), r & 31, v);
     } else if (!tr) {
-      load_block<S>(off, sl_blk(sptr, r, k), r & 31, v);
+      load_block<S>(off, sl_blk(sptr, r, src), r & 31, v);
     } else {
-      const int p = nbr_ptr[r] + k;
+      const int p = nbr_ptr[r] + src;
       const int sn = nbr_node[p];
       load_block<S>(off, sl_blk(sptr, sn, nbr_tpos[p] - nbr_ptr[sn]), sn & 31, v);
     }
-    if (flip) {
+    S o[25];
 #pragma unroll
-      for (int e = 0; e < 25; ++e) t[e] = v[5 * (e % 5) + e / 5];
-      ilu_store<S>(lu, (size_t)q, t);
-    } else {
-      ilu_store<S>(lu, (size_t)q, v);
-    }
+    for (int q = 0; q < 25; ++q) o[q] = (S)(tr ? v[5 * (q % 5) + q / 5] : v[q]);
+    store_block_vec<S>(lu, e * 800, wl, o);
   }
 }
 
-// numericILU for the rows [i0, i1) of one colour (all their lower
-// neighbours belong to earlier colours, already factored)
+// numericILU for the rows of one colour (all their lower neighbours belong
+// to earlier colours, already factored), thread per row, following the
+// precomputed schedule: per lower entry the multiplier A_ik U_kk^-1, then
+// the updates A_ij -= mult U_kj of the row's own pattern; finally the
+// diagonal inverted.  Entry e is lane e % 32 of block e / 32.
 template <class S>
-__global__ void k_ilu_factor(int i0, int i1, const int* __restrict__ ia, const int* __restrict__ ja,
-                             const int* __restrict__ ju, S* __restrict__ lu, int* __restrict__ bad) {
-  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= i1) return;
-  const int qd = ju[i], qe = ia[i + 1];
-  for (int k = ia[i]; k < qd; ++k) {
-    const int l = ja[k];
+__device__ __forceinline__ void ilu_ld(const S* __restrict__ lu, int e, double* v) {
+  load_block<S>(lu, (size_t)(e >> 5) * 800, e & 31, v);
+}
+template <class S>
+__device__ __forceinline__ void ilu_st(S* __restrict__ lu, int e, const double* v) {
+  S o[25];
+#pragma unroll
+  for (int q = 0; q < 25; ++q) o[q] = (S)v[q];
+  store_block_vec<S>(lu, (size_t)(e >> 5) * 800, e & 31, o);
+}
+template <class S>
+__global__ void k_ilu_factor(int i0, int cnt, int s0, const int* __restrict__ rju, const int* __restrict__ isp,
+                             const int* __restrict__ lo_ptr, const int2* __restrict__ lo,
+                             const int* __restrict__ up_ptr, const int2* __restrict__ up, S* __restrict__ lu,
+                             int* __restrict__ bad) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cnt) return;
+  const int i = i0 + t;
+  for (int q = lo_ptr[i]; q < lo_ptr[i + 1]; ++q) {
+    const int2 au = lo[q];
     double a[25], u[25], mult[25];
-    ilu_load<S>(lu, (size_t)k, a);
-    ilu_load<S>(lu, (size_t)ju[l], u);
+    ilu_ld<S>(lu, au.x, a);
+    ilu_ld<S>(lu, au.y, u);
 #pragma unroll
     for (int r = 0; r < 5; ++r)
 #pragma unroll
       for (int cc = 0; cc < 5; ++cc) {
-        double t = 0.0;
+        double x = 0.0;
 #pragma unroll
-        for (int x = 0; x < 5; ++x) t += a[5 * r + x] * u[5 * x + cc];
-        mult[5 * r + cc] = t;
+        for (int k = 0; k < 5; ++k) x += a[5 * r + k] * u[5 * k + cc];
+        mult[5 * r + cc] = x;
       }
-    ilu_store<S>(lu, (size_t)k, mult);
-    // a[m] -= mult a[j] for the upper entries j of row l whose column is
-    // in row i (both column lists ascending)
-    int m = k + 1;
-    for (int j = ju[l] + 1; j < ia[l + 1]; ++j) {
-      const int cj = ja[j];
-      while (m < qe && ja[m] < cj) ++m;
-      if (m >= qe) break;
-      if (ja[m] != cj) continue;
-      double b[25], am[25];
-      ilu_load<S>(lu, (size_t)j, b);
-      ilu_load<S>(lu, (size_t)m, am);
+    ilu_st<S>(lu, au.x, mult);
+    for (int p = up_ptr[q]; p < up_ptr[q + 1]; ++p) {
+      const int2 bm = up[p];
+      double bb[25], am[25];
+      ilu_ld<S>(lu, bm.x, bb);
+      ilu_ld<S>(lu, bm.y, am);
 #pragma unroll
       for (int r = 0; r < 5; ++r)
 #pragma unroll
         for (int cc = 0; cc < 5; ++cc) {
-          double t = am[5 * r + cc];
+          double x = am[5 * r + cc];
 #pragma unroll
-          for (int x = 0; x < 5; ++x) t -= mult[5 * r + x] * b[5 * x + cc];
-          am[5 * r + cc] = t;
+          for (int k = 0; k < 5; ++k) x -= mult[5 * r + k] * bb[5 * k + cc];
+          am[5 * r + cc] = x;
         }
-      ilu_store<S>(lu, (size_t)m, am);
+      ilu_st<S>(lu, bm.y, am);
     }
   }
-  double d[25];
-  ilu_load<S>(lu, (size_t)qd, d);
-  if (invert5<double>(d)) atomicAdd(bad, 1);
-  ilu_store<S>(lu, (size_t)qd, d);
+  const int ed = (isp[s0 + (t >> 5)] + rju[i]) * 32 + (t & 31);
+  double dg[25];
+  ilu_ld<S>(lu, ed, dg);
+  if (invert5<double>(dg)) atomicAdd(bad, 1);
+  ilu_st<S>(lu, ed, dg);
 }
 
-// lusol forward sweep for one colour: w_i = x_(perm i) - sum_{k<i} L_ik w_k
-template <class S, class TI>
-__global__ void k_ilu_fwd(int i0, int i1, const int* __restrict__ cperm, const int* __restrict__ ia,
-                          const int* __restrict__ ja, const int* __restrict__ ju, const S* __restrict__ lu,
+// lusol sweeps for one colour, L lanes per row (entries r, r + L, ... of
+// the row, fixed xor-tree lane sum): row t of the colour is in slice
+// s0 + t / 32 at lane t % 32.
+// Forward: w_i = x_(perm i) - sum_{k<i} L_ik w_k.
+template <int L, class S, class TI>
+__global__ void k_ilu_fwd(int i0, int cnt, int s0, const int* __restrict__ cperm, const int* __restrict__ rju,
+                          const int* __restrict__ isp, const int* __restrict__ jc, const S* __restrict__ lu,
                           const TI* __restrict__ x, double* __restrict__ w) {
-  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= i1) return;
-  const size_t r = (size_t)cperm[i];
-  double acc[5];
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = g / L, sub = g % L;
+  const bool act = t < cnt;
+  double acc[5] = {0, 0, 0, 0, 0};
+  if (act) {
+    const int lane = t & 31;
+    const size_t base = (size_t)isp[s0 + (t >> 5)];
+    const int d = rju[i0 + t];
+    for (int k = sub; k < d; k += L) {
+      double a[25];
+      load_block<S>(lu, (base + k) * 800, lane, a);
+      const double* wk = w + 5 * (size_t)jc[(base + k) * 32 + lane];
+      double v[5];
 #pragma unroll
-  for (int c = 0; c < 5; ++c) acc[c] = (double)x[5 * r + c];
-  for (int k = ia[i]; k < ju[i]; ++k) {
-    double a[25];
-    ilu_load<S>(lu, (size_t)k, a);
-    const double* wk = w + 5 * (size_t)ja[k];
-    double v[5];
+      for (int c = 0; c < 5; ++c) v[c] = wk[c];
 #pragma unroll
-    for (int c = 0; c < 5; ++c) v[c] = wk[c];
+      for (int rr = 0; rr < 5; ++rr)
 #pragma unroll
-    for (int rr = 0; rr < 5; ++rr)
-#pragma unroll
-      for (int c = 0; c < 5; ++c) acc[rr] -= a[5 * rr + c] * v[c];
+        for (int c = 0; c < 5; ++c) acc[rr] -= a[5 * rr + c] * v[c];
+    }
   }
 #pragma unroll
-  for (int c = 0; c < 5; ++c) w[5 * (size_t)i + c] = acc[c];
+  for (int o = 1; o < L; o <<= 1)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+  if (!act || sub != 0) return;
+  const int i = i0 + t;
+  const size_t r = (size_t)cperm[i];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) w[5 * (size_t)i + c] = (double)x[5 * r + c] + acc[c];
 }
 
-// lusol backward sweep for one colour: w_i = U_ii^-1 (w_i - sum_{j>i}
-// U_ij w_j), written to z in the caller's numbering as well
-template <class S, class TO>
-__global__ void k_ilu_bwd(int i0, int i1, const int* __restrict__ cperm, const int* __restrict__ ia,
-                          const int* __restrict__ ja, const int* __restrict__ ju, const S* __restrict__ lu,
-                          double* __restrict__ w, TO* __restrict__ z) {
-  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= i1) return;
-  double acc[5];
+// Backward: w_i = U_ii^-1 (w_i - sum_{j>i} U_ij w_j), also written to z in
+// the caller's numbering.
+template <int L, class S, class TO>
+__global__ void k_ilu_bwd(int i0, int cnt, int s0, const int* __restrict__ cperm, const int* __restrict__ rlen,
+                          const int* __restrict__ rju, const int* __restrict__ isp, const int* __restrict__ jc,
+                          const S* __restrict__ lu, double* __restrict__ w, TO* __restrict__ z) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = g / L, sub = g % L;
+  const bool act = t < cnt;
+  double acc[5] = {0, 0, 0, 0, 0};
+  int lane = 0, d = 0;
+  size_t base = 0;
+  if (act) {
+    lane = t & 31;
+    base = (size_t)isp[s0 + (t >> 5)];
+    d = rju[i0 + t];
+    const int len = rlen[i0 + t];
+    for (int k = d + 1 + sub; k < len; k += L) {
+      double a[25];
+      load_block<S>(lu, (base + k) * 800, lane, a);
+      const double* wk = w + 5 * (size_t)jc[(base + k) * 32 + lane];
+      double v[5];
 #pragma unroll
-  for (int c = 0; c < 5; ++c) acc[c] = w[5 * (size_t)i + c];
-  for (int k = ju[i] + 1; k < ia[i + 1]; ++k) {
-    double a[25];
-    ilu_load<S>(lu, (size_t)k, a);
-    const double* wk = w + 5 * (size_t)ja[k];
-    double v[5];
+      for (int c = 0; c < 5; ++c) v[c] = wk[c];
 #pragma unroll
-    for (int c = 0; c < 5; ++c) v[c] = wk[c];
+      for (int rr = 0; rr < 5; ++rr)
 #pragma unroll
-    for (int rr = 0; rr < 5; ++rr)
-#pragma unroll
-      for (int c = 0; c < 5; ++c) acc[rr] -= a[5 * rr + c] * v[c];
+        for (int c = 0; c < 5; ++c) acc[rr] -= a[5 * rr + c] * v[c];
+    }
   }
-  double d[25], res[5];
-  ilu_load<S>(lu, (size_t)ju[i], d);
+#pragma unroll
+  for (int o = 1; o < L; o <<= 1)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+  if (!act || sub != 0) return;
+  const int i = i0 + t;
+#pragma unroll
+  for (int c = 0; c < 5; ++c) acc[c] += w[5 * (size_t)i + c];
+  double dg[25], res[5];
+  load_block<S>(lu, (base + d) * 800, lane, dg);
 #pragma unroll
   for (int rr = 0; rr < 5; ++rr) {
-    double t = 0.0;
+    double x = 0.0;
 #pragma unroll
-    for (int c = 0; c < 5; ++c) t += d[5 * rr + c] * acc[c];
-    res[rr] = t;
+    for (int c = 0; c < 5; ++c) x += dg[5 * rr + c] * acc[c];
+    res[rr] = x;
   }
   const size_t r = (size_t)cperm[i];
 #pragma unroll
@@ -751,24 +762,24 @@ static int ilu_setup(aerof_gpu_ctx* c, int tr) {
   c->s.counters.ensure(8);
   int* bad = c->s.counters.p + 5;
   AEROF_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
-  const size_t nnz = (size_t)m.N + 2 * (size_t)m.E;
   const int gn = grid_for(m.N, kIB);
   auto run = [&](auto* lu, auto* diag, auto* off) {
     using S = std::remove_pointer_t<decltype(lu)>;
-    k_ilu_gather<S><<<gn, kIB, 0, s>>>(m.N, tr, m.cperm.p, m.ia.p, m.isrc.p, m.nbr_ptr.p, m.nbr_node.p,
-                                       m.nbr_tpos.p, m.sptr.p, diag, off, lu);
+    k_ilu_gather<S><<<gn, kIB, 0, s>>>(m.N, tr, m.cperm.p, m.rlen.p, m.rsl.p, m.sr0.p, m.isp.p, m.jsrc.p,
+                                       m.nbr_ptr.p, m.nbr_node.p, m.nbr_tpos.p, m.sptr.p, diag, off, lu);
     AEROF_LAUNCH_CHECK();
     for (int col = 0; col < m.ncolor; ++col) {
-      const int i0 = m.h_cptr[col], i1 = m.h_cptr[col + 1];
-      k_ilu_factor<S><<<grid_for(i1 - i0, kIB), kIB, 0, s>>>(i0, i1, m.ia.p, m.ja.p, m.ju.p, lu, bad);
+      const int i0 = m.h_cptr[col], cnt = m.h_cptr[col + 1] - i0;
+      k_ilu_factor<S><<<grid_for(cnt, kIB), kIB, 0, s>>>(i0, cnt, m.h_cslice[col], m.rju.p, m.isp.p, m.lo_ptr.p,
+                                                         m.lo.p, m.up_ptr.p, m.up.p, lu, bad);
       AEROF_LAUNCH_CHECK();
     }
   };
   if (J.precision == AEROF_PREC_FP32) {
-    J.ilu32.ensure(28 * nnz);
+    J.ilu32.ensure(800 * m.ilu_blocks);
     run(J.ilu32.p, J.diag32.p, J.off32.p);
   } else {
-    J.ilu64.ensure(26 * nnz);
+    J.ilu64.ensure(800 * m.ilu_blocks);
     run(J.ilu64.p, J.diag64.p, J.off64.p);
   }
   int h = 0;
@@ -788,14 +799,18 @@ static void ilu_apply(aerof_gpu_ctx* c, const TI* x, TO* z) {
   double* w = J.iluw.p;
   auto run = [&](const auto* lu) {
     using S = std::remove_const_t<std::remove_pointer_t<decltype(lu)>>;
+    constexpr int L = 4;  // lanes per row
     for (int col = 0; col < m.ncolor; ++col) {
-      const int i0 = m.h_cptr[col], i1 = m.h_cptr[col + 1];
-      k_ilu_fwd<S, TI><<<grid_for(i1 - i0, kIB), kIB, 0, s>>>(i0, i1, m.cperm.p, m.ia.p, m.ja.p, m.ju.p, lu, x, w);
+      const int i0 = m.h_cptr[col], cnt = m.h_cptr[col + 1] - i0;
+      k_ilu_fwd<L, S, TI><<<grid_for((size_t)L * cnt, kIB), kIB, 0, s>>>(i0, cnt, m.h_cslice[col], m.cperm.p,
+                                                                         m.rju.p, m.isp.p, m.jc.p, lu, x, w);
       AEROF_LAUNCH_CHECK();
     }
     for (int col = m.ncolor - 1; col >= 0; --col) {
-      const int i0 = m.h_cptr[col], i1 = m.h_cptr[col + 1];
-      k_ilu_bwd<S, TO><<<grid_for(i1 - i0, kIB), kIB, 0, s>>>(i0, i1, m.cperm.p, m.ia.p, m.ja.p, m.ju.p, lu, w, z);
+      const int i0 = m.h_cptr[col], cnt = m.h_cptr[col + 1] - i0;
+      k_ilu_bwd<L, S, TO><<<grid_for((size_t)L * cnt, kIB), kIB, 0, s>>>(i0, cnt, m.h_cslice[col], m.cperm.p,
+                                                                         m.rlen.p, m.rju.p, m.isp.p, m.jc.p, lu, w,
+                                                                         z);
       AEROF_LAUNCH_CHECK();
     }
   };

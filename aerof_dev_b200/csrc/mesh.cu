@@ -557,32 +557,81 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
         for (int r = 0; r < N; ++r) perm[fill[col[r]]++] = r;
       }
       for (int i = 0; i < N; ++i) iperm[perm[i]] = i;
-      const size_t nnz = (size_t)N + h.nbr_ptr[N];
-      std::vector<int> ia(N + 1), ja(nnz), isrc(nnz), ju(N);
-      std::vector<std::pair<int, int>> row;
-      size_t q0 = 0;
+      // slices of 32 rows inside each colour
+      std::vector<int> cslice(nc + 1, 0);
+      for (int c0 = 0; c0 < nc; ++c0) cslice[c0 + 1] = cslice[c0] + (cptr[c0 + 1] - cptr[c0] + 31) / 32;
+      const int nsl = cslice[nc];
+      std::vector<int> rsl(N), sr0(std::max(nsl, 1)), rlen(N), rju(N), isp(nsl + 1, 0);
+      for (int c0 = 0; c0 < nc; ++c0)
+        for (int t = 0; t < cptr[c0 + 1] - cptr[c0]; ++t) {
+          const int sl = cslice[c0] + t / 32;
+          rsl[cptr[c0] + t] = sl;
+          if (t % 32 == 0) sr0[sl] = cptr[c0] + t;
+        }
+      // rows: diagonal + neighbours in colour order, ascending
+      std::vector<std::vector<std::pair<int, int>>> rows(N);
       for (int i = 0; i < N; ++i) {
         const int r = perm[i];
-        row.clear();
+        auto& row = rows[i];
         row.emplace_back(i, -1);
         for (int q = h.nbr_ptr[r]; q < h.nbr_ptr[r + 1]; ++q) row.emplace_back(iperm[h.nbr_node[q]], q - h.nbr_ptr[r]);
         std::sort(row.begin(), row.end());
-        ia[i] = (int)q0;
-        for (const auto& e : row) {
-          if (e.second < 0) ju[i] = (int)q0;
-          ja[q0] = e.first;
-          isrc[q0] = e.second;
-          ++q0;
+        rlen[i] = (int)row.size();
+        for (int k = 0; k < rlen[i]; ++k)
+          if (row[k].second < 0) rju[i] = k;
+      }
+      for (int sl = 0; sl < nsl; ++sl) {
+        int kmax = 0;
+        for (int i = sr0[sl]; i < N && rsl[i] == sl; ++i) kmax = std::max(kmax, rlen[i]);
+        isp[sl + 1] = isp[sl] + kmax;
+      }
+      const size_t nb = (size_t)isp[nsl];
+      std::vector<int> jc(nb * 32, -1), jsrc(nb * 32, -2);
+      for (int i = 0; i < N; ++i) {
+        const int sl = rsl[i], lane = i - sr0[sl];
+        for (int k = 0; k < rlen[i]; ++k) {
+          jc[((size_t)isp[sl] + k) * 32 + lane] = rows[i][k].first;
+          jsrc[((size_t)isp[sl] + k) * 32 + lane] = rows[i][k].second;
         }
       }
-      ia[N] = (int)q0;
+      // numericILU schedule: entry id of (row i, position k)
+      auto eid = [&](int i, int k) { return (isp[rsl[i]] + k) * 32 + (i - sr0[rsl[i]]); };
+      std::vector<int> lo_ptr(N + 1, 0), up_ptr(1, 0);
+      std::vector<int2> lo, up;
+      for (int i = 0; i < N; ++i) {
+        const auto& ri = rows[i];
+        for (int k = 0; k < rju[i]; ++k) {
+          const int l = ri[k].first;
+          const auto& rl = rows[l];
+          lo.push_back(make_int2(eid(i, k), eid(l, rju[l])));
+          int mm = k + 1;
+          for (int j = rju[l] + 1; j < rlen[l]; ++j) {
+            while (mm < rlen[i] && ri[mm].first < rl[j].first) ++mm;
+            if (mm >= rlen[i]) break;
+            if (ri[mm].first == rl[j].first) up.push_back(make_int2(eid(l, j), eid(i, mm)));
+          }
+          up_ptr.push_back((int)up.size());
+        }
+        lo_ptr[i + 1] = (int)lo.size();
+      }
+      if (lo.empty()) lo.push_back(make_int2(0, 0));
+      if (up.empty()) up.push_back(make_int2(0, 0));
+      m.lo_ptr.upload(lo_ptr.data(), lo_ptr.size(), s);
+      m.up_ptr.upload(up_ptr.data(), up_ptr.size(), s);
+      m.lo.upload(lo.data(), lo.size(), s);
+      m.up.upload(up.data(), up.size(), s);
       m.ncolor = nc;
+      m.ilu_blocks = nb;
       m.h_cptr.swap(cptr);
+      m.h_cslice.swap(cslice);
       m.cperm.upload(perm.data(), (size_t)N, s);
-      m.ia.upload(ia.data(), ia.size(), s);
-      m.ja.upload(ja.data(), ja.size(), s);
-      m.ju.upload(ju.data(), ju.size(), s);
-      m.isrc.upload(isrc.data(), isrc.size(), s);
+      m.rlen.upload(rlen.data(), (size_t)N, s);
+      m.rju.upload(rju.data(), (size_t)N, s);
+      m.rsl.upload(rsl.data(), (size_t)N, s);
+      m.sr0.upload(sr0.data(), sr0.size(), s);
+      m.isp.upload(isp.data(), isp.size(), s);
+      m.jc.upload(jc.data(), jc.size(), s);
+      m.jsrc.upload(jsrc.data(), jsrc.size(), s);
       AEROF_CUDA(cudaStreamSynchronize(s));
     }
     // sliced layout of the implicit operator

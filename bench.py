@@ -457,13 +457,13 @@ def run_sensitivities(args):
     Uh = U.cpu().numpy()
     torch.cuda.synchronize()
     t1 = time.perf_counter()
-    gb, binfo = S.direct_gradient_batch(ctx, Uh, X, F, modes)
+    gb, binfo = S.direct_gradient_batch(ctx, Uh, X, F, modes, inner_its=args.inner_its)
     batch_s = time.perf_counter() - t1
     t1 = time.perf_counter()
-    g1, info1 = S.direct_gradient(ctx, Uh, X, F, modes[:1])
+    g1, info1 = S.direct_gradient(ctx, Uh, X, F, modes[:1], inner_its=args.inner_its)
     single_s = time.perf_counter() - t1
     t1 = time.perf_counter()
-    ga, ainfo = S.adjoint_gradient(ctx, Uh, X, F, modes)
+    ga, ainfo = S.adjoint_gradient(ctx, Uh, X, F, modes, inner_its=args.inner_its)
     adj_s = time.perf_counter() - t1
     nfd = min(args.fd_modes, args.modes)
     g6 = S.fd_gradient(ctx, Uh, X, F, modes[:nfd], h=1e-6, tol=1e-10, max_steps=args.max_steps) if nfd else None
@@ -474,7 +474,7 @@ def run_sensitivities(args):
             "config": {"workload": f"batched direct shape sensitivities, {args.n}^3 jittered mesh with a base bump "
                                    f"N={s['N']} E={s['E']}, {args.modes} Gaussian-bump modes, Mach 0.8",
                        "reconstruction": {1: "constant", 2: "van Albada", 3: "linear"}[args.rec],
-                       "preconditioner": args.pc},
+                       "preconditioner": args.pc, "inner_its": args.inner_its},
             "batch_s": batch_s, "batch": binfo, "single_rhs_matrix_free_s": single_s,
             "single_rhs_its": info1["direct_its"], "converge_s": conv_s, "adjoint_gradient_s": adj_s,
             "adjoint": ainfo, "grad_batched_direct": gb.tolist(), "grad_adjoint": ga.tolist(),
@@ -557,6 +557,8 @@ def main():
     ap.add_argument("--fd-modes", type=int, default=4)
     ap.add_argument("--rec", type=int, choices=[1, 2, 3], default=2,
                     help="adjoint workload reconstruction: 1 constant, 2 van Albada, 3 linear")
+    ap.add_argument("--inner-its", type=int, default=20,
+                    help="inner FP32 GMRES iterations of the sensitivity solves")
     ap.add_argument("--pc", choices=["jacobi", "ilu"], default="jacobi",
                     help="preconditioner of the Newton and sensitivity workloads")
     ap.add_argument("--kernel", choices=["blocked", "edge"], default="blocked",

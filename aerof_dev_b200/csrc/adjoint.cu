@@ -912,15 +912,18 @@ static size_t lsq_blocked_smem(const DeviceMesh& m) {
 // blocked organisation.  fj: stored face Jacobians, or null for forward mode
 // per face (needs P at dU).  False (nothing launched) when the staging does
 // not fit in shared memory.
-static bool assemble_lsq_blocked(aerof_gpu_ctx* c, const double* dU, const double* dw, const double* fj, int rec,
-                                 double* dout) {
+static bool lsq_blocked_fits(const DeviceMesh& m) {
+  const int L = kLsqThreads / m.NB;
+  return lsq_blocked_smem(m) <= 200 * 1024 && L >= 2 && L <= 8 && L * m.NB == kLsqThreads;
+}
+
+// node assembly of a blocked reverse sweep into gV2 / gG2 (blocked
+// numbering), with the faces
+static void assemble_blocked(aerof_gpu_ctx* c, const double* dw, const double* fj) {
   DeviceMesh& m = c->mesh;
   AdjWork& a = c->adj;
   cudaStream_t s = c->stream;
   const Gas g = make_gas(c->cfg.gamma);
-  const size_t smem = lsq_blocked_smem(m);
-  const int L = kLsqThreads / m.NB;
-  if (smem > 200 * 1024 || L < 2 || L > 8 || L * m.NB != kLsqThreads) return false;
   a.gV2.ensure(5 * (size_t)m.N);
   a.gG2.ensure(16 * (size_t)m.N);
   k_a_nodes_b<<<grid_for(m.N, kAB), kAB, 0, s>>>(m.N, m.n2o.p, a.gVp.p, a.gGp.p, m.xin_ptr.p, a.spill.p, m.brow.p,
@@ -931,6 +934,16 @@ static bool assemble_lsq_blocked(aerof_gpu_ctx* c, const double* dU, const doubl
                                                        m.nf_face.p, m.fcode.p, m.fnrm.p, m.P.p, dw, m.vol.p, a.gV2.p);
     AEROF_LAUNCH_CHECK();
   }
+}
+
+// LSQ transpose and (dV/dU)^T at dU of gV2 / gG2 into dout
+static void lsq_transpose_blocked(aerof_gpu_ctx* c, const double* dU, int rec, double* dout) {
+  DeviceMesh& m = c->mesh;
+  AdjWork& a = c->adj;
+  cudaStream_t s = c->stream;
+  const Gas g = make_gas(c->cfg.gamma);
+  const size_t smem = lsq_blocked_smem(m);
+  const int L = kLsqThreads / m.NB;
   auto go = [&](auto kern) {
     AEROF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<m.nblk, kLsqThreads, smem, s>>>(m.N, m.NB, g, rec, m.n2o.p, dU, m.P2.p, m.W2.p, m.nb2_ptr.p, m.lnb.p,
@@ -940,6 +953,18 @@ static bool assemble_lsq_blocked(aerof_gpu_ctx* c, const double* dU, const doubl
   if (L == 8) go(k_a_lsq_blocked<8>);
   else if (L == 4) go(k_a_lsq_blocked<4>);
   else go(k_a_lsq_blocked<2>);
+}
+
+// After a blocked edge sweep (gVp, gGp, spill current): node assembly with
+// the faces, the LSQ transpose and (dV/dU)^T at dU into dout, all in the
+// blocked organisation.  fj: stored face Jacobians, or null for forward mode
+// per face (needs P at dU).  False (nothing launched) when the staging does
+// not fit in shared memory.
+static bool assemble_lsq_blocked(aerof_gpu_ctx* c, const double* dU, const double* dw, const double* fj, int rec,
+                                 double* dout) {
+  if (!lsq_blocked_fits(c->mesh)) return false;
+  assemble_blocked(c, dw, fj);
+  lsq_transpose_blocked(c, dU, rec, dout);
   return true;
 }
 
@@ -1001,7 +1026,7 @@ void vjp_dev(aerof_gpu_ctx* c, const double* dU, const double* dw, double* dout)
   a.gG.ensure(16 * (size_t)m.N);
   if (reverse_blocked_fits(m)) {
     prim_grad_blocked_dev(c, dU, nullptr);
-    if (lsq_blocked_smem(m) <= 200 * 1024 && kLsqThreads % m.NB == 0) {
+    if (lsq_blocked_fits(m)) {
       // edges, then assembly, faces, LSQ transpose and (dV/dU)^T in the
       // blocked organisation
       reverse_sweep_blocked(c, dw, false, false);
@@ -1081,14 +1106,15 @@ __global__ void k_a_face_normal(int F, Gas g, const double* __restrict__ Ub0, co
 __global__ void __launch_bounds__(256) k_a_lsq_x(int N, const double* __restrict__ P, const double* __restrict__ lsqR,
                                                  const double* __restrict__ lsqW, const int* __restrict__ nbr_ptr,
                                                  const int* __restrict__ nbr_node, const double* __restrict__ gG,
-                                                 double* __restrict__ gd) {
+                                                 const int* __restrict__ o2n, double* __restrict__ gd) {
   // four lanes per node share its neighbours (lane, lane+4, ...) in both passes;
-  // the cotangent of the node's constants is summed in a fixed xor tree
+  // the cotangent of the node's constants is summed in a fixed xor tree.
+  // gG is in the caller's numbering, or in the blocked one when o2n is given
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = min(t >> 2, N - 1), lane = t & 3;
   const bool act = (t >> 2) < N;
   const double* pi = P + 8 * (size_t)i;
-  const double* gg = gG + 16 * (size_t)i;
+  const double* gg = gG + 16 * (size_t)(o2n ? o2n[i] : i);
   double w[6], r[6];
 #pragma unroll
   for (int k = 0; k < 6; ++k) { w[k] = lsqW[(size_t)k * N + i]; r[k] = lsqR[(size_t)k * N + i]; }
@@ -1340,9 +1366,15 @@ void dRdX_T_dev(aerof_gpu_ctx* c, const double* dU, const double* dlam, double* 
   AEROF_LAUNCH_CHECK();
   k_a_gvol<<<gn, kAB, 0, s>>>(m.N, dlam, R, m.vol.p, a.gvol.p);
   AEROF_LAUNCH_CHECK();
+  // blocked organisation: node assembly and LSQ transposes read the
+  // blocked-numbered cotangents
+  const bool blk = reverse_blocked_fits(m) && lsq_blocked_fits(m);
   if (reverse_blocked_fits(m)) {
-    prim_grad_blocked_dev(c, dU, nullptr);
-    reverse_sweep_blocked(c, dlam, true);
+    // the residual above leaves P2 / G2 of dU when it ran blocked and
+    // untagged
+    if (!c->s.p2g2_valid) prim_grad_blocked_dev(c, dU, nullptr);
+    reverse_sweep_blocked(c, dlam, true, !blk);
+    if (blk) assemble_blocked(c, dlam, nullptr);
   } else {
     c->s.G.ensure(16 * (size_t)m.N);
     if (rec != AEROF_REC_CONSTANT) gradients_dev(c);
@@ -1362,10 +1394,13 @@ void dRdX_T_dev(aerof_gpu_ctx* c, const double* dU, const double* dlam, double* 
   }
   if (rec != AEROF_REC_CONSTANT) {
     k_a_lsq_x<<<grid_for(4 * (size_t)m.N, kAB), kAB, 0, s>>>(m.N, m.P.p, m.lsqR.p, m.lsqW.p, m.nbr_ptr.p,
-                                                             m.nbr_node.p, a.gG.p, a.gd.p);
+                                                             m.nbr_node.p, blk ? a.gG2.p : a.gG.p,
+                                                             blk ? m.o2n.p : nullptr, a.gd.p);
     AEROF_LAUNCH_CHECK();
   }
-  if (dJT) {
+  if (dJT && blk) {
+    lsq_transpose_blocked(c, dU, rec, dJT);
+  } else if (dJT) {
     k_a_lsq_prim<<<grid_for(4 * (size_t)m.N, kAB), kAB, 0, s>>>(m.N, g, rec, dU, m.P.p, m.lsqW.p, m.nbr_ptr.p,
                                                                 m.nbr_node.p, a.gV.p, a.gG.p, dJT);
     AEROF_LAUNCH_CHECK();

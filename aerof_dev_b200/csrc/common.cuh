@@ -185,6 +185,9 @@ struct Scratch {
   DBuf<int> tag;           // [N] failsafe tags
   DBuf<int> counters;      // [8] device counters
   DBuf<double> red;        // reduction partials
+  // set by the blocked residual: P2 / G2 hold the untagged primitive
+  // records and gradients of the state it evaluated
+  bool p2g2_valid = false;
   DBuf<double> redout;     // reduction results
 };
 

@@ -1003,9 +1003,11 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
     AEROF_CUDA(cudaMemcpyAsync(&bad, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
     AEROF_CUDA(cudaStreamSynchronize(s));
   }
+  c->s.p2g2_valid = true;
   if (bad && c->cfg.failsafe && rec != AEROF_REC_CONSTANT) {
     TimerScope t(c, AEROF_T_FV_TERM);
     prim_grad_blocked_dev(c, dU, c->s.tag.p);
+    c->s.p2g2_valid = false;
     fv(0, cnt + 1);
   }
   {
@@ -1024,6 +1026,7 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
 
 int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
   DeviceMesh& m = c->mesh;
+  c->s.p2g2_valid = false;
   if (c->cfg.residual_kernel == AEROF_KERNEL_BLOCKED && fv_blocked_smem(m) <= 200 * 1024)
     return residual_blocked_dev(c, dU, dR, sync);
   const Gas g = make_gas(c->cfg.gamma);

@@ -428,7 +428,9 @@ class MatVecProdH1:
 
 
 class JacobiPrec:
-    """Block-Jacobi preconditioner (``JacobiPrec``, KspPrec.C:9-124)."""
+    """Block-Jacobi preconditioner (``JacobiPrec``, KspPrec.C:9-124); with
+    ``Context.set_preconditioner(PC_ILU0)`` the same calls set up and apply
+    the block ILU(0) preconditioner (``IluPrec``, KspPrec.C:138-330)."""
 
     def __init__(self, ctx: Context):
         self.ctx = ctx
@@ -469,7 +471,8 @@ class GmresSolver:
 
 
 class ImplicitSteadySolver:
-    """Pseudo-transient backward-Euler Newton with GMRES + block-Jacobi."""
+    """Pseudo-transient backward-Euler Newton with GMRES, preconditioned by
+    block-Jacobi or block ILU(0) (Context.set_preconditioner)."""
 
     def __init__(self, ctx: Context, precision: int = PREC_FP32, cfl0: float = 10.0, cfl_min: float = 0.0,
                  cfl_max: float = 1e4, ser: float = 0.7, ksp_eps: float = 1e-2, krylov: int = 30,
@@ -579,3 +582,6 @@ class Sensitivity:
         ctx._check(ctx.L.aerof_gpu_linearized_solve(ctx.h, u.ptr, bb.ptr, xx.ptr, krylov, maxits, eps,
                                                     int(transpose), int(inner_its), C.byref(its), C.byref(res)))
         return xx.obj, its.value, res.value
+
+
+IluPrec = JacobiPrec

@@ -215,6 +215,12 @@ struct Implicit {
   DBuf<float> ilu32;
   // flexible GMRES on the exact linearisation (outer FP64 vectors)
   DBuf<double> fV, fZ, fw, fr, fh;
+  // lockstep solves of several right-hand sides: outer (FP64) and inner
+  // (FP32) bases and work vectors, Hessenberg columns, pointer arrays of the
+  // batched kernels
+  DBuf<double> bV, bZ, bw, br, bh, ih, bB, bX;
+  DBuf<float> iV, iw, ir, iz;
+  DBuf<unsigned long long> bptr, iptr;
 };
 
 // Dual-number work arrays of the forward-mode linearisation.

@@ -313,6 +313,66 @@ __global__ void __launch_bounds__(256) k_spmv(int N, const int* __restrict__ nbr
   for (int k = 0; k < 5; ++k) y[5 * (size_t)r + k] = (TO)acc[k];
 }
 
+// y_q = A p_q (or A^T p_q) for the R vectors of a batch (pointer arrays):
+// every block is read once per group of RB vectors and applied to each in
+// k_spmv's per-row order (diagonal block, then the neighbours ascending).
+template <class S, bool TRANS, class TV, int RB>
+__global__ void __launch_bounds__(256) k_spmv_batch(int N, int R, const int* __restrict__ nbr_ptr,
+                                                    const int* __restrict__ nbr_tpos, const int* __restrict__ sptr,
+                                                    const int* __restrict__ scol, const S* __restrict__ diag,
+                                                    const S* __restrict__ off, const TV* const* __restrict__ P,
+                                                    TV* const* __restrict__ Y) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= N) return;
+  const int p0 = nbr_ptr[r], cnt = nbr_ptr[r + 1] - p0;
+  const size_t cb = (size_t)sptr[r >> 5] * 32 + (r & 31);
+  for (int q0 = 0; q0 < R; q0 += RB) {
+    double acc[RB][5];
+#pragma unroll
+    for (int q = 0; q < RB; ++q)
+#pragma unroll
+      for (int k = 0; k < 5; ++k) acc[q][k] = 0.0;
+    auto apply = [&](const double* av, int col, bool tr) {
+#pragma unroll
+      for (int q = 0; q < RB; ++q) {
+        if (q0 + q >= R) break;
+        const TV* x = P[q0 + q] + 5 * (size_t)col;
+        double xv[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) xv[k] = (double)x[k];
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr) {
+          double t = (tr ? av[rr] : av[5 * rr]) * xv[0];
+#pragma unroll
+          for (int k = 1; k < 5; ++k) t += (tr ? av[5 * k + rr] : av[5 * rr + k]) * xv[k];
+          acc[q][rr] += t;
+        }
+      }
+    };
+    double av[25];
+    load_block<S>(diag, sl_dblk(r), r & 31, av);
+    apply(av, r, TRANS);
+    for (int k = 0; k < cnt; ++k) {
+      const int sn = scol[cb + (size_t)32 * k];
+      if (!TRANS) {
+        load_block<S>(off, sl_blk(sptr, r, k), r & 31, av);
+        apply(av, sn, false);
+      } else {
+        const int kt = nbr_tpos[p0 + k] - nbr_ptr[sn];
+        load_block<S>(off, sl_blk(sptr, sn, kt), sn & 31, av);
+        apply(av, sn, true);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < RB; ++q) {
+      if (q0 + q >= R) break;
+      TV* y = Y[q0 + q] + 5 * (size_t)r;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) y[k] = (TV)acc[q][k];
+    }
+  }
+}
+
 // Block-Jacobi set-up (JacobiPrec::setup -> DiagMat::invert, DiagMatrix.C:
 // 44-80): blocks with a zero diagonal entry are left as they are (as the
 // reference does); a zero pivot counts into bad[0].
@@ -753,6 +813,126 @@ __global__ void k_ilu_bwd(int i0, int cnt, int s0, const int* __restrict__ cperm
   }
 }
 
+// The same sweeps for R vectors at once (pointer arrays X, Z; work vectors
+// W + q * ldw): every factor block is read once per group of RB vectors.
+template <int L, int RB, class S, class TI>
+__global__ void k_ilu_fwd_b(int i0, int cnt, int s0, int R, const int* __restrict__ cperm,
+                            const int* __restrict__ rju, const int* __restrict__ isp, const int* __restrict__ jc,
+                            const S* __restrict__ lu, const TI* const* __restrict__ X, double* __restrict__ W,
+                            size_t ldw) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = g / L, sub = g % L;
+  const bool act = t < cnt;
+  const int lane = t & 31;
+  const size_t base = act ? (size_t)isp[s0 + (t >> 5)] : 0;
+  const int d = act ? rju[i0 + t] : 0;
+  for (int q0 = 0; q0 < R; q0 += RB) {
+    double acc[RB][5];
+#pragma unroll
+    for (int q = 0; q < RB; ++q)
+#pragma unroll
+      for (int c = 0; c < 5; ++c) acc[q][c] = 0.0;
+    for (int k = sub; k < d; k += L) {
+      double a[25];
+      load_block<S>(lu, (base + k) * 800, lane, a);
+      const size_t col = 5 * (size_t)jc[(base + k) * 32 + lane];
+#pragma unroll
+      for (int q = 0; q < RB; ++q) {
+        if (q0 + q >= R) break;
+        const double* wk = W + (size_t)(q0 + q) * ldw + col;
+        double v[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) v[c] = wk[c];
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+          for (int c = 0; c < 5; ++c) acc[q][rr] -= a[5 * rr + c] * v[c];
+      }
+    }
+#pragma unroll
+    for (int o = 1; o < L; o <<= 1)
+#pragma unroll
+      for (int q = 0; q < RB; ++q)
+#pragma unroll
+        for (int c = 0; c < 5; ++c) acc[q][c] += __shfl_xor_sync(0xffffffffu, acc[q][c], o);
+    if (act && sub == 0) {
+      const int i = i0 + t;
+      const size_t r = (size_t)cperm[i];
+#pragma unroll
+      for (int q = 0; q < RB; ++q) {
+        if (q0 + q >= R) break;
+        double* wi = W + (size_t)(q0 + q) * ldw + 5 * (size_t)i;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) wi[c] = (double)X[q0 + q][5 * r + c] + acc[q][c];
+      }
+    }
+  }
+}
+template <int L, int RB, class S, class TO>
+__global__ void k_ilu_bwd_b(int i0, int cnt, int s0, int R, const int* __restrict__ cperm,
+                            const int* __restrict__ rlen, const int* __restrict__ rju, const int* __restrict__ isp,
+                            const int* __restrict__ jc, const S* __restrict__ lu, double* __restrict__ W, size_t ldw,
+                            TO* const* __restrict__ Z) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = g / L, sub = g % L;
+  const bool act = t < cnt;
+  const int lane = t & 31;
+  const size_t base = act ? (size_t)isp[s0 + (t >> 5)] : 0;
+  const int d = act ? rju[i0 + t] : 0, len = act ? rlen[i0 + t] : 0;
+  for (int q0 = 0; q0 < R; q0 += RB) {
+    double acc[RB][5];
+#pragma unroll
+    for (int q = 0; q < RB; ++q)
+#pragma unroll
+      for (int c = 0; c < 5; ++c) acc[q][c] = 0.0;
+    for (int k = d + 1 + sub; k < len; k += L) {
+      double a[25];
+      load_block<S>(lu, (base + k) * 800, lane, a);
+      const size_t col = 5 * (size_t)jc[(base + k) * 32 + lane];
+#pragma unroll
+      for (int q = 0; q < RB; ++q) {
+        if (q0 + q >= R) break;
+        const double* wk = W + (size_t)(q0 + q) * ldw + col;
+        double v[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) v[c] = wk[c];
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+          for (int c = 0; c < 5; ++c) acc[q][rr] -= a[5 * rr + c] * v[c];
+      }
+    }
+#pragma unroll
+    for (int o = 1; o < L; o <<= 1)
+#pragma unroll
+      for (int q = 0; q < RB; ++q)
+#pragma unroll
+        for (int c = 0; c < 5; ++c) acc[q][c] += __shfl_xor_sync(0xffffffffu, acc[q][c], o);
+    if (act && sub == 0) {
+      const int i = i0 + t;
+      const size_t r = (size_t)cperm[i];
+      double dg[25];
+      load_block<S>(lu, (base + d) * 800, lane, dg);
+#pragma unroll
+      for (int q = 0; q < RB; ++q) {
+        if (q0 + q >= R) break;
+        double* wi = W + (size_t)(q0 + q) * ldw + 5 * (size_t)i;
+        double v[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) v[c] = acc[q][c] + wi[c];
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr) {
+          double x = 0.0;
+#pragma unroll
+          for (int c = 0; c < 5; ++c) x += dg[5 * rr + c] * v[c];
+          wi[rr] = x;
+          Z[q0 + q][5 * r + rr] = (TO)x;
+        }
+      }
+    }
+  }
+}
+
 // gather + factorisation of the operator read with orientation tr;
 // returns the number of singular diagonal blocks (waits for the stream)
 static int ilu_setup(aerof_gpu_ctx* c, int tr) {
@@ -811,6 +991,45 @@ static void ilu_apply(aerof_gpu_ctx* c, const TI* x, TO* z) {
       k_ilu_bwd<L, S, TO><<<grid_for((size_t)L * cnt, kIB), kIB, 0, s>>>(i0, cnt, m.h_cslice[col], m.cperm.p,
                                                                          m.rlen.p, m.rju.p, m.isp.p, m.jc.p, lu, w,
                                                                          z);
+      AEROF_LAUNCH_CHECK();
+    }
+  };
+  if (J.precision == AEROF_PREC_FP32) run((const float*)J.ilu32.p);
+  else run((const double*)J.ilu64.p);
+}
+
+// z_q = (LU)^-1 x_q for R vectors (device pointer arrays on the host)
+template <class TI, class TO>
+static void ilu_apply_batch(aerof_gpu_ctx* c, int R, const TI* const* x, TO* const* z) {
+  DeviceMesh& m = c->mesh;
+  Implicit& J = c->imp;
+  cudaStream_t s = c->stream;
+  const size_t ldw = 5 * (size_t)m.N;
+  J.iluw.ensure((size_t)R * ldw);
+  J.iptr.ensure(2 * (size_t)R);
+  std::vector<unsigned long long> p(2 * (size_t)R);
+  for (int q = 0; q < R; ++q) {
+    p[q] = (unsigned long long)x[q];
+    p[R + q] = (unsigned long long)z[q];
+  }
+  AEROF_CUDA(cudaMemcpyAsync(J.iptr.p, p.data(), sizeof(unsigned long long) * 2 * (size_t)R, cudaMemcpyHostToDevice,
+                             s));
+  const TI* const* X = reinterpret_cast<const TI* const*>(J.iptr.p);
+  TO* const* Z = reinterpret_cast<TO* const*>(J.iptr.p + R);
+  double* w = J.iluw.p;
+  auto run = [&](const auto* lu) {
+    using S = std::remove_const_t<std::remove_pointer_t<decltype(lu)>>;
+    constexpr int L = 4, RB = 4;
+    for (int col = 0; col < m.ncolor; ++col) {
+      const int i0 = m.h_cptr[col], cnt = m.h_cptr[col + 1] - i0;
+      k_ilu_fwd_b<L, RB, S, TI><<<grid_for((size_t)L * cnt, kIB), kIB, 0, s>>>(
+          i0, cnt, m.h_cslice[col], R, m.cperm.p, m.rju.p, m.isp.p, m.jc.p, lu, X, w, ldw);
+      AEROF_LAUNCH_CHECK();
+    }
+    for (int col = m.ncolor - 1; col >= 0; --col) {
+      const int i0 = m.h_cptr[col], cnt = m.h_cptr[col + 1] - i0;
+      k_ilu_bwd_b<L, RB, S, TO><<<grid_for((size_t)L * cnt, kIB), kIB, 0, s>>>(
+          i0, cnt, m.h_cslice[col], R, m.cperm.p, m.rlen.p, m.rju.p, m.isp.p, m.jc.p, lu, w, ldw, Z);
       AEROF_LAUNCH_CHECK();
     }
   };
@@ -1132,6 +1351,255 @@ static int fgmres_exact(aerof_gpu_ctx* c, const double* b, double* x, int numVec
   return iter;
 }
 
+// Lockstep GMRES over R right-hand sides (batched sensitivities): every
+// system runs the algorithm of gmres_t (FLEX = false: FP32 Krylov vectors,
+// right-preconditioned, products with H1 batched over the running systems)
+// or of fgmres_exact (FLEX = true: FP64, the preconditioner one inner
+// lockstep solve of all running systems, exact products), the iterations of
+// all systems together; a system that converges stops, the others go on.
+// B[q] / X[q] are the right-hand sides and solutions (device, [N][5]); X is
+// zeroed first.  The inner solve (FLEX = false) runs one cycle: maxits <=
+// numVec.
+template <class TV, bool FLEX>
+static void gmres_lockstep(aerof_gpu_ctx* c, int R, const double* const* B, double* const* X, int numVec, int maxits,
+                           double eps, int trans, const double* exactU, int inner_m, int inner_its, double inner_eps,
+                           int* its, double* res) {
+  DeviceMesh& m = c->mesh;
+  Implicit& J = c->imp;
+  const size_t n = 5 * (size_t)m.N;
+  const size_t ld = (n + 63) / 64 * 64;
+  const int gv = grid_for(n, kIB);
+  cudaStream_t s = c->stream;
+  const int M1 = numVec + 1, HS = numVec + 2;
+  TV *Vb, *Zb = nullptr, *w, *rr, *pz = nullptr;
+  double* hd;
+  if constexpr (FLEX) {
+    J.bV.ensure((size_t)R * M1 * ld);
+    J.bZ.ensure((size_t)R * numVec * ld);
+    J.bw.ensure((size_t)R * ld);
+    J.br.ensure((size_t)R * ld);
+    J.bh.ensure((size_t)R * (HS + M1));
+    Vb = J.bV.p; Zb = J.bZ.p; w = J.bw.p; rr = J.br.p; hd = J.bh.p;
+  } else {
+    J.iV.ensure((size_t)R * M1 * ld);
+    J.iw.ensure((size_t)R * ld);
+    J.ir.ensure((size_t)R * ld);
+    J.iz.ensure((size_t)R * ld);
+    J.ih.ensure((size_t)R * (HS + M1));
+    J.bptr.ensure(2 * (size_t)R);
+    Vb = J.iV.p; w = J.iw.p; rr = J.ir.p; pz = J.iz.p; hd = J.ih.p;
+  }
+  double* yd = hd + (size_t)R * HS;
+  J.ticket.ensure(1);
+  c->s.red.ensure(kGB);
+  double* part = c->s.red.p;
+  unsigned* ticket = J.ticket.p;
+  AEROF_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), s));
+  auto V = [&](int q, int j) { return Vb + ((size_t)q * M1 + j) * ld; };
+  auto Zv = [&](int q, int j) { return Zb + ((size_t)q * numVec + j) * ld; };
+  auto W = [&](int q) { return w + (size_t)q * ld; };
+  auto Rv = [&](int q) { return rr + (size_t)q * ld; };
+  auto Hq = [&](int q) { return hd + (size_t)q * HS; };
+  // host state per system
+  std::vector<double> H((size_t)R * M1 * numVec, 0.0), cs((size_t)R * 2 * numVec), g((size_t)R * M1), y(numVec),
+      hcol((size_t)R * HS), target(R, 0.0), l2(R, 0.0), bnorm(R);
+  std::vector<int> iter(R, 0), jl(R, -1);
+  std::vector<char> active(R, 1), run(R, 0), fin(R, 0);
+  auto h = [&](int q, int i, int j) -> double& { return H[((size_t)q * M1 + i) * numVec + j]; };
+  auto fetch = [&]() {
+    AEROF_CUDA(cudaMemcpyAsync(hcol.data(), hd, sizeof(double) * (size_t)R * HS, cudaMemcpyDeviceToHost, s));
+    AEROF_CUDA(cudaStreamSynchronize(s));
+  };
+  // the reductions read 16-byte vectors of the right-hand sides
+  for (int q = 0; q < R; ++q)
+    if (reinterpret_cast<uintptr_t>(B[q]) % 16 != 0)
+      throw ApiError{AEROF_EINVAL, "lockstep GMRES: right-hand side not 16-byte aligned"};
+  for (int q = 0; q < R; ++q) {
+    AEROF_CUDA(cudaMemsetAsync(X[q], 0, n * sizeof(double), s));
+    k_mgs<double, true><<<kGB, kIB, 0, s>>>(n, nullptr, nullptr, nullptr, const_cast<double*>(B[q]), part, ticket,
+                                            Hq(q));
+    AEROF_LAUNCH_CHECK();
+  }
+  fetch();
+  for (int q = 0; q < R; ++q) bnorm[q] = std::sqrt(hcol[(size_t)q * HS]);
+  std::vector<unsigned long long> ptrs(2 * (size_t)R);
+  while (true) {
+    // residuals of the active systems
+    for (int q = 0; q < R; ++q) {
+      if (!active[q]) continue;
+      if (iter[q] == 0) {
+        k_scale<double, TV><<<gv, kIB, 0, s>>>(n, 1.0, B[q], Rv(q));
+        AEROF_LAUNCH_CHECK();
+      } else {
+        TimerScope t(c, AEROF_T_KSP_MATVEC);
+        if constexpr (FLEX) {
+          exact_product(c, exactU, X[q], W(q), trans);
+        } else {
+          k_scale<double, TV><<<gv, kIB, 0, s>>>(n, 1.0, X[q], Rv(q));
+          AEROF_LAUNCH_CHECK();
+          matvec_t<TV, TV>(c, Rv(q), W(q), trans);
+        }
+        k_sub<TV, TV><<<gv, kIB, 0, s>>>(n, B[q], W(q), Rv(q));
+        AEROF_LAUNCH_CHECK();
+      }
+      k_mgs<TV, true><<<kGB, kIB, 0, s>>>(n, nullptr, nullptr, nullptr, Rv(q), part, ticket, Hq(q));
+      AEROF_LAUNCH_CHECK();
+    }
+    fetch();
+    bool any = false;
+    for (int q = 0; q < R; ++q) {
+      run[q] = 0;
+      jl[q] = -1;
+      if (!active[q]) continue;
+      const double beta = std::sqrt(hcol[(size_t)q * HS]);
+      if (iter[q] == 0) target[q] = eps * bnorm[q];
+      if (beta == 0.0) {
+        active[q] = 0;
+        l2[q] = 0.0;
+        continue;
+      }
+      k_scale<TV, TV><<<gv, kIB, 0, s>>>(n, 1.0 / beta, Rv(q), V(q, 0));
+      AEROF_LAUNCH_CHECK();
+      std::fill(g.begin() + (size_t)q * M1, g.begin() + (size_t)(q + 1) * M1, 0.0);
+      g[(size_t)q * M1] = beta;
+      run[q] = 1;
+      fin[q] = 0;
+      any = true;
+    }
+    if (!any) break;
+    for (int j = 0; j < numVec; ++j) {
+      std::vector<int> rl;
+      for (int q = 0; q < R; ++q)
+        if (run[q]) rl.push_back(q);
+      if (rl.empty()) break;
+      const int nr = (int)rl.size();
+      // direction and product of every running system
+      if constexpr (FLEX) {
+        std::vector<const double*> bi(nr);
+        std::vector<double*> xi(nr);
+        for (int k = 0; k < nr; ++k) { bi[k] = V(rl[k], j); xi[k] = Zv(rl[k], j); }
+        gmres_lockstep<float, false>(c, nr, bi.data(), xi.data(), inner_m, inner_its, inner_eps, trans, nullptr, 0, 0,
+                                     0.0, nullptr, nullptr);
+        TimerScope t(c, AEROF_T_KSP_MATVEC);
+        for (int k = 0; k < nr; ++k) exact_product(c, exactU, Zv(rl[k], j), W(rl[k]), trans);
+      } else {
+        {
+          TimerScope t(c, AEROF_T_KSP_OTHER);
+          const int tr = ((trans != 0) != J.transposed) ? 1 : 0;
+          if (J.pc == AEROF_PC_ILU0 && J.ilu_ready && J.ilu_tr == tr) {
+            // every factor block read once for the running systems
+            std::vector<const TV*> xs(nr);
+            std::vector<TV*> zs(nr);
+            for (int k = 0; k < nr; ++k) { xs[k] = V(rl[k], j); zs[k] = pz + (size_t)rl[k] * ld; }
+            ilu_apply_batch<TV, TV>(c, nr, xs.data(), zs.data());
+          } else {
+            for (int k = 0; k < nr; ++k) prec_apply_t<TV, TV>(c, V(rl[k], j), pz + (size_t)rl[k] * ld, trans);
+          }
+        }
+        TimerScope t(c, AEROF_T_KSP_MATVEC);
+        for (int k = 0; k < nr; ++k) {
+          ptrs[k] = (unsigned long long)(pz + (size_t)rl[k] * ld);
+          ptrs[R + k] = (unsigned long long)W(rl[k]);
+        }
+        AEROF_CUDA(cudaMemcpyAsync(J.bptr.p, ptrs.data(), sizeof(unsigned long long) * 2 * (size_t)R,
+                                   cudaMemcpyHostToDevice, s));
+        const TV* const* P = reinterpret_cast<const TV* const*>(J.bptr.p);
+        TV* const* Y = reinterpret_cast<TV* const*>(J.bptr.p + R);
+        const bool tr = (trans != 0) != J.transposed;
+        auto go = [&](auto kern, auto* diag, auto* off) {
+          kern<<<grid_for(m.N, kIB), kIB, 0, s>>>(m.N, nr, m.nbr_ptr.p, m.nbr_tpos.p, m.sptr.p, m.scol.p, diag, off,
+                                                 P, Y);
+          AEROF_LAUNCH_CHECK();
+        };
+        if (J.precision == AEROF_PREC_FP32) {
+          if (tr) go(k_spmv_batch<float, true, TV, 4>, J.diag32.p, J.off32.p);
+          else go(k_spmv_batch<float, false, TV, 4>, J.diag32.p, J.off32.p);
+        } else {
+          if (tr) go(k_spmv_batch<double, true, TV, 4>, J.diag64.p, J.off64.p);
+          else go(k_spmv_batch<double, false, TV, 4>, J.diag64.p, J.off64.p);
+        }
+      }
+      TimerScope t(c, AEROF_T_KSP_OTHER);
+      for (int q : rl) {
+        for (int i = 0; i <= j; ++i) {
+          k_mgs<TV, false><<<kGB, kIB, 0, s>>>(n, i ? Hq(q) + (i - 1) : nullptr, i ? V(q, i - 1) : nullptr, V(q, i),
+                                               W(q), part, ticket, Hq(q) + i);
+          AEROF_LAUNCH_CHECK();
+        }
+        k_mgs<TV, true><<<kGB, kIB, 0, s>>>(n, Hq(q) + j, V(q, j), nullptr, W(q), part, ticket, Hq(q) + j + 1);
+        AEROF_LAUNCH_CHECK();
+      }
+      fetch();
+      for (int q : rl) {
+        const double* hc = hcol.data() + (size_t)q * HS;
+        double* csq = cs.data() + (size_t)q * 2 * numVec;
+        double* gq = g.data() + (size_t)q * M1;
+        for (int i = 0; i <= j; ++i) h(q, i, j) = hc[i];
+        h(q, j + 1, j) = std::sqrt(hc[j + 1]);
+        const bool breakdown = (h(q, j + 1, j) == 0.0);
+        if (!breakdown) {
+          k_scale<TV, TV><<<gv, kIB, 0, s>>>(n, 1. / h(q, j + 1, j), W(q), V(q, j + 1));
+          AEROF_LAUNCH_CHECK();
+        }
+        for (int i = 0; i < j; ++i) {
+          double hj = csq[2 * i + 1] * h(q, i, j) + csq[2 * i] * h(q, i + 1, j);
+          double hjp1 = -csq[2 * i] * h(q, i, j) + csq[2 * i + 1] * h(q, i + 1, j);
+          h(q, i, j) = hj; h(q, i + 1, j) = hjp1;
+        }
+        if (h(q, j, j) * h(q, j, j) == 0.0) { csq[2 * j + 1] = 0.0; csq[2 * j] = 1.0; }
+        else {
+          double coef = 1.0 / std::sqrt(h(q, j, j) * h(q, j, j) + h(q, j + 1, j) * h(q, j + 1, j));
+          csq[2 * j + 1] = std::sqrt(h(q, j, j) * h(q, j, j)) * coef;
+          csq[2 * j] = csq[2 * j + 1] * h(q, j + 1, j) / h(q, j, j);
+        }
+        h(q, j, j) = csq[2 * j + 1] * h(q, j, j) + csq[2 * j] * h(q, j + 1, j);
+        h(q, j + 1, j) = 0.0;
+        gq[j + 1] = -csq[2 * j] * gq[j];
+        gq[j] = csq[2 * j + 1] * gq[j];
+        ++iter[q];
+        jl[q] = j;
+        if (breakdown) { run[q] = 0; fin[q] = 1; continue; }
+        l2[q] = std::fabs(gq[j + 1]);
+        if (l2[q] <= target[q] || iter[q] >= maxits) { run[q] = 0; fin[q] = 1; }
+      }
+    }
+    // solution update of every system that ran in this cycle
+    for (int q = 0; q < R; ++q) {
+      if (jl[q] < 0) continue;
+      const int jj = jl[q];
+      const double* gq = g.data() + (size_t)q * M1;
+      for (int i = jj; i >= 0; --i) {
+        y[i] = gq[i];
+        for (int k = jj; k >= i + 1; --k) y[i] -= h(q, i, k) * y[k];
+        y[i] /= h(q, i, i);
+      }
+      double* yq = yd + (size_t)q * M1;
+      AEROF_CUDA(cudaMemcpyAsync(yq, y.data(), sizeof(double) * (jj + 1), cudaMemcpyHostToDevice, s));
+      if constexpr (FLEX) {
+        k_combine<double><<<gv, kIB, 0, s>>>(n, jj + 1, yq, Zv(q, 0), ld, W(q));
+        AEROF_LAUNCH_CHECK();
+        k_add<double><<<gv, kIB, 0, s>>>(n, W(q), X[q]);
+        AEROF_LAUNCH_CHECK();
+      } else {
+        k_combine<TV><<<gv, kIB, 0, s>>>(n, jj + 1, yq, V(q, 0), ld, W(q));
+        AEROF_LAUNCH_CHECK();
+        prec_apply_t<TV, TV>(c, W(q), Rv(q), trans);
+        k_add<TV><<<gv, kIB, 0, s>>>(n, Rv(q), X[q]);
+        AEROF_LAUNCH_CHECK();
+      }
+      if (fin[q]) active[q] = 0;
+    }
+    bool left = false;
+    for (int q = 0; q < R; ++q) left = left || active[q];
+    if (!left) break;
+  }
+  AEROF_CUDA(cudaStreamSynchronize(s));
+  for (int q = 0; q < R; ++q) {
+    if (its) its[q] = iter[q];
+    if (res) res[q] = l2[q];
+  }
+}
+
 int gmres_dev(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int maxits, double eps, int trans,
               double* final_res, const double* exactU) {
   if (!exactU && c->imp.precision == AEROF_PREC_FP32)
@@ -1423,6 +1891,42 @@ extern "C" int aerof_gpu_linearized_solve_batch(aerof_gpu_ctx* c, const double* 
     if (int nb = prec_setup_dev(c, transpose)) {
       c->last_error = std::to_string(nb) + " singular diagonal block(s)";
       return AEROF_ESINGULAR;
+    }
+    // lockstep flexible GMRES over groups of right-hand sides (the inner
+    // FP32 solves of a group share every pass over H1); the group is as
+    // large as 70 % of the free device memory allows
+    const char* lv = std::getenv("AEROF_LOCKSTEP");
+    const bool lockstep = inner_its > 0 && inner_its <= 30 && (!lv || std::atoi(lv) != 0);
+    if (lockstep) {
+      // right-hand sides and solutions staged at a 512-byte aligned stride
+      // (the reductions read 16-byte vectors)
+      const size_t ld = (n + 63) / 64 * 64;
+      const cudaMemcpyKind kb = is_device_ptr(B) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+      const cudaMemcpyKind kx = is_device_ptr(X) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+      const size_t per = ((size_t)2 * krylov + 5) * ld * sizeof(double) + ((size_t)inner_its + 5) * ld * sizeof(float);
+      size_t freeb = 0, totalb = 0;
+      AEROF_CUDA(cudaMemGetInfo(&freeb, &totalb));
+      const int G = (int)std::max<size_t>(1, std::min<size_t>((size_t)nrhs, (size_t)(0.7 * (double)freeb) / per));
+      c->imp.bB.ensure((size_t)std::min(G, nrhs) * ld);
+      c->imp.bX.ensure((size_t)std::min(G, nrhs) * ld);
+      for (int k0 = 0; k0 < nrhs; k0 += G) {
+        const int g = std::min(G, nrhs - k0);
+        std::vector<const double*> bq(g);
+        std::vector<double*> xq(g);
+        for (int q = 0; q < g; ++q) {
+          AEROF_CUDA(cudaMemcpyAsync(c->imp.bB.p + (size_t)q * ld, B + (size_t)(k0 + q) * n, n * sizeof(double), kb,
+                                     c->stream));
+          bq[q] = c->imp.bB.p + (size_t)q * ld;
+          xq[q] = c->imp.bX.p + (size_t)q * ld;
+        }
+        gmres_lockstep<double, true>(c, g, bq.data(), xq.data(), krylov, maxits, eps, transpose, dU,
+                                     std::min(inner_its, 30), inner_its, 1e-3, its ? its + k0 : nullptr,
+                                     res ? res + k0 : nullptr);
+        for (int q = 0; q < g; ++q)
+          AEROF_CUDA(cudaMemcpyAsync(X + (size_t)(k0 + q) * n, xq[q], n * sizeof(double), kx, c->stream));
+        AEROF_CUDA(cudaStreamSynchronize(c->stream));
+      }
+      return AEROF_OK;
     }
     for (int k = 0; k < nrhs; ++k) {
       const double* db = in_dev(c, B + (size_t)k * n, n, c->s.Vstage);

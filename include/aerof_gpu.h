@@ -308,9 +308,11 @@ int aerof_gpu_linearized_solve(aerof_gpu_ctx* ctx, const double* U, const double
  * sensitivities of several shape modes, FluidShapeOptimizationHandler.C:
  * 2362-2433, one fsoLinearSolver per mode): B and X are [nrhs][N][5]; the
  * stored exact linearisation at U is evaluated once (as
- * aerof_gpu_h2_evaluate), the first-order operator and its block-Jacobi are
- * assembled once, and every right-hand side is solved as
- * aerof_gpu_linearized_solve does with the stored operator's products.
+ * aerof_gpu_h2_evaluate), the first-order operator and its preconditioner
+ * are assembled once, and every right-hand side is solved as
+ * aerof_gpu_linearized_solve does with the stored operator's products; with
+ * 0 < inner_its <= 30 the right-hand sides run in lockstep groups whose
+ * inner FP32 solves share the passes over H1 and its preconditioner.
  * its[k], res[k]: outer iterations and final residual norm of each.       */
 int aerof_gpu_linearized_solve_batch(aerof_gpu_ctx* ctx, const double* U, int nrhs, const double* B, double* X,
                                      int krylov, int maxits, double eps, int transpose, int inner_its, int* its,

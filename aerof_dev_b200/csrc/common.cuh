@@ -205,9 +205,9 @@ struct Implicit {
   DBuf<unsigned> ticket;   // grid-reduction ticket of the fused Gram-Schmidt kernels
   DBuf<double> fsum;       // [nbrow][25] boundary-face blocks of the boundary rows
   // preconditioner: AEROF_PC_JACOBI or AEROF_PC_ILU0 (block ILU(0) in the
-  // multicolour ordering, blocks at a padded stride of 16-byte multiples,
-  // inverted diagonal; factored for the operator read plainly (ilu_tr = 0)
-  // or transposed (1))
+  // multicolour ordering, factors in the sliced layout of the colour-ordered
+  // rows with the diagonal inverted; factored for the operator read plainly
+  // (ilu_tr = 0) or transposed (1)); iluw: the sweeps' work vectors
   int pc = 0;
   bool ilu_ready = false;
   int ilu_tr = 0;

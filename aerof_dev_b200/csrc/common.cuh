@@ -171,6 +171,7 @@ struct DeviceMesh {
   DBuf<int> lptr, lidx;    // per node (new): owned local edge slots, sign bit = second endpoint
   DBuf<int> xslot;         // [E] spill slot of a block-crossing edge, -1 otherwise
   DBuf<int> xin_ptr;       // per node (new): its incoming spill slots [xin_ptr[n], xin_ptr[n+1])
+  DBuf<int> bnf_ptr, bnf_ent;   // per node (new): its boundary subface fluxes, rows 3 f + l of fbuf, face order
 };
 
 struct Scratch {

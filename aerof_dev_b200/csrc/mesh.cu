@@ -521,6 +521,22 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
       else m.lidx.upload(hb.lidx.data(), hb.lidx.size(), s);
       m.xslot.upload(hb.xslot.data(), (size_t)E, s);
       m.xin_ptr.upload(hb.xin_ptr.data(), N + 1, s);
+      {
+        // boundary subface fluxes of each node, blocked numbering
+        std::vector<int> bp(N + 1, 0), be;
+        for (int n = 0; n < N; ++n) {
+          const int o = hb.n2o[n];
+          for (int q = h.nf_ptr[o]; q < h.nf_ptr[o + 1]; ++q) {
+            const int f = h.nf_face[q];
+            const int l = faces[3 * (size_t)f] == o ? 0 : (faces[3 * (size_t)f + 1] == o ? 1 : 2);
+            be.push_back(3 * f + l);
+          }
+          bp[n + 1] = (int)be.size();
+        }
+        if (be.empty()) be.push_back(0);
+        m.bnf_ptr.upload(bp.data(), bp.size(), s);
+        m.bnf_ent.upload(be.data(), be.size(), s);
+      }
       AEROF_CUDA(cudaStreamSynchronize(s));  // host vectors die at scope end
     }
     // rows with boundary faces (their face blocks are formed apart)

@@ -567,20 +567,18 @@ __global__ void __launch_bounds__(THREADS, MINB)
   }
 }
 
-// BLOCKED organisation, per node: block-local sum (new numbering), minus the
-// spilled fluxes of incoming block-crossing edges, plus the boundary faces
-// of the node (face order), times 1/ctrlVol; written to R in the caller's
-// numbering.
-__global__ void k_fv_nodes(int N, const int* __restrict__ o2n, const double* __restrict__ part,
-                           const int* __restrict__ xin_ptr, const double* __restrict__ spill,
-                           const int* __restrict__ nf_ptr,
-                           const int* __restrict__ nf_face, const int* __restrict__ faces,
-                           const double* __restrict__ fbuf, const double* __restrict__ vol, double* __restrict__ R) {
-  // one thread per row of R in the caller's numbering (coalesced writes);
-  // the blocked partial sums and spills are read through o2n
-  int o = blockIdx.x * blockDim.x + threadIdx.x;
-  if (o >= N) return;
-  const int n = o2n[o];
+// BLOCKED organisation, per node in the blocked numbering: block-local sum,
+// minus the spilled fluxes of incoming block-crossing edges, plus the
+// node's boundary subface fluxes (face order), times 1/ctrlVol; written to
+// R in the caller's numbering through n2o.  Partial sums, spills and
+// subface fluxes are read in node order (coalesced); the caller-order
+// variant that gathers them through o2n measured slower.
+__global__ void k_fv_nodes_b(int N, const int* __restrict__ n2o, const double* __restrict__ part,
+                             const int* __restrict__ xin_ptr, const double* __restrict__ spill,
+                             const int* __restrict__ bnf_ptr, const int* __restrict__ bnf_ent,
+                             const double* __restrict__ fbuf, const double* __restrict__ vol2, double* __restrict__ R) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
   double acc[5];
 #pragma unroll
   for (int c = 0; c < 5; ++c) acc[c] = part[5 * (size_t)n + c];
@@ -589,17 +587,15 @@ __global__ void k_fv_nodes(int N, const int* __restrict__ o2n, const double* __r
 #pragma unroll
     for (int c = 0; c < 5; ++c) acc[c] -= sp[c];
   }
-  for (int q = nf_ptr[o]; q < nf_ptr[o + 1]; ++q) {
-    const int f = nf_face[q];
-    const int* fd = faces + 3 * (size_t)f;
-    const int l = fd[0] == o ? 0 : (fd[1] == o ? 1 : 2);
-    const double* ff = fbuf + 5 * (3 * (size_t)f + l);
+  for (int q = bnf_ptr[n]; q < bnf_ptr[n + 1]; ++q) {
+    const double* ff = fbuf + 5 * (size_t)bnf_ent[q];
 #pragma unroll
     for (int c = 0; c < 5; ++c) acc[c] += ff[c];
   }
-  const double invcv = 1.0 / vol[o];
+  const double invcv = 1.0 / vol2[n];
+  const size_t o = (size_t)n2o[n];
 #pragma unroll
-  for (int c = 0; c < 5; ++c) R[5 * (size_t)o + c] = acc[c] * invcv;
+  for (int c = 0; c < 5; ++c) R[5 * o + c] = acc[c] * invcv;
 }
 
 // U[N][5] (caller numbering) -> blocked node records P2[n].V
@@ -846,14 +842,21 @@ static GradStage grad_stage(const DeviceMesh& m) {
   return st;
 }
 
+// U -> the V part of the blocked records P2 (thread per blocked row,
+// gathering U through n2o: measured faster than scattering the records
+// through o2n)
+static void prim_to_P2(const DeviceMesh& m, const Gas& g, const double* dU, cudaStream_t s) {
+  k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
+  AEROF_LAUNCH_CHECK();
+}
+
 // persistent pipelined gradients of the records P2src (with dU,
 // k_prim_blocked writes the mesh's P2 first and P2src is that)
 static void launch_grad_pipe(aerof_gpu_ctx* c, const Gas& g, const double* dU, const int* tag, double* G2,
                              cudaStream_t s, const double* P2src = nullptr) {
   const DeviceMesh& m = c->mesh;
   if (dU) {
-    k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
-    AEROF_LAUNCH_CHECK();
+    prim_to_P2(m, g, dU, s);
   }
   if (!P2src) P2src = m.P2.p;
   const GradStage st = grad_stage(m);
@@ -881,8 +884,7 @@ static void launch_grad_staged(const DeviceMesh& m, const Gas& g, const double* 
                                size_t smem, bool fused, cudaStream_t s) {
   const int L = kBlock / m.NB;
   if (!fused) {
-    k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
-    AEROF_LAUNCH_CHECK();
+    prim_to_P2(m, g, dU, s);
   }
   auto go = [&](auto kern) {
     AEROF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -909,8 +911,7 @@ void prim_grad_blocked_dev(aerof_gpu_ctx* c, const double* dU, const int* tag) {
   cudaStream_t s = c->stream;
   c->s.G2.ensure(16 * (size_t)m.N);
   if (c->cfg.reconstruction == AEROF_REC_CONSTANT) {
-    k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
-    AEROF_LAUNCH_CHECK();
+    prim_to_P2(m, g, dU, s);
     return;
   }
   const size_t gsmem = ((size_t)8 * kPS * (m.NB + m.maxH) + (size_t)2 * m.maxL + 15) / 16 * 16;
@@ -925,8 +926,7 @@ void prim_grad_blocked_dev(aerof_gpu_ctx* c, const double* dU, const int* tag) {
   } else if (staged) {
     launch_grad_staged(m, g, dU, tag, c->s.G2.p, gsmem, gk == 1, s);
   } else {
-    k_prim_blocked<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, g, m.n2o.p, dU, m.P2.p);
-    AEROF_LAUNCH_CHECK();
+    prim_to_P2(m, g, dU, s);
     k_grad<<<grid_for(4 * (size_t)m.N, kBlock), kBlock, 0, s>>>(m.N, m.P2.p, m.W2.p, m.nb2_ptr.p, m.nb2_node.p, tag,
                                                                 c->s.G2.p);
     AEROF_LAUNCH_CHECK();
@@ -1017,8 +1017,8 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
                                                            m.o2n.p, c->s.fbuf.p);
       AEROF_LAUNCH_CHECK();
     }
-    k_fv_nodes<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.o2n.p, c->s.part.p, m.xin_ptr.p, c->s.spill.p,
-                                                        m.nf_ptr.p, m.nf_face.p, m.faces.p, c->s.fbuf.p, m.vol.p, dR);
+    k_fv_nodes_b<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.n2o.p, c->s.part.p, m.xin_ptr.p, c->s.spill.p,
+                                                          m.bnf_ptr.p, m.bnf_ent.p, c->s.fbuf.p, m.vol2.p, dR);
     AEROF_LAUNCH_CHECK();
   }
   return bad;

@@ -950,7 +950,10 @@ static int ilu_setup(aerof_gpu_ctx* c, int tr) {
     AEROF_LAUNCH_CHECK();
     for (int col = 0; col < m.ncolor; ++col) {
       const int i0 = m.h_cptr[col], cnt = m.h_cptr[col + 1] - i0;
-      k_ilu_factor<S><<<grid_for(cnt, kIB), kIB, 0, s>>>(i0, cnt, m.h_cslice[col], m.rju.p, m.isp.p, m.lo_ptr.p,
+      // 64-thread CTAs: one colour's rows spread over every SM and several
+      // CTAs of this register-heavy kernel fit on each
+      constexpr int kFT = 64;
+      k_ilu_factor<S><<<grid_for(cnt, kFT), kFT, 0, s>>>(i0, cnt, m.h_cslice[col], m.rju.p, m.isp.p, m.lo_ptr.p,
                                                          m.lo.p, m.up_ptr.p, m.up.p, lu, bad);
       AEROF_LAUNCH_CHECK();
     }

@@ -33,7 +33,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libaerof_gpu.so")
 
 AEROF_OK = 0
-ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ETIMEDOUT", -5: "ESINGULAR", -6: "ESTATE"}
+ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ETIMEDOUT", -5: "ESINGULAR", -6: "ESTATE",
+          -7: "EDIVERGED"}
 REC_CONSTANT, REC_VANALBADA, REC_LINEAR = 1, 2, 3
 KERNEL_BLOCKED, KERNEL_EDGE = 0, 1
 PREC_FP32, PREC_FP64 = 32, 64
@@ -51,7 +52,7 @@ EXPORTS = [
     "aerof_gpu_residual_async", "aerof_gpu_status", "aerof_gpu_profile", "aerof_gpu_timers",
     "aerof_gpu_update_coordinates", "aerof_gpu_linearized_solve", "aerof_gpu_residual_noalloc",
     "aerof_gpu_h2_evaluate", "aerof_gpu_h2_apply", "aerof_gpu_h2_release", "aerof_gpu_set_exact_operator",
-    "aerof_gpu_linearized_solve_batch", "aerof_gpu_set_preconditioner",
+    "aerof_gpu_linearized_solve_batch", "aerof_gpu_set_preconditioner", "aerof_gpu_set_jacobian",
 ]
 TIMER_NAMES = ["nodal_grad", "fv_term", "time_step", "fv_jac", "prec_setup", "ksp_matvec", "ksp_other", "other"]
 
@@ -77,7 +78,7 @@ class NewtonParams(C.Structure):
 
 class NewtonResult(C.Structure):
     _fields_ = [("steps", C.c_int), ("linear_its", C.c_int), ("rel_residual", C.c_double),
-                ("seconds", C.c_double)]
+                ("seconds", C.c_double), ("redos", C.c_int), ("reserved", C.c_int * 3)]
 
 
 _lib = None
@@ -134,6 +135,7 @@ def library(path: str | None = None):
             "aerof_gpu_linearized_solve_batch": [vp, dp, C.c_int, dp, dp, C.c_int, C.c_int, C.c_double, C.c_int,
                                                  C.c_int, dp, dp],
             "aerof_gpu_set_preconditioner": [vp, C.c_int],
+            "aerof_gpu_set_jacobian": [vp, dp, C.c_int],
         }
         for name, args in sig.items():
             if hasattr(L, name):
@@ -419,6 +421,13 @@ class MatVecProdH1:
     def applyTranspose(self, p):
         return self.apply(p, transpose=True)
 
+    def set_blocks(self, A):
+        """Make an operator given in MvpMat layout a[N+2E][5][5] (reference
+        numbering) the context's H1 in this object's precision."""
+        ctx = self.ctx
+        a = _Arg(A, np.float64, (ctx.N + 2 * ctx.E, 5, 5))
+        ctx._check(ctx.L.aerof_gpu_set_jacobian(ctx.h, a.ptr, int(self.precision)))
+
     def blocks(self) -> np.ndarray:
         """The operator in MvpMat layout a[N+2E][5][5] (reference numbering)."""
         ctx = self.ctx
@@ -489,7 +498,7 @@ class ImplicitSteadySolver:
         ctx._check(ctx.L.aerof_gpu_newton(ctx.h, a.ptr, C.byref(self.p), C.byref(res),
                                           C.c_void_p(hist.ctypes.data)))
         return a.obj, {"steps": res.steps, "linear_its": res.linear_its, "rel_residual": res.rel_residual,
-                       "seconds": res.seconds, "history": hist[: res.steps + 1]}
+                       "seconds": res.seconds, "redos": res.redos, "history": hist[: res.steps + 1]}
 
 
 class Sensitivity:

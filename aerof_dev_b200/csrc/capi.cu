@@ -36,9 +36,17 @@ void out_finish(aerof_gpu_ctx* c, double* user, const double* dev, size_t count)
   AEROF_CUDA(cudaStreamSynchronize(c->stream));
 }
 
+// Only the outermost scope records: a scope opened inside another one
+// (a preconditioner apply inside the Gram-Schmidt scope, say) is charged to
+// the enclosing category, so the categories' intervals never overlap and
+// their sum never exceeds the solve.
 int timer_begin(aerof_gpu_ctx* c, int cat) {
   Timers& t = c->timers;
   if (!t.on) return -1;
+  if (t.depth > 0) {
+    ++t.depth;
+    return -2;
+  }
   cudaEvent_t e[2];
   for (int k = 0; k < 2; ++k) {
     if (!t.pool.empty()) { e[k] = t.pool.back(); t.pool.pop_back(); }
@@ -46,10 +54,13 @@ int timer_begin(aerof_gpu_ctx* c, int cat) {
   }
   AEROF_CUDA(cudaEventRecord(e[0], c->stream));
   t.recs.push_back({cat, e[0], e[1]});
+  ++t.depth;
   return (int)t.recs.size() - 1;
 }
 
 void timer_end(aerof_gpu_ctx* c, int h) {
+  if (h == -1) return;
+  --c->timers.depth;
   if (h < 0) return;
   cudaEventRecord(c->timers.recs[h].b, c->stream);
 }
@@ -120,6 +131,9 @@ extern "C" int aerof_gpu_create(const aerof_gpu_config* cfg, aerof_gpu_ctx** out
     return AEROF_ECUDA;
   }
   c->stream = c->own_stream;
+  // loads the residual module and reserves the allocation-free scratch now,
+  // before the caller can hand the rest of the device to its own pool
+  noalloc_attach(c);
   *out = c;
   return AEROF_OK;
 }

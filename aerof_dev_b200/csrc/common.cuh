@@ -274,6 +274,7 @@ struct H2Op {
 // CUDA-event timers per category (AEROF_T_*), recorded without host sync.
 struct Timers {
   bool on = false;
+  int depth = 0;           // open scopes (only the outermost records)
   struct Rec { int cat; cudaEvent_t a, b; };
   std::vector<Rec> recs;
   std::vector<cudaEvent_t> pool;
@@ -301,6 +302,10 @@ struct aerof_gpu_ctx {
   aerof::H2Op h2;
   aerof::Timers timers;
   std::string last_error;
+  // device address of the allocation-free residual's fixed scratch array,
+  // looked up at context creation (residual.cu)
+  double* noalloc_scratch = nullptr;
+  std::string noalloc_error;
 };
 
 namespace aerof {
@@ -390,5 +395,8 @@ void exact_product(aerof_gpu_ctx* c, const double* dU, const double* p, double* 
 void h2_evaluate_dev(aerof_gpu_ctx* c, const double* dU);
 // implemented in mesh.cu: recompute the geometry for new coordinates
 void compute_geometry(aerof_gpu_ctx* c);
+// implemented in residual.cu: device address of the allocation-free
+// residual's scratch array for the current device, kept in the context
+void noalloc_attach(aerof_gpu_ctx* c);
 
 }  // namespace aerof

@@ -528,6 +528,20 @@ __global__ void k_add(size_t n, const TA* __restrict__ a, double* __restrict__ x
   if (q < n) x[q] += (double)a[q];
 }
 
+// SubDomain::checkSolution (SubDomain.C:6746-6806): per node, one count for
+// a non-positive density and one for a non-positive pressure of the
+// conservative state (NaN counts too: such a state is not physical either).
+__global__ void k_check_solution(int N, Gas g, const double* __restrict__ U, int* __restrict__ nbad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double u[5], v[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) u[k] = U[5 * (size_t)i + k];
+  cons2prim(g, u, v);
+  const int b = (int)!(v[0] > 0.0) + (int)!(v[4] > 0.0);
+  if (b) atomicAdd(nbad, b);
+}
+
 }  // namespace aerof
 
 // ====================================================================== host
@@ -1688,6 +1702,63 @@ extern "C" int aerof_gpu_get_jacobian(aerof_gpu_ctx* c, double* A) {
   });
 }
 
+// The reverse of aerof_gpu_get_jacobian: H1 given in the MvpMat layout
+// a[N+2E][25] (reference numbering) is stored in the sliced layout in the
+// requested precision, as if aerof_gpu_jacobian had assembled it.
+extern "C" int aerof_gpu_set_jacobian(aerof_gpu_ctx* c, const double* A, int precision) {
+  return guard(c, [&]() -> int {
+    need_mesh_or_throw(c);
+    if (!A || (precision != AEROF_PREC_FP32 && precision != AEROF_PREC_FP64)) return AEROF_EINVAL;
+    DeviceMesh& m = c->mesh;
+    Implicit& J = c->imp;
+    const size_t nd = sl_diag_size(m), no = sl_off_size(m);
+    const size_t nA = 25 * (size_t)m.N + 50 * (size_t)m.E;
+    std::vector<double> hA;
+    if (is_device_ptr(A)) {
+      hA.resize(nA);
+      AEROF_CUDA(cudaMemcpyAsync(hA.data(), A, nA * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      AEROF_CUDA(cudaStreamSynchronize(c->stream));
+      A = hA.data();
+    }
+    std::vector<double> diag(nd, 0.0), off(no, 0.0);
+    const bool f32 = precision == AEROF_PREC_FP32;
+    auto elo = [&](int e, int l) { return f32 ? sl_el<float>(e, l) : sl_el<double>(e, l); };
+    for (int r = 0; r < m.N; ++r)
+      for (int e = 0; e < 25; ++e) diag[(size_t)(r >> 5) * 800 + elo(e, r & 31)] = A[25 * (size_t)r + e];
+    const std::vector<int>& sp = m.h_sptr;
+    const std::vector<int>& np = m.h_nbr_ptr;
+    std::vector<int2> epos(m.E);
+    AEROF_CUDA(cudaMemcpyAsync(epos.data(), m.edge_pos.p, sizeof(int2) * m.E, cudaMemcpyDeviceToHost, c->stream));
+    AEROF_CUDA(cudaStreamSynchronize(c->stream));
+    auto put = [&](int r, int p, const double* src) {
+      for (int e = 0; e < 25; ++e) off[((size_t)sp[r >> 5] + (p - np[r])) * 800 + elo(e, r & 31)] = src[e];
+    };
+    const double* edge_blocks = A + 25 * (size_t)m.N;
+    for (int l = 0; l < m.E; ++l) {
+      const int i = m.h_edges[2 * (size_t)l], j = m.h_edges[2 * (size_t)l + 1];
+      put(i, epos[l].x, edge_blocks + 50 * (size_t)l);
+      put(j, epos[l].y, edge_blocks + 50 * (size_t)l + 25);
+    }
+    if (f32) {
+      J.diag64.release(); J.off64.release(); J.dinv64.release();
+      std::vector<float> d32(diag.begin(), diag.end()), o32(off.begin(), off.end());
+      J.diag32.upload(d32.data(), nd, c->stream);
+      J.off32.upload(o32.data(), no, c->stream);
+      AEROF_CUDA(cudaStreamSynchronize(c->stream));
+    } else {
+      J.diag32.release(); J.off32.release(); J.dinv32.release();
+      J.diag64.upload(diag.data(), nd, c->stream);
+      J.off64.upload(off.data(), no, c->stream);
+      AEROF_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    J.precision = precision;
+    J.transposed = false;
+    J.prec_ready = false;
+    J.ilu_ready = false;
+    return AEROF_OK;
+  });
+}
+
 extern "C" int aerof_gpu_matvec(aerof_gpu_ctx* c, const double* p, double* y, int transpose) {
   return guard(c, [&]() -> int {
     need_jac(c);
@@ -1766,28 +1837,35 @@ extern "C" int aerof_gpu_newton(aerof_gpu_ctx* c, double* U, const aerof_newton_
       AEROF_CUDA(cudaMemcpyAsync(c->s.Ustage.p, U, n * sizeof(double), cudaMemcpyHostToDevice, s));
       dU = c->s.Ustage.p;
     }
-    c->imp.b.ensure(n); c->imp.x.ensure(n); c->s.dt.ensure(m.N); c->s.k1.ensure(n);
+    c->imp.b.ensure(n); c->imp.x.ensure(n); c->s.dt.ensure(m.N); c->s.k1.ensure(n); c->s.U0.ensure(n);
+    c->s.counters.ensure(8);
     double* R = c->s.k1.p;
     double* rhs = c->imp.b.p;
     double* dQ = c->imp.x.p;
     double* dt = c->s.dt.p;
+    double* Uprev = c->s.U0.p;
+    int* nbad_d = c->s.counters.p + 5;
     const int gv = grid_for(n, kIB);
     cudaEvent_t e0, e1;
     AEROF_CUDA(cudaEventCreate(&e0));
     AEROF_CUDA(cudaEventCreate(&e1));
     AEROF_CUDA(cudaEventRecord(e0, s));
     double res0 = 0.0, rel = 1.0, rel_prev = 1.0, cfl = p->cfl0;
-    int k, lits = 0, bad = 0;
-    for (k = 0; k <= p->max_steps; ++k) {
-      bad += residual_dev(c, dU, R);
-      double res = norm2_dev(c, R, n);
-      if (k == 0) res0 = res;
-      rel = res0 > 0.0 ? res / res0 : 0.0;
-      if (history) history[k] = rel;
-      if (!std::isfinite(rel)) throw ApiError{AEROF_EINVAL, "non-finite residual in Newton step " + std::to_string(k)};
-      if (rel <= p->tol || k == p->max_steps) break;
-      if (k > 0) cfl = std::min(std::max(cfl * std::pow(rel_prev / rel, p->ser), p->cfl_min), p->cfl_max);
-      rel_prev = rel;
+    int k = 0, lits = 0, bad = 0, redos = 0;
+    bool redo = false;
+    while (k <= p->max_steps) {
+      if (!redo) {
+        bad += residual_dev(c, dU, R);
+        double res = norm2_dev(c, R, n);
+        if (k == 0) res0 = res;
+        rel = res0 > 0.0 ? res / res0 : 0.0;
+        if (history) history[k] = rel;
+        if (!std::isfinite(rel)) throw ApiError{AEROF_EINVAL, "non-finite residual in Newton step " + std::to_string(k)};
+        if (rel <= p->tol || k == p->max_steps) break;
+        if (k > 0) cfl = std::min(std::max(cfl * std::pow(rel_prev / rel, p->ser), p->cfl_min), p->cfl_max);
+        rel_prev = rel;
+      }
+      redo = false;
       timestep_dev(c, dU, cfl, dt);
       jacobian_dev(c, dU, dt, p->precision, false);
       if (int nb = prec_setup_dev(c)) {
@@ -1797,8 +1875,44 @@ extern "C" int aerof_gpu_newton(aerof_gpu_ctx* c, double* U, const aerof_newton_
       k_scale<double, double><<<gv, kIB, 0, s>>>(n, -1.0, R, rhs);
       AEROF_LAUNCH_CHECK();
       lits += gmres_dev(c, rhs, dQ, p->ksp_krylov, p->ksp_maxits, p->ksp_eps, 0, nullptr, nullptr);
+      // rhs = Q; Q += dQ, then the physical-solution check
+      // (NewtonSolver.h:187-215): on a non-positive density or pressure the
+      // state is restored and the step redone with half the CFL number
+      // (TsParameters::computeCflNumber, TsParameters.C:187-195), which
+      // gives up below cfl0/1000
+      AEROF_CUDA(cudaMemcpyAsync(Uprev, dU, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
       k_add<double><<<gv, kIB, 0, s>>>(n, dQ, dU);
       AEROF_LAUNCH_CHECK();
+      AEROF_CUDA(cudaMemsetAsync(nbad_d, 0, sizeof(int), s));
+      k_check_solution<<<grid_for(m.N, kIB), kIB, 0, s>>>(m.N, make_gas(c->cfg.gamma), dU, nbad_d);
+      AEROF_LAUNCH_CHECK();
+      int nbad = 0;
+      AEROF_CUDA(cudaMemcpyAsync(&nbad, nbad_d, sizeof(int), cudaMemcpyDeviceToHost, s));
+      AEROF_CUDA(cudaStreamSynchronize(s));
+      if (nbad) {
+        AEROF_CUDA(cudaMemcpyAsync(dU, Uprev, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        ++redos;
+        cfl *= 0.5;
+        if (cfl < p->cfl0 / 1000.0) {
+          AEROF_CUDA(cudaStreamSynchronize(s));
+          cudaEventDestroy(e0);
+          cudaEventDestroy(e1);
+          if (dU != U) AEROF_CUDA(cudaMemcpy(U, dU, n * sizeof(double), cudaMemcpyDeviceToHost));
+          if (out) {
+            out->steps = k;
+            out->linear_its = lits;
+            out->rel_residual = rel;
+            out->seconds = 0.0;
+            out->redos = redos;
+          }
+          c->last_error = "Newton update non-physical at " + std::to_string(nbad) + " node value(s) in step " +
+                          std::to_string(k) + "; the CFL number fell below cfl0/1000";
+          return AEROF_EDIVERGED;
+        }
+        redo = true;
+        continue;
+      }
+      ++k;
     }
     AEROF_CUDA(cudaEventRecord(e1, s));
     AEROF_CUDA(cudaEventSynchronize(e1));
@@ -1813,6 +1927,7 @@ extern "C" int aerof_gpu_newton(aerof_gpu_ctx* c, double* U, const aerof_newton_
       out->linear_its = lits;
       out->rel_residual = rel;
       out->seconds = ms * 1e-3;
+      out->redos = redos;
     }
     return bad;
   });
@@ -1906,7 +2021,11 @@ extern "C" int aerof_gpu_linearized_solve_batch(aerof_gpu_ctx* c, const double* 
       const size_t ld = (n + 63) / 64 * 64;
       const cudaMemcpyKind kb = is_device_ptr(B) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
       const cudaMemcpyKind kx = is_device_ptr(X) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-      const size_t per = ((size_t)2 * krylov + 5) * ld * sizeof(double) + ((size_t)inner_its + 5) * ld * sizeof(float);
+      // per right-hand side: the outer FP64 bases and work vectors, the inner
+      // FP32 basis and work vectors and, with ILU(0), the sweeps' FP64 work
+      // vector (5N doubles)
+      const size_t per = ((size_t)2 * krylov + 5 + (c->imp.pc == AEROF_PC_ILU0 ? 1 : 0)) * ld * sizeof(double) +
+                         ((size_t)inner_its + 5) * ld * sizeof(float);
       size_t freeb = 0, totalb = 0;
       AEROF_CUDA(cudaMemGetInfo(&freeb, &totalb));
       const int G = (int)std::max<size_t>(1, std::min<size_t>((size_t)nrhs, (size_t)(0.7 * (double)freeb) / per));

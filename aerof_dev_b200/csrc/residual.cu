@@ -9,7 +9,6 @@
 // Edge.C:391-435, SubDomain.C:341-370), then its boundary faces in face
 // order (Face.C:1185-1215).  No floating-point atomics are used.
 #include <cstdlib>
-#include <mutex>
 
 #include "common.cuh"
 #include "physics.cuh"
@@ -388,8 +387,9 @@ __device__ __forceinline__ void edge_flux_rec(const Gas& g, int rec, double beta
       else linear_rec(beta, pi[k], ddVij, pj[k], ddVji, Vi[k], Vj[k]);
     }
   }
-  const bool bi = Vi[0] <= 0.0 || Vi[4] <= 0.0;
-  const bool bj = Vj[0] <= 0.0 || Vj[4] <= 0.0;
+  // written as !(x > 0) so that a non-finite state counts as unphysical too
+  const bool bi = !(Vi[0] > 0.0) || !(Vi[4] > 0.0);
+  const bool bj = !(Vj[0] > 0.0) || !(Vj[4] > 0.0);
 #pragma unroll
   for (int k = 0; k < 5; ++k) f[k] = 0.0;
   if (bi || bj) {
@@ -1256,34 +1256,67 @@ extern "C" int aerof_gpu_rk2(aerof_gpu_ctx* c, double* U, double cfl, int nsteps
 // capture.  All calls share the one array: two calls that overlap on the
 // GPU (other streams, other contexts on the same device) race on it.
 //
-// Limit: the scratch holds 5E + 16N doubles (fluxes, gradients) plus N ints
-// (failsafe tags) plus 8 ints (counters), at most kNoAllocScratchDoubles =
-// 2,097,152 doubles (16 MiB), i.e. meshes up to roughly 40,000 nodes (a 34^3
-// lattice).  Every GPU that loads the library holds these 16 MiB until the
-// process exits.
+// Limit: the scratch holds the per-edge fluxes (5E doubles), the gradients
+// (16N doubles, 16-byte vector stores) and 8 counters plus N failsafe tags
+// (ints), each part starting on a 256-byte boundary:
+//   noalloc_need(N, E) = a(a(5E) + 16N) + ceil((N + 8)/2) doubles, a(x) = x
+//   rounded up to a multiple of 32,
+// at most kNoAllocScratchDoubles = 2,097,152 doubles (16 MiB), i.e. meshes
+// up to roughly 40,000 nodes (a 34^3 lattice).
+//
+// Residency: with lazy module loading (the CUDA 12 default) the array would
+// only be reserved when this file's module first loads, which for a caller
+// that hands the rest of the device to its own pool could be too late.  So
+// aerof_gpu_create looks up its device address (noalloc_attach, with the
+// context's device current), which loads the module and reserves the 16 MiB
+// at context creation; the address is kept in the context, so a context
+// created after a device reset looks it up afresh.  Every GPU on which a
+// context is created holds these 16 MiB until the process exits.
 namespace aerof {
 
 constexpr size_t kNoAllocScratchDoubles = 2u * 1024u * 1024u;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
 
-// Device address of g_noalloc_scratch per device, looked up once per device
-// with that device current (host code cannot use the symbol itself).
-static std::mutex g_noalloc_mu;
-static double* g_noalloc_addr[128] = {nullptr};
+static size_t align32(size_t n) { return (n + 31) / 32 * 32; }
 
-static double* noalloc_scratch(int dev) {
-  if (dev < 0 || dev >= 128) throw ApiError{AEROF_EINVAL, "device ordinal out of range"};
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      cudaGetLastError();
-      throw ApiError{AEROF_ECUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e)};
-    }
-    g_noalloc_addr[dev] = static_cast<double*>(p);
+struct NoAllocLayout {
+  size_t G, cnt, need;  // offsets of the gradients and the counters, total doubles
+};
+static NoAllocLayout noalloc_layout(size_t N, size_t E) {
+  NoAllocLayout l;
+  l.G = align32(5 * E);
+  l.cnt = align32(l.G + 16 * N);
+  l.need = l.cnt + (N + 8 + 1) / 2;
+  return l;
+}
+
+// Called by aerof_gpu_create with the context's device current: host code
+// cannot hand g_noalloc_scratch itself to a kernel (in host code the name is
+// a host-side stand-in), so the device address is looked up here.
+void noalloc_attach(aerof_gpu_ctx* c) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    cudaGetLastError();
+    c->noalloc_scratch = nullptr;
+    c->noalloc_error = std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e);
+    return;
   }
-  return g_noalloc_addr[dev];
+  // with lazy loading a kernel's code is also placed in device memory on its
+  // first launch; the kernels of the allocation-free path are loaded here
+  const void* kernels[] = {(const void*)k_prim, (const void*)k_grad, (const void*)k_edge_flux,
+                           (const void*)k_node_residual_t<false>};
+  for (const void* k : kernels) {
+    cudaFuncAttributes a;
+    e = cudaFuncGetAttributes(&a, k);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      c->noalloc_scratch = nullptr;
+      c->noalloc_error = std::string("cudaFuncGetAttributes: ") + cudaGetErrorString(e);
+      return;
+    }
+  }
+  c->noalloc_scratch = static_cast<double*>(p);
 }
 
 }  // namespace aerof
@@ -1297,18 +1330,29 @@ extern "C" int aerof_gpu_residual_noalloc(aerof_gpu_ctx* c, const double* U, dou
       return AEROF_EINVAL;
     }
     DeviceMesh& m = c->mesh;
-    const size_t need = 5 * (size_t)m.E + 16 * (size_t)m.N + ((size_t)m.N + 1) / 2 + 4;
-    if (need > kNoAllocScratchDoubles) {
-      c->last_error = "mesh too large for aerof_gpu_residual_noalloc: needs " + std::to_string(need) +
-                      " doubles of scratch (5E + 16N + N/2 + 4), the fixed array holds " +
-                      std::to_string(kNoAllocScratchDoubles);
+    const NoAllocLayout lay = noalloc_layout(m.N, m.E);
+    if (lay.need > kNoAllocScratchDoubles) {
+      c->last_error = "mesh too large for aerof_gpu_residual_noalloc: needs " + std::to_string(lay.need) +
+                      " doubles of scratch (5E + 16N + (N + 8)/2, parts on 256-byte boundaries), the fixed "
+                      "array holds " + std::to_string(kNoAllocScratchDoubles);
       return AEROF_EINVAL;
     }
-    double* base = noalloc_scratch(c->dev);
+    double* base = c->noalloc_scratch;
+    if (!base) {
+      c->last_error = "allocation-free scratch unavailable on this device: " + c->noalloc_error;
+      return AEROF_ECUDA;
+    }
     double* flux = base;
-    double* G = flux + 5 * (size_t)m.E;
-    int* cnt = reinterpret_cast<int*>(G + 16 * (size_t)m.N);
+    double* G = base + lay.G;
+    int* cnt = reinterpret_cast<int*>(base + lay.cnt);
     int* tag = cnt + 8;
+    // every part must start on a 256-byte boundary (G takes 16-byte vector
+    // stores); a wrong offset fails here, never on the GPU
+    if (reinterpret_cast<uintptr_t>(base) % 256 || reinterpret_cast<uintptr_t>(G) % 256 ||
+        reinterpret_cast<uintptr_t>(cnt) % 256) {
+      c->last_error = "allocation-free scratch misaligned";
+      return AEROF_EINVAL;
+    }
     cudaStream_t s = c->stream;
     const Gas g = make_gas(c->cfg.gamma);
     const int rec = c->cfg.reconstruction;

@@ -107,6 +107,14 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def gpu_uuid(local: int):
+    import torch
+    try:
+        return "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        return None
+
+
 def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
         int(os.environ.get("LOCAL_RANK", "0"))
@@ -120,13 +128,26 @@ def build_workload(n: int):
     return W, mesh, Ub, U
 
 
-def cpu_baseline(mesh, Ub, U, E: int, budget_s: float = 20.0, max_evals: int = 20) -> dict:
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline(mesh, Ub, U, E: int, budget_s: float = 20.0, max_evals: int = 20, o=None,
+                 out=None) -> dict:
     """CPU oracle (restatement of the reference's loops), all host threads,
-    on a bounded number of full evaluations of the same workload."""
+    on a bounded number of full evaluations of the same workload.  The last
+    evaluation is left in `out` (the parity check reads it)."""
     from oracle.oracle import Oracle
-    o = Oracle(mesh)
+    o = o or Oracle(mesh)
     cores = os.cpu_count() or 1
-    out = np.empty_like(U)
+    out = np.empty_like(U) if out is None else out
     o.residual_threaded(U, Ub, 2, nthreads=cores, out=out)  # warm-up
     t0 = time.perf_counter()
     k = 0
@@ -137,6 +158,7 @@ def cpu_baseline(mesh, Ub, U, E: int, budget_s: float = 20.0, max_evals: int = 2
             break
     dt = time.perf_counter() - t0
     return {"value": E * k / dt / 1e6, "unit": "Medges/s", "cores": cores, "kind": "port",
+            "cpu_model": cpu_model(),
             "sample": f"{k} full second-order residual evaluations of the 101^3 mesh after 1 warm-up "
                       f"({dt:.1f} s), OpenMP over {cores} threads, g++ -O3 -march=x86-64-v3"}
 
@@ -151,9 +173,14 @@ def run_reference(args):
     o = Oracle(mesh)
     cores = os.cpu_count() or 1
     out = np.empty_like(U)
+    # the requested warm-up evaluations, within a bounded share of the budget
+    t0 = time.perf_counter()
+    nw = 0
     for _ in range(max(args.warmup, 1)):
         o.residual_threaded(U, Ub, 2, nthreads=cores, out=out)
-        break  # one warm-up evaluation is enough on the CPU
+        nw += 1
+        if time.perf_counter() - t0 > 0.25 * args.ref_budget:
+            break
     # each step is one full evaluation; the number of timed steps is capped
     # so the run stays within a few minutes
     t0 = time.perf_counter()
@@ -167,10 +194,11 @@ def run_reference(args):
     value = s["E"] * k / dt / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Medges/s", "n_gpus": args.gpus,
-        "steps": k, "requested_steps": args.steps, "warmup": 1, "ms_per_step": dt / k * 1e3,
+        "steps": k, "requested_steps": args.steps, "warmup": nw, "ms_per_step": dt / k * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config_dict(args, s),
         "cpu_baseline": {"value": value, "unit": "Medges/s", "cores": cores, "kind": "port",
+                         "cpu_model": cpu_model(),
                          "sample": f"{k} full evaluations (capped at {args.ref_budget:.0f} s of the "
                                    f"{args.steps} requested), OpenMP over {cores} threads"},
         "e2e": {"value": value, "unit": "Medges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -185,6 +213,97 @@ def config_dict(args, s) -> dict:
             "mesh_n": args.n, "N": s["N"], "E": s["E"], "F_b": s["F"], "evals_per_step": 1,
             "l2": "working set > 126 MB L2 (node data 0.2 GB + edge data 0.5 GB); no flush",
             "parallelism": f"replicas x{args.gpus}", "kernel": getattr(args, "kernel", "blocked")}
+
+
+def timed_on(stream, fn, reps: int, warm: int = 3) -> float:
+    """Mean device milliseconds of fn() over reps calls, CUDA events on the
+    stream the library runs on, after warm calls."""
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def parity_part(A, ctx, o, U, Rgpu, Rref) -> dict:
+    """Relative L2 of the GPU residual (the timed evaluations' output) and of
+    the LSQ gradients (aerof_gpu_gradients) against the CPU oracle on the
+    benchmark's own state and mesh."""
+    def rel(a, b):
+        a = np.asarray(a, dtype=np.float64)
+        b = np.asarray(b, dtype=np.float64)
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    V = o.prim(U)
+    got = A.SpaceOperator(ctx).computeGradients(V)
+    ref = o.gradients(V)
+    return {"residual_rel_l2": rel(Rgpu, Rref),
+            "gradients_rel_l2": [rel(a, b) for a, b in zip(got, ref)],
+            "tolerance": 1e-12,
+            "oracle": "C++ restatement of the reference's CPU loops (FP64), same U and mesh"}
+
+
+def newton_part(A, ctx, U, args, uuid) -> dict:
+    """Mixed-precision vs all-FP64 pseudo-transient Newton-GMRES to
+    ||R||/||R0|| <= 1e-8 (CFL 10 -> 1e4, RESIDUAL law ser 0.7, GMRES(30)
+    eps 1e-2, block-Jacobi) on the benchmark's mesh and state; device time of
+    aerof_gpu_newton, clocks sampled during both solves."""
+    import torch
+    res, states = {}, {}
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    time.sleep(0.2)
+    for name, prec in (("mixed", A.PREC_FP32), ("fp64", A.PREC_FP64)):
+        sol = A.ImplicitSteadySolver(ctx, precision=prec, cfl0=10.0, cfl_max=1e4, ser=0.7, ksp_eps=1e-2,
+                                     krylov=30, maxits=30, tol=1e-8, max_steps=args.max_steps)
+        ctx.timers()
+        ctx.profile(True)
+        Uo, info = sol.solve(torch.from_numpy(U).cuda())
+        tm = ctx.timers()
+        ctx.profile(False)
+        states[name] = Uo
+        res[name] = {"seconds": info["seconds"], "steps": info["steps"], "gmres_its": info["linear_its"],
+                     "rel_residual": info["rel_residual"],
+                     "timers_s": {k: v[0] / 1e3 for k, v in tm.items() if v[1]}}
+    clk = clocks.stop()
+    d = (torch.linalg.norm(states["mixed"] - states["fp64"]) / torch.linalg.norm(states["fp64"])).item()
+    return {"speedup_mixed_vs_fp64": res["fp64"]["seconds"] / res["mixed"]["seconds"],
+            "unit": "x (FP64 time / mixed time to ||R||/||R0|| <= 1e-8)",
+            "mixed": res["mixed"], "fp64": res["fp64"], "state_rel_l2_mixed_vs_fp64": d,
+            "config": "second-order FP64 residual, first-order H1 Jacobian (FP32 or FP64 blocks), block-Jacobi, "
+                      "GMRES(30) eps 1e-2, CFL 10 -> 1e4; timers are disjoint device-time categories",
+            "clocks": clk}
+
+
+def adjoint_cost_part(A, ctx, Ud, stream, uuid) -> dict:
+    """Device time of the adjoint products over one primal residual on the
+    benchmark's mesh and state: both products of the adjoint gradient from
+    one reverse sweep (J^T lambda and dR/dX^T lambda), and J^T w / J p from
+    the stored exact linearisation (the operator the adjoint GMRES applies)."""
+    import torch
+    sp, S = A.SpaceOperator(ctx), A.Sensitivity(ctx)
+    lam = torch.from_numpy(np.random.default_rng(3).standard_normal((ctx.N, 5))).cuda()
+    R = torch.empty_like(Ud)
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    time.sleep(0.2)
+    t_res = timed_on(stream, lambda: sp.computeResidual(Ud, R), 20)
+    t_both = timed_on(stream, lambda: S.adjoint_products(Ud, lam), 10)
+    S.h2_evaluate(Ud)
+    t_h2t = timed_on(stream, lambda: S.h2_apply(lam, transpose=True), 20)
+    t_h2 = timed_on(stream, lambda: S.h2_apply(lam), 20)
+    S.h2_release()
+    clk = clocks.stop()
+    return {"adjoint_products_over_residual": t_both / t_res,
+            "stored_JT_over_residual": t_h2t / t_res, "stored_J_over_residual": t_h2 / t_res,
+            "ms": {"residual_sync_call": t_res, "adjoint_products": t_both, "stored_JT": t_h2t, "stored_J": t_h2},
+            "unit": "x one primal residual (synchronous calls, device time)", "clocks": clk}
 
 
 def run_ours(args):
@@ -300,7 +419,16 @@ def run_ours(args):
         "unphysical_states": bad,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(mesh, Ub, U, s["E"])
+        from oracle.oracle import Oracle
+        o = Oracle(mesh)
+        Rref = np.empty_like(U)
+        line["cpu_baseline"] = cpu_baseline(mesh, Ub, U, s["E"], o=o, out=Rref)
+        line["parity"] = parity_part(A, ctx, o, U, Rd.cpu().numpy(), Rref)
+        del o
+    if world == 1 and not args.no_adjoint_cost:
+        line["adjoint_cost"] = adjoint_cost_part(A, ctx, Ud, stream, uuid)
+    if world == 1 and not args.no_newton:
+        line["newton"] = newton_part(A, ctx, U, args, uuid)
     ctx.close()
     if pg:
         pg.destroy_process_group()
@@ -316,6 +444,8 @@ def run_newton(args):
     import torch
     import aerof_dev_b200 as A
     torch.cuda.set_device(0)
+    clocks = ClockSampler(gpu_uuid(0))
+    clocks.start()
     W, mesh, Ub, U = build_workload(args.n)
     s = W.lattice_sizes(args.n)
     t0 = time.perf_counter()
@@ -344,6 +474,7 @@ def run_newton(args):
                                    + ("block ILU(0), multicolour" if args.pc == "ilu" else "block-Jacobi") + ", GMRES(30)",
                        "preconditioner": args.pc, "mesh_setup_s": setup_s},
             "mixed": res["mixed"], "fp64": res["fp64"], "state_rel_l2_mixed_vs_fp64": d}
+    line["clocks"] = clocks.stop()
     print(json.dumps(line), flush=True)
     ctx.close()
     return 0
@@ -357,6 +488,8 @@ def run_adjoint(args):
     import aerof_dev_b200 as A
     from aerof_dev_b200 import sensitivity as S
     torch.cuda.set_device(0)
+    clocks = ClockSampler(gpu_uuid(0))
+    clocks.start()
     W = __import__("aerof_dev_b200.workloads", fromlist=["x"])
     mesh = W.make_lattice_mesh(args.n, jitter=0.2, codes="channel")
     X = mesh["X"] + W.shape_modes(mesh["X"], 1, sigma=0.25, amplitude=0.04, seed=7)[0]
@@ -423,6 +556,7 @@ def run_adjoint(args):
             "max_rel_err_vs_richardson": float(np.abs(ga[:nfd] - gr).max() / np.abs(gr).max()),
             "max_rel_err_vs_fd_1e-6": float(np.abs(ga[:nfd] - g6).max() / np.abs(g6).max()),
             "newton": {k: v for k, v in info.items() if k != "history"}}
+    line["clocks"] = clocks.stop()
     print(json.dumps(line), flush=True)
     return 0
 
@@ -438,6 +572,8 @@ def run_sensitivities(args):
     import aerof_dev_b200 as A
     from aerof_dev_b200 import sensitivity as S
     torch.cuda.set_device(0)
+    clocks = ClockSampler(gpu_uuid(0))
+    clocks.start()
     W = __import__("aerof_dev_b200.workloads", fromlist=["x"])
     mesh = W.make_lattice_mesh(args.n, jitter=0.2, codes="channel")
     X = mesh["X"] + W.shape_modes(mesh["X"], 1, sigma=0.25, amplitude=0.04, seed=7)[0]
@@ -484,6 +620,7 @@ def run_sensitivities(args):
     if g6 is not None:
         line["fd_step_1e-6"] = g6.tolist()
         line["max_rel_batched_vs_fd_1e-6"] = float(np.abs(gb[:nfd] - g6).max() / np.abs(g6).max())
+    line["clocks"] = clocks.stop()
     print(json.dumps(line), flush=True)
     ctx.close()
     return 0
@@ -498,6 +635,8 @@ def run_adjoint_products(args):
     import aerof_dev_b200 as A
     from aerof_dev_b200 import workloads as W
     torch.cuda.set_device(0)
+    clocks = ClockSampler(gpu_uuid(0))
+    clocks.start()
     mesh = W.make_lattice_mesh(args.n, jitter=0.2, codes="channel")
     Ub = W.freestream(0.8)
     ctx = A.Context.from_mesh(mesh, Ub, reconstruction=args.rec)
@@ -535,6 +674,7 @@ def run_adjoint_products(args):
             "h2_jvp_over_residual": out["h2_jvp"] / out["residual"],
             "config": {"workload": f"{args.n}^3 jittered Kuhn tet mesh N={s['N']} E={s['E']}, smooth Mach 0.8 state",
                        "reconstruction": {1: "constant", 2: "van Albada", 3: "linear"}[args.rec]}}
+    line["clocks"] = clocks.stop()
     print(json.dumps(line), flush=True)
     ctx.close()
     return 0
@@ -550,6 +690,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=200)
     ap.add_argument("--ref-budget", type=float, default=120.0, help="seconds of timed CPU work (reference arm)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-newton", action="store_true", help="leave the Newton part out of the residual line")
+    ap.add_argument("--no-adjoint-cost", action="store_true",
+                    help="leave the adjoint-cost part out of the residual line")
     ap.add_argument("--workload", choices=["residual", "newton", "adjoint", "adjoint_products", "sensitivities"],
                     default="residual")
     ap.add_argument("--max-steps", type=int, default=400)

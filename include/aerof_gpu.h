@@ -6,8 +6,8 @@
  * template classes (SpaceOperator<dim>, MatVecProd<dim,neq>,
  * KspPrec<dim,Scalar>, KspSolver<...>).  Each entry point below replaces one
  * member of that call surface; the citation names the reference function
- * (file:line in the AERO-F tree) whose contract it keeps.  A C++ shim that
- * subclasses those classes and forwards here is shown in INTEGRATION.md.
+ * (file:line in the AERO-F tree) whose contract it keeps.  A C++ shim
+ * subclasses those classes and forwards to these entry points.
  *
  * Conventions
  *  - Every function returns int: 0 = AEROF_OK, > 0 = number of unphysical
@@ -39,6 +39,8 @@ extern "C" {
 #define AEROF_ETIMEDOUT -4 /* bounded wait expired */
 #define AEROF_ESINGULAR -5 /* zero pivot in a 5x5 diagonal block */
 #define AEROF_ESTATE -6    /* call order violated (e.g. no mesh set) */
+#define AEROF_EDIVERGED -7 /* Newton updates stayed non-physical down to
+                              CFL cfl0/1000 (TsParameters.C:187-195)      */
 
 /* Boundary codes (BcDef.h:5-28) understood by the face kernels. */
 #define AEROF_BC_SLIP_WALL_MOVING -2
@@ -105,6 +107,9 @@ typedef struct aerof_newton_result {
   int linear_its;       /* total GMRES iterations                    */
   double rel_residual;  /* final ||R||/||R0||                        */
   double seconds;       /* device time of the solve (CUDA events)    */
+  int redos;            /* steps redone at half the CFL number after a
+                           non-physical update (NewtonSolver.h:195-205) */
+  int reserved[3];
 } aerof_newton_result;
 
 /* ---- context ---------------------------------------------------------- */
@@ -169,12 +174,14 @@ int aerof_gpu_status(aerof_gpu_ctx* ctx);
  * counterpart in the reference; it is an addition of this library.
  * - U and R must be device pointers (host arrays would need staging buffers).
  * - Scratch (per-edge fluxes, gradients, tags, counters) lives in one fixed
- *   16 MiB array of device memory inside the library, held by every GPU that
- *   loads it until the process exits.  Meshes needing more than
- *   5E + 16N + N/2 + 4 <= 2,097,152 doubles (about 40,000 nodes) are rejected
- *   with AEROF_EINVAL and a message in aerof_gpu_last_error.
- * - The first call on a device looks up the array's device address; make
- *   that first call before any stream capture.
+ *   16 MiB array of device memory inside the library.  aerof_gpu_create
+ *   claims it on the context's device (it loads the library's residual
+ *   module and looks up the array's device address there), so the 16 MiB
+ *   are taken at context set-up, before the caller hands the rest of the
+ *   device to its own pool, and stay taken until the process exits.
+ *   Meshes needing more than a(a(5E) + 16N) + (N + 8)/2 <= 2,097,152 doubles
+ *   (a(x): x rounded up to a multiple of 32; about 40,000 nodes) are
+ *   rejected with AEROF_EINVAL and a message in aerof_gpu_last_error.
  * - Every call shares the array and the previous call's contents stay in it
  *   (the call clears what must start at zero).  Calls that overlap on the GPU
  *   -- on other streams or from other contexts on the same device -- race.
@@ -202,6 +209,13 @@ int aerof_gpu_jacobian(aerof_gpu_ctx* ctx, const double* U, const double* dt, in
 /* The assembled H1 operator in MvpMat layout a[N+2E][25] (MvpMatrix.h:10-80),
  * reference numbering, as double.                                          */
 int aerof_gpu_get_jacobian(aerof_gpu_ctx* ctx, double* A);
+/* The reverse of aerof_gpu_get_jacobian: an H1 operator assembled by the
+ * caller, in the MvpMat layout a[N+2E][25] (reference numbering, as
+ * MvpMat<Scalar,5> holds it, MvpMatrix.h:10-80), becomes the context's
+ * operator in the given precision, as if aerof_gpu_jacobian had assembled it
+ * (a caller that adds terms of its own to the matrix, or one that keeps
+ * the reference's assembly).                                              */
+int aerof_gpu_set_jacobian(aerof_gpu_ctx* ctx, const double* A, int precision);
 /* MatVecProdH1::apply / applyTranspose (MatVecProd.C:1165-1208,
  * SubDomain.C:3916-3995): y = A p or A^T p, p,y [N][5].                   */
 int aerof_gpu_matvec(aerof_gpu_ctx* ctx, const double* p, double* y, int transpose);
@@ -226,7 +240,13 @@ int aerof_gpu_gmres(aerof_gpu_ctx* ctx, const double* b, double* x, int krylov, 
 /* TsSolver::resolve + NewtonSolver::solve (maxIts=1) for a steady problem
  * (TsSolver.h:231-380, NewtonSolver.h:70-231, ImplicitCoupledTsDesc.C:
  * 85-300): U[N][5] updated in place; history (optional, max_steps+1
- * entries) receives ||R||/||R0|| per step.                                 */
+ * entries) receives ||R||/||R0|| per step.  After every update the state
+ * is checked (SubDomain::checkSolution, SubDomain.C:6746-6806): if a node
+ * has a non-positive (or non-finite) density or pressure, U is restored and
+ * the step redone at half the CFL number (NewtonSolver.h:195-205,
+ * TsParameters.C:187-195); out->redos counts those.  When the CFL number
+ * falls below cfl0/1000 the call returns AEROF_EDIVERGED with U restored to
+ * the last physical state.  A non-finite residual returns AEROF_EINVAL.    */
 int aerof_gpu_newton(aerof_gpu_ctx* ctx, double* U, const aerof_newton_params* p,
                      aerof_newton_result* out, double* history);
 

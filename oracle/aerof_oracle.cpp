@@ -1418,31 +1418,61 @@ int orc_gmres(void* h, const double* A, const double* Dinv, const double* b, dou
 // FP64; block-Jacobi in FP32 (fp32_prec) or FP64.  Stops when
 // ||R(Q)||/||R(Q0)|| <= tol or after max_steps.  history (max_steps+1
 // entries) receives the relative residuals; returns the steps taken.
+//
+// After every update the physical-solution check (NewtonSolver.h:187-215,
+// SubDomain::checkSolution SubDomain.C:6746-6806): a node value with a
+// non-positive density or pressure restores the state and the step is
+// redone at half the CFL number (TsParameters::computeCflNumber,
+// TsParameters.C:187-195); below cfl0/1000 the reference aborts, here the
+// call returns -7.  *redos (optional) counts the redone steps.
 int orc_newton(void* h, double* U, const double* Ub, int order, double cfl0, double cflMin,
                double cflMax, double ser, int numVec, int maxits, double eps, double tol,
-               int max_steps, int fp32_prec, double* history, int* lin_its) {
+               int max_steps, int fp32_prec, double* history, int* lin_its, int* redos) {
   Mesh* m = (Mesh*)h;
   const int N = m->N;
   const size_t n5 = 5 * (size_t)N;
-  std::vector<double> R(n5), dt(N), A(25 * ((size_t)N + 2 * (size_t)m->E)), Dinv(25 * (size_t)N), dQ(n5);
+  std::vector<double> R(n5), rhs(n5), dt(N), A(25 * ((size_t)N + 2 * (size_t)m->E)), Dinv(25 * (size_t)N),
+      dQ(n5), Uprev(n5);
   double res0 = 0.0, cfl = cfl0, rel_prev = 1.0;
-  int k;
-  for (k = 0; k <= max_steps; ++k) {
-    orc_residual(h, U, Ub, order, 1.0 / 3.0, 0, R.data());
-    double res = std::sqrt(std::inner_product(R.begin(), R.end(), R.begin(), 0.0));
-    if (k == 0) res0 = res;
-    double rel = res / res0;
-    if (history) history[k] = rel;
-    if (rel <= tol || k == max_steps) break;
-    if (k > 0) cfl = std::min(std::max(cfl * std::pow(rel_prev / rel, ser), cflMin), cflMax);
-    rel_prev = rel;
+  int k = 0, nredo = 0;
+  bool redo = false;
+  if (redos) *redos = 0;
+  while (k <= max_steps) {
+    if (!redo) {
+      orc_residual(h, U, Ub, order, 1.0 / 3.0, 0, R.data());
+      double res = std::sqrt(std::inner_product(R.begin(), R.end(), R.begin(), 0.0));
+      if (k == 0) res0 = res;
+      double rel = res / res0;
+      if (history) history[k] = rel;
+      if (rel <= tol || k == max_steps) break;
+      if (k > 0) cfl = std::min(std::max(cfl * std::pow(rel_prev / rel, ser), cflMin), cflMax);
+      rel_prev = rel;
+    }
+    redo = false;
     timestep(*m, U, cfl, dt.data());
     jacobian(*m, U, Ub, dt.data(), A.data());
     orc_bj_invert(h, A.data(), Dinv.data(), fp32_prec);
-    for (size_t q = 0; q < n5; ++q) R[q] = -1.0 * R[q];
-    int its = orc_gmres(h, A.data(), Dinv.data(), R.data(), dQ.data(), numVec, maxits, eps, 0, nullptr);
+    for (size_t q = 0; q < n5; ++q) rhs[q] = -1.0 * R[q];
+    int its = orc_gmres(h, A.data(), Dinv.data(), rhs.data(), dQ.data(), numVec, maxits, eps, 0, nullptr);
     if (lin_its) lin_its[k] = its;
+    std::copy(U, U + n5, Uprev.begin());
     for (size_t q = 0; q < n5; ++q) U[q] += dQ[q];
+    int bad = 0;
+    for (int i = 0; i < N; ++i) {
+      double V[5];
+      cons2prim<double>(1.4, U + 5 * (size_t)i, V);
+      bad += (V[0] <= 0.0 || std::isnan(V[0])) + (V[4] <= 0.0 || std::isnan(V[4]));
+    }
+    if (bad) {
+      std::copy(Uprev.begin(), Uprev.end(), U);
+      ++nredo;
+      if (redos) *redos = nredo;
+      cfl *= 0.5;
+      if (cfl < cfl0 / 1000.0) return -7;
+      redo = true;
+      continue;
+    }
+    ++k;
   }
   return k;
 }

@@ -5,7 +5,7 @@ Runs oracle/_ref/ref_golden (built from the AERO-F sources by
 and outputs in tests/golden/reference_pointwise.npz.  Only this script needs
 the reference tree; the tests read the committed .npz.
 
-    python tests/golden/make_golden.py [--ref /path/to/aerof]
+    python tests/golden/make_golden.py --ref /path/to/aerof
 """
 from __future__ import annotations
 
@@ -35,8 +35,11 @@ def run(kind: str, rows: np.ndarray, width: int) -> np.ndarray:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("AEROF_REF", "/root/reference"))
+    ap.add_argument("--ref", default=os.environ.get("AEROF_REFERENCE_TREE"),
+                    help="AERO-F source tree (or set AEROF_REFERENCE_TREE)")
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("name the AERO-F source tree with --ref or AEROF_REFERENCE_TREE")
     subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={a.ref}"])
     rng = np.random.Generator(np.random.PCG64(SEED))
     out = {}

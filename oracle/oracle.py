@@ -68,7 +68,7 @@ def lib():
         L.orc_ilu0.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, _dp, _dp, C.POINTER(C.c_int), _ip]
         L.orc_newton.argtypes = [C.c_void_p, _dp, _dp, C.c_int, C.c_double, C.c_double, C.c_double,
                                  C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
-                                 _dp, _ip]
+                                 _dp, _ip, _ip]
         L.orc_jvp.argtypes = [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp]
         L.orc_dRdX.argtypes = [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp, _dp]
         L.orc_residual_at.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_int, _dp]
@@ -200,10 +200,17 @@ class Oracle:
 
     def newton(self, U, Ub, order=2, cfl0=10.0, cfl_min=0.0, cfl_max=1e4, ser=0.7, numVec=30,
                maxits=30, eps=1e-2, tol=1e-8, max_steps=200, fp32_prec=True):
+        """Pseudo-transient Newton; returns (U, history, GMRES its per step).
+        self.last_redos holds the steps redone at half the CFL number after a
+        non-physical update; a CFL number driven below cfl0/1000 raises."""
         U = f64(U).copy()
         hist = np.zeros(max_steps + 1); lits = np.zeros(max_steps + 1, dtype=np.int32)
+        redos = np.zeros(1, dtype=np.int32)
         k = self.L.orc_newton(self.h, _d(U), _d(f64(Ub)), order, cfl0, cfl_min, cfl_max, ser, numVec,
-                              maxits, eps, tol, max_steps, int(fp32_prec), _d(hist), _i(lits))
+                              maxits, eps, tol, max_steps, int(fp32_prec), _d(hist), _i(lits), _i(redos))
+        self.last_redos = int(redos[0])
+        if k < 0:
+            raise RuntimeError(f"oracle Newton diverged (code {k}) after {self.last_redos} redone steps")
         return U, hist[:k + 1], lits[:k]
 
     def jvp(self, U, Ub, v, order=2):

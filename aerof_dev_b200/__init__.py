@@ -53,6 +53,7 @@ EXPORTS = [
     "aerof_gpu_update_coordinates", "aerof_gpu_linearized_solve", "aerof_gpu_residual_noalloc",
     "aerof_gpu_h2_evaluate", "aerof_gpu_h2_apply", "aerof_gpu_h2_release", "aerof_gpu_set_exact_operator",
     "aerof_gpu_linearized_solve_batch", "aerof_gpu_set_preconditioner", "aerof_gpu_set_jacobian",
+    "aerof_gpu_matvec_fd",
 ]
 TIMER_NAMES = ["nodal_grad", "fv_term", "time_step", "fv_jac", "prec_setup", "ksp_matvec", "ksp_other", "other"]
 
@@ -136,6 +137,7 @@ def library(path: str | None = None):
                                                  C.c_int, dp, dp],
             "aerof_gpu_set_preconditioner": [vp, C.c_int],
             "aerof_gpu_set_jacobian": [vp, dp, C.c_int],
+            "aerof_gpu_matvec_fd": [vp, dp, dp, dp, dp, C.c_int, dp, C.POINTER(C.c_double)],
         }
         for name, args in sig.items():
             if hasattr(L, name):
@@ -434,6 +436,34 @@ class MatVecProdH1:
         A = np.empty((ctx.N + 2 * ctx.E, 5, 5))
         ctx._check(ctx.L.aerof_gpu_get_jacobian(ctx.h, C.c_void_p(A.ctypes.data)))
         return A
+
+
+class MatVecProdFD:
+    """``MatVecProdFD`` (MatVecProd.C:262-372): finite-difference products
+    of the residual at the state given to ``evaluate``."""
+
+    def __init__(self, ctx: Context, fd_order: int = 1):
+        self.ctx, self.fd_order = ctx, fd_order
+        self.U = self.F = self.dt = None
+
+    def evaluate(self, U, F=None, dt=None):
+        """Keep the linearisation point (and R(U) when known, and the time
+        steps of the backward-Euler term)."""
+        self.U, self.F, self.dt = U, F, dt
+
+    def apply(self, p):
+        ctx = self.ctx
+        u = _Arg(self.U, np.float64, (ctx.N, 5))
+        f = _Arg(self.F, np.float64, (ctx.N, 5)) if self.F is not None else None
+        d = _Arg(self.dt, np.float64, (ctx.N,)) if self.dt is not None else None
+        a = _Arg(p, np.float64, (ctx.N, 5))
+        y = _like(p, (ctx.N, 5))
+        b = _Arg(y, np.float64, writable=True)
+        eps = C.c_double()
+        ctx._check(ctx.L.aerof_gpu_matvec_fd(ctx.h, u.ptr, f.ptr if f else None, a.ptr, d.ptr if d else None,
+                                             int(self.fd_order), b.ptr, C.byref(eps)))
+        self.eps = eps.value
+        return b.obj
 
 
 class JacobiPrec:

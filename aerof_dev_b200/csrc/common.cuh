@@ -216,6 +216,9 @@ struct Implicit {
   DBuf<float> ilu32;
   // flexible GMRES on the exact linearisation (outer FP64 vectors)
   DBuf<double> fV, fZ, fw, fr, fh;
+  // finite-difference products (MatVecProdFD): perturbed states and
+  // residuals, staged inputs, reduction partials
+  DBuf<double> fdQ, fdFp, fdFm, fdIn, fdRed;
   // lockstep solves of several right-hand sides: outer (FP64) and inner
   // (FP32) bases and work vectors, Hessenberg columns, pointer arrays of the
   // batched kernels

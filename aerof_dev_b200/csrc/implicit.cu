@@ -1702,6 +1702,110 @@ extern "C" int aerof_gpu_get_jacobian(aerof_gpu_ctx* c, double* A) {
   });
 }
 
+// ---------------------------------------------------------------------
+// MatVecProdFD::apply (MatVecProd.C:262-372): finite-difference products
+// of the residual (plus the backward-Euler time term when dt is given)
+// with the reference's step computeEpsilon (MatVecProd.C:879-929).
+
+// per block: sum of (1e-6 |U| + 1e-6) and of p^2 over a grid-stride
+// range, block tree in a fixed order (the partials are added on the host in
+// block order)
+__global__ void k_fd_eps_partial(size_t n, const double* __restrict__ U, const double* __restrict__ p,
+                                 double* __restrict__ part) {
+  __shared__ double su[kIB], sp[kIB];
+  double a = 0.0, b = 0.0;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    a += 1.e-6 * fabs(U[q]) + 1.e-6;
+    b += p[q] * p[q];
+  }
+  su[threadIdx.x] = a;
+  sp[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      su[threadIdx.x] += su[threadIdx.x + w];
+      sp[threadIdx.x] += sp[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = su[0];
+    part[gridDim.x + blockIdx.x] = sp[0];
+  }
+}
+// Q = U + a p
+__global__ void k_fd_shift(size_t n, double a, const double* __restrict__ U, const double* __restrict__ p,
+                           double* __restrict__ Q) {
+  const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) Q[q] = U[q] + a * p[q];
+}
+// F += (Q - U) / dt (the time term of add_dAW_dt with Un = U)
+__global__ void k_fd_time(size_t n, const double* __restrict__ Q, const double* __restrict__ U,
+                          const double* __restrict__ dt, double* __restrict__ F) {
+  const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) F[q] += (Q[q] - U[q]) / dt[q / 5];
+}
+// y = s (Fp - Fm)
+__global__ void k_fd_diff(size_t n, double s, const double* __restrict__ Fp, const double* __restrict__ Fm,
+                          double* __restrict__ y) {
+  const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) y[q] = s * (Fp[q] - Fm[q]);
+}
+
+// y = finite-difference product at device state dU; dF (R(dU), may be null),
+// ddt (may be null).  Returns eps.
+double matvec_fd_dev(aerof_gpu_ctx* c, const double* dU, const double* dF, const double* dp, const double* ddt,
+                     int fd_order, double* dy) {
+  DeviceMesh& m = c->mesh;
+  Implicit& J = c->imp;
+  cudaStream_t s = c->stream;
+  const size_t n = 5 * (size_t)m.N;
+  const int gv = grid_for(n, kIB);
+  constexpr int kFdBlocks = 296;  // 2 x 148 SMs
+  J.fdRed.ensure(2 * kFdBlocks);
+  k_fd_eps_partial<<<kFdBlocks, kIB, 0, s>>>(n, dU, dp, J.fdRed.p);
+  AEROF_LAUNCH_CHECK();
+  std::vector<double> part(2 * kFdBlocks);
+  AEROF_CUDA(cudaMemcpyAsync(part.data(), J.fdRed.p, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, s));
+  AEROF_CUDA(cudaStreamSynchronize(s));
+  double su = 0.0, sp = 0.0;
+  for (int b = 0; b < kFdBlocks; ++b) {
+    su += part[b];
+    sp += part[kFdBlocks + b];
+  }
+  const double norm = std::sqrt(sp);
+  const double eps = norm < 1.0e-14 ? 1.e-6 : su / ((double)n * norm);
+  J.fdQ.ensure(n);
+  J.fdFp.ensure(n);
+  J.fdFm.ensure(n);
+  k_fd_shift<<<gv, kIB, 0, s>>>(n, eps, dU, dp, J.fdQ.p);
+  AEROF_LAUNCH_CHECK();
+  residual_dev(c, J.fdQ.p, J.fdFp.p, true);
+  if (ddt) {
+    k_fd_time<<<gv, kIB, 0, s>>>(n, J.fdQ.p, dU, ddt, J.fdFp.p);
+    AEROF_LAUNCH_CHECK();
+  }
+  if (fd_order == 2) {
+    k_fd_shift<<<gv, kIB, 0, s>>>(n, -eps, dU, dp, J.fdQ.p);
+    AEROF_LAUNCH_CHECK();
+    residual_dev(c, J.fdQ.p, J.fdFm.p, true);
+    if (ddt) {
+      k_fd_time<<<gv, kIB, 0, s>>>(n, J.fdQ.p, dU, ddt, J.fdFm.p);
+      AEROF_LAUNCH_CHECK();
+    }
+    k_fd_diff<<<gv, kIB, 0, s>>>(n, 0.5 / eps, J.fdFp.p, J.fdFm.p, dy);
+  } else {
+    const double* Fm = dF;
+    if (!Fm) {
+      residual_dev(c, dU, J.fdFm.p, true);
+      Fm = J.fdFm.p;
+    }
+    k_fd_diff<<<gv, kIB, 0, s>>>(n, 1.0 / eps, J.fdFp.p, Fm, dy);
+  }
+  AEROF_LAUNCH_CHECK();
+  return eps;
+}
+
 // The reverse of aerof_gpu_get_jacobian: H1 given in the MvpMat layout
 // a[N+2E][25] (reference numbering) is stored in the sliced layout in the
 // requested precision, as if aerof_gpu_jacobian had assembled it.
@@ -1755,6 +1859,34 @@ extern "C" int aerof_gpu_set_jacobian(aerof_gpu_ctx* c, const double* A, int pre
     J.transposed = false;
     J.prec_ready = false;
     J.ilu_ready = false;
+    return AEROF_OK;
+  });
+}
+
+extern "C" int aerof_gpu_matvec_fd(aerof_gpu_ctx* c, const double* U, const double* F, const double* p,
+                                   const double* dt, int fd_order, double* y, double* eps) {
+  return guard(c, [&]() -> int {
+    need_mesh_or_throw(c);
+    if (!U || !p || !y || (fd_order != 1 && fd_order != 2)) return AEROF_EINVAL;
+    DeviceMesh& m = c->mesh;
+    Implicit& J = c->imp;
+    const size_t n = 5 * (size_t)m.N;
+    // inputs staged side by side: U, p, F, dt
+    J.fdIn.ensure(3 * n + (size_t)m.N);
+    auto stage = [&](const double* a, size_t cnt, size_t off) -> const double* {
+      if (!a) return nullptr;
+      if (is_device_ptr(a)) return a;
+      AEROF_CUDA(cudaMemcpyAsync(J.fdIn.p + off, a, cnt * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      return J.fdIn.p + off;
+    };
+    const double* dU = stage(U, n, 0);
+    const double* dp = stage(p, n, n);
+    const double* dF = stage(F, n, 2 * n);
+    const double* ddt = stage(dt, m.N, 3 * n);
+    double* dy = out_dev(c, y, n, c->s.Rstage);
+    const double e = matvec_fd_dev(c, dU, dF, dp, ddt, fd_order, dy);
+    out_finish(c, y, dy, n);
+    if (eps) *eps = e;
     return AEROF_OK;
   });
 }

@@ -41,13 +41,19 @@ template <class T> AEROF_HD T tabs(T a) { return vof(a) < 0.0 ? -a : a; }
 // ------------------------------------------------------------ fast reciprocals
 // Reciprocal and reciprocal square root for the primal double kernels: the
 // hardware approximation (PTX rcp.approx.ftz.f64 / rsqrt.approx.ftz.f64,
-// about 23 correct bits) refined by Newton-Raphson iteration: for 1/x the
-// third-order step r <- r + r (e + e^2), e = 1 - x r (one step takes 23
-// correct bits past double precision); for 1/sqrt x two second-order steps
-// y <- y + y/2 (1 - x y^2).  Results are within a few ulp of the correctly
-// rounded value.  Inputs are positive normal numbers (densities,
-// pressures, squared norms, positive denominators).  The dual-number
-// instantiation keeps exact division and square root.
+// about 23 correct bits) refined by Newton-Raphson iteration.  For 1/x:
+// with e = 1 - x r, 1/x = r / (1 - e) = r (1 + e + e^2 + ...), and the step
+// r <- r + r (e + e^2) keeps the series to second order, a third-order
+// iteration (one step takes 23 correct bits past double precision); this is
+// the series-expansion refinement of division described by Markstein
+// ("IA-64 and Elementary Functions", 2000) and by Ercegovac and Lang
+// ("Digital Arithmetic", 2004).  For 1/sqrt x: Newton's iteration on
+// f(y) = y^-2 - x, y <- y + y/2 (1 - x y^2), twice.  Inputs are positive
+// normal numbers (densities, pressures, squared norms, positive
+// denominators).  tests/test_gpu_fastmath.py bounds the error against the
+// correctly rounded values: at most 1 ulp (1/x) and 2 ulp (1/sqrt x) over a
+// sweep of inputs.  The dual-number instantiation keeps exact division and
+// square root.
 AEROF_HD double rcp_(double x) {
 #ifdef __CUDA_ARCH__
   double r;

@@ -219,6 +219,17 @@ int aerof_gpu_set_jacobian(aerof_gpu_ctx* ctx, const double* A, int precision);
 /* MatVecProdH1::apply / applyTranspose (MatVecProd.C:1165-1208,
  * SubDomain.C:3916-3995): y = A p or A^T p, p,y [N][5].                   */
 int aerof_gpu_matvec(aerof_gpu_ctx* ctx, const double* p, double* y, int transpose);
+/* MatVecProdFD::apply (MatVecProd.C:262-372): finite-difference product of
+ * the configured residual, prod = (F(U + eps p) - F(U)) / eps (fd_order 1)
+ * or (F(U + eps p) - F(U - eps p)) / (2 eps) (fd_order 2), with
+ * F = R + (U' - U)/dt when dt[N] is given (the backward-Euler time term,
+ * TimeState::add_dAW_dt, TimeState.C:40-73) and the reference's step
+ * (computeEpsilon, MatVecProd.C:879-929): eps = sum over the 5N state
+ * entries of (1e-6 |U| + 1e-6) / (5N ||p||), or 1e-6 when ||p|| < 1e-14.
+ * F (optional, first order only) is R(U) as MatVecProdFD::evaluate keeps
+ * it; without it R(U) is evaluated.  eps (optional) receives the step.    */
+int aerof_gpu_matvec_fd(aerof_gpu_ctx* ctx, const double* U, const double* F, const double* p, const double* dt,
+                        int fd_order, double* prod, double* eps);
 /* JacobiPrec::getData + setup (KspPrec.C:75-82,115-124; DiagMatrix.C:44-80):
  * invert the 5x5 diagonal blocks (LINPACK dgefa/dgedi) in the Jacobian's
  * precision.  Returns AEROF_ESINGULAR on a zero pivot.                    */

@@ -1460,7 +1460,7 @@ int orc_newton(void* h, double* U, const double* Ub, int order, double cfl0, dou
     int bad = 0;
     for (int i = 0; i < N; ++i) {
       double V[5];
-      cons2prim<double>(1.4, U + 5 * (size_t)i, V);
+      cons2prim<double>(m->gam, U + 5 * (size_t)i, V);
       bad += (V[0] <= 0.0 || std::isnan(V[0])) + (V[4] <= 0.0 || std::isnan(V[4]));
     }
     if (bad) {
@@ -1475,6 +1475,46 @@ int orc_newton(void* h, double* U, const double* Ub, int order, double cfl0, dou
     ++k;
   }
   return k;
+}
+
+// MatVecProdFD::apply (MatVecProd.C:262-372) with computeEpsilon
+// (MatVecProd.C:879-929): eps = sum over the state entries of
+// (1e-6 |U| + 1e-6) / (5 N ||p||), or 1e-6 when ||p|| < 1e-14; first order
+// prod = (F(U + eps p) - F(U)) / eps, second order (F(U + eps p) -
+// F(U - eps p)) / (2 eps), with F = R + (U - Un)/dt when dt is given (the
+// backward-Euler time term add_dAW_dt, TimeState.C:40-73, with Un = U).
+// F (optional) is R(U), as MatVecProdFD::evaluate keeps it.
+double orc_matvec_fd(void* h, const double* U, const double* Ub, int order, const double* F, const double* p,
+                     const double* dt, int fd_order, double* prod) {
+  Mesh* m = (Mesh*)h;
+  const size_t n5 = 5 * (size_t)m->N;
+  const double eps0 = 1.e-6;
+  double pp = 0.0;
+  for (size_t q = 0; q < n5; ++q) pp += p[q] * p[q];
+  const double norm = std::sqrt(pp);
+  double eps = eps0;
+  if (!(norm < 1.0e-14)) {
+    double loceps = 0.0;
+    for (size_t q = 0; q < n5; ++q) loceps += eps0 * std::fabs(U[q]) + eps0;
+    eps = loceps / (double(n5) * norm);
+  }
+  std::vector<double> Qp(n5), Qm(n5), Fp(n5), Fm(n5);
+  for (size_t q = 0; q < n5; ++q) Qp[q] = U[q] + eps * p[q];
+  orc_residual(h, Qp.data(), Ub, order, 1.0 / 3.0, 0, Fp.data());
+  if (dt)
+    for (size_t q = 0; q < n5; ++q) Fp[q] += (Qp[q] - U[q]) / dt[q / 5];
+  if (fd_order == 2) {
+    for (size_t q = 0; q < n5; ++q) Qm[q] = U[q] - eps * p[q];
+    orc_residual(h, Qm.data(), Ub, order, 1.0 / 3.0, 0, Fm.data());
+    if (dt)
+      for (size_t q = 0; q < n5; ++q) Fm[q] += (Qm[q] - U[q]) / dt[q / 5];
+    for (size_t q = 0; q < n5; ++q) prod[q] = (0.5 / eps) * (Fp[q] - Fm[q]);
+  } else {
+    if (F) std::copy(F, F + n5, Fm.begin());
+    else orc_residual(h, U, Ub, order, 1.0 / 3.0, 0, Fm.data());
+    for (size_t q = 0; q < n5; ++q) prod[q] = (1.0 / eps) * (Fp[q] - Fm[q]);
+  }
+  return eps;
 }
 
 // Exact forward-mode linearisation of the residual (T = Dual):

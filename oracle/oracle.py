@@ -70,6 +70,8 @@ def lib():
                                  C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
                                  _dp, _ip, _ip]
         L.orc_jvp.argtypes = [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp]
+        L.orc_matvec_fd.restype = C.c_double
+        L.orc_matvec_fd.argtypes = [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp, _dp, C.c_int, _dp]
         L.orc_dRdX.argtypes = [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp, _dp]
         L.orc_residual_at.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_int, _dp]
         L.orc_zforce.restype = C.c_double
@@ -212,6 +214,14 @@ class Oracle:
         if k < 0:
             raise RuntimeError(f"oracle Newton diverged (code {k}) after {self.last_redos} redone steps")
         return U, hist[:k + 1], lits[:k]
+
+    def matvec_fd(self, U, Ub, p, order=2, dt=None, fd_order=1, F=None):
+        """MatVecProdFD::apply: finite-difference Jacobian product; returns
+        (prod, eps)."""
+        U = f64(U); p = f64(p); prod = np.empty_like(U)
+        eps = self.L.orc_matvec_fd(self.h, _d(U), _d(f64(Ub)), order, _d(f64(F)) if F is not None else None,
+                                   _d(p), _d(f64(dt)) if dt is not None else None, int(fd_order), _d(prod))
+        return prod, eps
 
     def jvp(self, U, Ub, v, order=2):
         U = f64(U); v = f64(v); Jv = np.empty_like(U)

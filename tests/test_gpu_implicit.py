@@ -151,3 +151,38 @@ def test_newton_matches_oracle(gpu_lib, oracle_mod, prec):
     assert rel_l2(Ug, Ur) < (1e-9 if prec == 64 else 1e-7)
     R, _ = gpu_lib.SpaceOperator(ctx).computeResidual(Ug)
     assert np.linalg.norm(R) <= 1.01e-8 * np.linalg.norm(o.residual(U, Ub, 2)[0])
+
+
+@pytest.mark.parametrize("fd_order", [1, 2])
+def test_matvec_fd_parity(gpu_lib, oracle_mod, fd_order):
+    # MatVecProdFD::apply with the reference's computeEpsilon against the
+    # oracle's restatement (same step), and against the exact product
+    m = W.make_lattice_mesh(9, jitter=0.2, codes="channel")
+    Ub = W.freestream(0.8)
+    o = oracle_mod.Oracle(m)
+    U = W.perturbed_state(o.N, 0.8)
+    p = np.random.default_rng(5).standard_normal(U.shape)
+    ctx = gpu_lib.Context.from_mesh(m, Ub)
+    dt = gpu_lib.SpaceOperator(ctx).computeTimeStep(U, 50.0)
+    for with_dt in (False, True):
+        mv = gpu_lib.MatVecProdFD(ctx, fd_order)
+        mv.evaluate(U, dt=dt if with_dt else None)
+        y = mv.apply(p)
+        yr, eps_r = o.matvec_fd(U, Ub, p, 2, dt=dt if with_dt else None, fd_order=fd_order)
+        assert abs(mv.eps - eps_r) <= 1e-14 * eps_r
+        # the difference quotient amplifies the residuals' last-bit
+        # differences by |R| / (eps |J p|)
+        assert rel_l2(y, yr) < 1e-7
+        Jp = gpu_lib.Sensitivity(ctx).jvp(U, p)
+        if with_dt:
+            Jp = Jp + p / dt[:, None]
+        assert rel_l2(y, Jp) < (1e-4 if fd_order == 1 else 1e-7)
+    # R(U) given (evaluate keeps F): same product as evaluating it
+    if fd_order == 1:
+        R, _ = gpu_lib.SpaceOperator(ctx).computeResidual(U)
+        mv = gpu_lib.MatVecProdFD(ctx, 1)
+        mv.evaluate(U, F=R)
+        mv2 = gpu_lib.MatVecProdFD(ctx, 1)
+        mv2.evaluate(U)
+        assert np.array_equal(mv.apply(p), mv2.apply(p))
+    ctx.close()

@@ -1989,10 +1989,11 @@ extern "C" int aerof_gpu_newton(aerof_gpu_ctx* c, double* U, const aerof_newton_
       if (!redo) {
         bad += residual_dev(c, dU, R);
         double res = norm2_dev(c, R, n);
+        // a NaN initial residual would make res0 > 0 false and look converged
+        if (!std::isfinite(res)) throw ApiError{AEROF_EINVAL, "non-finite residual in Newton step " + std::to_string(k)};
         if (k == 0) res0 = res;
         rel = res0 > 0.0 ? res / res0 : 0.0;
         if (history) history[k] = rel;
-        if (!std::isfinite(rel)) throw ApiError{AEROF_EINVAL, "non-finite residual in Newton step " + std::to_string(k)};
         if (rel <= p->tol || k == p->max_steps) break;
         if (k > 0) cfl = std::min(std::max(cfl * std::pow(rel_prev / rel, p->ser), p->cfl_min), p->cfl_max);
         rel_prev = rel;

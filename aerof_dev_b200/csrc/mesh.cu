@@ -429,32 +429,24 @@ void geometry_dual(aerof_gpu_ctx* c, const Dual* XD, Dual* volD, Dual* enD, Dual
   AEROF_LAUNCH_CHECK();
 }
 
-// Rejects non-finite coordinates and tets whose volume
-// ((x1-x0) x (x2-x0)) . (x3-x0) / 6 is not positive: a degenerate or
-// inverted tet gives a zero or negative control-volume share
-// (ElemTetCore.C:102-112) and 1/ctrlVol would blow up.
-static int check_tets(aerof_gpu_ctx* c, int N, int T, const double* X, const int* tets) {
+// Rejects non-finite coordinates.
+static int check_coordinates(aerof_gpu_ctx* c, int N, const double* X) {
   for (size_t q = 0; q < 3 * (size_t)N; ++q)
     if (!std::isfinite(X[q])) {
       c->last_error = "non-finite coordinate of node " + std::to_string(q / 3);
       return AEROF_EINVAL;
     }
-  for (int t = 0; t < T; ++t) {
-    const double* x0 = X + 3 * (size_t)tets[4 * (size_t)t];
-    const double* x1 = X + 3 * (size_t)tets[4 * (size_t)t + 1];
-    const double* x2 = X + 3 * (size_t)tets[4 * (size_t)t + 2];
-    const double* x3 = X + 3 * (size_t)tets[4 * (size_t)t + 3];
-    const double a0 = x1[0] - x0[0], a1 = x1[1] - x0[1], a2 = x1[2] - x0[2];
-    const double b0 = x2[0] - x0[0], b1 = x2[1] - x0[1], b2 = x2[2] - x0[2];
-    const double d0 = x3[0] - x0[0], d1 = x3[1] - x0[1], d2 = x3[2] - x0[2];
-    const double vol = ((a1 * b2 - a2 * b1) * d0 + (a2 * b0 - a0 * b2) * d1 + (a0 * b1 - a1 * b0) * d2) / 6.0;
-    if (!(vol > 0.0)) {
-      c->last_error = "tet " + std::to_string(t) + " has a non-positive volume (" + std::to_string(vol) +
-                      "): tets must be positively oriented and not degenerate";
-      return AEROF_EINVAL;
-    }
-  }
   return AEROF_OK;
+}
+
+// Counts nodes whose dual control volume (ElemTetCore.C:102-112) is not
+// positive or not finite: the residual divides by it (SpaceOperator.C:
+// 614-620).  Inverted tets alone are accepted, as the reference accepts
+// them: the signed tet volumes around an interior node always add up to the
+// volume of its star.
+__global__ void k_check_vol(int N, const double* __restrict__ vol, int* __restrict__ nbad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < N && !(vol[i] > 0.0 && vol[i] < INFINITY)) atomicAdd(nbad, 1);
 }
 
 }  // namespace aerof
@@ -475,7 +467,7 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
         c->last_error = "unsupported boundary code " + std::to_string(codes[f]);
         return AEROF_EINVAL;
       }
-    if (int e = check_tets(c, N, T, X, tets)) return e;
+    if (int e = check_coordinates(c, N, X)) return e;
     c->has_mesh = false;
     c->imp.precision = 0;
     c->imp.prec_ready = false;
@@ -710,6 +702,21 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
     m.h_edges.swap(h.edges);
     compute_geometry(c);
     c->dual.geom_static = false;
+    {
+      DBuf<int> nb;
+      nb.alloc(1);
+      nb.zero(s);
+      k_check_vol<<<grid_for(m.N, kMBlock), kMBlock, 0, s>>>(m.N, m.vol.p, nb.p);
+      AEROF_LAUNCH_CHECK();
+      int bad = 0;
+      AEROF_CUDA(cudaMemcpyAsync(&bad, nb.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      AEROF_CUDA(cudaStreamSynchronize(s));
+      if (bad) {
+        c->last_error = std::to_string(bad) + " node(s) with a non-positive or non-finite control volume "
+                        "(degenerate tets)";
+        return AEROF_EINVAL;
+      }
+    }
     AEROF_CUDA(cudaStreamSynchronize(s));
     c->has_mesh = true;
     return AEROF_OK;

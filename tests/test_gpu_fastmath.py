@@ -2,11 +2,12 @@
 flux kernels (rcp_ / rsqrt_ in physics.cuh: the hardware rcp.approx /
 rsqrt.approx seeds refined by Newton-Raphson, the cubic series step
 r + r(e + e^2) for 1/x and two steps y + y/2 (1 - x y^2) for 1/sqrt x),
-measured in ulps against correctly rounded values (computed on the host in
-extended precision) beside CUDA's own 1.0/x and rsqrt(x), over a log-uniform
+measured in ulps against correctly rounded values (computed on the host with
+60-digit decimal arithmetic) beside CUDA's own 1.0/x and rsqrt(x), over a log-uniform
 sweep of positive normal inputs and the ranges the flux arithmetic sees."""
 import ctypes as C
 import os
+from decimal import Decimal, localcontext
 import subprocess
 
 import numpy as np
@@ -46,9 +47,12 @@ def test_fast_reciprocals_ulp_bounds(probe):
     out = np.empty((4, x.size))
     assert probe.fastmath_probe(x.ctypes.data, x.size, out.ctypes.data) == 0
     rcp_fast, rcp_cuda, rsq_fast, rsq_cuda = out
-    xl = x.astype(np.longdouble)
-    rcp_ref = (1 / xl).astype(np.float64)
-    rsq_ref = (1 / np.sqrt(xl)).astype(np.float64)
+    # correctly rounded references: 60-digit decimal arithmetic, rounded once
+    # to double (extended precision followed by a cast can round twice)
+    with localcontext() as ctx:
+        ctx.prec = 60
+        rcp_ref = np.array([float(1 / Decimal(v)) for v in x.tolist()])
+        rsq_ref = np.array([float(1 / Decimal(v).sqrt()) for v in x.tolist()])
     # CUDA's 1.0/x is the IEEE quotient: the extended-precision reference agrees
     assert _ulps(rcp_cuda, rcp_ref).max() <= 0.5
     e_rcp = _ulps(rcp_fast, rcp_ref)

@@ -2,8 +2,8 @@
 is provoked): a Newton update that makes the state non-physical (redone at
 half the CFL number, NewtonSolver.h:195-205, TsParameters.C:187-195), a CFL
 number driven below cfl0/1000 (AEROF_EDIVERGED), a singular diagonal block
-(AEROF_ESINGULAR, DiagMatrix.C:65-67), a non-finite input state, and a mesh
-with a degenerate tet (rejected at set_mesh)."""
+(AEROF_ESINGULAR, DiagMatrix.C:65-67), a non-finite input state, and a
+degenerate mesh (zero control volumes, rejected at set_mesh)."""
 import numpy as np
 import pytest
 
@@ -100,20 +100,20 @@ def test_nonfinite_state(gpu_lib, harsh, rec):
     ctx.close()
 
 
-def test_degenerate_tet_rejected(gpu_lib):
+def test_degenerate_mesh_rejected(gpu_lib):
     m = W.make_lattice_mesh(4, codes="channel")
     ctx = gpu_lib.Context()
-    tets = m["tets"].copy()
-    tets[7, [1, 2]] = tets[7, [2, 1]]          # inverted: negative volume
-    with pytest.raises(gpu_lib.AerofError) as e:
-        ctx.set_mesh(m["X"], tets, m["faces"], m["codes"], W.freestream(0.8))
-    assert e.value.code == -1 and "non-positive volume" in str(e.value)
+    # an inverted tet alone is accepted (the reference accepts it; the
+    # control volumes stay positive)
     X = m["X"].copy()
-    t = m["tets"][0]
-    X[t[3]] = X[t[0]] + 0.5 * (X[t[1]] - X[t[0]]) + 0.5 * (X[t[2]] - X[t[0]])   # flat tet
+    X[21] += np.array([0.2, -0.2, 0.0])   # inverts two tets around node 21
+    ctx.set_mesh(X, m["tets"], m["faces"], m["codes"], W.freestream(0.8))
+    # a flat mesh: every tet and control volume is zero
+    X = m["X"].copy()
+    X[:, 2] = 0.0
     with pytest.raises(gpu_lib.AerofError) as e:
         ctx.set_mesh(X, m["tets"], m["faces"], m["codes"], W.freestream(0.8))
-    assert e.value.code == -1
+    assert e.value.code == -1 and "control volume" in str(e.value)
     X = m["X"].copy()
     X[3, 1] = np.inf
     with pytest.raises(gpu_lib.AerofError) as e:

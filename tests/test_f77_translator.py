@@ -4,14 +4,13 @@ powers, column-major arrays, labelled and block DO loops, IF chains and the
 intrinsics, on a routine written here for the purpose."""
 import ctypes as C
 import os
+import importlib.util
 import subprocess
-import sys
 
 import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 SRC = """
       SUBROUTINE PROBE(n, a, b, out)
@@ -54,7 +53,9 @@ c     a comment line
 
 @pytest.fixture(scope="module")
 def probe(tmp_path_factory):
-    import f77_to_c
+    spec = importlib.util.spec_from_file_location("f77_to_c", os.path.join(ROOT, "oracle", "f77_to_c.py"))
+    f77_to_c = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(f77_to_c)
     d = tmp_path_factory.mktemp("f77")
     f = d / "probe.f"
     f.write_text(SRC)

@@ -203,6 +203,10 @@ struct Implicit {
   DBuf<double> basis;      // [(m+1)][5N]
   DBuf<double> w, r, x, b, t;
   DBuf<double> hcol;       // device scratch for one Hessenberg column
+  // device-driven GMRES: Hessenberg matrix, rotations, g, y, estimate and
+  // target, per-CTA partials; counters and barrier arrivals
+  DBuf<double> gst;
+  DBuf<int> gsti;
   DBuf<unsigned> ticket;   // grid-reduction ticket of the fused Gram-Schmidt kernels
   DBuf<double> fsum;       // [nbrow][25] boundary-face blocks of the boundary rows
   // preconditioner: AEROF_PC_JACOBI or AEROF_PC_ILU0 (block ILU(0) in the

@@ -293,14 +293,56 @@ template <class S, bool TRANS, class TI, class TO>
 __global__ void __launch_bounds__(256) k_spmv(int N, const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_tpos,
                                               const int* __restrict__ sptr, const int* __restrict__ scol,
                                               const S* __restrict__ diag, const S* __restrict__ off,
-                                              const TI* __restrict__ p, TO* __restrict__ y) {
+                                              const TI* __restrict__ p, TO* __restrict__ y,
+                                              const int* __restrict__ skip) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= N) return;
+  if (r >= N || (skip && *skip)) return;
   double acc[5] = {0, 0, 0, 0, 0};
   gemv_sl(diag, sl_dblk(r), r & 31, p + 5 * (size_t)r, acc, TRANS);
   const int p0 = nbr_ptr[r], cnt = nbr_ptr[r + 1] - p0;
   const size_t cb = (size_t)sptr[r >> 5] * 32 + (r & 31);
-  for (int k = 0; k < cnt; ++k) {
+  int k0 = 0;
+  if constexpr (std::is_same<S, float>::value && !TRANS) {
+    // FP32 blocks: two neighbours per trip with all their loads issued
+    // before the arithmetic (more bytes in flight per thread); the blocks
+    // stay in FP32 registers until used; same accumulation order
+    const int l = r & 31;
+    for (; k0 + 1 < cnt; k0 += 2) {
+      const int s0 = scol[cb + (size_t)32 * k0], s1 = scol[cb + (size_t)32 * (k0 + 1)];
+      float a0[25], a1[25];
+      const float4* q0 = reinterpret_cast<const float4*>(off + sl_blk(sptr, r, k0)) + l;
+      const float4* q1 = reinterpret_cast<const float4*>(off + sl_blk(sptr, r, k0 + 1)) + l;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        const float4 t0 = q0[32 * i], t1 = q1[32 * i];
+        a0[4 * i] = t0.x; a0[4 * i + 1] = t0.y; a0[4 * i + 2] = t0.z; a0[4 * i + 3] = t0.w;
+        a1[4 * i] = t1.x; a1[4 * i + 1] = t1.y; a1[4 * i + 2] = t1.z; a1[4 * i + 3] = t1.w;
+      }
+      a0[24] = off[sl_blk(sptr, r, k0) + 768 + l];
+      a1[24] = off[sl_blk(sptr, r, k0 + 1) + 768 + l];
+      double x0[5], x1[5];
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        x0[c] = (double)p[5 * (size_t)s0 + c];
+        x1[c] = (double)p[5 * (size_t)s1 + c];
+      }
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr) {
+        double t = (double)a0[5 * rr] * x0[0];
+#pragma unroll
+        for (int c = 1; c < 5; ++c) t += (double)a0[5 * rr + c] * x0[c];
+        acc[rr] += t;
+      }
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr) {
+        double t = (double)a1[5 * rr] * x1[0];
+#pragma unroll
+        for (int c = 1; c < 5; ++c) t += (double)a1[5 * rr + c] * x1[c];
+        acc[rr] += t;
+      }
+    }
+  }
+  for (int k = k0; k < cnt; ++k) {
     const int s = scol[cb + (size_t)32 * k];
     if (!TRANS) {
       gemv_sl(off, sl_blk(sptr, r, k), r & 31, p + 5 * (size_t)s, acc, false);
@@ -399,9 +441,9 @@ __global__ void k_bj_invert(int N, const S* __restrict__ diag, S* __restrict__ d
 // z = D^-1 x (or D^-T x): JacobiPrec::apply/applyT (KspPrec.C:86-111)
 template <class S, class TI, class TO>
 __global__ void k_bj_apply(int N, const S* __restrict__ dinv, const TI* __restrict__ x, TO* __restrict__ z,
-                           int trans) {
+                           int trans, const int* __restrict__ skip) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+  if (i >= N || (skip && *skip)) return;
   double acc[5] = {0, 0, 0, 0, 0};
   gemv_sl(dinv, sl_dblk(i), i & 31, x + 5 * (size_t)i, acc, trans != 0);
 #pragma unroll
@@ -522,6 +564,228 @@ __global__ void k_combine(size_t n, int k, const double* __restrict__ y, const T
   for (int m = 0; m < k; ++m) s += y[m] * (double)V[(size_t)m * ld + q];
   out[q] = (TV)s;
 }
+// ---------------------------------------------------------------------
+// Device-driven GMRES iteration (GmresSolver::solve, KspSolver.C:396-449,
+// with applyPreviousRotations / applyNewRotation / backwardSolve,
+// KspSolver.C:917-982): the modified Gram-Schmidt steps of one iteration,
+// the Givens update of the Hessenberg column and the next basis vector in
+// one cooperative launch.  Every CTA owns a fixed slice of the vectors; the
+// projections run in the reference's MGS order, one grid-wide sum per step
+// (partials in CTA order, identical in every CTA); the grid barriers are
+// bounded spins that record a timeout in ist[3] and never hang.  The
+// rotation arithmetic is written with explicitly rounded operations (no
+// contraction), so it is the host loop's arithmetic.  Once ist[1] (done)
+// is set, the rest of the cycle's kernels return at once, so the host
+// waits for the GPU only once per restart cycle.
+constexpr int kMaxKrylov = 64;
+constexpr int kCoopThreads = 256;
+struct GmresState {
+  double* H;        // [(m+1) * m], h(i, j) = H[i m + j]
+  double* cs;       // [2 m] rotations
+  double* g;        // [m + 1] right-hand side of the least-squares problem
+  double* y;        // [m] its solution
+  double* scal;     // [0] estimated residual norm, [1] target
+  int* ist;         // [0] iterations, [1] done, [2] last column, [3] barrier timeout, [4] maxits, [5] breakdown
+  double* part;     // [2][grid] per-CTA partial sums
+  unsigned* bar;    // grid barrier arrivals (zeroed per cycle)
+};
+
+// bounded grid barrier: every CTA adds one arrival and waits until the
+// count reaches target (co-residency is guaranteed by the cooperative
+// launch); after about a second a timeout is recorded and the CTA goes on
+__device__ __forceinline__ void grid_barrier(unsigned* bar, unsigned target, int* timeout) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(bar, 1u);
+    unsigned spins = 0;
+    while (*(volatile unsigned*)bar < target) {
+      if (++spins > (1u << 23)) {
+        atomicExch(timeout, 1);
+        break;
+      }
+      __nanosleep(128);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+template <class TV>
+__global__ void __launch_bounds__(kCoopThreads, 4) k_gmres_iter(size_t n, int j, int m, TV* __restrict__ V,
+                                                               size_t ld, TV* __restrict__ w, GmresState st,
+                                                               unsigned base) {
+  if (*(volatile int*)(st.ist + 1)) return;
+  __shared__ double ws[32];
+  __shared__ double hsh[kMaxKrylov + 2];
+  __shared__ double css[2 * kMaxKrylov];
+  __shared__ double sprev[3];  // g[j], estimated residual, target
+  __shared__ int iprev[2];     // iterations, maxits
+  __shared__ double sinv;
+  __shared__ int sdone;
+  // the previous state is read before the first barrier: CTA 0 overwrites
+  // it only after the last one
+  for (int k = threadIdx.x; k < 2 * j; k += blockDim.x) css[k] = st.cs[k];
+  if (threadIdx.x == 0) {
+    sprev[0] = st.g[j];
+    sprev[1] = st.scal[0];
+    sprev[2] = st.scal[1];
+    iprev[0] = st.ist[0];
+    iprev[1] = st.ist[4];
+  }
+  using VT = typename Vec16<TV>::T;
+  constexpr int W = Vec16<TV>::W;
+  const size_t nv = n / W;
+  const size_t per = (nv + gridDim.x - 1) / gridDim.x;
+  const size_t lo = min(nv, (size_t)blockIdx.x * per), hi = min(nv, lo + per);
+  const bool tail = blockIdx.x == gridDim.x - 1;
+  unsigned target = base;
+  for (int i = 0; i <= j + 1; ++i) {
+    const bool norm = i == j + 1;
+    const bool proj = i > 0;
+    const double h = proj ? hsh[i - 1] : 0.0;
+    const TV* Vp = proj ? V + (size_t)(i - 1) * ld : nullptr;
+    const TV* Vc = norm ? nullptr : V + (size_t)i * ld;
+    double s = 0.0;
+    // two vectors of each array per thread and trip, loads issued first
+    constexpr int U = 2;
+    for (size_t q0 = lo + threadIdx.x; q0 < hi; q0 += (size_t)U * blockDim.x) {
+      VT wv[U], pv[U], cv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const size_t q = q0 + (size_t)u * blockDim.x;
+        if (q < hi) {
+          wv[u] = reinterpret_cast<const VT*>(w)[q];
+          if (proj) pv[u] = reinterpret_cast<const VT*>(Vp)[q];
+          if (!norm) cv[u] = reinterpret_cast<const VT*>(Vc)[q];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const size_t q = q0 + (size_t)u * blockDim.x;
+        if (q >= hi) break;
+        TV* wp = reinterpret_cast<TV*>(&wv[u]);
+        if (proj) {
+          const TV* pp = reinterpret_cast<const TV*>(&pv[u]);
+#pragma unroll
+          for (int k = 0; k < W; ++k) wp[k] = (TV)((double)wp[k] - h * (double)pp[k]);
+          reinterpret_cast<VT*>(w)[q] = wv[u];
+        }
+        if (norm) {
+#pragma unroll
+          for (int k = 0; k < W; ++k) s += (double)wp[k] * (double)wp[k];
+        } else {
+          const TV* cp = reinterpret_cast<const TV*>(&cv[u]);
+#pragma unroll
+          for (int k = 0; k < W; ++k) s += (double)wp[k] * (double)cp[k];
+        }
+      }
+    }
+    if (tail)
+      for (size_t q = nv * W + threadIdx.x; q < n; q += blockDim.x) {
+        double wq = (double)w[q];
+        if (proj) {
+          w[q] = (TV)(wq - h * (double)Vp[q]);
+          wq = (double)w[q];
+        }
+        s += wq * (norm ? wq : (double)Vc[q]);
+      }
+    const double b = block_sum(s, ws);
+    double* part = st.part + (size_t)(i & 1) * gridDim.x;
+    if (threadIdx.x == 0) part[blockIdx.x] = b;
+    target += gridDim.x;
+    grid_barrier(st.bar, target, st.ist + 3);
+    double t = 0.0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) t += __ldcg(part + k);
+    t = block_sum(t, ws);
+    if (threadIdx.x == 0) hsh[i] = t;
+    __syncthreads();
+  }
+  // Givens update of column j (every CTA computes it; CTA 0 stores it)
+  if (threadIdx.x == 0) {
+    double hc[kMaxKrylov + 1];
+    for (int i = 0; i <= j; ++i) hc[i] = hsh[i];
+    const double hj1 = __dsqrt_rn(hsh[j + 1]);
+    const bool breakdown = hj1 == 0.0;
+    for (int i = 0; i < j; ++i) {
+      const double c0 = css[2 * i], c1 = css[2 * i + 1];
+      const double a = hc[i], bb = hc[i + 1];
+      hc[i] = __dadd_rn(__dmul_rn(c1, a), __dmul_rn(c0, bb));
+      hc[i + 1] = __dadd_rn(__dmul_rn(-c0, a), __dmul_rn(c1, bb));
+    }
+    double c0, c1;
+    const double hjj = hc[j];
+    if (__dmul_rn(hjj, hjj) == 0.0) {
+      c1 = 0.0;
+      c0 = 1.0;
+    } else {
+      const double coef = __ddiv_rn(1.0, __dsqrt_rn(__dadd_rn(__dmul_rn(hjj, hjj), __dmul_rn(hj1, hj1))));
+      c1 = __dmul_rn(__dsqrt_rn(__dmul_rn(hjj, hjj)), coef);
+      c0 = __ddiv_rn(__dmul_rn(c1, hj1), hjj);
+    }
+    hc[j] = __dadd_rn(__dmul_rn(c1, hjj), __dmul_rn(c0, hj1));
+    const double gj = sprev[0];
+    const double gj1 = __dmul_rn(-c0, gj);
+    const int iter = iprev[0] + 1;
+    double l2res = sprev[1];
+    bool done = breakdown;
+    if (!breakdown) {
+      l2res = fabs(gj1);
+      done = l2res <= sprev[2] || iter >= iprev[1];
+    }
+    sdone = done;
+    sinv = breakdown ? 0.0 : 1. / hj1;
+    if (blockIdx.x == 0) {
+      for (int i = 0; i <= j; ++i) st.H[(size_t)i * m + j] = hc[i];
+      st.H[(size_t)(j + 1) * m + j] = 0.0;
+      st.cs[2 * j] = c0;
+      st.cs[2 * j + 1] = c1;
+      st.g[j + 1] = gj1;
+      st.g[j] = __dmul_rn(c1, gj);
+      st.scal[0] = l2res;
+      st.ist[0] = iter;
+      st.ist[2] = j;
+      st.ist[5] = breakdown;
+    }
+  }
+  __syncthreads();
+  // every CTA has read what it needs of the previous state; CTA 0's done
+  // flag is written after the grid's last barrier, so no CTA of this launch
+  // reads it again
+  if (sdone) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) st.ist[1] = 1;
+    return;
+  }
+  const double a = sinv;
+  TV* Vn = V + (size_t)(j + 1) * ld;
+  for (size_t q = lo * W + threadIdx.x; q < hi * W; q += blockDim.x) Vn[q] = (TV)(a * (double)w[q]);
+  if (tail)
+    for (size_t q = nv * W + threadIdx.x; q < n; q += blockDim.x) Vn[q] = (TV)(a * (double)w[q]);
+}
+
+// back substitution (KspSolver.C:966-982) of the last cycle, one thread:
+// y[0..jl] from the rotated Hessenberg matrix and g
+__global__ void k_gmres_backsolve(int m, GmresState st) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int j = st.ist[2];
+  for (int i = j; i >= 0; --i) {
+    double yi = st.g[i];
+    for (int k = j; k >= i + 1; --k) yi = __dsub_rn(yi, __dmul_rn(st.H[(size_t)i * m + k], st.y[k]));
+    st.y[i] = __ddiv_rn(yi, st.H[(size_t)i * m + i]);
+  }
+}
+// out = sum_{m <= last column} y_m V_m
+template <class TV>
+__global__ void k_combine_dev(size_t n, const int* __restrict__ jl, const double* __restrict__ y,
+                              const TV* __restrict__ V, size_t ld, TV* __restrict__ out) {
+  size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int k = *jl + 1;
+  double s = 0.0;
+  for (int mm = 0; mm < k; ++mm) s += y[mm] * (double)V[(size_t)mm * ld + q];
+  out[q] = (TV)s;
+}
+
 template <class TA>
 __global__ void k_add(size_t n, const TA* __restrict__ a, double* __restrict__ x) {
   size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -602,15 +866,17 @@ void jacobian_dev(aerof_gpu_ctx* c, const double* dU, const double* ddt, int pre
 
 // products with H1 (trans = 0) or H1^T (trans = 1); the stored blocks may
 // hold either, so the kernel reads them plainly or transposed
+// skip (device flag, may be null): when set, the kernel returns at once
+// (the device-driven GMRES leaves the rest of a converged cycle idle)
 template <class TI, class TO>
-void matvec_t(aerof_gpu_ctx* c, const TI* p, TO* y, int trans) {
+void matvec_t(aerof_gpu_ctx* c, const TI* p, TO* y, int trans, const int* skip = nullptr) {
   DeviceMesh& m = c->mesh;
   TimerScope tm(c, AEROF_T_KSP_MATVEC);
   Implicit& J = c->imp;
   const int gn = grid_for(m.N, kIB);
   const bool tr = (trans != 0) != J.transposed;
   auto go = [&](auto kern, auto* diag, auto* off) {
-    kern<<<gn, kIB, 0, c->stream>>>(m.N, m.nbr_ptr.p, m.nbr_tpos.p, m.sptr.p, m.scol.p, diag, off, p, y);
+    kern<<<gn, kIB, 0, c->stream>>>(m.N, m.nbr_ptr.p, m.nbr_tpos.p, m.sptr.p, m.scol.p, diag, off, p, y, skip);
     AEROF_LAUNCH_CHECK();
   };
   if (J.precision == AEROF_PREC_FP32) {
@@ -1085,7 +1351,7 @@ int prec_setup_dev(aerof_gpu_ctx* c, int trans = 0) {
 // z = D^-1 x or D^-T x; with transposed storage the inverted blocks are
 // those of D^T, so the roles swap
 template <class TI, class TO>
-void prec_apply_t(aerof_gpu_ctx* c, const TI* x, TO* z, int trans) {
+void prec_apply_t(aerof_gpu_ctx* c, const TI* x, TO* z, int trans, const int* skip = nullptr) {
   DeviceMesh& m = c->mesh;
   TimerScope tp(c, AEROF_T_KSP_OTHER);
   Implicit& J = c->imp;
@@ -1101,13 +1367,142 @@ void prec_apply_t(aerof_gpu_ctx* c, const TI* x, TO* z, int trans) {
     return;
   }
   if (J.precision == AEROF_PREC_FP32)
-    k_bj_apply<float, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, J.dinv32.p, x, z, tr);
+    k_bj_apply<float, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, J.dinv32.p, x, z, tr, skip);
   else
-    k_bj_apply<double, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, J.dinv64.p, x, z, tr);
+    k_bj_apply<double, TI, TO><<<gn, kIB, 0, c->stream>>>(m.N, J.dinv64.p, x, z, tr, skip);
   AEROF_LAUNCH_CHECK();
 }
 void prec_apply_dev(aerof_gpu_ctx* c, const double* x, double* z, int trans) {
   prec_apply_t<double, double>(c, x, z, trans);
+}
+
+// Device-driven form of gmres_t for the assembled operator with the
+// block-Jacobi preconditioner: per iteration three launches (preconditioner,
+// product, k_gmres_iter), no host synchronisation inside a restart cycle;
+// the host reads the cycle's status once at its end (AEROF_GMRES_DEVICE=0
+// selects the host-driven loop).
+static bool gmres_device_loop_enabled() {
+  static const int v = [] {
+    const char* e = std::getenv("AEROF_GMRES_DEVICE");
+    return e ? std::atoi(e) : 1;
+  }();
+  return v != 0;
+}
+
+template <class TV>
+static int gmres_devloop(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int maxits, double eps, int trans,
+                         double* final_res) {
+  DeviceMesh& m = c->mesh;
+  Implicit& J = c->imp;
+  const size_t n = 5 * (size_t)m.N;
+  const int gv = grid_for(n, kIB);
+  cudaStream_t s = c->stream;
+  const size_t ld = (n + 63) / 64 * 64;
+  J.basis.ensure(((size_t)(numVec + 1) * ld * sizeof(TV) + 7) / 8);
+  J.w.ensure((n * sizeof(TV) + 7) / 8);
+  J.r.ensure((n * sizeof(TV) + 7) / 8);
+  J.ticket.ensure(1);
+  AEROF_CUDA(cudaMemsetAsync(J.ticket.p, 0, sizeof(unsigned), s));
+  c->s.red.ensure(kGB);
+  J.hcol.ensure(1);
+  TV* Vb = reinterpret_cast<TV*>(J.basis.p);
+  TV* w = reinterpret_cast<TV*>(J.w.p);
+  TV* r = reinterpret_cast<TV*>(J.r.p);
+  // cooperative grid: every CTA resident at once
+  static int coop_grid = 0;
+  if (!coop_grid) {
+    int per_sm = 0, sms = 0;
+    AEROF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gmres_iter<TV>, kCoopThreads, 0));
+    AEROF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
+    coop_grid = std::max(1, std::min(per_sm, 4)) * sms;
+  }
+  const int grid = coop_grid;
+  // device state: H, cs, g, y, scal | ist, part, bar
+  const size_t nH = (size_t)(numVec + 1) * numVec;
+  J.gst.ensure(nH + 2 * (size_t)numVec + (numVec + 1) + numVec + 2 + 2 * (size_t)grid);
+  J.gsti.ensure(8 + 1);
+  GmresState st;
+  st.H = J.gst.p;
+  st.cs = st.H + nH;
+  st.g = st.cs + 2 * numVec;
+  st.y = st.g + numVec + 1;
+  st.scal = st.y + numVec;
+  st.part = st.scal + 2;
+  st.ist = J.gsti.p;
+  st.bar = reinterpret_cast<unsigned*>(J.gsti.p + 8);
+  double* part = c->s.red.p;
+  unsigned* ticket = J.ticket.p;
+  double* hd = J.hcol.p;
+  auto norm2 = [&](TV* v) -> double {
+    k_mgs<TV, true><<<kGB, kIB, 0, s>>>(n, nullptr, nullptr, nullptr, v, part, ticket, hd);
+    AEROF_LAUNCH_CHECK();
+    double h = 0.0;
+    AEROF_CUDA(cudaMemcpyAsync(&h, hd, sizeof(double), cudaMemcpyDeviceToHost, s));
+    AEROF_CUDA(cudaStreamSynchronize(s));
+    return std::sqrt(h);
+  };
+  AEROF_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
+  int iter = 0;
+  double target = 0.0, l2res = 0.0;
+  const double bnorm = norm2_dev(c, b, n);
+  std::vector<double> ginit(numVec + 1 + numVec + 2);
+  for (;;) {
+    if (iter == 0) {
+      k_scale<double, TV><<<gv, kIB, 0, s>>>(n, 1.0, b, r);
+      AEROF_LAUNCH_CHECK();
+    } else {
+      k_scale<double, TV><<<gv, kIB, 0, s>>>(n, 1.0, x, r);
+      AEROF_LAUNCH_CHECK();
+      matvec_t<TV, TV>(c, r, w, trans);
+      k_sub<TV, TV><<<gv, kIB, 0, s>>>(n, b, w, r);
+      AEROF_LAUNCH_CHECK();
+    }
+    const double beta = norm2(r);
+    if (iter == 0) target = eps * bnorm;
+    if (beta == 0.0) {
+      if (final_res) *final_res = 0.0;
+      return iter;
+    }
+    k_scale<TV, TV><<<gv, kIB, 0, s>>>(n, 1.0 / beta, r, Vb);
+    AEROF_LAUNCH_CHECK();
+    // this cycle's state: g = (beta, 0, ...), the estimate, the target,
+    // the counters, zero barrier arrivals
+    std::fill(ginit.begin(), ginit.end(), 0.0);
+    ginit[0] = beta;
+    ginit[2 * (size_t)numVec + 1] = l2res;
+    ginit[2 * (size_t)numVec + 2] = target;
+    AEROF_CUDA(cudaMemcpyAsync(st.g, ginit.data(), ginit.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    const int iinit[9] = {iter, 0, -1, 0, maxits, 0, 0, 0, 0};
+    AEROF_CUDA(cudaMemcpyAsync(st.ist, iinit, sizeof(iinit), cudaMemcpyHostToDevice, s));
+    unsigned base = 0;
+    const int* done = st.ist + 1;
+    for (int j = 0; j < numVec; ++j) {
+      prec_apply_t<TV, TV>(c, Vb + (size_t)j * ld, r, trans, done);
+      matvec_t<TV, TV>(c, r, w, trans, done);
+      TimerScope t(c, AEROF_T_KSP_OTHER);
+      void* args[] = {(void*)&n, (void*)&j, (void*)&numVec, (void*)&Vb, (void*)&ld, (void*)&w, (void*)&st,
+                      (void*)&base};
+      AEROF_CUDA(cudaLaunchCooperativeKernel((const void*)k_gmres_iter<TV>, grid, kCoopThreads, args, 0, s));
+      AEROF_LAUNCH_CHECK();
+      base += (unsigned)(j + 2) * (unsigned)grid;
+    }
+    k_gmres_backsolve<<<1, 32, 0, s>>>(numVec, st);
+    AEROF_LAUNCH_CHECK();
+    k_combine_dev<TV><<<gv, kIB, 0, s>>>(n, st.ist + 2, st.y, Vb, ld, w);
+    AEROF_LAUNCH_CHECK();
+    prec_apply_t<TV, TV>(c, w, r, trans);
+    k_add<TV><<<gv, kIB, 0, s>>>(n, r, x);
+    AEROF_LAUNCH_CHECK();
+    int ist[6];
+    AEROF_CUDA(cudaMemcpyAsync(ist, st.ist, sizeof(ist), cudaMemcpyDeviceToHost, s));
+    AEROF_CUDA(cudaMemcpyAsync(&l2res, st.scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+    AEROF_CUDA(cudaStreamSynchronize(s));
+    if (ist[3]) throw ApiError{AEROF_ETIMEDOUT, "GMRES grid barrier timed out"};
+    iter = ist[0];
+    if (ist[1]) break;  // converged, saturated or broke down
+  }
+  if (final_res) *final_res = l2res;
+  return iter;
 }
 
 // GmresSolver::solve (KspSolver.C:351-492), typePrec = 2 (right
@@ -1120,6 +1515,8 @@ void prec_apply_dev(aerof_gpu_ctx* c, const double* x, double* z, int trans) {
 template <class TV>
 static int gmres_t(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int maxits, double eps, int trans,
                    double* final_res, const double* exactU) {
+  if (!exactU && c->imp.pc == AEROF_PC_JACOBI && numVec <= kMaxKrylov && gmres_device_loop_enabled())
+    return gmres_devloop<TV>(c, b, x, numVec, maxits, eps, trans, final_res);
   DeviceMesh& m = c->mesh;
   Implicit& J = c->imp;
   const size_t n = 5 * (size_t)m.N;

@@ -53,7 +53,7 @@ EXPORTS = [
     "aerof_gpu_update_coordinates", "aerof_gpu_linearized_solve", "aerof_gpu_residual_noalloc",
     "aerof_gpu_h2_evaluate", "aerof_gpu_h2_apply", "aerof_gpu_h2_release", "aerof_gpu_set_exact_operator",
     "aerof_gpu_linearized_solve_batch", "aerof_gpu_set_preconditioner", "aerof_gpu_set_jacobian",
-    "aerof_gpu_matvec_fd",
+    "aerof_gpu_matvec_fd", "aerof_gpu_set_owned_rows",
 ]
 TIMER_NAMES = ["nodal_grad", "fv_term", "time_step", "fv_jac", "prec_setup", "ksp_matvec", "ksp_other", "other"]
 
@@ -138,6 +138,7 @@ def library(path: str | None = None):
             "aerof_gpu_set_preconditioner": [vp, C.c_int],
             "aerof_gpu_set_jacobian": [vp, dp, C.c_int],
             "aerof_gpu_matvec_fd": [vp, dp, dp, dp, dp, C.c_int, dp, C.POINTER(C.c_double)],
+            "aerof_gpu_set_owned_rows": [vp, C.c_int],
         }
         for name, args in sig.items():
             if hasattr(L, name):
@@ -294,6 +295,10 @@ class Context:
         self._check(self.L.aerof_gpu_mesh_sizes(self.h, C.byref(n), C.byref(e), C.byref(ff)))
         self.N, self.E, self.F = n.value, e.value, ff.value
         return self
+
+    def set_owned_rows(self, n_owned: int):
+        """Rows [n_owned, N) are ghost rows of a subdomain mesh."""
+        self._check(self.L.aerof_gpu_set_owned_rows(self.h, int(n_owned)))
 
     def status(self) -> int:
         """Wait for the stream; unphysical count of async calls since last status."""

@@ -313,6 +313,8 @@ struct aerof_gpu_ctx {
   // looked up at context creation (residual.cu)
   double* noalloc_scratch = nullptr;
   std::string noalloc_error;
+  // rows [n_owned, N) are ghost rows of a subdomain mesh (set-up only)
+  int n_owned = 0;
 };
 
 namespace aerof {

@@ -419,11 +419,19 @@ __global__ void __launch_bounds__(256) k_spmv_batch(int N, int R, const int* __r
 // 44-80): blocks with a zero diagonal entry are left as they are (as the
 // reference does); a zero pivot counts into bad[0].
 template <class S>
-__global__ void k_bj_invert(int N, const S* __restrict__ diag, S* __restrict__ dinv, int* __restrict__ bad) {
+__global__ void k_bj_invert(int N, int n_owned, const S* __restrict__ diag, S* __restrict__ dinv,
+                            int* __restrict__ bad) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const size_t b = sl_dblk(i);
   S a[25];
+  if (i >= n_owned) {
+    // ghost row of a subdomain mesh: identity (its partial block is not used)
+#pragma unroll
+    for (int k = 0; k < 25; ++k) a[k] = (k % 6 == 0) ? S(1) : S(0);
+    store_block_vec<S>(dinv, b, i & 31, a);
+    return;
+  }
   {
     double t[25];
     load_block<S>(diag, b, i & 31, t);
@@ -1335,10 +1343,10 @@ int prec_setup_dev(aerof_gpu_ctx* c, int trans = 0) {
   const int gn = grid_for(m.N, kIB);
   if (J.precision == AEROF_PREC_FP32) {
     J.dinv32.alloc(sl_diag_size(m));
-    k_bj_invert<float><<<gn, kIB, 0, c->stream>>>(m.N, J.diag32.p, J.dinv32.p, bad);
+    k_bj_invert<float><<<gn, kIB, 0, c->stream>>>(m.N, c->n_owned, J.diag32.p, J.dinv32.p, bad);
   } else {
     J.dinv64.alloc(sl_diag_size(m));
-    k_bj_invert<double><<<gn, kIB, 0, c->stream>>>(m.N, J.diag64.p, J.dinv64.p, bad);
+    k_bj_invert<double><<<gn, kIB, 0, c->stream>>>(m.N, c->n_owned, J.diag64.p, J.dinv64.p, bad);
   }
   AEROF_LAUNCH_CHECK();
   int h = 0;
@@ -2256,6 +2264,17 @@ extern "C" int aerof_gpu_set_jacobian(aerof_gpu_ctx* c, const double* A, int pre
     J.transposed = false;
     J.prec_ready = false;
     J.ilu_ready = false;
+    return AEROF_OK;
+  });
+}
+
+extern "C" int aerof_gpu_set_owned_rows(aerof_gpu_ctx* c, int n_owned) {
+  return guard(c, [&]() -> int {
+    need_mesh_or_throw(c);
+    if (n_owned < 0 || n_owned > c->mesh.N) return AEROF_EINVAL;
+    c->n_owned = n_owned;
+    c->imp.prec_ready = false;
+    c->imp.ilu_ready = false;
     return AEROF_OK;
   });
 }

@@ -439,14 +439,15 @@ static int check_coordinates(aerof_gpu_ctx* c, int N, const double* X) {
   return AEROF_OK;
 }
 
-// Counts nodes whose dual control volume (ElemTetCore.C:102-112) is not
-// positive or not finite: the residual divides by it (SpaceOperator.C:
-// 614-620).  Inverted tets alone are accepted, as the reference accepts
-// them: the signed tet volumes around an interior node always add up to the
-// volume of its star.
+// Counts nodes whose dual control volume (ElemTetCore.C:102-112) is zero or
+// not finite: the residual divides by it (SpaceOperator.C:614-620).
+// Inverted tets are accepted, as the reference accepts them (the signed tet
+// volumes around an interior node add up to the volume of its star), and
+// so are negative volumes, which the outer ghost nodes of a subdomain mesh
+// can have (their rows are not used).
 __global__ void k_check_vol(int N, const double* __restrict__ vol, int* __restrict__ nbad) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < N && !(vol[i] > 0.0 && vol[i] < INFINITY)) atomicAdd(nbad, 1);
+  if (i < N && !(vol[i] != 0.0 && fabs(vol[i]) < INFINITY)) atomicAdd(nbad, 1);
 }
 
 }  // namespace aerof
@@ -712,12 +713,13 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
       AEROF_CUDA(cudaMemcpyAsync(&bad, nb.p, sizeof(int), cudaMemcpyDeviceToHost, s));
       AEROF_CUDA(cudaStreamSynchronize(s));
       if (bad) {
-        c->last_error = std::to_string(bad) + " node(s) with a non-positive or non-finite control volume "
+        c->last_error = std::to_string(bad) + " node(s) with a zero or non-finite control volume "
                         "(degenerate tets)";
         return AEROF_EINVAL;
       }
     }
     AEROF_CUDA(cudaStreamSynchronize(s));
+    c->n_owned = N;
     c->has_mesh = true;
     return AEROF_OK;
   });

@@ -238,6 +238,13 @@ int aerof_gpu_prec_setup(aerof_gpu_ctx* ctx);
  * with AEROF_PC_ILU0, IluPrec::apply (y = (LU)^-1 x, factors of H1 or, for
  * transpose = 1, of H1^T).                                                 */
 int aerof_gpu_prec_apply(aerof_gpu_ctx* ctx, const double* x, double* y, int transpose);
+/* Subdomain meshes (one per rank of a decomposed mesh, owned nodes first,
+ * then the ghost nodes whose states the caller exchanges between ranks,
+ * the role of DistInfo::masterFlag, DistVector.h:1435-1452): rows
+ * [n_owned, N) are ghost rows, whose block-Jacobi blocks are taken as the
+ * identity (their partial diagonal blocks are not used and may be
+ * singular).  Default after aerof_gpu_set_mesh: n_owned = N.              */
+int aerof_gpu_set_owned_rows(aerof_gpu_ctx* ctx, int n_owned);
 /* Selects the preconditioner of aerof_gpu_prec_setup / _apply, the GMRES,
  * Newton and linearised solves: AEROF_PC_JACOBI (default) or
  * AEROF_PC_ILU0 (IluPrec::setup / apply, KspPrec.C:220-260).               */

@@ -54,6 +54,8 @@ EXPORTS = [
     "aerof_gpu_h2_evaluate", "aerof_gpu_h2_apply", "aerof_gpu_h2_release", "aerof_gpu_set_exact_operator",
     "aerof_gpu_linearized_solve_batch", "aerof_gpu_set_preconditioner", "aerof_gpu_set_jacobian",
     "aerof_gpu_matvec_fd", "aerof_gpu_set_owned_rows",
+    "aerof_sower_open", "aerof_sower_close", "aerof_sower_num_subdomains", "aerof_sower_subdomain_sizes",
+    "aerof_sower_read_subdomain", "aerof_sower_last_error",
 ]
 TIMER_NAMES = ["nodal_grad", "fv_term", "time_step", "fv_jac", "prec_setup", "ksp_matvec", "ksp_other", "other"]
 

@@ -356,6 +356,32 @@ int aerof_gpu_linearized_solve_batch(aerof_gpu_ctx* ctx, const double* U, int nr
                                      int krylov, int maxits, double eps, int transpose, int inner_its, int* its,
                                      double* res);
 
+/* ---- pre-partitioned mesh files ---------------------------------------
+ * Reader of AERO-F's binary mesh and decomposition files (host only):
+ * GeoSource::readConnectivityInfo (GeoSource.C:94-141) opens the
+ * connectivity file and names the clusters' geometry and decomposition
+ * files (prefix + cluster suffix, computeClusterSuffix in
+ * BinFileHandler.h); GeoSource::getSubDomain (GeoSource.C:256-444) reads
+ * one subdomain: nodes (NodeSet::read, Node.C:7-50), tets
+ * (ElemSet::read, ElemCore.C:135-199), boundary triangles
+ * (FaceSet::read, FaceCore.C:270-330; file code 6 becomes symmetry, 11),
+ * neighbour subdomains and shared nodes.  Both byte orders are read
+ * (BinFileHandler's header).  Arrays come back in the subdomain's local
+ * node numbering (cluster order), with local-to-global maps (0-based).
+ * aerof_sower_subdomain_sizes then aerof_sower_read_subdomain with arrays
+ * of those sizes: X[nn][3], node_l2g[nn], tets[ne][4], elem_l2g[ne],
+ * faces[nf][3], codes[nf], face_l2g[nf], neighb[nb], shared_ptr[nb+1],
+ * shared[ns]; any array may be NULL.                                      */
+typedef struct aerof_sower aerof_sower;
+int aerof_sower_open(const char* con_file, const char* geo_prefix, const char* dec_prefix, aerof_sower** out);
+int aerof_sower_close(aerof_sower* s);
+int aerof_sower_num_subdomains(aerof_sower* s, int* nsub, int* nclusters);
+int aerof_sower_subdomain_sizes(aerof_sower* s, int isub, int* nnodes, int* nelems, int* nfaces, int* nneighb,
+                                int* nshared);
+int aerof_sower_read_subdomain(aerof_sower* s, int isub, double* X, int* node_l2g, int* tets, int* elem_l2g,
+                               int* faces, int* codes, int* face_l2g, int* neighb, int* shared_ptr, int* shared);
+int aerof_sower_last_error(aerof_sower* s, char* buf, int len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -12,7 +12,7 @@ HEADER = os.path.join(ROOT, "include", "aerof_gpu.h")
 
 def declared():
     txt = open(HEADER).read()
-    return sorted(set(re.findall(r"^int\s+(aerof_gpu_\w+)\s*\(", txt, flags=re.M)))
+    return sorted(set(re.findall(r"^int\s+(aerof_(?:gpu|sower)_\w+)\s*\(", txt, flags=re.M)))
 
 
 @pytest.fixture(scope="module")

@@ -59,3 +59,26 @@ def test_gpu_pieces_newton(gpu_lib, oracle_mod, prec):
     assert rel_l2(got, Uref) <= (1e-9 if prec == 64 else 1e-7)
     for be in team.backends:
         be.close()
+
+
+def test_gpu_pieces_from_sower_files(gpu_lib, oracle_mod, tmp_path):
+    # a mesh written in AERO-F's pre-partitioned format and read back: the
+    # single-domain residual is unchanged, and GPU pieces built from the
+    # files' subdomains (the reference's ownership rule) give it too
+    from aerof_dev_b200 import sower
+    m = W.make_lattice_mesh(11, jitter=0.2, codes="channel")
+    Ub = W.freestream(0.8)
+    U = W.perturbed_state(m["X"].shape[0], 0.8)
+    names = sower.write(str(tmp_path / "mesh"), m, sower.element_partition(m, 3))
+    gs = sower.GeoSource(names["con"], names["geo"], names["dec"])
+    g = gs.global_mesh()
+    R0, _ = gpu_lib.SpaceOperator(gpu_lib.Context.from_mesh(m, Ub)).computeResidual(U)
+    R1, _ = gpu_lib.SpaceOperator(gpu_lib.Context.from_mesh(g, Ub)).computeResidual(U)
+    assert np.array_equal(R0, R1)
+    subs = D.decompose(g, gs.owners())
+    team = DS.Team([(s, DS.GpuBackend(s, Ub)) for s in subs])
+    R, _ = team.residual(_local(subs, U))
+    assert rel_l2(D.gather_owned(subs, [r.cpu().numpy() for r in R], U.shape[0]), R0) <= 1e-12
+    for be in team.backends:
+        be.close()
+    gs.close()

@@ -53,7 +53,7 @@ EXPORTS = [
     "aerof_gpu_update_coordinates", "aerof_gpu_linearized_solve", "aerof_gpu_residual_noalloc",
     "aerof_gpu_h2_evaluate", "aerof_gpu_h2_apply", "aerof_gpu_h2_release", "aerof_gpu_set_exact_operator",
     "aerof_gpu_linearized_solve_batch", "aerof_gpu_set_preconditioner", "aerof_gpu_set_jacobian",
-    "aerof_gpu_matvec_fd", "aerof_gpu_set_owned_rows",
+    "aerof_gpu_matvec_fd", "aerof_gpu_set_owned_rows", "aerof_gpu_set_viscosity",
     "aerof_sower_open", "aerof_sower_close", "aerof_sower_num_subdomains", "aerof_sower_subdomain_sizes",
     "aerof_sower_read_subdomain", "aerof_sower_last_error",
 ]
@@ -77,6 +77,12 @@ class NewtonParams(C.Structure):
                 ("ser", C.c_double), ("ksp_eps", C.c_double), ("tol", C.c_double),
                 ("ksp_krylov", C.c_int), ("ksp_maxits", C.c_int), ("max_steps", C.c_int),
                 ("precision", C.c_int), ("reserved", C.c_int * 4)]
+
+
+class ViscousParams(C.Structure):
+    _fields_ = [("model", C.c_int), ("reynolds_mu", C.c_double), ("prandtl", C.c_double),
+                ("bulk_viscosity", C.c_double), ("sutherland_alpha", C.c_double), ("sutherland_Ts", C.c_double),
+                ("reserved", C.c_int * 4)]
 
 
 class NewtonResult(C.Structure):
@@ -141,6 +147,7 @@ def library(path: str | None = None):
             "aerof_gpu_set_jacobian": [vp, dp, C.c_int],
             "aerof_gpu_matvec_fd": [vp, dp, dp, dp, dp, C.c_int, dp, C.POINTER(C.c_double)],
             "aerof_gpu_set_owned_rows": [vp, C.c_int],
+            "aerof_gpu_set_viscosity": [vp, C.POINTER(ViscousParams)],
         }
         for name, args in sig.items():
             if hasattr(L, name):
@@ -301,6 +308,13 @@ class Context:
     def set_owned_rows(self, n_owned: int):
         """Rows [n_owned, N) are ghost rows of a subdomain mesh."""
         self._check(self.L.aerof_gpu_set_owned_rows(self.h, int(n_owned)))
+
+    def set_viscosity(self, model: int = 1, reynolds_mu: float = 100.0, prandtl: float = 0.72,
+                      bulk_viscosity: float = 0.0, sutherland_alpha: float = 1.0, sutherland_Ts: float = 0.0):
+        """Laminar viscous Galerkin term in every residual (model 0 off,
+        1 constant viscosity, 2 Sutherland)."""
+        p = ViscousParams(model, reynolds_mu, prandtl, bulk_viscosity, sutherland_alpha, sutherland_Ts)
+        self._check(self.L.aerof_gpu_set_viscosity(self.h, C.byref(p)))
 
     def status(self) -> int:
         """Wait for the stream; unphysical count of async calls since last status."""

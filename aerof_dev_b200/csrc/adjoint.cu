@@ -2134,6 +2134,7 @@ static int need(aerof_gpu_ctx* c) {
 
 extern "C" int aerof_gpu_jvp(aerof_gpu_ctx* c, const double* U, const double* v, double* Jv) {
   return guard(c, [&]() -> int {
+    need_inviscid(c);
     if (int e = need(c)) return e;
     if (!U || !v || !Jv) return AEROF_EINVAL;
     const size_t n = 5 * (size_t)c->mesh.N;
@@ -2148,6 +2149,7 @@ extern "C" int aerof_gpu_jvp(aerof_gpu_ctx* c, const double* U, const double* v,
 
 extern "C" int aerof_gpu_dRdX(aerof_gpu_ctx* c, const double* U, const double* Xdot, double* dR) {
   return guard(c, [&]() -> int {
+    need_inviscid(c);
     if (int e = need(c)) return e;
     if (!U || !Xdot || !dR) return AEROF_EINVAL;
     const size_t N = c->mesh.N;
@@ -2162,6 +2164,7 @@ extern "C" int aerof_gpu_dRdX(aerof_gpu_ctx* c, const double* U, const double* X
 
 extern "C" int aerof_gpu_vjp(aerof_gpu_ctx* c, const double* U, const double* w, double* JTw) {
   return guard(c, [&]() -> int {
+    need_inviscid(c);
     if (int e = need(c)) return e;
     if (!U || !w || !JTw) return AEROF_EINVAL;
     const size_t n = 5 * (size_t)c->mesh.N;
@@ -2177,6 +2180,7 @@ extern "C" int aerof_gpu_vjp(aerof_gpu_ctx* c, const double* U, const double* w,
 extern "C" int aerof_gpu_adjoint_products(aerof_gpu_ctx* c, const double* U, const double* lambda, double* JTl,
                                           double* gX) {
   return guard(c, [&]() -> int {
+    need_inviscid(c);
     if (int e = need(c)) return e;
     if (!U || !lambda || !JTl || !gX) return AEROF_EINVAL;
     const size_t N = c->mesh.N;
@@ -2193,6 +2197,7 @@ extern "C" int aerof_gpu_adjoint_products(aerof_gpu_ctx* c, const double* U, con
 
 extern "C" int aerof_gpu_dRdX_T(aerof_gpu_ctx* c, const double* U, const double* lambda, double* gX) {
   return guard(c, [&]() -> int {
+    need_inviscid(c);
     if (int e = need(c)) return e;
     if (!U || !lambda || !gX) return AEROF_EINVAL;
     const size_t N = c->mesh.N;
@@ -2209,6 +2214,7 @@ extern "C" int aerof_gpu_dRdX_T(aerof_gpu_ctx* c, const double* U, const double*
 // at U stored in device memory.
 extern "C" int aerof_gpu_h2_evaluate(aerof_gpu_ctx* c, const double* U) {
   return guard(c, [&]() -> int {
+    need_inviscid(c);
     if (int e = need(c)) return e;
     if (!U) return AEROF_EINVAL;
     const double* dU = in_dev(c, U, 5 * (size_t)c->mesh.N, c->s.Ustage);
@@ -2222,6 +2228,7 @@ extern "C" int aerof_gpu_h2_evaluate(aerof_gpu_ctx* c, const double* U) {
 // stored operator.
 extern "C" int aerof_gpu_h2_apply(aerof_gpu_ctx* c, const double* p, double* y, int transpose) {
   return guard(c, [&]() -> int {
+    need_inviscid(c);
     if (int e = need(c)) return e;
     if (!p || !y) return AEROF_EINVAL;
     if (!c->h2.ready) {

@@ -315,6 +315,8 @@ struct aerof_gpu_ctx {
   std::string noalloc_error;
   // rows [n_owned, N) are ghost rows of a subdomain mesh (set-up only)
   int n_owned = 0;
+  // viscous Galerkin term (model 0: inviscid)
+  aerof_viscous_params visc = {};
 };
 
 namespace aerof {
@@ -404,6 +406,14 @@ void exact_product(aerof_gpu_ctx* c, const double* dU, const double* p, double* 
 void h2_evaluate_dev(aerof_gpu_ctx* c, const double* dU);
 // implemented in mesh.cu: recompute the geometry for new coordinates
 void compute_geometry(aerof_gpu_ctx* c);
+// implemented in viscous.cu: R += (viscous Galerkin term of U) / ctrlVol
+// when a viscous model is set (no allocation)
+void galerkin_add(aerof_gpu_ctx* c, const double* dU, double* dR);
+// the exact linearisations cover the inviscid residual only
+inline void need_inviscid(aerof_gpu_ctx* c) {
+  if (c->visc.model != 0)
+    throw ApiError{AEROF_EINVAL, "the exact linearisation of the viscous term is not built: set model 0"};
+}
 // implemented in residual.cu: device address of the allocation-free
 // residual's scratch array for the current device, kept in the context
 void noalloc_attach(aerof_gpu_ctx* c);

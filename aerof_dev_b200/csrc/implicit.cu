@@ -2491,6 +2491,7 @@ extern "C" int aerof_gpu_linearized_solve(aerof_gpu_ctx* c, const double* U, con
                                           int maxits, double eps, int transpose, int inner_its, int* its,
                                           double* res) {
   return guard(c, [&]() -> int {
+    need_inviscid(c);
     need_mesh_or_throw(c);
     if (!U || !b || !x || krylov < 1 || maxits < 1 || !(eps >= 0.0) || inner_its < 0) return AEROF_EINVAL;
     const size_t n = 5 * (size_t)c->mesh.N;
@@ -2538,6 +2539,7 @@ extern "C" int aerof_gpu_linearized_solve_batch(aerof_gpu_ctx* c, const double* 
                                                 double* X, int krylov, int maxits, double eps, int transpose,
                                                 int inner_its, int* its, double* res) {
   return guard(c, [&]() -> int {
+    need_inviscid(c);
     need_mesh_or_throw(c);
     if (!U || !B || !X || nrhs < 0 || krylov < 1 || maxits < 1 || !(eps >= 0.0) || inner_its < 0)
       return AEROF_EINVAL;

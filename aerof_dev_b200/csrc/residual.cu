@@ -1020,6 +1020,7 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
     k_fv_nodes_b<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.n2o.p, c->s.part.p, m.xin_ptr.p, c->s.spill.p,
                                                           m.bnf_ptr.p, m.bnf_ent.p, c->s.fbuf.p, m.vol2.p, dR);
     AEROF_LAUNCH_CHECK();
+    galerkin_add(c, dU, dR);
   }
   return bad;
 }
@@ -1079,6 +1080,7 @@ int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
         m.N, m.E, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_edge.p, c->s.flux.p, m.nf_ptr.p, m.nf_face.p, m.fcode.p, m.fnrm.p,
         m.F, m.faces.p, c->s.fbuf.p, m.P.p, m.vol.p, dR);
     AEROF_LAUNCH_CHECK();
+    galerkin_add(c, dU, dR);
   }
   return bad;
 }
@@ -1383,6 +1385,7 @@ extern "C" int aerof_gpu_residual_noalloc(aerof_gpu_ctx* c, const double* U, dou
         m.N, m.E, g, m.Ubd.p, m.nbr_ptr.p, m.nbr_edge.p, flux, m.nf_ptr.p, m.nf_face.p, m.fcode.p, m.fnrm.p, m.F,
         m.faces.p, nullptr, m.P.p, m.vol.p, R);
     AEROF_LAUNCH_CHECK();
+    galerkin_add(c, U, R);
     AEROF_CUDA(cudaStreamSynchronize(s));
     return bad;
   });

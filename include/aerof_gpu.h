@@ -198,6 +198,34 @@ int aerof_gpu_timestep(aerof_gpu_ctx* ctx, const double* U, double cfl, double* 
  * local-time-step Heun steps at fixed cfl, U[N][5] updated in place.     */
 int aerof_gpu_rk2(aerof_gpu_ctx* ctx, double* U, double cfl, int nsteps);
 
+/* ---- viscous term -----------------------------------------------------
+ * The laminar Navier-Stokes Galerkin term that SpaceOperator::
+ * computeResidual adds when a FemEquationTerm is present (SpaceOperator.C:
+ * 570-573; ElemTet::computeGalerkinTerm, ElemTet.C:24-127;
+ * FemEquationTermNS::computeVolumeTerm, FemEquationTermDesc.C:98-160):
+ * model 0 inviscid (default), 1 constant viscosity (ConstantViscoFcn,
+ * mu = 1, lambda = bulk_viscosity - 2/3 mu), 2 Sutherland (mu = T^1.5
+ * (1 + Ts)/(T + Ts) with T = sutherland_alpha * T_adim, alpha =
+ * gamma (gamma - 1) M^2, Ts = sutherlandReferenceTemperature / reference
+ * temperature; lambda = -2/3 mu), conductivity cp mu / prandtl, all scaled
+ * by 1/reynolds_mu (ViscoFcn.h:46-103, ThermalCondFcn.h:52-75).  Every
+ * residual evaluation (aerof_gpu_residual and its variants, RK2, Newton)
+ * then includes it.  The local time step keeps the inviscid spectral
+ * radius (the reference's default, TsData::viscousCst = 0), and the H1
+ * operator of the Newton solves stays the first-order inviscid one (a
+ * defect correction); the exact linearisations (jvp, vjp, dR/dX, the stored
+ * operator, linearised solves) return AEROF_EINVAL with a viscous model.   */
+typedef struct aerof_viscous_params {
+  int model;               /* 0, 1 or 2 as above                              */
+  double reynolds_mu;      /* Reynolds number of the viscosity               */
+  double prandtl;          /* Prandtl number                                  */
+  double bulk_viscosity;   /* constant model                                  */
+  double sutherland_alpha; /* gamma (gamma - 1) M^2                           */
+  double sutherland_Ts;    /* Sutherland temperature / reference temperature */
+  int reserved[4];
+} aerof_viscous_params;
+int aerof_gpu_set_viscosity(aerof_gpu_ctx* ctx, const aerof_viscous_params* p);
+
 /* ---- implicit operator ------------------------------------------------
  * MatVecProdH1<5,MatScalar,5>::evaluate (MatVecProd.C:1074-1160) =
  * SpaceOperator::computeJacobian (SpaceOperator.C:2088-2150) +

@@ -1167,6 +1167,120 @@ int orc_residual(void* h, const double* U, const double* Ub, int order, double b
                             order, beta, failsafe, R, w);
 }
 
+// ---------------------------------------------------------------------------
+// Viscous (laminar Navier-Stokes) Galerkin term, the SpaceOperator's
+// computeGalerkinTerm (SpaceOperator.C:570-573) for tets:
+// ElemTet::computeGalerkinTerm (ElemTet.C:24-127, the non-embedded branch)
+// with FemEquationTermNS::computeVolumeTerm (FemEquationTermDesc.C:98-160):
+// per tet the P1 shape-function gradients (ElemTet::computeGradientP1Function,
+// ElemTetCore.C:1961-2010), the velocity and temperature at the nodes and
+// their means (NavierStokesTerm.h:205-295), their P1 gradients
+// (NavierStokesTerm.h:357-497), the transport coefficients at the mean
+// temperature (constant viscosity or Sutherland, ViscoFcn.h:46-103; constant
+// Prandtl conductivity kappa = cp mu / Pr, ThermalCondFcn.h:52-75) scaled by
+// 1/Re_mu, the stress tensor and heat flux (NavierStokesTerm.h:561-576,
+// 647-654), r = (0, tau_kj, u_i tau_ij - q_j) for j = x, y, z
+// (NavierStokesTerm.h:690-724), then R[node] += vol (r_0 dN_x + r_1 dN_y +
+// r_2 dN_z) for the tet's four nodes in tet order.  Temperature
+// T = p/(rho (gamma - 1)) (VarFcnSGEuler.h:120-126, Pstiff = 0).
+struct Visc {
+  int model = 0;              // 0 inviscid, 1 constant viscosity, 2 Sutherland
+  double ooreynolds = 0.0;    // 1 / Re_mu
+  double ooprandtl = 0.0;     // 1 / Pr
+  double bulk = 0.0;          // bulk viscosity (constant model)
+  double alpha = 0.0, Ts = 0.0;  // Sutherland: T = alpha T_adim, Ts
+};
+
+static double p1_gradients(const double* X, const int* t, double g[4][3]) {
+  const double* x0 = X + 3 * (size_t)t[0];
+  const double* x1 = X + 3 * (size_t)t[1];
+  const double* x2 = X + 3 * (size_t)t[2];
+  const double* x3 = X + 3 * (size_t)t[3];
+  double jac[3][3];
+  for (int a = 0; a < 3; ++a) {
+    jac[a][0] = x1[a] - x0[a];
+    jac[a][1] = x2[a] - x0[a];
+    jac[a][2] = x3[a] - x0[a];
+  }
+  const double dOmega = jac[0][0] * (jac[1][1] * jac[2][2] - jac[1][2] * jac[2][1]) +
+                        jac[1][0] * (jac[0][2] * jac[2][1] - jac[0][1] * jac[2][2]) +
+                        jac[2][0] * (jac[0][1] * jac[1][2] - jac[0][2] * jac[1][1]);
+  const double t17 = -1.0 / dOmega;
+  g[1][0] = (-jac[1][1] * jac[2][2] + jac[1][2] * jac[2][1]) * t17;
+  g[1][1] = (jac[0][1] * jac[2][2] - jac[0][2] * jac[2][1]) * t17;
+  g[1][2] = -(jac[0][1] * jac[1][2] - jac[0][2] * jac[1][1]) * t17;
+  g[2][0] = -(-jac[1][0] * jac[2][2] + jac[1][2] * jac[2][0]) * t17;
+  g[2][1] = -(jac[0][0] * jac[2][2] - jac[0][2] * jac[2][0]) * t17;
+  g[2][2] = (jac[0][0] * jac[1][2] - jac[0][2] * jac[1][0]) * t17;
+  g[3][0] = -(jac[1][0] * jac[2][1] - jac[1][1] * jac[2][0]) * t17;
+  g[3][1] = (jac[0][0] * jac[2][1] - jac[0][1] * jac[2][0]) * t17;
+  g[3][2] = -(jac[0][0] * jac[1][1] - jac[0][1] * jac[1][0]) * t17;
+  for (int a = 0; a < 3; ++a) g[0][a] = -(g[1][a] + g[2][a] + g[3][a]);
+  return (1.0 / 6.0) * dOmega;
+}
+
+static void galerkin_term(const Mesh& m, const double* V, const Visc& vp, double* R) {
+  const double gam1 = m.gam - 1.0, invgam1 = 1.0 / gam1, cp = m.gam * invgam1;
+  const double fourth = 0.25, twothird = 2.0 / 3.0;
+  for (int t = 0; t < m.T; ++t) {
+    const int* nd = &m.tets[4 * (size_t)t];
+    double g[4][3];
+    const double vol = p1_gradients(m.X.data(), nd, g);
+    double u[4][3], T[4];
+    for (int k = 0; k < 4; ++k) {
+      const double* v = V + 5 * (size_t)nd[k];
+      u[k][0] = v[1]; u[k][1] = v[2]; u[k][2] = v[3];
+      T[k] = invgam1 * (v[4] + 0.0) / v[0];
+    }
+    double ucg[3];
+    for (int a = 0; a < 3; ++a) ucg[a] = fourth * (u[0][a] + u[1][a] + u[2][a] + u[3][a]);
+    const double Tcg = fourth * (T[0] + T[1] + T[2] + T[3]);
+    double dudxj[3][3], dTdxj[3];
+    for (int a = 0; a < 3; ++a)
+      for (int j = 0; j < 3; ++j)
+        dudxj[a][j] = g[0][j] * u[0][a] + g[1][j] * u[1][a] + g[2][j] * u[2][a] + g[3][j] * u[3][a];
+    for (int j = 0; j < 3; ++j) dTdxj[j] = g[0][j] * T[0] + g[1][j] * T[1] + g[2][j] * T[2] + g[3][j] * T[3];
+    double mu, lambda;
+    if (vp.model == 2) {
+      const double Ta = vp.alpha * Tcg;
+      mu = Ta * std::sqrt(Ta) * (1.0 + vp.Ts) / (Ta + vp.Ts);
+      lambda = -twothird * mu;
+    } else {
+      mu = 1.0;
+      lambda = vp.bulk - twothird * mu;
+    }
+    double kappa = vp.ooprandtl * cp * mu;
+    mu *= vp.ooreynolds;
+    lambda *= vp.ooreynolds;
+    kappa *= vp.ooreynolds;
+    const double div = dudxj[0][0] + dudxj[1][1] + dudxj[2][2];
+    double tij[3][3];
+    tij[0][0] = lambda * div + 2.0 * mu * dudxj[0][0];
+    tij[1][1] = lambda * div + 2.0 * mu * dudxj[1][1];
+    tij[2][2] = lambda * div + 2.0 * mu * dudxj[2][2];
+    tij[0][1] = mu * (dudxj[1][0] + dudxj[0][1]);
+    tij[0][2] = mu * (dudxj[2][0] + dudxj[0][2]);
+    tij[1][2] = mu * (dudxj[2][1] + dudxj[1][2]);
+    tij[1][0] = tij[0][1];
+    tij[2][0] = tij[0][2];
+    tij[2][1] = tij[1][2];
+    const double qj[3] = {-kappa * dTdxj[0], -kappa * dTdxj[1], -kappa * dTdxj[2]};
+    double r[3][5];
+    for (int j = 0; j < 3; ++j) {
+      r[j][0] = 0.0;
+      r[j][1] = tij[0][j];
+      r[j][2] = tij[1][j];
+      r[j][3] = tij[2][j];
+      r[j][4] = ucg[0] * tij[0][j] + ucg[1] * tij[1][j] + ucg[2] * tij[2][j] - qj[j];
+    }
+    for (int j = 0; j < 4; ++j) {
+      double* Rj = R + 5 * (size_t)nd[j];
+      for (int k = 0; k < 5; ++k)
+        Rj[k] += vol * (r[0][k] * g[j][0] + r[1][k] * g[j][1] + r[2][k] * g[j][2]);
+    }
+  }
+}
+
 // Timed CPU baseline: threaded residual (order 1 or 2, van Albada).
 struct Baseline {
   std::vector<double> V, G, priv;
@@ -1178,6 +1292,25 @@ void orc_residual_threaded(void* h, void* b, const double* U, const double* Ub, 
   Mesh* m = (Mesh*)h;
   Baseline* bl = (Baseline*)b;
   residual_threaded(*m, U, Ub, order, 1.0 / 3.0, nthreads, R, bl->V, bl->G, bl->priv);
+}
+
+// Residual with the viscous Galerkin term: (R_fv + G) / ctrlVol, evaluated
+// as R_fv / ctrlVol + G / ctrlVol.  model, ooreynolds, ooprandtl, bulk,
+// alpha, Ts as in Visc.
+int orc_residual_visc(void* h, const double* U, const double* Ub, int order, int model, double ooreynolds,
+                      double ooprandtl, double bulk, double alpha, double Ts, double* R) {
+  Mesh* m = (Mesh*)h;
+  const int bad = orc_residual(h, U, Ub, order, 1.0 / 3.0, 0, R);
+  if (model == 0) return bad;
+  Visc vp;
+  vp.model = model; vp.ooreynolds = ooreynolds; vp.ooprandtl = ooprandtl; vp.bulk = bulk;
+  vp.alpha = alpha; vp.Ts = Ts;
+  std::vector<double> V(5 * (size_t)m->N), G(5 * (size_t)m->N, 0.0);
+  for (int i = 0; i < m->N; ++i) cons2prim(m->gam, &U[5 * (size_t)i], &V[5 * (size_t)i]);
+  galerkin_term(*m, V.data(), vp, G.data());
+  for (int i = 0; i < m->N; ++i)
+    for (int k = 0; k < 5; ++k) R[5 * (size_t)i + k] += G[5 * (size_t)i + k] / m->ctrlVol[i];
+  return bad;
 }
 
 void orc_timestep(void* h, const double* U, double cfl, double* dt) { timestep(*(Mesh*)h, U, cfl, dt); }

@@ -70,6 +70,9 @@ def lib():
                                  C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
                                  _dp, _ip, _ip]
         L.orc_jvp.argtypes = [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp]
+        L.orc_residual_visc.restype = C.c_int
+        L.orc_residual_visc.argtypes = [C.c_void_p, _dp, _dp, C.c_int, C.c_int, C.c_double, C.c_double,
+                                        C.c_double, C.c_double, C.c_double, _dp]
         L.orc_matvec_fd.restype = C.c_double
         L.orc_matvec_fd.argtypes = [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp, _dp, C.c_int, _dp]
         L.orc_dRdX.argtypes = [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp, _dp]
@@ -147,6 +150,15 @@ class Oracle:
     def residual(self, U, Ub, order=2, beta=1.0 / 3.0, failsafe=0):
         U = f64(U); Ub = f64(Ub); R = np.empty_like(U)
         ierr = self.L.orc_residual(self.h, _d(U), _d(Ub), order, beta, failsafe, _d(R))
+        return R, ierr
+
+    def residual_visc(self, U, Ub, order=2, model=1, reynolds=100.0, prandtl=0.72, bulk=0.0, alpha=1.0,
+                      Ts=0.0):
+        """Residual plus the laminar viscous Galerkin term (model 1:
+        constant viscosity, 2: Sutherland)."""
+        U = f64(U); R = np.empty_like(U)
+        ierr = self.L.orc_residual_visc(self.h, _d(U), _d(f64(Ub)), order, model, 1.0 / reynolds, 1.0 / prandtl,
+                                        bulk, alpha, Ts, _d(R))
         return R, ierr
 
     def residual_threaded(self, U, Ub, order=2, nthreads=None, out=None):

@@ -228,3 +228,46 @@ def test_roejac6_bitwise(oracle_mod, gold_f77):
         jl, jr = oracle_mod.roejac6(1.4, r[0:3], r[3:8], r[8:13])
         assert np.array_equal(np.asarray(jl).reshape(-1), o[:25])
         assert np.array_equal(np.asarray(jr).reshape(-1), o[25:])
+
+
+# --------------------------------------------------------------------------
+# The viscous Galerkin term (FemEquationTermNS on tets): properties that pin
+# the restatement (the reference's NavierStokesTerm.h needs its MPI headers
+# and cannot be compiled here)
+
+
+def test_viscous_term_vanishes_for_uniform_flow(oracle_mod):
+    m = W.make_lattice_mesh(7, jitter=0.2, codes="channel")
+    o = oracle_mod.Oracle(m)
+    Ub = W.freestream(0.8)
+    U = np.tile(Ub, (o.N, 1))
+    for model, kw in ((1, {}), (2, {"alpha": 1.4 * 0.4 * 0.64, "Ts": 0.38})):
+        Rv, _ = o.residual_visc(U, Ub, 2, model=model, reynolds=50.0, **kw)
+        R, _ = o.residual(U, Ub, 2)
+        assert np.abs(Rv - R).max() < 1e-12
+
+
+def test_viscous_stress_of_linear_velocity_is_divergence_free(oracle_mod):
+    # u = A x + b with uniform temperature: the P1 stress is the same in every
+    # tet, so the momentum rows of the Galerkin term vanish at interior nodes
+    # (the shape-function gradients of a node's star sum to zero)
+    m = W.make_lattice_mesh(7, jitter=0.2, codes="channel")
+    o = oracle_mod.Oracle(m)
+    X = m["X"]
+    A = np.array([[0.1, 0.3, -0.2], [0.05, -0.1, 0.2], [0.3, 0.1, 0.0]])
+    V = np.empty((o.N, 5))
+    V[:, 0] = 1.0
+    V[:, 1:4] = X @ A.T + np.array([1.0, 0.0, 0.0])
+    V[:, 4] = 1.0 / (1.4 * 0.64)
+    U = W.prim_to_cons(V)
+    Ub = W.freestream(0.8)
+    Rv, _ = o.residual_visc(U, Ub, 1, model=1, reynolds=10.0)
+    R, _ = o.residual(U, Ub, 1)
+    G = Rv - R
+    n = 7
+    idx = np.arange(o.N)
+    i, j, k = idx % n, (idx // n) % n, idx // (n * n)
+    interior = (i > 0) & (i < n - 1) & (j > 0) & (j < n - 1) & (k > 0) & (k < n - 1)
+    scale = np.abs(G[:, 1:4]).max()
+    assert scale > 1e-3
+    assert np.abs(G[interior, 1:4]).max() < 1e-11 * max(scale, 1.0)

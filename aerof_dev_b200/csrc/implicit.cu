@@ -1013,7 +1013,8 @@ __global__ void k_ilu_factor(int i0, int cnt, int s0, const int* __restrict__ rj
 template <int L, class S, class TI>
 __global__ void k_ilu_fwd(int i0, int cnt, int s0, const int* __restrict__ cperm, const int* __restrict__ rju,
                           const int* __restrict__ isp, const int* __restrict__ jc, const S* __restrict__ lu,
-                          const TI* __restrict__ x, double* __restrict__ w) {
+                          const TI* __restrict__ x, double* __restrict__ w, const int* __restrict__ skip) {
+  if (skip && *skip) return;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int t = g / L, sub = g % L;
   const bool act = t < cnt;
@@ -1051,7 +1052,9 @@ __global__ void k_ilu_fwd(int i0, int cnt, int s0, const int* __restrict__ cperm
 template <int L, class S, class TO>
 __global__ void k_ilu_bwd(int i0, int cnt, int s0, const int* __restrict__ cperm, const int* __restrict__ rlen,
                           const int* __restrict__ rju, const int* __restrict__ isp, const int* __restrict__ jc,
-                          const S* __restrict__ lu, double* __restrict__ w, TO* __restrict__ z) {
+                          const S* __restrict__ lu, double* __restrict__ w, TO* __restrict__ z,
+                          const int* __restrict__ skip) {
+  if (skip && *skip) return;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int t = g / L, sub = g % L;
   const bool act = t < cnt;
@@ -1262,7 +1265,7 @@ static int ilu_setup(aerof_gpu_ctx* c, int tr) {
 }
 
 template <class TI, class TO>
-static void ilu_apply(aerof_gpu_ctx* c, const TI* x, TO* z) {
+static void ilu_apply(aerof_gpu_ctx* c, const TI* x, TO* z, const int* skip = nullptr) {
   DeviceMesh& m = c->mesh;
   Implicit& J = c->imp;
   cudaStream_t s = c->stream;
@@ -1274,14 +1277,14 @@ static void ilu_apply(aerof_gpu_ctx* c, const TI* x, TO* z) {
     for (int col = 0; col < m.ncolor; ++col) {
       const int i0 = m.h_cptr[col], cnt = m.h_cptr[col + 1] - i0;
       k_ilu_fwd<L, S, TI><<<grid_for((size_t)L * cnt, kIB), kIB, 0, s>>>(i0, cnt, m.h_cslice[col], m.cperm.p,
-                                                                         m.rju.p, m.isp.p, m.jc.p, lu, x, w);
+                                                                         m.rju.p, m.isp.p, m.jc.p, lu, x, w, skip);
       AEROF_LAUNCH_CHECK();
     }
     for (int col = m.ncolor - 1; col >= 0; --col) {
       const int i0 = m.h_cptr[col], cnt = m.h_cptr[col + 1] - i0;
       k_ilu_bwd<L, S, TO><<<grid_for((size_t)L * cnt, kIB), kIB, 0, s>>>(i0, cnt, m.h_cslice[col], m.cperm.p,
                                                                          m.rlen.p, m.rju.p, m.isp.p, m.jc.p, lu, w,
-                                                                         z);
+                                                                         z, skip);
       AEROF_LAUNCH_CHECK();
     }
   };
@@ -1371,7 +1374,7 @@ void prec_apply_t(aerof_gpu_ctx* c, const TI* x, TO* z, int trans, const int* sk
       if (int nb = ilu_setup(c, tr))
         throw ApiError{AEROF_ESINGULAR, std::to_string(nb) + " singular diagonal block(s) in the ILU(0) factors"};
     }
-    ilu_apply(c, x, z);
+    ilu_apply(c, x, z, skip);
     return;
   }
   if (J.precision == AEROF_PREC_FP32)
@@ -1384,9 +1387,9 @@ void prec_apply_dev(aerof_gpu_ctx* c, const double* x, double* z, int trans) {
   prec_apply_t<double, double>(c, x, z, trans);
 }
 
-// Device-driven form of gmres_t for the assembled operator with the
-// block-Jacobi preconditioner: per iteration three launches (preconditioner,
-// product, k_gmres_iter), no host synchronisation inside a restart cycle;
+// Device-driven form of gmres_t for the assembled operator (block-Jacobi or
+// block ILU(0)): per iteration the preconditioner, the product and
+// k_gmres_iter, no host synchronisation inside a restart cycle;
 // the host reads the cycle's status once at its end (AEROF_GMRES_DEVICE=0
 // selects the host-driven loop).
 static bool gmres_device_loop_enabled() {
@@ -1523,7 +1526,7 @@ static int gmres_devloop(aerof_gpu_ctx* c, const double* b, double* x, int numVe
 template <class TV>
 static int gmres_t(aerof_gpu_ctx* c, const double* b, double* x, int numVec, int maxits, double eps, int trans,
                    double* final_res, const double* exactU) {
-  if (!exactU && c->imp.pc == AEROF_PC_JACOBI && numVec <= kMaxKrylov && gmres_device_loop_enabled())
+  if (!exactU && numVec <= kMaxKrylov && gmres_device_loop_enabled())
     return gmres_devloop<TV>(c, b, x, numVec, maxits, eps, trans, final_res);
   DeviceMesh& m = c->mesh;
   Implicit& J = c->imp;

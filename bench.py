@@ -428,7 +428,24 @@ def run_ours(args):
     if world == 1 and not args.no_adjoint_cost:
         line["adjoint_cost"] = adjoint_cost_part(A, ctx, Ud, stream, uuid)
     if world == 1 and not args.no_newton:
-        line["newton"] = newton_part(A, ctx, U, args, uuid)
+        # the configuration the Newton metric names (161^3, block-Jacobi)
+        # on its own mesh, and the benchmark's 101^3 mesh
+        sizes = [int(v) for v in args.newton_meshes.split(",") if v]
+        for nm in sizes:
+            if nm == args.n:
+                part = newton_part(A, ctx, U, args, uuid)
+            else:
+                t0 = time.perf_counter()
+                Wn, mesh_n, Ub_n, U_n = build_workload(nm)
+                ctx_n = A.Context.from_mesh(mesh_n, Ub_n, reconstruction=A.REC_VANALBADA, device=local)
+                ctx_n.set_stream(stream)
+                setup_s = time.perf_counter() - t0
+                part = newton_part(A, ctx_n, U_n, args, uuid)
+                part["mesh_setup_s"] = setup_s
+                ctx_n.close()
+            sn = Wn.lattice_sizes(nm) if nm != args.n else s
+            part["mesh"] = f"{nm}^3 jittered Kuhn tet mesh N={sn['N']} E={sn['E']}"
+            line["newton" if nm == sizes[-1] else f"newton_{nm}"] = part
     ctx.close()
     if pg:
         pg.destroy_process_group()
@@ -691,6 +708,8 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=120.0, help="seconds of timed CPU work (reference arm)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-newton", action="store_true", help="leave the Newton part out of the residual line")
+    ap.add_argument("--newton-meshes", default="101,161",
+                    help="lattice sizes of the Newton part (the last one is reported as 'newton')")
     ap.add_argument("--no-adjoint-cost", action="store_true",
                     help="leave the adjoint-cost part out of the residual line")
     ap.add_argument("--workload", choices=["residual", "newton", "adjoint", "adjoint_products", "sensitivities"],

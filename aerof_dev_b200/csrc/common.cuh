@@ -207,6 +207,16 @@ struct Implicit {
   // target, per-CTA partials; counters and barrier arrivals
   DBuf<double> gst;
   DBuf<int> gsti;
+  // pinned copy of its done flag and the event that marks it current, for
+  // the host's non-blocking polls inside a cycle
+  struct Poll {
+    int* done = nullptr;
+    cudaEvent_t ev = nullptr;
+    ~Poll() {
+      if (done) cudaFreeHost(done);
+      if (ev) cudaEventDestroy(ev);
+    }
+  } poll;
   DBuf<unsigned> ticket;   // grid-reduction ticket of the fused Gram-Schmidt kernels
   DBuf<double> fsum;       // [nbrow][25] boundary-face blocks of the boundary rows
   // preconditioner: AEROF_PC_JACOBI or AEROF_PC_ILU0 (block ILU(0) in the

@@ -1487,16 +1487,44 @@ static int gmres_devloop(aerof_gpu_ctx* c, const double* b, double* x, int numVe
     AEROF_CUDA(cudaMemcpyAsync(st.ist, iinit, sizeof(iinit), cudaMemcpyHostToDevice, s));
     unsigned base = 0;
     const int* done = st.ist + 1;
+    // every four iterations the done flag is copied to pinned memory behind
+    // an event; the host looks at the previous copy without waiting and
+    // stops issuing the cycle once it shows convergence (the kernels issued
+    // after convergence return at once anyway)
+    if (!J.poll.done) {
+      AEROF_CUDA(cudaMallocHost((void**)&J.poll.done, sizeof(int)));
+      AEROF_CUDA(cudaEventCreateWithFlags(&J.poll.ev, cudaEventDisableTiming));
+    }
+    bool polled = false;
     for (int j = 0; j < numVec; ++j) {
+      if (polled) {
+        const cudaError_t q = cudaEventQuery(J.poll.ev);
+        if (q == cudaSuccess) {
+          polled = false;
+          if (*J.poll.done) break;
+        } else if (q != cudaErrorNotReady) {
+          AEROF_CUDA(q);
+        } else if (cudaPeekAtLastError() == cudaErrorNotReady) {
+          cudaGetLastError();  // "not ready" is a state, not an error for the next launch check
+        }
+      }
       prec_apply_t<TV, TV>(c, Vb + (size_t)j * ld, r, trans, done);
       matvec_t<TV, TV>(c, r, w, trans, done);
-      TimerScope t(c, AEROF_T_KSP_OTHER);
-      void* args[] = {(void*)&n, (void*)&j, (void*)&numVec, (void*)&Vb, (void*)&ld, (void*)&w, (void*)&st,
-                      (void*)&base};
-      AEROF_CUDA(cudaLaunchCooperativeKernel((const void*)k_gmres_iter<TV>, grid, kCoopThreads, args, 0, s));
-      AEROF_LAUNCH_CHECK();
-      base += (unsigned)(j + 2) * (unsigned)grid;
+      {
+        TimerScope t(c, AEROF_T_KSP_OTHER);
+        void* args[] = {(void*)&n, (void*)&j, (void*)&numVec, (void*)&Vb, (void*)&ld, (void*)&w, (void*)&st,
+                        (void*)&base};
+        AEROF_CUDA(cudaLaunchCooperativeKernel((const void*)k_gmres_iter<TV>, grid, kCoopThreads, args, 0, s));
+        AEROF_LAUNCH_CHECK();
+        base += (unsigned)(j + 2) * (unsigned)grid;
+      }
+      if ((j & 3) == 3 && !polled && j + 1 < numVec) {
+        AEROF_CUDA(cudaMemcpyAsync(J.poll.done, done, sizeof(int), cudaMemcpyDeviceToHost, s));
+        AEROF_CUDA(cudaEventRecord(J.poll.ev, s));
+        polled = true;
+      }
     }
+    if (polled) AEROF_CUDA(cudaEventSynchronize(J.poll.ev));
     k_gmres_backsolve<<<1, 32, 0, s>>>(numVec, st);
     AEROF_LAUNCH_CHECK();
     k_combine_dev<TV><<<gv, kIB, 0, s>>>(n, st.ist + 2, st.y, Vb, ld, w);

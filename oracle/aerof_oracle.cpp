@@ -1023,11 +1023,177 @@ static int invert5(S* a) {
 // GmresSolver::solve (KspSolver.C:351-492) with right preconditioning
 // (typePrec = 2), modified Gram-Schmidt and Givens rotations
 // (KspSolver.C:917-982).  x starts at 0 (ImplicitCoupledTsDesc.C:292).
+// Factors of the block ILU(0) of one operator on one node ordering
+// (SparseMat after numericILU): rows in the order perm (perm[i] = node of
+// row i), CSR pattern ia/ja of the node graph plus the diagonal, ju the
+// diagonal's position, a the L\U blocks with the inverted diagonal.
+struct IluFactors {
+  int N = 0, bad = 0;
+  std::vector<int> perm, ia, ja, ju;
+  std::vector<double> a;
+};
+
+// Block ILU(0) preconditioner (IluPrec, KspPrec.C:138-330, fill 0):
+// SparseMat::numericILU and lusol (SparseMatrix.C:353-450) restated on a
+// node ordering: by default the multicolour ordering the GPU uses (greedy
+// colouring of the node graph in ascending node order, smallest colour not
+// taken by an already coloured neighbour, rows sorted by (colour, node)),
+// or the given order; columns of each row ascending in that order.  A is
+// the MvpMat layout a[N + 2E][25]; the factored operator is A (transpose =
+// 0) or A^T (1).  fp32 != 0 rounds every stored block to float
+// (PrecScalar = float), arithmetic in double.  ilu_solve: y = (LU)^-1 x in
+// the caller's numbering.  F->bad counts singular diagonal blocks.
+static IluFactors* ilu_factor(const Mesh* m, const double* A, int fp32, int transpose, const int* order,
+                              int* ncolor_out, int* colour_out) {
+  const int N = m->N;
+  // neighbours ascending (edges are lexicographic: node -> incident edges
+  // ascending gives ascending neighbours)
+  std::vector<int> col(N, -1);
+  int nc = 0;
+  auto nbr = [&](int i, int k) {
+    const int l = m->nodeEdgeIdx[k];
+    return m->edges[2 * l] == i ? m->edges[2 * l + 1] : m->edges[2 * l];
+  };
+  for (int i = 0; i < N; ++i) {
+    std::vector<char> seen(nc + 1, 0);
+    for (int k = m->nodeEdgePtr[i]; k < m->nodeEdgePtr[i + 1]; ++k) {
+      const int c = col[nbr(i, k)];
+      if (c >= 0) seen[c] = 1;
+    }
+    int c = 0;
+    while (seen[c]) ++c;
+    col[i] = c;
+    nc = std::max(nc, c + 1);
+  }
+  if (ncolor_out) *ncolor_out = nc;
+  if (colour_out) std::memcpy(colour_out, col.data(), sizeof(int) * N);
+  std::vector<int> perm, iperm(N);
+  if (order) {
+    perm.assign(order, order + N);
+  } else {
+    for (int c = 0; c < nc; ++c)
+      for (int i = 0; i < N; ++i)
+        if (col[i] == c) perm.push_back(i);
+  }
+  for (int i = 0; i < N; ++i) iperm[perm[i]] = i;
+  // pattern and blocks in colour order
+  std::vector<int> ia(N + 1), ja, ju(N);
+  std::vector<double> a;
+  auto block = [&](int r, int cnode, double* out) {
+    // block (r, cnode) of the operator
+    const double* src;
+    bool tr = transpose != 0;
+    int rr = r, cc = cnode;
+    if (tr) std::swap(rr, cc);
+    if (rr == cc) {
+      src = &A[25 * (size_t)rr];
+    } else {
+      const int lo = std::min(rr, cc), hi = std::max(rr, cc);
+      int l = -1;
+      for (int k = m->nodeEdgePtr[lo]; k < m->nodeEdgePtr[lo + 1]; ++k)
+        if (nbr(lo, k) == hi) l = m->nodeEdgeIdx[k];
+      src = &A[25 * ((size_t)N + 2 * (size_t)l + (rr < cc ? 0 : 1))];
+    }
+    for (int e = 0; e < 25; ++e) {
+      double v = tr ? src[5 * (e % 5) + e / 5] : src[e];
+      out[e] = fp32 ? (double)(float)v : v;
+    }
+  };
+  for (int i = 0; i < N; ++i) {
+    const int r = perm[i];
+    std::vector<int> cols{i};
+    for (int k = m->nodeEdgePtr[r]; k < m->nodeEdgePtr[r + 1]; ++k) cols.push_back(iperm[nbr(r, k)]);
+    std::sort(cols.begin(), cols.end());
+    ia[i] = (int)ja.size();
+    for (int c : cols) {
+      if (c == i) ju[i] = (int)ja.size();
+      ja.push_back(c);
+      a.resize(a.size() + 25);
+      block(r, perm[c], &a[a.size() - 25]);
+    }
+  }
+  ia[N] = (int)ja.size();
+  auto rnd = [&](double v) { return fp32 ? (double)(float)v : v; };
+  // numericILU
+  int bad = 0;
+  std::vector<int> marker(N, -1);
+  for (int i = 0; i < N; ++i) {
+    for (int k = ia[i]; k < ia[i + 1]; ++k) marker[ja[k]] = k;
+    for (int k = ia[i]; k < ju[i]; ++k) {
+      const int l = ja[k];
+      double mult[25];
+      for (int r = 0; r < 5; ++r)
+        for (int c = 0; c < 5; ++c) {
+          double t = 0.0;
+          for (int q = 0; q < 5; ++q) t += a[25 * (size_t)k + 5 * r + q] * a[25 * (size_t)ju[l] + 5 * q + c];
+          mult[5 * r + c] = t;
+        }
+      for (int e = 0; e < 25; ++e) a[25 * (size_t)k + e] = rnd(mult[e]);
+      for (int j = ju[l] + 1; j < ia[l + 1]; ++j) {
+        const int mm = marker[ja[j]];
+        if (mm == -1) continue;
+        for (int r = 0; r < 5; ++r)
+          for (int c = 0; c < 5; ++c) {
+            double t = a[25 * (size_t)mm + 5 * r + c];
+            for (int q = 0; q < 5; ++q) t -= mult[5 * r + q] * a[25 * (size_t)j + 5 * q + c];
+            a[25 * (size_t)mm + 5 * r + c] = rnd(t);
+          }
+      }
+    }
+    for (int k = ia[i]; k < ia[i + 1]; ++k) marker[ja[k]] = -1;
+    double d[25];
+    for (int e = 0; e < 25; ++e) d[e] = a[25 * (size_t)ju[i] + e];
+    if (invert5<double>(d)) ++bad;
+    for (int e = 0; e < 25; ++e) a[25 * (size_t)ju[i] + e] = rnd(d[e]);
+  }
+  IluFactors* F = new IluFactors;
+  F->N = N;
+  F->bad = bad;
+  F->perm = std::move(perm);
+  F->ia = std::move(ia);
+  F->ja = std::move(ja);
+  F->ju = std::move(ju);
+  F->a = std::move(a);
+  return F;
+}
+
+static void ilu_solve(const IluFactors& F, const double* x, double* y) {
+  const int N = F.N;
+  const std::vector<int>& perm = F.perm;
+  const std::vector<int>& ia = F.ia;
+  const std::vector<int>& ja = F.ja;
+  const std::vector<int>& ju = F.ju;
+  const std::vector<double>& a = F.a;
+  std::vector<double> w(5 * (size_t)N);
+  for (int i = 0; i < N; ++i) {
+    double acc[5];
+    for (int c = 0; c < 5; ++c) acc[c] = x[5 * (size_t)perm[i] + c];
+    for (int k = ia[i]; k < ju[i]; ++k)
+      for (int r = 0; r < 5; ++r)
+        for (int c = 0; c < 5; ++c) acc[r] -= a[25 * (size_t)k + 5 * r + c] * w[5 * (size_t)ja[k] + c];
+    for (int c = 0; c < 5; ++c) w[5 * (size_t)i + c] = acc[c];
+  }
+  for (int i = N - 1; i >= 0; --i) {
+    double acc[5];
+    for (int c = 0; c < 5; ++c) acc[c] = w[5 * (size_t)i + c];
+    for (int k = ju[i] + 1; k < ia[i + 1]; ++k)
+      for (int r = 0; r < 5; ++r)
+        for (int c = 0; c < 5; ++c) acc[r] -= a[25 * (size_t)k + 5 * r + c] * w[5 * (size_t)ja[k] + c];
+    for (int r = 0; r < 5; ++r) {
+      double t = 0.0;
+      for (int c = 0; c < 5; ++c) t += a[25 * (size_t)ju[i] + 5 * r + c] * acc[c];
+      w[5 * (size_t)i + r] = t;
+      y[5 * (size_t)perm[i] + r] = t;
+    }
+  }
+}
+
 struct Operator {
   const Mesh* m;
   const double* A;           // H1 Jacobian (MvpMat layout)
   std::vector<double> Dinv;  // block-Jacobi inverses (FP64 or rounded FP32)
   int transpose = 0;
+  const IluFactors* ilu = nullptr;  // when set, the preconditioner instead of Dinv
 };
 
 static double dotv(const std::vector<double>& a, const std::vector<double>& b) {
@@ -1037,6 +1203,10 @@ static double dotv(const std::vector<double>& a, const std::vector<double>& b) {
 }
 
 static void bj_apply(const Operator& op, const std::vector<double>& x, std::vector<double>& y) {
+  if (op.ilu) {
+    ilu_solve(*op.ilu, x.data(), y.data());
+    return;
+  }
   const int N = op.m->N;
   for (int i = 0; i < N; ++i) {
     const double* d = &op.Dinv[25 * (size_t)i];
@@ -1394,140 +1564,156 @@ int orc_bj_invert(void* h, const double* A, double* Dinv, int fp32) {
   return bad;
 }
 
-// Block ILU(0) preconditioner (IluPrec, KspPrec.C:138-330, fill 0):
-// SparseMat::numericILU and lusol (SparseMatrix.C:353-450) restated on the
-// multicolour node ordering the GPU uses: greedy colouring of the node
-// graph in ascending node order (smallest colour not taken by an already
-// coloured neighbour), rows sorted by (colour, node), columns of each row
-// ascending in that order.  A is the MvpMat layout a[N + 2E][25]; the
-// factored operator is A (transpose = 0) or A^T (1).  fp32 != 0 rounds every
-// stored block to float (PrecScalar = float), arithmetic in double.  y =
-// (LU)^-1 x in the caller's numbering.  Returns the number of singular
-// diagonal blocks, or -1 when ncolor / colour are requested and too small.
 int orc_ilu0(void* h, const double* A, int fp32, int transpose, const double* x, double* y, int* ncolor_out,
              int* colour_out) {
+  IluFactors* F = ilu_factor((Mesh*)h, A, fp32, transpose, nullptr, ncolor_out, colour_out);
+  if (!F) return -1;
+  ilu_solve(*F, x, y);
+  const int bad = F->bad;
+  delete F;
+  return bad;
+}
+
+// The same factorisation kept for repeated solves, on the multicolour
+// order (order == null) or on a given node order (order[i] = node of row
+// i, e.g. the reverse Cuthill-McKee order of orc_rcm_order).
+void* orc_ilu_factor(void* h, const double* A, int fp32, int transpose, const int* order, int* bad) {
+  IluFactors* F = ilu_factor((Mesh*)h, A, fp32, transpose, order, nullptr, nullptr);
+  if (bad) *bad = F ? F->bad : -1;
+  return F;
+}
+void orc_ilu_apply(void* f, const double* x, double* y) { ilu_solve(*(IluFactors*)f, x, y); }
+void orc_ilu_free(void* f) { delete (IluFactors*)f; }
+
+// Reverse Cuthill-McKee order of the ILU(0) rows, as the reference
+// renumbers a subdomain's ILU matrix (PcData::renumbering = RCM,
+// IoDataCore.C:2744-2745; SubDomain::createMaskILU, SubDomain.C:3371-3390):
+// the node graph with each node's own entry, neighbours ascending
+// (SubDomain::createEdgeBasedConnectivity, SubDomainCore.C:253-318), one
+// connected component after another from the lowest-numbered unvisited node
+// (Connectivity::renumByComponent), each renumbered by renumRCM
+// (ConnectivityCore.C:582-626): a pseudo-peripheral end node from
+// findPseudoDiam (:324-383, rooted level structures of rootLS, :386-420),
+// breadth-first from it with neighbours in ascending order, then reversed.
+// renumRCM's sort of each new level segment by degree swaps nothing
+// (order[k] is written twice), so neighbours keep their ascending order, as
+// in the reference.  order[r] = node of row r.
+namespace {
+struct NodeGraph {
+  int n;
+  std::vector<int> ptr, tgt;  // with the node's own entry, ascending
+  int num(int i, const std::vector<int>& mask) const {
+    int r = 0;
+    for (int k = ptr[i]; k < ptr[i + 1]; ++k)
+      if (mask[tgt[k]]) ++r;
+    return r;
+  }
+  // rooted level structure: ls (levels xls[0..h]), width w; returns h
+  int rootLS(int root, std::vector<int>& xls, std::vector<int>& ls, int& w, const std::vector<int>& mask) const {
+    std::vector<int> loc(mask);
+    w = 0;
+    loc[root] = 0;
+    ls[0] = root;
+    xls[0] = 0;
+    int nlvl = 1, nf = 1;
+    while (nf > xls[nlvl - 1]) {
+      xls[nlvl] = nf;
+      const int lb = xls[nlvl - 1], le = xls[nlvl];
+      for (int i = lb; i < le; ++i) {
+        const int n1 = ls[i];
+        for (int k = ptr[n1]; k < ptr[n1 + 1]; ++k) {
+          const int n2 = tgt[k];
+          if (loc[n2]) { loc[n2] = 0; ls[nf++] = n2; }
+        }
+      }
+      if (nf - xls[nlvl] > w) w = nf - xls[nlvl];
+      ++nlvl;
+    }
+    return nlvl - 1;
+  }
+};
+}  // namespace
+
+void orc_rcm_order(void* h, int* order) {
   Mesh* m = (Mesh*)h;
   const int N = m->N;
-  // neighbours ascending (edges are lexicographic: node -> incident edges
-  // ascending gives ascending neighbours)
-  std::vector<int> col(N, -1);
-  int nc = 0;
-  auto nbr = [&](int i, int k) {
-    const int l = m->nodeEdgeIdx[k];
-    return m->edges[2 * l] == i ? m->edges[2 * l + 1] : m->edges[2 * l];
-  };
+  NodeGraph G;
+  G.n = N;
+  G.ptr.assign(N + 1, 0);
+  for (int i = 0; i < N; ++i) G.ptr[i + 1] = G.ptr[i] + 1 + (m->nodeEdgePtr[i + 1] - m->nodeEdgePtr[i]);
+  G.tgt.resize(G.ptr[N]);
   for (int i = 0; i < N; ++i) {
-    std::vector<char> seen(nc + 1, 0);
+    int q = G.ptr[i];
+    G.tgt[q++] = i;
     for (int k = m->nodeEdgePtr[i]; k < m->nodeEdgePtr[i + 1]; ++k) {
-      const int c = col[nbr(i, k)];
-      if (c >= 0) seen[c] = 1;
+      const int l = m->nodeEdgeIdx[k];
+      G.tgt[q++] = m->edges[2 * l] == i ? m->edges[2 * l + 1] : m->edges[2 * l];
     }
-    int c = 0;
-    while (seen[c]) ++c;
-    col[i] = c;
-    nc = std::max(nc, c + 1);
+    std::stable_sort(G.tgt.begin() + G.ptr[i], G.tgt.begin() + G.ptr[i + 1]);
   }
-  if (ncolor_out) *ncolor_out = nc;
-  if (colour_out) std::memcpy(colour_out, col.data(), sizeof(int) * N);
-  std::vector<int> perm, iperm(N);
-  for (int c = 0; c < nc; ++c)
+  std::vector<int> mark(N, 1), renum(N, -1), ls(N), xls(N + 1), loc(N, 0), all(N, 1);
+  int next = 0;
+  for (int inode = 0; inode < N; ++inode) {
+    if (!mark[inode]) continue;
+    int w;
+    const int hc = G.rootLS(inode, xls, ls, w, all);  // the component of inode
+    for (int j = 0; j < xls[hc]; ++j) { loc[ls[j]] = 1; mark[ls[j]] = 0; }
+    // findPseudoDiam on the component
+    int s = 0, e = 0, cmin = G.ptr[N] + 1, cmax = 0;
     for (int i = 0; i < N; ++i)
-      if (col[i] == c) perm.push_back(i);
-  for (int i = 0; i < N; ++i) iperm[perm[i]] = i;
-  // pattern and blocks in colour order
-  std::vector<int> ia(N + 1), ja, ju(N);
-  std::vector<double> a;
-  auto block = [&](int r, int cnode, double* out) {
-    // block (r, cnode) of the operator
-    const double* src;
-    bool tr = transpose != 0;
-    int rr = r, cc = cnode;
-    if (tr) std::swap(rr, cc);
-    if (rr == cc) {
-      src = &A[25 * (size_t)rr];
-    } else {
-      const int lo = std::min(rr, cc), hi = std::max(rr, cc);
-      int l = -1;
-      for (int k = m->nodeEdgePtr[lo]; k < m->nodeEdgePtr[lo + 1]; ++k)
-        if (nbr(lo, k) == hi) l = m->nodeEdgeIdx[k];
-      src = &A[25 * ((size_t)N + 2 * (size_t)l + (rr < cc ? 0 : 1))];
-    }
-    for (int e = 0; e < 25; ++e) {
-      double v = tr ? src[5 * (e % 5) + e / 5] : src[e];
-      out[e] = fp32 ? (double)(float)v : v;
-    }
-  };
-  for (int i = 0; i < N; ++i) {
-    const int r = perm[i];
-    std::vector<int> cols{i};
-    for (int k = m->nodeEdgePtr[r]; k < m->nodeEdgePtr[r + 1]; ++k) cols.push_back(iperm[nbr(r, k)]);
-    std::sort(cols.begin(), cols.end());
-    ia[i] = (int)ja.size();
-    for (int c : cols) {
-      if (c == i) ju[i] = (int)ja.size();
-      ja.push_back(c);
-      a.resize(a.size() + 25);
-      block(r, perm[c], &a[a.size() - 25]);
-    }
-  }
-  ia[N] = (int)ja.size();
-  auto rnd = [&](double v) { return fp32 ? (double)(float)v : v; };
-  // numericILU
-  int bad = 0;
-  std::vector<int> marker(N, -1);
-  for (int i = 0; i < N; ++i) {
-    for (int k = ia[i]; k < ia[i + 1]; ++k) marker[ja[k]] = k;
-    for (int k = ia[i]; k < ju[i]; ++k) {
-      const int l = ja[k];
-      double mult[25];
-      for (int r = 0; r < 5; ++r)
-        for (int c = 0; c < 5; ++c) {
-          double t = 0.0;
-          for (int q = 0; q < 5; ++q) t += a[25 * (size_t)k + 5 * r + q] * a[25 * (size_t)ju[l] + 5 * q + c];
-          mult[5 * r + c] = t;
-        }
-      for (int e = 0; e < 25; ++e) a[25 * (size_t)k + e] = rnd(mult[e]);
-      for (int j = ju[l] + 1; j < ia[l + 1]; ++j) {
-        const int mm = marker[ja[j]];
-        if (mm == -1) continue;
-        for (int r = 0; r < 5; ++r)
-          for (int c = 0; c < 5; ++c) {
-            double t = a[25 * (size_t)mm + 5 * r + c];
-            for (int q = 0; q < 5; ++q) t -= mult[5 * r + q] * a[25 * (size_t)j + 5 * q + c];
-            a[25 * (size_t)mm + 5 * r + c] = rnd(t);
+      if (loc[i]) {
+        const int nw = G.num(i, loc);
+        if (nw < cmin) { cmin = nw; s = i; }
+        if (nw > cmax) cmax = nw;
+      }
+    int hh = G.rootLS(s, xls, ls, w, loc);
+    const int sub = xls[hh];
+    e = ls[xls[hh - 1]];
+    std::vector<int> sorted(cmax + 1);
+    while (hh < sub) {
+      std::fill(sorted.begin(), sorted.end(), -1);
+      for (int k = xls[hh - 1]; k < xls[hh]; ++k) sorted[G.num(ls[k], loc)] = ls[k];
+      int w_e = sub, k;
+      for (k = 0; k <= cmax; ++k)
+        if (sorted[k] >= 0) {
+          const int nh = G.rootLS(sorted[k], xls, ls, w, loc);
+          if (w < w_e) {
+            if (nh > hh) { s = sorted[k]; hh = nh; break; }
+            e = sorted[k];
+            w_e = w;
           }
+        }
+      if (k > cmax) break;
+    }
+    // renumRCM from e
+    std::vector<int> sign(loc), ord;
+    ord.push_back(e);
+    sign[e] = -sign[e];
+    for (size_t i = 0; i < ord.size(); ++i) {
+      const int cur = ord[i];
+      for (int k = G.ptr[cur]; k < G.ptr[cur + 1]; ++k) {
+        const int nb = G.tgt[k];
+        if (sign[nb] > 0) { ord.push_back(nb); sign[nb] = -sign[nb]; }
       }
     }
-    for (int k = ia[i]; k < ia[i + 1]; ++k) marker[ja[k]] = -1;
-    double d[25];
-    for (int e = 0; e < 25; ++e) d[e] = a[25 * (size_t)ju[i] + e];
-    if (invert5<double>(d)) ++bad;
-    for (int e = 0; e < 25; ++e) a[25 * (size_t)ju[i] + e] = rnd(d[e]);
+    for (size_t i = ord.size(); i--;) renum[ord[i]] = next++;
+    for (int j = 0; j < N; ++j) loc[j] = 0;
   }
-  // lusol
-  std::vector<double> w(5 * (size_t)N);
-  for (int i = 0; i < N; ++i) {
-    double acc[5];
-    for (int c = 0; c < 5; ++c) acc[c] = x[5 * (size_t)perm[i] + c];
-    for (int k = ia[i]; k < ju[i]; ++k)
-      for (int r = 0; r < 5; ++r)
-        for (int c = 0; c < 5; ++c) acc[r] -= a[25 * (size_t)k + 5 * r + c] * w[5 * (size_t)ja[k] + c];
-    for (int c = 0; c < 5; ++c) w[5 * (size_t)i + c] = acc[c];
-  }
-  for (int i = N - 1; i >= 0; --i) {
-    double acc[5];
-    for (int c = 0; c < 5; ++c) acc[c] = w[5 * (size_t)i + c];
-    for (int k = ju[i] + 1; k < ia[i + 1]; ++k)
-      for (int r = 0; r < 5; ++r)
-        for (int c = 0; c < 5; ++c) acc[r] -= a[25 * (size_t)k + 5 * r + c] * w[5 * (size_t)ja[k] + c];
-    for (int r = 0; r < 5; ++r) {
-      double t = 0.0;
-      for (int c = 0; c < 5; ++c) t += a[25 * (size_t)ju[i] + 5 * r + c] * acc[c];
-      w[5 * (size_t)i + r] = t;
-      y[5 * (size_t)perm[i] + r] = t;
-    }
-  }
-  return bad;
+  for (int i = 0; i < N; ++i) order[renum[i]] = i;
+}
+
+// Right-preconditioned GMRES with the block ILU(0) factors f (orc_ilu_factor)
+// as the preconditioner, otherwise as orc_gmres.
+int orc_gmres_ilu(void* h, const double* A, void* f, const double* b, double* x, int numVec, int maxits,
+                  double eps, int transpose, double* final_res) {
+  Mesh* m = (Mesh*)h;
+  Operator op;
+  op.m = m; op.A = A; op.transpose = transpose;
+  op.ilu = (const IluFactors*)f;
+  std::vector<double> bb(b, b + 5 * (size_t)m->N), xx(5 * (size_t)m->N, 0.0);
+  int its = gmres(op, bb, xx, numVec, maxits, eps, final_res);
+  std::memcpy(x, xx.data(), sizeof(double) * xx.size());
+  return its;
 }
 
 int orc_gmres(void* h, const double* A, const double* Dinv, const double* b, double* x, int numVec,

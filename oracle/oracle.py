@@ -66,6 +66,14 @@ def lib():
         L.orc_gmres.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.c_int, C.c_int, C.c_double, C.c_int, _dp]
         L.orc_ilu0.restype = C.c_int
         L.orc_ilu0.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, _dp, _dp, C.POINTER(C.c_int), _ip]
+        L.orc_ilu_factor.restype = C.c_void_p
+        L.orc_ilu_factor.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, _ip, C.POINTER(C.c_int)]
+        L.orc_ilu_apply.argtypes = [C.c_void_p, _dp, _dp]
+        L.orc_ilu_free.argtypes = [C.c_void_p]
+        L.orc_rcm_order.argtypes = [C.c_void_p, _ip]
+        L.orc_gmres_ilu.restype = C.c_int
+        L.orc_gmres_ilu.argtypes = [C.c_void_p, _dp, C.c_void_p, _dp, _dp, C.c_int, C.c_int, C.c_double, C.c_int,
+                                    _dp]
         L.orc_newton.argtypes = [C.c_void_p, _dp, _dp, C.c_int, C.c_double, C.c_double, C.c_double,
                                  C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
                                  _dp, _ip, _ip]
@@ -205,6 +213,27 @@ class Oracle:
         bad = self.L.orc_ilu0(self.h, _d(f64(A)), int(fp32), int(transpose), _d(x), _d(y), C.byref(nc),
                               _i(colour))
         return y, bad, nc.value, colour
+
+    def rcm_order(self):
+        """Reverse Cuthill-McKee order of the ILU rows (order[r] = node of
+        row r), the reference's default ILU renumbering."""
+        order = np.empty(self.N, dtype=np.int32)
+        self.L.orc_rcm_order(self.h, _i(order))
+        return order
+
+    def gmres_ilu(self, A, b, order=None, fp32=True, numVec=30, maxits=30, eps=1e-2, transpose=False):
+        """GMRES right-preconditioned by the block ILU(0) of A factored on
+        the multicolour order (order None) or on the given node order."""
+        b = f64(b); x = np.empty_like(b); res = C.c_double(0); bad = C.c_int(0)
+        o = None if order is None else np.ascontiguousarray(order, dtype=np.int32)
+        f = self.L.orc_ilu_factor(self.h, _d(f64(A)), int(fp32), int(transpose),
+                                  _i(o) if o is not None else None, C.byref(bad))
+        try:
+            its = self.L.orc_gmres_ilu(self.h, _d(f64(A)), f, _d(b), _d(x), numVec, maxits, eps, int(transpose),
+                                       C.byref(res))
+        finally:
+            self.L.orc_ilu_free(f)
+        return x, its, res.value
 
     def gmres(self, A, Dinv, b, numVec=30, maxits=30, eps=1e-2, transpose=False):
         b = f64(b); x = np.empty_like(b); res = C.c_double(0)

@@ -61,3 +61,39 @@ def test_stronger_than_block_jacobi(system, tr):
                 x = x + o.ilu0(A, r, fp32=False, transpose=tr)[0]
         out[name] = np.linalg.norm(b - o.matvec(A, x, transpose=tr)) / np.linalg.norm(b)
     assert out["ilu"] < 0.1 * out["bj"]
+
+
+def test_rcm_order_is_a_breadth_first_permutation(system):
+    # reverse Cuthill-McKee (renumRCM): a permutation of the nodes whose
+    # reversal visits every node after at least one already visited
+    # neighbour (breadth-first from the pseudo-peripheral end node)
+    o, A = system
+    order = o.rcm_order()
+    assert sorted(order.tolist()) == list(range(o.N))
+    e = o.edges()
+    nb = [set() for _ in range(o.N)]
+    for a, b in e:
+        nb[a].add(b); nb[b].add(a)
+    seen = {int(order[-1])}
+    for v in order[::-1][1:]:
+        assert nb[int(v)] & seen
+        seen.add(int(v))
+
+
+@pytest.mark.parametrize("cfl", [100.0, 1e4])
+def test_rcm_ilu_converges_in_fewer_iterations_than_multicolour(system, cfl):
+    # the price of the multicolour ordering the GPU sweeps use: the
+    # reference's RCM-ordered ILU(0) (PcData::renumbering = RCM) needs fewer
+    # GMRES iterations on the same H1 system; both beat block-Jacobi
+    o, _ = system
+    U = W.perturbed_state(o.N, 0.8)
+    Ub = W.freestream(0.8)
+    A = o.jacobian(U, Ub, o.timestep(U, cfl))
+    b = -o.residual(U, Ub, 2)[0]
+    D, _ = o.bj_invert(A)
+    _, its_bj, _ = o.gmres(A, D, b, maxits=2000, eps=1e-6)
+    _, its_col, r_col = o.gmres_ilu(A, b, None, maxits=2000, eps=1e-6)
+    _, its_rcm, r_rcm = o.gmres_ilu(A, b, o.rcm_order(), maxits=2000, eps=1e-6)
+    bn = np.linalg.norm(b)
+    assert r_col <= 1e-6 * bn and r_rcm <= 1e-6 * bn
+    assert its_rcm < its_col < its_bj

@@ -57,7 +57,7 @@ EXPORTS = [
     "aerof_sower_open", "aerof_sower_close", "aerof_sower_num_subdomains", "aerof_sower_subdomain_sizes",
     "aerof_sower_read_subdomain", "aerof_sower_last_error",
 ]
-TIMER_NAMES = ["nodal_grad", "fv_term", "time_step", "fv_jac", "prec_setup", "ksp_matvec", "ksp_other", "other"]
+TIMER_NAMES = ["nodal_grad", "fv_term", "time_step", "fv_jac", "prec_setup", "ksp_matvec", "ksp_other", "fv_edges"]
 
 
 class AerofError(RuntimeError):

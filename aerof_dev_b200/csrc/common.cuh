@@ -7,6 +7,7 @@
 
 #include <cstdio>
 #include <atomic>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -172,6 +173,34 @@ struct DeviceMesh {
   DBuf<int> xslot;         // [E] spill slot of a block-crossing edge, -1 otherwise
   DBuf<int> xin_ptr;       // per node (new): its incoming spill slots [xin_ptr[n], xin_ptr[n+1])
   DBuf<int> bnf_ptr, bnf_ent;   // per node (new): its boundary subface fluxes, rows 3 f + l of fbuf, face order
+  // dependencies of the blocked residual on the caller's rows (for the
+  // residual of host arrays with its copies overlapped, residual.cu): per
+  // block the highest caller row that its primitive conversion, its
+  // gradients, its edge fluxes and its node assembly need
+  std::vector<int> h_prow, h_grow, h_frow, h_nrow;
+  std::vector<int> h_face_prow; // per boundary face: the highest row its nodes' conversions need
+  std::vector<int> h_o2n;       // [N] caller row -> blocked node
+};
+
+// Residual of host arrays in K chunks of caller rows: the copy of chunk s
+// of U, then the blocks whose stages it completes, while the next chunk is
+// copied in and finished chunks of R are copied out (residual.cu).
+struct ResidualPipe {
+  int K = 0;
+  cudaStream_t sin = nullptr, sout = nullptr;
+  std::vector<cudaEvent_t> ev_in, ev_stage;  // [K] chunk of U on the device; [K] stage s computed
+  cudaEvent_t ev_go = nullptr, ev_out = nullptr;
+  DBuf<int> lists;                   // block (face) lists of every (kind, stage)
+  std::vector<int> off;              // [5 kinds][K + 1] offsets into lists
+  std::vector<int> out_stage;        // [K] stage after which caller chunk c of R is final
+  ~ResidualPipe() {
+    for (auto e : ev_in) cudaEventDestroy(e);
+    for (auto e : ev_stage) cudaEventDestroy(e);
+    if (ev_go) cudaEventDestroy(ev_go);
+    if (ev_out) cudaEventDestroy(ev_out);
+    if (sin) cudaStreamDestroy(sin);
+    if (sout) cudaStreamDestroy(sout);
+  }
 };
 
 struct Scratch {
@@ -327,6 +356,9 @@ struct aerof_gpu_ctx {
   int n_owned = 0;
   // viscous Galerkin term (model 0: inviscid)
   aerof_viscous_params visc = {};
+  // schedule and streams of the residual of host arrays (built on first use
+  // for the current mesh)
+  std::unique_ptr<aerof::ResidualPipe> pipe;
 };
 
 namespace aerof {
@@ -393,6 +425,17 @@ __device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+// Bulk prefetch of a contiguous global range into L2 (no destination, no
+// completion to wait for): src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void prefetch_l2_bulk(const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(src), "r"(bytes) : "memory");
+}
+// The stored operator's pairs of edges [e0, e1): one bulk L2 prefetch per
+// pair array ([npair][E] double2), issued by the first npair threads.
+__device__ __forceinline__ void prefetch_pairs_l2(const double2* h2, size_t E, int e0, int e1, int npair) {
+  const int k = threadIdx.x;
+  if (k < npair && e1 > e0) prefetch_l2_bulk(h2 + (size_t)k * E + e0, 16u * (unsigned)(e1 - e0));
+}
 
 // implemented in residual.cu (used by implicit.cu and adjoint.cu).  With
 // sync == false the unphysical count is left on the device (counters[2]).

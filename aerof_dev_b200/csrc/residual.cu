@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(256, 2) k_grad_pipe(int N, int NB, int nblk, i
                                                       const int* __restrict__ nb2_ptr,
                                                       const unsigned short* __restrict__ lpad,
                                                       const int* __restrict__ hpad, const int* __restrict__ tag,
-                                                      double* __restrict__ G2) {
+                                                      double* __restrict__ G2, const int* __restrict__ blist) {
   extern __shared__ double sm[];
   const int tid = threadIdx.x;
   auto load_ids = [&](int b, int& a0, int& a1) {
@@ -289,18 +289,21 @@ __global__ void __launch_bounds__(256, 2) k_grad_pipe(int N, int NB, int nblk, i
     for (int k = tid; 4 * k < nn + 1; k += blockDim.x) cp_async16(S + st.ptr + 2 * k, nb2_ptr + n0 + 4 * k);
     for (int k = tid; 8 * k < maxLp; k += blockDim.x) cp_async16(S + st.ls + 2 * k, lpad + (size_t)b * maxLp + 8 * k);
   };
-  int b = blockIdx.x;
-  if (b >= nblk) return;
+  // blocks blist[0, nblk) (all blocks in order when blist is null)
+  auto bid = [&](int i) { return blist ? blist[i] : i; };
+  int i = blockIdx.x;
+  if (i >= nblk) return;
   int a0, a1;
-  load_ids(b, a0, a1);
-  issue(b, sm, a0, a1);
+  load_ids(bid(i), a0, a1);
+  issue(bid(i), sm, a0, a1);
   cp_async_commit();
-  if (b + (int)gridDim.x < nblk) load_ids(b + gridDim.x, a0, a1);
-  for (int k = 0; b < nblk; ++k, b += gridDim.x) {
-    const int bn = b + gridDim.x;
-    if (bn < nblk) issue(bn, sm + ((k + 1) & 1) * st.size, a0, a1);
+  if (i + (int)gridDim.x < nblk) load_ids(bid(i + gridDim.x), a0, a1);
+  for (int k = 0; i < nblk; ++k, i += gridDim.x) {
+    const int b = bid(i);
+    const int in = i + gridDim.x;
+    if (in < nblk) issue(bid(in), sm + ((k + 1) & 1) * st.size, a0, a1);
     cp_async_commit();
-    if (bn + (int)gridDim.x < nblk) load_ids(bn + gridDim.x, a0, a1);
+    if (in + (int)gridDim.x < nblk) load_ids(bid(in + gridDim.x), a0, a1);
     cp_async_wait_prev();
     __syncthreads();
     const double* S = sm + (k & 1) * st.size;
@@ -446,9 +449,10 @@ __global__ void __launch_bounds__(THREADS, MINB)
                                                     const double* __restrict__ G, const int* __restrict__ lptr,
                                                     const int* __restrict__ lidx, const int* __restrict__ xslot,
                                                     double* __restrict__ part, double* __restrict__ spill,
-                                                    int* __restrict__ tag, int* __restrict__ counters) {
+                                                    int* __restrict__ tag, int* __restrict__ counters,
+                                                    const int* __restrict__ blist) {
   extern __shared__ double sm[];
-  const int blk = blockIdx.x;
+  const int blk = blist ? blist[blockIdx.x] : blockIdx.x;
   const int n0 = blk * NB;
   const int nn = min(NB, N - n0);
   const int h0 = hfptr[blk], nh = hfptr[blk + 1] - h0;
@@ -572,12 +576,25 @@ __global__ void __launch_bounds__(THREADS, MINB)
 // node's boundary subface fluxes (face order), times 1/ctrlVol; written to
 // R in the caller's numbering through n2o.  Partial sums, spills and
 // subface fluxes are read in node order (coalesced); the caller-order
-// variant that gathers them through o2n measured slower.
-__global__ void k_fv_nodes_b(int N, const int* __restrict__ n2o, const double* __restrict__ part,
+// variant that gathers them through o2n measured slower.  FACES: the
+// subface fluxes are evaluated here from the node's own state (the
+// operations of k_face_flux: normal n_f / 3, face_flux), instead of being
+// read from fbuf.
+template <bool FACES>
+__global__ void k_fv_nodes_b(int N, Gas g, const int* __restrict__ n2o, const double* __restrict__ part,
                              const int* __restrict__ xin_ptr, const double* __restrict__ spill,
                              const int* __restrict__ bnf_ptr, const int* __restrict__ bnf_ent,
-                             const double* __restrict__ fbuf, const double* __restrict__ vol2, double* __restrict__ R) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+                             const double* __restrict__ fbuf, int F, const double* __restrict__ Ub0,
+                             const int* __restrict__ fcode, const double* __restrict__ fn,
+                             const double* __restrict__ P2, const double* __restrict__ vol2, double* __restrict__ R,
+                             const int* __restrict__ blist, int nlist, int NB) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (blist) {
+    // the nodes of blocks blist[0, nlist)
+    const int i = n / NB;
+    if (i >= nlist) return;
+    n = blist[i] * NB + n % NB;
+  }
   if (n >= N) return;
   double acc[5];
 #pragma unroll
@@ -587,10 +604,27 @@ __global__ void k_fv_nodes_b(int N, const int* __restrict__ n2o, const double* _
 #pragma unroll
     for (int c = 0; c < 5; ++c) acc[c] -= sp[c];
   }
-  for (int q = bnf_ptr[n]; q < bnf_ptr[n + 1]; ++q) {
-    const double* ff = fbuf + 5 * (size_t)bnf_ent[q];
+  const int q0 = bnf_ptr[n], q1 = bnf_ptr[n + 1];
+  if (FACES) {
+    if (q0 < q1) {
+      const double third = 1.0 / 3.0;
+      double V[5], Ub[5];
 #pragma unroll
-    for (int c = 0; c < 5; ++c) acc[c] += ff[c];
+      for (int k = 0; k < 5; ++k) { V[k] = P2[8 * (size_t)n + k]; Ub[k] = Ub0[k]; }
+      for (int q = q0; q < q1; ++q) {
+        const int f = bnf_ent[q] / 3;
+        double ff[5];
+        face_flux(g, fcode[f], third * fn[f], third * fn[(size_t)F + f], third * fn[2 * (size_t)F + f], V, Ub, ff);
+#pragma unroll
+        for (int c = 0; c < 5; ++c) acc[c] += ff[c];
+      }
+    }
+  } else {
+    for (int q = q0; q < q1; ++q) {
+      const double* ff = fbuf + 5 * (size_t)bnf_ent[q];
+#pragma unroll
+      for (int c = 0; c < 5; ++c) acc[c] += ff[c];
+    }
   }
   const double invcv = 1.0 / vol2[n];
   const size_t o = (size_t)n2o[n];
@@ -612,12 +646,35 @@ __global__ void k_prim_blocked(int N, Gas g, const int* __restrict__ n2o, const 
   for (int k = 0; k < 5; ++k) P2[8 * (size_t)n + k] = v[k];
 }
 
+// k_prim_blocked for the nodes of blocks blist[0, nlist) only.
+__global__ void k_prim_blocks(int N, int NB, const int* __restrict__ blist, int nlist, Gas g,
+                              const int* __restrict__ n2o, const double* __restrict__ U, double* __restrict__ P2) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / NB;
+  if (i >= nlist) return;
+  const int n = blist[i] * NB + t % NB;
+  if (n >= N) return;
+  const int o = n2o[n];
+  double u[5], v[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) u[k] = U[5 * (size_t)o + k];
+  cons2prim(g, u, v);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) P2[8 * (size_t)n + k] = v[k];
+}
+
 // Boundary fluxes, one thread per face, the three subface fluxes with
 // normal n_f/3 (FaceTriaCore.C:288-308) into fbuf[3F][5].
 __global__ void k_face_flux(int F, Gas g, const double* __restrict__ Ub0, const int* __restrict__ faces,
                             const int* __restrict__ fcode, const double* __restrict__ fn,
-                            const double* __restrict__ P, const int* __restrict__ o2n, double* __restrict__ fbuf) {
+                            const double* __restrict__ P, const int* __restrict__ o2n, double* __restrict__ fbuf,
+                            const int* __restrict__ flist = nullptr, int nlist = 0) {
   int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (flist) {
+    // faces flist[0, nlist)
+    if (f >= nlist) return;
+    f = flist[f];
+  }
   if (f >= F) return;
   const double third = 1.0 / 3.0;
   double Ub[5];
@@ -870,7 +927,7 @@ static void launch_grad_pipe(aerof_gpu_ctx* c, const Gas& g, const double* dU, c
     AEROF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
     const int grid = std::max(1, std::min(m.nblk, std::max(per_sm, 1) * sms));
     kern<<<grid, kBlock, smem, s>>>(m.N, m.NB, m.nblk, m.maxH, m.maxLp, st, P2src, m.W2.p, m.nb2_ptr.p, m.lpad.p,
-                                    m.hpad.p, tag, G2);
+                                    m.hpad.p, tag, G2, nullptr);
     AEROF_LAUNCH_CHECK();
   };
   if (L == 4) go(k_grad_pipe<4>);
@@ -990,12 +1047,12 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
   }
   auto fv = [&](int fs, int* counter) {
     fvk<<<m.nblk, fv_threads, smem, s>>>(m.N, m.E, m.NB, g, rec, c->cfg.beta, fs, m.bl.p, m.bnorm.p, m.beptr.p,
-                                            m.hfptr.p, m.hfpad.p, m.maxHf, m.P2.p, c->s.G2.p, m.lptr.p, m.lidx.p,
-                                            m.xslot.p, c->s.part.p, c->s.spill.p, c->s.tag.p, counter);
+                                         m.hfptr.p, m.hfpad.p, m.maxHf, m.P2.p, c->s.G2.p, m.lptr.p, m.lidx.p,
+                                         m.xslot.p, c->s.part.p, c->s.spill.p, c->s.tag.p, counter, nullptr);
     AEROF_LAUNCH_CHECK();
   };
   {
-    TimerScope t(c, AEROF_T_FV_TERM);
+    TimerScope t(c, AEROF_T_FV_EDGES);
     fv(c->cfg.failsafe, ecnt);
   }
   int bad = 0;
@@ -1012,13 +1069,26 @@ static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, 
   }
   {
     TimerScope t(c, AEROF_T_FV_TERM);
-    if (m.F) {
-      k_face_flux<<<grid_for(m.F, kBlock), kBlock, 0, s>>>(m.F, g, m.Ubd.p, m.faces.p, m.fcode.p, m.fnrm.p, m.P2.p,
-                                                           m.o2n.p, c->s.fbuf.p);
-      AEROF_LAUNCH_CHECK();
+    // boundary fluxes in their own kernel (thread per face) or inside the
+    // node assembly (tuning knob AEROF_FACES_IN_NODES=1)
+    static const bool faces_in_nodes = [] {
+      const char* e = std::getenv("AEROF_FACES_IN_NODES");
+      return e && std::atoi(e) == 1;
+    }();
+    if (faces_in_nodes) {
+      k_fv_nodes_b<true><<<grid_for(m.N, kBlock), kBlock, 0, s>>>(
+          m.N, g, m.n2o.p, c->s.part.p, m.xin_ptr.p, c->s.spill.p, m.bnf_ptr.p, m.bnf_ent.p, nullptr, m.F, m.Ubd.p,
+          m.fcode.p, m.fnrm.p, m.P2.p, m.vol2.p, dR, nullptr, 0, m.NB);
+    } else {
+      if (m.F) {
+        k_face_flux<<<grid_for(m.F, kBlock), kBlock, 0, s>>>(m.F, g, m.Ubd.p, m.faces.p, m.fcode.p, m.fnrm.p,
+                                                             m.P2.p, m.o2n.p, c->s.fbuf.p);
+        AEROF_LAUNCH_CHECK();
+      }
+      k_fv_nodes_b<false><<<grid_for(m.N, kBlock), kBlock, 0, s>>>(
+          m.N, g, m.n2o.p, c->s.part.p, m.xin_ptr.p, c->s.spill.p, m.bnf_ptr.p, m.bnf_ent.p, c->s.fbuf.p, m.F,
+          m.Ubd.p, m.fcode.p, m.fnrm.p, m.P2.p, m.vol2.p, dR, nullptr, 0, m.NB);
     }
-    k_fv_nodes_b<<<grid_for(m.N, kBlock), kBlock, 0, s>>>(m.N, m.n2o.p, c->s.part.p, m.xin_ptr.p, c->s.spill.p,
-                                                          m.bnf_ptr.p, m.bnf_ent.p, c->s.fbuf.p, m.vol2.p, dR);
     AEROF_LAUNCH_CHECK();
     galerkin_add(c, dU, dR);
   }
@@ -1085,6 +1155,191 @@ int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
   return bad;
 }
 
+// ------------------------------------------------------------------
+// Residual of HOST arrays with the copies overlapped with the computation.
+// U arrives in K chunks of caller rows on a copy stream; for every chunk s
+// that has arrived the compute stream runs the stages -- primitive
+// conversion, gradients, edge fluxes, boundary fluxes, node assembly -- of
+// the blocks and boundary faces whose dependencies (DeviceMesh::h_prow ..
+// h_nrow, h_face_prow) lie in chunks 0..s (a face's nodes are neighbours
+// of the node it is assembled into, so its fluxes are ready by that node's
+// stage), and a second copy stream takes every chunk
+// of R out as soon as the stage that completes it is done, while later
+// stages and copies still run.  The kernels and the arithmetic per block
+// are those of residual_blocked_dev (bitwise the same residual).  Used for
+// page-locked host U and R with the blocked kernel, the pipelined gradient
+// kernel, failsafe off, no viscous term and timers off, on meshes of at
+// least kPipeMinNodes nodes; otherwise aerof_gpu_residual stages the
+// arrays around one residual_dev.
+constexpr int kPipeChunks = 8;
+constexpr int kPipeMinNodes = 1 << 17;
+
+static bool pinned_host(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// first caller row of chunk k of K (rows o with floor(o K / N) == k)
+static size_t pipe_row0(size_t N, int K, int k) { return ((size_t)k * N + K - 1) / K; }
+
+static ResidualPipe& pipe_for(aerof_gpu_ctx* c) {
+  if (c->pipe) return *c->pipe;
+  const DeviceMesh& m = c->mesh;
+  auto p = std::make_unique<ResidualPipe>();
+  const int K = kPipeChunks;
+  p->K = K;
+  AEROF_CUDA(cudaStreamCreateWithFlags(&p->sin, cudaStreamNonBlocking));
+  AEROF_CUDA(cudaStreamCreateWithFlags(&p->sout, cudaStreamNonBlocking));
+  p->ev_in.assign(K, nullptr);
+  p->ev_stage.assign(K, nullptr);
+  for (auto& e : p->ev_in) AEROF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (auto& e : p->ev_stage) AEROF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  AEROF_CUDA(cudaEventCreateWithFlags(&p->ev_go, cudaEventDisableTiming));
+  AEROF_CUDA(cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming));
+  const long long N = m.N;
+  auto chunk = [&](int row) { return (int)((long long)row * K / N); };
+  // kinds 0-3: blocks whose conversion / gradients / edge fluxes / node
+  // assembly a stage runs; kind 4: the boundary faces whose fluxes it runs
+  const std::vector<int>* rows[5] = {&m.h_prow, &m.h_grow, &m.h_frow, &m.h_nrow, &m.h_face_prow};
+  std::vector<int> lists;
+  p->off.assign(5 * (K + 1), 0);
+  for (int kind = 0; kind < 5; ++kind) {
+    const std::vector<int>& r = *rows[kind];
+    for (int st = 0; st < K; ++st) {
+      p->off[kind * (K + 1) + st] = (int)lists.size();
+      for (int b = 0; b < (int)r.size(); ++b)
+        if (chunk(r[b]) == st) lists.push_back(b);
+    }
+    p->off[kind * (K + 1) + K] = (int)lists.size();
+  }
+  if (lists.empty()) lists.push_back(0);
+  p->out_stage.assign(K, 0);
+  for (int o = 0; o < m.N; ++o) {
+    const int cs = chunk(o);
+    p->out_stage[cs] = std::max(p->out_stage[cs], chunk(m.h_nrow[m.h_o2n[o] / m.NB]));
+  }
+  p->lists.upload(lists.data(), lists.size(), c->stream);
+  AEROF_CUDA(cudaStreamSynchronize(c->stream));
+  c->pipe = std::move(p);
+  return *c->pipe;
+}
+
+// false: not applicable (the caller takes the staged path)
+static bool residual_host_pipelined(aerof_gpu_ctx* c, const double* U, double* R, int& bad) {
+  DeviceMesh& m = c->mesh;
+  const int rec = c->cfg.reconstruction;
+  const bool grad = rec != AEROF_REC_CONSTANT;
+  if (m.N < kPipeMinNodes || c->cfg.failsafe || c->visc.model != 0 || c->timers.on) return false;
+  if (c->cfg.residual_kernel != AEROF_KERNEL_BLOCKED || fv_blocked_smem(m) > 200 * 1024) return false;
+  if (grad && grad_kernel_choice() != 3) return false;
+  if (grad && !(m.maxH <= 512 && 2 * grad_stage(m).size * sizeof(double) <= kMaxStagedSmem)) return false;
+  if (!pinned_host(U) || !pinned_host(R)) return false;
+  ResidualPipe& p = pipe_for(c);
+  const int K = p.K;
+  const Gas g = make_gas(c->cfg.gamma);
+  cudaStream_t s = c->stream;
+  const size_t n5 = 5 * (size_t)m.N;
+  c->s.Ustage.ensure(n5);
+  c->s.Rstage.ensure(n5);
+  c->s.G2.ensure(16 * (size_t)m.N);
+  c->s.part.ensure(5 * (size_t)m.N);
+  c->s.spill.ensure(5 * (size_t)std::max(m.nX, 1));
+  c->s.fbuf.ensure(15 * (size_t)std::max(m.F, 1));
+  int* cnt = counters(c);
+  double* dU = c->s.Ustage.p;
+  double* dR = c->s.Rstage.p;
+  // kernels and launch shapes of residual_blocked_dev
+  const size_t fsmem = fv_blocked_smem(m);
+  const int by_smem = (int)std::min<size_t>(4, (228 * 1024) / (fsmem + 1024));
+  auto fvk = by_smem >= 4 ? k_fv_blocked<256, 4> : by_smem == 3 ? k_fv_blocked<256, 3> : k_fv_blocked<256, 2>;
+  AEROF_CUDA(cudaFuncSetAttribute(fvk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem));
+  const GradStage gst = grad_stage(m);
+  const size_t gsmem = (size_t)2 * gst.size * sizeof(double);
+  const int L = kBlock / m.NB;
+  auto gk = L == 4 ? k_grad_pipe<4> : L == 2 ? k_grad_pipe<2> : k_grad_pipe<1>;
+  int ggrid = 1;
+  if (grad) {
+    AEROF_CUDA(cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem));
+    int per_sm = 0, sms = 0;
+    AEROF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gk, kBlock, gsmem));
+    AEROF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
+    ggrid = std::max(per_sm, 1) * sms;
+  }
+  AEROF_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * 2, s));
+  // the copy streams start after the work already queued on s (which may
+  // still read Ustage or write Rstage)
+  AEROF_CUDA(cudaEventRecord(p.ev_go, s));
+  AEROF_CUDA(cudaStreamWaitEvent(p.sin, p.ev_go, 0));
+  AEROF_CUDA(cudaStreamWaitEvent(p.sout, p.ev_go, 0));
+  for (int k = 0; k < K; ++k) {
+    const size_t r0 = pipe_row0(m.N, K, k), r1 = pipe_row0(m.N, K, k + 1);
+    if (r1 > r0)
+      AEROF_CUDA(cudaMemcpyAsync(dU + 5 * r0, U + 5 * r0, 5 * (r1 - r0) * sizeof(double), cudaMemcpyHostToDevice,
+                                 p.sin));
+    AEROF_CUDA(cudaEventRecord(p.ev_in[k], p.sin));
+  }
+  const int* lists = p.lists.p;
+  for (int st = 0; st < K; ++st) {
+    AEROF_CUDA(cudaStreamWaitEvent(s, p.ev_in[st], 0));
+    auto seg = [&](int kind, int& cntb) {
+      const int a = p.off[kind * (K + 1) + st];
+      cntb = p.off[kind * (K + 1) + st + 1] - a;
+      return lists + a;
+    };
+    int nb = 0;
+    const int* lp = seg(0, nb);
+    if (nb) {
+      k_prim_blocks<<<grid_for((size_t)nb * m.NB, kBlock), kBlock, 0, s>>>(m.N, m.NB, lp, nb, g, m.n2o.p, dU, m.P2.p);
+      AEROF_LAUNCH_CHECK();
+    }
+    lp = seg(1, nb);
+    if (nb && grad) {
+      gk<<<std::min(nb, ggrid), kBlock, gsmem, s>>>(m.N, m.NB, nb, m.maxH, m.maxLp, gst, m.P2.p, m.W2.p, m.nb2_ptr.p,
+                                                     m.lpad.p, m.hpad.p, nullptr, c->s.G2.p, lp);
+      AEROF_LAUNCH_CHECK();
+    }
+    lp = seg(2, nb);
+    if (nb) {
+      fvk<<<nb, 256, fsmem, s>>>(m.N, m.E, m.NB, g, rec, c->cfg.beta, 0, m.bl.p, m.bnorm.p, m.beptr.p, m.hfptr.p,
+                                 m.hfpad.p, m.maxHf, m.P2.p, c->s.G2.p, m.lptr.p, m.lidx.p, m.xslot.p, c->s.part.p,
+                                 c->s.spill.p, c->s.tag.p, cnt, lp);
+      AEROF_LAUNCH_CHECK();
+    }
+    lp = seg(4, nb);
+    if (nb) {
+      k_face_flux<<<grid_for(nb, kBlock), kBlock, 0, s>>>(m.F, g, m.Ubd.p, m.faces.p, m.fcode.p, m.fnrm.p, m.P2.p,
+                                                          m.o2n.p, c->s.fbuf.p, lp, nb);
+      AEROF_LAUNCH_CHECK();
+    }
+    lp = seg(3, nb);
+    if (nb) {
+      k_fv_nodes_b<false><<<grid_for((size_t)nb * m.NB, kBlock), kBlock, 0, s>>>(
+          m.N, g, m.n2o.p, c->s.part.p, m.xin_ptr.p, c->s.spill.p, m.bnf_ptr.p, m.bnf_ent.p, c->s.fbuf.p, m.F,
+          m.Ubd.p, m.fcode.p, m.fnrm.p, m.P2.p, m.vol2.p, dR, lp, nb, m.NB);
+      AEROF_LAUNCH_CHECK();
+    }
+    AEROF_CUDA(cudaEventRecord(p.ev_stage[st], s));
+    for (int k = 0; k < K; ++k) {
+      if (p.out_stage[k] != st) continue;
+      const size_t r0 = pipe_row0(m.N, K, k), r1 = pipe_row0(m.N, K, k + 1);
+      AEROF_CUDA(cudaStreamWaitEvent(p.sout, p.ev_stage[st], 0));
+      if (r1 > r0)
+        AEROF_CUDA(cudaMemcpyAsync(R + 5 * r0, dR + 5 * r0, 5 * (r1 - r0) * sizeof(double), cudaMemcpyDeviceToHost,
+                                   p.sout));
+    }
+  }
+  AEROF_CUDA(cudaEventRecord(p.ev_out, p.sout));
+  AEROF_CUDA(cudaStreamWaitEvent(s, p.ev_out, 0));
+  AEROF_CUDA(cudaMemcpyAsync(&bad, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
+  AEROF_CUDA(cudaStreamSynchronize(s));
+  c->s.p2g2_valid = true;
+  return true;
+}
+
 void timestep_dev(aerof_gpu_ctx* c, const double* dU, double cfl, double* ddt) {
   DeviceMesh& m = c->mesh;
   TimerScope t(c, AEROF_T_TIME_STEP);
@@ -1127,9 +1382,11 @@ extern "C" int aerof_gpu_residual(aerof_gpu_ctx* c, const double* U, double* R) 
     if (int e = need_mesh(c)) return e;
     if (!U || !R) return AEROF_EINVAL;
     const size_t n5 = 5 * (size_t)c->mesh.N;
+    int bad = 0;
+    if (residual_host_pipelined(c, U, R, bad)) return bad;
     const double* dU = in_dev(c, U, n5, c->s.Ustage);
     double* dR = out_dev(c, R, n5, c->s.Rstage);
-    int bad = residual_dev(c, dU, dR);
+    bad = residual_dev(c, dU, dR);
     out_finish(c, R, dR, n5);
     return bad;
   });

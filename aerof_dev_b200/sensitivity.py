@@ -112,7 +112,8 @@ def adjoint_gradient(ctx, U, X, functional: ZForce, modes, eps=1e-10, krylov=30,
                      stored_operator=False):
     """dJ/ds_k for every mode by the adjoint method.  stored_operator: the
     adjoint solve applies the stored exact linearisation (evaluated once)
-    instead of re-evaluating it per product."""
+    instead of re-evaluating it per product.  The info dict also holds the
+    adjoint state lambda ([N][5], host)."""
     import aerof_dev_b200 as A
     S = A.Sensitivity(ctx)
     U = _host(U)
@@ -125,7 +126,7 @@ def adjoint_gradient(ctx, U, X, functional: ZForce, modes, eps=1e-10, krylov=30,
         if stored_operator:
             S.h2_release()
     gX = functional.dX(U, X) - S.dRdX_T(U, lam)
-    return np.einsum("kni,ni->k", modes, gX), {"adjoint_its": its, "adjoint_res": res}
+    return np.einsum("kni,ni->k", modes, gX), {"adjoint_its": its, "adjoint_res": res, "lambda": _host(lam)}
 
 
 def direct_gradient(ctx, U, X, functional: ZForce, modes, eps=1e-10, krylov=30, maxits=2000, inner_its=20):

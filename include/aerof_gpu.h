@@ -302,12 +302,15 @@ int aerof_gpu_newton(aerof_gpu_ctx* ctx, double* U, const aerof_newton_params* p
  * addPrecSetupTime, addKspTime) measured with CUDA events on the context's
  * stream while profiling is enabled.                                        */
 #define AEROF_T_NODAL_GRAD 0    /* conservative->primitive + LSQ gradients   */
-#define AEROF_T_FV_TERM 1       /* edge fluxes + boundary fluxes + assembly  */
+#define AEROF_T_FV_TERM 1       /* boundary fluxes + node assembly; edge
+                                   fluxes too outside the blocked kernel    */
 #define AEROF_T_TIME_STEP 2
 #define AEROF_T_FV_JAC 3
 #define AEROF_T_PREC_SETUP 4
 #define AEROF_T_KSP_MATVEC 5
 #define AEROF_T_KSP_OTHER 6     /* orthogonalisation, preconditioner apply   */
+#define AEROF_T_FV_EDGES 7      /* edge fluxes of the blocked residual kernel
+                                   (with AEROF_T_FV_TERM: the whole term)   */
 #define AEROF_T_COUNT 8
 int aerof_gpu_profile(aerof_gpu_ctx* ctx, int enable);
 /* Waits for the stream, then returns per category the summed device time

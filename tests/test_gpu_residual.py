@@ -200,3 +200,30 @@ def test_launch_count(gpu_lib, case):
     sp.computeResidual(U)
     n = gpu_lib.launch_count()
     assert 3 <= n <= 6
+
+
+@pytest.mark.parametrize("rec", [1, 2])
+def test_host_array_residual_overlapped_copies(gpu_lib, oracle_mod, rec):
+    # page-locked host U and R on a mesh large enough for the overlapped
+    # copies (chunks of U in, stages of blocks computed as their rows
+    # arrive, chunks of R out): the same residual, bit for bit, as the
+    # device-array call, and the oracle's to 1e-12; twice in a row, so the
+    # second call reuses the schedule
+    import torch
+    m = W.make_lattice_mesh(51, jitter=0.2, codes="channel")
+    Ub = W.freestream(0.8)
+    ctx = ctx_for(gpu_lib, m, Ub, rec=rec)
+    assert ctx.N >= 1 << 17
+    sp = gpu_lib.SpaceOperator(ctx)
+    U = W.perturbed_state(ctx.N, 0.8)
+    Ud = torch.from_numpy(U).cuda()
+    Rd, bad_d = sp.computeResidual(Ud)
+    Uh = torch.from_numpy(U).pin_memory()
+    for _ in range(2):
+        Rh = torch.full_like(Uh, float("nan")).pin_memory()
+        _, bad_h = sp.computeResidual(Uh, Rh)
+        assert bad_h == bad_d == 0
+        assert torch.equal(Rh, Rd.cpu())
+    o = oracle_mod.Oracle(m)
+    Rr, _ = o.residual(U, Ub, rec)
+    assert rel_l2(Rh.numpy(), Rr) < TOL

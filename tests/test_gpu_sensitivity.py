@@ -69,3 +69,30 @@ def test_batched_direct_equals_adjoint(flow):
     assert np.abs(ga - gb).max() <= 1e-8 * np.abs(ga).max()
     gs, _ = S.adjoint_gradient(ctx, U, m["X"], F, modes, stored_operator=True)
     assert np.abs(ga - gs).max() <= 1e-8 * np.abs(ga).max()
+
+
+def test_adjoint_matches_oracle_dual_numbers(flow):
+    # every mode's adjoint gradient against the oracle's exact directional
+    # derivatives: the oracle forms dR/dU column by column from its
+    # dual-number J v (FP64, CPU), solves the adjoint system densely, and
+    # takes dJ/ds_k = dJ/dX . Xdot_k - lambda . (dR/dX . Xdot_k) with its
+    # dual-number dR/dX, so no GPU product enters the reference value
+    from aerof_dev_b200 import sensitivity as S
+    from oracle.oracle import Oracle, zfaces_of
+    ctx, m, U, info, F, modes = flow
+    rec = ctx.cfg.reconstruction
+    U = S._host(U)
+    Ub = W.freestream(0.8)
+    o = Oracle(m)
+    n = 5 * o.N
+    Jd = np.empty((n, n))
+    e = np.zeros((o.N, 5))
+    for c in range(n):
+        e.flat[c] = 1.0
+        Jd[:, c] = o.jvp(U, Ub, e, order=rec).reshape(-1)
+        e.flat[c] = 0.0
+    zf = zfaces_of(m)
+    lam = np.linalg.solve(Jd.T, o.zforce_dU(U, zf).reshape(-1))
+    g_or = np.array([o.zforce_dX(U, zf, Xd) - lam @ o.dRdX(U, Ub, Xd, order=rec)[0].reshape(-1) for Xd in modes])
+    ga, _ = S.adjoint_gradient(ctx, U, m["X"], F, modes)
+    assert np.abs(ga - g_or).max() <= 1e-8 * np.abs(g_or).max()

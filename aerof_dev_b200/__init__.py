@@ -54,6 +54,7 @@ EXPORTS = [
     "aerof_gpu_h2_evaluate", "aerof_gpu_h2_apply", "aerof_gpu_h2_release", "aerof_gpu_set_exact_operator",
     "aerof_gpu_linearized_solve_batch", "aerof_gpu_set_preconditioner", "aerof_gpu_set_jacobian",
     "aerof_gpu_matvec_fd", "aerof_gpu_set_owned_rows", "aerof_gpu_set_viscosity",
+    "aerof_gpu_set_turbulence", "aerof_gpu_residual_sa",
     "aerof_sower_open", "aerof_sower_close", "aerof_sower_num_subdomains", "aerof_sower_subdomain_sizes",
     "aerof_sower_read_subdomain", "aerof_sower_last_error",
 ]
@@ -83,6 +84,18 @@ class ViscousParams(C.Structure):
     _fields_ = [("model", C.c_int), ("reynolds_mu", C.c_double), ("prandtl", C.c_double),
                 ("bulk_viscosity", C.c_double), ("sutherland_alpha", C.c_double), ("sutherland_Ts", C.c_double),
                 ("reserved", C.c_int * 4)]
+
+
+class SAParams(C.Structure):
+    _fields_ = [("cb1", C.c_double), ("cb2", C.c_double), ("cw2", C.c_double), ("cw3", C.c_double),
+                ("cv1", C.c_double), ("cv2", C.c_double), ("sigma", C.c_double), ("vkcst", C.c_double),
+                ("prandtl_turbulent", C.c_double), ("fv3", C.c_int), ("reserved", C.c_int * 3)]
+
+
+# Spalart-Allmaras constants: SAModelData's and TurbulenceClosureData's
+# defaults (IoDataCore.C:1411-1418, 1839)
+SA_DEFAULTS = dict(cb1=0.1355, cb2=0.622, cw2=0.3, cw3=2.0, cv1=7.1, cv2=5.0, sigma=2.0 / 3.0, vkcst=0.41,
+                   prandtl_turbulent=0.9, fv3=0)
 
 
 class NewtonResult(C.Structure):
@@ -148,6 +161,8 @@ def library(path: str | None = None):
             "aerof_gpu_matvec_fd": [vp, dp, dp, dp, dp, C.c_int, dp, C.POINTER(C.c_double)],
             "aerof_gpu_set_owned_rows": [vp, C.c_int],
             "aerof_gpu_set_viscosity": [vp, C.POINTER(ViscousParams)],
+            "aerof_gpu_set_turbulence": [vp, C.POINTER(SAParams), dp, dp],
+            "aerof_gpu_residual_sa": [vp, dp, dp],
         }
         for name, args in sig.items():
             if hasattr(L, name):
@@ -316,6 +331,20 @@ class Context:
         p = ViscousParams(model, reynolds_mu, prandtl, bulk_viscosity, sutherland_alpha, sutherland_Ts)
         self._check(self.L.aerof_gpu_set_viscosity(self.h, C.byref(p)))
 
+    def set_turbulence(self, d2wall, Ub, **constants):
+        """Spalart-Allmaras model on (wall distances d2wall [N], conservative
+        free stream Ub [6] with rho nu~ last, constants overriding
+        SA_DEFAULTS); d2wall None turns it off."""
+        if d2wall is None:
+            self._check(self.L.aerof_gpu_set_turbulence(self.h, None, None, None))
+            return
+        c = dict(SA_DEFAULTS, **constants)
+        p = SAParams(c["cb1"], c["cb2"], c["cw2"], c["cw3"], c["cv1"], c["cv2"], c["sigma"], c["vkcst"],
+                     c["prandtl_turbulent"], int(c["fv3"]))
+        d = _Arg(d2wall, np.float64, (self.N,))
+        ub = _Arg(np.asarray(Ub, dtype=np.float64), np.float64, (6,))
+        self._check(self.L.aerof_gpu_set_turbulence(self.h, C.byref(p), d.ptr, ub.ptr))
+
     def status(self) -> int:
         """Wait for the stream; unphysical count of async calls since last status."""
         return self._check(self.L.aerof_gpu_status(self.h))
@@ -368,6 +397,16 @@ class SpaceOperator:
         R = _like(U, (ctx.N, 5)) if R is None else R
         r = _Arg(R, np.float64, (ctx.N, 5), writable=True)
         bad = ctx._check(ctx.L.aerof_gpu_residual(ctx.h, u.ptr, r.ptr))
+        return r.obj, bad
+
+    def computeResidualSA(self, U, R=None):
+        """Spalart-Allmaras residual of U [N][6] (after Context.set_turbulence).
+        Returns (R, n_unphysical)."""
+        ctx = self.ctx
+        u = _Arg(U, np.float64, (ctx.N, 6))
+        R = _like(U, (ctx.N, 6)) if R is None else R
+        r = _Arg(R, np.float64, (ctx.N, 6), writable=True)
+        bad = ctx._check(ctx.L.aerof_gpu_residual_sa(ctx.h, u.ptr, r.ptr))
         return r.obj, bad
 
     def computeResidualAsync(self, U, R):

@@ -303,6 +303,21 @@ struct AdjWork {
 // q2 dddji.  Per boundary row, SoA [25][nbrow]: the summed face-flux
 // Jacobian d F / d V of its faces.
 constexpr int kH2Rec = 70;
+// Spalart-Allmaras model (turbulence.cu): constants, wall distances and
+// the work arrays of its six-component residual
+struct TurbWork {
+  bool on = false;
+  aerof_sa_params p = {};
+  double Ub[6] = {0, 0, 0, 0, 0, 0};
+  DBuf<double> Ubd;        // [6]
+  DBuf<double> d2wall;     // [N]
+  DBuf<double> V6;         // [N][6] primitive
+  DBuf<double> G6;         // [N][18] LSQ gradients (x, y, z of the six components)
+  DBuf<double> flux6;      // [6][E]
+  DBuf<double> fbuf6;      // [3F][6]
+  DBuf<double> Ustage, Rstage;
+};
+
 struct H2Op {
   bool ready = false;      // evaluated for the current mesh and coordinates
   bool use = false;        // exact products of linearised solves read it
@@ -346,6 +361,7 @@ struct aerof_gpu_ctx {
   aerof::DualWork dual;
   aerof::AdjWork adj;
   aerof::H2Op h2;
+  aerof::TurbWork turb;
   aerof::Timers timers;
   std::string last_error;
   // device address of the allocation-free residual's fixed scratch array,

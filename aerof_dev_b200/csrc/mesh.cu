@@ -471,6 +471,7 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
     if (int e = check_coordinates(c, N, X)) return e;
     c->has_mesh = false;
     c->pipe.reset();
+    c->turb.on = false;
     c->imp.precision = 0;
     c->imp.prec_ready = false;
     c->imp.ilu_ready = false;

@@ -226,6 +226,38 @@ typedef struct aerof_viscous_params {
 } aerof_viscous_params;
 int aerof_gpu_set_viscosity(aerof_gpu_ctx* ctx, const aerof_viscous_params* p);
 
+/* ---- Spalart-Allmaras turbulence model ---------------------------------
+ * The one-equation model strongly coupled to the flow, state U = (rho,
+ * rho u, rho v, rho w, E, rho nu~) per node (dim 6; VarFcnSGSA.h:210-224).
+ * Finite-volume term: the second-order edge loop on six components with
+ * the Roe flux's advected sixth component (FluxFcnSGApprJacRoeSA3D::compute,
+ * FluxFcnDescSG.C:1886-1901 -> roeflux7.f type 1), slip walls
+ * (FluxFcnSGWallSA3D, FluxFcnDescSG.C:2024-2035) and far field
+ * (FluxFcnSGOutflowSA3D for inlet and outlet, FluxFcn.h:246-262 ->
+ * boundflux5.f type 1).  Galerkin term (with the viscous model of
+ * aerof_gpu_set_viscosity; model 0 leaves it out):
+ * FemEquationTermSA::computeVolumeTerm (FemEquationTermDesc.C:669-787):
+ * eddy viscosity mu_t = mu~ fv1, lambda_t = -2/3 mu_t, kappa_t = cp mu_t /
+ * prandtl_turbulent in the Navier-Stokes stress and heat flux, SA
+ * diffusion and source (production, destruction with the wall distance,
+ * cb2 gradient term) per tet; constants as SATerm::SATerm
+ * (SpalartAllmarasTerm.h:77-112).                                         */
+typedef struct aerof_sa_params {
+  double cb1, cb2, cw2, cw3, cv1, cv2, sigma, vkcst; /* reference defaults
+                             0.1355 0.622 0.3 2.0 7.1 5.0 2/3 0.41        */
+  double prandtl_turbulent;  /* 0.9                                          */
+  int fv3;                   /* 1: the fv3 form (SAModelData::FV3)           */
+  int reserved[3];
+} aerof_sa_params;
+/* Turns the model on: constants, the wall distance of every node d2wall
+ * [N] (caller numbering) and the conservative free stream Ub [6] of the
+ * far-field boundaries (rho nu~ last).  p == NULL turns it off.             */
+int aerof_gpu_set_turbulence(aerof_gpu_ctx* ctx, const aerof_sa_params* p, const double* d2wall,
+                             const double* Ub);
+/* R = residual(U) / ctrlVol for U, R [N][6] (host or device).  Returns the
+ * number of non-positive reconstructed states (>= 0) or an error.          */
+int aerof_gpu_residual_sa(aerof_gpu_ctx* ctx, const double* U, double* R);
+
 /* ---- implicit operator ------------------------------------------------
  * MatVecProdH1<5,MatScalar,5>::evaluate (MatVecProd.C:1074-1160) =
  * SpaceOperator::computeJacobian (SpaceOperator.C:2088-2150) +

@@ -1483,6 +1483,279 @@ int orc_residual_visc(void* h, const double* U, const double* Ub, int order, int
   return bad;
 }
 
+// ---------------------------------------------------------------------------
+// Spalart-Allmaras turbulence model, strongly coupled (state U = (rho, rho
+// u, rho v, rho w, E, rho nu~), dim 6).  The finite-volume term is the
+// Euler path's on six components:
+// * VarFcnSGSA::conservativeToPrimitive (VarFcnSGSA.h:210-224): V[5] =
+//   U[5] / rho;
+// * LSQ gradients and the reconstruction componentwise (the same
+//   SubDomain::computeGradientsLeastSquares and RecFcn functions on dim
+//   6), the positivity check on the reconstructed density and pressure;
+// * the Roe flux FluxFcnSGApprJacRoeSA3D::compute (FluxFcnDescSG.C:
+//   1886-1901) = roeflux7.f with type 1: phi(6) = phi(1) (updir nu~_L +
+//   (1 - updir) nu~_R), updir = 0.5 + sign(0.5, phi(1)) (roeflux7.f:
+//   190-196);
+// * slip walls FluxFcnSGWallSA3D::compute (FluxFcnDescSG.C:2024-2035:
+//   flux[5] = 0); inlet and outlet both FluxFcnSGOutflowSA3D (FluxFcn.h:
+//   246-262) = boundflux5.f with type 1: flux(6) = phiro (updir nu~ + (1 -
+//   updir) (rho nu~)_b / rho_b), phiro = flux(1) (boundflux5.f:92-103).
+// The Galerkin term is FemEquationTermSA::computeVolumeTerm
+// (FemEquationTermDesc.C:669-787) assembled by ElemTet::computeGalerkinTerm
+// (ElemTet.C:99-114, R += vol (r . dN_j) - vol/4 s): the laminar
+// coefficients at the tet's mean temperature, mu~ = mean(rho nu~),
+// mu_t = mu~ fv1 (SATerm::computeTurbulentViscosity,
+// SpalartAllmarasTerm.h:139-151), lambda_t = -2/3 mu_t, kappa_t = cp mu_t /
+// Pr_t (ConstantPrandtlThermalCondFcn::turbulentConductivity,
+// ThermalCondFcn.h:84-87), the Navier-Stokes stress and heat flux with mu
+// + mu_t, lambda + lambda_t, kappa + kappa_t scaled by 1/Re, the SA
+// diffusion r[j][5] = (mul + |mu~|) / (sigma Re) dnu~/dx_j and the source
+// s[5] = cb2/(sigma Re) rho |grad nu~|^2 + cb1 S~ |mu~| - cw1/Re fw
+// max(mu~,0)^2 / (rho d^2) (production with S~ = max(s fv3 + zz fv2,
+// 1e-12), zz = max(mu~,0) / (Re kappa^2 rho d^2); destruction with r =
+// min(zz / S~, 2), g = r + cw2 (r^6 - r), fw = g ((1 + cw3^6) / (g^6 +
+// cw3^6))^(1/6)), applied when the tet's mean wall distance is >= 1e-15
+// (constants as SATerm::SATerm, SpalartAllmarasTerm.h:77-112).  No trip
+// (its box is empty by default), no porous media, no wall functions.
+struct SAParams {
+  double cb1, cb2, cw2, cw3, cv1, cv2, sigma, vkcst, prandtl_t;
+  int fv3;
+};
+
+// roeflux7 with type 1 (six components)
+static void roeflux7_sa(double gam, const double* n, const double* Vg, const double* Vd, double* phi) {
+  roeflux7<double>(gam, 0.0, n, 0.0, Vg, Vd, phi);
+  const double updir = 0.5 + std::copysign(0.5, phi[0]);
+  phi[5] = phi[0] * (updir * Vg[5] + (1.0 - updir) * Vd[5]);
+}
+
+// the SA boundary fluxes (wall, or boundflux5 with type 1)
+static void face_flux_sa(double gam, int code, const double* n3, const double* V, const double* Ub, double* flux) {
+  face_flux<double>(gam, code, n3, V, Ub, flux);
+  if (code == BC_SLIP_WALL_MOVING) {
+    flux[5] = 0.0;
+  } else {
+    const double phiro = flux[0];
+    const double updir = 0.5 + std::copysign(0.5, phiro);
+    const double usro = 1.0 / Ub[0];
+    flux[5] = phiro * (updir * V[5] + (1.0 - updir) * Ub[5] * usro);
+  }
+}
+
+static void galerkin_term_sa(const Mesh& m, const double* V, const Visc& vp, const SAParams& sa,
+                             const double* d2wall, double* R) {
+  const double gam1 = m.gam - 1.0, invgam1 = 1.0 / gam1, cp = m.gam * invgam1;
+  const double fourth = 0.25, twothird = 2.0 / 3.0, sixth_ = 1.0 / 6.0;
+  const double oorey = vp.ooreynolds;
+  const double oovkcst2 = 1.0 / (sa.vkcst * sa.vkcst);
+  const double cw3_pow6 = std::pow(sa.cw3, 6.0);
+  const double opcw3_pow = std::pow(1.0 + cw3_pow6, 1.0 / 6.0);
+  const double cv1_pow3 = sa.cv1 * sa.cv1 * sa.cv1;
+  const double oocv2 = 1.0 / sa.cv2;
+  const double oosigma = 1.0 / sa.sigma * oorey;
+  const double cw1 = (sa.cb1 * oovkcst2 + (1.0 + sa.cb2) / sa.sigma) * oorey;
+  for (int t = 0; t < m.T; ++t) {
+    const int* nd = &m.tets[4 * (size_t)t];
+    double g[4][3];
+    const double vol = p1_gradients(m.X.data(), nd, g);
+    const double* v[4];
+    double u[4][3], T[4];
+    for (int k = 0; k < 4; ++k) {
+      v[k] = V + 6 * (size_t)nd[k];
+      u[k][0] = v[k][1]; u[k][1] = v[k][2]; u[k][2] = v[k][3];
+      T[k] = invgam1 * v[k][4] / v[k][0];
+    }
+    double ucg[3];
+    for (int a = 0; a < 3; ++a) ucg[a] = fourth * (u[0][a] + u[1][a] + u[2][a] + u[3][a]);
+    const double Tcg = fourth * (T[0] + T[1] + T[2] + T[3]);
+    double dudxj[3][3], dTdxj[3];
+    for (int a = 0; a < 3; ++a)
+      for (int j = 0; j < 3; ++j)
+        dudxj[a][j] = g[0][j] * u[0][a] + g[1][j] * u[1][a] + g[2][j] * u[2][a] + g[3][j] * u[3][a];
+    for (int j = 0; j < 3; ++j) dTdxj[j] = g[0][j] * T[0] + g[1][j] * T[1] + g[2][j] * T[2] + g[3][j] * T[3];
+    // laminar coefficients (not yet scaled by 1/Re)
+    double mul, lambdal;
+    if (vp.model == 2) {
+      const double Ta = vp.alpha * Tcg;
+      mul = Ta * std::sqrt(Ta) * (1.0 + vp.Ts) / (Ta + vp.Ts);
+      lambdal = -twothird * mul;
+    } else {
+      mul = 1.0;
+      lambdal = vp.bulk - twothird * mul;
+    }
+    const double kappal = vp.ooprandtl * cp * mul;
+    // turbulent coefficients
+    const double mutilde = 0.25 * (v[0][0] * v[0][5] + v[1][0] * v[1][5] + v[2][0] * v[2][5] + v[3][0] * v[3][5]);
+    const double chi0 = mutilde / mul;
+    const double chi03 = chi0 * chi0 * chi0;
+    const double mut = mutilde * (chi03 / (chi03 + cv1_pow3));
+    const double lambdat = -2.0 * mut / 3.0;
+    const double kappat = cp * mut / sa.prandtl_t;
+    double r[3][6], s5 = 0.0;
+    const double absmutilde = std::fabs(mutilde), maxmutilde = std::max(mutilde, 0.0);
+    const double mu5 = oosigma * (mul + absmutilde);
+    double dnu[3];
+    for (int j = 0; j < 3; ++j) dnu[j] = g[0][j] * v[0][5] + g[1][j] * v[1][5] + g[2][j] * v[2][5] + g[3][j] * v[3][5];
+    for (int j = 0; j < 3; ++j) r[j][5] = mu5 * dnu[j];
+    const double d2w = 0.25 * (d2wall[nd[0]] + d2wall[nd[1]] + d2wall[nd[2]] + d2wall[nd[3]]);
+    if (d2w >= 1.e-15) {
+      const double chi = std::max(mutilde / mul, 0.001);
+      const double chi3 = chi * chi * chi;
+      const double fv1 = chi3 / (chi3 + cv1_pow3);
+      double fv2 = 1. - chi / (1. + chi * fv1);
+      double fv3 = 1.0;
+      if (sa.fv3) {
+        fv2 = 1.0 + oocv2 * chi;
+        fv2 = 1.0 / (fv2 * fv2 * fv2);
+        fv3 = (1.0 + chi * fv1) * (1.0 - fv2) / chi;
+      }
+      const double ood2wall2 = 1.0 / (d2w * d2w);
+      const double rho = 0.25 * (v[0][0] + v[1][0] + v[2][0] + v[3][0]);
+      const double oorho = 1.0 / rho;
+      const double zz = oorey * oovkcst2 * maxmutilde * oorho * ood2wall2;
+      const double s12 = dudxj[0][1] - dudxj[1][0];
+      const double s23 = dudxj[1][2] - dudxj[2][1];
+      const double s31 = dudxj[2][0] - dudxj[0][2];
+      const double sv = std::sqrt(s12 * s12 + s23 * s23 + s31 * s31);
+      const double Stilde = std::max(sv * fv3 + zz * fv2, 1.0e-12);
+      const double rr = std::min(zz / Stilde, 2.0);
+      const double rr2 = rr * rr;
+      const double gg = rr + sa.cw2 * (rr2 * rr2 * rr2 - rr);
+      const double gg2 = gg * gg;
+      const double fw = opcw3_pow * gg * std::pow(gg2 * gg2 * gg2 + cw3_pow6, -sixth_);
+      const double AA = oosigma * sa.cb2 * rho * (dnu[0] * dnu[0] + dnu[1] * dnu[1] + dnu[2] * dnu[2]);
+      const double BB = sa.cb1 * Stilde * absmutilde;
+      const double CC = -cw1 * fw * oorho * maxmutilde * maxmutilde * ood2wall2;
+      s5 = AA + BB + CC;
+    }
+    // NavierStokesTerm::computeVolumeTermNS with the summed coefficients
+    const double mu = oorey * (mul + mut), lambda = oorey * (lambdal + lambdat), kappa = oorey * (kappal + kappat);
+    const double div = dudxj[0][0] + dudxj[1][1] + dudxj[2][2];
+    double tij[3][3];
+    tij[0][0] = lambda * div + 2.0 * mu * dudxj[0][0];
+    tij[1][1] = lambda * div + 2.0 * mu * dudxj[1][1];
+    tij[2][2] = lambda * div + 2.0 * mu * dudxj[2][2];
+    tij[0][1] = mu * (dudxj[1][0] + dudxj[0][1]);
+    tij[0][2] = mu * (dudxj[2][0] + dudxj[0][2]);
+    tij[1][2] = mu * (dudxj[2][1] + dudxj[1][2]);
+    tij[1][0] = tij[0][1];
+    tij[2][0] = tij[0][2];
+    tij[2][1] = tij[1][2];
+    for (int j = 0; j < 3; ++j) {
+      r[j][0] = 0.0;
+      r[j][1] = tij[0][j];
+      r[j][2] = tij[1][j];
+      r[j][3] = tij[2][j];
+      r[j][4] = ucg[0] * tij[0][j] + ucg[1] * tij[1][j] + ucg[2] * tij[2][j] - (-kappa * dTdxj[j]);
+    }
+    for (int j = 0; j < 4; ++j) {
+      double* Rj = R + 6 * (size_t)nd[j];
+      for (int k = 0; k < 6; ++k)
+        Rj[k] += vol * ((r[0][k] * g[j][0] + r[1][k] * g[j][1] + r[2][k] * g[j][2]) - (k == 5 ? fourth * s5 : 0.0));
+    }
+  }
+}
+
+// Spalart-Allmaras residual (R_fv + G) / ctrlVol of U [N][6], evaluated as
+// R_fv / ctrlVol + G / ctrlVol; Ub [6] conservative free stream; sa = (cb1,
+// cb2, cw2, cw3, cv1, cv2, sigma, vkcst, Pr_t); d2wall [N].  Returns the
+// number of non-positive reconstructed states.
+int orc_residual_sa(void* h, const double* U, const double* Ub, int order, int model, double ooreynolds,
+                    double ooprandtl, double bulk, double alpha, double Ts, const double* sa, int fv3,
+                    const double* d2wall, double* R) {
+  Mesh* mp = (Mesh*)h;
+  const Mesh& m = *mp;
+  const int N = m.N;
+  const double gam = m.gam;
+  std::vector<double> V(6 * (size_t)N);
+  for (int i = 0; i < N; ++i) {
+    const double* u = U + 6 * (size_t)i;
+    double* v = &V[6 * (size_t)i];
+    v[0] = u[0];
+    const double invRho = 1.0 / u[0];
+    v[1] = u[1] * invRho;
+    v[2] = u[2] * invRho;
+    v[3] = u[3] * invRho;
+    const double vel2 = v[1] * v[1] + v[2] * v[2] + v[3] * v[3];
+    v[4] = (gam - 1.0) * (u[4] - 0.5 * u[0] * vel2) - gam * 0.0;
+    v[5] = u[5] * invRho;
+  }
+  const double* X = m.X.data();
+  std::vector<double> ddx(6 * (size_t)N, 0.0), ddy(6 * (size_t)N, 0.0), ddz(6 * (size_t)N, 0.0);
+  if (order > 1)
+    for (int l = 0; l < m.E; ++l) {
+      const int i = m.edges[2 * l], j = m.edges[2 * l + 1];
+      double Wi[3], Wj[3];
+      double dx[3] = {X[3 * j] - X[3 * i], X[3 * j + 1] - X[3 * i + 1], X[3 * j + 2] - X[3 * i + 2]};
+      lsq_weights(dx, &m.Rlsq[6 * (size_t)i], Wi);
+      dx[0] = -dx[0]; dx[1] = -dx[1]; dx[2] = -dx[2];
+      lsq_weights(dx, &m.Rlsq[6 * (size_t)j], Wj);
+      for (int k = 0; k < 6; ++k) {
+        const double dv = V[6 * (size_t)j + k] - V[6 * (size_t)i + k];
+        ddx[6 * (size_t)i + k] += Wi[0] * dv;
+        ddy[6 * (size_t)i + k] += Wi[1] * dv;
+        ddz[6 * (size_t)i + k] += Wi[2] * dv;
+        ddx[6 * (size_t)j + k] -= Wj[0] * dv;
+        ddy[6 * (size_t)j + k] -= Wj[1] * dv;
+        ddz[6 * (size_t)j + k] -= Wj[2] * dv;
+      }
+    }
+  RecParams rp = rec_params(order == 1 ? 0.0 : 1.0 / 3.0);
+  std::fill(R, R + 6 * (size_t)N, 0.0);
+  int ierr = 0;
+  for (int l = 0; l < m.E; ++l) {
+    const int i = m.edges[2 * l], j = m.edges[2 * l + 1];
+    const double dx[3] = {X[3 * j] - X[3 * i], X[3 * j + 1] - X[3 * i + 1], X[3 * j + 2] - X[3 * i + 2]};
+    double Vi[6], Vj[6];
+    for (int k = 0; k < 6; ++k) {
+      const double vi = V[6 * (size_t)i + k], vj = V[6 * (size_t)j + k];
+      if (order == 1) { Vi[k] = vi; Vj[k] = vj; continue; }
+      const double ddVij = dx[0] * ddx[6 * (size_t)i + k] + dx[1] * ddy[6 * (size_t)i + k] + dx[2] * ddz[6 * (size_t)i + k];
+      const double ddVji = dx[0] * ddx[6 * (size_t)j + k] + dx[1] * ddy[6 * (size_t)j + k] + dx[2] * ddz[6 * (size_t)j + k];
+      if (order == 2) vanalbada(rp, vi, ddVij, vj, ddVji, Vi[k], Vj[k]);
+      else linear_rec(rp, vi, ddVij, vj, ddVji, Vi[k], Vj[k]);
+    }
+    const bool bi = Vi[0] <= 0.0 || Vi[4] <= 0.0;
+    const bool bj = Vj[0] <= 0.0 || Vj[4] <= 0.0;
+    if (bi || bj) { ierr += (int)bi + (int)bj; continue; }
+    const double* nl = &m.edgeNorm[3 * (size_t)l];
+    if (std::sqrt(nl[0] * nl[0] + nl[1] * nl[1] + nl[2] * nl[2]) < 1e-18) continue;
+    double flux[6];
+    roeflux7_sa(gam, nl, Vi, Vj, flux);
+    for (int k = 0; k < 6; ++k) { R[6 * (size_t)i + k] += flux[k]; R[6 * (size_t)j + k] -= flux[k]; }
+  }
+  for (int f = 0; f < m.F; ++f) {
+    const double n3[3] = {third * m.faceNorm[3 * f], third * m.faceNorm[3 * f + 1], third * m.faceNorm[3 * f + 2]};
+    for (int l = 0; l < 3; ++l) {
+      const int nd = m.faces[3 * f + l];
+      double flux[6];
+      face_flux_sa(gam, m.codes[f], n3, &V[6 * (size_t)nd], Ub, flux);
+      for (int k = 0; k < 6; ++k) R[6 * (size_t)nd + k] += flux[k];
+    }
+  }
+  for (int i = 0; i < N; ++i) {
+    const double invcv = 1.0 / m.ctrlVol[i];
+    for (int k = 0; k < 6; ++k) R[6 * (size_t)i + k] *= invcv;
+  }
+  if (model == 0) return ierr;
+  Visc vp;
+  vp.model = model; vp.ooreynolds = ooreynolds; vp.ooprandtl = ooprandtl; vp.bulk = bulk;
+  vp.alpha = alpha; vp.Ts = Ts;
+  SAParams sp{sa[0], sa[1], sa[2], sa[3], sa[4], sa[5], sa[6], sa[7], sa[8], fv3};
+  std::vector<double> G(6 * (size_t)N, 0.0);
+  galerkin_term_sa(m, V.data(), vp, sp, d2wall, G.data());
+  for (int i = 0; i < N; ++i)
+    for (int k = 0; k < 6; ++k) R[6 * (size_t)i + k] += G[6 * (size_t)i + k] / m.ctrlVol[i];
+  return ierr;
+}
+
+void orc_roeflux7_sa(double gam, const double* n, const double* Vi, const double* Vj, double* phi) {
+  roeflux7_sa(gam, n, Vi, Vj, phi);
+}
+void orc_face_flux_sa(double gam, int code, const double* n3, const double* V, const double* Ub, double* flux) {
+  face_flux_sa(gam, code, n3, V, Ub, flux);
+}
+
 void orc_timestep(void* h, const double* U, double cfl, double* dt) { timestep(*(Mesh*)h, U, cfl, dt); }
 
 // ExplicitTsDesc::computeRKSecondOrder (ExplicitTsDesc.C:98-117) with local

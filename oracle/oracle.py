@@ -78,6 +78,11 @@ def lib():
                                  C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
                                  _dp, _ip, _ip]
         L.orc_jvp.argtypes = [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp]
+        L.orc_residual_sa.restype = C.c_int
+        L.orc_residual_sa.argtypes = [C.c_void_p, _dp, _dp, C.c_int, C.c_int, C.c_double, C.c_double,
+                                      C.c_double, C.c_double, C.c_double, _dp, C.c_int, _dp, _dp]
+        L.orc_roeflux7_sa.argtypes = [C.c_double, _dp, _dp, _dp, _dp]
+        L.orc_face_flux_sa.argtypes = [C.c_double, C.c_int, _dp, _dp, _dp, _dp]
         L.orc_residual_visc.restype = C.c_int
         L.orc_residual_visc.argtypes = [C.c_void_p, _dp, _dp, C.c_int, C.c_int, C.c_double, C.c_double,
                                         C.c_double, C.c_double, C.c_double, _dp]
@@ -92,6 +97,12 @@ def lib():
         L.orc_zforce_dX.argtypes = [C.c_void_p, _dp, _ip, C.c_int, _dp]
         _lib = L
     return _lib
+
+
+# Spalart-Allmaras constants (cb1, cb2, cw2, cw3, cv1, cv2, sigma, vkcst,
+# prandtl_turbulent): SAModelData's and TurbulenceClosureData's defaults
+# (IoDataCore.C:1411-1418, 1839)
+SA_DEFAULTS = (0.1355, 0.622, 0.3, 2.0, 7.1, 5.0, 2.0 / 3.0, 0.41, 0.9)
 
 
 def _d(a):
@@ -158,6 +169,17 @@ class Oracle:
     def residual(self, U, Ub, order=2, beta=1.0 / 3.0, failsafe=0):
         U = f64(U); Ub = f64(Ub); R = np.empty_like(U)
         ierr = self.L.orc_residual(self.h, _d(U), _d(Ub), order, beta, failsafe, _d(R))
+        return R, ierr
+
+    def residual_sa(self, U, Ub, d2wall, order=2, model=1, reynolds=100.0, prandtl=0.72, bulk=0.0, alpha=1.0,
+                    Ts=0.0, sa=None, fv3=False):
+        """Spalart-Allmaras residual of U [N][6] (rho nu~ last) with the
+        viscous Galerkin term; sa = (cb1, cb2, cw2, cw3, cv1, cv2, sigma,
+        vkcst, prandtl_turbulent), the reference's defaults when None."""
+        U = f64(U); R = np.empty_like(U)
+        sa = f64(SA_DEFAULTS if sa is None else sa)
+        ierr = self.L.orc_residual_sa(self.h, _d(U), _d(f64(Ub)), order, model, 1.0 / reynolds, 1.0 / prandtl,
+                                      bulk, alpha, Ts, _d(sa), int(fv3), _d(f64(d2wall)), _d(R))
         return R, ierr
 
     def residual_visc(self, U, Ub, order=2, model=1, reynolds=100.0, prandtl=0.72, bulk=0.0, alpha=1.0,
@@ -299,6 +321,18 @@ class Oracle:
 def roeflux7(gam, n, Vi, Vj, ndot=0.0):
     out = np.empty(5)
     lib().orc_roeflux7(gam, _d(f64(n)), ndot, _d(f64(Vi)), _d(f64(Vj)), _d(out))
+    return out
+
+
+def roeflux7_sa(gam, n, Vi, Vj):
+    out = np.empty(6)
+    lib().orc_roeflux7_sa(gam, _d(f64(n)), _d(f64(Vi)), _d(f64(Vj)), _d(out))
+    return out
+
+
+def face_flux_sa(gam, code, n3, V, Ub):
+    out = np.empty(6)
+    lib().orc_face_flux_sa(gam, int(code), _d(f64(n3)), _d(f64(V)), _d(f64(Ub)), _d(out))
     return out
 
 

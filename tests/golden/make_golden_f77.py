@@ -121,6 +121,38 @@ def main() -> None:
     out["jac_in"] = np.column_stack([nrm, Vi, Vj])
     out["jac_out"] = jac
 
+    # the Spalart-Allmaras variants (type 1: a sixth, advected component,
+    # nu~ primitive, rho nu~ in the conservative boundary state), both
+    # upwind directions of the mass flux
+    n = 300
+    Vi = np.column_stack([states(rng, n), 1e-3 * (0.5 + rng.random(n))])
+    Vj = np.column_stack([Vi[:, :5] * (1 + 0.1 * rng.standard_normal((n, 5))), 1e-3 * (0.5 + rng.random(n))])
+    Vj[:, 0] = np.abs(Vj[:, 0]) + 0.05
+    Vj[:, 4] = np.abs(Vj[:, 4]) + 0.05
+    Vj[: n // 3, 1:4] = -Vj[: n // 3, 1:4]
+    nrm = rng.standard_normal((n, 3)) * 10.0 ** rng.uniform(-4, 0, (n, 1))
+    phi = np.empty((n, 6))
+    for k in range(n):
+        o = np.zeros(7)
+        L.roeflux7_f77_(_i(1), _d(GAM), _d(0.0), _p(nrm[k]), _d(0.0), _p(Vi[k]), _p(Vj[k]), o.ctypes.data_as(dp))
+        phi[k] = o[:6]
+    out["roe_sa_in"] = np.column_stack([nrm, Vi, Vj])
+    out["roe_sa_out"] = phi
+    n = 300
+    V = np.column_stack([states(rng, n, mach_spread=1.5), 1e-3 * (0.5 + rng.random(n))])
+    Vb = states(rng, n)
+    Ub = np.column_stack([Vb[:, 0], Vb[:, 0:1] * Vb[:, 1:4],
+                          Vb[:, 4] / (GAM - 1) + 0.5 * Vb[:, 0] * (Vb[:, 1:4] ** 2).sum(1),
+                          Vb[:, 0] * 1e-3 * (0.5 + rng.random(n))])
+    nrm = rng.standard_normal((n, 3)) * 10.0 ** rng.uniform(-4, 0, (n, 1))
+    fl = np.empty((n, 6))
+    for k in range(n):
+        o = np.zeros(7)
+        L.boundflux5_f77_(_i(1), _d(GAM), _p(nrm[k]), _d(0.0), _p(V[k]), _p(Ub[k]), o.ctypes.data_as(dp))
+        fl[k] = o[:6]
+    out["bf_sa_in"] = np.column_stack([nrm, V, Ub])
+    out["bf_sa_out"] = fl
+
     dst = os.path.join(HERE, "reference_fortran.npz")
     np.savez_compressed(dst, **out)
     print("wrote", dst, {k: v.shape for k, v in out.items()})

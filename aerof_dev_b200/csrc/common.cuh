@@ -173,27 +173,60 @@ struct DeviceMesh {
   DBuf<int> xslot;         // [E] spill slot of a block-crossing edge, -1 otherwise
   DBuf<int> xin_ptr;       // per node (new): its incoming spill slots [xin_ptr[n], xin_ptr[n+1])
   DBuf<int> bnf_ptr, bnf_ent;   // per node (new): its boundary subface fluxes, rows 3 f + l of fbuf, face order
-  // dependencies of the blocked residual on the caller's rows (for the
-  // residual of host arrays with its copies overlapped, residual.cu): per
-  // block the highest caller row that its primitive conversion, its
-  // gradients, its edge fluxes and its node assembly need
-  std::vector<int> h_prow, h_grow, h_frow, h_nrow;
-  std::vector<int> h_face_prow; // per boundary face: the highest row its nodes' conversions need
+  // schedule of the residual of host arrays with its copies overlapped
+  // (residual.cu), for kPipeChunks chunks of caller rows: the stage (the
+  // chunk after whose arrival it can run) of every blocked node's
+  // primitive conversion (its own row) and gradient (its and its
+  // neighbours' rows), of every block's edge fluxes (the gradients of its
+  // nodes and forward halo) and node assembly (its edge fluxes, those of
+  // the blocks that spill into it, and its boundary fluxes)
+  std::vector<unsigned char> h_st_prim, h_st_grad;  // [N] blocked nodes
+  std::vector<unsigned char> h_st_flux, h_st_node;  // [nblk]
   std::vector<int> h_o2n;       // [N] caller row -> blocked node
 };
 
 // Residual of host arrays in K chunks of caller rows: the copy of chunk s
 // of U, then the blocks whose stages it completes, while the next chunk is
 // copied in and finished chunks of R are copied out (residual.cu).
+constexpr int kPipeChunks = 8;
 struct ResidualPipe {
   int K = 0;
+  int ggrid = 1;                     // CTAs of the persistent gradient kernel
+  long long launches = 0;            // kernels in one call
   cudaStream_t sin = nullptr, sout = nullptr;
   std::vector<cudaEvent_t> ev_in, ev_stage;  // [K] chunk of U on the device; [K] stage s computed
   cudaEvent_t ev_go = nullptr, ev_out = nullptr;
-  DBuf<int> lists;                   // block (face) lists of every (kind, stage)
+  DBuf<int> lists;                   // node or block lists of every (kind, stage)
   std::vector<int> off;              // [5 kinds][K + 1] offsets into lists
-  std::vector<int> out_stage;        // [K] stage after which caller chunk c of R is final
+  std::vector<int> out_stage;        // [K] stage after which caller chunk c of R is copied out
+  // caller rows of R still being written when their chunk is copied out:
+  // gathered on the device after the last stage, copied once, and put in
+  // place on the host
+  DBuf<int> late;                    // [nlate] caller rows
+  DBuf<double> late_buf;             // [nlate][5]
+  std::vector<int> h_late;
+  double* h_late_buf = nullptr;      // page-locked [nlate][5]
+  int* h_bad = nullptr;              // page-locked unphysical count
+  // the whole call captured once as a graph for the host arrays (U, R) it
+  // was captured with, with the stream it was captured on
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const double* gU = nullptr;
+  double* gR = nullptr;
+  cudaStream_t gs = nullptr;
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+    gU = nullptr;
+    gR = nullptr;
+    gs = nullptr;
+  }
   ~ResidualPipe() {
+    drop_graph();
+    if (h_bad) cudaFreeHost(h_bad);
+    if (h_late_buf) cudaFreeHost(h_late_buf);
     for (auto e : ev_in) cudaEventDestroy(e);
     for (auto e : ev_stage) cudaEventDestroy(e);
     if (ev_go) cudaEventDestroy(ev_go);

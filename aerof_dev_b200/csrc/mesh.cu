@@ -563,32 +563,28 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
         m.bnf_ent.upload(be.data(), be.size(), s);
       }
       {
-        // highest caller row each residual stage of a block depends on:
-        // primitive conversion (its nodes), gradients (+ its halo's
-        // blocks' conversions), edge fluxes (+ its forward halo's blocks'
-        // gradients), node assembly (+ the fluxes of the blocks that spill
-        // into it)
-        const int nb = hb.nblk, NBk = m.NB;
-        m.h_prow.assign(nb, 0);
-        for (int n = 0; n < N; ++n) m.h_prow[n / NBk] = std::max(m.h_prow[n / NBk], hb.n2o[n]);
-        m.h_grow = m.h_prow;
-        for (int b = 0; b < nb; ++b)
-          for (int q = hb.hptr[b]; q < hb.hptr[b + 1]; ++q)
-            m.h_grow[b] = std::max(m.h_grow[b], m.h_prow[hb.hnode[q] / NBk]);
-        m.h_frow = m.h_grow;
+        // stages of the residual of host arrays with overlapped copies
+        // (DeviceMesh::h_st_*): chunk k of kPipeChunks holds the caller rows
+        // o with floor(o K / N) == k
+        const int nb = hb.nblk, NBk = m.NB, K = kPipeChunks;
+        auto chunk = [&](int o) { return (unsigned char)((long long)o * K / N); };
+        m.h_st_prim.resize(N);
+        for (int n = 0; n < N; ++n) m.h_st_prim[n] = chunk(hb.n2o[n]);
+        m.h_st_grad = m.h_st_prim;
+        for (int n = 0; n < N; ++n)
+          for (int q = hb.nb2_ptr[n]; q < hb.nb2_ptr[n + 1]; ++q)
+            m.h_st_grad[n] = std::max(m.h_st_grad[n], m.h_st_prim[hb.nb2_node[q]]);
+        m.h_st_flux.assign(nb, 0);
+        for (int n = 0; n < N; ++n) m.h_st_flux[n / NBk] = std::max(m.h_st_flux[n / NBk], m.h_st_grad[n]);
         for (int b = 0; b < nb; ++b)
           for (int q = hb.hfptr[b]; q < hb.hfptr[b + 1]; ++q)
-            m.h_frow[b] = std::max(m.h_frow[b], m.h_grow[hb.hfnode[q] / NBk]);
-        m.h_nrow = m.h_frow;
+            m.h_st_flux[b] = std::max(m.h_st_flux[b], m.h_st_grad[hb.hfnode[q]]);
+        m.h_st_node = m.h_st_flux;
         for (int q = 0; q < E; ++q)
           if (hb.xslot[q] >= 0) {
             const int bs = hb.bedges[q].y / NBk;
-            m.h_nrow[bs] = std::max(m.h_nrow[bs], m.h_frow[hb.bedges[q].x / NBk]);
+            m.h_st_node[bs] = std::max(m.h_st_node[bs], m.h_st_flux[hb.bedges[q].x / NBk]);
           }
-        m.h_face_prow.assign(F, 0);
-        for (int f = 0; f < F; ++f)
-          for (int l = 0; l < 3; ++l)
-            m.h_face_prow[f] = std::max(m.h_face_prow[f], m.h_prow[hb.o2n[faces[3 * (size_t)f + l]] / NBk]);
         m.h_o2n = hb.o2n;
       }
       AEROF_CUDA(cudaStreamSynchronize(s));  // host vectors die at scope end

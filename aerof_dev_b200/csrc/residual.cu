@@ -9,6 +9,7 @@
 // Edge.C:391-435, SubDomain.C:341-370), then its boundary faces in face
 // order (Face.C:1185-1215).  No floating-point atomics are used.
 #include <cstdlib>
+#include <cstring>
 
 #include "common.cuh"
 #include "physics.cuh"
@@ -646,14 +647,12 @@ __global__ void k_prim_blocked(int N, Gas g, const int* __restrict__ n2o, const 
   for (int k = 0; k < 5; ++k) P2[8 * (size_t)n + k] = v[k];
 }
 
-// k_prim_blocked for the nodes of blocks blist[0, nlist) only.
-__global__ void k_prim_blocks(int N, int NB, const int* __restrict__ blist, int nlist, Gas g,
-                              const int* __restrict__ n2o, const double* __restrict__ U, double* __restrict__ P2) {
+// k_prim_blocked for the blocked nodes nlist[0, count) only.
+__global__ void k_prim_nodes(const int* __restrict__ nlist, int count, Gas g, const int* __restrict__ n2o,
+                             const double* __restrict__ U, double* __restrict__ P2) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / NB;
-  if (i >= nlist) return;
-  const int n = blist[i] * NB + t % NB;
-  if (n >= N) return;
+  if (t >= count) return;
+  const int n = nlist[t];
   const int o = n2o[n];
   double u[5], v[5];
 #pragma unroll
@@ -663,18 +662,69 @@ __global__ void k_prim_blocks(int N, int NB, const int* __restrict__ blist, int 
   for (int k = 0; k < 5; ++k) P2[8 * (size_t)n + k] = v[k];
 }
 
+// The gradients of k_grad_pipe<L> for the blocked nodes nlist[0, count)
+// only, from the records in global memory: the same L lanes per node with
+// the same neighbour partition (r, r + L, ... of the ascending list) and
+// the same xor tree, so the same sums bit for bit.
+template <int L>
+__global__ void __launch_bounds__(256) k_grad_nodes(const int* __restrict__ nlist, int count, int N,
+                                                    const double* __restrict__ P2, const double* __restrict__ W2,
+                                                    const int* __restrict__ nb2_ptr,
+                                                    const int* __restrict__ nb2_node, double* __restrict__ G2) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / L, r = t % L;
+  const bool act = i < count;
+  const int n = act ? nlist[i] : 0;
+  double gs[15];
+#pragma unroll
+  for (int q = 0; q < 15; ++q) gs[q] = 0.0;
+  if (act) {
+    double w[6], pi[8];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) w[a] = W2[(size_t)a * N + n];
+    load_rec(P2, n, pi);
+#pragma unroll 1
+    for (int p = nb2_ptr[n] + r; p < nb2_ptr[n + 1]; p += L) {
+      double pj[8];
+      load_rec(P2, nb2_node[p], pj);
+      grad_acc(w, pi, pi + 5, pj, gs, gs + 5, gs + 10);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 15; ++q) {
+    if (L > 1) gs[q] += __shfl_xor_sync(0xffffffffu, gs[q], 1);
+    if (L > 2) gs[q] += __shfl_xor_sync(0xffffffffu, gs[q], 2);
+  }
+  if (!act) return;
+  constexpr int SL = 16 / L;
+  double o[SL];
+#pragma unroll
+  for (int q = 0; q < SL; ++q) {
+    double v = 0.0;
+#pragma unroll
+    for (int rr = 0; rr < L; ++rr)
+      if (SL * rr + q < 15 && r == rr) v = gs[SL * rr + q < 15 ? SL * rr + q : 0];
+    o[q] = v;
+  }
+  double2* gi = reinterpret_cast<double2*>(G2 + 16 * (size_t)n + SL * r);
+#pragma unroll
+  for (int q = 0; q < SL / 2; ++q) gi[q] = make_double2(o[2 * q], o[2 * q + 1]);
+}
+
+// R rows rows[0, count) (caller numbering) gathered into out[count][5]
+__global__ void k_gather_rows(const int* __restrict__ rows, int count, const double* __restrict__ R,
+                              double* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 5 * count) return;
+  out[t] = R[5 * (size_t)rows[t / 5] + t % 5];
+}
+
 // Boundary fluxes, one thread per face, the three subface fluxes with
 // normal n_f/3 (FaceTriaCore.C:288-308) into fbuf[3F][5].
 __global__ void k_face_flux(int F, Gas g, const double* __restrict__ Ub0, const int* __restrict__ faces,
                             const int* __restrict__ fcode, const double* __restrict__ fn,
-                            const double* __restrict__ P, const int* __restrict__ o2n, double* __restrict__ fbuf,
-                            const int* __restrict__ flist = nullptr, int nlist = 0) {
+                            const double* __restrict__ P, const int* __restrict__ o2n, double* __restrict__ fbuf) {
   int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (flist) {
-    // faces flist[0, nlist)
-    if (f >= nlist) return;
-    f = flist[f];
-  }
   if (f >= F) return;
   const double third = 1.0 / 3.0;
   double Ub[5];
@@ -880,6 +930,29 @@ static int grad_kernel_choice() {
   return v;
 }
 
+// Preferred shared-memory carveout of the residual's kernels (tuning knob
+// AEROF_CARVEOUT, percent; unset: the driver's choice per kernel).  Giving
+// every kernel of the sequence the same carveout keeps the SMs from being
+// reconfigured between a kernel with large dynamic shared memory and one
+// without.
+static void residual_carveout() {
+  static const int v = [] {
+    const char* e = std::getenv("AEROF_CARVEOUT");
+    return e ? std::atoi(e) : -1;
+  }();
+  static bool done = false;
+  if (v < 0 || done) return;
+  done = true;
+  const void* ks[] = {(const void*)k_prim_blocked, (const void*)k_prim_nodes, (const void*)k_grad_nodes<1>,
+                      (const void*)k_grad_nodes<2>, (const void*)k_grad_nodes<4>, (const void*)k_grad_pipe<1>,
+                      (const void*)k_grad_pipe<2>, (const void*)k_grad_pipe<4>, (const void*)k_face_flux,
+                      (const void*)k_fv_nodes_b<true>, (const void*)k_fv_nodes_b<false>,
+                      (const void*)k_fv_blocked<256, 2>, (const void*)k_fv_blocked<256, 3>,
+                      (const void*)k_fv_blocked<256, 4>, (const void*)k_fv_blocked<512, 2>};
+  for (const void* k : ks)
+    AEROF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, v));
+}
+
 // dynamic shared memory of k_fv_blocked: staged records of the block's
 // nodes and forward halo, the fluxes of its edges, the halo node ids
 static size_t fv_blocked_smem(const DeviceMesh& m) {
@@ -1009,6 +1082,7 @@ void grad_records_blocked_dev(aerof_gpu_ctx* c, const double* P2src, double* G2d
 
 // BLOCKED organisation of residual_dev (see k_fv_blocked).
 static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
+  residual_carveout();
   DeviceMesh& m = c->mesh;
   const Gas g = make_gas(c->cfg.gamma);
   const int rec = c->cfg.reconstruction;
@@ -1157,21 +1231,26 @@ int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
 
 // ------------------------------------------------------------------
 // Residual of HOST arrays with the copies overlapped with the computation.
-// U arrives in K chunks of caller rows on a copy stream; for every chunk s
-// that has arrived the compute stream runs the stages -- primitive
-// conversion, gradients, edge fluxes, boundary fluxes, node assembly -- of
-// the blocks and boundary faces whose dependencies (DeviceMesh::h_prow ..
-// h_nrow, h_face_prow) lie in chunks 0..s (a face's nodes are neighbours
-// of the node it is assembled into, so its fluxes are ready by that node's
-// stage), and a second copy stream takes every chunk
-// of R out as soon as the stage that completes it is done, while later
-// stages and copies still run.  The kernels and the arithmetic per block
-// are those of residual_blocked_dev (bitwise the same residual).  Used for
-// page-locked host U and R with the blocked kernel, the pipelined gradient
-// kernel, failsafe off, no viscous term and timers off, on meshes of at
-// least kPipeMinNodes nodes; otherwise aerof_gpu_residual stages the
-// arrays around one residual_dev.
-constexpr int kPipeChunks = 8;
+// U arrives in K chunks of caller rows on a copy stream.  For every chunk s
+// that has arrived, the compute stream runs the work whose inputs are then
+// complete (DeviceMesh::h_st_*): the primitive conversion of the nodes of
+// chunk s, the gradients of the nodes whose neighbourhoods are complete
+// (whole blocks by the persistent block kernel, the rest by a node
+// kernel), the edge fluxes of the blocks whose nodes and forward halo have
+// gradients, the node assembly with the boundary fluxes of the blocks
+// whose own and incoming fluxes are done.
+// A second copy stream (the copy engines run both directions at once)
+// takes chunk c of R out after stage c + 1; its rows whose assembly runs in
+// a later stage (their block depends on rows further on) are copied again
+// after the last stage, gathered into one buffer and put in place on the
+// host.  The conversion runs per node (k_prim_nodes), the gradients per
+// block (k_grad_pipe) or per node (k_grad_nodes, with the block kernel's
+// lanes and order), the fluxes and assembly per block (k_fv_blocked,
+// k_fv_nodes_b with the boundary fluxes of k_face_flux inside): the same
+// arithmetic as residual_blocked_dev, so the same residual bit for bit.  Used for page-locked host U and R with
+// the blocked kernel, failsafe off, no viscous term and timers off, on
+// meshes of at least kPipeMinNodes nodes; otherwise aerof_gpu_residual
+// stages the arrays around one residual_dev.
 constexpr int kPipeMinNodes = 1 << 17;
 
 static bool pinned_host(const void* p) {
@@ -1186,12 +1265,30 @@ static bool pinned_host(const void* p) {
 // first caller row of chunk k of K (rows o with floor(o K / N) == k)
 static size_t pipe_row0(size_t N, int K, int k) { return ((size_t)k * N + K - 1) / K; }
 
+// the edge-flux kernel of residual_blocked_dev for this mesh
+static decltype(&k_fv_blocked<256, 2>) pipe_fv_kernel(const DeviceMesh& m) {
+  const int by_smem = (int)std::min<size_t>(4, (228 * 1024) / (fv_blocked_smem(m) + 1024));
+  return by_smem >= 4 ? k_fv_blocked<256, 4> : by_smem == 3 ? k_fv_blocked<256, 3> : k_fv_blocked<256, 2>;
+}
+
 static ResidualPipe& pipe_for(aerof_gpu_ctx* c) {
   if (c->pipe) return *c->pipe;
   const DeviceMesh& m = c->mesh;
   auto p = std::make_unique<ResidualPipe>();
   const int K = kPipeChunks;
   p->K = K;
+  {
+    AEROF_CUDA(cudaFuncSetAttribute(pipe_fv_kernel(m), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)fv_blocked_smem(m)));
+    const int L = kBlock / m.NB;
+    auto gp = L == 4 ? k_grad_pipe<4> : L == 2 ? k_grad_pipe<2> : k_grad_pipe<1>;
+    const size_t gsmem = (size_t)2 * grad_stage(m).size * sizeof(double);
+    AEROF_CUDA(cudaFuncSetAttribute(gp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem));
+    int per_sm = 0, sms = 0;
+    AEROF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gp, kBlock, gsmem));
+    AEROF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
+    p->ggrid = std::max(per_sm, 1) * sms;
+  }
   AEROF_CUDA(cudaStreamCreateWithFlags(&p->sin, cudaStreamNonBlocking));
   AEROF_CUDA(cudaStreamCreateWithFlags(&p->sout, cudaStreamNonBlocking));
   p->ev_in.assign(K, nullptr);
@@ -1200,75 +1297,83 @@ static ResidualPipe& pipe_for(aerof_gpu_ctx* c) {
   for (auto& e : p->ev_stage) AEROF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   AEROF_CUDA(cudaEventCreateWithFlags(&p->ev_go, cudaEventDisableTiming));
   AEROF_CUDA(cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming));
-  const long long N = m.N;
-  auto chunk = [&](int row) { return (int)((long long)row * K / N); };
-  // kinds 0-3: blocks whose conversion / gradients / edge fluxes / node
-  // assembly a stage runs; kind 4: the boundary faces whose fluxes it runs
-  const std::vector<int>* rows[5] = {&m.h_prow, &m.h_grow, &m.h_frow, &m.h_nrow, &m.h_face_prow};
+  // kinds, by stage: 0 nodes converted; 1 blocks whose nodes all get their
+  // gradients in the stage (the persistent block kernel); 2 blocks' edge
+  // fluxes; 3 blocks' assembly (with their boundary fluxes); 4 the other
+  // nodes getting their gradients (node kernel)
+  const int NB = m.NB;
+  std::vector<unsigned char> gmin(m.nblk, 255), gmax(m.nblk, 0);
+  for (int n = 0; n < m.N; ++n) {
+    gmin[n / NB] = std::min(gmin[n / NB], m.h_st_grad[n]);
+    gmax[n / NB] = std::max(gmax[n / NB], m.h_st_grad[n]);
+  }
   std::vector<int> lists;
   p->off.assign(5 * (K + 1), 0);
   for (int kind = 0; kind < 5; ++kind) {
-    const std::vector<int>& r = *rows[kind];
-    for (int st = 0; st < K; ++st) {
-      p->off[kind * (K + 1) + st] = (int)lists.size();
-      for (int b = 0; b < (int)r.size(); ++b)
-        if (chunk(r[b]) == st) lists.push_back(b);
+    for (int s = 0; s < K; ++s) {
+      p->off[kind * (K + 1) + s] = (int)lists.size();
+      if (kind == 0) {
+        for (int n = 0; n < m.N; ++n)
+          if (m.h_st_prim[n] == s) lists.push_back(n);
+      } else if (kind == 1) {
+        for (int b = 0; b < m.nblk; ++b)
+          if (gmin[b] == gmax[b] && gmax[b] == s) lists.push_back(b);
+      } else if (kind == 2 || kind == 3) {
+        const std::vector<unsigned char>& v = kind == 2 ? m.h_st_flux : m.h_st_node;
+        for (int b = 0; b < m.nblk; ++b)
+          if (v[b] == s) lists.push_back(b);
+      } else {
+        for (int n = 0; n < m.N; ++n)
+          if (gmin[n / NB] != gmax[n / NB] && m.h_st_grad[n] == s) lists.push_back(n);
+      }
     }
     p->off[kind * (K + 1) + K] = (int)lists.size();
   }
   if (lists.empty()) lists.push_back(0);
+  // chunk c of R goes out after stage c + 1; its rows assembled later are
+  // the late rows
   p->out_stage.assign(K, 0);
-  for (int o = 0; o < m.N; ++o) {
-    const int cs = chunk(o);
-    p->out_stage[cs] = std::max(p->out_stage[cs], chunk(m.h_nrow[m.h_o2n[o] / m.NB]));
+  for (int k = 0; k < K; ++k) p->out_stage[k] = std::min(k + 1, K - 1);
+  for (int k = 0; k < K; ++k) {
+    const size_t r0 = pipe_row0(m.N, K, k), r1 = pipe_row0(m.N, K, k + 1);
+    for (size_t o = r0; o < r1; ++o)
+      if (m.h_st_node[m.h_o2n[o] / m.NB] > p->out_stage[k]) p->h_late.push_back((int)o);
   }
   p->lists.upload(lists.data(), lists.size(), c->stream);
+  AEROF_CUDA(cudaHostAlloc((void**)&p->h_bad, sizeof(int), cudaHostAllocDefault));
+  if (!p->h_late.empty()) {
+    p->late.upload(p->h_late.data(), p->h_late.size(), c->stream);
+    p->late_buf.ensure(5 * p->h_late.size());
+    AEROF_CUDA(cudaHostAlloc((void**)&p->h_late_buf, 5 * p->h_late.size() * sizeof(double), cudaHostAllocDefault));
+  }
   AEROF_CUDA(cudaStreamSynchronize(c->stream));
   c->pipe = std::move(p);
   return *c->pipe;
 }
 
-// false: not applicable (the caller takes the staged path)
-static bool residual_host_pipelined(aerof_gpu_ctx* c, const double* U, double* R, int& bad) {
+// Queue the whole overlapped residual of U into R on c->stream and the
+// pipe's copy streams (joined back into c->stream at the end); the
+// unphysical count goes to p.h_bad and the late rows to p.h_late_buf.
+static void pipelined_enqueue(aerof_gpu_ctx* c, ResidualPipe& p, const double* U, double* R) {
   DeviceMesh& m = c->mesh;
   const int rec = c->cfg.reconstruction;
   const bool grad = rec != AEROF_REC_CONSTANT;
-  if (m.N < kPipeMinNodes || c->cfg.failsafe || c->visc.model != 0 || c->timers.on) return false;
-  if (c->cfg.residual_kernel != AEROF_KERNEL_BLOCKED || fv_blocked_smem(m) > 200 * 1024) return false;
-  if (grad && grad_kernel_choice() != 3) return false;
-  if (grad && !(m.maxH <= 512 && 2 * grad_stage(m).size * sizeof(double) <= kMaxStagedSmem)) return false;
-  if (!pinned_host(U) || !pinned_host(R)) return false;
-  ResidualPipe& p = pipe_for(c);
   const int K = p.K;
   const Gas g = make_gas(c->cfg.gamma);
   cudaStream_t s = c->stream;
-  const size_t n5 = 5 * (size_t)m.N;
-  c->s.Ustage.ensure(n5);
-  c->s.Rstage.ensure(n5);
-  c->s.G2.ensure(16 * (size_t)m.N);
-  c->s.part.ensure(5 * (size_t)m.N);
-  c->s.spill.ensure(5 * (size_t)std::max(m.nX, 1));
-  c->s.fbuf.ensure(15 * (size_t)std::max(m.F, 1));
   int* cnt = counters(c);
   double* dU = c->s.Ustage.p;
   double* dR = c->s.Rstage.p;
-  // kernels and launch shapes of residual_blocked_dev
+  // the kernels and launch shapes of residual_blocked_dev (attributes set
+  // by pipe_for, outside any capture)
   const size_t fsmem = fv_blocked_smem(m);
-  const int by_smem = (int)std::min<size_t>(4, (228 * 1024) / (fsmem + 1024));
-  auto fvk = by_smem >= 4 ? k_fv_blocked<256, 4> : by_smem == 3 ? k_fv_blocked<256, 3> : k_fv_blocked<256, 2>;
-  AEROF_CUDA(cudaFuncSetAttribute(fvk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem));
+  auto fvk = pipe_fv_kernel(m);
+  const int L = kBlock / m.NB;
+  auto gk = L == 4 ? k_grad_nodes<4> : L == 2 ? k_grad_nodes<2> : k_grad_nodes<1>;
+  auto gp = L == 4 ? k_grad_pipe<4> : L == 2 ? k_grad_pipe<2> : k_grad_pipe<1>;
   const GradStage gst = grad_stage(m);
   const size_t gsmem = (size_t)2 * gst.size * sizeof(double);
-  const int L = kBlock / m.NB;
-  auto gk = L == 4 ? k_grad_pipe<4> : L == 2 ? k_grad_pipe<2> : k_grad_pipe<1>;
-  int ggrid = 1;
-  if (grad) {
-    AEROF_CUDA(cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem));
-    int per_sm = 0, sms = 0;
-    AEROF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gk, kBlock, gsmem));
-    AEROF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
-    ggrid = std::max(per_sm, 1) * sms;
-  }
+  const int ggrid = p.ggrid;
   AEROF_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * 2, s));
   // the copy streams start after the work already queued on s (which may
   // still read Ustage or write Rstage)
@@ -1285,41 +1390,43 @@ static bool residual_host_pipelined(aerof_gpu_ctx* c, const double* U, double* R
   const int* lists = p.lists.p;
   for (int st = 0; st < K; ++st) {
     AEROF_CUDA(cudaStreamWaitEvent(s, p.ev_in[st], 0));
-    auto seg = [&](int kind, int& cntb) {
+    auto seg = [&](int kind, int& count) {
       const int a = p.off[kind * (K + 1) + st];
-      cntb = p.off[kind * (K + 1) + st + 1] - a;
+      count = p.off[kind * (K + 1) + st + 1] - a;
       return lists + a;
     };
-    int nb = 0;
-    const int* lp = seg(0, nb);
-    if (nb) {
-      k_prim_blocks<<<grid_for((size_t)nb * m.NB, kBlock), kBlock, 0, s>>>(m.N, m.NB, lp, nb, g, m.n2o.p, dU, m.P2.p);
+    int nl = 0;
+    const int* lp = seg(0, nl);
+    if (nl) {
+      k_prim_nodes<<<grid_for(nl, kBlock), kBlock, 0, s>>>(lp, nl, g, m.n2o.p, dU, m.P2.p);
       AEROF_LAUNCH_CHECK();
     }
-    lp = seg(1, nb);
-    if (nb && grad) {
-      gk<<<std::min(nb, ggrid), kBlock, gsmem, s>>>(m.N, m.NB, nb, m.maxH, m.maxLp, gst, m.P2.p, m.W2.p, m.nb2_ptr.p,
-                                                     m.lpad.p, m.hpad.p, nullptr, c->s.G2.p, lp);
+    lp = seg(1, nl);
+    if (nl && grad) {
+      gp<<<std::min(nl, ggrid), kBlock, gsmem, s>>>(m.N, m.NB, nl, m.maxH, m.maxLp, gst, m.P2.p, m.W2.p, m.nb2_ptr.p,
+                                                    m.lpad.p, m.hpad.p, nullptr, c->s.G2.p, lp);
       AEROF_LAUNCH_CHECK();
     }
-    lp = seg(2, nb);
-    if (nb) {
-      fvk<<<nb, 256, fsmem, s>>>(m.N, m.E, m.NB, g, rec, c->cfg.beta, 0, m.bl.p, m.bnorm.p, m.beptr.p, m.hfptr.p,
+    lp = seg(4, nl);
+    if (nl && grad) {
+      gk<<<grid_for((size_t)nl * L, kBlock), kBlock, 0, s>>>(lp, nl, m.N, m.P2.p, m.W2.p, m.nb2_ptr.p, m.nb2_node.p,
+                                                              c->s.G2.p);
+      AEROF_LAUNCH_CHECK();
+    }
+    lp = seg(2, nl);
+    if (nl) {
+      fvk<<<nl, 256, fsmem, s>>>(m.N, m.E, m.NB, g, rec, c->cfg.beta, 0, m.bl.p, m.bnorm.p, m.beptr.p, m.hfptr.p,
                                  m.hfpad.p, m.maxHf, m.P2.p, c->s.G2.p, m.lptr.p, m.lidx.p, m.xslot.p, c->s.part.p,
                                  c->s.spill.p, c->s.tag.p, cnt, lp);
       AEROF_LAUNCH_CHECK();
     }
-    lp = seg(4, nb);
-    if (nb) {
-      k_face_flux<<<grid_for(nb, kBlock), kBlock, 0, s>>>(m.F, g, m.Ubd.p, m.faces.p, m.fcode.p, m.fnrm.p, m.P2.p,
-                                                          m.o2n.p, c->s.fbuf.p, lp, nb);
-      AEROF_LAUNCH_CHECK();
-    }
-    lp = seg(3, nb);
-    if (nb) {
-      k_fv_nodes_b<false><<<grid_for((size_t)nb * m.NB, kBlock), kBlock, 0, s>>>(
-          m.N, g, m.n2o.p, c->s.part.p, m.xin_ptr.p, c->s.spill.p, m.bnf_ptr.p, m.bnf_ent.p, c->s.fbuf.p, m.F,
-          m.Ubd.p, m.fcode.p, m.fnrm.p, m.P2.p, m.vol2.p, dR, lp, nb, m.NB);
+    lp = seg(3, nl);
+    if (nl) {
+      // the boundary fluxes inside the assembly (one launch instead of a
+      // small face kernel per stage)
+      k_fv_nodes_b<true><<<grid_for((size_t)nl * m.NB, kBlock), kBlock, 0, s>>>(
+          m.N, g, m.n2o.p, c->s.part.p, m.xin_ptr.p, c->s.spill.p, m.bnf_ptr.p, m.bnf_ent.p, nullptr, m.F, m.Ubd.p,
+          m.fcode.p, m.fnrm.p, m.P2.p, m.vol2.p, dR, lp, nl, m.NB);
       AEROF_LAUNCH_CHECK();
     }
     AEROF_CUDA(cudaEventRecord(p.ev_stage[st], s));
@@ -1332,10 +1439,93 @@ static bool residual_host_pipelined(aerof_gpu_ctx* c, const double* U, double* R
                                    p.sout));
     }
   }
+  const int nlate = (int)p.h_late.size();
+  if (nlate) {
+    // the late rows, final now: one gathered copy
+    k_gather_rows<<<grid_for(5 * (size_t)nlate, kBlock), kBlock, 0, s>>>(p.late.p, nlate, dR, p.late_buf.p);
+    AEROF_LAUNCH_CHECK();
+    AEROF_CUDA(cudaMemcpyAsync(p.h_late_buf, p.late_buf.p, 5 * (size_t)nlate * sizeof(double),
+                               cudaMemcpyDeviceToHost, s));
+  }
+  AEROF_CUDA(cudaMemcpyAsync(p.h_bad, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
   AEROF_CUDA(cudaEventRecord(p.ev_out, p.sout));
   AEROF_CUDA(cudaStreamWaitEvent(s, p.ev_out, 0));
-  AEROF_CUDA(cudaMemcpyAsync(&bad, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
+}
+
+// false: not applicable (the caller takes the staged path)
+static bool residual_host_pipelined(aerof_gpu_ctx* c, const double* U, double* R, int& bad) {
+  DeviceMesh& m = c->mesh;
+  const int rec = c->cfg.reconstruction;
+  const bool grad = rec != AEROF_REC_CONSTANT;
+  if (m.N < kPipeMinNodes || c->cfg.failsafe || c->visc.model != 0 || c->timers.on) return false;
+  if (c->cfg.residual_kernel != AEROF_KERNEL_BLOCKED || fv_blocked_smem(m) > 200 * 1024) return false;
+  if (grad && grad_kernel_choice() != 3) return false;
+  if (grad && !(m.maxH <= 512 && 2 * grad_stage(m).size * sizeof(double) <= kMaxStagedSmem)) return false;
+  if (!pinned_host(U) || !pinned_host(R)) return false;
+  ResidualPipe& p = pipe_for(c);
+  cudaStream_t s = c->stream;
+  const size_t n5 = 5 * (size_t)m.N;
+  c->s.Ustage.ensure(n5);
+  c->s.Rstage.ensure(n5);
+  c->s.G2.ensure(16 * (size_t)m.N);
+  c->s.part.ensure(5 * (size_t)m.N);
+  c->s.spill.ensure(5 * (size_t)std::max(m.nX, 1));
+  counters(c);
+  // The call's ~40 launches interleave with copies that saturate the host
+  // link in both directions, which stretches the gaps between launches
+  // that the host submits; as one graph (captured once per U, R and stream,
+  // then replayed) they are submitted at once.  A stream that cannot be
+  // captured (the legacy default stream) takes the direct path.
+  if (!(p.exec && p.gU == U && p.gR == R && p.gs == s)) {
+    p.drop_graph();
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    AEROF_CUDA(cudaStreamIsCapturing(s, &cs));
+    bool captured = false;
+    if (cs == cudaStreamCaptureStatusNone && s != cudaStreamLegacy && s != nullptr &&
+        cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      cudaGraph_t gph = nullptr;
+      const long long l0 = g_launch_count.load();
+      try {
+        pipelined_enqueue(c, p, U, R);
+        // launches are counted when the graph runs
+        p.launches = g_launch_count.load() - l0;
+        g_launch_count.fetch_sub(p.launches);
+      } catch (...) {
+        cudaStreamEndCapture(s, &gph);
+        if (gph) cudaGraphDestroy(gph);
+        cudaGetLastError();
+        throw;
+      }
+      if (cudaStreamEndCapture(s, &gph) == cudaSuccess && gph) {
+        cudaGraphExec_t ex = nullptr;
+        if (cudaGraphInstantiate(&ex, gph, 0) == cudaSuccess) {
+          p.graph = gph;
+          p.exec = ex;
+          p.gU = U;
+          p.gR = R;
+          p.gs = s;
+          captured = true;
+        } else {
+          cudaGraphDestroy(gph);
+        }
+      }
+      cudaGetLastError();
+    }
+    if (!captured) {
+      pipelined_enqueue(c, p, U, R);
+    }
+  }
+  if (p.exec) {
+    AEROF_CUDA(cudaGraphLaunch(p.exec, s));
+    g_launch_count.fetch_add(p.launches);
+  }
   AEROF_CUDA(cudaStreamSynchronize(s));
+  // every copy of R has landed (the late rows' first copies too): the late
+  // rows' final values over them
+  const int nlate = (int)p.h_late.size();
+  for (int q = 0; q < nlate; ++q)
+    std::memcpy(R + 5 * (size_t)p.h_late[q], p.h_late_buf + 5 * (size_t)q, 5 * sizeof(double));
+  bad = *p.h_bad;
   c->s.p2g2_valid = true;
   return true;
 }

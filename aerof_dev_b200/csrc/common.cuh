@@ -174,12 +174,13 @@ struct DeviceMesh {
   DBuf<int> xin_ptr;       // per node (new): its incoming spill slots [xin_ptr[n], xin_ptr[n+1])
   DBuf<int> bnf_ptr, bnf_ent;   // per node (new): its boundary subface fluxes, rows 3 f + l of fbuf, face order
   // schedule of the residual of host arrays with its copies overlapped
-  // (residual.cu), for kPipeChunks chunks of caller rows: the stage (the
+  // (residual.cu), for pipeK chunks of caller rows: the stage (the
   // chunk after whose arrival it can run) of every blocked node's
   // primitive conversion (its own row) and gradient (its and its
   // neighbours' rows), of every block's edge fluxes (the gradients of its
   // nodes and forward halo) and node assembly (its edge fluxes, those of
   // the blocks that spill into it, and its boundary fluxes)
+  int pipeK = 8;                                    // chunks of caller rows
   std::vector<unsigned char> h_st_prim, h_st_grad;  // [N] blocked nodes
   std::vector<unsigned char> h_st_flux, h_st_node;  // [nblk]
   std::vector<int> h_o2n;       // [N] caller row -> blocked node
@@ -188,7 +189,6 @@ struct DeviceMesh {
 // Residual of host arrays in K chunks of caller rows: the copy of chunk s
 // of U, then the blocks whose stages it completes, while the next chunk is
 // copied in and finished chunks of R are copied out (residual.cu).
-constexpr int kPipeChunks = 8;
 struct ResidualPipe {
   int K = 0;
   int ggrid = 1;                     // CTAs of the persistent gradient kernel
@@ -200,13 +200,13 @@ struct ResidualPipe {
   std::vector<int> off;              // [5 kinds][K + 1] offsets into lists
   std::vector<int> out_stage;        // [K] stage after which caller chunk c of R is copied out
   // caller rows of R still being written when their chunk is copied out:
-  // gathered on the device after the last stage, copied once, and put in
-  // place on the host
+  // after the last stage (and after that chunk's copy has landed) a kernel
+  // writes their final values into the page-locked R through its device
+  // address
   DBuf<int> late;                    // [nlate] caller rows
-  DBuf<double> late_buf;             // [nlate][5]
   std::vector<int> h_late;
-  double* h_late_buf = nullptr;      // page-locked [nlate][5]
   int* h_bad = nullptr;              // page-locked unphysical count
+  cudaEvent_t ev_pre = nullptr;      // the copies before the last stage's
   // the whole call captured once as a graph for the host arrays (U, R) it
   // was captured with, with the stream it was captured on
   cudaGraph_t graph = nullptr;
@@ -226,7 +226,7 @@ struct ResidualPipe {
   ~ResidualPipe() {
     drop_graph();
     if (h_bad) cudaFreeHost(h_bad);
-    if (h_late_buf) cudaFreeHost(h_late_buf);
+    if (ev_pre) cudaEventDestroy(ev_pre);
     for (auto e : ev_in) cudaEventDestroy(e);
     for (auto e : ev_stage) cudaEventDestroy(e);
     if (ev_go) cudaEventDestroy(ev_go);

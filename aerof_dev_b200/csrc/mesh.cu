@@ -564,9 +564,14 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
       }
       {
         // stages of the residual of host arrays with overlapped copies
-        // (DeviceMesh::h_st_*): chunk k of kPipeChunks holds the caller rows
-        // o with floor(o K / N) == k
-        const int nb = hb.nblk, NBk = m.NB, K = kPipeChunks;
+        // (DeviceMesh::h_st_*): chunk k of K holds the caller rows o with
+        // floor(o K / N) == k; K = 8 (tuning knob AEROF_PIPE_CHUNKS, 2-32)
+        m.pipeK = 8;
+        if (const char* env = std::getenv("AEROF_PIPE_CHUNKS")) {
+          const int v = std::atoi(env);
+          if (v >= 2 && v <= 32) m.pipeK = v;
+        }
+        const int nb = hb.nblk, NBk = m.NB, K = m.pipeK;
         auto chunk = [&](int o) { return (unsigned char)((long long)o * K / N); };
         m.h_st_prim.resize(N);
         for (int n = 0; n < N; ++n) m.h_st_prim[n] = chunk(hb.n2o[n]);

@@ -711,12 +711,14 @@ __global__ void __launch_bounds__(256) k_grad_nodes(const int* __restrict__ nlis
   for (int q = 0; q < SL / 2; ++q) gi[q] = make_double2(o[2 * q], o[2 * q + 1]);
 }
 
-// R rows rows[0, count) (caller numbering) gathered into out[count][5]
-__global__ void k_gather_rows(const int* __restrict__ rows, int count, const double* __restrict__ R,
-                              double* __restrict__ out) {
+// R rows rows[0, count) (caller numbering) copied into Rh, the device
+// address of a page-locked host array of the same layout
+__global__ void k_put_rows(const int* __restrict__ rows, int count, const double* __restrict__ R,
+                           double* __restrict__ Rh) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 5 * count) return;
-  out[t] = R[5 * (size_t)rows[t / 5] + t % 5];
+  const size_t q = 5 * (size_t)rows[t / 5] + t % 5;
+  Rh[q] = R[q];
 }
 
 // Boundary fluxes, one thread per face, the three subface fluxes with
@@ -930,29 +932,6 @@ static int grad_kernel_choice() {
   return v;
 }
 
-// Preferred shared-memory carveout of the residual's kernels (tuning knob
-// AEROF_CARVEOUT, percent; unset: the driver's choice per kernel).  Giving
-// every kernel of the sequence the same carveout keeps the SMs from being
-// reconfigured between a kernel with large dynamic shared memory and one
-// without.
-static void residual_carveout() {
-  static const int v = [] {
-    const char* e = std::getenv("AEROF_CARVEOUT");
-    return e ? std::atoi(e) : -1;
-  }();
-  static bool done = false;
-  if (v < 0 || done) return;
-  done = true;
-  const void* ks[] = {(const void*)k_prim_blocked, (const void*)k_prim_nodes, (const void*)k_grad_nodes<1>,
-                      (const void*)k_grad_nodes<2>, (const void*)k_grad_nodes<4>, (const void*)k_grad_pipe<1>,
-                      (const void*)k_grad_pipe<2>, (const void*)k_grad_pipe<4>, (const void*)k_face_flux,
-                      (const void*)k_fv_nodes_b<true>, (const void*)k_fv_nodes_b<false>,
-                      (const void*)k_fv_blocked<256, 2>, (const void*)k_fv_blocked<256, 3>,
-                      (const void*)k_fv_blocked<256, 4>, (const void*)k_fv_blocked<512, 2>};
-  for (const void* k : ks)
-    AEROF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, v));
-}
-
 // dynamic shared memory of k_fv_blocked: staged records of the block's
 // nodes and forward halo, the fluxes of its edges, the halo node ids
 static size_t fv_blocked_smem(const DeviceMesh& m) {
@@ -1082,7 +1061,6 @@ void grad_records_blocked_dev(aerof_gpu_ctx* c, const double* P2src, double* G2d
 
 // BLOCKED organisation of residual_dev (see k_fv_blocked).
 static int residual_blocked_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
-  residual_carveout();
   DeviceMesh& m = c->mesh;
   const Gas g = make_gas(c->cfg.gamma);
   const int rec = c->cfg.reconstruction;
@@ -1241,9 +1219,9 @@ int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
 // whose own and incoming fluxes are done.
 // A second copy stream (the copy engines run both directions at once)
 // takes chunk c of R out after stage c + 1; its rows whose assembly runs in
-// a later stage (their block depends on rows further on) are copied again
-// after the last stage, gathered into one buffer and put in place on the
-// host.  The conversion runs per node (k_prim_nodes), the gradients per
+// a later stage (their block depends on rows further on) are written again
+// after the last stage, once that chunk's copy has landed, by a kernel
+// storing into R through its device address.  The conversion runs per node (k_prim_nodes), the gradients per
 // block (k_grad_pipe) or per node (k_grad_nodes, with the block kernel's
 // lanes and order), the fluxes and assembly per block (k_fv_blocked,
 // k_fv_nodes_b with the boundary fluxes of k_face_flux inside): the same
@@ -1253,13 +1231,19 @@ int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
 // stages the arrays around one residual_dev.
 constexpr int kPipeMinNodes = 1 << 17;
 
-static bool pinned_host(const void* p) {
+// page-locked host memory (with its device address when dev is given)
+static bool pinned_host(const void* p, void** dev = nullptr) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeHost;
+  if (a.type != cudaMemoryTypeHost) return false;
+  if (dev) {
+    *dev = a.devicePointer;
+    if (!*dev) return false;
+  }
+  return true;
 }
 
 // first caller row of chunk k of K (rows o with floor(o K / N) == k)
@@ -1275,7 +1259,7 @@ static ResidualPipe& pipe_for(aerof_gpu_ctx* c) {
   if (c->pipe) return *c->pipe;
   const DeviceMesh& m = c->mesh;
   auto p = std::make_unique<ResidualPipe>();
-  const int K = kPipeChunks;
+  const int K = m.pipeK;
   p->K = K;
   {
     AEROF_CUDA(cudaFuncSetAttribute(pipe_fv_kernel(m), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1341,20 +1325,18 @@ static ResidualPipe& pipe_for(aerof_gpu_ctx* c) {
   }
   p->lists.upload(lists.data(), lists.size(), c->stream);
   AEROF_CUDA(cudaHostAlloc((void**)&p->h_bad, sizeof(int), cudaHostAllocDefault));
-  if (!p->h_late.empty()) {
-    p->late.upload(p->h_late.data(), p->h_late.size(), c->stream);
-    p->late_buf.ensure(5 * p->h_late.size());
-    AEROF_CUDA(cudaHostAlloc((void**)&p->h_late_buf, 5 * p->h_late.size() * sizeof(double), cudaHostAllocDefault));
-  }
+  AEROF_CUDA(cudaEventCreateWithFlags(&p->ev_pre, cudaEventDisableTiming));
+  if (!p->h_late.empty()) p->late.upload(p->h_late.data(), p->h_late.size(), c->stream);
   AEROF_CUDA(cudaStreamSynchronize(c->stream));
   c->pipe = std::move(p);
   return *c->pipe;
 }
 
 // Queue the whole overlapped residual of U into R on c->stream and the
-// pipe's copy streams (joined back into c->stream at the end); the
-// unphysical count goes to p.h_bad and the late rows to p.h_late_buf.
-static void pipelined_enqueue(aerof_gpu_ctx* c, ResidualPipe& p, const double* U, double* R) {
+// pipe's copy streams (joined back into c->stream at the end); Rdev is R's
+// device address (for the late rows); the unphysical count goes to
+// p.h_bad.
+static void pipelined_enqueue(aerof_gpu_ctx* c, ResidualPipe& p, const double* U, double* R, double* Rdev) {
   DeviceMesh& m = c->mesh;
   const int rec = c->cfg.reconstruction;
   const bool grad = rec != AEROF_REC_CONSTANT;
@@ -1430,6 +1412,8 @@ static void pipelined_enqueue(aerof_gpu_ctx* c, ResidualPipe& p, const double* U
       AEROF_LAUNCH_CHECK();
     }
     AEROF_CUDA(cudaEventRecord(p.ev_stage[st], s));
+    // every copy queued so far (the chunks that can hold late rows)
+    if (st == K - 1) AEROF_CUDA(cudaEventRecord(p.ev_pre, p.sout));
     for (int k = 0; k < K; ++k) {
       if (p.out_stage[k] != st) continue;
       const size_t r0 = pipe_row0(m.N, K, k), r1 = pipe_row0(m.N, K, k + 1);
@@ -1441,11 +1425,11 @@ static void pipelined_enqueue(aerof_gpu_ctx* c, ResidualPipe& p, const double* U
   }
   const int nlate = (int)p.h_late.size();
   if (nlate) {
-    // the late rows, final now: one gathered copy
-    k_gather_rows<<<grid_for(5 * (size_t)nlate, kBlock), kBlock, 0, s>>>(p.late.p, nlate, dR, p.late_buf.p);
+    // the late rows, final now, over their chunks' earlier copies (which
+    // must have landed first)
+    AEROF_CUDA(cudaStreamWaitEvent(s, p.ev_pre, 0));
+    k_put_rows<<<grid_for(5 * (size_t)nlate, kBlock), kBlock, 0, s>>>(p.late.p, nlate, dR, Rdev);
     AEROF_LAUNCH_CHECK();
-    AEROF_CUDA(cudaMemcpyAsync(p.h_late_buf, p.late_buf.p, 5 * (size_t)nlate * sizeof(double),
-                               cudaMemcpyDeviceToHost, s));
   }
   AEROF_CUDA(cudaMemcpyAsync(p.h_bad, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
   AEROF_CUDA(cudaEventRecord(p.ev_out, p.sout));
@@ -1461,7 +1445,8 @@ static bool residual_host_pipelined(aerof_gpu_ctx* c, const double* U, double* R
   if (c->cfg.residual_kernel != AEROF_KERNEL_BLOCKED || fv_blocked_smem(m) > 200 * 1024) return false;
   if (grad && grad_kernel_choice() != 3) return false;
   if (grad && !(m.maxH <= 512 && 2 * grad_stage(m).size * sizeof(double) <= kMaxStagedSmem)) return false;
-  if (!pinned_host(U) || !pinned_host(R)) return false;
+  void* Rdev = nullptr;
+  if (!pinned_host(U) || !pinned_host(R, &Rdev)) return false;
   ResidualPipe& p = pipe_for(c);
   cudaStream_t s = c->stream;
   const size_t n5 = 5 * (size_t)m.N;
@@ -1486,7 +1471,7 @@ static bool residual_host_pipelined(aerof_gpu_ctx* c, const double* U, double* R
       cudaGraph_t gph = nullptr;
       const long long l0 = g_launch_count.load();
       try {
-        pipelined_enqueue(c, p, U, R);
+        pipelined_enqueue(c, p, U, R, static_cast<double*>(Rdev));
         // launches are counted when the graph runs
         p.launches = g_launch_count.load() - l0;
         g_launch_count.fetch_sub(p.launches);
@@ -1512,7 +1497,7 @@ static bool residual_host_pipelined(aerof_gpu_ctx* c, const double* U, double* R
       cudaGetLastError();
     }
     if (!captured) {
-      pipelined_enqueue(c, p, U, R);
+      pipelined_enqueue(c, p, U, R, static_cast<double*>(Rdev));
     }
   }
   if (p.exec) {
@@ -1520,11 +1505,6 @@ static bool residual_host_pipelined(aerof_gpu_ctx* c, const double* U, double* R
     g_launch_count.fetch_add(p.launches);
   }
   AEROF_CUDA(cudaStreamSynchronize(s));
-  // every copy of R has landed (the late rows' first copies too): the late
-  // rows' final values over them
-  const int nlate = (int)p.h_late.size();
-  for (int q = 0; q < nlate; ++q)
-    std::memcpy(R + 5 * (size_t)p.h_late[q], p.h_late_buf + 5 * (size_t)q, 5 * sizeof(double));
   bad = *p.h_bad;
   c->s.p2g2_valid = true;
   return true;

@@ -787,6 +787,101 @@ def run_adjoint_products(args):
     return 0
 
 
+def run_sa_residual(args):
+    """Spalart-Allmaras residual (six variables, van Albada, Sutherland
+    viscosity, Re 1e6 per unit length, nu~ 3 nu_inf with a bump, wall
+    distance to z = 0) on the lattice mesh: device time per evaluation with
+    device arrays (CUDA events), against the five-variable laminar residual
+    of the same mesh and flow."""
+    import torch
+    import aerof_dev_b200 as A
+    torch.cuda.set_device(0)
+    clocks = ClockSampler(gpu_uuid(0))
+    clocks.start()
+    W, mesh, Ub, U = build_workload(args.n)
+    ctx = A.Context.from_mesh(mesh, Ub, reconstruction=A.REC_VANALBADA)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream)
+    ctx.set_viscosity(model=2, reynolds_mu=1e6, prandtl=0.72, sutherland_alpha=1.4 * 0.4 * 0.64,
+                      sutherland_Ts=0.37)
+    X = mesh["X"]
+    nu = 3e-6 * (1.0 + 4.0 * np.exp(-((X - 0.5) ** 2).sum(1) / 0.05))
+    U6 = np.column_stack([U, U[:, 0] * nu])
+    Ub6 = np.concatenate([Ub, [3e-6 * Ub[0]]])
+    ctx.set_turbulence(np.abs(X[:, 2]) + 1e-3, Ub6)
+    sp = A.SpaceOperator(ctx)
+    U6d = torch.from_numpy(U6).cuda()
+    R6d = torch.empty_like(U6d)
+    Ud = torch.from_numpy(U).cuda()
+    Rd = torch.empty_like(Ud)
+    t_sa = timed_on(stream, lambda: sp.computeResidualSA(U6d, R6d), args.steps, args.warmup)
+    t_lam = timed_on(stream, lambda: sp.computeResidual(Ud, Rd), args.steps, args.warmup)
+    s = W.lattice_sizes(args.n)
+    line = {"metric": METRIC, "workload": "sa_residual", "value": s["E"] / (t_sa * 1e-3) / 1e6,
+            "unit": "Medges/s", "higher_is_better": True, "ms_per_eval": t_sa,
+            "laminar_ms_per_eval": t_lam, "sa_over_laminar": t_sa / t_lam,
+            "config": {"workload": f"Spalart-Allmaras residual (6 variables, van Albada + LSQ + Roe, Sutherland "
+                                   f"viscosity), {args.n}^3 jittered Kuhn tet mesh N={s['N']} E={s['E']}",
+                       "organisation": "edge (thread per edge, per-node gather)"}}
+    line["clocks"] = clocks.stop()
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
+def run_e2e_timeline(args):
+    """Device timeline of the residual of page-locked host arrays (the e2e
+    call): three calls traced with CUPTI (torch.profiler), per call its span
+    and, per kind of work, the summed device time of the copies in, the
+    copies out and the kernels (they overlap)."""
+    import torch
+    import aerof_dev_b200 as A
+    from torch.profiler import ProfilerActivity, profile
+    torch.cuda.set_device(0)
+    W, mesh, Ub, U = build_workload(args.n)
+    ctx = A.Context.from_mesh(mesh, Ub, reconstruction=A.REC_VANALBADA)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream)
+    sp = A.SpaceOperator(ctx)
+    Uh = torch.from_numpy(U).pin_memory()
+    Rh = torch.empty_like(Uh).pin_memory()
+    for _ in range(max(args.warmup, 3)):
+        sp.computeResidual(Uh, Rh)
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        for _ in range(3):
+            sp.computeResidual(Uh, Rh)
+        torch.cuda.synchronize()
+    ev = sorted((e for e in prof.events() if e.device_type.name == "CUDA"), key=lambda e: e.time_range.start)
+    # every call starts with the memset of its counters
+    calls = []
+    for e in ev:
+        if "Memset" in e.name or not calls:
+            calls.append([e])
+        else:
+            calls[-1].append(e)
+    out = []
+    for c in calls:
+        t0 = min(e.time_range.start for e in c)
+        t1 = max(e.time_range.end for e in c)
+        kinds = {"h2d_us": 0.0, "d2h_us": 0.0, "kernel_us": 0.0}
+        for e in c:
+            d = e.time_range.end - e.time_range.start
+            if "HtoD" in e.name:
+                kinds["h2d_us"] += d
+            elif "DtoH" in e.name:
+                kinds["d2h_us"] += d
+            elif "Memset" not in e.name:
+                kinds["kernel_us"] += d
+        out.append({"span_us": t1 - t0, **{k: round(v, 1) for k, v in kinds.items()},
+                    "kernels": sum(1 for e in c if "Memcpy" not in e.name and "Memset" not in e.name)})
+    s = W.lattice_sizes(args.n)
+    print(json.dumps({"metric": METRIC, "workload": "e2e_timeline", "n": args.n, "E": s["E"],
+                      "bytes_each_way": int(U.nbytes), "calls": out}), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -802,7 +897,8 @@ def main():
                     help="lattice sizes of the Newton part (the last one is reported as 'newton')")
     ap.add_argument("--no-adjoint-cost", action="store_true",
                     help="leave the adjoint-cost part out of the residual line")
-    ap.add_argument("--workload", choices=["residual", "newton", "adjoint", "adjoint_products", "sensitivities"],
+    ap.add_argument("--workload", choices=["residual", "newton", "adjoint", "adjoint_products", "sensitivities",
+                                           "e2e_timeline", "sa_residual"],
                     default="residual")
     ap.add_argument("--max-steps", type=int, default=400)
     ap.add_argument("--modes", type=int, default=32)
@@ -826,6 +922,10 @@ def main():
         return run_adjoint(args)
     if args.workload == "adjoint_products":
         return run_adjoint_products(args)
+    if args.workload == "e2e_timeline":
+        return run_e2e_timeline(args)
+    if args.workload == "sa_residual":
+        return run_sa_residual(args)
     if args.workload == "sensitivities":
         return run_sensitivities(args)
     return run_ours(args)

@@ -181,6 +181,7 @@ struct DeviceMesh {
   // nodes and forward halo) and node assembly (its edge fluxes, those of
   // the blocks that spill into it, and its boundary fluxes)
   int pipeK = 8;                                    // chunks of caller rows
+  std::vector<int> pipe_rows;                       // [pipeK + 1] first caller row of each chunk
   std::vector<unsigned char> h_st_prim, h_st_grad;  // [N] blocked nodes
   std::vector<unsigned char> h_st_flux, h_st_node;  // [nblk]
   std::vector<int> h_o2n;       // [N] caller row -> blocked node
@@ -192,7 +193,6 @@ struct DeviceMesh {
 struct ResidualPipe {
   int K = 0;
   int ggrid = 1;                     // CTAs of the persistent gradient kernel
-  long long launches = 0;            // kernels in one call
   cudaStream_t sin = nullptr, sout = nullptr;
   std::vector<cudaEvent_t> ev_in, ev_stage;  // [K] chunk of U on the device; [K] stage s computed
   cudaEvent_t ev_go = nullptr, ev_out = nullptr;
@@ -207,24 +207,11 @@ struct ResidualPipe {
   std::vector<int> h_late;
   int* h_bad = nullptr;              // page-locked unphysical count
   cudaEvent_t ev_pre = nullptr;      // the copies before the last stage's
-  // the whole call captured once as a graph for the host arrays (U, R) it
-  // was captured with, with the stream it was captured on
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  const double* gU = nullptr;
-  double* gR = nullptr;
-  cudaStream_t gs = nullptr;
-  void drop_graph() {
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    exec = nullptr;
-    graph = nullptr;
-    gU = nullptr;
-    gR = nullptr;
-    gs = nullptr;
-  }
+  // each stage's kernels captured once as a graph, with its kernel count
+  std::vector<cudaGraphExec_t> stage_exec;
+  std::vector<long long> stage_launches;
   ~ResidualPipe() {
-    drop_graph();
+    for (auto e : stage_exec) cudaGraphExecDestroy(e);
     if (h_bad) cudaFreeHost(h_bad);
     if (ev_pre) cudaEventDestroy(ev_pre);
     for (auto e : ev_in) cudaEventDestroy(e);
@@ -248,6 +235,8 @@ struct Scratch {
   DBuf<int> tag;           // [N] failsafe tags
   DBuf<int> counters;      // [8] device counters
   DBuf<double> red;        // reduction partials
+  DBuf<double> tetc;       // [4T][4] Galerkin shares of each (tet, vertex)
+  DBuf<double> viscq;      // [N][8] node records of the Galerkin term
   // set by the blocked residual: P2 / G2 hold the untagged primitive
   // records and gradients of the state it evaluated
   bool p2g2_valid = false;
@@ -348,6 +337,8 @@ struct TurbWork {
   DBuf<double> G6;         // [N][18] LSQ gradients (x, y, z of the six components)
   DBuf<double> flux6;      // [6][E]
   DBuf<double> fbuf6;      // [3F][6]
+  DBuf<double> tetc;       // [4T][5] SA Galerkin shares of each (tet, vertex)
+  DBuf<double> q;          // [N][12] node records of the SA Galerkin term
   DBuf<double> Ustage, Rstage;
 };
 
@@ -509,8 +500,39 @@ void h2_evaluate_dev(aerof_gpu_ctx* c, const double* dU);
 // implemented in mesh.cu: recompute the geometry for new coordinates
 void compute_geometry(aerof_gpu_ctx* c);
 // implemented in viscous.cu: R += (viscous Galerkin term of U) / ctrlVol
-// when a viscous model is set (no allocation)
+// when a viscous model is set (no allocation: the per-tet buffer is sized
+// by galerkin_reserve, which set_mesh and set_viscosity call)
 void galerkin_add(aerof_gpu_ctx* c, const double* dU, double* dR);
+void galerkin_reserve(aerof_gpu_ctx* c);
+
+// Node side of a Galerkin term evaluated once per tet: the tet kernel wrote
+// node k's share of tet t as the W-double record C[W (4t + k)]; thread
+// (i, k) sums component k of the records of node i's tets in ascending tet
+// order (nt_tet holds 4t + k, ascending in t) and adds the sum / vol[i] to
+// R[RS i + R0 + k].  W consecutive threads read one record.
+template <int W, int RS, int R0>
+__global__ void k_tet_gather(int N, const int* __restrict__ nt_ptr, const int* __restrict__ nt_tet,
+                             const double* __restrict__ C, const double* __restrict__ vol, double* __restrict__ R) {
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= (long long)N * W) return;
+  const int i = (int)(j / W), k = (int)(j - (long long)i * W);
+  double acc = 0.0;
+  int q = nt_ptr[i];
+  const int qe = nt_ptr[i + 1];
+  // four records in flight per step; the sum keeps ascending tet order
+  for (; q + 4 <= qe; q += 4) {
+    const int4 tl = make_int4(nt_tet[q], nt_tet[q + 1], nt_tet[q + 2], nt_tet[q + 3]);
+    const double c0 = __ldcs(C + W * (size_t)tl.x + k), c1 = __ldcs(C + W * (size_t)tl.y + k);
+    const double c2 = __ldcs(C + W * (size_t)tl.z + k), c3 = __ldcs(C + W * (size_t)tl.w + k);
+    acc += c0;
+    acc += c1;
+    acc += c2;
+    acc += c3;
+  }
+  for (; q < qe; ++q) acc += __ldcs(C + W * (size_t)nt_tet[q] + k);
+  const double iv = 1.0 / vol[i];
+  R[RS * (size_t)i + R0 + k] += acc * iv;
+}
 // the exact linearisations cover the inviscid residual only
 inline void need_inviscid(aerof_gpu_ctx* c) {
   if (c->visc.model != 0)

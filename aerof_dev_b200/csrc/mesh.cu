@@ -564,17 +564,46 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
       }
       {
         // stages of the residual of host arrays with overlapped copies
-        // (DeviceMesh::h_st_*): chunk k of K holds the caller rows o with
-        // floor(o K / N) == k; K = 8 (tuning knob AEROF_PIPE_CHUNKS, 2-32)
-        m.pipeK = 8;
+        // (DeviceMesh::h_st_*): K chunks of consecutive caller rows, their
+        // sizes in proportion to the weights w_k.  Short first chunks let
+        // the copies of R start early, short last ones shorten what remains
+        // after the last copy of U.  Default K = 8 equal chunks (tuning
+        // knobs AEROF_PIPE_CHUNKS, 2-32 equal chunks, or AEROF_PIPE_WEIGHTS,
+        // 2-32 comma-separated positive weights)
+        std::vector<double> w(8, 1.0);
         if (const char* env = std::getenv("AEROF_PIPE_CHUNKS")) {
           const int v = std::atoi(env);
-          if (v >= 2 && v <= 32) m.pipeK = v;
+          if (v >= 2 && v <= 32) w.assign(v, 1.0);
         }
+        if (const char* env = std::getenv("AEROF_PIPE_WEIGHTS")) {
+          std::vector<double> v;
+          for (const char* q = env; *q;) {
+            char* e = nullptr;
+            const double x = std::strtod(q, &e);
+            if (e == q || !(x > 0.0)) { v.clear(); break; }
+            v.push_back(x);
+            q = *e == ',' ? e + 1 : e;
+            if (*e && *e != ',') { v.clear(); break; }
+          }
+          if (v.size() >= 2 && v.size() <= 32) w = v;
+        }
+        m.pipeK = (int)w.size();
         const int nb = hb.nblk, NBk = m.NB, K = m.pipeK;
-        auto chunk = [&](int o) { return (unsigned char)((long long)o * K / N); };
+        {
+          double tot = 0.0, acc = 0.0;
+          for (double x : w) tot += x;
+          m.pipe_rows.assign(K + 1, N);
+          m.pipe_rows[0] = 0;
+          for (int k = 1; k < K; ++k) {
+            acc += w[k - 1];
+            m.pipe_rows[k] = std::max(m.pipe_rows[k - 1], std::min(N, (int)std::llround(acc / tot * N)));
+          }
+        }
+        std::vector<unsigned char> row_chunk(N);
+        for (int k = 0; k < K; ++k)
+          for (int o = m.pipe_rows[k]; o < m.pipe_rows[k + 1]; ++o) row_chunk[o] = (unsigned char)k;
         m.h_st_prim.resize(N);
-        for (int n = 0; n < N; ++n) m.h_st_prim[n] = chunk(hb.n2o[n]);
+        for (int n = 0; n < N; ++n) m.h_st_prim[n] = row_chunk[hb.n2o[n]];
         m.h_st_grad = m.h_st_prim;
         for (int n = 0; n < N; ++n)
           for (int q = hb.nb2_ptr[n]; q < hb.nb2_ptr[n + 1]; ++q)
@@ -753,6 +782,7 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
     AEROF_CUDA(cudaStreamSynchronize(s));
     c->n_owned = N;
     c->has_mesh = true;
+    galerkin_reserve(c);
     return AEROF_OK;
   });
 }

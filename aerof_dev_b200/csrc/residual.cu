@@ -1221,14 +1221,16 @@ int residual_dev(aerof_gpu_ctx* c, const double* dU, double* dR, bool sync) {
 // takes chunk c of R out after stage c + 1; its rows whose assembly runs in
 // a later stage (their block depends on rows further on) are written again
 // after the last stage, once that chunk's copy has landed, by a kernel
-// storing into R through its device address.  The conversion runs per node (k_prim_nodes), the gradients per
-// block (k_grad_pipe) or per node (k_grad_nodes, with the block kernel's
-// lanes and order), the fluxes and assembly per block (k_fv_blocked,
-// k_fv_nodes_b with the boundary fluxes of k_face_flux inside): the same
-// arithmetic as residual_blocked_dev, so the same residual bit for bit.  Used for page-locked host U and R with
-// the blocked kernel, failsafe off, no viscous term and timers off, on
-// meshes of at least kPipeMinNodes nodes; otherwise aerof_gpu_residual
-// stages the arrays around one residual_dev.
+// storing into R through its device address.  The conversion runs per
+// node (k_prim_nodes), the gradients per block (k_grad_pipe) or per node
+// (k_grad_nodes, with the block kernel's lanes and order), the fluxes and
+// assembly per block (k_fv_blocked, k_fv_nodes_b with the boundary fluxes
+// of k_face_flux inside): the same arithmetic as residual_blocked_dev, so
+// the same residual bit for bit.  Each stage's kernels are replayed as one
+// CUDA graph.  Used for page-locked host U and R with the blocked kernel,
+// failsafe off, no viscous term and timers off, on meshes of at least
+// kPipeMinNodes nodes; otherwise aerof_gpu_residual stages the arrays
+// around one residual_dev.
 constexpr int kPipeMinNodes = 1 << 17;
 
 // page-locked host memory (with its device address when dev is given)
@@ -1246,8 +1248,6 @@ static bool pinned_host(const void* p, void** dev = nullptr) {
   return true;
 }
 
-// first caller row of chunk k of K (rows o with floor(o K / N) == k)
-static size_t pipe_row0(size_t N, int K, int k) { return ((size_t)k * N + K - 1) / K; }
 
 // the edge-flux kernel of residual_blocked_dev for this mesh
 static decltype(&k_fv_blocked<256, 2>) pipe_fv_kernel(const DeviceMesh& m) {
@@ -1314,12 +1314,14 @@ static ResidualPipe& pipe_for(aerof_gpu_ctx* c) {
     p->off[kind * (K + 1) + K] = (int)lists.size();
   }
   if (lists.empty()) lists.push_back(0);
-  // chunk c of R goes out after stage c + 1; its rows assembled later are
-  // the late rows
+  // chunk c of R goes out after stage c + lag (lag 1; tuning knob
+  // AEROF_PIPE_OUT_LAG, 0-2); its rows assembled later are the late rows
+  int lag = 1;
+  if (const char* env = std::getenv("AEROF_PIPE_OUT_LAG")) lag = std::min(std::max(std::atoi(env), 0), 2);
   p->out_stage.assign(K, 0);
-  for (int k = 0; k < K; ++k) p->out_stage[k] = std::min(k + 1, K - 1);
+  for (int k = 0; k < K; ++k) p->out_stage[k] = std::min(k + lag, K - 1);
   for (int k = 0; k < K; ++k) {
-    const size_t r0 = pipe_row0(m.N, K, k), r1 = pipe_row0(m.N, K, k + 1);
+    const size_t r0 = m.pipe_rows[k], r1 = m.pipe_rows[k + 1];
     for (size_t o = r0; o < r1; ++o)
       if (m.h_st_node[m.h_o2n[o] / m.NB] > p->out_stage[k]) p->h_late.push_back((int)o);
   }
@@ -1332,17 +1334,16 @@ static ResidualPipe& pipe_for(aerof_gpu_ctx* c) {
   return *c->pipe;
 }
 
-// Queue the whole overlapped residual of U into R on c->stream and the
-// pipe's copy streams (joined back into c->stream at the end); Rdev is R's
-// device address (for the late rows); the unphysical count goes to
-// p.h_bad.
-static void pipelined_enqueue(aerof_gpu_ctx* c, ResidualPipe& p, const double* U, double* R, double* Rdev) {
+// The kernels of stage st of the overlapped residual, on stream s: the
+// nodes converted in the stage, their gradients (per block where a whole
+// block's gradients fall in the stage, else per node), the edge fluxes and
+// the assembly (boundary fluxes inside) of the blocks the stage completes.
+static void stage_kernels(aerof_gpu_ctx* c, ResidualPipe& p, int st, cudaStream_t s) {
   DeviceMesh& m = c->mesh;
   const int rec = c->cfg.reconstruction;
   const bool grad = rec != AEROF_REC_CONSTANT;
   const int K = p.K;
   const Gas g = make_gas(c->cfg.gamma);
-  cudaStream_t s = c->stream;
   int* cnt = counters(c);
   double* dU = c->s.Ustage.p;
   double* dR = c->s.Rstage.p;
@@ -1355,7 +1356,111 @@ static void pipelined_enqueue(aerof_gpu_ctx* c, ResidualPipe& p, const double* U
   auto gp = L == 4 ? k_grad_pipe<4> : L == 2 ? k_grad_pipe<2> : k_grad_pipe<1>;
   const GradStage gst = grad_stage(m);
   const size_t gsmem = (size_t)2 * gst.size * sizeof(double);
-  const int ggrid = p.ggrid;
+  const int* lists = p.lists.p;
+  auto seg = [&](int kind, int& count) {
+    const int a = p.off[kind * (K + 1) + st];
+    count = p.off[kind * (K + 1) + st + 1] - a;
+    return lists + a;
+  };
+  int nl = 0;
+  const int* lp = seg(0, nl);
+  if (nl) {
+    k_prim_nodes<<<grid_for(nl, kBlock), kBlock, 0, s>>>(lp, nl, g, m.n2o.p, dU, m.P2.p);
+    AEROF_LAUNCH_CHECK();
+  }
+  lp = seg(1, nl);
+  if (nl && grad) {
+    gp<<<std::min(nl, p.ggrid), kBlock, gsmem, s>>>(m.N, m.NB, nl, m.maxH, m.maxLp, gst, m.P2.p, m.W2.p,
+                                                    m.nb2_ptr.p, m.lpad.p, m.hpad.p, nullptr, c->s.G2.p, lp);
+    AEROF_LAUNCH_CHECK();
+  }
+  lp = seg(4, nl);
+  if (nl && grad) {
+    gk<<<grid_for((size_t)nl * L, kBlock), kBlock, 0, s>>>(lp, nl, m.N, m.P2.p, m.W2.p, m.nb2_ptr.p, m.nb2_node.p,
+                                                            c->s.G2.p);
+    AEROF_LAUNCH_CHECK();
+  }
+  lp = seg(2, nl);
+  if (nl) {
+    fvk<<<nl, 256, fsmem, s>>>(m.N, m.E, m.NB, g, rec, c->cfg.beta, 0, m.bl.p, m.bnorm.p, m.beptr.p, m.hfptr.p,
+                               m.hfpad.p, m.maxHf, m.P2.p, c->s.G2.p, m.lptr.p, m.lidx.p, m.xslot.p, c->s.part.p,
+                               c->s.spill.p, c->s.tag.p, cnt, lp);
+    AEROF_LAUNCH_CHECK();
+  }
+  lp = seg(3, nl);
+  if (nl) {
+    // the boundary fluxes inside the assembly (one launch instead of a
+    // small face kernel per stage)
+    k_fv_nodes_b<true><<<grid_for((size_t)nl * m.NB, kBlock), kBlock, 0, s>>>(
+        m.N, g, m.n2o.p, c->s.part.p, m.xin_ptr.p, c->s.spill.p, m.bnf_ptr.p, m.bnf_ent.p, nullptr, m.F, m.Ubd.p,
+        m.fcode.p, m.fnrm.p, m.P2.p, m.vol2.p, dR, lp, nl, m.NB);
+    AEROF_LAUNCH_CHECK();
+  }
+}
+
+// The stages' kernels captured once as graphs (they touch device buffers
+// only, so one capture serves every U and R).  False when s cannot be
+// captured (the legacy default stream, or a capture already running).
+static bool pipe_graphs(aerof_gpu_ctx* c, ResidualPipe& p, cudaStream_t s) {
+  if (!p.stage_exec.empty()) return true;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  AEROF_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusNone || s == cudaStreamLegacy || s == nullptr) return false;
+  std::vector<cudaGraphExec_t> ex(p.K, nullptr);
+  std::vector<long long> nk(p.K, 0);
+  auto drop = [&]() {
+    for (auto e : ex)
+      if (e) cudaGraphExecDestroy(e);
+  };
+  for (int st = 0; st < p.K; ++st) {
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      drop();
+      return false;
+    }
+    cudaGraph_t gph = nullptr;
+    const long long l0 = g_launch_count.load();
+    try {
+      stage_kernels(c, p, st, s);
+    } catch (...) {
+      cudaStreamEndCapture(s, &gph);
+      if (gph) cudaGraphDestroy(gph);
+      cudaGetLastError();
+      drop();
+      throw;
+    }
+    // launches are counted when the graph runs
+    nk[st] = g_launch_count.load() - l0;
+    g_launch_count.fetch_sub(nk[st]);
+    const bool ok = cudaStreamEndCapture(s, &gph) == cudaSuccess && gph &&
+                    cudaGraphInstantiate(&ex[st], gph, 0) == cudaSuccess;
+    if (gph) cudaGraphDestroy(gph);
+    if (!ok) {
+      cudaGetLastError();
+      drop();
+      return false;
+    }
+  }
+  p.stage_exec = ex;
+  p.stage_launches = nk;
+  return true;
+}
+
+// The overlapped residual of U into R, queued on c->stream and the pipe's
+// copy streams (joined back into c->stream at the end): the copies of U's
+// chunks back to back on one stream, each stage's kernels (one graph, or
+// launch by launch) on c->stream once its chunk has landed, the copies of
+// R's chunks on the other stream as their stages complete, then the late
+// rows.  Rdev is R's device address (for the late rows); the unphysical
+// count goes to p.h_bad.
+static void pipelined_enqueue(aerof_gpu_ctx* c, ResidualPipe& p, const double* U, double* R, double* Rdev,
+                              bool graphs) {
+  DeviceMesh& m = c->mesh;
+  const int K = p.K;
+  cudaStream_t s = c->stream;
+  int* cnt = counters(c);
+  double* dU = c->s.Ustage.p;
+  double* dR = c->s.Rstage.p;
   AEROF_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * 2, s));
   // the copy streams start after the work already queued on s (which may
   // still read Ustage or write Rstage)
@@ -1363,60 +1468,29 @@ static void pipelined_enqueue(aerof_gpu_ctx* c, ResidualPipe& p, const double* U
   AEROF_CUDA(cudaStreamWaitEvent(p.sin, p.ev_go, 0));
   AEROF_CUDA(cudaStreamWaitEvent(p.sout, p.ev_go, 0));
   for (int k = 0; k < K; ++k) {
-    const size_t r0 = pipe_row0(m.N, K, k), r1 = pipe_row0(m.N, K, k + 1);
+    const size_t r0 = m.pipe_rows[k], r1 = m.pipe_rows[k + 1];
     if (r1 > r0)
       AEROF_CUDA(cudaMemcpyAsync(dU + 5 * r0, U + 5 * r0, 5 * (r1 - r0) * sizeof(double), cudaMemcpyHostToDevice,
                                  p.sin));
     AEROF_CUDA(cudaEventRecord(p.ev_in[k], p.sin));
   }
-  const int* lists = p.lists.p;
   for (int st = 0; st < K; ++st) {
     AEROF_CUDA(cudaStreamWaitEvent(s, p.ev_in[st], 0));
-    auto seg = [&](int kind, int& count) {
-      const int a = p.off[kind * (K + 1) + st];
-      count = p.off[kind * (K + 1) + st + 1] - a;
-      return lists + a;
-    };
-    int nl = 0;
-    const int* lp = seg(0, nl);
-    if (nl) {
-      k_prim_nodes<<<grid_for(nl, kBlock), kBlock, 0, s>>>(lp, nl, g, m.n2o.p, dU, m.P2.p);
-      AEROF_LAUNCH_CHECK();
-    }
-    lp = seg(1, nl);
-    if (nl && grad) {
-      gp<<<std::min(nl, ggrid), kBlock, gsmem, s>>>(m.N, m.NB, nl, m.maxH, m.maxLp, gst, m.P2.p, m.W2.p, m.nb2_ptr.p,
-                                                    m.lpad.p, m.hpad.p, nullptr, c->s.G2.p, lp);
-      AEROF_LAUNCH_CHECK();
-    }
-    lp = seg(4, nl);
-    if (nl && grad) {
-      gk<<<grid_for((size_t)nl * L, kBlock), kBlock, 0, s>>>(lp, nl, m.N, m.P2.p, m.W2.p, m.nb2_ptr.p, m.nb2_node.p,
-                                                              c->s.G2.p);
-      AEROF_LAUNCH_CHECK();
-    }
-    lp = seg(2, nl);
-    if (nl) {
-      fvk<<<nl, 256, fsmem, s>>>(m.N, m.E, m.NB, g, rec, c->cfg.beta, 0, m.bl.p, m.bnorm.p, m.beptr.p, m.hfptr.p,
-                                 m.hfpad.p, m.maxHf, m.P2.p, c->s.G2.p, m.lptr.p, m.lidx.p, m.xslot.p, c->s.part.p,
-                                 c->s.spill.p, c->s.tag.p, cnt, lp);
-      AEROF_LAUNCH_CHECK();
-    }
-    lp = seg(3, nl);
-    if (nl) {
-      // the boundary fluxes inside the assembly (one launch instead of a
-      // small face kernel per stage)
-      k_fv_nodes_b<true><<<grid_for((size_t)nl * m.NB, kBlock), kBlock, 0, s>>>(
-          m.N, g, m.n2o.p, c->s.part.p, m.xin_ptr.p, c->s.spill.p, m.bnf_ptr.p, m.bnf_ent.p, nullptr, m.F, m.Ubd.p,
-          m.fcode.p, m.fnrm.p, m.P2.p, m.vol2.p, dR, lp, nl, m.NB);
-      AEROF_LAUNCH_CHECK();
+    if (graphs) {
+      AEROF_CUDA(cudaGraphLaunch(p.stage_exec[st], s));
+      g_launch_count.fetch_add(p.stage_launches[st]);
+    } else {
+      stage_kernels(c, p, st, s);
     }
     AEROF_CUDA(cudaEventRecord(p.ev_stage[st], s));
+  }
+  // the copies of R's chunks as their stages complete
+  for (int st = 0; st < K; ++st) {
     // every copy queued so far (the chunks that can hold late rows)
     if (st == K - 1) AEROF_CUDA(cudaEventRecord(p.ev_pre, p.sout));
     for (int k = 0; k < K; ++k) {
       if (p.out_stage[k] != st) continue;
-      const size_t r0 = pipe_row0(m.N, K, k), r1 = pipe_row0(m.N, K, k + 1);
+      const size_t r0 = m.pipe_rows[k], r1 = m.pipe_rows[k + 1];
       AEROF_CUDA(cudaStreamWaitEvent(p.sout, p.ev_stage[st], 0));
       if (r1 > r0)
         AEROF_CUDA(cudaMemcpyAsync(R + 5 * r0, dR + 5 * r0, 5 * (r1 - r0) * sizeof(double), cudaMemcpyDeviceToHost,
@@ -1456,54 +1530,12 @@ static bool residual_host_pipelined(aerof_gpu_ctx* c, const double* U, double* R
   c->s.part.ensure(5 * (size_t)m.N);
   c->s.spill.ensure(5 * (size_t)std::max(m.nX, 1));
   counters(c);
-  // The call's ~40 launches interleave with copies that saturate the host
-  // link in both directions, which stretches the gaps between launches
-  // that the host submits; as one graph (captured once per U, R and stream,
-  // then replayed) they are submitted at once.  A stream that cannot be
-  // captured (the legacy default stream) takes the direct path.
-  if (!(p.exec && p.gU == U && p.gR == R && p.gs == s)) {
-    p.drop_graph();
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    AEROF_CUDA(cudaStreamIsCapturing(s, &cs));
-    bool captured = false;
-    if (cs == cudaStreamCaptureStatusNone && s != cudaStreamLegacy && s != nullptr &&
-        cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-      cudaGraph_t gph = nullptr;
-      const long long l0 = g_launch_count.load();
-      try {
-        pipelined_enqueue(c, p, U, R, static_cast<double*>(Rdev));
-        // launches are counted when the graph runs
-        p.launches = g_launch_count.load() - l0;
-        g_launch_count.fetch_sub(p.launches);
-      } catch (...) {
-        cudaStreamEndCapture(s, &gph);
-        if (gph) cudaGraphDestroy(gph);
-        cudaGetLastError();
-        throw;
-      }
-      if (cudaStreamEndCapture(s, &gph) == cudaSuccess && gph) {
-        cudaGraphExec_t ex = nullptr;
-        if (cudaGraphInstantiate(&ex, gph, 0) == cudaSuccess) {
-          p.graph = gph;
-          p.exec = ex;
-          p.gU = U;
-          p.gR = R;
-          p.gs = s;
-          captured = true;
-        } else {
-          cudaGraphDestroy(gph);
-        }
-      }
-      cudaGetLastError();
-    }
-    if (!captured) {
-      pipelined_enqueue(c, p, U, R, static_cast<double*>(Rdev));
-    }
-  }
-  if (p.exec) {
-    AEROF_CUDA(cudaGraphLaunch(p.exec, s));
-    g_launch_count.fetch_add(p.launches);
-  }
+  // Each stage's ~5 kernels are one graph: launched one by one while the
+  // copies saturate the host link, dependent kernels wait 5-9 us for their
+  // launch commands.  The copies stay outside the graphs, in their own
+  // streams, so that nothing holds them back.
+  const bool graphs = pipe_graphs(c, p, s);
+  pipelined_enqueue(c, p, U, R, static_cast<double*>(Rdev), graphs);
   AEROF_CUDA(cudaStreamSynchronize(s));
   bad = *p.h_bad;
   c->s.p2g2_valid = true;

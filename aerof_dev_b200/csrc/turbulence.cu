@@ -12,9 +12,10 @@
 // fluxes in ascending-neighbour order and the subface fluxes in face order,
 // times 1/ctrlVol.  Galerkin term (FemEquationTermSA::computeVolumeTerm,
 // FemEquationTermDesc.C:669-787, assembled as ElemTet::computeGalerkinTerm,
-// ElemTet.C:99-114): one thread per node walks the node's tets in tet order
-// and adds vol (r . dN_j) - vol/4 s of each, divided by the control
-// volume.  Every sum is a gather in a fixed order (no atomics on doubles).
+// ElemTet.C:99-114): one thread per tet forms vol (r . dN_j) - vol/4 s for
+// each of its four nodes, then each node sums its tets' shares in tet order
+// and adds the sum divided by the control volume.  Every sum is a gather in
+// a fixed order (no atomics on doubles).
 #include "common.cuh"
 #include "physics.cuh"
 
@@ -193,14 +194,13 @@ __global__ void k_node_residual6(int N, int E, const int* __restrict__ nbr_ptr, 
 
 // P1 shape-function gradients of tet nd (ElemTet::computeGradientP1Function,
 // ElemTetCore.C:1961-2010); returns the volume.
-__device__ __forceinline__ double p1_grad6(const double* __restrict__ X, const int* nd, double g[4][3]) {
+__device__ __forceinline__ double p1_grad6(const double x[4][3], double g[4][3]) {
   double jac[3][3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const double x0 = X[3 * (size_t)nd[0] + a];
-    jac[a][0] = X[3 * (size_t)nd[1] + a] - x0;
-    jac[a][1] = X[3 * (size_t)nd[2] + a] - x0;
-    jac[a][2] = X[3 * (size_t)nd[3] + a] - x0;
+    jac[a][0] = x[1][a] - x[0][a];
+    jac[a][1] = x[2][a] - x[0][a];
+    jac[a][2] = x[3][a] - x[0][a];
   }
   const double dOmega = jac[0][0] * (jac[1][1] * jac[2][2] - jac[1][2] * jac[2][1]) +
                         jac[1][0] * (jac[0][2] * jac[2][1] - jac[0][1] * jac[2][2]) +
@@ -220,37 +220,38 @@ __device__ __forceinline__ double p1_grad6(const double* __restrict__ X, const i
   return (1.0 / 6.0) * dOmega;
 }
 
-// R[i] += (sum over the node's tets of its SA Galerkin share) / vol[i]
-__global__ void k_galerkin_sa(int N, Gas gs, SADev sp, const double* __restrict__ X, const int* __restrict__ tets,
-                              const int* __restrict__ nt_ptr, const int* __restrict__ nt_tet,
-                              const double* __restrict__ V, const double* __restrict__ d2wall,
-                              const double* __restrict__ vol, double* __restrict__ R) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  const double invgam1 = gs.invgam1, cp = gs.gam * gs.invgam1;
-  const double twothird = 2.0 / 3.0, sixth = 1.0 / 6.0;
-  double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int q = nt_ptr[i]; q < nt_ptr[i + 1]; ++q) {
-    const int tl = nt_tet[q];
-    const int t = tl >> 2, kj = tl & 3;
-    int nd[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) nd[k] = tets[4 * (size_t)t + k];
-    double g[4][3];
-    const double tv = p1_grad6(X, nd, g);
-    double u[4][3], T[4], rh[4], nu[4];
+// One thread per tet: node k's share of the tet's SA Galerkin term,
+// vol (r_1..5 . dN_k) - vol/4 s in the last component (component 0 of r
+// is zero), written as the record C[5 (4t + k) .. +4]; the block's records
+// are staged in shared memory (row stride 21 doubles: conflict-free) and
+// stored contiguously with evict-first stores (each record is read once,
+// by k_tet_gather).  Q: per-node records of k_sa_records
+template <int TB>
+__global__ void __launch_bounds__(TB) k_galerkin_sa_tets(int T, Gas gs, SADev sp, const int* __restrict__ tets,
+                                                         const double* __restrict__ Q, double* __restrict__ C) {
+  constexpr int REC = 20, RS = REC + 1;
+  __shared__ double st[TB * RS];
+  const int t0 = blockIdx.x * TB, t = t0 + threadIdx.x;
+  if (t < T) {
+    const double cp = gs.gam * gs.invgam1;
+    const double twothird = 2.0 / 3.0, sixth = 1.0 / 6.0;
+    const int4 q4 = *reinterpret_cast<const int4*>(tets + 4 * (size_t)t);
+    const int nd[4] = {q4.x, q4.y, q4.z, q4.w};
+    double u[4][3], Tn[4], rh[4], nu[4], dw[4], x[4][3];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const double* v = V + 6 * (size_t)nd[k];
-      rh[k] = v[0];
-      u[k][0] = v[1]; u[k][1] = v[2]; u[k][2] = v[3];
-      T[k] = invgam1 * v[4] / v[0];
-      nu[k] = v[5];
+      const double2* q = reinterpret_cast<const double2*>(Q + 12 * (size_t)nd[k]);
+      const double2 a = q[0], b = q[1], c = q[2], d = q[3], e = q[4];
+      rh[k] = a.x; u[k][0] = a.y; u[k][1] = b.x; u[k][2] = b.y;
+      Tn[k] = c.x; nu[k] = c.y; dw[k] = d.x;
+      x[k][0] = d.y; x[k][1] = e.x; x[k][2] = e.y;
     }
+    double g[4][3];
+    const double tv = p1_grad6(x, g);
     double ucg[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) ucg[a] = 0.25 * (u[0][a] + u[1][a] + u[2][a] + u[3][a]);
-    const double Tcg = 0.25 * (T[0] + T[1] + T[2] + T[3]);
+    const double Tcg = 0.25 * (Tn[0] + Tn[1] + Tn[2] + Tn[3]);
     double du[3][3], dT[3], dnu[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a)
@@ -258,7 +259,7 @@ __global__ void k_galerkin_sa(int N, Gas gs, SADev sp, const double* __restrict_
       for (int j = 0; j < 3; ++j) du[a][j] = g[0][j] * u[0][a] + g[1][j] * u[1][a] + g[2][j] * u[2][a] + g[3][j] * u[3][a];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      dT[j] = g[0][j] * T[0] + g[1][j] * T[1] + g[2][j] * T[2] + g[3][j] * T[3];
+      dT[j] = g[0][j] * Tn[0] + g[1][j] * Tn[1] + g[2][j] * Tn[2] + g[3][j] * Tn[3];
       dnu[j] = g[0][j] * nu[0] + g[1][j] * nu[1] + g[2][j] * nu[2] + g[3][j] * nu[3];
     }
     // laminar coefficients at the mean temperature (before 1/Re)
@@ -282,7 +283,7 @@ __global__ void k_galerkin_sa(int N, Gas gs, SADev sp, const double* __restrict_
     const double absmutilde = fabs(mutilde), maxmutilde = fmax(mutilde, 0.0);
     const double mu5 = sp.oosigma * (mul + absmutilde);
     double s5 = 0.0;
-    const double d2w = 0.25 * (d2wall[nd[0]] + d2wall[nd[1]] + d2wall[nd[2]] + d2wall[nd[3]]);
+    const double d2w = 0.25 * (dw[0] + dw[1] + dw[2] + dw[3]);
     if (d2w >= 1.e-15) {
       const double chi = fmax(mutilde / mul, 0.001);
       const double chi3 = chi * chi * chi;
@@ -326,26 +327,45 @@ __global__ void k_galerkin_sa(int N, Gas gs, SADev sp, const double* __restrict_
     tij[1][0] = tij[0][1];
     tij[2][0] = tij[0][2];
     tij[2][1] = tij[1][2];
-    double r[3][6];
+    double r[3][5];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      r[j][0] = 0.0;
-      r[j][1] = tij[0][j];
-      r[j][2] = tij[1][j];
-      r[j][3] = tij[2][j];
-      r[j][4] = ucg[0] * tij[0][j] + ucg[1] * tij[1][j] + ucg[2] * tij[2][j] - (-kappa * dT[j]);
-      r[j][5] = mu5 * dnu[j];
+      r[j][0] = tij[0][j];
+      r[j][1] = tij[1][j];
+      r[j][2] = tij[2][j];
+      r[j][3] = ucg[0] * tij[0][j] + ucg[1] * tij[1][j] + ucg[2] * tij[2][j] - (-kappa * dT[j]);
+      r[j][4] = mu5 * dnu[j];
     }
-    double gk[3];
+    double* row = st + threadIdx.x * RS;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) gk[a] = kj == 0 ? g[0][a] : kj == 1 ? g[1][a] : kj == 2 ? g[2][a] : g[3][a];
+    for (int kj = 0; kj < 4; ++kj) {
 #pragma unroll
-    for (int k = 0; k < 5; ++k) acc[k] += tv * (r[0][k] * gk[0] + r[1][k] * gk[1] + r[2][k] * gk[2]);
-    acc[5] += tv * ((r[0][5] * gk[0] + r[1][5] * gk[1] + r[2][5] * gk[2]) - 0.25 * s5);
+      for (int k = 0; k < 4; ++k) row[5 * kj + k] = tv * (r[0][k] * g[kj][0] + r[1][k] * g[kj][1] + r[2][k] * g[kj][2]);
+      row[5 * kj + 4] = tv * ((r[0][4] * g[kj][0] + r[1][4] * g[kj][1] + r[2][4] * g[kj][2]) - 0.25 * s5);
+    }
   }
-  const double iv = 1.0 / vol[i];
-#pragma unroll
-  for (int k = 0; k < 6; ++k) R[6 * (size_t)i + k] += acc[k] * iv;
+  __syncthreads();
+  const int cnt = min(TB, T - t0) * REC;
+  double* out = C + (size_t)t0 * REC;
+  for (int f = threadIdx.x; f < cnt; f += TB) __stcs(out + f, st[(f / REC) * RS + (f % REC)]);
+}
+
+// Per-node records of the SA Galerkin term: (rho, u, v, w, T, nu~, d2wall,
+// x, y, z, 0, 0) with T = p / ((gamma - 1) rho), formed once per node
+// instead of once per (tet, vertex); V: primitive records of k_prim6
+__global__ void k_sa_records(int N, Gas g, const double* __restrict__ V, const double* __restrict__ X,
+                             const double* __restrict__ d2wall, double* __restrict__ Q) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double* v = V + 6 * (size_t)i;
+  const double* xi = X + 3 * (size_t)i;
+  double2* q = reinterpret_cast<double2*>(Q + 12 * (size_t)i);
+  q[0] = make_double2(v[0], v[1]);
+  q[1] = make_double2(v[2], v[3]);
+  q[2] = make_double2(g.invgam1 * v[4] / v[0], v[5]);
+  q[3] = make_double2(d2wall[i], xi[0]);
+  q[4] = make_double2(xi[1], xi[2]);
+  q[5] = make_double2(0.0, 0.0);
 }
 
 static SADev sa_dev(const aerof_gpu_ctx* c) {
@@ -407,8 +427,16 @@ static int residual_sa_dev(aerof_gpu_ctx* c, const double* dU, double* dR) {
                                                       m.nf_face.p, m.faces.p, t.fbuf6.p, m.vol.p, dR);
   AEROF_LAUNCH_CHECK();
   if (c->visc.model != 0) {
-    k_galerkin_sa<<<grid_for(m.N, 128), 128, 0, s>>>(m.N, g, sa_dev(c), m.X.p, m.tets.p, m.nt_ptr.p, m.nt_tet.p,
-                                                     t.V6.p, t.d2wall.p, m.vol.p, dR);
+    t.tetc.ensure(20 * (size_t)std::max(m.T, 1));
+    t.q.ensure(12 * (size_t)m.N);
+    k_sa_records<<<grid_for(m.N, 256), 256, 0, s>>>(m.N, g, t.V6.p, m.X.p, t.d2wall.p, t.q.p);
+    AEROF_LAUNCH_CHECK();
+    if (m.T) {
+      k_galerkin_sa_tets<128><<<grid_for(m.T, 128), 128, 0, s>>>(m.T, g, sa_dev(c), m.tets.p, t.q.p, t.tetc.p);
+      AEROF_LAUNCH_CHECK();
+    }
+    k_tet_gather<5, 6, 1><<<grid_for(5 * (size_t)m.N, 256), 256, 0, s>>>(m.N, m.nt_ptr.p, m.nt_tet.p, t.tetc.p,
+                                                                        m.vol.p, dR);
     AEROF_LAUNCH_CHECK();
   }
   int bad = 0;

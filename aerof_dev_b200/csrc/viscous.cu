@@ -6,15 +6,16 @@
 // Sutherland, ViscoFcn.h:46-103), constant-Prandtl conductivity
 // (ThermalCondFcn.h:52-75).
 //
-// One thread per node walks the node's tets in ascending tet order (the
-// order in which the reference's element loop adds into the node) and, per
-// tet, recomputes the P1 shape-function gradients from the coordinates
-// (ElemTet::computeGradientP1Function, ElemTetCore.C:1961-2010), the
-// velocity and temperature gradients, the transport coefficients at the
-// tet's mean temperature, the stress tensor and heat flux, and the node's
-// share vol (r_0 dN_x + r_1 dN_y + r_2 dN_z); the sum, divided by the
-// control volume, is added to R.  Deterministic (a gather, no atomics) and
-// allocation-free; each tet is evaluated by its four nodes.
+// One thread per tet computes the P1 shape-function gradients from the
+// coordinates (ElemTet::computeGradientP1Function, ElemTetCore.C:1961-2010),
+// the velocity and temperature gradients, the transport coefficients at the
+// tet's mean temperature, the stress tensor and heat flux, and each of its
+// four nodes' shares vol (r_0 dN_x + r_1 dN_y + r_2 dN_z), stored per
+// (tet, vertex).  A gather then sums each node's shares in ascending tet
+// order (the order in which the reference's element loop adds into the
+// node) and adds the sum divided by the control volume to R.  Deterministic
+// (no atomics); the per-tet buffer is reserved at set-up, so a residual
+// call allocates nothing.
 #include "common.cuh"
 #include "physics.cuh"
 
@@ -25,12 +26,7 @@ struct ViscDev {
   double ooreynolds, ooprandtl, bulk, alpha, Ts;
 };
 
-__device__ __forceinline__ double p1_grad(const double* __restrict__ X, const int* nd, double g[4][3]) {
-  double x[4][3];
-#pragma unroll
-  for (int k = 0; k < 4; ++k)
-#pragma unroll
-    for (int a = 0; a < 3; ++a) x[k][a] = X[3 * (size_t)nd[k] + a];
+__device__ __forceinline__ double p1_grad(const double x[4][3], double g[4][3]) {
   double jac[3][3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -56,43 +52,44 @@ __device__ __forceinline__ double p1_grad(const double* __restrict__ X, const in
   return (1.0 / 6.0) * dOmega;
 }
 
-// R[i] += (sum over the node's tets of its Galerkin share) / vol[i];
-// P: node records (V, X) in caller numbering
-__global__ void k_galerkin_nodes(int N, Gas gs, ViscDev vp, const double* __restrict__ X,
-                                 const int* __restrict__ tets, const int* __restrict__ nt_ptr,
-                                 const int* __restrict__ nt_tet, const double* __restrict__ P,
-                                 const double* __restrict__ vol, double* __restrict__ R) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  const double invgam1 = gs.invgam1, cp = gs.gam * gs.invgam1;
-  const double twothird = 2.0 / 3.0;
-  double acc[5] = {0, 0, 0, 0, 0};
-  for (int q = nt_ptr[i]; q < nt_ptr[i + 1]; ++q) {
-    const int tl = nt_tet[q];
-    const int t = tl >> 2, kj = tl & 3;
-    int nd[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) nd[k] = tets[4 * (size_t)t + k];
-    double g[4][3];
-    const double tv = p1_grad(X, nd, g);
-    double u[4][3], T[4];
+// One thread per tet: node k's share of the tet's Galerkin term,
+// vol (r_1..4 . dN_k) (component 0 of r is zero), written as the record
+// C[4 (4t + k) .. +3].  The block's records are staged in shared memory
+// (row stride 17 doubles: conflict-free) and stored contiguously with
+// evict-first stores (each record is read once, by k_tet_gather).
+// Q: per-node records (u, v, w, T, x, y, z, 0) of k_visc_records
+template <int TB>
+__global__ void __launch_bounds__(TB) k_galerkin_tets(int T, Gas gs, ViscDev vp, const int* __restrict__ tets,
+                                                      const double* __restrict__ Q, double* __restrict__ C) {
+  constexpr int REC = 16, RS = REC + 1;
+  __shared__ double st[TB * RS];
+  const int t0 = blockIdx.x * TB, t = t0 + threadIdx.x;
+  if (t < T) {
+    const double cp = gs.gam * gs.invgam1;
+    const double twothird = 2.0 / 3.0;
+    const int4 q4 = *reinterpret_cast<const int4*>(tets + 4 * (size_t)t);
+    const int nd[4] = {q4.x, q4.y, q4.z, q4.w};
+    double u[4][3], Tn[4], x[4][3];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const double* v = P + 8 * (size_t)nd[k];
-      u[k][0] = v[1]; u[k][1] = v[2]; u[k][2] = v[3];
-      T[k] = invgam1 * v[4] / v[0];
+      const double2* q = reinterpret_cast<const double2*>(Q + 8 * (size_t)nd[k]);
+      const double2 a = q[0], b = q[1], c = q[2], d = q[3];
+      u[k][0] = a.x; u[k][1] = a.y; u[k][2] = b.x; Tn[k] = b.y;
+      x[k][0] = c.x; x[k][1] = c.y; x[k][2] = d.x;
     }
+    double g[4][3];
+    const double tv = p1_grad(x, g);
     double ucg[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) ucg[a] = 0.25 * (u[0][a] + u[1][a] + u[2][a] + u[3][a]);
-    const double Tcg = 0.25 * (T[0] + T[1] + T[2] + T[3]);
+    const double Tcg = 0.25 * (Tn[0] + Tn[1] + Tn[2] + Tn[3]);
     double du[3][3], dT[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
       for (int j = 0; j < 3; ++j) du[a][j] = g[0][j] * u[0][a] + g[1][j] * u[1][a] + g[2][j] * u[2][a] + g[3][j] * u[3][a];
 #pragma unroll
-    for (int j = 0; j < 3; ++j) dT[j] = g[0][j] * T[0] + g[1][j] * T[1] + g[2][j] * T[2] + g[3][j] * T[3];
+    for (int j = 0; j < 3; ++j) dT[j] = g[0][j] * Tn[0] + g[1][j] * Tn[1] + g[2][j] * Tn[2] + g[3][j] * Tn[3];
     double mu, lambda;
     if (vp.model == 2) {
       const double Ta = vp.alpha * Tcg;
@@ -117,51 +114,71 @@ __global__ void k_galerkin_nodes(int N, Gas gs, ViscDev vp, const double* __rest
     tij[1][0] = tij[0][1];
     tij[2][0] = tij[0][2];
     tij[2][1] = tij[1][2];
-    double r[3][5];
+    double r[3][4];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      r[j][0] = 0.0;
-      r[j][1] = tij[0][j];
-      r[j][2] = tij[1][j];
-      r[j][3] = tij[2][j];
-      r[j][4] = ucg[0] * tij[0][j] + ucg[1] * tij[1][j] + ucg[2] * tij[2][j] - (-kappa * dT[j]);
+      r[j][0] = tij[0][j];
+      r[j][1] = tij[1][j];
+      r[j][2] = tij[2][j];
+      r[j][3] = ucg[0] * tij[0][j] + ucg[1] * tij[1][j] + ucg[2] * tij[2][j] - (-kappa * dT[j]);
     }
-    double gk[3];
+    double* row = st + threadIdx.x * RS;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) gk[a] = kj == 0 ? g[0][a] : kj == 1 ? g[1][a] : kj == 2 ? g[2][a] : g[3][a];
+    for (int kj = 0; kj < 4; ++kj)
 #pragma unroll
-    for (int k = 0; k < 5; ++k) acc[k] += tv * (r[0][k] * gk[0] + r[1][k] * gk[1] + r[2][k] * gk[2]);
+      for (int k = 0; k < 4; ++k) row[4 * kj + k] = tv * (r[0][k] * g[kj][0] + r[1][k] * g[kj][1] + r[2][k] * g[kj][2]);
   }
-  const double iv = 1.0 / vol[i];
-#pragma unroll
-  for (int k = 0; k < 5; ++k) R[5 * (size_t)i + k] += acc[k] * iv;
+  __syncthreads();
+  const int cnt = min(TB, T - t0) * REC;
+  double* out = C + (size_t)t0 * REC;
+  for (int f = threadIdx.x; f < cnt; f += TB) __stcs(out + f, st[(f / REC) * RS + (f % REC)]);
 }
 
-// k_prim is defined in residual.cu; a local copy keeps the node records of
-// caller numbering current for the viscous term
-__global__ void k_prim_visc(int N, Gas g, const double* __restrict__ U, double* __restrict__ P) {
+// Per-node records of the Galerkin term: (u, v, w, T, x, y, z, 0) with
+// T = p / ((gamma - 1) rho) from VarFcnSGEuler::conservativeToPrimitive,
+// formed once per node instead of once per (tet, vertex)
+__global__ void k_visc_records(int N, Gas g, const double* __restrict__ U, const double* __restrict__ X,
+                               double* __restrict__ Q) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double u[5], v[5];
 #pragma unroll
   for (int k = 0; k < 5; ++k) u[k] = U[5 * (size_t)i + k];
   cons2prim(g, u, v);
-#pragma unroll
-  for (int k = 0; k < 5; ++k) P[8 * (size_t)i + k] = v[k];
+  double2* q = reinterpret_cast<double2*>(Q + 8 * (size_t)i);
+  q[0] = make_double2(v[1], v[2]);
+  q[1] = make_double2(v[3], g.invgam1 * v[4] / v[0]);
+  q[2] = make_double2(X[3 * (size_t)i], X[3 * (size_t)i + 1]);
+  q[3] = make_double2(X[3 * (size_t)i + 2], 0.0);
+}
+
+// the per-tet buffer of the Galerkin term, sized at set-up so that the
+// residual calls allocate nothing
+void galerkin_reserve(aerof_gpu_ctx* c) {
+  if (c->visc.model == 0 || !c->has_mesh) return;
+  c->s.tetc.ensure(16 * (size_t)std::max(c->mesh.T, 1));
+  c->s.viscq.ensure(8 * (size_t)c->mesh.N);
 }
 
 // R += G(U) / vol (R already holds the finite-volume residual divided by
-// the control volumes); no allocation
+// the control volumes): each tet evaluated once (k_galerkin_tets), then
+// each node sums its tets' shares in ascending tet order (k_tet_gather)
 void galerkin_add(aerof_gpu_ctx* c, const double* dU, double* dR) {
   if (c->visc.model == 0) return;
   DeviceMesh& m = c->mesh;
+  if (c->s.tetc.n < 16 * (size_t)m.T || c->s.viscq.n < 8 * (size_t)m.N)
+    throw ApiError{AEROF_ESTATE, "viscous term: per-tet buffer not reserved"};
   const Gas g = make_gas(c->cfg.gamma);
   ViscDev vp{c->visc.model, 1.0 / c->visc.reynolds_mu, 1.0 / c->visc.prandtl, c->visc.bulk_viscosity,
              c->visc.sutherland_alpha, c->visc.sutherland_Ts};
-  k_prim_visc<<<grid_for(m.N, 256), 256, 0, c->stream>>>(m.N, g, dU, m.P.p);
+  k_visc_records<<<grid_for(m.N, 256), 256, 0, c->stream>>>(m.N, g, dU, m.X.p, c->s.viscq.p);
   AEROF_LAUNCH_CHECK();
-  k_galerkin_nodes<<<grid_for(m.N, 128), 128, 0, c->stream>>>(m.N, g, vp, m.X.p, m.tets.p, m.nt_ptr.p, m.nt_tet.p,
-                                                             m.P.p, m.vol.p, dR);
+  if (m.T) {
+    k_galerkin_tets<128><<<grid_for(m.T, 128), 128, 0, c->stream>>>(m.T, g, vp, m.tets.p, c->s.viscq.p, c->s.tetc.p);
+    AEROF_LAUNCH_CHECK();
+  }
+  k_tet_gather<4, 5, 1><<<grid_for(4 * (size_t)m.N, 256), 256, 0, c->stream>>>(m.N, m.nt_ptr.p, m.nt_tet.p,
+                                                                                c->s.tetc.p, m.vol.p, dR);
   AEROF_LAUNCH_CHECK();
 }
 
@@ -175,6 +192,7 @@ extern "C" int aerof_gpu_set_viscosity(aerof_gpu_ctx* c, const aerof_viscous_par
     if (p->model != 0 && !(p->reynolds_mu > 0.0 && p->prandtl > 0.0)) return AEROF_EINVAL;
     if (p->model == 2 && !(p->sutherland_alpha > 0.0 && p->sutherland_Ts >= 0.0)) return AEROF_EINVAL;
     c->visc = *p;
+    galerkin_reserve(c);
     c->imp.precision = 0;
     c->h2.ready = false;
     return AEROF_OK;

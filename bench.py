@@ -816,10 +816,13 @@ def run_sa_residual(args):
     Rd = torch.empty_like(Ud)
     t_sa = timed_on(stream, lambda: sp.computeResidualSA(U6d, R6d), args.steps, args.warmup)
     t_lam = timed_on(stream, lambda: sp.computeResidual(Ud, Rd), args.steps, args.warmup)
+    ctx.set_viscosity(model=0)
+    t_inv = timed_on(stream, lambda: sp.computeResidual(Ud, Rd), args.steps, args.warmup)
     s = W.lattice_sizes(args.n)
     line = {"metric": METRIC, "workload": "sa_residual", "value": s["E"] / (t_sa * 1e-3) / 1e6,
             "unit": "Medges/s", "higher_is_better": True, "ms_per_eval": t_sa,
-            "laminar_ms_per_eval": t_lam, "sa_over_laminar": t_sa / t_lam,
+            "laminar_ms_per_eval": t_lam, "sa_over_laminar": t_sa / t_lam, "inviscid_ms_per_eval": t_inv,
+            "laminar_galerkin_ms": t_lam - t_inv,
             "config": {"workload": f"Spalart-Allmaras residual (6 variables, van Albada + LSQ + Roe, Sutherland "
                                    f"viscosity), {args.n}^3 jittered Kuhn tet mesh N={s['N']} E={s['E']}",
                        "organisation": "edge (thread per edge, per-node gather)"}}

@@ -219,8 +219,8 @@ def test_host_array_residual_overlapped_copies(gpu_lib, oracle_mod, rec):
     Rd, bad_d = sp.computeResidual(Ud)
     Uh = torch.from_numpy(U).pin_memory()
     Rh = torch.empty_like(Uh).pin_memory()
-    # new output arrays (a new schedule of the copies), then the same ones
-    # again (the recorded call replayed)
+    # new output arrays, then the same ones again (the stages' recorded
+    # kernels replayed with other copies around them)
     for k in range(4):
         if k < 2:
             Rh = torch.empty_like(Uh).pin_memory()

@@ -836,7 +836,8 @@ def run_e2e_timeline(args):
     """Device timeline of the residual of page-locked host arrays (the e2e
     call): three calls traced with CUPTI (torch.profiler), per call its span
     and, per kind of work, the summed device time of the copies in, the
-    copies out and the kernels (they overlap)."""
+    copies out and the kernels (they overlap); for the second call every
+    event as [kind, start us, duration us]."""
     import torch
     import aerof_dev_b200 as A
     from torch.profiler import ProfilerActivity, profile
@@ -878,9 +879,15 @@ def run_e2e_timeline(args):
                 kinds["kernel_us"] += d
         out.append({"span_us": t1 - t0, **{k: round(v, 1) for k, v in kinds.items()},
                     "kernels": sum(1 for e in c if "Memcpy" not in e.name and "Memset" not in e.name)})
+    def kind(name):
+        return "copy_in" if "HtoD" in name else "copy_out" if "DtoH" in name else name.split("(")[0][:48]
+    mid = calls[len(calls) // 2]
+    m0 = min(e.time_range.start for e in mid)
+    events = [[kind(e.name), round(e.time_range.start - m0, 1), round(e.time_range.end - e.time_range.start, 1)]
+              for e in mid]
     s = W.lattice_sizes(args.n)
     print(json.dumps({"metric": METRIC, "workload": "e2e_timeline", "n": args.n, "E": s["E"],
-                      "bytes_each_way": int(U.nbytes), "calls": out}), flush=True)
+                      "bytes_each_way": int(U.nbytes), "calls": out, "events": events}), flush=True)
     ctx.close()
     return 0
 

@@ -579,12 +579,10 @@ __global__ void __launch_bounds__(256, 1) k_a_fv_blocked(int N, int E, int NB, G
         const int src = bsrc[q];
         const size_t l = (size_t)(src & 0x7fffffff);
         const double sg = src < 0 ? -1.0 : 1.0;
-        geo[l] = sg * gn[0];
-        geo[(size_t)E + l] = sg * gn[1];
-        geo[2 * (size_t)E + l] = sg * gn[2];
-        geo[3 * (size_t)E + l] = sg * gdx0;
-        geo[4 * (size_t)E + l] = sg * gdx1;
-        geo[5 * (size_t)E + l] = sg * gdx2;
+        double2* ge = reinterpret_cast<double2*>(geo + 6 * l);
+        ge[0] = make_double2(sg * gn[0], sg * gn[1]);
+        ge[1] = make_double2(sg * gn[2], sg * gdx0);
+        ge[2] = make_double2(sg * gdx1, sg * gdx2);
       }
     }
   }
@@ -1119,8 +1117,14 @@ __global__ void __launch_bounds__(256) k_a_lsq_x(int N, const double* __restrict
 #pragma unroll
   for (int k = 0; k < 6; ++k) { w[k] = lsqW[(size_t)k * N + i]; r[k] = lsqR[(size_t)k * N + i]; }
   double gw[6] = {0, 0, 0, 0, 0, 0};
+  // the lane's first KM entries keep their pass-1 cotangents in shared
+  // memory for pass 2 (one store of gd each); further entries (nodes with
+  // more than 4 KM neighbours) store gd in pass 1 and add to it in pass 2
+  constexpr int KM = 4;
+  __shared__ double kg[KM * 3][256];
+  const int pb = nbr_ptr[i], pe = nbr_ptr[i + 1];
   // pass 1: through W(w, d)
-  for (int p = nbr_ptr[i] + lane; act && p < nbr_ptr[i + 1]; p += 4) {
+  for (int p = pb + lane, m = 0; act && p < pe; p += 4, ++m) {
     const double* pj = P + 8 * (size_t)nbr_node[p];
     const double d0 = pj[5] - pi[5], d1 = pj[6] - pi[6], d2 = pj[7] - pi[7];
     double gW0 = 0.0, gW1 = 0.0, gW2 = 0.0;
@@ -1147,7 +1151,11 @@ __global__ void __launch_bounds__(256) k_a_lsq_x(int N, const double* __restrict
     const double ge3 = w[2] * w[2] * ga3;
     gw[2] += 2.0 * e3 * w[2] * ga3;
     gd2 += ge3; gw[4] += -d1 * ge3; gd1 += -w[4] * ge3; gw[5] += d0 * ge3; gd0 += w[5] * ge3;
-    gd[3 * (size_t)p] = gd0; gd[3 * (size_t)p + 1] = gd1; gd[3 * (size_t)p + 2] = gd2;
+    if (m < KM) {
+      kg[3 * m][threadIdx.x] = gd0; kg[3 * m + 1][threadIdx.x] = gd1; kg[3 * m + 2][threadIdx.x] = gd2;
+    } else {
+      gd[3 * (size_t)p] = gd0; gd[3 * (size_t)p + 1] = gd1; gd[3 * (size_t)p + 2] = gd2;
+    }
   }
 #pragma unroll
   for (int o = 1; o < 4; o <<= 1)
@@ -1184,7 +1192,16 @@ __global__ void __launch_bounds__(256) k_a_lsq_x(int N, const double* __restrict
   gr[0] += -r12 / r11 * gr[1];
   gS[0] = 0.5 / r11 * gr[0];
   // pass 2: S = sum d d^T
-  for (int p = nbr_ptr[i] + lane; p < nbr_ptr[i + 1]; p += 4) {
+  for (int k = 0; k < KM; ++k) {
+    const int p = pb + lane + 4 * k;
+    if (p >= pe) break;
+    const double* pj = P + 8 * (size_t)nbr_node[p];
+    const double d0 = pj[5] - pi[5], d1 = pj[6] - pi[6], d2 = pj[7] - pi[7];
+    gd[3 * (size_t)p] = kg[3 * k][threadIdx.x] + (2.0 * d0 * gS[0] + d1 * gS[1] + d2 * gS[2]);
+    gd[3 * (size_t)p + 1] = kg[3 * k + 1][threadIdx.x] + (d0 * gS[1] + 2.0 * d1 * gS[3] + d2 * gS[4]);
+    gd[3 * (size_t)p + 2] = kg[3 * k + 2][threadIdx.x] + (d0 * gS[2] + d1 * gS[4] + 2.0 * d2 * gS[5]);
+  }
+  for (int p = pb + lane + 4 * KM; p < pe; p += 4) {
     const double* pj = P + 8 * (size_t)nbr_node[p];
     const double d0 = pj[5] - pi[5], d1 = pj[6] - pi[6], d2 = pj[7] - pi[7];
     gd[3 * (size_t)p] += 2.0 * d0 * gS[0] + d1 * gS[1] + d2 * gS[2];
@@ -1209,11 +1226,10 @@ __global__ void k_a_gvol(int N, const double* __restrict__ w, const double* __re
 //   edge dx in the reconstruction:  +-g_dx of incident edges
 //   tets: volume and dual-cell edge normals, forward mode in x_q's 3 directions
 //   boundary faces: face normals, forward mode in x_q's 3 directions
-__global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const int* __restrict__ tets,
-                             const int* __restrict__ tet_edge, const int* __restrict__ faces,
+__global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const int* __restrict__ faces,
                              const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_edge,
                              const int* __restrict__ nbr_tpos, const double* __restrict__ gd,
-                             const double* __restrict__ geo, int E, const int* __restrict__ nt_ptr,
+                             const double* __restrict__ geo, const int* __restrict__ nt_ptr,
                              const int* __restrict__ nt_tet, const int* __restrict__ nf_ptr,
                              const int* __restrict__ nf_face, const double* __restrict__ tg,
                              const double* __restrict__ gfn, double* __restrict__ gX);
@@ -1229,87 +1245,97 @@ namespace aerof {
 // (ElemTetCore.C:281-330), so g_xg1 = xg0 x g_c, g_xg0 = g_c x xg1 with
 // g_c = 1.5 s g_n, then a third to each vertex of the face and minus a
 // quarter to every vertex for the centroid.  tg[t][3 a + c].
-__global__ void k_a_tet_x(int T, const double* __restrict__ X, const int* __restrict__ tets,
-                          const int* __restrict__ tet_edge, const double* __restrict__ geo, int E,
-                          const double* __restrict__ gvol, double* __restrict__ tg) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= T) return;
-  const int* nd = tets + 4 * (size_t)t;
-  const double gvt = 0.25 * (gvol[nd[0]] + gvol[nd[1]] + gvol[nd[2]] + gvol[nd[3]]);
-  Vec3<double> x[4];
+template <int TB>
+__global__ void __launch_bounds__(TB) k_a_tet_x(int T, const double* __restrict__ X, const int* __restrict__ tets,
+                                                const int* __restrict__ tet_edge, const double* __restrict__ geo,
+                                                const double* __restrict__ gvol, double* __restrict__ tg) {
+  // the block's 12-double rows are staged in shared memory (row stride 13:
+  // conflict-free) and stored contiguously
+  __shared__ double st[TB * 13];
+  const int t0 = blockIdx.x * TB, t = t0 + threadIdx.x;
+  if (t < T) {
+    const int4 q4 = *reinterpret_cast<const int4*>(tets + 4 * (size_t)t);
+    const int nd[4] = {q4.x, q4.y, q4.z, q4.w};
+    const double gvt = 0.25 * (gvol[nd[0]] + gvol[nd[1]] + gvol[nd[2]] + gvol[nd[3]]);
+    Vec3<double> x[4];
 #pragma unroll
-  for (int v = 0; v < 4; ++v) x[v] = node_x(X, nd[v]);
-  const Vec3<double> e1 = x[1] - x[0], e2 = x[2] - x[0], e3 = x[3] - x[0];
-  const double sv = gvt / 6.0;
-  Vec3<double> g[4];
-  g[1] = scale(sv, cross(e2, e3));
-  g[2] = scale(sv, cross(e3, e1));
-  g[3] = scale(sv, cross(e1, e2));
-  g[0] = v3(0.0, 0.0, 0.0) - (g[1] + g[2] + g[3]);
-  const double third = 1.0 / 3.0;
-  Vec3<double> f[4];
-  f[0] = scale(third, x[0] + x[1] + x[2]);
-  f[1] = scale(third, x[0] + x[1] + x[3]);
-  f[2] = scale(third, x[0] + x[2] + x[3]);
-  f[3] = scale(third, x[1] + x[2] + x[3]);
-  const Vec3<double> gc0 = scale(0.25, x[0] + x[1] + x[2] + x[3]);
-  Vec3<double> gf[4] = {v3(0.0, 0.0, 0.0), v3(0.0, 0.0, 0.0), v3(0.0, 0.0, 0.0), v3(0.0, 0.0, 0.0)};
-  Vec3<double> gcen = v3(0.0, 0.0, 0.0);
+    for (int v = 0; v < 4; ++v) x[v] = node_x(X, nd[v]);
+    const Vec3<double> e1 = x[1] - x[0], e2 = x[2] - x[0], e3 = x[3] - x[0];
+    const double sv = gvt / 6.0;
+    Vec3<double> g[4];
+    g[1] = scale(sv, cross(e2, e3));
+    g[2] = scale(sv, cross(e3, e1));
+    g[3] = scale(sv, cross(e1, e2));
+    g[0] = v3(0.0, 0.0, 0.0) - (g[1] + g[2] + g[3]);
+    const double third = 1.0 / 3.0;
+    Vec3<double> f[4];
+    f[0] = scale(third, x[0] + x[1] + x[2]);
+    f[1] = scale(third, x[0] + x[1] + x[3]);
+    f[2] = scale(third, x[0] + x[2] + x[3]);
+    f[3] = scale(third, x[1] + x[2] + x[3]);
+    const Vec3<double> gc0 = scale(0.25, x[0] + x[1] + x[2] + x[3]);
+    Vec3<double> gf[4] = {v3(0.0, 0.0, 0.0), v3(0.0, 0.0, 0.0), v3(0.0, 0.0, 0.0), v3(0.0, 0.0, 0.0)};
+    Vec3<double> gcen = v3(0.0, 0.0, 0.0);
 #pragma unroll
-  for (int l = 0; l < 6; ++l) {
-    const int F0 = tet_edge_face(l, 0), F1 = tet_edge_face(l, 1);
-    const Vec3<double> xg0 = f[F0] - gc0, xg1 = f[F1] - gc0;
-    const size_t el = (size_t)tet_edge[6 * (size_t)t + l];
-    const double sl = nd[tet_edge_end(l, 0)] < nd[tet_edge_end(l, 1)] ? 1.5 : -1.5;
-    const Vec3<double> gcv = v3(sl * geo[el], sl * geo[(size_t)E + el], sl * geo[2 * (size_t)E + el]);
-    const Vec3<double> g1 = cross(xg0, gcv), g0 = cross(gcv, xg1);
-    gf[F0] = gf[F0] + g0;
-    gf[F1] = gf[F1] + g1;
-    gcen = gcen + g0 + g1;
+    for (int l = 0; l < 6; ++l) {
+      const int F0 = tet_edge_face(l, 0), F1 = tet_edge_face(l, 1);
+      const Vec3<double> xg0 = f[F0] - gc0, xg1 = f[F1] - gc0;
+      const size_t el = (size_t)tet_edge[6 * (size_t)t + l];
+      const double sl = nd[tet_edge_end(l, 0)] < nd[tet_edge_end(l, 1)] ? 1.5 : -1.5;
+      const double2 g01 = *reinterpret_cast<const double2*>(geo + 6 * el);
+      const Vec3<double> gcv = v3(sl * g01.x, sl * g01.y, sl * geo[6 * el + 2]);
+      const Vec3<double> g1 = cross(xg0, gcv), g0 = cross(gcv, xg1);
+      gf[F0] = gf[F0] + g0;
+      gf[F1] = gf[F1] + g1;
+      gcen = gcen + g0 + g1;
+    }
+    // face k holds every vertex but 3 - k
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      Vec3<double> s = v3(0.0, 0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (a != 3 - k) s = s + gf[k];
+      const Vec3<double> d = g[a] + scale(third, s) - scale(0.25, gcen);
+      st[13 * threadIdx.x + 3 * a] = d.x;
+      st[13 * threadIdx.x + 3 * a + 1] = d.y;
+      st[13 * threadIdx.x + 3 * a + 2] = d.z;
+    }
   }
-  // face k holds every vertex but 3 - k
-#pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    Vec3<double> s = v3(0.0, 0.0, 0.0);
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (a != 3 - k) s = s + gf[k];
-    const Vec3<double> d = g[a] + scale(third, s) - scale(0.25, gcen);
-    tg[12 * (size_t)t + 3 * a] = d.x;
-    tg[12 * (size_t)t + 3 * a + 1] = d.y;
-    tg[12 * (size_t)t + 3 * a + 2] = d.z;
-  }
+  __syncthreads();
+  const int cnt = 12 * min(TB, T - t0);
+  double* out = tg + 12 * (size_t)t0;
+  for (int f = threadIdx.x; f < cnt; f += TB) out[f] = st[13 * (f / 12) + f % 12];
 }
 
-__global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const int* __restrict__ tets,
-                             const int* __restrict__ tet_edge, const int* __restrict__ faces,
+__global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const int* __restrict__ faces,
                              const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_edge,
                              const int* __restrict__ nbr_tpos, const double* __restrict__ gd,
-                             const double* __restrict__ geo, int E, const int* __restrict__ nt_ptr,
+                             const double* __restrict__ geo, const int* __restrict__ nt_ptr,
                              const int* __restrict__ nt_tet, const int* __restrict__ nf_ptr,
                              const int* __restrict__ nf_face, const double* __restrict__ tg,
                              const double* __restrict__ gfn, double* __restrict__ gX) {
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= N) return;
-  double gx[3] = {0, 0, 0};
+  // three lanes per node, lane c summing component c (each in the order of
+  // the one-thread form: edges, tets, faces)
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= 3 * (long long)N) return;
+  const int q = (int)(j / 3), c = (int)(j - 3 * (long long)q);
+  double gx = 0.0;
   for (int p = nbr_ptr[q]; p < nbr_ptr[q + 1]; ++p) {
     const int e = nbr_edge[p];
     const size_t el = (size_t)(e & 0x7fffffff);
     const double s = e < 0 ? 1.0 : -1.0;  // dx = X_second - X_first
-#pragma unroll
-    for (int c = 0; c < 3; ++c) gx[c] += s * geo[(3 + c) * (size_t)E + el];
+    gx += s * geo[6 * el + 3 + c];
     if (rec != AEROF_REC_CONSTANT) {
       const size_t tp = (size_t)nbr_tpos[p];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) gx[c] += gd[3 * tp + c] - gd[3 * (size_t)p + c];
+      gx += gd[3 * tp + c] - gd[3 * (size_t)p + c];
     }
   }
   // tets: the per-tet vertex cotangents of k_a_tet_x
   for (int p = nt_ptr[q]; p < nt_ptr[q + 1]; ++p) {
     const size_t t = (size_t)(nt_tet[p] >> 2);
     const int a = nt_tet[p] & 3;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) gx[c] += tg[12 * t + 3 * a + c];
+    gx += tg[12 * t + 3 * a + c];
   }
   // boundary faces: n = (3 x02 x x01 + 3 x02 x x01) / 12 (FaceTriaCore.C:
   // 65-82) = x02 x x01 / 2, so g_x02 = x01 x g_n / 2, g_x01 = g_n x x02 / 2
@@ -1322,13 +1348,9 @@ __global__ void k_a_gather_x(int N, int rec, const double* __restrict__ X, const
     const Vec3<double> gn = v3(gfn[3 * (size_t)f], gfn[3 * (size_t)f + 1], gfn[3 * (size_t)f + 2]);
     const Vec3<double> g02 = scale(0.5, cross(x01, gn)), g01 = scale(0.5, cross(gn, x02));
     const Vec3<double> d = a == 2 ? g02 : (a == 1 ? g01 : v3(0.0, 0.0, 0.0) - (g02 + g01));
-    gx[0] += d.x;
-    gx[1] += d.y;
-    gx[2] += d.z;
+    gx += c == 0 ? d.x : (c == 1 ? d.y : d.z);
   }
-  gX[3 * (size_t)q] = gx[0];
-  gX[3 * (size_t)q + 1] = gx[1];
-  gX[3 * (size_t)q + 2] = gx[2];
+  gX[3 * (size_t)q + c] = gx;
 }
 
 // cotangents of the edge normals and dx out of the per-edge records of the
@@ -1337,7 +1359,7 @@ __global__ void k_a_geo_from_rec(int E, const double* __restrict__ erec, double*
   int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= E) return;
 #pragma unroll
-  for (int k = 0; k < 6; ++k) geo[(size_t)k * E + l] = erec[32 * (size_t)l + 20 + k];
+  for (int k = 0; k < 6; ++k) geo[6 * (size_t)l + k] = erec[32 * (size_t)l + 20 + k];
 }
 
 // (dR/dX)^T lambda for device state dU, cotangent dlam, into dgX [N][3];
@@ -1406,11 +1428,13 @@ void dRdX_T_dev(aerof_gpu_ctx* c, const double* dU, const double* dlam, double* 
     AEROF_LAUNCH_CHECK();
   }
   a.tg.ensure(12 * (size_t)std::max(m.T, 1));
-  k_a_tet_x<<<grid_for(m.T, kAB), kAB, 0, s>>>(m.T, m.X.p, m.tets.p, m.tet_edge.p, a.geo.p, m.E, a.gvol.p, a.tg.p);
-  AEROF_LAUNCH_CHECK();
-  k_a_gather_x<<<gn, kAB, 0, s>>>(m.N, rec, m.X.p, m.tets.p, m.tet_edge.p, m.faces.p, m.nbr_ptr.p, m.nbr_edge.p,
-                                  m.nbr_tpos.p, a.gd.p, a.geo.p, m.E, m.nt_ptr.p, m.nt_tet.p, m.nf_ptr.p,
-                                  m.nf_face.p, a.tg.p, a.gfn.p, dgX);
+  if (m.T) {
+    k_a_tet_x<128><<<grid_for(m.T, 128), 128, 0, s>>>(m.T, m.X.p, m.tets.p, m.tet_edge.p, a.geo.p, a.gvol.p, a.tg.p);
+    AEROF_LAUNCH_CHECK();
+  }
+  k_a_gather_x<<<grid_for(3 * (size_t)m.N, kAB), kAB, 0, s>>>(m.N, rec, m.X.p, m.faces.p, m.nbr_ptr.p, m.nbr_edge.p,
+                                                             m.nbr_tpos.p, a.gd.p, a.geo.p, m.nt_ptr.p, m.nt_tet.p,
+                                                             m.nf_ptr.p, m.nf_face.p, a.tg.p, a.gfn.p, dgX);
   AEROF_LAUNCH_CHECK();
 }
 

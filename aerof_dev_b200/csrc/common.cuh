@@ -311,7 +311,7 @@ struct AdjWork {
   DBuf<double> lam2;       // [N][6] w / vol in the blocked numbering (16-byte records)
   DBuf<double> gVp, gGp;   // [N][5], [N][16] in-block partial sums (blocked numbering)
   DBuf<double> spill;      // [nX][13] second-endpoint parts of block-crossing edges
-  DBuf<double> geo;        // [6][E] cotangents of edge normals and dx (original edge order)
+  DBuf<double> geo;        // [E][6] cotangents of edge normal and dx per edge (original edge order)
   DBuf<double> tg;         // [T][12] per-tet vertex coordinate cotangents
   DBuf<double> gV2, gG2;   // [N][5], [N][16] assembled cotangents, blocked numbering
 };

@@ -75,6 +75,11 @@ class ClockSampler:
             return
         self.t = threading.Thread(target=self._read, daemon=True)
         self.t.start()
+        # nvidia-smi can take a second to print its first sample on a fresh
+        # box: the timed region starts once sampling runs
+        t0 = time.time()
+        while not self.lines and self.proc.poll() is None and time.time() - t0 < 5.0:
+            time.sleep(0.01)
 
     def _read(self):
         for ln in self.proc.stdout:
@@ -83,6 +88,11 @@ class ClockSampler:
     def stop(self) -> dict:
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        # a timed region shorter than the sampling period still gets the
+        # sample that follows it
+        n0, t0 = len(self.lines), time.time()
+        while len(self.lines) == n0 and self.proc.poll() is None and time.time() - t0 < 1.0:
+            time.sleep(0.01)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)

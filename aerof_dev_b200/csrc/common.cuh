@@ -209,6 +209,7 @@ struct ResidualPipe {
   cudaEvent_t ev_pre = nullptr;      // the copies before the last stage's
   // each stage's kernels captured once as a graph, with its kernel count
   std::vector<cudaGraphExec_t> stage_exec;
+  std::vector<const void*> graph_key;   // the device buffers they were recorded with
   std::vector<long long> stage_launches;
   ~ResidualPipe() {
     for (auto e : stage_exec) cudaGraphExecDestroy(e);

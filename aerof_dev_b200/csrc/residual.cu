@@ -1402,7 +1402,14 @@ static void stage_kernels(aerof_gpu_ctx* c, ResidualPipe& p, int st, cudaStream_
 // only, so one capture serves every U and R).  False when s cannot be
 // captured (the legacy default stream, or a capture already running).
 static bool pipe_graphs(aerof_gpu_ctx* c, ResidualPipe& p, cudaStream_t s) {
-  if (!p.stage_exec.empty()) return true;
+  // the device buffers the recorded kernels name: a buffer reallocated
+  // since the capture invalidates the graphs
+  const std::vector<const void*> key = {c->s.Ustage.p, c->s.Rstage.p, c->s.G2.p,  c->s.part.p,
+                                        c->s.spill.p,  c->s.tag.p,    c->s.counters.p, c->mesh.P2.p};
+  if (!p.stage_exec.empty() && key == p.graph_key) return true;
+  for (auto e : p.stage_exec) cudaGraphExecDestroy(e);
+  p.stage_exec.clear();
+  p.stage_launches.clear();
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   AEROF_CUDA(cudaStreamIsCapturing(s, &cs));
   if (cs != cudaStreamCaptureStatusNone || s == cudaStreamLegacy || s == nullptr) return false;
@@ -1443,6 +1450,7 @@ static bool pipe_graphs(aerof_gpu_ctx* c, ResidualPipe& p, cudaStream_t s) {
   }
   p.stage_exec = ex;
   p.stage_launches = nk;
+  p.graph_key = key;
   return true;
 }
 

@@ -336,7 +336,7 @@ struct TurbWork {
   DBuf<double> d2wall;     // [N]
   DBuf<double> V6;         // [N][6] primitive
   DBuf<double> G6;         // [N][18] LSQ gradients (x, y, z of the six components)
-  DBuf<double> flux6;      // [6][E]
+  DBuf<double> flux6;      // [E][6]
   DBuf<double> fbuf6;      // [3F][6]
   DBuf<double> tetc;       // [4T][5] SA Galerkin shares of each (tet, vertex)
   DBuf<double> q;          // [N][12] node records of the SA Galerkin term

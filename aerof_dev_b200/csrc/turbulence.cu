@@ -94,8 +94,9 @@ __device__ __forceinline__ double sa_upwind(double phi1, double a, double b) {
   return phi1 * (updir * a + (1.0 - updir) * b);
 }
 
-// Roe flux of every edge into flux[6][E]; non-positive reconstructed
-// densities or pressures skip the edge and are counted.
+// Roe flux of every edge into flux[E][6] (one 48-byte record per edge);
+// non-positive reconstructed densities or pressures skip the edge and are
+// counted.
 __global__ void k_edge_flux6(int E, Gas g, int rec, double beta, const int2* __restrict__ edges,
                              const double* __restrict__ en, const double* __restrict__ V,
                              const double* __restrict__ X, const double* __restrict__ G,
@@ -133,8 +134,10 @@ __global__ void k_edge_flux6(int E, Gas g, int rec, double beta, const int2* __r
     roe_flux(g, n0, n1, n2, Vi, Vj, f);
     f[5] = sa_upwind(f[0], Vi[5], Vj[5]);
   }
-#pragma unroll
-  for (int k = 0; k < 6; ++k) flux[(size_t)k * E + l] = f[k];
+  double2* o = reinterpret_cast<double2*>(flux + 6 * (size_t)l);
+  o[0] = make_double2(f[0], f[1]);
+  o[1] = make_double2(f[2], f[3]);
+  o[2] = make_double2(f[4], f[5]);
 }
 
 // Boundary subface fluxes (normal n_f / 3) into fbuf[3F][6].
@@ -163,33 +166,38 @@ __global__ void k_face_flux6(int F, Gas g, const double* __restrict__ Ub0, const
 }
 
 // Per node: edges in ascending-neighbour order (+ first endpoint, -
-// second), boundary subfaces in face order, times 1/ctrlVol.
-__global__ void k_node_residual6(int N, int E, const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_edge,
+// second), boundary subfaces in face order, times 1/ctrlVol; three lanes
+// per node, lane c summing components 2c and 2c + 1 (16-byte loads of the
+// 48-byte edge and subface records)
+__global__ void k_node_residual6(int N, const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_edge,
                                  const double* __restrict__ flux, const int* __restrict__ nf_ptr,
                                  const int* __restrict__ nf_face, const int* __restrict__ faces,
                                  const double* __restrict__ fbuf, const double* __restrict__ vol,
                                  double* __restrict__ R) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= 3 * (long long)N) return;
+  const int i = (int)(j / 3), c = (int)(j - 3 * (long long)i);
+  double a0 = 0.0, a1 = 0.0;
   for (int p = nbr_ptr[i]; p < nbr_ptr[i + 1]; ++p) {
     const int e = nbr_edge[p];
     const size_t l = (size_t)(e & 0x7fffffff);
     const double sg = e < 0 ? -1.0 : 1.0;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) acc[k] += sg * flux[k * (size_t)E + l];
+    const double2 v = reinterpret_cast<const double2*>(flux + 6 * l)[c];
+    a0 += sg * v.x;
+    a1 += sg * v.y;
   }
   for (int q = nf_ptr[i]; q < nf_ptr[i + 1]; ++q) {
     const int f = nf_face[q];
     const int* fd = faces + 3 * (size_t)f;
     const int l = fd[0] == i ? 0 : (fd[1] == i ? 1 : 2);
-    const double* ff = fbuf + 6 * (3 * (size_t)f + l);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) acc[k] += ff[k];
+    const double2 v = reinterpret_cast<const double2*>(fbuf + 6 * (3 * (size_t)f + l))[c];
+    a0 += v.x;
+    a1 += v.y;
   }
   const double invcv = 1.0 / vol[i];
-#pragma unroll
-  for (int k = 0; k < 6; ++k) R[6 * (size_t)i + k] = acc[k] * invcv;
+  // R is the caller's array: 8-byte stores (no alignment beyond a double's)
+  R[6 * (size_t)i + 2 * c] = a0 * invcv;
+  R[6 * (size_t)i + 2 * c + 1] = a1 * invcv;
 }
 
 // P1 shape-function gradients of tet nd (ElemTet::computeGradientP1Function,
@@ -423,8 +431,9 @@ static int residual_sa_dev(aerof_gpu_ctx* c, const double* dU, double* dR) {
                                                     t.fbuf6.p);
     AEROF_LAUNCH_CHECK();
   }
-  k_node_residual6<<<grid_for(m.N, 256), 256, 0, s>>>(m.N, m.E, m.nbr_ptr.p, m.nbr_edge.p, t.flux6.p, m.nf_ptr.p,
-                                                      m.nf_face.p, m.faces.p, t.fbuf6.p, m.vol.p, dR);
+  k_node_residual6<<<grid_for(3 * (size_t)m.N, 256), 256, 0, s>>>(m.N, m.nbr_ptr.p, m.nbr_edge.p, t.flux6.p,
+                                                                  m.nf_ptr.p, m.nf_face.p, m.faces.p, t.fbuf6.p,
+                                                                  m.vol.p, dR);
   AEROF_LAUNCH_CHECK();
   if (c->visc.model != 0) {
     t.tetc.ensure(20 * (size_t)std::max(m.T, 1));

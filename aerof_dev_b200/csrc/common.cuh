@@ -504,7 +504,7 @@ void compute_geometry(aerof_gpu_ctx* c);
 // when a viscous model is set (no allocation: the per-tet buffer is sized
 // by galerkin_reserve, which set_mesh and set_viscosity call)
 void galerkin_add(aerof_gpu_ctx* c, const double* dU, double* dR);
-void galerkin_reserve(aerof_gpu_ctx* c);
+void galerkin_reserve(aerof_gpu_ctx* c, int model);
 
 // Node side of a Galerkin term evaluated once per tet: the tet kernel wrote
 // node k's share of tet t as the W-double record C[W (4t + k)]; thread

@@ -782,7 +782,7 @@ extern "C" int aerof_gpu_set_mesh(aerof_gpu_ctx* c, int N, int T, int F, const d
     AEROF_CUDA(cudaStreamSynchronize(s));
     c->n_owned = N;
     c->has_mesh = true;
-    galerkin_reserve(c);
+    galerkin_reserve(c, c->visc.model);
     return AEROF_OK;
   });
 }

@@ -154,8 +154,8 @@ __global__ void k_visc_records(int N, Gas g, const double* __restrict__ U, const
 
 // the per-tet buffer of the Galerkin term, sized at set-up so that the
 // residual calls allocate nothing
-void galerkin_reserve(aerof_gpu_ctx* c) {
-  if (c->visc.model == 0 || !c->has_mesh) return;
+void galerkin_reserve(aerof_gpu_ctx* c, int model) {
+  if (model == 0 || !c->has_mesh) return;
   c->s.tetc.ensure(16 * (size_t)std::max(c->mesh.T, 1));
   c->s.viscq.ensure(8 * (size_t)c->mesh.N);
 }
@@ -191,8 +191,9 @@ extern "C" int aerof_gpu_set_viscosity(aerof_gpu_ctx* c, const aerof_viscous_par
     if (!p || p->model < 0 || p->model > 2) return AEROF_EINVAL;
     if (p->model != 0 && !(p->reynolds_mu > 0.0 && p->prandtl > 0.0)) return AEROF_EINVAL;
     if (p->model == 2 && !(p->sutherland_alpha > 0.0 && p->sutherland_Ts >= 0.0)) return AEROF_EINVAL;
+    // the buffers first: a failed reservation leaves the previous model set
+    galerkin_reserve(c, p->model);
     c->visc = *p;
-    galerkin_reserve(c);
     c->imp.precision = 0;
     c->h2.ready = false;
     return AEROF_OK;

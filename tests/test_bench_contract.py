@@ -38,3 +38,25 @@ def test_reference_arm_only_rank0_prints():
     p = run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}, "--gpus", "2")
     assert p.returncode == 0, p.stderr
     assert not [l for l in p.stdout.splitlines() if l.startswith("{")]
+
+
+def test_clock_sampler_brackets_a_short_timed_region(tmp_path, monkeypatch):
+    # a stand-in nvidia-smi that needs half a second for its first sample
+    # and reports one throttle reason: the sampler waits for that sample
+    # before the timed region and for the one after it, so a region far
+    # shorter than the sampling period still gets a clock record
+    fake = tmp_path / "nvidia-smi"
+    fake.write_text("#!/bin/bash\nsleep 0.5\nwhile true; do "
+                    "echo '1965, 1965, 500.0, 0x4, Not Active, Not Active, Not Active, Active'; "
+                    "sleep 0.1; done\n")
+    fake.chmod(0o755)
+    monkeypatch.setenv("PATH", f"{tmp_path}:{os.environ['PATH']}")
+    sys.path.insert(0, ROOT)
+    import bench
+    c = bench.ClockSampler(None)
+    c.start()
+    assert c.lines, "the timed region must start after the first sample"
+    clk = c.stop()
+    assert clk["samples"] >= 2
+    assert clk["sm_mhz"] == 1965.0 and clk["sm_max_mhz"] == 1965.0
+    assert clk["reasons"] == ["sw_power_cap"]
